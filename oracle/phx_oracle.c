@@ -1,0 +1,890 @@
+/* Oracle: plain-C restatement of the reference's unstructured NS/SA path.
+ * TEST INFRASTRUCTURE ONLY (parity checker and CPU baseline); see
+ * phx_oracle.h.  Line citations are to the reference project's files. */
+#include "phx_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OX_SMALL 1.0e-40   /* API/Common/include/Precision.h:27 */
+#define OX_TINY 1.0e-40
+#define OX_LARGE 1.0e40
+#define OX_PI 3.141592653589793
+
+static inline double omin(double a, double b) { return a < b ? a : b; }
+static inline double omax(double a, double b) { return a > b ? a : b; }
+static inline int ntot(const ox_grid *g) { return g->n_cell + g->n_bface; }
+
+/* ------------------------------------------------------------------------ */
+/* Metrics                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* UnstructGrid::ComputeFaceCenterAreaNormal3DNew2, Geo_UnstructGrid.cpp:5911-6043:
+ * centre = node average, refined 4 times as the area-weighted centroid of the
+ * fan triangles, then normal = sum of fan cross products. */
+static void face_metrics(const ox_grid *g, ox_metrics *m)
+{
+    for (int f = 0; f < g->n_face; ++f) {
+        int b = g->face_off[f], nn = g->face_off[f + 1] - b;
+        double xc = 0, yc = 0, zc = 0;
+        for (int j = 0; j < nn; ++j) {
+            int p = g->face2node[b + j];
+            xc += g->x[p]; yc += g->y[p]; zc += g->z[p];
+        }
+        double coef = 1.0 / nn;
+        xc *= coef; yc *= coef; zc *= coef;
+        double xn = 0, yn = 0, zn = 0;
+        for (int cyc = 0; cyc < 5; ++cyc) {
+            double xt = 0, yt = 0, zt = 0, at = 0;
+            xn = yn = zn = 0;
+            for (int j = 0; j < nn; ++j) {
+                int p1 = g->face2node[b + j], p2 = g->face2node[b + (j + 1) % nn];
+                double dx1 = g->x[p1] - xc, dy1 = g->y[p1] - yc, dz1 = g->z[p1] - zc;
+                double dx2 = g->x[p2] - xc, dy2 = g->y[p2] - yc, dz2 = g->z[p2] - zc;
+                double anx = dy1 * dz2 - dy2 * dz1;
+                double any = dz1 * dx2 - dz2 * dx1;
+                double anz = dx1 * dy2 - dx2 * dy1;
+                double a = sqrt(anx * anx + any * any + anz * anz);
+                double x00 = g->x[p1] + g->x[p2] + xc;
+                double y00 = g->y[p1] + g->y[p2] + yc;
+                double z00 = g->z[p1] + g->z[p2] + zc;
+                at += a; xt += a * x00; yt += a * y00; zt += a * z00;
+                xn += anx; yn += any; zn += anz;
+            }
+            if (at > OX_SMALL) {
+                double t = 1.0 / at / 3.0;
+                xc = xt * t; yc = yt * t; zc = zt * t;
+            }
+        }
+        /* the fifth pass above is the final one of the reference: its normal
+         * sums use the centre of the fourth refinement (computed before the
+         * centre update of that same pass) */
+        double a = sqrt(xn * xn + yn * yn + zn * zn);
+        m->area[f] = a * 0.5;
+        double oa = 1.0 / (a + OX_SMALL);
+        m->xfn[f] = xn * oa; m->yfn[f] = yn * oa; m->zfn[f] = zn * oa;
+        m->xfc[f] = xc; m->yfc[f] = yc; m->zfc[f] = zc;
+    }
+}
+
+/* UnstructGrid::ComputeCellCenterVol3DNew2, Geo_UnstructGrid.cpp:6545-6819:
+ * tetra decomposition (face centre, edge, cell node-average) for volume and
+ * centroid; the centroid is kept only if it lies inside every face plane;
+ * ghost centres mirror the owner across the face. */
+static void cell_metrics(const ox_grid *g, ox_metrics *m)
+{
+    int nc = g->n_cell, nb = g->n_bface;
+    double *xcc = m->xcc, *ycc = m->ycc, *zcc = m->zcc, *vol = m->vol;
+    for (int c = 0; c < nc; ++c) {
+        int b = g->cell_off[c], nn = g->cell_off[c + 1] - b;
+        double xs = 0, ys = 0, zs = 0;
+        for (int j = 0; j < nn; ++j) {
+            int p = g->cell2node[b + j];
+            xs += g->x[p]; ys += g->y[p]; zs += g->z[p];
+        }
+        xcc[c] = xs / nn; ycc[c] = ys / nn; zcc[c] = zs / nn;
+    }
+    double *xt = calloc(nc, sizeof(double)), *yt = calloc(nc, sizeof(double)), *zt = calloc(nc, sizeof(double));
+    for (int c = 0; c < nc; ++c) vol[c] = 0.0;
+    for (int f = 0; f < g->n_face; ++f) {
+        int b = g->face_off[f], nn = g->face_off[f + 1] - b;
+        int le = g->left[f], re = g->right[f];
+        for (int j = 0; j < nn; ++j) {
+            int p2 = g->face2node[b + j], p3 = g->face2node[b + (j + 1) % nn];
+            double x21 = g->x[p2] - m->xfc[f], y21 = g->y[p2] - m->yfc[f], z21 = g->z[p2] - m->zfc[f];
+            double x31 = g->x[p3] - m->xfc[f], y31 = g->y[p3] - m->yfc[f], z31 = g->z[p3] - m->zfc[f];
+            double nx = y21 * z31 - y31 * z21;
+            double ny = z21 * x31 - z31 * x21;
+            double nz = x21 * y31 - x31 * y21;
+            double x41 = xcc[le] - m->xfc[f], y41 = ycc[le] - m->yfc[f], z41 = zcc[le] - m->zfc[f];
+            double xc = m->xfc[f] + g->x[p2] + g->x[p3] + xcc[le];
+            double yc = m->yfc[f] + g->y[p2] + g->y[p3] + ycc[le];
+            double zc = m->zfc[f] + g->z[p2] + g->z[p3] + zcc[le];
+            double tmp = -(nx * x41 + ny * y41 + nz * z41);
+            xt[le] += xc * tmp; yt[le] += yc * tmp; zt[le] += zc * tmp; vol[le] += tmp;
+            if (f >= nb) {
+                x41 = xcc[re] - m->xfc[f]; y41 = ycc[re] - m->yfc[f]; z41 = zcc[re] - m->zfc[f];
+                xc = m->xfc[f] + g->x[p2] + g->x[p3] + xcc[re];
+                yc = m->yfc[f] + g->y[p2] + g->y[p3] + ycc[re];
+                zc = m->zfc[f] + g->z[p2] + g->z[p3] + zcc[re];
+                tmp = nx * x41 + ny * y41 + nz * z41;
+                xt[re] += xc * tmp; yt[re] += yc * tmp; zt[re] += zc * tmp; vol[re] += tmp;
+            }
+        }
+    }
+    for (int c = 0; c < nc; ++c) {
+        double tmp = 1.0 / (4.0 * vol[c] + OX_SMALL);
+        xt[c] *= tmp; yt[c] *= tmp; zt[c] *= tmp;
+        vol[c] /= 6.0;
+    }
+    char *mark = malloc(nc);
+    memset(mark, 1, nc);
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = g->right[f];
+        double d = (xt[le] - m->xfc[f]) * m->xfn[f] + (yt[le] - m->yfc[f]) * m->yfn[f] + (zt[le] - m->zfc[f]) * m->zfn[f];
+        if (d > 0.0) mark[le] = 0;
+        if (f >= nb) {
+            d = (xt[re] - m->xfc[f]) * m->xfn[f] + (yt[re] - m->yfc[f]) * m->yfn[f] + (zt[re] - m->zfc[f]) * m->zfn[f];
+            if (d < 0.0) mark[re] = 0;
+        }
+    }
+    for (int c = 0; c < nc; ++c)
+        if (mark[c]) { xcc[c] = xt[c]; ycc[c] = yt[c]; zcc[c] = zt[c]; }
+    free(mark); free(xt); free(yt); free(zt);
+    for (int f = 0; f < nb; ++f) {
+        int le = g->left[f], re = nc + f;
+        if (m->area[f] > OX_SMALL) {
+            double tmp = 2.0 * ((xcc[le] - m->xfc[f]) * m->xfn[f] + (ycc[le] - m->yfc[f]) * m->yfn[f] +
+                                (zcc[le] - m->zfc[f]) * m->zfn[f]);
+            xcc[re] = xcc[le] - m->xfn[f] * tmp;
+            ycc[re] = ycc[le] - m->yfn[f] * tmp;
+            zcc[re] = zcc[le] - m->zfn[f] * tmp;
+        } else {
+            xcc[re] = -xcc[le] + 2.0 * m->xfc[f];
+            ycc[re] = -ycc[le] + 2.0 * m->yfc[f];
+            zcc[re] = -zcc[le] + 2.0 * m->zfc[f];
+        }
+        vol[re] = vol[le];
+    }
+}
+
+/* UnstructGrid::SkewnessSummary, Geo_UnstructGrid.cpp:2206-2330. */
+static void skewness(const ox_grid *g, ox_metrics *m)
+{
+    int nc = g->n_cell, nb = g->n_bface;
+    for (int c = 0; c < nc; ++c) m->skew[c] = 180.0;
+    for (int f = nb; f < g->n_face; ++f) {
+        if (m->area[f] <= OX_TINY) continue;
+        int le = g->left[f], re = g->right[f];
+        double x1 = m->xfc[f] - m->xcc[le], y1 = m->yfc[f] - m->ycc[le], z1 = m->zfc[f] - m->zcc[le];
+        double d1 = sqrt(x1 * x1 + y1 * y1 + z1 * z1);
+        double p1 = (m->xfn[f] * x1 + m->yfn[f] * y1 + m->zfn[f] * z1) / (d1 + OX_TINY);
+        if (p1 > 1.0) p1 = 1.0;
+        if (p1 < -1.0) p1 = -1.0;
+        double x2 = m->xcc[re] - m->xfc[f], y2 = m->ycc[re] - m->yfc[f], z2 = m->zcc[re] - m->zfc[f];
+        double d2 = sqrt(x2 * x2 + y2 * y2 + z2 * z2);
+        double p2 = (m->xfn[f] * x2 + m->yfn[f] * y2 + m->zfn[f] * z2) / (d2 + OX_TINY);
+        if (p2 > 1.0) p2 = 1.0;
+        if (p2 < -1.0) p2 = -1.0;
+        double ang = omin(asin(p1), asin(p2)) * 180.0 / OX_PI;
+        m->skew[le] = omin(m->skew[le], ang);
+        m->skew[re] = omin(m->skew[re], ang);
+    }
+    for (int f = 0; f < nb; ++f) {
+        if (m->area[f] <= OX_TINY) continue;
+        int le = g->left[f];
+        double x1 = m->xfc[f] - m->xcc[le], y1 = m->yfc[f] - m->ycc[le], z1 = m->zfc[f] - m->zcc[le];
+        double d1 = sqrt(x1 * x1 + y1 * y1 + z1 * z1);
+        double p1 = (m->xfn[f] * x1 + m->yfn[f] * y1 + m->zfn[f] * z1) / (d1 + OX_TINY);
+        if (p1 > 1.0) p1 = 1.0;
+        if (p1 < -1.0) p1 = -1.0;
+        m->skew[le] = omin(m->skew[le], asin(p1) * 180.0 / OX_PI);
+    }
+}
+
+void ox_compute_metrics(const ox_grid *g, ox_metrics *m)
+{
+    face_metrics(g, m);
+    cell_metrics(g, m);
+    skewness(g, m);
+    double s = 0.0;
+    for (int c = 0; c < g->n_cell; ++c) s += m->vol[c];
+    m->avg_vol = s / (double)g->n_cell;
+    /* UnstructGrid::ComputeCell2Face, Geo_UnstructGrid.cpp:1246-1290: faces in
+     * ascending index order per cell. */
+    if (m->c2f_off && m->c2f) {
+        int nc = g->n_cell;
+        int *cnt = calloc(nc + 1, sizeof(int));
+        for (int f = 0; f < g->n_face; ++f) {
+            cnt[g->left[f]]++;
+            if (f >= g->n_bface) cnt[g->right[f]]++;
+        }
+        m->c2f_off[0] = 0;
+        for (int c = 0; c < nc; ++c) m->c2f_off[c + 1] = m->c2f_off[c] + cnt[c];
+        for (int c = 0; c < nc; ++c) cnt[c] = m->c2f_off[c];
+        for (int f = 0; f < g->n_face; ++f) {
+            m->c2f[cnt[g->left[f]]++] = f;
+            if (f >= g->n_bface) m->c2f[cnt[g->right[f]]++] = f;
+        }
+        free(cnt);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Boundary conditions (NSSolverUnstruct::Boundary, NSSolverUnstruct.cpp:13404-13515) */
+/* ------------------------------------------------------------------------ */
+
+/* SymmetryBCRegion, NSSolverUnstruct.cpp:19413-19455 (also inviscid walls). */
+static void bc_symmetry(const ox_grid *g, const ox_metrics *m, int f, double *q, int nt)
+{
+    int le = g->left[f], re = g->n_cell + f;
+    for (int k = 0; k < 5; ++k) q[k * nt + re] = q[k * nt + le];
+    double uL = q[1 * nt + le], vL = q[2 * nt + le], wL = q[3 * nt + le];
+    double vn = m->xfn[f] * uL + m->yfn[f] * vL + m->zfn[f] * wL;
+    q[1 * nt + re] = uL - 2.0 * m->xfn[f] * vn;
+    q[2 * nt + re] = vL - 2.0 * m->yfn[f] * vn;
+    q[3 * nt + re] = wL - 2.0 * m->zfn[f] * vn;
+}
+
+/* ViscousAdiabaticWallBCRegion, NSSolverUnstruct.cpp:20988-21060 (no-slip,
+ * static wall): ghost velocity is the reflection -u, density and pressure
+ * copied. */
+static void bc_adiabatic_wall(const ox_grid *g, int f, double *q, int nt)
+{
+    int le = g->left[f], re = g->n_cell + f;
+    q[0 * nt + re] = q[0 * nt + le];
+    q[1 * nt + re] = -q[1 * nt + le];
+    q[2 * nt + re] = -q[2 * nt + le];
+    q[3 * nt + re] = -q[3 * nt + le];
+    q[4 * nt + re] = q[4 * nt + le];
+}
+
+/* FarfieldBCRegion, NSSolverUnstruct.cpp:21195-21330 (Riemann invariants). */
+static void bc_farfield(const ox_grid *g, const ox_metrics *m, const ox_params *p, int f, double *q,
+                        const double *gama, int nt)
+{
+    int le = g->left[f], re = g->n_cell + f;
+    const double *pi = p->prim_inf;
+    double rO = pi[0], uO = pi[1], vO = pi[2], wO = pi[3], pO = pi[4];
+    double cO = sqrt(fabs(p->gama * pO / rO));
+    double xn = m->xfn[f], yn = m->yfn[f], zn = m->zfn[f];
+    for (int k = 0; k < 5; ++k) q[k * nt + re] = q[k * nt + le];
+    double rI = q[le], uI = q[nt + le], vI = q[2 * nt + le], wI = q[3 * nt + le], pI = q[4 * nt + le];
+    double vnO = xn * uO + yn * vO + zn * wO;
+    double vnI = xn * uI + yn * vI + zn * wI;
+    double gl = gama[le];
+    double cI = sqrt(fabs(gl * pI / rI));
+    double gm1 = gl - 1.0;
+    double velI = sqrt(uI * uI + vI * vI + wI * wI);
+    if (velI > cI) {
+        if (vnI < 0.0)
+            for (int k = 0; k < 5; ++k) q[k * nt + re] = pi[k];
+        return;
+    }
+    double Rp = vnI + 2.0 * cI / gm1;
+    double Rm = vnO - 2.0 * cO / gm1;
+    double vnB = 0.5 * (Rp + Rm);
+    double cB = 0.25 * (Rp - Rm) * gm1;
+    double s, vtx, vty, vtz;
+    if (vnB >= 0.0) {
+        s = pI / pow(rI, gl);
+        vtx = uI - xn * vnI; vty = vI - yn * vnI; vtz = wI - zn * vnI;
+    } else {
+        s = pO / pow(rO, gl);
+        vtx = uO - xn * vnO; vty = vO - yn * vnO; vtz = wO - zn * vnO;
+    }
+    double rB = pow((cB * cB / (s * gl)), 1.0 / gm1);
+    q[0 * nt + re] = rB;
+    q[1 * nt + re] = vtx + xn * vnB;
+    q[2 * nt + re] = vty + yn * vnB;
+    q[3 * nt + re] = vtz + zn * vnB;
+    q[4 * nt + re] = cB * cB * rB / gl;
+}
+
+static int is_wall(int t) { return t == OX_BC_SOLID_SURFACE; }
+
+void ox_ns_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, double *q, const double *gama)
+{
+    int nt = ntot(g);
+    /* Regions are visited in region order; faces within a region in face order.
+     * A face belongs to exactly one region, so visiting faces directly is
+     * equivalent. */
+    for (int f = 0; f < g->n_bface; ++f) {
+        int t = g->region_type[g->bface_region[f]];
+        if (is_wall(t)) {
+            if (!p->viscous) bc_symmetry(g, m, f, q, nt);
+            else bc_adiabatic_wall(g, f, q, nt);
+        } else if (t == OX_BC_SYMMETRY) {
+            bc_symmetry(g, m, f, q, nt);
+        } else if (t == OX_BC_FARFIELD) {
+            bc_farfield(g, m, p, f, q, gama, nt);
+        } else {
+            /* extrapolation / outflow: ghost copies the owner */
+            int le = g->left[f], re = g->n_cell + f;
+            for (int k = 0; k < 5; ++k) q[k * nt + re] = q[k * nt + le];
+        }
+    }
+}
+
+/* NSSolverUnstruct::ComputeGamaAndTemperature, NSSolverUnstruct.cpp:4717-4730. */
+void ox_gamma_temperature(const ox_grid *g, const ox_params *p, const double *q, double *gama, double *t)
+{
+    int nt = ntot(g);
+    for (int c = 0; c < nt; ++c) {
+        gama[c] = p->gama;
+        t[c] = q[4 * nt + c] / (p->coef_state * q[c]);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Gradient                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* UnstructGrid::CompGradientGGCell, Geo_UnstructGrid.cpp:3220-3284: ghost
+ * gradients stay zero. */
+static void gradient_ggcell(const ox_grid *g, const ox_metrics *m, const double *q, double *dx, double *dy,
+                            double *dz)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int c = 0; c < nt; ++c) dx[c] = dy[c] = dz[c] = 0.0;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double qf = 0.5 * (q[le] + q[re]);
+        double nx = m->xfn[f] * m->area[f], ny = m->yfn[f] * m->area[f], nz = m->zfn[f] * m->area[f];
+        dx[le] += qf * nx; dy[le] += qf * ny; dz[le] += qf * nz;
+        if (f >= nb) { dx[re] -= qf * nx; dy[re] -= qf * ny; dz[re] -= qf * nz; }
+    }
+    for (int c = 0; c < nc; ++c) {
+        double ov = 1.0 / m->vol[c];
+        dx[c] *= ov; dy[c] *= ov; dz[c] *= ov;
+    }
+}
+
+void ox_gradient(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *f,
+                 double *dfdx, double *dfdy, double *dfdz)
+{
+    (void)p;
+    gradient_ggcell(g, m, f, dfdx, dfdy, dfdz);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Limiter                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* VenFun, API/Math/include/Math_Limiter.h:174-180. */
+static inline double venfun(double x, double y, double eps)
+{
+    double x2 = x * x, xy = x * y, y2 = y * y;
+    return (x2 + eps + 2.0 * xy) / (x2 + 2.0 * y2 + xy + eps);
+}
+
+/* Limiter::MinMaxDiff, Limiter.cpp:1202-1252 (boundary faces excluded). */
+static void minmaxdiff(const ox_grid *g, const double *q, double *dmin, double *dmax)
+{
+    int nc = g->n_cell;
+    for (int c = 0; c < nc; ++c) dmin[c] = dmax[c] = q[c];
+    for (int f = g->n_bface; f < g->n_face; ++f) {
+        int le = g->left[f], re = g->right[f];
+        dmin[le] = omin(dmin[le], q[re]); dmax[le] = omax(dmax[le], q[re]);
+        dmin[re] = omin(dmin[re], q[le]); dmax[re] = omax(dmax[re], q[le]);
+    }
+    for (int c = 0; c < nc; ++c) { dmin[c] -= q[c]; dmax[c] -= q[c]; }
+}
+
+/* Limiter::VencatLimiter7, Limiter.cpp:1091-1200 (3-D: n = 3). */
+static void vencat7(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                    const double *dqdx, const double *dqdy, const double *dqdz, double *limit)
+{
+    int nc = g->n_cell, nb = g->n_bface;
+    double *dmin = malloc(sizeof(double) * nc), *dmax = malloc(sizeof(double) * nc);
+    double *eps = malloc(sizeof(double) * nc);
+    minmaxdiff(g, q, dmin, dmax);
+    double K = p->venkat_coeff;
+    double eps_tmp = K * K * K;
+    eps_tmp *= 1.0 / pow(pow(m->avg_vol, 1.0 / 3.0), 3.0);
+    for (int c = 0; c < nc; ++c) {
+        eps[c] = eps_tmp * q[c] * q[c];
+        eps[c] *= pow(pow(m->vol[c], 1.0 / 3.0), 3.0);
+    }
+    for (int f = 0; f < g->n_face; ++f) {
+        for (int side = 0; side < (f < nb ? 1 : 2); ++side) {
+            int c = side == 0 ? g->left[f] : g->right[f];
+            double dx = m->xfc[f] - m->xcc[c], dy = m->yfc[f] - m->ycc[c], dz = m->zfc[f] - m->zcc[c];
+            double dqf = dqdx[c] * dx + dqdy[c] * dy + dqdz[c] * dz;
+            if (dqf > OX_SMALL) limit[c] = omin(limit[c], venfun(dmax[c], dqf, eps[c]));
+            else if (dqf < -OX_SMALL) limit[c] = omin(limit[c], venfun(dmin[c], dqf, eps[c]));
+        }
+    }
+    free(dmin); free(dmax); free(eps);
+}
+
+/* NSSolverUnstruct::ComputeLimiter (NSSolverUnstruct.cpp:18189-18240) with a
+ * scalar Venkatakrishnan limiter from rho and p (limitVariables=0,
+ * limitVector=0, Limiter.cpp:91-135), then SetLimitBoundary
+ * (Geo_UnstructGrid.cpp:10744-10775): zero on both sides of far-field /
+ * inflow faces.  `limit` holds nTotal values. */
+void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                const double *dqdx, const double *dqdy, const double *dqdz, double *limit)
+{
+    int nt = ntot(g);
+    for (int c = 0; c < nt; ++c) limit[c] = 1.0;
+    if (p->limiter == 0) return;
+    vencat7(g, m, p, q, dqdx, dqdy, dqdz, limit);
+    vencat7(g, m, p, q + 4 * nt, dqdx + 4 * nt, dqdy + 4 * nt, dqdz + 4 * nt, limit);
+    for (int f = 0; f < g->n_bface; ++f) {
+        int t = g->region_type[g->bface_region[f]];
+        if (t != OX_BC_SYMMETRY && !is_wall(t) && t != OX_BC_OUTFLOW) {
+            limit[g->left[f]] = 0.0;
+            limit[g->n_cell + f] = 0.0;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Inviscid flux                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Harten fix, API/Physics/include/Flux_RoeEntropyCorrection.h:66-74. */
+static inline double harten(double e, double lim)
+{
+    double a = fabs(e);
+    if (a < lim) a = 0.5 * (e * e + lim * lim) / lim;
+    return a;
+}
+
+/* Roe_Scheme_ConservativeForm, API/Physics/src/Flux_Inviscid.cpp:136-399
+ * (perfect gas, no preconditioning, static grid), with the entropy fix of
+ * Flux_RoeEntropyCorrection method 3 (Flux_RoeEntropyCorrection.cpp:126-135).
+ * Returns the flux per unit area in f[5]. */
+static void roe_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                     double zsn, double acoustic, double convective, double *f)
+{
+    const double LITTLE = 1.0e-10;
+    double rL = omax(ql[0], LITTLE), uL = ql[1], vL = ql[2], wL = ql[3], pL = omax(ql[4], LITTLE);
+    double rR = omax(qr[0], LITTLE), uR = qr[1], vR = qr[2], wR = qr[3], pR = omax(qr[4], LITTLE);
+    double v2L = uL * uL + vL * vL + wL * wL;
+    double v2R = uR * uR + vR * vR + wR * wR;
+    double hL = (gl / (gl - 1.0)) * (pL / rL) + 0.5 * v2L;
+    double hR = (gr / (gr - 1.0)) * (pR / rR) + 0.5 * v2R;
+    double vnL = xsn * uL + ysn * vL + zsn * wL;
+    double vnR = xsn * uR + ysn * vR + zsn * wR;
+    double rvnL = rL * vnL, rvnR = rR * vnR;
+    f[0] = 0.5 * (rvnL + rvnR);
+    f[1] = 0.5 * (rvnL * uL + xsn * pL + rvnR * uR + xsn * pR);
+    f[2] = 0.5 * (rvnL * vL + ysn * pL + rvnR * vR + ysn * pR);
+    f[3] = 0.5 * (rvnL * wL + zsn * pL + rvnR * wR + zsn * pR);
+    f[4] = 0.5 * (rvnL * hL + rvnR * hR);
+    double ratio = sqrt(rR / rL);
+    double coef = 1.0 / (1.0 + ratio);
+    double um = (uL + uR * ratio) * coef;
+    double vm = (vL + vR * ratio) * coef;
+    double wm = (wL + wR * ratio) * coef;
+    double pm = (pL + pR * ratio) * coef;
+    double rm = sqrt(rL * rR);
+    double gama = (gl + gr * ratio) * coef;
+    double gm1 = gama - 1.0;
+    double v2 = um * um + vm * vm + wm * wm;
+    double absv = sqrt(v2);
+    double hm = gama / gm1 * pm / rm + 0.5 * v2;
+    double vn = xsn * um + ysn * vm + zsn * wm;
+    double theta = vn;
+    double c2 = gm1 * (hm - 0.5 * v2);
+    double cm = sqrt(fabs(c2));
+    double e1 = fabs(vn), e2 = fabs(vn + cm), e3 = fabs(vn - cm);
+    (void)absv;
+    double EL = (1.0 / (gl - 1.0)) * (pL / rL) + 0.5 * v2L;
+    double ER = (1.0 / (gr - 1.0)) * (pR / rR) + 0.5 * v2R;
+    double dq0 = rR - rL, dq1 = rR * uR - rL * uL, dq2 = rR * vR - rL * vL, dq3 = rR * wR - rL * wL;
+    double dq4 = rR * ER - rL * EL;
+    double maxe = fabs(vn) + cm;
+    e1 = harten(e1, convective * maxe);
+    e2 = harten(e2, acoustic * maxe);
+    e3 = harten(e3, acoustic * maxe);
+    double xi1 = (2.0 * e1 - e2 - e3) / (2.0 * c2);
+    double xi2 = (e2 - e3) / (2.0 * cm);
+    double dc = theta * dq0 - xsn * dq1 - ysn * dq2 - zsn * dq3;
+    double c2dc = c2 * dc;
+    double dh = -gm1 * (um * dq1 + vm * dq2 + wm * dq3 - dq4) + 0.5 * gm1 * v2 * dq0;
+    f[0] -= 0.5 * (e1 * dq0 - dh * xi1 - dc * xi2);
+    f[1] -= 0.5 * (e1 * dq1 + (xsn * c2dc - um * dh) * xi1 + (xsn * dh - um * dc) * xi2);
+    f[2] -= 0.5 * (e1 * dq2 + (ysn * c2dc - vm * dh) * xi1 + (ysn * dh - vm * dc) * xi2);
+    f[3] -= 0.5 * (e1 * dq3 + (zsn * c2dc - wm * dh) * xi1 + (zsn * dh - wm * dc) * xi2);
+    f[4] -= 0.5 * (e1 * dq4 + (theta * c2dc - hm * dh) * xi1 + (theta * dh - hm * dc) * xi2);
+}
+
+/* PositiveCheckForDensityAndPressure: rho > 0 and p > 0. */
+static inline int positive(const double *q) { return q[0] > 0.0 && q[4] > 0.0; }
+
+/* NSSolverUnstruct::InviscidFlux (NSSolverUnstruct.cpp:6912-6973): per face
+ * GetQlQr / GetGamaLR (5507-5571), ReConstructFaceValue (13991-14193),
+ * BoundaryQlQrFix (13725-13951), the scheme times the face area
+ * (InviscidFluxWrap, 14466-14488), LoadFlux (6435-6495).  res is
+ * accumulated (callers zero it first, as Controller::LoadResiduals does). */
+void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                      const double *gama, const double *dqdx, const double *dqdy, const double *dqdz,
+                      const double *limit, double *res)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double ql[5], qr[5], tr[5];
+        for (int k = 0; k < 5; ++k) { ql[k] = q[k * nt + le]; qr[k] = q[k * nt + re]; }
+        if (p->limiter != 0 || 1) {
+            double lim_l = limit[le], lim_r = limit[re];
+            if (p->recon_method == 1) lim_l = lim_r = omin(limit[le], limit[re]);
+            double dx = m->xfc[f] - m->xcc[le], dy = m->yfc[f] - m->ycc[le], dz = m->zfc[f] - m->zcc[le];
+            for (int k = 0; k < 5; ++k)
+                tr[k] = ql[k] + lim_l * (dqdx[k * nt + le] * dx + dqdy[k * nt + le] * dy + dqdz[k * nt + le] * dz);
+            if (positive(tr)) for (int k = 0; k < 5; ++k) ql[k] = tr[k];
+            dx = m->xfc[f] - m->xcc[re]; dy = m->yfc[f] - m->ycc[re]; dz = m->zfc[f] - m->zcc[re];
+            for (int k = 0; k < 5; ++k)
+                tr[k] = qr[k] + lim_r * (dqdx[k * nt + re] * dx + dqdy[k * nt + re] * dy + dqdz[k * nt + re] * dz);
+            if (positive(tr)) for (int k = 0; k < 5; ++k) qr[k] = tr[k];
+        }
+        double xn = m->xfn[f], yn = m->yfn[f], zn = m->zfn[f];
+        if (f < nb) {
+            int t = g->region_type[g->bface_region[f]];
+            if (t == OX_BC_SOLID_SURFACE || t == OX_BC_SYMMETRY) {
+                for (int k = 0; k < 5; ++k) { double a = 0.5 * (q[k * nt + le] + q[k * nt + re]); ql[k] = qr[k] = a; }
+                if (t == OX_BC_SYMMETRY) {
+                    double vn = 2.0 * (xn * ql[1] + yn * ql[2] + zn * ql[3]);
+                    qr[1] = ql[1] - vn * xn; qr[2] = ql[2] - vn * yn; qr[3] = ql[3] - vn * zn;
+                } else if (p->viscous) {
+                    ql[1] = ql[2] = ql[3] = 0.0;
+                    qr[1] = qr[2] = qr[3] = 0.0;
+                }
+            }
+        }
+        double fl[5];
+        roe_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->entropy_acoustic, p->entropy_convective, fl);
+        for (int k = 0; k < 5; ++k) {
+            double fa = fl[k] * m->area[f];
+            res[k * nt + le] -= fa;
+            if (f >= nb) res[k * nt + re] += fa;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Spectral radius and time step                                             */
+/* ------------------------------------------------------------------------ */
+
+/* SpectrumRadiusInviscid, NSSolverUnstruct.cpp:5749-5850; the viscous part
+ * (SpectrumRadiusViscous, 5852-5940) is added for viscous runs. */
+void ox_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                 const double *gama, const double *visl, const double *vist, double *inv_spec, double *vis_spec)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int c = 0; c < nc; ++c) { inv_spec[c] = 0.0; if (vis_spec) vis_spec[c] = 0.0; }
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double xn = m->xfn[f], yn = m->yfn[f], zn = m->zfn[f];
+        double vnl = xn * q[nt + le] + yn * q[2 * nt + le] + zn * q[3 * nt + le];
+        double vnr = xn * q[nt + re] + yn * q[2 * nt + re] + zn * q[3 * nt + re];
+        double gm = 0.5 * (gama[le] + gama[re]);
+        double pm = 0.5 * (q[4 * nt + le] + q[4 * nt + re]);
+        double rm = 0.5 * (q[le] + q[re]);
+        double vn = 0.5 * (vnl + vnr);
+        double cm = sqrt(gm * pm / rm);
+        double s = 0.5 * m->area[f] * (fabs(vn) + cm);
+        inv_spec[le] += s;
+        if (re < nc) inv_spec[re] += s;
+    }
+    (void)p; (void)visl; (void)vist;
+}
+
+/* NSSolver::ComputeCFL, CFD/NSSolver/src/NSSolver.cpp:595-668 (cflMethod 0,
+ * single grid level: the outer step drives the ramp). */
+double ox_cfl(const ox_params *p, int step)
+{
+    if (step >= p->cfl_vary_step) return p->cfl_end;
+    return p->cfl_start + (p->cfl_end - p->cfl_start) * step / p->cfl_vary_step;
+}
+
+/* LocalTimeStep + LimitCFL (NSSolverUnstruct.cpp:5999-6118),
+ * Controller::ComputeMinTimeStep / ReduceMaxTimeStep (Controller.cpp:706-788,
+ * NSSolverUnstruct.cpp:5696-5745): dt = CFL_cell vol / spec, clamped to
+ * ktmax * min(dt), divided by vol; ghosts copy the owner. */
+void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
+                 const double *inv_spec, const double *vis_spec, double *dt)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    double cfl = ox_cfl(p, step);
+    double plo = 0.001 * p->p_total, phi = 0.02 * p->p_total;
+    double mindt = OX_LARGE;
+    for (int c = 0; c < nc; ++c) {
+        double cc = cfl;
+        double pc = q[4 * nt + c];
+        if (pc < plo) cc = p->cfl_start;
+        else if (pc < phi) cc = (pc - phi) * (cfl - p->cfl_start) / (phi - plo) + cfl;
+        if (m->skew[c] < 0.1) cc *= 0.1;
+        else if (m->skew[c] < 10.0) cc *= (1.0 - exp(0.0 - m->skew[c]));
+        double spec = inv_spec[c];
+        if (p->viscous) spec += vis_spec[c];
+        dt[c] = cc * m->vol[c] / spec;
+        mindt = omin(mindt, dt[c]);
+    }
+    for (int c = 0; c < nc; ++c) {
+        if (p->ktmax > 0) dt[c] = omin(dt[c], p->ktmax * mindt);
+        dt[c] /= m->vol[c];
+    }
+    for (int f = 0; f < g->n_bface; ++f) dt[nc + f] = dt[g->left[f]];
+}
+
+/* ------------------------------------------------------------------------ */
+/* LU-SGS                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* RoeAveragedVariables, API/Physics/src/Flux_Inviscid.cpp:15440-15465. */
+static void roe_average(const double *a, double ga, const double *b, double gb, double *o)
+{
+    double hL = ga / (ga - 1.0) * a[4] / a[0] + 0.5 * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+    double hR = gb / (gb - 1.0) * b[4] / b[0] + 0.5 * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]);
+    double t0 = sqrt(b[0] / a[0]);
+    double t1 = 1.0 / (1.0 + t0);
+    o[0] = sqrt(b[0] * a[0]);
+    o[1] = (a[1] + b[1] * t0) * t1;
+    o[2] = (a[2] + b[2] * t0) * t1;
+    o[3] = (a[3] + b[3] * t0) * t1;
+    double hm = (hL + hR * t0) * t1;
+    o[4] = o[0] * (hm - 0.5 * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3])) * (ga - 1.0) / ga;
+}
+
+/* MXDQ_STD, API/Physics/src/Jacobian.cpp:13-86 (static grid, ipn = -1) with
+ * PerfectGas::ComputeTotalEnthalpyAndDH (PerfectGas.cpp:368-395). */
+static void mxdq(const double *prim, double nx, double ny, double nz, double area, double gama,
+                 const double *dq, double *f, double radius)
+{
+    double rm = prim[0], um = prim[1], vm = prim[2], wm = prim[3], pm = prim[4];
+    double c2 = fabs(gama * pm / rm);
+    double cm = sqrt(c2);
+    double cits = nx * um + ny * vm + nz * wm;
+    double ipnrad = -radius / omax(OX_SMALL, area);
+    double l1 = 0.5 * (cits + ipnrad);
+    double l2 = 0.5 * (cits + cm + ipnrad);
+    double l3 = 0.5 * (cits - cm + ipnrad);
+    double x1 = (l1 + l1 - l2 - l3) / (c2 + c2);
+    double x2 = (l2 - l3) / (cm + cm);
+    double dc = cits * dq[0] - nx * dq[1] - ny * dq[2] - nz * dq[3];
+    double c2dc = c2 * dc;
+    double v2 = um * um + vm * vm + wm * wm;
+    double g1 = gama - 1.0;
+    double dh = -g1 * (um * dq[1] + vm * dq[2] + wm * dq[3] - dq[4]);
+    dh += 0.5 * g1 * v2 * dq[0];
+    double hm = (gama / g1) * (pm / rm) + 0.5 * v2;
+    double a = dh * x1 + dc * x2;
+    double b = c2dc * x1 + dh * x2;
+    f[0] = (l1 * dq[0] - a) * area;
+    f[1] = (l1 * dq[1] - um * a + nx * b) * area;
+    f[2] = (l1 * dq[2] - vm * a + ny * b) * area;
+    f[3] = (l1 * dq[3] - wm * a + nz * b) * area;
+    f[4] = (l1 * dq[4] - hm * a + cits * b) * area;
+}
+
+/* Contribution of the neighbour across face f to the sweep of cell c
+ * (SolveLUSGSForward body, NSSolverUnstruct.cpp:15251-15370). */
+static void lusgs_face(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                       const double *gama, const double *visl, const double *vist, const double *dq, int c, int f,
+                       double *df)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+    double nx = m->xfn[f], ny = m->yfn[f], nz = m->zfn[f];
+    if (re == c) { int s = le; le = re; re = s; nx = -nx; ny = -ny; nz = -nz; }
+    double ql[5], qn[5], dqn[5], fp[5];
+    for (int k = 0; k < 5; ++k) { ql[k] = q[k * nt + le]; qn[k] = q[k * nt + re]; dqn[k] = dq[k * nt + re]; }
+    roe_average(ql, gama[le], qn, gama[re], fp);
+    double gm = gama[re];
+    double vn = nx * fp[1] + ny * fp[2] + nz * fp[3];
+    double rad = (fabs(vn) + sqrt(gm * fp[4] / fp[0])) * m->area[f];
+    mxdq(qn, nx, ny, nz, m->area[f], gm, dqn, df, rad);
+    if (p->viscous) {
+        double dist = fabs(m->xfn[f] * (m->xcc[re] - m->xcc[le]) + m->yfn[f] * (m->ycc[re] - m->ycc[le]) +
+                           m->zfn[f] * (m->zcc[re] - m->zcc[le]));
+        double mul = 0.5 * (visl[le] + visl[re]);
+        double mut = 0.5 * (vist[le] + vist[re]);
+        double rho = 0.5 * (q[le] + q[re]);
+        double vs = 2.0 * (mul + mut) / (rho * dist * p->reynolds + OX_SMALL);
+        vs *= 0.5 * m->area[f];
+        for (int k = 0; k < 5; ++k) df[k] -= vs * dqn[k];
+    }
+}
+
+/* SetGhostDQLUSGS (NSSolverUnstruct.cpp:14767-14810) with
+ * SetSymmBCGhostDQLUSGS (14812-14915) and SetWallBCGhostDQLUSGS (14917-15006);
+ * far field: zero. */
+static void ghost_dq(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                     const double *gama, double *dq)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    for (int f = 0; f < g->n_bface; ++f) {
+        int t = g->region_type[g->bface_region[f]];
+        int le = g->left[f], re = nc + f;
+        if (t == OX_BC_SYMMETRY || (is_wall(t) && !p->viscous)) {
+            double r = q[le], u = q[nt + le], v = q[2 * nt + le], w = q[3 * nt + le], pp = q[4 * nt + le];
+            double em = (pp / r) / (gama[le] - 1.0) + 0.5 * (u * u + v * v + w * w);
+            double Q[5] = {r, r * u, r * v, r * w, r * em};
+            for (int k = 0; k < 5; ++k) Q[k] += dq[k * nt + le];
+            double rm = q[re], um = q[nt + re], vm = q[2 * nt + re], wm = q[3 * nt + re], pm = q[4 * nt + re];
+            double xn = m->xfn[f], yn = m->yfn[f], zn = m->zfn[f];
+            dq[re] = dq[le];
+            double rvn = 2.0 * (xn * dq[nt + le] + yn * dq[2 * nt + le] + zn * dq[3 * nt + le]);
+            dq[nt + re] = dq[nt + le] - xn * rvn;
+            dq[2 * nt + re] = dq[2 * nt + le] - yn * rvn;
+            dq[3 * nt + re] = dq[3 * nt + le] - zn * rvn;
+            rvn = 2.0 * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
+            double ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
+            double pnew = Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
+            double g1 = gama[le] - 1.0;
+            dq[4 * nt + re] = pnew - pm / g1 + 0.5 * ((ru * ru + rv * rv + rw * rw) / Q[0] - rm * (um * um + vm * vm + wm * wm));
+        } else if (is_wall(t)) {
+            dq[re] = dq[le];
+            dq[nt + re] = -dq[nt + le];
+            dq[2 * nt + re] = -dq[2 * nt + le];
+            dq[3 * nt + re] = -dq[3 * nt + le];
+            dq[4 * nt + re] = dq[4 * nt + le];
+        } else {
+            for (int k = 0; k < 5; ++k) dq[k * nt + re] = 0.0;
+        }
+    }
+}
+
+/* Controller::LUSGS (Controller.cpp:1878-1955), one or more symmetric sweeps:
+ * Diagonal (NSSolverUnstruct.cpp:15867-15935), SolveLUSGSForward
+ * (15118-15444, lower neighbours j < i, interior faces only),
+ * SetGhostDQLUSGS, SolveLUSGSBackward (15446-15690, upper neighbours j > i,
+ * boundary ghosts included).  dq [5][nTotal] is the output. */
+void ox_lusgs(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
+              const double *t, const double *visl, const double *vist, const double *res, const double *dt,
+              const double *inv_spec, const double *vis_spec, double *dq)
+{
+    (void)t;
+    int nt = ntot(g), nc = g->n_cell;
+    double *diag = malloc(sizeof(double) * nc);
+    double *dflux = calloc((size_t)5 * nt, sizeof(double));
+    for (int c = 0; c < nc; ++c) {
+        diag[c] = 1.0 / dt[c] + inv_spec[c];
+        if (p->viscous) diag[c] += vis_spec[c];
+    }
+    /* LUSGSInitialization (Controller.cpp:1732-1785): dq = res for a single
+     * sweep (ghost residuals are zero), zero otherwise. */
+    for (int i = 0; i < 5 * nt; ++i) dq[i] = p->n_sweeps == 1 ? res[i] : 0.0;
+    double norm0 = 0.0;
+    for (int sweep = 0; sweep < p->n_sweeps; ++sweep) {
+        double norm = 0.0;
+        for (int c = 0; c < nc; ++c) {
+            double rhs0[5] = {0, 0, 0, 0, 0}, ux[5], old[5];
+            for (int k = 0; k < 5; ++k) {
+                old[k] = dq[k * nt + c];
+                dq[k * nt + c] = res[k * nt + c];
+                ux[k] = dflux[k * nt + c];
+                dflux[k * nt + c] = 0.0;
+            }
+            for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+                int f = m->c2f[j];
+                if (f < g->n_bface) continue;
+                int le = g->left[f], re = g->right[f];
+                if (le > c || re > c) continue;
+                double df[5];
+                lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
+                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+            }
+            for (int k = 0; k < 5; ++k) {
+                double v = (dq[k * nt + c] - ux[k] - rhs0[k]) / diag[c];
+                dflux[k * nt + c] += rhs0[k];
+                dq[k * nt + c] = v;
+                norm += (v - old[k]) * (v - old[k]);
+            }
+        }
+        ghost_dq(g, m, p, q, gama, dq);
+        for (int c = nc - 1; c >= 0; --c) {
+            double rhs0[5] = {0, 0, 0, 0, 0}, lx[5], old[5];
+            for (int k = 0; k < 5; ++k) {
+                old[k] = dq[k * nt + c];
+                dq[k * nt + c] = res[k * nt + c];
+                lx[k] = dflux[k * nt + c];
+                dflux[k * nt + c] = 0.0;
+            }
+            for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+                int f = m->c2f[j];
+                int le = g->left[f], re = f < g->n_bface ? nc + f : g->right[f];
+                if (le < c || re < c) continue;
+                double df[5];
+                lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
+                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+            }
+            for (int k = 0; k < 5; ++k) {
+                double v = (dq[k * nt + c] - lx[k] - rhs0[k]) / diag[c];
+                dflux[k * nt + c] += rhs0[k];
+                dq[k * nt + c] = v;
+                norm += (v - old[k]) * (v - old[k]);
+            }
+        }
+        if (sweep == 0) norm0 = norm;
+        else if (norm / norm0 < p->lusgs_tol) break;
+    }
+    free(diag); free(dflux);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Update                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* NSSolverUnstruct::UpdateFlowField (NSSolverUnstruct.cpp:14587-14765) with
+ * SolutionFix (14509-14585): in place, cells in ascending order, so a repair
+ * sees already-updated lower neighbours.  Returns the repaired-cell count. */
+int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double *q, const double *gama,
+              const double *dq)
+{
+    int nt = ntot(g), nc = g->n_cell, nneg = 0;
+    double rlim = 1.0e-6 * p->prim_inf[0], plim = 1.0e-6 * p->prim_inf[4];
+    for (int c = 0; c < nc; ++c) {
+        double r = q[c], u = q[nt + c], v = q[2 * nt + c], w = q[3 * nt + c], pp = q[4 * nt + c];
+        double gm = gama[c];
+        double em = (pp / r) / (gm - 1.0) + 0.5 * (u * u + v * v + w * w);
+        double Q[5] = {r, r * u, r * v, r * w, r * em};
+        for (int k = 0; k < 5; ++k) Q[k] += dq[k * nt + c];
+        double prim[5];
+        if (Q[0] <= 0.0) {
+            prim[0] = Q[0];
+            for (int k = 1; k < 5; ++k) prim[k] = q[k * nt + c];
+        } else {
+            double od = 1.0 / Q[0];
+            double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
+            double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
+            prim[0] = Q[0]; prim[1] = um; prim[2] = vm; prim[3] = wm; prim[4] = (gm - 1.0) * ie;
+        }
+        if (prim[0] < rlim || prim[4] < plim) {
+            ++nneg;
+            double acc[5] = {0, 0, 0, 0, 0}, wsum = 0.0;
+            for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+                int f = m->c2f[j];
+                int le = g->left[f], re = f < g->n_bface ? nc + f : g->right[f];
+                int nbr = (c == le) ? re : le;
+                if (q[nbr] < rlim || q[4 * nt + nbr] < plim) continue;
+                wsum += 1.0;
+                for (int k = 0; k < 5; ++k) {
+                    double fv = q[k * nt + nbr];
+                    if (k == 0 || k == 4) fv = fabs(fv);
+                    acc[k] += fv;
+                }
+            }
+            if (wsum > 0.0) { double o = 1.0 / wsum; for (int k = 0; k < 5; ++k) prim[k] = acc[k] * o; }
+            else for (int k = 0; k < 5; ++k) prim[k] = p->prim_inf[k];
+        }
+        for (int k = 0; k < 5; ++k) q[k * nt + c] = prim[k];
+    }
+    return nneg;
+}
+
+/* Residual monitor, API/Physics/src/Residual.cpp:534-600 and 184-224 (unit
+ * grid scale): sqrt(sum res_rho^2 / nCell). */
+double ox_residual_norm(const ox_grid *g, const double *res)
+{
+    double s = 0.0;
+    for (int c = 0; c < g->n_cell; ++c) s += res[c] * res[c];
+    return sqrt(s / g->n_cell);
+}
+
+/* One outer iteration (Controller::Relaxation, tscheme = LU_SGS):
+ * LoadResiduals, UpdateResiduals (boundary, gamma/T, viscosity, gradient,
+ * limiter, inviscid and viscous flux), SpectrumRadius, TimeStep, LUSGS,
+ * UpdateFlowField. */
+void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, double *q, ox_ns_work *w)
+{
+    int nt = ntot(g);
+    ox_gamma_temperature(g, p, q, w->gama, w->t);  /* gama of the ghosts is needed by the far field */
+    ox_ns_boundary(g, m, p, q, w->gama);
+    ox_gamma_temperature(g, p, q, w->gama, w->t);
+    for (int k = 0; k < 5; ++k)
+        ox_gradient(g, m, p, q + (size_t)k * nt, w->dqdx + (size_t)k * nt, w->dqdy + (size_t)k * nt, w->dqdz + (size_t)k * nt);
+    ox_limiter(g, m, p, q, w->dqdx, w->dqdy, w->dqdz, w->limit);
+    memset(w->res, 0, sizeof(double) * 5 * nt);
+    ox_inviscid_flux(g, m, p, q, w->gama, w->dqdx, w->dqdy, w->dqdz, w->limit, w->res);
+    ox_spectrum(g, m, p, q, w->gama, w->visl, w->vist, w->inv_spec, w->vis_spec);
+    ox_timestep(g, m, p, step, q, w->inv_spec, w->vis_spec, w->dt);
+    ox_lusgs(g, m, p, q, w->gama, w->t, w->visl, w->vist, w->res, w->dt, w->inv_spec, w->vis_spec, w->dq);
+    w->n_negative = ox_update(g, m, p, q, w->gama, w->dq);
+    w->res_norm = ox_residual_norm(g, w->res);
+}

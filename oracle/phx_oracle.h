@@ -1,0 +1,122 @@
+/* Oracle: a plain-C, single-threaded restatement of the reference's
+ * unstructured NS / SA per-iteration path (PHengLEI NSSolverUnstruct /
+ * TurbSolverUnstr).  TEST INFRASTRUCTURE ONLY: it is the parity checker for
+ * the CUDA product and the timed CPU baseline ("port"); the product never
+ * links, loads or calls it.  Each function cites the reference lines it
+ * restates.  Arrays are the reference's SoA layout: cell fields hold nTotal =
+ * nCell + nBFace entries, the ghost cell of boundary face f being nCell + f;
+ * multi-variable fields are [var][nTotal]. */
+#ifndef PHX_ORACLE_H
+#define PHX_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary condition codes (API/Geometry/include/Geo_SimpleBC.h:32-39). */
+enum { OX_BC_EXTRAPOLATION = 1, OX_BC_SOLID_SURFACE = 2, OX_BC_SYMMETRY = 3,
+       OX_BC_FARFIELD = 4, OX_BC_INFLOW = 5, OX_BC_OUTFLOW = 6 };
+
+typedef struct {
+    int n_node, n_face, n_cell, n_bface;
+    const double *x, *y, *z;
+    const int *face_off;     /* [n_face+1] offsets into face2node */
+    const int *face2node;
+    const int *left, *right; /* right of boundary face f = n_cell + f */
+    const int *cell_off;     /* [n_cell+1] offsets into cell2node */
+    const int *cell2node;
+    int n_region;
+    const int *region_type;  /* [n_region] bcType, regions in the solver's order */
+    const int *bface_region; /* [n_bface] region index */
+} ox_grid;
+
+typedef struct {
+    double *xfn, *yfn, *zfn, *area;   /* [n_face] */
+    double *xfc, *yfc, *zfc;          /* [n_face] */
+    double *xcc, *ycc, *zcc, *vol;    /* [nTotal] */
+    double *skew;                     /* [n_cell] degrees, 90 = orthogonal */
+    double *walldist;                 /* [n_cell] or NULL */
+    double avg_vol;
+    /* cell -> face lists in ascending face order, [n_cell+1] offsets */
+    int *c2f_off, *c2f;
+} ox_metrics;
+
+typedef struct {
+    double gama;            /* refGama */
+    double mach, attack, sideslip;  /* attack / sideslip in radians */
+    double prim_inf[5];     /* non-dimensional freestream primitive state */
+    double coef_state;      /* 1 / (gama M^2) */
+    double p_total;         /* pTotal of PerfectGas::ComputePTotal */
+    int viscous;            /* 0 inviscid, 1 laminar, 3 SA */
+    double reynolds;        /* refReNumber (non-dimensional, per unit grid length) */
+    double prandtl, prandtl_turb;
+    double tsuth_nd;        /* Sutherland constant / reference temperature */
+    double wall_temperature;/* <= 0: adiabatic */
+    int gradient;           /* 0 ggcell, 1 lsq */
+    int limiter;            /* 0 nolim, 1 vencat(ivencat=7, scalar from rho and p) */
+    double venkat_coeff;
+    int recon_method;       /* reconmeth: 0 own limiter, 1 min(L,R) */
+    int scheme;             /* 0 roe, 1 ausmpw+ */
+    int entropy_fix;        /* roeEntropyFixMethod (3 supported) */
+    double entropy_acoustic, entropy_convective;
+    double cfl_start, cfl_end;
+    int cfl_vary_step;
+    double ktmax;
+    int n_sweeps;           /* nLUSGSSweeps */
+    double lusgs_tol;
+    double skewness_angle;  /* viscous-flux skewness switch, degrees */
+} ox_params;
+
+/* Grid metrics: API/Geometry/src/Geo_UnstructGrid.cpp:5911-6156 (faces),
+ * 6545-6819 (cells), 2206-2340 (skewness), Region.cpp:2655-2734 (avg volume),
+ * Geo_UnstructGrid.cpp:1246-1304 (cell2face). */
+void ox_compute_metrics(const ox_grid *g, ox_metrics *m);
+
+/* One full outer iteration of NSSolverUnstruct (Controller::Relaxation
+ * tscheme=LU_SGS, CFD/Solver/src/Controller.cpp:549-587) at outer step
+ * `step` (1-based, drives the CFL ramp).  q [5][nTotal] is updated in place.
+ * Work arrays (may be NULL to use internal scratch): see ox_ns_work. */
+typedef struct {
+    double *gama, *t;            /* [nTotal] */
+    double *dqdx, *dqdy, *dqdz;  /* [5][nTotal] */
+    double *limit;               /* [nTotal] scalar limiter */
+    double *res;                 /* [5][nTotal] */
+    double *inv_spec, *vis_spec; /* [n_cell] */
+    double *dt;                  /* [nTotal] dt / vol after the reduction */
+    double *dq;                  /* [5][nTotal] */
+    double *visl, *vist;         /* [nTotal] */
+    double *dtdx, *dtdy, *dtdz;  /* [nTotal] temperature gradient */
+    double res_norm;             /* sqrt(sum res_rho^2 / nCell) */
+    int n_negative;              /* cells repaired by SolutionFix */
+} ox_ns_work;
+
+void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p,
+                     int step, double *q, ox_ns_work *w);
+
+/* Individual phases (for per-kernel parity tests). */
+void ox_ns_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, double *q, const double *gama);
+void ox_gamma_temperature(const ox_grid *g, const ox_params *p, const double *q, double *gama, double *t);
+void ox_gradient(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *f,
+                 double *dfdx, double *dfdy, double *dfdz);
+void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                const double *dqdx, const double *dqdy, const double *dqdz, double *limit);
+void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                      const double *gama, const double *dqdx, const double *dqdy, const double *dqdz,
+                      const double *limit, double *res);
+void ox_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                 const double *gama, const double *visl, const double *vist, double *inv_spec, double *vis_spec);
+double ox_cfl(const ox_params *p, int step);
+void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
+                 const double *inv_spec, const double *vis_spec, double *dt);
+void ox_lusgs(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
+              const double *t, const double *visl, const double *vist, const double *res, const double *dt,
+              const double *inv_spec, const double *vis_spec, double *dq);
+int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double *q, const double *gama,
+              const double *dq);
+double ox_residual_norm(const ox_grid *g, const double *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
