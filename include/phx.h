@@ -1,0 +1,199 @@
+/* phx — B200-native (sm_100a) per-iteration hot path of PHengLEI's unstructured
+ * compressible NS solver (NSSolverUnstruct) and its Spalart-Allmaras solver
+ * (TurbSolverUnstr), exposed as a C ABI.
+ *
+ * Plain pointers and sizes only; no exceptions cross the boundary; every call
+ * returns PHX_OK or a negative error code and leaves a message in
+ * phx_last_error().  One context per host thread; all device work of a
+ * context is issued on its stream (phx_set_stream); calls are synchronous with
+ * respect to the host only where they return data to host memory.
+ *
+ * Each entry point names the reference solver method(s) it replaces (file:line
+ * in the reference project).  The reference's own accelerator hook pattern is
+ * `#ifdef USE_CUDA CallGPUxxx(grid, ...); return; #endif` at the top of those
+ * methods (e.g. CFD/NSSolver/src/NSSolverUnstruct.cpp:13406-13412); the
+ * replacement binding is shown in INTEGRATION.md.
+ *
+ * Layout conventions (the reference's, API/Geometry/include/Geo_UnstructGrid.h):
+ *  - faces: boundary faces first (nBFace of them), then interior faces;
+ *  - the face normal points from the left to the right cell;
+ *  - cell fields hold nTotal = nCell + nBFace entries; the ghost cell of
+ *    boundary face f is nCell + f;
+ *  - multi-variable fields are structure-of-arrays [var][nTotal], primitive
+ *    variables (rho, u, v, w, p), non-dimensionalised by the free stream. */
+#ifndef PHX_H
+#define PHX_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHX_OK 0
+#define PHX_ERR_ARG -1       /* invalid argument (null pointer, bad size, unsupported option) */
+#define PHX_ERR_CUDA -2      /* a CUDA runtime call failed */
+#define PHX_ERR_TIMEOUT -3   /* a bounded device-side wait gave up (level barrier) */
+#define PHX_ERR_NUMERIC -4   /* NaN / divergence detected in a reduction */
+#define PHX_ERR_STATE -5     /* call out of order (e.g. no state uploaded) */
+
+/* precision modes */
+#define PHX_FP64 0   /* everything in FP64 (the reference's PH_DOUBLE_PREC) */
+#define PHX_MIXED 1  /* FP32 flux/gradient/limiter/LU-SGS, FP64 metrics, update and reductions */
+
+/* boundary condition codes: the reference's bcType values
+ * (API/Geometry/include/Geo_SimpleBC.h:32-39) */
+#define PHX_BC_EXTRAPOLATION 1
+#define PHX_BC_SOLID_SURFACE 2
+#define PHX_BC_SYMMETRY 3
+#define PHX_BC_FARFIELD 4
+#define PHX_BC_OUTFLOW 6
+
+/* state selectors for phx_set_state / phx_get_state */
+#define PHX_Q 0          /* primitive state [5][nTotal] */
+#define PHX_RES 1        /* residual [5][nTotal] (the reference's "res") */
+#define PHX_DT 2         /* time step / volume [nTotal] (the reference's "dt") */
+#define PHX_LIMIT 3      /* scalar limiter [nTotal] ("limit2D" row 0) */
+#define PHX_GRADX 4      /* primitive gradients [5][nTotal] ("gradPrimtiveVarX/Y/Z") */
+#define PHX_GRADY 5
+#define PHX_GRADZ 6
+#define PHX_DQ 7         /* LU-SGS increment of the conservative variables [5][nTotal] */
+#define PHX_INVSPEC 8    /* inviscid spectral radius [nCell] ("invSpectralRadius") */
+#define PHX_VISSPEC 9    /* viscous spectral radius [nCell] ("visSpectralRadius") */
+#define PHX_Q_TURB 10    /* SA working variable nu~ [nTotal] ("q_turb") */
+#define PHX_VISL 11      /* laminar viscosity [nTotal] ("visl") */
+#define PHX_VIST 12      /* eddy viscosity [nTotal] ("vist") */
+#define PHX_RES_TURB 13  /* SA residual [nTotal] */
+#define PHX_GEOM 14      /* geometry, see phx_get_geometry */
+
+typedef struct phx_ctx phx_ctx;
+
+/* Grid, as UnstructGrid holds it (Geo_UnstructGrid.h).  Host arrays are read
+ * during phx_ctx_create only. */
+typedef struct {
+    int64_t n_node, n_face, n_cell, n_bface;
+    const double *x, *y, *z;              /* [n_node] node coordinates */
+    const int32_t *face_nnode;            /* [n_face] node_number_of_each_face */
+    const int32_t *face2node;             /* [sum face_nnode] */
+    const int32_t *left_cell;             /* [n_face] leftCellOfFace */
+    const int32_t *right_cell;            /* [n_face] rightCellOfFace (boundary: ignored) */
+    const int32_t *cell_nnode;            /* [n_cell] node_number_of_each_cell */
+    const int32_t *cell2node;             /* [sum cell_nnode] (sorted node set per cell) */
+    int32_t n_region;                     /* boundary regions (UnstructBCSet) */
+    const int32_t *region_type;           /* [n_region] bcType */
+    const int32_t *bface_region;          /* [n_bface] region of each boundary face */
+    const double *wall_dist;              /* [n_cell] wall distance, or NULL to compute */
+} phx_grid_desc;
+
+/* Parameters: the hypara keys of the reference (PHengLEI/examples/bin/cfd_para.hypara)
+ * that the path reads, with the same meaning.  String keys become codes. */
+typedef struct {
+    int32_t precision;          /* PHX_FP64 or PHX_MIXED */
+    double refGama;             /* ratio of specific heats */
+    double refMachNumber;
+    double attackd, angleSlide; /* degrees */
+    int32_t viscousType;        /* 0 inviscid, 1 laminar, 3 one-equation SA */
+    double refReNumber;         /* Reynolds number per unit grid length */
+    double refDimensionalTemperature;
+    double prl, prt;            /* laminar / turbulent Prandtl numbers */
+    double tsuth;               /* Sutherland constant, K */
+    double wallTemperature;     /* <= 0: adiabatic wall */
+    int32_t gradientName;       /* 0 "ggcell", 1 "lsq" */
+    int32_t uns_limiter_name;   /* 0 "nolim", 1 "vencat" */
+    int32_t ivencat;            /* Venkatakrishnan variant (7 supported) */
+    double venkatCoeff;
+    int32_t reconmeth;          /* 0 own limiter, 1 min of both sides */
+    int32_t uns_scheme_name;    /* 0 "roe", 1 "ausmpw+" */
+    int32_t roeEntropyFixMethod;/* 3 (Harten) supported */
+    double roeEntropyScale;
+    double CFLStart, CFLEnd;
+    int32_t CFLVaryStep;
+    double ktmax;
+    int32_t nLUSGSSweeps;
+    double LUSGSTolerance;
+    double skewnessAngle;
+    double muoo;                /* SA free-stream nu~ / nu */
+    double turbCFLScale;
+    int32_t sa_source;          /* 0 exact SA source, 1 MLP, 2 MLP with exact fallback */
+} phx_params;
+
+/* Fills `p` with the reference's defaults for every key. */
+void phx_default_params(phx_params *p);
+
+/* Creates a context: uploads the grid, computes the FP64 metrics on the
+ * device side of the context (face normals/areas/centres, cell centres and
+ * volumes, skewness, wall distance), the cell-to-face lists and the LU-SGS
+ * level schedules, and initialises the state to the free stream.
+ * Replaces: Simulation::RunCFD grid set-up (Main/src/Simulation.cpp:205-260),
+ * UnstructGrid::ComputeMetrics (API/Geometry/src/Geo_UnstructGrid.cpp:5695),
+ * NSSolverUnstruct::AllocateGlobalVar / InitFlow, GPUGeomInfoAllocCopy. */
+int phx_ctx_create(const phx_grid_desc *grid, const phx_params *params, phx_ctx **out);
+int phx_ctx_destroy(phx_ctx *ctx);
+const char *phx_last_error(const phx_ctx *ctx);
+/* cudaStream_t as void*; NULL = the legacy default stream. */
+int phx_set_stream(phx_ctx *ctx, void *stream);
+/* Device on which the context was created. */
+int phx_device(const phx_ctx *ctx);
+
+/* Host <-> device state copies in the reference SoA layout.  n is the element
+ * count of the host array (checked against the selector's size). */
+int phx_set_state(phx_ctx *ctx, int which, const double *host, int64_t n);
+int phx_get_state(phx_ctx *ctx, int which, double *host, int64_t n);
+/* Device-pointer variants (FP64 device memory of the same layout). */
+int phx_set_state_device(phx_ctx *ctx, int which, const double *dev, int64_t n);
+int phx_get_state_device(phx_ctx *ctx, int which, double *dev, int64_t n);
+/* Geometry as computed by the context: names "xfn","yfn","zfn","area","xfc",
+ * "yfc","zfc" ([n_face]), "xcc","ycc","zcc","vol" ([nTotal]), "skew",
+ * "walldist" ([n_cell]). */
+int phx_get_geometry(phx_ctx *ctx, const char *name, double *host, int64_t n);
+
+/* --- NS residual phases ---------------------------------------------------- */
+
+/* Ghost-cell state of every boundary face.
+ * Replaces NSSolverUnstruct::Boundary (CFD/NSSolver/src/NSSolverUnstruct.cpp:13404). */
+int phx_ns_boundary(phx_ctx *ctx);
+
+/* Gas state (gamma, T), laminar viscosity, primitive and temperature gradients
+ * and the limiter.  Replaces NSSolverUnstruct::ComputeGamaAndTemperature
+ * (:4666), ComputeViscousCoefficientWithoutChemical (:6722), ComputeGradient /
+ * GetGradientField (:18171/:18244) and ComputeLimiter (:18189). */
+int phx_ns_gradient_limiter(phx_ctx *ctx);
+
+/* Inviscid and viscous face fluxes summed into res, the spectral radii and the
+ * local time step (with the ktmax clamp).  Replaces NSSolver::UpdateResiduals
+ * (CFD/NSSolver/src/NSSolver.cpp:71): InviscidFlux (NSSolverUnstruct.cpp:6912),
+ * ViscousFlux (:7058), LoadFlux (:6435); plus SpectrumRadius (:15795),
+ * NSSolver::TimeStep (NSSolver.cpp:51) and ReduceMaxTimeStep (:5717). */
+int phx_ns_residual(phx_ctx *ctx);
+
+/* Implicit LU-SGS solve for dq.  Replaces Controller::LUSGS
+ * (CFD/Solver/src/Controller.cpp:1878): Diagonal (NSSolverUnstruct.cpp:15867),
+ * SolveLUSGSForward (:15118), SetGhostDQLUSGS (:14767), SolveLUSGSBackward (:15446). */
+int phx_ns_lusgs(phx_ctx *ctx);
+
+/* Q += dq in conservative variables, back to primitive, positivity repair.
+ * Replaces NSSolverUnstruct::UpdateFlowField (:14587) and SolutionFix (:14509). */
+int phx_ns_update(phx_ctx *ctx);
+
+/* nsteps outer iterations of the NS solver (and the SA solver when
+ * viscousType = 3): the sequence of Controller::Relaxation with tscheme =
+ * LU_SGS (Controller.cpp:549-587), driven as Simulation::SolveSteady
+ * (Main/src/Simulation.cpp:1527).  If res_hist is not NULL it receives, per
+ * step, the residual monitor of NSSolverUnstruct::GetResidual (:14258,
+ * API/Physics/src/Residual.cpp:534): sqrt(sum res_rho^2 / nCell). */
+int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist);
+
+/* Residual monitor of the current res, per equation: out[m] =
+ * sqrt(sum res_m^2 / nCell) (FP64 device reduction). */
+int phx_residual_norm(phx_ctx *ctx, double out[5]);
+
+/* Outer step counter (drives the CFL ramp of NSSolver::ComputeCFL). */
+int phx_set_step(phx_ctx *ctx, int step);
+int phx_get_step(const phx_ctx *ctx);
+
+/* Number of kernel launches the context has issued so far (for accounting). */
+int64_t phx_launch_count(const phx_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

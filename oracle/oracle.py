@@ -97,7 +97,9 @@ def total_pressure(gama: float, mach: float) -> float:
     t0t = 1.0 + 0.5 * gm1 * c1 / c2
     if mach > 1.0:
         p *= (2.0 * gama / gp1 * m12 - gm1 / gp1)
-    return p * math.pow(t0t, cc)
+    # pow of a negative base is NaN in C, as in the reference (subsonic Mach
+    # numbers make t0t negative); NaN disables the pressure-based CFL limit.
+    return p * (math.pow(t0t, cc) if t0t >= 0.0 else float("nan"))
 
 
 def make_params(**kw) -> _Params:

@@ -1,0 +1,854 @@
+// Host side of the phx library: context creation (grid metrics in FP64, the
+// cell-to-face lists, the LU-SGS level schedules, boundary classification),
+// device memory, and the C ABI declared in include/phx.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "phx_internal.h"
+
+using namespace phx;
+
+struct phx_ctx {
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    phx_params prm{};
+    NsConst nc{};
+    int nNode = 0, nFace = 0, nCell = 0, nBFace = 0, nTotal = 0;
+    bool mixed = false;
+    // host copies used to build schedules and to answer phx_get_geometry
+    std::vector<double> geom[12];  // xfn yfn zfn area xfc yfc zfc xcc ycc zcc vol skew
+    std::vector<double> walldist;
+    std::vector<void *> allocs;
+    DevGrid g{};
+    double *q64[2] = {nullptr, nullptr};
+    int cur = 0;
+    Work<double> w64{};
+    Work<float> w32{};
+    Reduce *red = nullptr;
+    int *neglist = nullptr;
+    double *hist = nullptr;
+    int histCap = 0;
+    int step = 0;
+    bool haveResidual = false;
+};
+
+namespace {
+
+const char *kGeomNames[12] = {"xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol", "skew"};
+
+int fail(phx_ctx *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+#define PHX_CUDA(ctx, call)                                                                      \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(ctx, PHX_ERR_CUDA, std::string(#call " failed: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(phx_ctx *ctx, T **p, size_t n)
+{
+    void *v = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&v, n * sizeof(T));
+    if (e != cudaSuccess) return fail(ctx, PHX_ERR_CUDA, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    ctx->allocs.push_back(v);
+    *p = static_cast<T *>(v);
+    return PHX_OK;
+}
+
+template <class T>
+int upload(phx_ctx *ctx, const T **dst, const std::vector<T> &src)
+{
+    T *d = nullptr;
+    int rc = dalloc(ctx, &d, src.size());
+    if (rc) return rc;
+    if (!src.empty()) PHX_CUDA(ctx, cudaMemcpy(d, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = d;
+    return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Grid metrics, FP64, following the reference's UnstructGrid::ComputeMetrics
+// for 3-D grids (API/Geometry/src/Geo_UnstructGrid.cpp:5695-5709):
+//  faces  ComputeFaceCenterAreaNormal3DNew2 (:5911-6043): node-average
+//         centre refined 4 times to the area-weighted fan centroid, normal
+//         from the fan cross products of the final pass;
+//  cells  ComputeCellCenterVol3DNew2 (:6545-6819): fan tetrahedra against the
+//         node-average centre, centroid kept when inside all face planes,
+//         ghost centres mirrored across the boundary face;
+//  skew   SkewnessSummary (:2206-2330), degrees.
+// ---------------------------------------------------------------------------
+struct HostGrid {
+    int nNode, nFace, nCell, nBFace;
+    const double *x, *y, *z;
+    std::vector<int> foff, f2n, left, right, coff, c2n;
+};
+
+void face_metrics(const HostGrid &h, std::vector<double> *G)
+{
+    double *xfn = G[0].data(), *yfn = G[1].data(), *zfn = G[2].data(), *area = G[3].data();
+    double *xfc = G[4].data(), *yfc = G[5].data(), *zfc = G[6].data();
+    for (int f = 0; f < h.nFace; ++f) {
+        const int b = h.foff[f], nn = h.foff[f + 1] - b;
+        double cx = 0, cy = 0, cz = 0;
+        for (int j = 0; j < nn; ++j) {
+            const int p = h.f2n[b + j];
+            cx += h.x[p]; cy += h.y[p]; cz += h.z[p];
+        }
+        const double inv = 1.0 / nn;
+        cx *= inv; cy *= inv; cz *= inv;
+        double sx = 0, sy = 0, sz = 0;
+        for (int pass = 0; pass < 5; ++pass) {
+            double wx = 0, wy = 0, wz = 0, wa = 0;
+            sx = sy = sz = 0;
+            for (int j = 0; j < nn; ++j) {
+                const int a1 = h.f2n[b + j], a2 = h.f2n[b + (j + 1) % nn];
+                const double ux = h.x[a1] - cx, uy = h.y[a1] - cy, uz = h.z[a1] - cz;
+                const double vx = h.x[a2] - cx, vy = h.y[a2] - cy, vz = h.z[a2] - cz;
+                const double nx = uy * vz - vy * uz, ny = uz * vx - vz * ux, nz = ux * vy - vx * uy;
+                const double ta = std::sqrt(nx * nx + ny * ny + nz * nz);
+                wa += ta;
+                wx += ta * (h.x[a1] + h.x[a2] + cx);
+                wy += ta * (h.y[a1] + h.y[a2] + cy);
+                wz += ta * (h.z[a1] + h.z[a2] + cz);
+                sx += nx; sy += ny; sz += nz;
+            }
+            if (wa > kSmall) {
+                const double t = 1.0 / wa / 3.0;
+                cx = wx * t; cy = wy * t; cz = wz * t;
+            }
+        }
+        const double s = std::sqrt(sx * sx + sy * sy + sz * sz);
+        area[f] = s * 0.5;
+        const double os = 1.0 / (s + kSmall);
+        xfn[f] = sx * os; yfn[f] = sy * os; zfn[f] = sz * os;
+        xfc[f] = cx; yfc[f] = cy; zfc[f] = cz;
+    }
+}
+
+void cell_metrics(const HostGrid &h, std::vector<double> *G)
+{
+    const double *xfn = G[0].data(), *yfn = G[1].data(), *zfn = G[2].data(), *area = G[3].data();
+    const double *xfc = G[4].data(), *yfc = G[5].data(), *zfc = G[6].data();
+    double *xcc = G[7].data(), *ycc = G[8].data(), *zcc = G[9].data(), *vol = G[10].data();
+    const int nc = h.nCell, nb = h.nBFace;
+    for (int c = 0; c < nc; ++c) {
+        const int b = h.coff[c], nn = h.coff[c + 1] - b;
+        double sx = 0, sy = 0, sz = 0;
+        for (int j = 0; j < nn; ++j) {
+            const int p = h.c2n[b + j];
+            sx += h.x[p]; sy += h.y[p]; sz += h.z[p];
+        }
+        xcc[c] = sx / nn; ycc[c] = sy / nn; zcc[c] = sz / nn;
+    }
+    std::vector<double> tx(nc, 0.0), ty(nc, 0.0), tz(nc, 0.0);
+    std::fill(vol, vol + nc, 0.0);
+    auto add_tet = [&](int c, int f, int p2, int p3, double nx, double ny, double nz, double sign) {
+        const double dx = xcc[c] - xfc[f], dy = ycc[c] - yfc[f], dz = zcc[c] - zfc[f];
+        double ex = xfc[f] + h.x[p2] + h.x[p3] + xcc[c];
+        double ey = yfc[f] + h.y[p2] + h.y[p3] + ycc[c];
+        double ez = zfc[f] + h.z[p2] + h.z[p3] + zcc[c];
+        double t = nx * dx + ny * dy + nz * dz;
+        if (sign < 0) t = -t;
+        tx[c] += ex * t; ty[c] += ey * t; tz[c] += ez * t; vol[c] += t;
+    };
+    for (int f = 0; f < h.nFace; ++f) {
+        const int b = h.foff[f], nn = h.foff[f + 1] - b;
+        const int le = h.left[f], re = h.right[f];
+        for (int j = 0; j < nn; ++j) {
+            const int p2 = h.f2n[b + j], p3 = h.f2n[b + (j + 1) % nn];
+            const double ax = h.x[p2] - xfc[f], ay = h.y[p2] - yfc[f], az = h.z[p2] - zfc[f];
+            const double bx = h.x[p3] - xfc[f], by = h.y[p3] - yfc[f], bz = h.z[p3] - zfc[f];
+            const double nx = ay * bz - by * az, ny = az * bx - bz * ax, nz = ax * by - bx * ay;
+            add_tet(le, f, p2, p3, nx, ny, nz, -1.0);
+            if (f >= nb) add_tet(re, f, p2, p3, nx, ny, nz, +1.0);
+        }
+    }
+    for (int c = 0; c < nc; ++c) {
+        const double t = 1.0 / (4.0 * vol[c] + kSmall);
+        tx[c] *= t; ty[c] *= t; tz[c] *= t;
+        vol[c] /= 6.0;
+    }
+    std::vector<char> inside(nc, 1);
+    for (int f = 0; f < h.nFace; ++f) {
+        const int le = h.left[f];
+        if ((tx[le] - xfc[f]) * xfn[f] + (ty[le] - yfc[f]) * yfn[f] + (tz[le] - zfc[f]) * zfn[f] > 0.0) inside[le] = 0;
+        if (f >= nb) {
+            const int re = h.right[f];
+            if ((tx[re] - xfc[f]) * xfn[f] + (ty[re] - yfc[f]) * yfn[f] + (tz[re] - zfc[f]) * zfn[f] < 0.0) inside[re] = 0;
+        }
+    }
+    for (int c = 0; c < nc; ++c)
+        if (inside[c]) { xcc[c] = tx[c]; ycc[c] = ty[c]; zcc[c] = tz[c]; }
+    for (int f = 0; f < nb; ++f) {
+        const int le = h.left[f], re = nc + f;
+        if (area[f] > kSmall) {
+            const double d = 2.0 * ((xcc[le] - xfc[f]) * xfn[f] + (ycc[le] - yfc[f]) * yfn[f] + (zcc[le] - zfc[f]) * zfn[f]);
+            xcc[re] = xcc[le] - xfn[f] * d;
+            ycc[re] = ycc[le] - yfn[f] * d;
+            zcc[re] = zcc[le] - zfn[f] * d;
+        } else {
+            xcc[re] = -xcc[le] + 2.0 * xfc[f];
+            ycc[re] = -ycc[le] + 2.0 * yfc[f];
+            zcc[re] = -zcc[le] + 2.0 * zfc[f];
+        }
+        vol[re] = vol[le];
+    }
+}
+
+double clampunit(double v) { return v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v); }
+
+void skewness(const HostGrid &h, std::vector<double> *G)
+{
+    const double *xfn = G[0].data(), *yfn = G[1].data(), *zfn = G[2].data(), *area = G[3].data();
+    const double *xfc = G[4].data(), *yfc = G[5].data(), *zfc = G[6].data();
+    const double *xcc = G[7].data(), *ycc = G[8].data(), *zcc = G[9].data();
+    double *skew = G[11].data();
+    const double pi = 3.141592653589793;
+    std::fill(skew, skew + h.nCell, 180.0);
+    auto angle_to = [&](int f, double dx, double dy, double dz) {
+        const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+        return std::asin(clampunit((xfn[f] * dx + yfn[f] * dy + zfn[f] * dz) / (d + kSmall)));
+    };
+    for (int f = h.nBFace; f < h.nFace; ++f) {
+        if (area[f] <= kSmall) continue;
+        const int le = h.left[f], re = h.right[f];
+        const double a1 = angle_to(f, xfc[f] - xcc[le], yfc[f] - ycc[le], zfc[f] - zcc[le]);
+        const double a2 = angle_to(f, xcc[re] - xfc[f], ycc[re] - yfc[f], zcc[re] - zfc[f]);
+        const double ang = std::min(a1, a2) * 180.0 / pi;
+        skew[le] = std::min(skew[le], ang);
+        skew[re] = std::min(skew[re], ang);
+    }
+    for (int f = 0; f < h.nBFace; ++f) {
+        if (area[f] <= kSmall) continue;
+        const int le = h.left[f];
+        skew[le] = std::min(skew[le], angle_to(f, xfc[f] - xcc[le], yfc[f] - ycc[le], zfc[f] - zcc[le]) * 180.0 / pi);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void phx_default_params(phx_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    // defaults of PHengLEI/examples/bin/cfd_para.hypara
+    p->precision = PHX_FP64;
+    p->refGama = 1.4;
+    p->refMachNumber = 0.73;
+    p->attackd = 2.79;
+    p->angleSlide = 0.0;
+    p->viscousType = 3;
+    p->refReNumber = 6.5e6;
+    p->refDimensionalTemperature = 288.15;
+    p->prl = 0.72;
+    p->prt = 0.90;
+    p->tsuth = 110.4;
+    p->wallTemperature = -1.0;
+    p->gradientName = 0;
+    p->uns_limiter_name = 1;
+    p->ivencat = 7;
+    p->venkatCoeff = 5.0;
+    p->reconmeth = 1;
+    p->uns_scheme_name = 0;
+    p->roeEntropyFixMethod = 3;
+    p->roeEntropyScale = 1.0;
+    p->CFLStart = 0.01;
+    p->CFLEnd = 10.0;
+    p->CFLVaryStep = 500;
+    p->ktmax = 1.0e10;
+    p->nLUSGSSweeps = 1;
+    p->LUSGSTolerance = 0.01;
+    p->skewnessAngle = 60.0;
+    p->muoo = 3.0;
+    p->turbCFLScale = 1.0;
+    p->sa_source = 0;
+}
+
+static double entropy_fix_coefficient(double mach, double scale)
+{
+    // Param_NSSolver::SetEntropyFixCoefficients, CFD/NSSolver/src/Param_NSSolver.cpp:224-268
+    double e;
+    if (mach <= 0.6) e = 0.0001;
+    else if (mach <= 2.0) e = 0.0001 * (mach - 2.0) / (0.6 - 2.0) + 0.01 * (mach - 0.6) / (2.0 - 0.6);
+    else if (mach <= 5.0) e = 0.01 * (mach - 5.0) / (2.0 - 5.0) + 0.5 * (mach - 2.0) / (5.0 - 2.0);
+    else e = 1.0;
+    return e * scale;
+}
+
+static double total_pressure(double gama, double mach)
+{
+    // PerfectGas::ComputePTotal, API/Physics/src/PerfectGas.cpp:1609-1640
+    double p = 1.0 / (gama * mach * mach);
+    double m12 = mach * mach, gp1 = gama + 1.0, gm1 = gama - 1.0;
+    double c1 = 2.0 / gm1 + m12;
+    double c2 = 2.0 * gama / gm1 * m12 - 1.0;
+    double cc = gama / (gama - 1.0);
+    double t0t = 1.0 + 0.5 * gm1 * c1 / c2;
+    if (mach > 1.0) p *= (2.0 * gama / gp1 * m12 - gm1 / gp1);
+    return p * std::pow(t0t, cc);
+}
+
+static bool limiter_zeroed(int bcType)
+{
+    // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775
+    return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW;
+}
+
+int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out)
+{
+    if (!out) return PHX_ERR_ARG;
+    *out = nullptr;
+    if (!gd || !prm || !gd->x || !gd->y || !gd->z || !gd->face_nnode || !gd->face2node || !gd->left_cell ||
+        !gd->right_cell || !gd->cell_nnode || !gd->cell2node || !gd->region_type || (gd->n_bface > 0 && !gd->bface_region))
+        return PHX_ERR_ARG;
+    if (gd->n_cell <= 0 || gd->n_face <= 0 || gd->n_bface < 0 || gd->n_bface > gd->n_face || gd->n_node <= 0 ||
+        gd->n_cell + gd->n_bface > 0x7fffffffLL || gd->n_face > 0x7fffffffLL)
+        return PHX_ERR_ARG;
+    if (prm->precision != PHX_FP64 && prm->precision != PHX_MIXED) return PHX_ERR_ARG;
+    if (prm->viscousType != 0) return PHX_ERR_ARG;   // viscous paths are attached by later releases
+    if (prm->gradientName != 0 || prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
+        prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
+        return PHX_ERR_ARG;
+
+    phx_ctx *ctx = new phx_ctx();
+    ctx->prm = *prm;
+    ctx->mixed = prm->precision == PHX_MIXED;
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->numSMs, cudaDevAttrMultiProcessorCount, ctx->device);
+
+    HostGrid h;
+    h.nNode = (int)gd->n_node; h.nFace = (int)gd->n_face; h.nCell = (int)gd->n_cell; h.nBFace = (int)gd->n_bface;
+    h.x = gd->x; h.y = gd->y; h.z = gd->z;
+    const int nc = h.nCell, nb = h.nBFace, nf = h.nFace, nt = nc + nb;
+    ctx->nNode = h.nNode; ctx->nFace = nf; ctx->nCell = nc; ctx->nBFace = nb; ctx->nTotal = nt;
+    h.foff.resize(nf + 1);
+    h.foff[0] = 0;
+    for (int f = 0; f < nf; ++f) {
+        if (gd->face_nnode[f] < 3) { delete ctx; return PHX_ERR_ARG; }
+        h.foff[f + 1] = h.foff[f] + gd->face_nnode[f];
+    }
+    h.f2n.assign(gd->face2node, gd->face2node + h.foff[nf]);
+    h.left.assign(gd->left_cell, gd->left_cell + nf);
+    h.right.assign(gd->right_cell, gd->right_cell + nf);
+    for (int f = 0; f < nb; ++f) h.right[f] = nc + f;
+    for (int f = 0; f < nf; ++f) {
+        if (h.left[f] < 0 || h.left[f] >= nc || (f >= nb && (h.right[f] < 0 || h.right[f] >= nc))) {
+            delete ctx;
+            return PHX_ERR_ARG;
+        }
+    }
+    for (int i = 0; i < h.foff[nf]; ++i)
+        if (h.f2n[i] < 0 || h.f2n[i] >= h.nNode) { delete ctx; return PHX_ERR_ARG; }
+    h.coff.resize(nc + 1);
+    h.coff[0] = 0;
+    for (int c = 0; c < nc; ++c) h.coff[c + 1] = h.coff[c] + gd->cell_nnode[c];
+    h.c2n.assign(gd->cell2node, gd->cell2node + h.coff[nc]);
+
+    // metrics
+    for (int k = 0; k < 7; ++k) ctx->geom[k].assign(nf, 0.0);
+    for (int k = 7; k < 11; ++k) ctx->geom[k].assign(nt, 0.0);
+    ctx->geom[11].assign(nc, 0.0);
+    face_metrics(h, ctx->geom);
+    cell_metrics(h, ctx->geom);
+    skewness(h, ctx->geom);
+    double vsum = 0.0;
+    for (int c = 0; c < nc; ++c) vsum += ctx->geom[10][c];
+    const double avgVol = vsum / (double)nc;   // Region::ComputeGlobalGridSize, Region.cpp:2655-2734
+
+    // cell -> face lists in ascending face order (UnstructGrid::ComputeCell2Face, :1246-1290)
+    std::vector<int> c2f_off(nc + 1, 0), c2f;
+    for (int f = 0; f < nf; ++f) { c2f_off[h.left[f] + 1]++; if (f >= nb) c2f_off[h.right[f] + 1]++; }
+    for (int c = 0; c < nc; ++c) c2f_off[c + 1] += c2f_off[c];
+    c2f.resize(c2f_off[nc]);
+    {
+        std::vector<int> fill(c2f_off.begin(), c2f_off.end() - 1);
+        for (int f = 0; f < nf; ++f) { c2f[fill[h.left[f]]++] = f; if (f >= nb) c2f[fill[h.right[f]]++] = f; }
+    }
+
+    // LU-SGS level schedules from the reference's cell order
+    std::vector<int> lev(nc, 0);
+    int nfl = 0;
+    for (int c = 0; c < nc; ++c) {
+        int l = 0;
+        for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+            const int f = c2f[j];
+            if (f < nb) continue;
+            const int o = h.left[f] == c ? h.right[f] : h.left[f];
+            if (o < c) l = std::max(l, lev[o] + 1);
+        }
+        lev[c] = l;
+        nfl = std::max(nfl, l + 1);
+    }
+    auto bucket = [&](int nlev, std::vector<int> &cells, std::vector<int> &off, bool ascending) {
+        off.assign(nlev + 1, 0);
+        for (int c = 0; c < nc; ++c) off[lev[c] + 1]++;
+        for (int l = 0; l < nlev; ++l) off[l + 1] += off[l];
+        cells.resize(nc);
+        std::vector<int> fill(off.begin(), off.end() - 1);
+        if (ascending) for (int c = 0; c < nc; ++c) cells[fill[lev[c]]++] = c;
+        else for (int c = nc - 1; c >= 0; --c) cells[fill[lev[c]]++] = c;
+    };
+    std::vector<int> fwd_cells, fwd_off, bwd_cells, bwd_off;
+    bucket(nfl, fwd_cells, fwd_off, true);
+    std::fill(lev.begin(), lev.end(), 0);
+    int nbl = 0;
+    for (int c = nc - 1; c >= 0; --c) {
+        int l = 0;
+        for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+            const int f = c2f[j];
+            if (f < nb) continue;
+            const int o = h.left[f] == c ? h.right[f] : h.left[f];
+            if (o > c) l = std::max(l, lev[o] + 1);
+        }
+        lev[c] = l;
+        nbl = std::max(nbl, l + 1);
+    }
+    bucket(nbl, bwd_cells, bwd_off, false);
+
+    // boundary classification
+    std::vector<int32_t> bkind(nb), btype(nb);
+    std::vector<uint8_t> ffadj(nc, 0);
+    for (int f = 0; f < nb; ++f) {
+        const int r = gd->bface_region[f];
+        if (r < 0 || r >= gd->n_region) { delete ctx; return PHX_ERR_ARG; }
+        const int t = gd->region_type[r];
+        btype[f] = t;
+        if (t == PHX_BC_SOLID_SURFACE) bkind[f] = prm->viscousType ? BK_WALL : BK_SYMMETRY;
+        else if (t == PHX_BC_SYMMETRY) bkind[f] = BK_SYMMETRY;
+        else if (t == PHX_BC_FARFIELD) bkind[f] = BK_FARFIELD;
+        else { delete ctx; return PHX_ERR_ARG; }
+        if (limiter_zeroed(t)) ffadj[h.left[f]] = 1;
+    }
+    std::vector<double> volpow(nc);
+    for (int c = 0; c < nc; ++c) volpow[c] = std::pow(std::pow(ctx->geom[10][c], 1.0 / 3.0), 3.0);
+
+    // constants
+    NsConst &k = ctx->nc;
+    k.gama = prm->refGama;
+    k.coefState = 1.0 / (prm->refGama * prm->refMachNumber * prm->refMachNumber);
+    k.pTotal = total_pressure(prm->refGama, prm->refMachNumber);
+    const double dr = 3.141592653589793 / 180.0;
+    const double att = prm->attackd * dr, sid = prm->angleSlide * dr;
+    k.primInf[0] = 1.0;
+    k.primInf[1] = std::cos(att) * std::cos(sid);
+    k.primInf[2] = std::sin(att) * std::cos(sid);
+    k.primInf[3] = std::sin(sid);
+    k.primInf[4] = k.coefState;
+    k.acoustic = k.convective = entropy_fix_coefficient(prm->refMachNumber, prm->roeEntropyScale);
+    double K = prm->venkatCoeff;
+    double kt = K * K * K;
+    kt *= 1.0 / std::pow(std::pow(avgVol, 1.0 / 3.0), 3.0);
+    k.venkatK3 = kt;
+    k.viscous = prm->viscousType;
+    k.limiter = prm->uns_limiter_name;
+    k.reconMethod = prm->reconmeth;
+    k.cflStart = prm->CFLStart; k.cflEnd = prm->CFLEnd; k.cflVaryStep = prm->CFLVaryStep;
+    k.ktmax = prm->ktmax;
+    k.nSweeps = prm->nLUSGSSweeps;
+    k.lusgsTol = prm->LUSGSTolerance;
+    k.reynolds = prm->refReNumber;
+
+    // device grid
+    DevGrid &g = ctx->g;
+    g.nCell = nc; g.nBFace = nb; g.nFace = nf; g.nTotal = nt;
+    g.avgVol = avgVol;
+    int rc = 0;
+    rc |= upload(ctx, &g.left, h.left);
+    rc |= upload(ctx, &g.right, h.right);
+    const double **gp[12] = {&g.xfn, &g.yfn, &g.zfn, &g.area, &g.xfc, &g.yfc, &g.zfc, &g.xcc, &g.ycc, &g.zcc, &g.vol, &g.skew};
+    for (int i = 0; i < 12; ++i) rc |= upload(ctx, gp[i], ctx->geom[i]);
+    rc |= upload(ctx, &g.volpow, volpow);
+    rc |= upload(ctx, &g.c2f_off, c2f_off);
+    rc |= upload(ctx, &g.c2f, c2f);
+    rc |= upload(ctx, &g.bkind, bkind);
+    rc |= upload(ctx, &g.btype, btype);
+    rc |= upload(ctx, &g.farfield_adj, ffadj);
+    rc |= upload(ctx, &g.fwd_cells, fwd_cells);
+    rc |= upload(ctx, &g.fwd_off, fwd_off);
+    rc |= upload(ctx, &g.bwd_cells, bwd_cells);
+    rc |= upload(ctx, &g.bwd_off, bwd_off);
+    g.nFwdLevels = nfl; g.nBwdLevels = nbl;
+    g.walldist = nullptr;
+    if (rc) { std::string e = ctx->err; phx_ctx_destroy(ctx); (void)e; return PHX_ERR_CUDA; }
+
+    // state and work arrays
+    rc |= dalloc(ctx, &ctx->q64[0], (size_t)5 * nt);
+    rc |= dalloc(ctx, &ctx->q64[1], (size_t)5 * nt);
+    rc |= dalloc(ctx, &ctx->red, 1);
+    rc |= dalloc(ctx, &ctx->neglist, 1 << 16);
+    auto make_work = [&](auto &w, auto *tag) -> int {
+        using T = std::remove_pointer_t<decltype(tag)>;
+        int r = 0;
+        if (std::is_same<T, double>::value) w.qw = (T *)ctx->q64[0];
+        else r |= dalloc(ctx, &w.qw, (size_t)5 * nt);
+        r |= dalloc(ctx, &w.grad, (size_t)15 * nc);
+        r |= dalloc(ctx, &w.limit, (size_t)nt);
+        r |= dalloc(ctx, &w.res, (size_t)5 * nc);
+        r |= dalloc(ctx, &w.invspec, (size_t)nc);
+        r |= dalloc(ctx, &w.visspec, (size_t)nc);
+        r |= dalloc(ctx, &w.dtraw, (size_t)nc);
+        r |= dalloc(ctx, &w.dq, (size_t)5 * nt);
+        r |= dalloc(ctx, &w.dflux, (size_t)5 * nc);
+        r |= dalloc(ctx, &w.diag, (size_t)nc);
+        if (!r) {
+            // ghost limiter: 1 next to walls / symmetry, 0 next to far field (SetLimitBoundary)
+            std::vector<T> gl(nt, T(1));
+            for (int f = 0; f < nb; ++f) if (limiter_zeroed(btype[f])) gl[nc + f] = T(0);
+            if (cudaMemcpy(w.limit, gl.data(), sizeof(T) * nt, cudaMemcpyHostToDevice) != cudaSuccess) r = PHX_ERR_CUDA;
+            if (cudaMemset(w.dq, 0, sizeof(T) * 5 * (size_t)nt) != cudaSuccess) r = PHX_ERR_CUDA;
+            if (cudaMemset(w.visspec, 0, sizeof(T) * (size_t)nc) != cudaSuccess) r = PHX_ERR_CUDA;
+        }
+        return r;
+    };
+    if (ctx->mixed) rc |= make_work(ctx->w32, (float *)nullptr);
+    else rc |= make_work(ctx->w64, (double *)nullptr);
+    if (rc) { phx_ctx_destroy(ctx); return PHX_ERR_CUDA; }
+    if (cudaMemset(ctx->red, 0, sizeof(Reduce)) != cudaSuccess) { phx_ctx_destroy(ctx); return PHX_ERR_CUDA; }
+
+    // free-stream initial state (NSSolverUnstruct::InitFlow), ghosts included
+    std::vector<double> q0((size_t)5 * nt);
+    for (int m = 0; m < 5; ++m) std::fill(q0.begin() + (size_t)m * nt, q0.begin() + (size_t)(m + 1) * nt, k.primInf[m]);
+    *out = ctx;
+    return phx_set_state(ctx, PHX_Q, q0.data(), (int64_t)q0.size());
+}
+
+int phx_ctx_destroy(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_OK;
+    for (void *p : ctx->allocs) cudaFree(p);
+    delete ctx;
+    return PHX_OK;
+}
+
+const char *phx_last_error(const phx_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int phx_set_stream(phx_ctx *ctx, void *stream)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    ctx->stream = (cudaStream_t)stream;
+    return PHX_OK;
+}
+
+int phx_device(const phx_ctx *ctx) { return ctx ? ctx->device : -1; }
+int phx_set_step(phx_ctx *ctx, int step) { if (!ctx || step < 0) return PHX_ERR_ARG; ctx->step = step; return PHX_OK; }
+int phx_get_step(const phx_ctx *ctx) { return ctx ? ctx->step : -1; }
+int64_t phx_launch_count(const phx_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+// --- state I/O -------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct Sel {
+    void *ptr;         // device pointer
+    bool isFloat;      // element type of the device array
+    int rows;          // variables
+    int stride;        // device elements per row
+    int hostLen;       // host elements per row (nTotal or nCell)
+    bool writable;
+};
+
+template <class T>
+Sel select_work(phx_ctx *ctx, const Work<T> &w, int which)
+{
+    const bool f = std::is_same<T, float>::value;
+    const int nt = ctx->nTotal, nc = ctx->nCell;
+    switch (which) {
+    case PHX_RES: return {w.res, f, 5, nc, nt, true};
+    case PHX_LIMIT: return {w.limit, f, 1, nt, nt, true};
+    case PHX_GRADX: return {w.grad, f, 5, nc, nt, true};
+    case PHX_GRADY: return {w.grad + (size_t)5 * nc, f, 5, nc, nt, true};
+    case PHX_GRADZ: return {w.grad + (size_t)10 * nc, f, 5, nc, nt, true};
+    case PHX_DQ: return {w.dq, f, 5, nt, nt, true};
+    case PHX_INVSPEC: return {w.invspec, f, 1, nc, nc, true};
+    case PHX_VISSPEC: return {w.visspec, f, 1, nc, nc, true};
+    default: return {nullptr, false, 0, 0, 0, false};
+    }
+}
+
+Sel select_state(phx_ctx *ctx, int which)
+{
+    if (which == PHX_Q) return {ctx->q64[ctx->cur], false, 5, ctx->nTotal, ctx->nTotal, true};
+    return ctx->mixed ? select_work(ctx, ctx->w32, which) : select_work(ctx, ctx->w64, which);
+}
+
+}  // namespace
+
+extern "C" {
+
+static int copy_state(phx_ctx *ctx, int which, const double *src, double *dst, int64_t n, bool toDevice, bool hostSide)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (which == PHX_DT) {
+        if (toDevice) return fail(ctx, PHX_ERR_ARG, "dt is derived; it cannot be set");
+        // the reference's dt after ReduceMaxTimeStep: min(dt, ktmax * min dt) / vol, ghosts copied
+        const int nc = ctx->nCell, nt = ctx->nTotal;
+        if (n != nt) return fail(ctx, PHX_ERR_ARG, "dt holds nTotal values");
+        std::vector<double> raw(nc);
+        Reduce red;
+        PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        PHX_CUDA(ctx, cudaMemcpy(&red, ctx->red, sizeof(Reduce), cudaMemcpyDeviceToHost));
+        if (ctx->mixed) {
+            std::vector<float> t(nc);
+            PHX_CUDA(ctx, cudaMemcpy(t.data(), ctx->w32.dtraw, sizeof(float) * nc, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < nc; ++i) raw[i] = t[i];
+        } else {
+            PHX_CUDA(ctx, cudaMemcpy(raw.data(), ctx->w64.dtraw, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+        }
+        double mindt;
+        std::memcpy(&mindt, &red.mindt_bits, sizeof(double));
+        std::vector<double> out(nt);
+        for (int i = 0; i < nc; ++i) {
+            double d = raw[i];
+            if (ctx->nc.ktmax > 0) d = std::min(d, ctx->nc.ktmax * mindt);
+            out[i] = d / ctx->geom[10][i];
+        }
+        {
+            std::vector<int> left(ctx->nBFace);
+            if (ctx->nBFace)
+                PHX_CUDA(ctx, cudaMemcpy(left.data(), ctx->g.left, sizeof(int) * ctx->nBFace, cudaMemcpyDeviceToHost));
+            for (int f = 0; f < ctx->nBFace; ++f) out[nc + f] = out[left[f]];
+        }
+        if (hostSide) std::memcpy(dst, out.data(), sizeof(double) * nt);
+        else PHX_CUDA(ctx, cudaMemcpy(dst, out.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
+        return PHX_OK;
+    }
+    Sel s = select_state(ctx, which);
+    if (!s.ptr) return fail(ctx, PHX_ERR_ARG, "unknown or unavailable state selector");
+    if (n != (int64_t)s.rows * s.hostLen) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
+    const cudaMemcpyKind kin = hostSide ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind kout = hostSide ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int cols = std::min(s.stride, s.hostLen);
+    if (!s.isFloat) {
+        for (int r = 0; r < s.rows; ++r) {
+            double *d = (double *)s.ptr + (size_t)r * s.stride;
+            if (toDevice) {
+                PHX_CUDA(ctx, cudaMemcpy(d, src + (size_t)r * s.hostLen, sizeof(double) * cols, kin));
+            } else {
+                PHX_CUDA(ctx, cudaMemcpy(dst + (size_t)r * s.hostLen, d, sizeof(double) * cols, kout));
+                if (s.hostLen > cols) {
+                    if (hostSide) std::fill(dst + (size_t)r * s.hostLen + cols, dst + (size_t)(r + 1) * s.hostLen, 0.0);
+                    else PHX_CUDA(ctx, cudaMemset(dst + (size_t)r * s.hostLen + cols, 0, sizeof(double) * (s.hostLen - cols)));
+                }
+            }
+        }
+    } else {
+        if (!hostSide) return fail(ctx, PHX_ERR_ARG, "device-pointer copies of mixed-precision arrays are not supported");
+        std::vector<float> t(cols);
+        for (int r = 0; r < s.rows; ++r) {
+            float *d = (float *)s.ptr + (size_t)r * s.stride;
+            if (toDevice) {
+                for (int i = 0; i < cols; ++i) t[i] = (float)src[(size_t)r * s.hostLen + i];
+                PHX_CUDA(ctx, cudaMemcpy(d, t.data(), sizeof(float) * cols, cudaMemcpyHostToDevice));
+            } else {
+                PHX_CUDA(ctx, cudaMemcpy(t.data(), d, sizeof(float) * cols, cudaMemcpyDeviceToHost));
+                for (int i = 0; i < cols; ++i) dst[(size_t)r * s.hostLen + i] = t[i];
+                for (int i = cols; i < s.hostLen; ++i) dst[(size_t)r * s.hostLen + i] = 0.0;
+            }
+        }
+    }
+    if (toDevice && which == PHX_Q && ctx->mixed) {
+        // keep the FP32 working copy in step with the FP64 master state
+        std::vector<float> t((size_t)5 * ctx->nTotal);
+        std::vector<double> h((size_t)5 * ctx->nTotal);
+        PHX_CUDA(ctx, cudaMemcpy(h.data(), ctx->q64[ctx->cur], sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < h.size(); ++i) t[i] = (float)h[i];
+        PHX_CUDA(ctx, cudaMemcpy(ctx->w32.qw, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
+    }
+    return PHX_OK;
+}
+
+int phx_set_state(phx_ctx *ctx, int which, const double *host, int64_t n)
+{
+    if (!host) return fail(ctx, PHX_ERR_ARG, "null host pointer");
+    return copy_state(ctx, which, host, nullptr, n, true, true);
+}
+int phx_get_state(phx_ctx *ctx, int which, double *host, int64_t n)
+{
+    if (!host) return fail(ctx, PHX_ERR_ARG, "null host pointer");
+    return copy_state(ctx, which, nullptr, host, n, false, true);
+}
+int phx_set_state_device(phx_ctx *ctx, int which, const double *dev, int64_t n)
+{
+    if (!dev) return fail(ctx, PHX_ERR_ARG, "null device pointer");
+    return copy_state(ctx, which, dev, nullptr, n, true, false);
+}
+int phx_get_state_device(phx_ctx *ctx, int which, double *dev, int64_t n)
+{
+    if (!dev) return fail(ctx, PHX_ERR_ARG, "null device pointer");
+    return copy_state(ctx, which, nullptr, dev, n, false, false);
+}
+
+int phx_get_geometry(phx_ctx *ctx, const char *name, double *host, int64_t n)
+{
+    if (!ctx || !name || !host) return PHX_ERR_ARG;
+    for (int i = 0; i < 12; ++i) {
+        if (std::strcmp(name, kGeomNames[i]) == 0) {
+            if ((size_t)n != ctx->geom[i].size()) return fail(ctx, PHX_ERR_ARG, "geometry size mismatch");
+            std::memcpy(host, ctx->geom[i].data(), sizeof(double) * n);
+            return PHX_OK;
+        }
+    }
+    return fail(ctx, PHX_ERR_ARG, std::string("unknown geometry array ") + name);
+}
+
+// --- phases ----------------------------------------------------------------
+
+static __global__ void reset_reduce_kernel(Reduce *r)
+{
+    r->mindt_bits = 0x7FEFFFFFFFFFFFFFULL;  // largest finite double
+    for (int k = 0; k < 5; ++k) r->resnorm[k] = 0.0;
+    r->negcount = 0;
+}
+
+static __global__ void finish_step_kernel(Reduce *r, double *hist, int i, double ncell)
+{
+    double v = sqrt(r->resnorm[0] / ncell);
+    if (!(v == v) || v > 1.0e300) r->error = PHX_ERR_NUMERIC;
+    if (hist) hist[i] = v;
+}
+
+static double cfl_at(const NsConst &c, int step)
+{
+    // NSSolver::ComputeCFL, CFD/NSSolver/src/NSSolver.cpp:595-668 (cflMethod 0)
+    if (step >= c.cflVaryStep) return c.cflEnd;
+    return c.cflStart + (c.cflEnd - c.cflStart) * step / c.cflVaryStep;
+}
+
+static int check_launch(phx_ctx *ctx, int n = 1)
+{
+    ctx->launches += n;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, PHX_ERR_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+    return PHX_OK;
+}
+
+int phx_ns_boundary(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (ctx->mixed) launch_boundary<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32.qw, ctx->stream);
+    else launch_boundary<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->q64[ctx->cur], ctx->stream);
+    return check_launch(ctx);
+}
+
+int phx_ns_gradient_limiter(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (ctx->mixed) launch_gradient_limiter<float>(ctx->g, ctx->nc, ctx->w32, ctx->stream);
+    else launch_gradient_limiter<double>(ctx->g, ctx->nc, ctx->w64, ctx->stream);
+    return check_launch(ctx);
+}
+
+int phx_ns_residual(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    reset_reduce_kernel<<<1, 1, 0, ctx->stream>>>(ctx->red);
+    const double cfl = cfl_at(ctx->nc, ctx->step);
+    if (ctx->mixed) launch_residual<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, cfl, ctx->stream);
+    else launch_residual<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, cfl, ctx->stream);
+    ctx->haveResidual = true;
+    return check_launch(ctx, 2);
+}
+
+int phx_ns_lusgs(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs needs phx_ns_residual first");
+    int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->q64[ctx->cur], ctx->red, ctx->numSMs, ctx->stream)
+                       : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->q64[ctx->cur], ctx->red, ctx->numSMs, ctx->stream);
+    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
+    return check_launch(ctx);
+}
+
+int phx_ns_update(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    const int nxt = 1 - ctx->cur;
+    double *qo = ctx->q64[ctx->cur], *qn = ctx->q64[nxt];
+    if (ctx->mixed) {
+        launch_update<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->w32.qw, ctx->red, ctx->neglist, ctx->stream);
+        launch_solution_fix<float>(ctx->g, ctx->nc, qo, qn, ctx->w32.qw, ctx->red, ctx->neglist, ctx->stream);
+    } else {
+        launch_update<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, qn, ctx->red, ctx->neglist, ctx->stream);
+        launch_solution_fix<double>(ctx->g, ctx->nc, qo, qn, qn, ctx->red, ctx->neglist, ctx->stream);
+        ctx->w64.qw = qn;
+    }
+    ctx->cur = nxt;
+    return check_launch(ctx, 2);
+}
+
+static int relax_one(phx_ctx *ctx, double *dhist, int i)
+{
+    ctx->step += 1;   // Simulation::UpdateOuterIterationStep
+    int rc;
+    if ((rc = phx_ns_boundary(ctx))) return rc;
+    if ((rc = phx_ns_gradient_limiter(ctx))) return rc;
+    if ((rc = phx_ns_residual(ctx))) return rc;
+    if ((rc = phx_ns_lusgs(ctx))) return rc;
+    if ((rc = phx_ns_update(ctx))) return rc;
+    finish_step_kernel<<<1, 1, 0, ctx->stream>>>(ctx->red, dhist, i, (double)ctx->nCell);
+    return check_launch(ctx);
+}
+
+int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
+{
+    if (!ctx || nsteps < 0) return PHX_ERR_ARG;
+    if (nsteps > ctx->histCap) {
+        double *h = nullptr;
+        int rc = dalloc(ctx, &h, (size_t)nsteps);
+        if (rc) return rc;
+        ctx->hist = h;
+        ctx->histCap = nsteps;
+    }
+    for (int i = 0; i < nsteps; ++i) {
+        int rc = relax_one(ctx, ctx->hist, i);
+        if (rc) return rc;
+    }
+    Reduce red;
+    PHX_CUDA(ctx, cudaMemcpyAsync(&red, ctx->red, sizeof(Reduce), cudaMemcpyDeviceToHost, ctx->stream));
+    if (res_hist && nsteps > 0)
+        PHX_CUDA(ctx, cudaMemcpyAsync(res_hist, ctx->hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS level barrier timed out");
+    if (red.error == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
+    return PHX_OK;
+}
+
+int phx_residual_norm(phx_ctx *ctx, double out[5])
+{
+    if (!ctx || !out) return PHX_ERR_ARG;
+    const int nc = ctx->nCell;
+    std::vector<double> r((size_t)5 * ctx->nTotal);
+    int rc = phx_get_state(ctx, PHX_RES, r.data(), (int64_t)r.size());
+    if (rc) return rc;
+    for (int m = 0; m < 5; ++m) {
+        double s = 0.0;
+        for (int c = 0; c < nc; ++c) s += r[(size_t)m * ctx->nTotal + c] * r[(size_t)m * ctx->nTotal + c];
+        out[m] = std::sqrt(s / nc);
+    }
+    return PHX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,666 @@
+// sm_100a kernels of the NS per-iteration path.
+//
+// Every kernel is owner-computes over cells: a cell gathers from its faces in
+// ascending face order (the order LoadFlux and the Green-Gauss loop of the
+// reference accumulate in), so no atomics touch the state and the FP64 path
+// reproduces the reference's summation order.  Face metrics stay FP64; the
+// working state T is double (FP64 path) or float (mixed path).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "phx_internal.h"
+#include "phx_physics.cuh"
+
+namespace phx {
+
+static constexpr int kThreads = 256;
+
+template <class T> __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+// Loads of data written earlier in the same kernel by other blocks: bypass L1.
+template <class T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
+
+// ---------------------------------------------------------------------------
+// Boundary: ghost-cell state per boundary face (NSSolverUnstruct::Boundary,
+// NSSolverUnstruct.cpp:13404-13515): SymmetryBCRegion (:19413),
+// ViscousAdiabaticWallBCRegion (:20988), FarfieldBCRegion (:21195).
+// Computed in FP64 from the FP64 master state.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, T *qw)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= g.nBFace) return;
+    const int nt = g.nTotal;
+    const int le = g.left[f], re = g.nCell + f;
+    double r = q[le], u = q[nt + le], v = q[2 * nt + le], w = q[3 * nt + le], p = q[4 * nt + le];
+    double xn = g.xfn[f], yn = g.yfn[f], zn = g.zfn[f];
+    double o[5] = {r, u, v, w, p};
+    int kind = g.bkind[f];
+    if (kind == BK_SYMMETRY) {
+        double vn = xn * u + yn * v + zn * w;
+        o[1] = u - 2.0 * xn * vn;
+        o[2] = v - 2.0 * yn * vn;
+        o[3] = w - 2.0 * zn * vn;
+    } else if (kind == BK_WALL) {
+        o[1] = -u; o[2] = -v; o[3] = -w;
+    } else if (kind == BK_FARFIELD) {
+        const double *pi = c.primInf;
+        double rO = pi[0], uO = pi[1], vO = pi[2], wO = pi[3], pO = pi[4];
+        double gl = c.gama;
+        double cO = sqrt(fabs(gl * pO / rO));
+        double vnO = xn * uO + yn * vO + zn * wO;
+        double vnI = xn * u + yn * v + zn * w;
+        double cI = sqrt(fabs(gl * p / r));
+        double gm1 = gl - 1.0;
+        double velI = sqrt(u * u + v * v + w * w);
+        if (velI > cI) {
+            if (vnI < 0.0) { for (int k = 0; k < 5; ++k) o[k] = pi[k]; }
+        } else {
+            double Rp = vnI + 2.0 * cI / gm1;
+            double Rm = vnO - 2.0 * cO / gm1;
+            double vnB = 0.5 * (Rp + Rm);
+            double cB = 0.25 * (Rp - Rm) * gm1;
+            double s, vtx, vty, vtz;
+            if (vnB >= 0.0) {
+                s = p / pow(r, gl);
+                vtx = u - xn * vnI; vty = v - yn * vnI; vtz = w - zn * vnI;
+            } else {
+                s = pO / pow(rO, gl);
+                vtx = uO - xn * vnO; vty = vO - yn * vnO; vtz = wO - zn * vnO;
+            }
+            double rB = pow((cB * cB / (s * gl)), 1.0 / gm1);
+            o[0] = rB;
+            o[1] = vtx + xn * vnB;
+            o[2] = vty + yn * vnB;
+            o[3] = vtz + zn * vnB;
+            o[4] = cB * cB * rB / gl;
+        }
+    }
+    for (int k = 0; k < 5; ++k) {
+        q[k * nt + re] = o[k];
+        if ((void *)qw != (void *)q) qw[k * nt + re] = (T)o[k];
+    }
+}
+
+template <class T>
+void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, T *qw, cudaStream_t s)
+{
+    if (g.nBFace == 0) return;
+    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, qw);
+}
+
+// ---------------------------------------------------------------------------
+// Gradient + limiter, fused per cell:
+//  Green-Gauss cell gradient (UnstructGrid::CompGradientGGCell,
+//  Geo_UnstructGrid.cpp:3220-3284) of the 5 primitives; then the scalar
+//  Venkatakrishnan limiter from rho and p (Limiter::VencatLimiter7,
+//  Limiter.cpp:1091-1200, neighbour min/max of Limiter::MinMaxDiff
+//  :1202-1252 over interior faces), zeroed next to far-field boundaries
+//  (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, NsConst c, Work<T> w)
+{
+    int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= g.nCell) return;
+    const int nt = g.nTotal, nc = g.nCell;
+    const T *q = w.qw;
+    T qc[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qc[k] = q[k * nt + cell];
+    T gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
+    T rmin = qc[0], rmax = qc[0], pmin = qc[4], pmax = qc[4];
+    const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+    for (int j = j0; j < j1; ++j) {
+        const int f = ld(g.c2f + j);
+        const int le = ld(g.left + f);
+        const bool isLeft = (le == cell);
+        const int nb = isLeft ? (f < g.nBFace ? nc + f : ld(g.right + f)) : le;
+        const double a = ld(g.area + f);
+        const T nx = (T)(ld(g.xfn + f) * a), ny = (T)(ld(g.yfn + f) * a), nz = (T)(ld(g.zfn + f) * a);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            T qn = q[k * nt + nb];
+            T qf = T(0.5) * (isLeft ? (qc[k] + qn) : (qn + qc[k]));
+            if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
+            else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+        }
+        if (f >= g.nBFace) {
+            T rn = q[nb], pn = q[4 * nt + nb];
+            rmin = tmin(rmin, rn); rmax = tmax(rmax, rn);
+            pmin = tmin(pmin, pn); pmax = tmax(pmax, pn);
+        }
+    }
+    const T ovol = T(1) / (T)ld(g.vol + cell);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol;
+        w.grad[(0 * 5 + k) * nc + cell] = gx[k];
+        w.grad[(1 * 5 + k) * nc + cell] = gy[k];
+        w.grad[(2 * 5 + k) * nc + cell] = gz[k];
+    }
+    T lim = T(1);
+    if (c.limiter == 1) {
+        const T vp = (T)ld(g.volpow + cell);
+        T er = (T)c.venkatK3 * qc[0]; er = er * qc[0]; er = er * vp;
+        T ep = (T)c.venkatK3 * qc[4]; ep = ep * qc[4]; ep = ep * vp;
+        const T dminr = rmin - qc[0], dmaxr = rmax - qc[0];
+        const T dminp = pmin - qc[4], dmaxp = pmax - qc[4];
+        const double xc = ld(g.xcc + cell), yc = ld(g.ycc + cell), zc = ld(g.zcc + cell);
+        const T small = (T)kSmall;
+        for (int j = j0; j < j1; ++j) {
+            const int f = ld(g.c2f + j);
+            const T dx = (T)(ld(g.xfc + f) - xc), dy = (T)(ld(g.yfc + f) - yc), dz = (T)(ld(g.zfc + f) - zc);
+            T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
+            if (d > small) lim = tmin(lim, venfun(dmaxr, d, er));
+            else if (d < -small) lim = tmin(lim, venfun(dminr, d, er));
+            d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
+            if (d > small) lim = tmin(lim, venfun(dmaxp, d, ep));
+            else if (d < -small) lim = tmin(lim, venfun(dminp, d, ep));
+        }
+        if (g.farfield_adj[cell]) lim = T(0);
+    }
+    w.limit[cell] = lim;
+}
+
+template <class T>
+void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s)
+{
+    gradient_limiter_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
+}
+
+// ---------------------------------------------------------------------------
+// Residual: for every face of the cell, the MUSCL face states
+// (GetQlQr / ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193),
+// the wall / symmetry face fix (BoundaryQlQrFix, :13725-13951), the Roe flux
+// times the face area (InviscidFluxWrap, :14466-14488), gathered into res with
+// the sign LoadFlux applies (:6435-6495); the inviscid spectral radius
+// (SpectrumRadiusInviscid, :5749-5850); and in the epilogue the local time
+// step (LocalTimeStep / LimitCFL, :5999-6118) with its device-wide minimum
+// (Controller::ComputeMinTimeStep, Controller.cpp:706-752).
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void load_side(const DevGrid &g, const Work<T> &w, int cell, int face, T lim, T *qo)
+{
+    const int nt = g.nTotal, nc = g.nCell;
+    T qs[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qs[k] = w.qw[k * nt + cell];
+    if (cell < nc) {
+        const T dx = (T)(ld(g.xfc + face) - ld(g.xcc + cell));
+        const T dy = (T)(ld(g.yfc + face) - ld(g.ycc + cell));
+        const T dz = (T)(ld(g.zfc + face) - ld(g.zcc + cell));
+        T tr[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            tr[k] = qs[k] + lim * (w.grad[(0 * 5 + k) * nc + cell] * dx + w.grad[(1 * 5 + k) * nc + cell] * dy +
+                                   w.grad[(2 * 5 + k) * nc + cell] * dz);
+        if (tr[0] > T(0) && tr[4] > T(0)) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) qs[k] = tr[k];
+        }
+    }
+    // ghost cells carry a zero gradient (CompGradientGGCell never writes them),
+    // so their reconstruction returns the ghost state itself
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qo[k] = qs[k];
+}
+
+template <class T>
+__device__ __forceinline__ void face_flux(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, T *fa)
+{
+    const int nc = g.nCell, nt = g.nTotal;
+    const int le = ld(g.left + f);
+    const int re = f < g.nBFace ? nc + f : ld(g.right + f);
+    T limL = w.limit[le], limR = w.limit[re];
+    if (c.reconMethod == 1) { T m = tmin(limL, limR); limL = limR = m; }
+    T ql[5], qr[5];
+    load_side(g, w, le, f, limL, ql);
+    load_side(g, w, re, f, limR, qr);
+    const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
+    if (f < g.nBFace) {
+        const int kind = g.bkind[f];
+        const int bt = g.btype[f];
+        if (bt == PHX_BC_SOLID_SURFACE || bt == PHX_BC_SYMMETRY) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                T a = T(0.5) * (w.qw[k * nt + le] + w.qw[k * nt + re]);
+                ql[k] = a; qr[k] = a;
+            }
+            if (bt == PHX_BC_SYMMETRY) {
+                T vn = T(2) * (xn * ql[1] + yn * ql[2] + zn * ql[3]);
+                qr[1] = ql[1] - vn * xn; qr[2] = ql[2] - vn * yn; qr[3] = ql[3] - vn * zn;
+            } else if (kind == BK_WALL) {
+                ql[1] = ql[2] = ql[3] = T(0);
+                qr[1] = qr[2] = qr[3] = T(0);
+            }
+        }
+    }
+    const T gm = (T)c.gama;
+    roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fa);
+    const T a = (T)ld(g.area + f);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fa[k] *= a;
+}
+
+__device__ __forceinline__ void atomic_min_pos_double(unsigned long long *addr, double v)
+{
+    atomicMin(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) residual_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red, double cfl)
+{
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = g.nTotal, nc = g.nCell;
+    double mydt = kLarge;
+    if (cell < nc) {
+        T res[5] = {0, 0, 0, 0, 0};
+        T spec = T(0);
+        const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+        for (int j = j0; j < j1; ++j) {
+            const int f = ld(g.c2f + j);
+            const int le = ld(g.left + f);
+            const bool isLeft = (le == cell);
+            T fa[5];
+            face_flux<T>(g, c, w, f, fa);
+            if (isLeft) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) res[k] -= fa[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) res[k] += fa[k];
+            }
+            // inviscid spectral radius from the face-mean state
+            const int re = f < g.nBFace ? nc + f : ld(g.right + f);
+            const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
+            const T *q = w.qw;
+            T vnl = xn * q[nt + le] + yn * q[2 * nt + le] + zn * q[3 * nt + le];
+            T vnr = xn * q[nt + re] + yn * q[2 * nt + re] + zn * q[3 * nt + re];
+            T gm = T(0.5) * ((T)c.gama + (T)c.gama);
+            T pm = T(0.5) * (q[4 * nt + le] + q[4 * nt + re]);
+            T rm = T(0.5) * (q[le] + q[re]);
+            T vn = T(0.5) * (vnl + vnr);
+            T cm = sqrt(gm * pm / rm);
+            spec += T(0.5) * (T)ld(g.area + f) * (fabs(vn) + cm);
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w.res[k * nc + cell] = res[k];
+        w.invspec[cell] = spec;
+        if (c.viscous) spec += w.visspec[cell];
+        // LimitCFL: pressure- and skewness-based CFL of the cell
+        double cc = cfl;
+        const double pc = (double)w.qw[4 * nt + cell];
+        const double plo = 0.001 * c.pTotal, phi = 0.02 * c.pTotal;
+        if (pc < plo) cc = c.cflStart;
+        else if (pc < phi) cc = (pc - phi) * (cfl - c.cflStart) / (phi - plo) + cfl;
+        const double sk = ld(g.skew + cell);
+        if (sk < 0.1) cc *= 0.1;
+        else if (sk < 10.0) cc *= (1.0 - exp(0.0 - sk));
+        T dt = (T)cc * (T)ld(g.vol + cell) / spec;
+        w.dtraw[cell] = dt;
+        mydt = (double)dt;
+    }
+    // device-wide minimum of dt (positive doubles order like unsigned integers)
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    if ((threadIdx.x & 31) == 0 && mydt < kLarge) atomic_min_pos_double(&red->mindt_bits, mydt);
+}
+
+template <class T>
+void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
+{
+    residual_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, red, cfl);
+}
+
+// ---------------------------------------------------------------------------
+// LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955): one persistent kernel
+// per solve runs the forward sweep level by level, the ghost-cell dq, and the
+// backward sweep level by level.  Levels come from the reference's own cell
+// order (a cell depends on its face neighbours of lower index in the forward
+// sweep, higher index in the backward sweep), so every cell sees exactly the
+// neighbour values the sequential sweep of the reference sees.  Between
+// levels a device-wide barrier; every wait is bounded (a timeout sets
+// Reduce::error and the kernel returns).
+// ---------------------------------------------------------------------------
+static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling
+
+__device__ __forceinline__ bool grid_barrier(Reduce *red, unsigned int &gen, int nblocks)
+{
+    if (nblocks == 1) { __syncthreads(); return true; }
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        int arrived = atomicAdd(&red->barrier_count, 1);
+        if (arrived == nblocks - 1) {
+            atomicExch(&red->barrier_count, 0);
+            __threadfence();
+            atomicAdd(&red->barrier_gen, 1u);
+        } else {
+            long long spins = 0;
+            while (((volatile unsigned int *)&red->barrier_gen)[0] == gen) {
+                if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
+                    atomicExch(&red->error, PHX_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        gen += 1;
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Contribution of the neighbour across face f to the sweep of `cell`
+// (SolveLUSGSForward body, NSSolverUnstruct.cpp:15251-15370).
+template <class T>
+__device__ __forceinline__ void lusgs_face(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell, int f, T *df)
+{
+    const int nt = g.nTotal, nc = g.nCell;
+    int le = ld(g.left + f);
+    int re = f < g.nBFace ? nc + f : ld(g.right + f);
+    T nx = (T)ld(g.xfn + f), ny = (T)ld(g.yfn + f), nz = (T)ld(g.zfn + f);
+    if (re == cell) { int s = le; le = re; re = s; nx = -nx; ny = -ny; nz = -nz; }
+    T ql[5], qn[5], dqn[5], fp[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        ql[k] = w.qw[k * nt + le];
+        qn[k] = w.qw[k * nt + re];
+        dqn[k] = ldcg(w.dq + k * nt + re);
+    }
+    const T gm = (T)c.gama;
+    roe_average<T>(ql, gm, qn, gm, fp);
+    const T area = (T)ld(g.area + f);
+    T vn = nx * fp[1] + ny * fp[2] + nz * fp[3];
+    T rad = (fabs(vn) + sqrt(gm * fp[4] / fp[0])) * area;
+    mxdq<T>(qn, nx, ny, nz, area, gm, dqn, df, rad);
+}
+
+// Ghost-cell dq between the sweeps (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810;
+// SetSymmBCGhostDQLUSGS :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).
+template <class T>
+__device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, int f)
+{
+    const int nt = g.nTotal, nc = g.nCell;
+    const int le = g.left[f], re = nc + f;
+    const int kind = g.bkind[f];
+    T *dq = w.dq;
+    T dl[5];
+    for (int k = 0; k < 5; ++k) dl[k] = ldcg(dq + k * nt + le);
+    if (kind == BK_SYMMETRY) {
+        const T *q = w.qw;
+        T r = q[le], u = q[nt + le], v = q[2 * nt + le], ww = q[3 * nt + le], pp = q[4 * nt + le];
+        T gm = (T)c.gama;
+        T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
+        T Q[5] = {r, r * u, r * v, r * ww, r * em};
+        for (int k = 0; k < 5; ++k) Q[k] += dl[k];
+        T rm = q[re], um = q[nt + re], vm = q[2 * nt + re], wm = q[3 * nt + re], pm = q[4 * nt + re];
+        T xn = (T)g.xfn[f], yn = (T)g.yfn[f], zn = (T)g.zfn[f];
+        dq[re] = dl[0];
+        T rvn = T(2) * (xn * dl[1] + yn * dl[2] + zn * dl[3]);
+        dq[nt + re] = dl[1] - xn * rvn;
+        dq[2 * nt + re] = dl[2] - yn * rvn;
+        dq[3 * nt + re] = dl[3] - zn * rvn;
+        rvn = T(2) * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
+        T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
+        T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
+        T g1 = gm - T(1);
+        dq[4 * nt + re] = pnew - pm / g1 + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - rm * (um * um + vm * vm + wm * wm));
+    } else if (kind == BK_WALL) {
+        dq[re] = dl[0];
+        dq[nt + re] = -dl[1];
+        dq[2 * nt + re] = -dl[2];
+        dq[3 * nt + re] = -dl[3];
+        dq[4 * nt + re] = dl[4];
+    } else {
+        for (int k = 0; k < 5; ++k) dq[k * nt + re] = T(0);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+{
+    const int nt = g.nTotal, nc = g.nCell;
+    const int nblocks = gridDim.x;
+    const int stride = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ unsigned int sgen;
+    if (threadIdx.x == 0) sgen = ((volatile unsigned int *)&red->barrier_gen)[0];
+    __syncthreads();
+    unsigned int gen = sgen;
+    const double mindt = __longlong_as_double((long long)red->mindt_bits);
+
+    // Diagonal (NSSolverUnstruct.cpp:15867-15935) and dq initialisation
+    // (LUSGSInitialization, Controller.cpp:1765-1777: single sweep, dq = res,
+    // delta flux = 0).
+    for (int cell = tid; cell < nc; cell += stride) {
+        T dt = w.dtraw[cell];
+        if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
+        dt /= (T)g.vol[cell];
+        T d = T(1) / dt;
+        d += w.invspec[cell];
+        if (c.viscous) d += w.visspec[cell];
+        w.diag[cell] = d;
+    }
+    if (!grid_barrier(red, gen, nblocks)) return;
+
+    // forward sweep: dq = (res - Ux - L dq) / D over lower neighbours
+    for (int L = 0; L < g.nFwdLevels; ++L) {
+        const int b = g.fwd_off[L], e = g.fwd_off[L + 1];
+        for (int i = b + tid; i < e; i += stride) {
+            const int cell = g.fwd_cells[i];
+            T rhs0[5] = {0, 0, 0, 0, 0};
+            const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+            for (int j = j0; j < j1; ++j) {
+                const int f = g.c2f[j];
+                if (f < g.nBFace) continue;
+                const int le = g.left[f], re = g.right[f];
+                if (le > cell || re > cell) continue;
+                T df[5];
+                lusgs_face<T>(g, c, w, cell, f, df);
+#pragma unroll
+                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+            }
+            const T dg = ldcg(w.diag + cell);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                T v = (w.res[k * nc + cell] - T(0) - rhs0[k]) / dg;
+                w.dflux[k * nc + cell] = T(0) + rhs0[k];
+                w.dq[k * nt + cell] = v;
+            }
+        }
+        if (!grid_barrier(red, gen, nblocks)) return;
+    }
+    for (int f = tid; f < g.nBFace; f += stride) ghost_dq<T>(g, c, w, f);
+    if (!grid_barrier(red, gen, nblocks)) return;
+
+    // backward sweep: dq = (res - L dq* - U dq) / D over upper neighbours and ghosts
+    for (int L = 0; L < g.nBwdLevels; ++L) {
+        const int b = g.bwd_off[L], e = g.bwd_off[L + 1];
+        for (int i = b + tid; i < e; i += stride) {
+            const int cell = g.bwd_cells[i];
+            T rhs0[5] = {0, 0, 0, 0, 0};
+            const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+            for (int j = j0; j < j1; ++j) {
+                const int f = g.c2f[j];
+                const int le = g.left[f];
+                const int re = f < g.nBFace ? nc + f : g.right[f];
+                if (le < cell || re < cell) continue;
+                T df[5];
+                lusgs_face<T>(g, c, w, cell, f, df);
+#pragma unroll
+                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+            }
+            const T dg = ldcg(w.diag + cell);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                T v = (w.res[k * nc + cell] - ldcg(w.dflux + k * nc + cell) - rhs0[k]) / dg;
+                w.dq[k * nt + cell] = v;
+            }
+        }
+        if (!grid_barrier(red, gen, nblocks)) return;
+    }
+}
+
+template <class T>
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, Reduce *red, int numSMs,
+                 cudaStream_t s)
+{
+    (void)q64;
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kThreads, 0);
+    if (perSM < 1) perSM = 1;
+    // Widest level decides how many blocks are worth their barrier cost.
+    int blocks = numSMs * perSM;
+    int need = (g.nCell + kThreads - 1) / kThreads;
+    if (need < blocks) blocks = need;
+    if (blocks < 1) blocks = 1;
+    DevGrid gg = g;
+    NsConst cc = c;
+    Work<T> ww = w;
+    Reduce *rr = red;
+    void *args[] = {&gg, &cc, &ww, &rr};
+    cudaError_t e = cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kThreads), args, 0, s);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+// ---------------------------------------------------------------------------
+// Update (NSSolverUnstruct::UpdateFlowField, NSSolverUnstruct.cpp:14587-14765):
+// Q_cons (FP64, from the FP64 master primitive state) += dq, back to
+// primitive.  Cells whose density or pressure drop below 1e-6 of the free
+// stream are listed for the ordered SolutionFix pass.  Also reduces the
+// residual monitor sum res_m^2 in FP64 (Residual.cpp:534-600).
+// q_old is read, q_new written (ghosts copied), so the repair pass can see
+// the pre-update state of higher-index neighbours as the in-place sequential
+// loop of the reference does.
+// ---------------------------------------------------------------------------
+static constexpr int kMaxNeg = 1 << 16;
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) update_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo,
+                                                          double *qn, T *qw_out, Reduce *red, int *neglist)
+{
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = g.nTotal, nc = g.nCell;
+    double rs[5] = {0, 0, 0, 0, 0};
+    if (cell < nc) {
+        double r = qo[cell], u = qo[nt + cell], v = qo[2 * nt + cell], ww = qo[3 * nt + cell], p = qo[4 * nt + cell];
+        const double gm = c.gama;
+        double em = (p / r) / (gm - 1.0) + 0.5 * (u * u + v * v + ww * ww);
+        double Q[5] = {r, r * u, r * v, r * ww, r * em};
+#pragma unroll
+        for (int k = 0; k < 5; ++k) Q[k] += (double)w.dq[k * nt + cell];
+        double prim[5];
+        if (Q[0] <= 0.0) {
+            prim[0] = Q[0]; prim[1] = u; prim[2] = v; prim[3] = ww; prim[4] = p;
+        } else {
+            double od = 1.0 / Q[0];
+            double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
+            double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
+            prim[0] = Q[0]; prim[1] = um; prim[2] = vm; prim[3] = wm; prim[4] = (gm - 1.0) * ie;
+        }
+        if (prim[0] < 1.0e-6 * c.primInf[0] || prim[4] < 1.0e-6 * c.primInf[4]) {
+            int slot = atomicAdd(&red->negcount, 1);
+            if (slot < kMaxNeg) neglist[slot] = cell;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            qn[k * nt + cell] = prim[k];
+            if ((void *)qw_out != (void *)qn) qw_out[k * nt + cell] = (T)prim[k];
+            double rv = (double)w.res[k * nc + cell];
+            rs[k] = rv * rv;
+        }
+    }
+    if (cell < g.nBFace) {
+        const int gc = nc + cell;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qn[k * nt + gc] = qo[k * nt + gc];
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double v = rs[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&red->resnorm[k], v);
+    }
+}
+
+template <class T>
+void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new, T *qw_out,
+                   Reduce *red, int *neglist, cudaStream_t s)
+{
+    int n = g.nCell > g.nBFace ? g.nCell : g.nBFace;
+    update_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, q64, q64_new, qw_out, red, neglist);
+}
+
+// SolutionFix (NSSolverUnstruct.cpp:14509-14585) for the listed cells, in
+// ascending cell order: neighbour averages of rho,u,v,w,p (|rho|, |p|),
+// lower-index neighbours taken after their update, higher-index ones before.
+// One thread: the list is empty in healthy runs and short otherwise.
+template <class T>
+__global__ void solution_fix_kernel(DevGrid g, NsConst c, const double *qo, double *qn, T *qw_out, Reduce *red,
+                                    int *neglist)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int n = red->negcount;
+    if (n <= 0) return;
+    if (n > kMaxNeg) { red->error = PHX_ERR_NUMERIC; n = kMaxNeg; }
+    for (int i = 1; i < n; ++i) {  // insertion sort (short list)
+        int v = neglist[i], j = i - 1;
+        while (j >= 0 && neglist[j] > v) { neglist[j + 1] = neglist[j]; --j; }
+        neglist[j + 1] = v;
+    }
+    const int nt = g.nTotal, nc = g.nCell;
+    const double rlim = 1.0e-6 * c.primInf[0], plim = 1.0e-6 * c.primInf[4];
+    for (int i = 0; i < n; ++i) {
+        const int cell = neglist[i];
+        double acc[5] = {0, 0, 0, 0, 0}, wsum = 0.0;
+        for (int j = g.c2f_off[cell]; j < g.c2f_off[cell + 1]; ++j) {
+            const int f = g.c2f[j];
+            const int le = g.left[f], re = f < g.nBFace ? nc + f : g.right[f];
+            const int nb = (cell == le) ? re : le;
+            const double *src = (nb < cell) ? qn : qo;
+            if (src[nb] < rlim || src[4 * nt + nb] < plim) continue;
+            wsum += 1.0;
+            for (int k = 0; k < 5; ++k) {
+                double fv = src[k * nt + nb];
+                if (k == 0 || k == 4) fv = fabs(fv);
+                acc[k] += fv;
+            }
+        }
+        double prim[5];
+        if (wsum > 0.0) { double o = 1.0 / wsum; for (int k = 0; k < 5; ++k) prim[k] = acc[k] * o; }
+        else for (int k = 0; k < 5; ++k) prim[k] = c.primInf[k];
+        for (int k = 0; k < 5; ++k) {
+            qn[k * nt + cell] = prim[k];
+            if ((void *)qw_out != (void *)qn) qw_out[k * nt + cell] = (T)prim[k];
+        }
+    }
+}
+
+template <class T>
+void launch_solution_fix(const DevGrid &g, const NsConst &c, const double *q64, double *q64_new, T *qw_out,
+                         Reduce *red, int *neglist, cudaStream_t s)
+{
+    solution_fix_kernel<T><<<1, 32, 0, s>>>(g, c, q64, q64_new, qw_out, red, neglist);
+}
+
+// Explicit instantiations for the FP64 and mixed paths.
+#define PHX_INSTANTIATE(T)                                                                                      \
+    template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, T *, cudaStream_t);             \
+    template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);   \
+    template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,        \
+                                     cudaStream_t);                                                              \
+    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, Reduce *, int, \
+                                 cudaStream_t);                                                                  \
+    template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *, T *, \
+                                   Reduce *, int *, cudaStream_t);                                               \
+    template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const double *, double *, T *, Reduce *, \
+                                         int *, cudaStream_t);
+PHX_INSTANTIATE(double)
+PHX_INSTANTIATE(float)
+
+}  // namespace phx

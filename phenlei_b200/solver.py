@@ -1,0 +1,220 @@
+"""Python front end of the phx C ABI (include/phx.h), mirroring the solver
+plug-in surface of PHengLEI's NSSolverUnstruct (CFD/NSSolver/include/NSSolverUnstruct.h):
+Boundary, ComputeGradient/ComputeLimiter, UpdateResiduals (+SpectrumRadius,
+TimeStep), LUSGS, UpdateFlowField and the Controller::Relaxation sequence.
+
+Parameters use the reference's hypara key names (cfd_para.hypara); string-valued
+keys take the reference's strings ("roe", "vencat", "ggcell", ...).
+
+The CUDA library is required: there is no CPU path.  Importing this module on
+a machine without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libphx.so")
+
+PHX_FP64, PHX_MIXED = 0, 1
+PHX_Q, PHX_RES, PHX_DT, PHX_LIMIT, PHX_GRADX, PHX_GRADY, PHX_GRADZ, PHX_DQ, PHX_INVSPEC, PHX_VISSPEC = range(10)
+PHX_Q_TURB, PHX_VISL, PHX_VIST, PHX_RES_TURB = 10, 11, 12, 13
+ERRORS = {-1: "PHX_ERR_ARG", -2: "PHX_ERR_CUDA", -3: "PHX_ERR_TIMEOUT", -4: "PHX_ERR_NUMERIC", -5: "PHX_ERR_STATE"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("n_node", C.c_int64), ("n_face", C.c_int64), ("n_cell", C.c_int64), ("n_bface", C.c_int64),
+                ("x", _dp), ("y", _dp), ("z", _dp), ("face_nnode", _ip), ("face2node", _ip),
+                ("left_cell", _ip), ("right_cell", _ip), ("cell_nnode", _ip), ("cell2node", _ip),
+                ("n_region", C.c_int32), ("region_type", _ip), ("bface_region", _ip), ("wall_dist", _dp)]
+
+
+class Params(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("refGama", C.c_double), ("refMachNumber", C.c_double),
+                ("attackd", C.c_double), ("angleSlide", C.c_double), ("viscousType", C.c_int32),
+                ("refReNumber", C.c_double), ("refDimensionalTemperature", C.c_double), ("prl", C.c_double),
+                ("prt", C.c_double), ("tsuth", C.c_double), ("wallTemperature", C.c_double),
+                ("gradientName", C.c_int32), ("uns_limiter_name", C.c_int32), ("ivencat", C.c_int32),
+                ("venkatCoeff", C.c_double), ("reconmeth", C.c_int32), ("uns_scheme_name", C.c_int32),
+                ("roeEntropyFixMethod", C.c_int32), ("roeEntropyScale", C.c_double), ("CFLStart", C.c_double),
+                ("CFLEnd", C.c_double), ("CFLVaryStep", C.c_int32), ("ktmax", C.c_double),
+                ("nLUSGSSweeps", C.c_int32), ("LUSGSTolerance", C.c_double), ("skewnessAngle", C.c_double),
+                ("muoo", C.c_double), ("turbCFLScale", C.c_double), ("sa_source", C.c_int32)]
+
+
+_STRING_KEYS = {
+    "gradientName": {"ggcell": 0, "lsq": 1},
+    "uns_limiter_name": {"nolim": 0, "vencat": 1},
+    "uns_scheme_name": {"roe": 0, "ausmpw+": 1},
+    "precision": {"fp64": PHX_FP64, "mixed": PHX_MIXED},
+    "sa_source": {"exact": 0, "mlp": 1, "mlp_fallback": 2},
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded phx library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"phx CUDA library not built: {LIB_PATH} (python -m phenlei_b200.build)")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.phx_last_error.restype = C.c_char_p
+        _lib.phx_launch_count.restype = C.c_int64
+        _lib.phx_ctx_create.argtypes = [C.POINTER(GridDesc), C.POINTER(Params), C.POINTER(C.c_void_p)]
+        for name in ("phx_set_state", "phx_get_state", "phx_set_state_device", "phx_get_state_device"):
+            getattr(_lib, name).argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+        _lib.phx_get_geometry.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]
+        _lib.phx_ns_relaxation.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.phx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        for name in ("phx_ns_boundary", "phx_ns_gradient_limiter", "phx_ns_residual", "phx_ns_lusgs",
+                     "phx_ns_update", "phx_ctx_destroy", "phx_launch_count", "phx_get_step"):
+            getattr(_lib, name).argtypes = [C.c_void_p]
+        _lib.phx_set_step.argtypes = [C.c_void_p, C.c_int]
+        _lib.phx_residual_norm.argtypes = [C.c_void_p, C.c_void_p]
+    return _lib
+
+
+class PhxError(RuntimeError):
+    pass
+
+
+def make_params(**keys) -> Params:
+    """phx_params from hypara keys on top of the reference defaults."""
+    p = Params()
+    lib().phx_default_params(C.byref(p))
+    for k, v in keys.items():
+        if k in _STRING_KEYS and isinstance(v, str):
+            v = _STRING_KEYS[k][v]
+        if not hasattr(p, k):
+            continue  # keys the path does not read (e.g. tscheme) are accepted and ignored
+        setattr(p, k, v)
+    return p
+
+
+class NSSolverUnstruct:
+    """One phx context: a grid, its FP64 metrics and the device-resident flow state."""
+
+    def __init__(self, mesh, precision="fp64", **params):
+        self.mesh = mesh
+        self._keep = []
+        nb, nc = mesh.n_bface, mesh.n_cell
+        self.nt = nc + nb
+        arr = lambda a, t: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+        a = dict(x=arr(mesh.x, np.float64), y=arr(mesh.y, np.float64), z=arr(mesh.z, np.float64),
+                 fnn=arr(mesh.face_nnode, np.int32), f2n=arr(mesh.face2node, np.int32),
+                 left=arr(mesh.left, np.int32), right=arr(mesh.right, np.int32),
+                 cnn=arr(mesh.cell_nnode, np.int32), c2n=arr(mesh.cell2node, np.int32),
+                 rtype=arr([t for t, _ in mesh.regions], np.int32), breg=arr(mesh.bface_region, np.int32))
+        self._keep.append(a)
+        g = GridDesc()
+        g.n_node, g.n_face, g.n_cell, g.n_bface = mesh.n_node, mesh.n_face, nc, nb
+        d = lambda v: v.ctypes.data_as(_dp)  # noqa: E731
+        i = lambda v: v.ctypes.data_as(_ip)  # noqa: E731
+        g.x, g.y, g.z = d(a["x"]), d(a["y"]), d(a["z"])
+        g.face_nnode, g.face2node, g.left_cell, g.right_cell = i(a["fnn"]), i(a["f2n"]), i(a["left"]), i(a["right"])
+        g.cell_nnode, g.cell2node = i(a["cnn"]), i(a["c2n"])
+        g.n_region, g.region_type, g.bface_region = len(mesh.regions), i(a["rtype"]), i(a["breg"])
+        g.wall_dist = _dp()
+        self.params = make_params(precision=precision, **params)
+        h = C.c_void_p()
+        rc = lib().phx_ctx_create(C.byref(g), C.byref(self.params), C.byref(h))
+        if rc != 0:
+            raise PhxError(f"phx_ctx_create failed: {ERRORS.get(rc, rc)}")
+        self.h = h
+
+    # -- plumbing ------------------------------------------------------------
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = lib().phx_last_error(self.h).decode()
+            raise PhxError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().phx_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int):
+        self._check(lib().phx_set_stream(self.h, C.c_void_p(stream_handle)), "phx_set_stream")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().phx_launch_count(self.h))
+
+    _SHAPES = {PHX_Q: 5, PHX_RES: 5, PHX_DT: 1, PHX_LIMIT: 1, PHX_GRADX: 5, PHX_GRADY: 5, PHX_GRADZ: 5,
+               PHX_DQ: 5, PHX_INVSPEC: -1, PHX_VISSPEC: -1}
+
+    def get(self, which) -> np.ndarray:
+        rows = self._SHAPES[which]
+        if rows < 0:
+            out = np.empty(self.mesh.n_cell)
+        else:
+            out = np.empty((rows, self.nt)) if rows > 1 else np.empty(self.nt)
+        self._check(lib().phx_get_state(self.h, which, out.ctypes.data, out.size), "phx_get_state")
+        return out
+
+    def set(self, which, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(lib().phx_set_state(self.h, which, v.ctypes.data, v.size), "phx_set_state")
+
+    def set_q_cells(self, q_cells: np.ndarray):
+        """Set the primitive state of the interior cells (ghosts are set by Boundary)."""
+        q = self.get(PHX_Q)
+        q[:, : self.mesh.n_cell] = q_cells
+        self.set(PHX_Q, q)
+
+    def geometry(self, name: str) -> np.ndarray:
+        n = self.mesh.n_face if name in ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc") else (
+            self.mesh.n_cell if name in ("skew", "walldist") else self.nt)
+        out = np.empty(n)
+        self._check(lib().phx_get_geometry(self.h, name.encode(), out.ctypes.data, n), "phx_get_geometry")
+        return out
+
+    @property
+    def step(self) -> int:
+        return int(lib().phx_get_step(self.h))
+
+    @step.setter
+    def step(self, v: int):
+        self._check(lib().phx_set_step(self.h, int(v)), "phx_set_step")
+
+    # -- the reference's solver methods ----------------------------------------
+    def Boundary(self):
+        self._check(lib().phx_ns_boundary(self.h), "phx_ns_boundary")
+
+    def ComputeGradientAndLimiter(self):
+        self._check(lib().phx_ns_gradient_limiter(self.h), "phx_ns_gradient_limiter")
+
+    def UpdateResiduals(self):
+        """InviscidFlux + ViscousFlux + LoadFlux, SpectrumRadius and TimeStep."""
+        self._check(lib().phx_ns_residual(self.h), "phx_ns_residual")
+
+    def LUSGS(self):
+        self._check(lib().phx_ns_lusgs(self.h), "phx_ns_lusgs")
+
+    def UpdateFlowField(self):
+        self._check(lib().phx_ns_update(self.h), "phx_ns_update")
+
+    def Relaxation(self, nsteps: int = 1) -> np.ndarray:
+        """nsteps outer iterations; returns the residual monitor per step."""
+        hist = np.zeros(max(nsteps, 1))
+        self._check(lib().phx_ns_relaxation(self.h, nsteps, hist.ctypes.data), "phx_ns_relaxation")
+        return hist[:nsteps]
+
+    def GetResidual(self) -> np.ndarray:
+        out = np.zeros(5)
+        self._check(lib().phx_residual_norm(self.h, out.ctypes.data), "phx_residual_norm")
+        return out

@@ -1,0 +1,67 @@
+"""Generates the golden fixtures in tests/golden/ by running the REFERENCE
+solver itself (oracle/_ref/ref_harness, built from the reference's own
+sources by oracle/refbuild/Makefile) on small seeded cases.
+
+    make -C oracle/refbuild REF=<reference root> -j8 all harness
+    python tests/golden/make_golden.py
+
+Each fixture is an .npz holding the case parameters (as JSON), the input state,
+and the reference's arrays after the requested number of outer iterations.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle.refrun import run_reference  # noqa: E402
+from phenlei_b200 import mesh as M  # noqa: E402
+from phenlei_b200.cases import perturbed_state  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "vencat", "ivencat": 7,
+              "venkatCoeff": 5.0, "gradientName": "ggcell", "reconmeth": 1, "roeEntropyFixMethod": 3, "tscheme": 4,
+              "nLUSGSSweeps": 1, "CFLStart": 0.01, "CFLEnd": 10.0, "CFLVaryStep": 500, "refMachNumber": 0.5,
+              "attackd": 0.0, "refGama": 1.4}
+
+
+def mesh_spec(m, kind, args):
+    return {"kind": kind, "args": args}
+
+
+def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02):
+    m = getattr(M, kind)(**args)
+    nc, nt = m.n_cell, m.n_cell + m.n_bface
+    state = None
+    if perturb_seed is not None:
+        state = perturbed_state(m, params, seed=perturb_seed, amplitude=amplitude)
+    dumps = [("q", 5, nt), ("res", 5, nt), ("dt", 0, nt), ("limit2D", 5, nt), ("gradPrimtiveVarX", 5, nt),
+             ("gradPrimtiveVarY", 5, nt), ("gradPrimtiveVarZ", 5, nt), ("invSpectralRadius", 0, nc)]
+    r = run_reference(m, params, nsteps, dumps=dumps, state=state)
+    out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}),
+           "nsteps": nsteps, "res_hist": r["res_hist"]}
+    if state is not None:
+        out["state_in"] = state
+    for k in ("q", "res", "dt", "gradPrimtiveVarX", "gradPrimtiveVarY", "gradPrimtiveVarZ", "invSpectralRadius",
+              "xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol"):
+        out[k] = r[k]
+    out["limit"] = r["limit2D"][0]
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    # Euler bump, seeded perturbation, one iteration: every intermediate array.
+    fixture("euler_bump_16x8x2_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, EULER_BUMP, 1, perturb_seed=7)
+    # Euler bump from the free stream, 40 iterations through the CFL ramp.
+    fixture("euler_bump_16x8x2_step40", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, EULER_BUMP, 40)
+    # Euler on a jittered tetrahedral cube (all far field), perturbed, 3 iterations.
+    fixture("euler_tetcube_4_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
+            dict(EULER_BUMP, refMachNumber=0.3), 3, perturb_seed=11)

@@ -1,0 +1,42 @@
+"""The oracle (C restatement) against golden vectors produced by the
+reference solver itself (tests/golden/make_golden.py).  CPU only."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from tests.conftest import rel_err
+
+GEOM = ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol")
+
+
+@pytest.mark.parametrize("name", ["euler_bump_16x8x2_step1", "euler_bump_16x8x2_step40", "euler_tetcube_4_step3"])
+def test_oracle_matches_reference(golden, name):
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    o = Oracle(m, d["params_dict"])
+    for k in GEOM:
+        assert rel_err(o.geo[k], d[k]) <= 1e-14, k
+    if "state_in" in d:
+        o.set_state(d["state_in"][:, :nc])
+    hist = o.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(o.q[:, :nc], d["q"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("res")[:, :nc], d["res"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dt")[:nc], d["dt"][:nc]) <= 1e-12
+    assert rel_err(o.work("limit"), d["limit"]) <= 1e-12
+    assert rel_err(o.work("dqdx")[:, :nc], d["gradPrimtiveVarX"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dqdz")[:, :nc], d["gradPrimtiveVarZ"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("inv_spec"), d["invSpectralRadius"]) <= 1e-12
+
+
+def test_oracle_detects_planted_error(golden):
+    """A mistake planted in the oracle's input shows up in the comparison."""
+    d = golden("euler_bump_16x8x2_step1")
+    m = d["mesh_obj"]
+    o = Oracle(m, d["params_dict"])
+    s = d["state_in"][:, : m.n_cell].copy()
+    s[4, 5] *= 1.0 + 1e-6
+    o.set_state(s)
+    o.iterate(1)
+    assert rel_err(o.work("res")[:, : m.n_cell], d["res"][:, : m.n_cell]) > 1e-10
