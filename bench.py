@@ -1,0 +1,331 @@
+"""Throughput benchmark of the phx per-iteration path on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phx|reference]
+                    [--workload NAME] [--precision fp64|mixed]
+
+One "step" is one outer iteration of the solver (Controller::Relaxation with
+LU-SGS) over the whole mesh.  `value` is Mcell-iterations/s with the state
+resident in HBM (CUDA events on the library's stream, max over ranks);
+`e2e` is the same metric through the public C ABI with the state in pinned
+host memory: every step uploads the primitive state, runs the iteration and
+downloads the updated state and the residual monitor.
+
+Multi-GPU: the path is not partitioned in this release (one zone per GPU);
+N ranks run N independent replicas of the same workload ("replicas only"),
+each timed on its own device, and `value` sums their throughput.
+
+`--impl reference` times the CPU restatement of the reference path
+(oracle/, single-threaded, the reference's LU-SGS is sequential) on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-iters/s on 1 B200: mixed+MLP-SA vs plain FP64, at |ΔCL|,|ΔCD|≤1e-4"
+
+# Bytes each cell moves per iteration under the compulsory-byte rule (each
+# array element counted once per pass that reads or writes it; gathered
+# neighbour values counted once per cell; face arrays once per face per pass),
+# computed for the kernels below from their actual array traffic; see
+# DESIGN.md for the derivation.  Element sizes: FP64 metrics 8 B, working
+# state 8 B (FP64) or 4 B (mixed), indices 4 B.
+
+
+def workloads():
+    from phenlei_b200 import cases
+    from phenlei_b200 import mesh as M
+
+    return {
+        # Config-5 mesh size and flow Mach number, inviscid physics.
+        "transonic_bump_euler_16M": dict(
+            mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001),
+            params=dict(cases.EULER_BUMP, refMachNumber=0.8, CFLEnd=20.0),
+            desc="3-D transonic channel bump 8% thick, 1024x92x128 hex (12.06M cells), M=0.8, Roe+Venkat, "
+                 "GG-cell, LU-SGS CFL 20, inviscid"),
+        "euler_bump_8k": dict(
+            mesh=lambda: M.channel_bump(64, 32, 4),
+            params=dict(cases.EULER_BUMP),
+            desc="config 1: Euler channel bump 64x32x4 hex (8,192 cells), M=0.5"),
+        "euler_bump_1M": dict(
+            mesh=lambda: M.channel_bump(256, 128, 32),
+            params=dict(cases.EULER_BUMP),
+            desc="Euler channel bump 256x128x32 hex (1.05M cells), M=0.5"),
+    }
+
+
+DEFAULT_WORKLOAD = "transonic_bump_euler_16M"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_bytes(m, precision: str) -> dict:
+    """Algorithmic bytes per launch of each kernel (compulsory-byte rule)."""
+    nc, nb, nf = m.n_cell, m.n_bface, m.n_face
+    nt = nc + nb
+    ni = nf - nb
+    lc2f = 2 * ni + nb
+    t = 8 if precision == "fp64" else 4
+    face_geo = 7 * 8          # normal (3), area, centre (3), FP64
+    idx = 8                   # left, right
+    out = {}
+    # boundary: read owner state (FP64 master) + normal, write ghost state (+ working copy) + c2, hm
+    out["boundary"] = nb * (5 * 8 + 3 * 8 + 4 + 5 * 8 + (5 * t if t == 4 else 0) + 2 * t)
+    # gradient+limiter: read q (5), c2f, face normal/area/centre per face, cell centre/vol/volpow; write grad (15) + limiter
+    out["gradient_limiter"] = nt * 5 * t + (lc2f + nc + 1) * 4 + nf * (face_geo + idx) + nc * 5 * 8 + nc * 16 * t
+    # residual: read q, grad, limiter, cell centres, face geometry, c2f; write res (5), invspec, dtraw, coef (3 per slot), c2, hm
+    out["residual"] = (nt * 5 * t + nc * 15 * t + nt * t + nt * 3 * 8 + nf * (face_geo + idx + 4)
+                       + (lc2f + nc + 1) * 4 + nc * 2 * 8 + nc * (5 + 2 + 2) * t + 3 * lc2f * t)
+    # LU-SGS: read res, dtraw, spec, vol, q (u,v,w), c2, hm, coef, normals/area, c2f, schedules; write dq, dflux, diag;
+    # dq of every cell read back by its neighbours (counted once per sweep)
+    out["lusgs"] = (nc * (5 + 3) * t + nc * 8 + nt * 5 * t + 2 * nt * t + 2 * 3 * lc2f * t + 2 * nf * (4 * 8 + idx)
+                    + 2 * (lc2f + nc + 1) * 4 + 2 * nc * 4 + nc * (5 + 5 + 1) * t + 2 * nt * 5 * t + nc * 5 * t)
+    # update: read q (FP64), dq, res; write q (FP64) (+ working copy)
+    out["update"] = nc * (5 * 8 + 5 * t + 5 * t + 5 * 8 + (5 * t if t == 4 else 0)) + nb * 10 * 8
+    out["iteration"] = sum(out.values())
+    return out
+
+
+def run_phx(args, rank, world):
+    import torch
+
+    from phenlei_b200 import solver as S
+
+    dev = rank % max(torch.cuda.device_count(), 1)
+    torch.cuda.set_device(dev)
+    wl = workloads()[args.workload]
+    t0 = time.time()
+    m = wl["mesh"]()
+    s = S.NSSolverUnstruct(m, precision=args.precision, **wl["params"])
+    stream = torch.cuda.current_stream()
+    s.set_stream(stream.cuda_stream)
+    setup_s = time.time() - t0
+    nc = m.n_cell
+    # warm-up
+    s.Relaxation(args.warmup)
+    torch.cuda.synchronize()
+    # timed region (device): K iterations
+    sampler = ClockSampler(dev)
+    sampler.start()
+    launches0 = s.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    hist = s.Relaxation(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = s.launches - launches0
+    clocks = sampler.stop()
+    # per-kernel timing pass (phase entry points, same stream)
+    phase_ms = {}
+    names = [("boundary", s.Boundary), ("gradient_limiter", s.ComputeGradientAndLimiter),
+             ("residual", s.UpdateResiduals), ("lusgs", s.LUSGS), ("update", s.UpdateFlowField)]
+    reps = max(1, min(args.steps, 10))
+    acc = {n: 0.0 for n, _ in names}
+    for _ in range(reps):
+        s.step = s.step + 1
+        for n, fn in names:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            acc[n] += a.elapsed_time(b)
+    phase_ms = {n: v / reps for n, v in acc.items()}
+    # end-to-end through the C ABI with pinned host buffers
+    qh = torch.empty((5, s.nt), dtype=torch.float64).pin_memory()
+    qh.copy_(torch.from_numpy(s.get(S.PHX_Q)))
+    qptr = qh.data_ptr()
+    lib = S.lib()
+    hist1 = np.zeros(1)
+    e2e_steps = max(1, min(args.steps, 20))
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s._check(lib.phx_set_state(s.h, S.PHX_Q, qptr, 5 * s.nt), "set_state")
+        s._check(lib.phx_ns_relaxation(s.h, 1, hist1.ctypes.data), "relaxation")
+        s._check(lib.phx_get_state(s.h, S.PHX_Q, qptr, 5 * s.nt), "get_state")
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t1) / e2e_steps
+    res = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=e2e_s, nc=nc, mesh=m,
+               hist=hist, setup_s=setup_s, nt=s.nt)
+    s.close()
+    return res
+
+
+def cpu_baseline(args, wl_name, sample_budget_s=20.0):
+    """The oracle (single-threaded CPU restatement of the reference path) on a
+    bounded sample of the workload: the same case kind at a size it finishes
+    in seconds, iterated until ~sample_budget_s."""
+    from oracle.oracle import Oracle
+    from phenlei_b200 import mesh as M
+
+    wl = workloads()[wl_name]
+    m = M.channel_bump(128, 46, 32, thickness=0.08, wall_spacing=0.001) if "16M" in wl_name else wl["mesh"]()
+    o = Oracle(m, wl["params"])
+    o.iterate(1)
+    n = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < sample_budget_s:
+        o.iterate(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": m.n_cell * n / dt / 1e6, "unit": "Mcell-iters/s", "cores": 1, "kind": "port",
+            "sample": f"{m.n_cell} cells of the same case kind, {n} iterations in {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="phx", choices=["phx", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    wl = workloads()[args.workload]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_baseline(args, args.workload)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Mcell-iters/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "1 CPU core"},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-iters/s",
+                                             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    r = run_phx(args, rank, world)
+    ms = r["ms"]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    nc = r["nc"]
+    per_gpu = nc * args.steps / (ms / 1e3) / 1e6
+    value = per_gpu * world
+    peak, peak_kind = measured_peaks()
+    kb = kernel_bytes(r["mesh"], args.precision)
+    phase = r["phase_ms"]
+    dom = max(phase, key=phase.get)
+    achieved = kb[dom] / (phase[dom] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mcell-iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded generated mesh, free-stream start)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "cells": nc, "precision": args.precision,
+                   "parallelism": "replicas only" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (state %.0f MB)" % (5 * 8 * r["nt"] / 1e6)},
+        "gpu_launches": int(r["launches"]),
+        "phase_ms": {k: round(v, 4) for k, v in phase.items()},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes": kb[dom], "traffic": None},
+        "iteration_bytes": kb["iteration"],
+        "iteration_roofline_frac": round(kb["iteration"] / (ms / args.steps / 1e3) / 1e9 / peak, 4),
+        "clocks": r["clocks"],
+        "e2e": {"value": round(nc / r["e2e_s"] / 1e6 * world, 3), "unit": "Mcell-iters/s",
+                "h2d_bytes_per_step": 5 * 8 * r["nt"], "d2h_bytes_per_step": 5 * 8 * r["nt"] + 8},
+        "residual_last": float(r["hist"][-1]) if len(r["hist"]) else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, args.workload)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -489,6 +489,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= upload(ctx, &g.bwd_cells, bwd_cells);
     rc |= upload(ctx, &g.bwd_off, bwd_off);
     g.nFwdLevels = nfl; g.nBwdLevels = nbl;
+    g.c2fLen = (int)c2f.size();
     g.walldist = nullptr;
     if (rc) { std::string e = ctx->err; phx_ctx_destroy(ctx); (void)e; return PHX_ERR_CUDA; }
 
@@ -511,6 +512,9 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         r |= dalloc(ctx, &w.dq, (size_t)5 * nt);
         r |= dalloc(ctx, &w.dflux, (size_t)5 * nc);
         r |= dalloc(ctx, &w.diag, (size_t)nc);
+        r |= dalloc(ctx, &w.coef, (size_t)3 * c2f.size());
+        r |= dalloc(ctx, &w.c2, (size_t)nt);
+        r |= dalloc(ctx, &w.hm, (size_t)nt);
         if (!r) {
             // ghost limiter: 1 next to walls / symmetry, 0 next to far field (SetLimitBoundary)
             std::vector<T> gl(nt, T(1));
@@ -748,8 +752,8 @@ static int check_launch(phx_ctx *ctx, int n = 1)
 int phx_ns_boundary(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
-    if (ctx->mixed) launch_boundary<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32.qw, ctx->stream);
-    else launch_boundary<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->q64[ctx->cur], ctx->stream);
+    if (ctx->mixed) launch_boundary<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->stream);
+    else launch_boundary<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->stream);
     return check_launch(ctx);
 }
 

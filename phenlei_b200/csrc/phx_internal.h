@@ -46,6 +46,7 @@ struct DevGrid {
     const int *fwd_cells, *fwd_off;          // LU-SGS forward schedule: cells by level
     const int *bwd_cells, *bwd_off;          // backward schedule
     int nFwdLevels, nBwdLevels;
+    int c2fLen;                              // c2f_off[nCell]
     double avgVol;
 };
 
@@ -80,21 +81,27 @@ struct Work {
     T *dq;          // [5][nTotal]
     T *dflux;       // [5][nCell] LU-SGS delta flux carried between sweeps
     T *diag;        // [nCell]
+    // LU-SGS coefficients that do not depend on dq, filled by the residual
+    // pass: per (cell, face slot) of the cell-to-face list the split
+    // eigenvalue l1 and the MXDQ weights x1, x2 of the neighbour across that
+    // face; per cell the squared sound speed and total enthalpy.
+    T *coef;        // [3][c2fLen]
+    T *c2;          // [nTotal]
+    T *hm;          // [nTotal]
 };
 
 struct Reduce {
     unsigned long long mindt_bits;  // min over cells of dtraw (positive doubles order as integers)
     double resnorm[5];
     int negcount;
-    int barrier_count;
-    unsigned int barrier_gen;
+    unsigned int barrier;           // monotonic arrival counter of the LU-SGS grid barrier
     int error;                      // PHX_ERR_TIMEOUT when a bounded wait gave up
     int step;                       // outer step (CFL ramp)
 };
 
 // Kernel launchers (phx_kernels.cu).
 template <class T>
-void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, T *qw, cudaStream_t s);
+void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s);
 template <class T>
 void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s);
 template <class T>

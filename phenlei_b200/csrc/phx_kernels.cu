@@ -26,7 +26,7 @@ template <class T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg
 // Computed in FP64 from the FP64 master state.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, T *qw)
+__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, T *qw, T *c2o, T *hmo)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nBFace) return;
@@ -76,17 +76,23 @@ __global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c
             o[4] = cB * cB * rB / gl;
         }
     }
+    T t[5];
     for (int k = 0; k < 5; ++k) {
         q[k * nt + re] = o[k];
-        if ((void *)qw != (void *)q) qw[k * nt + re] = (T)o[k];
+        t[k] = (T)o[k];
+        if ((void *)qw != (void *)q) qw[k * nt + re] = t[k];
     }
+    // squared sound speed and total enthalpy of the ghost for the LU-SGS sweep
+    const T gm = (T)c.gama;
+    c2o[re] = fabs(gm * t[4] / t[0]);
+    hmo[re] = (gm / (gm - T(1))) * (t[4] / t[0]) + T(0.5) * (t[1] * t[1] + t[2] * t[2] + t[3] * t[3]);
 }
 
 template <class T>
-void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, T *qw, cudaStream_t s)
+void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s)
 {
     if (g.nBFace == 0) return;
-    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, qw);
+    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w.qw, w.c2, w.hm);
 }
 
 // ---------------------------------------------------------------------------
@@ -243,6 +249,10 @@ __device__ __forceinline__ void face_flux(const DevGrid &g, const NsConst &c, co
     for (int k = 0; k < 5; ++k) fa[k] *= a;
 }
 
+template <class T>
+__device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny, T nz, T area, T gm, T *l1, T *x1,
+                                           T *x2);
+
 __device__ __forceinline__ void atomic_min_pos_double(unsigned long long *addr, double v)
 {
     atomicMin(addr, (unsigned long long)__double_as_longlong(v));
@@ -282,7 +292,28 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(DevGrid g, NsConst c
             T rm = T(0.5) * (q[le] + q[re]);
             T vn = T(0.5) * (vnl + vnr);
             T cm = sqrt(gm * pm / rm);
-            spec += T(0.5) * (T)ld(g.area + f) * (fabs(vn) + cm);
+            const T area = (T)ld(g.area + f);
+            spec += T(0.5) * area * (fabs(vn) + cm);
+            // LU-SGS factors of the neighbour across this face, as seen from this cell
+            {
+                const int nbr = isLeft ? re : le;
+                const T sg = isLeft ? T(1) : T(-1);
+                T qc[5], qn[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) { qc[k] = q[k * nt + cell]; qn[k] = q[k * nt + nbr]; }
+                T l1, x1, x2;
+                lusgs_coef<T>(qc, qn, sg * xn, sg * yn, sg * zn, area, (T)c.gama, &l1, &x1, &x2);
+                w.coef[j] = l1;
+                w.coef[g.c2fLen + j] = x1;
+                w.coef[2 * g.c2fLen + j] = x2;
+            }
+        }
+        {
+            const T *q = w.qw;
+            const T gm = (T)c.gama;
+            const T r = q[cell], u = q[nt + cell], v = q[2 * nt + cell], ww = q[3 * nt + cell], p = q[4 * nt + cell];
+            w.c2[cell] = fabs(gm * p / r);
+            w.hm[cell] = (gm / (gm - T(1))) * (p / r) + T(0.5) * (u * u + v * v + ww * ww);
         }
 #pragma unroll
         for (int k = 0; k < 5; ++k) w.res[k * nc + cell] = res[k];
@@ -313,71 +344,96 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 }
 
 // ---------------------------------------------------------------------------
-// LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955): one persistent kernel
-// per solve runs the forward sweep level by level, the ghost-cell dq, and the
-// backward sweep level by level.  Levels come from the reference's own cell
-// order (a cell depends on its face neighbours of lower index in the forward
-// sweep, higher index in the backward sweep), so every cell sees exactly the
-// neighbour values the sequential sweep of the reference sees.  Between
-// levels a device-wide barrier; every wait is bounded (a timeout sets
-// Reduce::error and the kernel returns).
+// LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955): one persistent
+// cooperative kernel runs the diagonal, the forward sweep level by level, the
+// ghost-cell dq and the backward sweep level by level.  Levels come from the
+// reference's own cell order (a cell depends on its face neighbours of lower
+// index in the forward sweep, higher index in the backward sweep), so every
+// cell sees exactly the neighbour values the sequential sweep of the
+// reference sees.  The dq-independent factors of MXDQ_STD (Roe-averaged
+// spectral radius, split eigenvalue, weights) were computed by the residual
+// pass, so the sequential critical path is multiply-adds only.  Between levels
+// a device-wide barrier on a monotonic counter; every wait is bounded (a
+// timeout sets Reduce::error and the kernel returns).
 // ---------------------------------------------------------------------------
-static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling
+static constexpr long long kSpinLimit = 50000000LL;  // a few seconds of polling
+static constexpr int kSweepThreads = 512;
 
-__device__ __forceinline__ bool grid_barrier(Reduce *red, unsigned int &gen, int nblocks)
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool grid_sync(Reduce *red, unsigned int &target, int nblocks)
 {
     if (nblocks == 1) { __syncthreads(); return true; }
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
+        target += (unsigned int)nblocks;
         __threadfence();
-        int arrived = atomicAdd(&red->barrier_count, 1);
-        if (arrived == nblocks - 1) {
-            atomicExch(&red->barrier_count, 0);
-            __threadfence();
-            atomicAdd(&red->barrier_gen, 1u);
-        } else {
-            long long spins = 0;
-            while (((volatile unsigned int *)&red->barrier_gen)[0] == gen) {
-                if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
-                    atomicExch(&red->error, PHX_ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
+        atomicAdd(&red->barrier, 1u);
+        long long spins = 0;
+        while (ld_acquire(&red->barrier) < target) {
+            if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
+                atomicExch(&red->error, PHX_ERR_TIMEOUT);
+                ok = 0;
+                break;
             }
         }
-        gen += 1;
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
 }
 
-// Contribution of the neighbour across face f to the sweep of `cell`
-// (SolveLUSGSForward body, NSSolverUnstruct.cpp:15251-15370).
+// dq-independent part of the neighbour's MXDQ_STD term for the use (cell ->
+// neighbour across face f): Roe-averaged spectral radius (RoeAveragedVariables
+// + GetRad, NSSolverUnstruct.cpp:15097-15116, 15297-15313) and the split
+// eigenvalue l1 and weights x1, x2 of MXDQ_STD (Jacobian.cpp:27-47).
 template <class T>
-__device__ __forceinline__ void lusgs_face(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell, int f, T *df)
+__device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny, T nz, T area, T gm, T *l1, T *x1,
+                                           T *x2)
 {
-    const int nt = g.nTotal, nc = g.nCell;
-    int le = ld(g.left + f);
-    int re = f < g.nBFace ? nc + f : ld(g.right + f);
-    T nx = (T)ld(g.xfn + f), ny = (T)ld(g.yfn + f), nz = (T)ld(g.zfn + f);
-    if (re == cell) { int s = le; le = re; re = s; nx = -nx; ny = -ny; nz = -nz; }
-    T ql[5], qn[5], dqn[5], fp[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        ql[k] = w.qw[k * nt + le];
-        qn[k] = w.qw[k * nt + re];
-        dqn[k] = ldcg(w.dq + k * nt + re);
-    }
-    const T gm = (T)c.gama;
-    roe_average<T>(ql, gm, qn, gm, fp);
-    const T area = (T)ld(g.area + f);
+    T fp[5];
+    roe_average<T>(qc, gm, qn, gm, fp);
     T vn = nx * fp[1] + ny * fp[2] + nz * fp[3];
     T rad = (fabs(vn) + sqrt(gm * fp[4] / fp[0])) * area;
-    mxdq<T>(qn, nx, ny, nz, area, gm, dqn, df, rad);
+    T c2 = fabs(gm * qn[4] / qn[0]);
+    T cm = sqrt(c2);
+    T cits = nx * qn[1] + ny * qn[2] + nz * qn[3];
+    T ipnrad = -rad / tmax(T(kSmall), area);
+    T a1 = T(0.5) * (cits + ipnrad);
+    T a2 = T(0.5) * (cits + cm + ipnrad);
+    T a3 = T(0.5) * (cits - cm + ipnrad);
+    *l1 = a1;
+    *x1 = (a1 + a1 - a2 - a3) / (c2 + c2);
+    *x2 = (a2 - a3) / (cm + cm);
+}
+
+// MXDQ_STD (Jacobian.cpp:48-86) with the precomputed factors.
+template <class T>
+__device__ __forceinline__ void mxdq_apply(const Work<T> &w, int nt, int nb, T nx, T ny, T nz, T area, T gm, T l1,
+                                           T x1, T x2, const T *dq, T *f)
+{
+    const T um = w.qw[nt + nb], vm = w.qw[2 * nt + nb], wm = w.qw[3 * nt + nb];
+    const T c2 = w.c2[nb], hm = w.hm[nb];
+    const T cits = nx * um + ny * vm + nz * wm;
+    const T dc = cits * dq[0] - nx * dq[1] - ny * dq[2] - nz * dq[3];
+    const T c2dc = c2 * dc;
+    const T v2 = um * um + vm * vm + wm * wm;
+    const T g1 = gm - T(1);
+    T dh = -g1 * (um * dq[1] + vm * dq[2] + wm * dq[3] - dq[4]);
+    dh += T(0.5) * g1 * v2 * dq[0];
+    const T a = dh * x1 + dc * x2;
+    const T b = c2dc * x1 + dh * x2;
+    f[0] = (l1 * dq[0] - a) * area;
+    f[1] = (l1 * dq[1] - um * a + nx * b) * area;
+    f[2] = (l1 * dq[2] - vm * a + ny * b) * area;
+    f[3] = (l1 * dq[3] - wm * a + nz * b) * area;
+    f[4] = (l1 * dq[4] - hm * a + cits * b) * area;
 }
 
 // Ghost-cell dq between the sweeps (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810;
@@ -421,22 +477,66 @@ __device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, i
     }
 }
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+// One cell of a sweep: rhs0 = sum over the faces of the given side of the
+// neighbour's delta flux, dq = (res - carried - rhs0) / D.
+template <class T, bool kForward>
+__device__ __forceinline__ void sweep_cell(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell)
 {
-    const int nt = g.nTotal, nc = g.nCell;
+    const int nt = g.nTotal, nc = g.nCell, len = g.c2fLen;
+    const T gm = (T)c.gama;
+    T rhs0[5] = {0, 0, 0, 0, 0};
+    const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+    for (int j = j0; j < j1; ++j) {
+        const int f = g.c2f[j];
+        int nb;
+        T sgn;
+        if (f < g.nBFace) {
+            if (kForward) continue;
+            nb = nc + f; sgn = T(1);
+        } else {
+            const int le = g.left[f], re = g.right[f];
+            const bool isLeft = (le == cell);
+            nb = isLeft ? re : le;
+            if (kForward ? (nb > cell) : (nb < cell)) continue;
+            sgn = isLeft ? T(1) : T(-1);
+        }
+        T dqn[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) dqn[k] = ldcg(w.dq + k * nt + nb);
+        const T nx = sgn * (T)ld(g.xfn + f), ny = sgn * (T)ld(g.yfn + f), nz = sgn * (T)ld(g.zfn + f);
+        const T area = (T)ld(g.area + f);
+        T df[5];
+        mxdq_apply<T>(w, nt, nb, nx, ny, nz, area, gm, w.coef[j], w.coef[len + j], w.coef[2 * len + j], dqn, df);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+    }
+    const T dg = ldcg(w.diag + cell);
+    if (kForward) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            w.dq[k * nt + cell] = (w.res[k * nc + cell] - T(0) - rhs0[k]) / dg;
+            w.dflux[k * nc + cell] = T(0) + rhs0[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            w.dq[k * nt + cell] = (w.res[k * nc + cell] - ldcg(w.dflux + k * nc + cell) - rhs0[k]) / dg;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+{
+    const int nc = g.nCell;
     const int nblocks = gridDim.x;
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    __shared__ unsigned int sgen;
-    if (threadIdx.x == 0) sgen = ((volatile unsigned int *)&red->barrier_gen)[0];
-    __syncthreads();
-    unsigned int gen = sgen;
+    unsigned int target = 0;
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
 
-    // Diagonal (NSSolverUnstruct.cpp:15867-15935) and dq initialisation
-    // (LUSGSInitialization, Controller.cpp:1765-1777: single sweep, dq = res,
-    // delta flux = 0).
+    // Diagonal (NSSolverUnstruct.cpp:15867-15935); single sweep: dq starts
+    // from res, the carried delta flux from zero (LUSGSInitialization,
+    // Controller.cpp:1765-1777).
     for (int cell = tid; cell < nc; cell += stride) {
         T dt = w.dtraw[cell];
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
@@ -446,85 +546,46 @@ __global__ void __launch_bounds__(kThreads) lusgs_kernel(DevGrid g, NsConst c, W
         if (c.viscous) d += w.visspec[cell];
         w.diag[cell] = d;
     }
-    if (!grid_barrier(red, gen, nblocks)) return;
-
-    // forward sweep: dq = (res - Ux - L dq) / D over lower neighbours
+    if (!grid_sync(red, target, nblocks)) return;
     for (int L = 0; L < g.nFwdLevels; ++L) {
         const int b = g.fwd_off[L], e = g.fwd_off[L + 1];
-        for (int i = b + tid; i < e; i += stride) {
-            const int cell = g.fwd_cells[i];
-            T rhs0[5] = {0, 0, 0, 0, 0};
-            const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-            for (int j = j0; j < j1; ++j) {
-                const int f = g.c2f[j];
-                if (f < g.nBFace) continue;
-                const int le = g.left[f], re = g.right[f];
-                if (le > cell || re > cell) continue;
-                T df[5];
-                lusgs_face<T>(g, c, w, cell, f, df);
-#pragma unroll
-                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
-            }
-            const T dg = ldcg(w.diag + cell);
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                T v = (w.res[k * nc + cell] - T(0) - rhs0[k]) / dg;
-                w.dflux[k * nc + cell] = T(0) + rhs0[k];
-                w.dq[k * nt + cell] = v;
-            }
-        }
-        if (!grid_barrier(red, gen, nblocks)) return;
+        for (int i = b + tid; i < e; i += stride) sweep_cell<T, true>(g, c, w, g.fwd_cells[i]);
+        if (!grid_sync(red, target, nblocks)) return;
     }
     for (int f = tid; f < g.nBFace; f += stride) ghost_dq<T>(g, c, w, f);
-    if (!grid_barrier(red, gen, nblocks)) return;
-
-    // backward sweep: dq = (res - L dq* - U dq) / D over upper neighbours and ghosts
+    if (!grid_sync(red, target, nblocks)) return;
     for (int L = 0; L < g.nBwdLevels; ++L) {
         const int b = g.bwd_off[L], e = g.bwd_off[L + 1];
-        for (int i = b + tid; i < e; i += stride) {
-            const int cell = g.bwd_cells[i];
-            T rhs0[5] = {0, 0, 0, 0, 0};
-            const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-            for (int j = j0; j < j1; ++j) {
-                const int f = g.c2f[j];
-                const int le = g.left[f];
-                const int re = f < g.nBFace ? nc + f : g.right[f];
-                if (le < cell || re < cell) continue;
-                T df[5];
-                lusgs_face<T>(g, c, w, cell, f, df);
-#pragma unroll
-                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
-            }
-            const T dg = ldcg(w.diag + cell);
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                T v = (w.res[k * nc + cell] - ldcg(w.dflux + k * nc + cell) - rhs0[k]) / dg;
-                w.dq[k * nt + cell] = v;
-            }
-        }
-        if (!grid_barrier(red, gen, nblocks)) return;
+        for (int i = b + tid; i < e; i += stride) sweep_cell<T, false>(g, c, w, g.bwd_cells[i]);
+        if (L + 1 < g.nBwdLevels && !grid_sync(red, target, nblocks)) return;
     }
 }
+
+static __global__ void reset_barrier_kernel(Reduce *r) { r->barrier = 0u; }
 
 template <class T>
 int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, Reduce *red, int numSMs,
                  cudaStream_t s)
 {
     (void)q64;
-    int perSM = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kThreads, 0);
-    if (perSM < 1) perSM = 1;
-    // Widest level decides how many blocks are worth their barrier cost.
+    static int perSMcache[2] = {-1, -1};
+    int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
+    if (perSM < 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kSweepThreads, 0);
+        if (perSM < 1) perSM = 1;
+        if (perSM > 2) perSM = 2;
+    }
     int blocks = numSMs * perSM;
-    int need = (g.nCell + kThreads - 1) / kThreads;
+    const int need = (g.nCell + kSweepThreads - 1) / kSweepThreads;
     if (need < blocks) blocks = need;
     if (blocks < 1) blocks = 1;
+    reset_barrier_kernel<<<1, 1, 0, s>>>(red);
     DevGrid gg = g;
     NsConst cc = c;
     Work<T> ww = w;
     Reduce *rr = red;
     void *args[] = {&gg, &cc, &ww, &rr};
-    cudaError_t e = cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kThreads), args, 0, s);
+    cudaError_t e = cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
 }
 
@@ -650,7 +711,7 @@ void launch_solution_fix(const DevGrid &g, const NsConst &c, const double *q64, 
 
 // Explicit instantiations for the FP64 and mixed paths.
 #define PHX_INSTANTIATE(T)                                                                                      \
-    template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, T *, cudaStream_t);             \
+    template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, const Work<T> &, cudaStream_t);\
     template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);   \
     template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,        \
                                      cudaStream_t);                                                              \
