@@ -490,6 +490,11 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= upload(ctx, &g.bwd_off, bwd_off);
     g.nFwdLevels = nfl; g.nBwdLevels = nbl;
     g.c2fLen = (int)c2f.size();
+    g.maxLevelWidth = 1;
+    for (int l = 0; l < nfl; ++l) g.maxLevelWidth = std::max(g.maxLevelWidth, fwd_off[l + 1] - fwd_off[l]);
+    for (int l = 0; l < nbl; ++l) g.maxLevelWidth = std::max(g.maxLevelWidth, bwd_off[l + 1] - bwd_off[l]);
+    for (int cc = 0; cc < nc; ++cc)
+        if (c2f_off[cc + 1] - c2f_off[cc] > 8) { phx_ctx_destroy(ctx); return PHX_ERR_ARG; }
     g.walldist = nullptr;
     if (rc) { std::string e = ctx->err; phx_ctx_destroy(ctx); (void)e; return PHX_ERR_CUDA; }
 

@@ -47,6 +47,7 @@ struct DevGrid {
     const int *bwd_cells, *bwd_off;          // backward schedule
     int nFwdLevels, nBwdLevels;
     int c2fLen;                              // c2f_off[nCell]
+    int maxLevelWidth;                       // widest LU-SGS level (cells)
     double avgVol;
 };
 

@@ -104,49 +104,95 @@ void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work
 //  :1202-1252 over interior faces), zeroed next to far-field boundaries
 //  (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
 // ---------------------------------------------------------------------------
+// Cells are processed by groups of kLanes lanes; lane k takes the k-th face of
+// the cell's ascending face list, and lane 0 adds the lanes' terms in face
+// order, so sums keep the reference's accumulation order.
+static constexpr int kLanes = 8;
+
 template <class T>
 __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, NsConst c, Work<T> w)
 {
-    int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= g.nCell) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cell = tid / kLanes, lane = tid % kLanes;
+    const int base = (threadIdx.x & 31) & ~(kLanes - 1);
+    const unsigned full = 0xffffffffu;
     const int nt = g.nTotal, nc = g.nCell;
+    const bool valid = cell < nc;
     const T *q = w.qw;
-    T qc[5];
+    int j0 = 0, j1 = 0;
+    if (valid) { j0 = g.c2f_off[cell]; j1 = g.c2f_off[cell + 1]; }
+    const int j = j0 + lane;
+    const bool act = valid && j < j1;
+    T qc[5] = {0, 0, 0, 0, 0};
+    if (valid) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) qc[k] = q[k * nt + cell];
-    T gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
-    T rmin = qc[0], rmax = qc[0], pmin = qc[4], pmax = qc[4];
-    const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-    for (int j = j0; j < j1; ++j) {
-        const int f = ld(g.c2f + j);
+        for (int k = 0; k < 5; ++k) qc[k] = q[k * nt + cell];
+    }
+    // this lane's face: signed contributions qf * n A, neighbour rho and p
+    T cx[5] = {0, 0, 0, 0, 0}, cy[5] = {0, 0, 0, 0, 0}, cz[5] = {0, 0, 0, 0, 0};
+    T rn = qc[0], pn = qc[4];
+    int f = 0;
+    bool interior = false, isLeft = true;
+    if (act) {
+        f = ld(g.c2f + j);
         const int le = ld(g.left + f);
-        const bool isLeft = (le == cell);
+        isLeft = (le == cell);
         const int nb = isLeft ? (f < g.nBFace ? nc + f : ld(g.right + f)) : le;
         const double a = ld(g.area + f);
         const T nx = (T)(ld(g.xfn + f) * a), ny = (T)(ld(g.yfn + f) * a), nz = (T)(ld(g.zfn + f) * a);
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            T qn = q[k * nt + nb];
-            T qf = T(0.5) * (isLeft ? (qc[k] + qn) : (qn + qc[k]));
-            if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
-            else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+            const T qn = q[k * nt + nb];
+            const T qf = T(0.5) * (isLeft ? (qc[k] + qn) : (qn + qc[k]));
+            cx[k] = qf * nx; cy[k] = qf * ny; cz[k] = qf * nz;
         }
-        if (f >= g.nBFace) {
-            T rn = q[nb], pn = q[4 * nt + nb];
-            rmin = tmin(rmin, rn); rmax = tmax(rmax, rn);
-            pmin = tmin(pmin, pn); pmax = tmax(pmax, pn);
-        }
+        interior = f >= g.nBFace;
+        if (interior) { rn = q[nb]; pn = q[4 * nt + nb]; }
     }
-    const T ovol = T(1) / (T)ld(g.vol + cell);
+    const unsigned actm = __ballot_sync(full, act);
+    const unsigned leftm = __ballot_sync(full, isLeft);
+    T gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol;
-        w.grad[(0 * 5 + k) * nc + cell] = gx[k];
-        w.grad[(1 * 5 + k) * nc + cell] = gy[k];
-        w.grad[(2 * 5 + k) * nc + cell] = gz[k];
+    for (int k = 0; k < kLanes; ++k) {
+        const int src = base + k;
+        const bool on = (actm >> src) & 1u;
+        const bool lf = (leftm >> src) & 1u;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            const T vx = __shfl_sync(full, cx[m], src), vy = __shfl_sync(full, cy[m], src), vz = __shfl_sync(full, cz[m], src);
+            if (on) {
+                if (lf) { gx[m] += vx; gy[m] += vy; gz[m] += vz; }
+                else { gx[m] -= vx; gy[m] -= vy; gz[m] -= vz; }
+            }
+        }
     }
+    // neighbour min / max of rho and p over interior faces (order-free)
+    T rmin = interior ? rn : qc[0], rmax = rmin, pmin = interior ? pn : qc[4], pmax = pmin;
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) {
+        rmin = tmin(rmin, __shfl_xor_sync(full, rmin, o));
+        rmax = tmax(rmax, __shfl_xor_sync(full, rmax, o));
+        pmin = tmin(pmin, __shfl_xor_sync(full, pmin, o));
+        pmax = tmax(pmax, __shfl_xor_sync(full, pmax, o));
+    }
+    rmin = tmin(rmin, qc[0]); rmax = tmax(rmax, qc[0]);
+    pmin = tmin(pmin, qc[4]); pmax = tmax(pmax, qc[4]);
+    T ovol = T(1);
+    if (valid) ovol = T(1) / (T)ld(g.vol + cell);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol; }
+    if (valid && lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            w.grad[(0 * 5 + k) * nc + cell] = gx[k];
+            w.grad[(1 * 5 + k) * nc + cell] = gy[k];
+            w.grad[(2 * 5 + k) * nc + cell] = gz[k];
+        }
+    }
+    // Venkatakrishnan limiter: every lane holds the group's gradient (each lane
+    // accumulated the same terms in the same order)
     T lim = T(1);
-    if (c.limiter == 1) {
+    if (c.limiter == 1 && act) {
         const T vp = (T)ld(g.volpow + cell);
         T er = (T)c.venkatK3 * qc[0]; er = er * qc[0]; er = er * vp;
         T ep = (T)c.venkatK3 * qc[4]; ep = ep * qc[4]; ep = ep * vp;
@@ -154,25 +200,27 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
         const T dminp = pmin - qc[4], dmaxp = pmax - qc[4];
         const double xc = ld(g.xcc + cell), yc = ld(g.ycc + cell), zc = ld(g.zcc + cell);
         const T small = (T)kSmall;
-        for (int j = j0; j < j1; ++j) {
-            const int f = ld(g.c2f + j);
-            const T dx = (T)(ld(g.xfc + f) - xc), dy = (T)(ld(g.yfc + f) - yc), dz = (T)(ld(g.zfc + f) - zc);
-            T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
-            if (d > small) lim = tmin(lim, venfun(dmaxr, d, er));
-            else if (d < -small) lim = tmin(lim, venfun(dminr, d, er));
-            d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
-            if (d > small) lim = tmin(lim, venfun(dmaxp, d, ep));
-            else if (d < -small) lim = tmin(lim, venfun(dminp, d, ep));
-        }
-        if (g.farfield_adj[cell]) lim = T(0);
+        const T dx = (T)(ld(g.xfc + f) - xc), dy = (T)(ld(g.yfc + f) - yc), dz = (T)(ld(g.zfc + f) - zc);
+        T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
+        if (d > small) lim = tmin(lim, venfun(dmaxr, d, er));
+        else if (d < -small) lim = tmin(lim, venfun(dminr, d, er));
+        d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
+        if (d > small) lim = tmin(lim, venfun(dmaxp, d, ep));
+        else if (d < -small) lim = tmin(lim, venfun(dminp, d, ep));
     }
-    w.limit[cell] = lim;
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) lim = tmin(lim, __shfl_xor_sync(full, lim, o));
+    if (valid && lane == 0) {
+        if (c.limiter == 1 && g.farfield_adj[cell]) lim = T(0);
+        w.limit[cell] = lim;
+    }
 }
 
 template <class T>
 void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s)
 {
-    gradient_limiter_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
+    const long long threads = (long long)g.nCell * kLanes;
+    gradient_limiter_kernel<T><<<(unsigned)((threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(g, c, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -261,67 +309,88 @@ __device__ __forceinline__ void atomic_min_pos_double(unsigned long long *addr, 
 template <class T>
 __global__ void __launch_bounds__(kThreads) residual_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red, double cfl)
 {
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cell = tid / kLanes, lane = tid % kLanes;
+    const int base = (threadIdx.x & 31) & ~(kLanes - 1);
+    const unsigned full = 0xffffffffu;
     const int nt = g.nTotal, nc = g.nCell;
-    double mydt = kLarge;
-    if (cell < nc) {
-        T res[5] = {0, 0, 0, 0, 0};
-        T spec = T(0);
-        const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-        for (int j = j0; j < j1; ++j) {
-            const int f = ld(g.c2f + j);
-            const int le = ld(g.left + f);
-            const bool isLeft = (le == cell);
-            T fa[5];
-            face_flux<T>(g, c, w, f, fa);
-            if (isLeft) {
+    const bool valid = cell < nc;
+    int j0 = 0, j1 = 0;
+    if (valid) { j0 = g.c2f_off[cell]; j1 = g.c2f_off[cell + 1]; }
+    const int j = j0 + lane;
+    const bool act = valid && j < j1;
+    T fa[5] = {0, 0, 0, 0, 0};
+    T sp = T(0);
+    bool isLeft = true;
+    if (act) {
+        const int f = ld(g.c2f + j);
+        const int le = ld(g.left + f);
+        isLeft = (le == cell);
+        face_flux<T>(g, c, w, f, fa);
+        // inviscid spectral radius from the face-mean state
+        const int re = f < g.nBFace ? nc + f : ld(g.right + f);
+        const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
+        const T *q = w.qw;
+        T vnl = xn * q[nt + le] + yn * q[2 * nt + le] + zn * q[3 * nt + le];
+        T vnr = xn * q[nt + re] + yn * q[2 * nt + re] + zn * q[3 * nt + re];
+        T gm = T(0.5) * ((T)c.gama + (T)c.gama);
+        T pm = T(0.5) * (q[4 * nt + le] + q[4 * nt + re]);
+        T rm = T(0.5) * (q[le] + q[re]);
+        T vn = T(0.5) * (vnl + vnr);
+        T cm = sqrt(gm * pm / rm);
+        const T area = (T)ld(g.area + f);
+        sp = T(0.5) * area * (fabs(vn) + cm);
+        // LU-SGS factors of the neighbour across this face, as seen from this cell
+        const int nbr = isLeft ? re : le;
+        const T sg = isLeft ? T(1) : T(-1);
+        T qc[5], qn[5];
 #pragma unroll
-                for (int k = 0; k < 5; ++k) res[k] -= fa[k];
+        for (int k = 0; k < 5; ++k) { qc[k] = q[k * nt + cell]; qn[k] = q[k * nt + nbr]; }
+        T l1, x1, x2;
+        lusgs_coef<T>(qc, qn, sg * xn, sg * yn, sg * zn, area, (T)c.gama, &l1, &x1, &x2);
+        w.coef[j] = l1;
+        w.coef[g.c2fLen + j] = x1;
+        w.coef[2 * g.c2fLen + j] = x2;
+    }
+    // LoadFlux order: lane 0 adds the faces in ascending face order
+    const unsigned actm = __ballot_sync(full, act);
+    const unsigned leftm = __ballot_sync(full, isLeft);
+    T res[5] = {0, 0, 0, 0, 0};
+    T spec = T(0);
+#pragma unroll
+    for (int k = 0; k < kLanes; ++k) {
+        const int src = base + k;
+        const bool on = (actm >> src) & 1u;
+        const bool lf = (leftm >> src) & 1u;
+        T v[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(full, fa[m], src);
+        const T vs = __shfl_sync(full, sp, src);
+        if (on) {
+            if (lf) {
+#pragma unroll
+                for (int m = 0; m < 5; ++m) res[m] -= v[m];
             } else {
 #pragma unroll
-                for (int k = 0; k < 5; ++k) res[k] += fa[k];
+                for (int m = 0; m < 5; ++m) res[m] += v[m];
             }
-            // inviscid spectral radius from the face-mean state
-            const int re = f < g.nBFace ? nc + f : ld(g.right + f);
-            const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
-            const T *q = w.qw;
-            T vnl = xn * q[nt + le] + yn * q[2 * nt + le] + zn * q[3 * nt + le];
-            T vnr = xn * q[nt + re] + yn * q[2 * nt + re] + zn * q[3 * nt + re];
-            T gm = T(0.5) * ((T)c.gama + (T)c.gama);
-            T pm = T(0.5) * (q[4 * nt + le] + q[4 * nt + re]);
-            T rm = T(0.5) * (q[le] + q[re]);
-            T vn = T(0.5) * (vnl + vnr);
-            T cm = sqrt(gm * pm / rm);
-            const T area = (T)ld(g.area + f);
-            spec += T(0.5) * area * (fabs(vn) + cm);
-            // LU-SGS factors of the neighbour across this face, as seen from this cell
-            {
-                const int nbr = isLeft ? re : le;
-                const T sg = isLeft ? T(1) : T(-1);
-                T qc[5], qn[5];
-#pragma unroll
-                for (int k = 0; k < 5; ++k) { qc[k] = q[k * nt + cell]; qn[k] = q[k * nt + nbr]; }
-                T l1, x1, x2;
-                lusgs_coef<T>(qc, qn, sg * xn, sg * yn, sg * zn, area, (T)c.gama, &l1, &x1, &x2);
-                w.coef[j] = l1;
-                w.coef[g.c2fLen + j] = x1;
-                w.coef[2 * g.c2fLen + j] = x2;
-            }
+            spec += vs;
         }
-        {
-            const T *q = w.qw;
-            const T gm = (T)c.gama;
-            const T r = q[cell], u = q[nt + cell], v = q[2 * nt + cell], ww = q[3 * nt + cell], p = q[4 * nt + cell];
-            w.c2[cell] = fabs(gm * p / r);
-            w.hm[cell] = (gm / (gm - T(1))) * (p / r) + T(0.5) * (u * u + v * v + ww * ww);
-        }
+    }
+    double mydt = kLarge;
+    if (valid && lane == 0) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) w.res[k * nc + cell] = res[k];
         w.invspec[cell] = spec;
         if (c.viscous) spec += w.visspec[cell];
+        const T *q = w.qw;
+        const T gm = (T)c.gama;
+        const T r = q[cell], u = q[nt + cell], v = q[2 * nt + cell], ww = q[3 * nt + cell], p = q[4 * nt + cell];
+        w.c2[cell] = fabs(gm * p / r);
+        w.hm[cell] = (gm / (gm - T(1))) * (p / r) + T(0.5) * (u * u + v * v + ww * ww);
         // LimitCFL: pressure- and skewness-based CFL of the cell
         double cc = cfl;
-        const double pc = (double)w.qw[4 * nt + cell];
+        const double pc = (double)p;
         const double plo = 0.001 * c.pTotal, phi = 0.02 * c.pTotal;
         if (pc < plo) cc = c.cflStart;
         else if (pc < phi) cc = (pc - phi) * (cfl - c.cflStart) / (phi - plo) + cfl;
@@ -333,14 +402,15 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(DevGrid g, NsConst c
         mydt = (double)dt;
     }
     // device-wide minimum of dt (positive doubles order like unsigned integers)
-    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(full, mydt, o));
     if ((threadIdx.x & 31) == 0 && mydt < kLarge) atomic_min_pos_double(&red->mindt_bits, mydt);
 }
 
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
 {
-    residual_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, red, cfl);
+    const long long threads = (long long)g.nCell * kLanes;
+    residual_kernel<T><<<(unsigned)((threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(g, c, w, red, cfl);
 }
 
 // ---------------------------------------------------------------------------
@@ -378,6 +448,7 @@ __device__ __forceinline__ bool grid_sync(Reduce *red, unsigned int &target, int
         atomicAdd(&red->barrier, 1u);
         long long spins = 0;
         while (ld_acquire(&red->barrier) < target) {
+            __nanosleep(20);
             if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
                 atomicExch(&red->error, PHX_ERR_TIMEOUT);
                 ok = 0;
@@ -477,60 +548,155 @@ __device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, i
     }
 }
 
-// One cell of a sweep: rhs0 = sum over the faces of the given side of the
-// neighbour's delta flux, dq = (res - carried - rhs0) / D.
+// A sweep is processed by groups of kGroup lanes, one cell per group: lane k
+// takes the k-th face of the cell, computes the neighbour's delta flux if the
+// neighbour is on the sweep's side, and lane 0 adds the lanes' terms in face
+// order (the reference's order).  All loads that do not depend on dq are
+// issued for the next level before the barrier (Slot), so after the barrier
+// only the neighbours' dq are read.
+static constexpr int kGroup = 8;
+
+template <class T>
+struct Slot {
+    int cell;          // -1: no cell for this group at this level
+    int nb;            // neighbour index, -1 if this lane's face does not take part
+    T nx, ny, nz, area, l1, x1, x2, um, vm, wm, c2, hm;
+    T r[5];            // lane 0: res (forward) or res - carried delta flux (backward)
+    T diag;            // lane 0
+};
+
 template <class T, bool kForward>
-__device__ __forceinline__ void sweep_cell(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell)
+__device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, int level_pos_end, int pos, int lane,
+                                          Slot<T> &s)
 {
     const int nt = g.nTotal, nc = g.nCell, len = g.c2fLen;
-    const T gm = (T)c.gama;
-    T rhs0[5] = {0, 0, 0, 0, 0};
+    s.cell = -1;
+    s.nb = -1;
+    if (pos >= level_pos_end) return;
+    const int cell = kForward ? g.fwd_cells[pos] : g.bwd_cells[pos];
+    s.cell = cell;
     const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-    for (int j = j0; j < j1; ++j) {
+    const int j = j0 + lane;
+    if (j < j1) {
         const int f = g.c2f[j];
-        int nb;
-        T sgn;
+        int nb = -1;
+        T sgn = T(1);
         if (f < g.nBFace) {
-            if (kForward) continue;
-            nb = nc + f; sgn = T(1);
+            if (!kForward) nb = nc + f;
         } else {
             const int le = g.left[f], re = g.right[f];
             const bool isLeft = (le == cell);
-            nb = isLeft ? re : le;
-            if (kForward ? (nb > cell) : (nb < cell)) continue;
+            const int o = isLeft ? re : le;
+            if (kForward ? (o < cell) : (o > cell)) nb = o;
             sgn = isLeft ? T(1) : T(-1);
         }
-        T dqn[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) dqn[k] = ldcg(w.dq + k * nt + nb);
-        const T nx = sgn * (T)ld(g.xfn + f), ny = sgn * (T)ld(g.yfn + f), nz = sgn * (T)ld(g.zfn + f);
-        const T area = (T)ld(g.area + f);
-        T df[5];
-        mxdq_apply<T>(w, nt, nb, nx, ny, nz, area, gm, w.coef[j], w.coef[len + j], w.coef[2 * len + j], dqn, df);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+        if (nb >= 0) {
+            s.nb = nb;
+            s.nx = sgn * (T)ld(g.xfn + f);
+            s.ny = sgn * (T)ld(g.yfn + f);
+            s.nz = sgn * (T)ld(g.zfn + f);
+            s.area = (T)ld(g.area + f);
+            s.l1 = w.coef[j];
+            s.x1 = w.coef[len + j];
+            s.x2 = w.coef[2 * len + j];
+            s.um = w.qw[nt + nb];
+            s.vm = w.qw[2 * nt + nb];
+            s.wm = w.qw[3 * nt + nb];
+            s.c2 = w.c2[nb];
+            s.hm = w.hm[nb];
+        }
     }
-    const T dg = ldcg(w.diag + cell);
-    if (kForward) {
+    if (lane == 0) {
+        s.diag = ldcg(w.diag + cell);
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            w.dq[k * nt + cell] = (w.res[k * nc + cell] - T(0) - rhs0[k]) / dg;
-            w.dflux[k * nc + cell] = T(0) + rhs0[k];
+            T rv = w.res[k * nc + cell];
+            if (!kForward) rv = rv - ldcg(w.dflux + k * nc + cell);
+            s.r[k] = kForward ? (rv - T(0)) : rv;
         }
-    } else {
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-            w.dq[k * nt + cell] = (w.res[k * nc + cell] - ldcg(w.dflux + k * nc + cell) - rhs0[k]) / dg;
     }
 }
 
+template <class T, bool kForward>
+__device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c, const Work<T> &w, const Slot<T> &s,
+                                             int lane, unsigned mask)
+{
+    const int nt = g.nTotal, nc = g.nCell;
+    T df[5] = {0, 0, 0, 0, 0};
+    const bool active = s.cell >= 0 && s.nb >= 0;
+    if (active) {
+        T dq[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) dq[k] = ldcg(w.dq + k * nt + s.nb);
+        const T gm = (T)c.gama;
+        const T cits = s.nx * s.um + s.ny * s.vm + s.nz * s.wm;
+        const T dc = cits * dq[0] - s.nx * dq[1] - s.ny * dq[2] - s.nz * dq[3];
+        const T c2dc = s.c2 * dc;
+        const T v2 = s.um * s.um + s.vm * s.vm + s.wm * s.wm;
+        const T g1 = gm - T(1);
+        T dh = -g1 * (s.um * dq[1] + s.vm * dq[2] + s.wm * dq[3] - dq[4]);
+        dh += T(0.5) * g1 * v2 * dq[0];
+        const T a = dh * s.x1 + dc * s.x2;
+        const T b = c2dc * s.x1 + dh * s.x2;
+        df[0] = (s.l1 * dq[0] - a) * s.area;
+        df[1] = (s.l1 * dq[1] - s.um * a + s.nx * b) * s.area;
+        df[2] = (s.l1 * dq[2] - s.vm * a + s.ny * b) * s.area;
+        df[3] = (s.l1 * dq[3] - s.wm * a + s.nz * b) * s.area;
+        df[4] = (s.l1 * dq[4] - s.hm * a + cits * b) * s.area;
+    }
+    // in-order accumulation on lane 0 of the group
+    const unsigned act = __ballot_sync(mask, active);
+    const int base = (threadIdx.x & 31) & ~(kGroup - 1);
+    T rhs0[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < kGroup; ++k) {
+        T v[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(mask, df[m], base + k);
+        if ((act >> (base + k)) & 1u) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) rhs0[m] += v[m];
+        }
+    }
+    if (lane == 0 && s.cell >= 0) {
+        const int cell = s.cell;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            w.dq[k * nt + cell] = (s.r[k] - rhs0[k]) / s.diag;
+            if (kForward) w.dflux[k * nc + cell] = T(0) + rhs0[k];
+        }
+    }
+}
+
+template <class T, bool kForward>
+__device__ __forceinline__ bool run_sweep(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
+                                          unsigned &target, int group, int ngroups, int lane)
+{
+    const int nlev = kForward ? g.nFwdLevels : g.nBwdLevels;
+    const int *off = kForward ? g.fwd_off : g.bwd_off;
+    Slot<T> cur;
+    load_slot<T, kForward>(g, w, off[1], off[0] + group, lane, cur);
+    for (int L = 0; L < nlev; ++L) {
+        const int b = off[L], e = off[L + 1];
+        process_slot<T, kForward>(g, c, w, cur, lane, 0xffffffffu);
+        for (int pos = b + group + ngroups; pos < e; pos += ngroups) {  // levels wider than the grid
+            Slot<T> extra;
+            load_slot<T, kForward>(g, w, e, pos, lane, extra);
+            process_slot<T, kForward>(g, c, w, extra, lane, 0xffffffffu);
+        }
+        if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, cur);
+        if (!grid_sync(red, target, gridDim.x)) return false;
+    }
+    return true;
+}
+
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+__global__ void __launch_bounds__(kSweepThreads, 1) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
 {
     const int nc = g.nCell;
-    const int nblocks = gridDim.x;
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int group = tid / kGroup, lane = tid % kGroup, ngroups = stride / kGroup;
     unsigned int target = 0;
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
 
@@ -546,19 +712,11 @@ __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst
         if (c.viscous) d += w.visspec[cell];
         w.diag[cell] = d;
     }
-    if (!grid_sync(red, target, nblocks)) return;
-    for (int L = 0; L < g.nFwdLevels; ++L) {
-        const int b = g.fwd_off[L], e = g.fwd_off[L + 1];
-        for (int i = b + tid; i < e; i += stride) sweep_cell<T, true>(g, c, w, g.fwd_cells[i]);
-        if (!grid_sync(red, target, nblocks)) return;
-    }
+    if (!grid_sync(red, target, gridDim.x)) return;
+    if (!run_sweep<T, true>(g, c, w, red, target, group, ngroups, lane)) return;
     for (int f = tid; f < g.nBFace; f += stride) ghost_dq<T>(g, c, w, f);
-    if (!grid_sync(red, target, nblocks)) return;
-    for (int L = 0; L < g.nBwdLevels; ++L) {
-        const int b = g.bwd_off[L], e = g.bwd_off[L + 1];
-        for (int i = b + tid; i < e; i += stride) sweep_cell<T, false>(g, c, w, g.bwd_cells[i]);
-        if (L + 1 < g.nBwdLevels && !grid_sync(red, target, nblocks)) return;
-    }
+    if (!grid_sync(red, target, gridDim.x)) return;
+    run_sweep<T, false>(g, c, w, red, target, group, ngroups, lane);
 }
 
 static __global__ void reset_barrier_kernel(Reduce *r) { r->barrier = 0u; }
@@ -573,11 +731,11 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const dou
     if (perSM < 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kSweepThreads, 0);
         if (perSM < 1) perSM = 1;
-        if (perSM > 2) perSM = 2;
     }
-    int blocks = numSMs * perSM;
-    const int need = (g.nCell + kSweepThreads - 1) / kSweepThreads;
-    if (need < blocks) blocks = need;
+    // one group per cell of the widest level; never more blocks than can be co-resident
+    const long long threads = (long long)g.maxLevelWidth * kGroup;
+    int blocks = (int)((threads + kSweepThreads - 1) / kSweepThreads);
+    if (blocks > numSMs * perSM) blocks = numSMs * perSM;
     if (blocks < 1) blocks = 1;
     reset_barrier_kernel<<<1, 1, 0, s>>>(red);
     DevGrid gg = g;
