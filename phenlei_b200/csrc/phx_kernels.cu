@@ -7,6 +7,7 @@
 // working state T is double (FP64 path) or float (mixed path).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "phx_internal.h"
 #include "phx_physics.cuh"
@@ -679,9 +680,14 @@ __device__ __forceinline__ bool run_sweep(const DevGrid &g, const NsConst &c, co
     for (int L = 0; L < nlev; ++L) {
         const int b = off[L], e = off[L + 1];
         process_slot<T, kForward>(g, c, w, cur, lane, 0xffffffffu);
-        for (int pos = b + group + ngroups; pos < e; pos += ngroups) {  // levels wider than the grid
+        // Levels wider than the grid: further rounds.  The loop bound depends
+        // only on the warp's first group, so every lane of a warp takes the same
+        // trip count (process_slot uses full-warp shuffles); groups past the end
+        // of the level carry an empty slot.
+        const int warpGroup0 = group - ((threadIdx.x & 31) / kGroup);
+        for (int round = b + ngroups; round + warpGroup0 < e; round += ngroups) {
             Slot<T> extra;
-            load_slot<T, kForward>(g, w, e, pos, lane, extra);
+            load_slot<T, kForward>(g, w, e, round + group, lane, extra);
             process_slot<T, kForward>(g, c, w, extra, lane, 0xffffffffu);
         }
         if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, cur);
@@ -736,6 +742,12 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const dou
     const long long threads = (long long)g.maxLevelWidth * kGroup;
     int blocks = (int)((threads + kSweepThreads - 1) / kSweepThreads);
     if (blocks > numSMs * perSM) blocks = numSMs * perSM;
+    // PHX_LUSGS_MAX_BLOCKS caps the sweep grid (tuning, and tests of levels
+    // wider than the grid on small meshes)
+    if (const char *cap = getenv("PHX_LUSGS_MAX_BLOCKS")) {
+        const int v = atoi(cap);
+        if (v > 0 && blocks > v) blocks = v;
+    }
     if (blocks < 1) blocks = 1;
     reset_barrier_kernel<<<1, 1, 0, s>>>(red);
     DevGrid gg = g;

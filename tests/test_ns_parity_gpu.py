@@ -149,3 +149,18 @@ def test_positivity_repair_matches_oracle():
     s.set_q_cells(q0)
     s.Relaxation(1)
     assert rel_err(s.get(S.PHX_Q)[:, : m.n_cell], o.q[:, : m.n_cell]) <= FP64_TOL
+
+
+@pytest.mark.parametrize("blocks", ["1", "2"])
+def test_levels_wider_than_grid(monkeypatch, blocks):
+    """Sweep levels wider than the cooperative grid (several rounds per level)."""
+    monkeypatch.setenv("PHX_LUSGS_MAX_BLOCKS", blocks)
+    m = M.channel_bump(64, 32, 8)      # widest level > 64 groups of one 512-thread block
+    params = cases.EULER_BUMP
+    o, q0 = _oracle_case(m, params, seed=6)
+    o.iterate(2)
+    s = _solver(m, params)
+    s.set_q_cells(q0)
+    s.Relaxation(2)
+    nc = m.n_cell
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= FP64_TOL
