@@ -426,6 +426,37 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     }
     bucket(nbl, bwd_cells, bwd_off, false);
 
+    // sweep entry tables in schedule order
+    auto entries = [&](const std::vector<int> &cells, bool forward, std::vector<int> &eoff, std::vector<int> &enb,
+                       std::vector<int> &ef, std::vector<int> &ej) {
+        eoff.assign(nc + 1, 0);
+        enb.clear(); ef.clear(); ej.clear();
+        for (int i = 0; i < nc; ++i) {
+            const int c = cells[i];
+            for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+                const int f = c2f[j];
+                int nbr = -1;
+                bool inward = false;
+                if (f < nb) {
+                    if (!forward) nbr = nc + f;
+                } else {
+                    const bool isLeft = h.left[f] == c;
+                    const int o = isLeft ? h.right[f] : h.left[f];
+                    if (forward ? (o < c) : (o > c)) nbr = o;
+                    inward = !isLeft;
+                }
+                if (nbr < 0) continue;
+                enb.push_back(nbr);
+                ef.push_back(inward ? (int)(f | 0x80000000u) : f);
+                ej.push_back(j);
+            }
+            eoff[i + 1] = (int)enb.size();
+        }
+    };
+    std::vector<int> fe_off, fe_nb, fe_f, fe_j, be_off, be_nb, be_f, be_j;
+    entries(fwd_cells, true, fe_off, fe_nb, fe_f, fe_j);
+    entries(bwd_cells, false, be_off, be_nb, be_f, be_j);
+
     // boundary classification
     std::vector<int32_t> bkind(nb), btype(nb);
     std::vector<uint8_t> ffadj(nc, 0);
@@ -488,6 +519,14 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= upload(ctx, &g.fwd_off, fwd_off);
     rc |= upload(ctx, &g.bwd_cells, bwd_cells);
     rc |= upload(ctx, &g.bwd_off, bwd_off);
+    rc |= upload(ctx, &g.fwd_eoff, fe_off);
+    rc |= upload(ctx, &g.fwd_enb, fe_nb);
+    rc |= upload(ctx, &g.fwd_ef, fe_f);
+    rc |= upload(ctx, &g.fwd_ej, fe_j);
+    rc |= upload(ctx, &g.bwd_eoff, be_off);
+    rc |= upload(ctx, &g.bwd_enb, be_nb);
+    rc |= upload(ctx, &g.bwd_ef, be_f);
+    rc |= upload(ctx, &g.bwd_ej, be_j);
     g.nFwdLevels = nfl; g.nBwdLevels = nbl;
     g.c2fLen = (int)c2f.size();
     g.maxLevelWidth = 1;

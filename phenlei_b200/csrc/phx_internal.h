@@ -45,6 +45,12 @@ struct DevGrid {
     const uint8_t *farfield_adj;             // [nCell] 1 if the cell touches a limiter-zeroing boundary
     const int *fwd_cells, *fwd_off;          // LU-SGS forward schedule: cells by level
     const int *bwd_cells, *bwd_off;          // backward schedule
+    // Per sweep, in schedule order: for position i the neighbours on the
+    // sweep's side, in the cell's face order, as entries eoff[i]..eoff[i+1]:
+    // neighbour cell, face (sign bit set when the normal points into the
+    // cell), and the slot j of the face in the cell's face list.
+    const int *fwd_eoff, *fwd_enb, *fwd_ef, *fwd_ej;
+    const int *bwd_eoff, *bwd_enb, *bwd_ef, *bwd_ej;
     int nFwdLevels, nBwdLevels;
     int c2fLen;                              // c2f_off[nCell]
     int maxLevelWidth;                       // widest LU-SGS level (cells)

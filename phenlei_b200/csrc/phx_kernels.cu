@@ -559,13 +559,15 @@ static constexpr int kGroup = 8;
 
 template <class T>
 struct Slot {
-    int cell;          // -1: no cell for this group at this level
-    int nb;            // neighbour index, -1 if this lane's face does not take part
+    int cell;          // -1: no cell for this group at this position
+    int nb;            // neighbour index, -1 if this lane has no entry
     T nx, ny, nz, area, l1, x1, x2, um, vm, wm, c2, hm;
     T r[5];            // lane 0: res (forward) or res - carried delta flux (backward)
     T diag;            // lane 0
 };
 
+// Loads everything the position needs except the neighbours' dq (which the
+// previous level produces): issued one level ahead, before the barrier.
 template <class T, bool kForward>
 __device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, int level_pos_end, int pos, int lane,
                                           Slot<T> &s)
@@ -574,38 +576,30 @@ __device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, in
     s.cell = -1;
     s.nb = -1;
     if (pos >= level_pos_end) return;
-    const int cell = kForward ? g.fwd_cells[pos] : g.bwd_cells[pos];
+    const int *cells = kForward ? g.fwd_cells : g.bwd_cells;
+    const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
+    const int cell = cells[pos];
     s.cell = cell;
-    const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
-    const int j = j0 + lane;
-    if (j < j1) {
-        const int f = g.c2f[j];
-        int nb = -1;
-        T sgn = T(1);
-        if (f < g.nBFace) {
-            if (!kForward) nb = nc + f;
-        } else {
-            const int le = g.left[f], re = g.right[f];
-            const bool isLeft = (le == cell);
-            const int o = isLeft ? re : le;
-            if (kForward ? (o < cell) : (o > cell)) nb = o;
-            sgn = isLeft ? T(1) : T(-1);
-        }
-        if (nb >= 0) {
-            s.nb = nb;
-            s.nx = sgn * (T)ld(g.xfn + f);
-            s.ny = sgn * (T)ld(g.yfn + f);
-            s.nz = sgn * (T)ld(g.zfn + f);
-            s.area = (T)ld(g.area + f);
-            s.l1 = w.coef[j];
-            s.x1 = w.coef[len + j];
-            s.x2 = w.coef[2 * len + j];
-            s.um = w.qw[nt + nb];
-            s.vm = w.qw[2 * nt + nb];
-            s.wm = w.qw[3 * nt + nb];
-            s.c2 = w.c2[nb];
-            s.hm = w.hm[nb];
-        }
+    const int e = eoff[pos] + lane;
+    if (e < eoff[pos + 1]) {
+        const int nb = (kForward ? g.fwd_enb : g.bwd_enb)[e];
+        const int fs = (kForward ? g.fwd_ef : g.bwd_ef)[e];
+        const int j = (kForward ? g.fwd_ej : g.bwd_ej)[e];
+        const int f = fs & 0x7fffffff;
+        const T sgn = fs < 0 ? T(-1) : T(1);
+        s.nb = nb;
+        s.nx = sgn * (T)ld(g.xfn + f);
+        s.ny = sgn * (T)ld(g.yfn + f);
+        s.nz = sgn * (T)ld(g.zfn + f);
+        s.area = (T)ld(g.area + f);
+        s.l1 = w.coef[j];
+        s.x1 = w.coef[len + j];
+        s.x2 = w.coef[2 * len + j];
+        s.um = w.qw[nt + nb];
+        s.vm = w.qw[2 * nt + nb];
+        s.wm = w.qw[3 * nt + nb];
+        s.c2 = w.c2[nb];
+        s.hm = w.hm[nb];
     }
     if (lane == 0) {
         s.diag = ldcg(w.diag + cell);
@@ -620,8 +614,9 @@ __device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, in
 
 template <class T, bool kForward>
 __device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c, const Work<T> &w, const Slot<T> &s,
-                                             int lane, unsigned mask)
+                                             int lane)
 {
+    const unsigned full = 0xffffffffu;
     const int nt = g.nTotal, nc = g.nCell;
     T df[5] = {0, 0, 0, 0, 0};
     const bool active = s.cell >= 0 && s.nb >= 0;
@@ -645,16 +640,19 @@ __device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c,
         df[3] = (s.l1 * dq[3] - s.wm * a + s.nz * b) * s.area;
         df[4] = (s.l1 * dq[4] - s.hm * a + cits * b) * s.area;
     }
-    // in-order accumulation on lane 0 of the group
-    const unsigned act = __ballot_sync(mask, active);
+    // In-order accumulation on lane 0 of the group.  Entries are compact and in
+    // face order, so the active lanes of a group are 0..n-1; the trip count is
+    // the warp's maximum (uniform across the warp).
+    const unsigned act = __ballot_sync(full, active);
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
+    const int ncnt = __popc((act >> base) & ((1u << kGroup) - 1u));
+    const int wmax = __reduce_max_sync(full, (unsigned)ncnt);
     T rhs0[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < kGroup; ++k) {
+    for (int k = 0; k < wmax; ++k) {
         T v[5];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(mask, df[m], base + k);
-        if ((act >> (base + k)) & 1u) {
+        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(full, df[m], base + k);
+        if (k < ncnt) {
 #pragma unroll
             for (int m = 0; m < 5; ++m) rhs0[m] += v[m];
         }
@@ -675,23 +673,23 @@ __device__ __forceinline__ bool run_sweep(const DevGrid &g, const NsConst &c, co
 {
     const int nlev = kForward ? g.nFwdLevels : g.nBwdLevels;
     const int *off = kForward ? g.fwd_off : g.bwd_off;
-    Slot<T> cur;
+    const int warpGroup0 = group - ((threadIdx.x & 31) / kGroup);
+    Slot<T> cur, nxt;
     load_slot<T, kForward>(g, w, off[1], off[0] + group, lane, cur);
     for (int L = 0; L < nlev; ++L) {
         const int b = off[L], e = off[L + 1];
-        process_slot<T, kForward>(g, c, w, cur, lane, 0xffffffffu);
-        // Levels wider than the grid: further rounds.  The loop bound depends
-        // only on the warp's first group, so every lane of a warp takes the same
-        // trip count (process_slot uses full-warp shuffles); groups past the end
-        // of the level carry an empty slot.
-        const int warpGroup0 = group - ((threadIdx.x & 31) / kGroup);
+        // next level's dq-independent data, in flight while this level runs
+        if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, nxt);
+        process_slot<T, kForward>(g, c, w, cur, lane);
+        // Levels wider than the grid: further rounds, warp-uniform trip count
+        // (process_slot uses full-warp collectives).
         for (int round = b + ngroups; round + warpGroup0 < e; round += ngroups) {
             Slot<T> extra;
             load_slot<T, kForward>(g, w, e, round + group, lane, extra);
-            process_slot<T, kForward>(g, c, w, extra, lane, 0xffffffffu);
+            process_slot<T, kForward>(g, c, w, extra, lane);
         }
-        if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, cur);
         if (!grid_sync(red, target, gridDim.x)) return false;
+        cur = nxt;
     }
     return true;
 }
