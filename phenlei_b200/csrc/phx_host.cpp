@@ -25,17 +25,17 @@ struct phx_ctx {
     NsConst nc{};
     int nNode = 0, nFace = 0, nCell = 0, nBFace = 0, nTotal = 0;
     bool mixed = false;
-    // host copies used to build schedules and to answer phx_get_geometry
+    // geometry in the reference's order (answers phx_get_geometry, derives dt)
     std::vector<double> geom[12];  // xfn yfn zfn area xfc yfc zfc xcc ycc zcc vol skew
-    std::vector<double> walldist;
     std::vector<void *> allocs;
     DevGrid g{};
-    double *q64[2] = {nullptr, nullptr};
+    double *q64[2] = {nullptr, nullptr};  // FP64 master state [5][nTotal], storage order
     int cur = 0;
     Work<double> w64{};
     Work<float> w32{};
     Reduce *red = nullptr;
     int *neglist = nullptr;
+    double *tmp = nullptr;                // [5][nTotal] staging buffer in the reference's order
     double *hist = nullptr;
     int histCap = 0;
     int step = 0;
@@ -243,6 +243,104 @@ void skewness(const HostGrid &h, std::vector<double> *G)
 
 }  // namespace
 
+
+// ---------------------------------------------------------------------------
+// Storage order: Morton code of the cell centroids (21 bits per axis over the
+// bounding box), ties by reference number.
+// ---------------------------------------------------------------------------
+namespace {
+
+uint64_t spread3(uint64_t v)
+{
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+}
+
+std::vector<int> morton_order(int n, const double *x, const double *y, const double *z)
+{
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    const double *a[3] = {x, y, z};
+    for (int d = 0; d < 3; ++d)
+        for (int i = 0; i < n; ++i) { lo[d] = std::min(lo[d], a[d][i]); hi[d] = std::max(hi[d], a[d][i]); }
+    std::vector<std::pair<uint64_t, int>> key(n);
+    for (int i = 0; i < n; ++i) {
+        uint64_t code = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double span = hi[d] - lo[d];
+            const double t = span > 0 ? (a[d][i] - lo[d]) / span : 0.0;
+            const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+            code |= spread3(q) << d;
+        }
+        key[i] = {code, i};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; ++i) ord[i] = key[i].second;
+    return ord;
+}
+
+double entropy_fix_coefficient(double mach, double scale)
+{
+    // Param_NSSolver::SetEntropyFixCoefficients, CFD/NSSolver/src/Param_NSSolver.cpp:224-268
+    double e;
+    if (mach <= 0.6) e = 0.0001;
+    else if (mach <= 2.0) e = 0.0001 * (mach - 2.0) / (0.6 - 2.0) + 0.01 * (mach - 0.6) / (2.0 - 0.6);
+    else if (mach <= 5.0) e = 0.01 * (mach - 5.0) / (2.0 - 5.0) + 0.5 * (mach - 2.0) / (5.0 - 2.0);
+    else e = 1.0;
+    return e * scale;
+}
+
+double total_pressure(double gama, double mach)
+{
+    // PerfectGas::ComputePTotal, API/Physics/src/PerfectGas.cpp:1609-1640 (NaN
+    // for the subsonic Mach numbers where the base of the power is negative,
+    // as in the reference; NaN switches the pressure-based CFL limit off)
+    double p = 1.0 / (gama * mach * mach);
+    const double m12 = mach * mach, gp1 = gama + 1.0, gm1 = gama - 1.0;
+    const double c1 = 2.0 / gm1 + m12;
+    const double c2 = 2.0 * gama / gm1 * m12 - 1.0;
+    const double cc = gama / (gama - 1.0);
+    const double t0t = 1.0 + 0.5 * gm1 * c1 / c2;
+    if (mach > 1.0) p *= (2.0 * gama / gp1 * m12 - gm1 / gp1);
+    return p * std::pow(t0t, cc);
+}
+
+bool limiter_zeroed(int bcType)
+{
+    // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775
+    return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW;
+}
+
+template <class T>
+int make_work(phx_ctx *ctx, Work<T> &w, const std::vector<double> &limInit)
+{
+    const size_t nt = ctx->nTotal, nc = ctx->nCell, nf = ctx->nFace;
+    int r = 0;
+    r |= dalloc(ctx, &w.qrec, nt * kQ);
+    r |= dalloc(ctx, &w.grec, nc * kG);
+    r |= dalloc(ctx, &w.flux, nf * kFlux);
+    r |= dalloc(ctx, &w.coef, 2 * nf * kCoef);
+    r |= dalloc(ctx, &w.crec, nc * kC);
+    r |= dalloc(ctx, &w.dtraw, nc);
+    r |= dalloc(ctx, &w.dqrec, nt * kD);
+    r |= dalloc(ctx, &w.dflux, nc * kD);
+    if (r) return r;
+    std::vector<T> q(nt * kQ, T(0));
+    for (size_t i = 0; i < nt; ++i) q[i * kQ + 7] = (T)limInit[i];
+    PHX_CUDA(ctx, cudaMemcpy(w.qrec, q.data(), sizeof(T) * q.size(), cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, cudaMemset(w.dqrec, 0, sizeof(T) * nt * kD));
+    PHX_CUDA(ctx, cudaMemset(w.crec, 0, sizeof(T) * nc * kC));
+    PHX_CUDA(ctx, cudaMemset(w.coef, 0, sizeof(T) * 2 * nf * kCoef));
+    return PHX_OK;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -285,36 +383,6 @@ void phx_default_params(phx_params *p)
     p->sa_source = 0;
 }
 
-static double entropy_fix_coefficient(double mach, double scale)
-{
-    // Param_NSSolver::SetEntropyFixCoefficients, CFD/NSSolver/src/Param_NSSolver.cpp:224-268
-    double e;
-    if (mach <= 0.6) e = 0.0001;
-    else if (mach <= 2.0) e = 0.0001 * (mach - 2.0) / (0.6 - 2.0) + 0.01 * (mach - 0.6) / (2.0 - 0.6);
-    else if (mach <= 5.0) e = 0.01 * (mach - 5.0) / (2.0 - 5.0) + 0.5 * (mach - 2.0) / (5.0 - 2.0);
-    else e = 1.0;
-    return e * scale;
-}
-
-static double total_pressure(double gama, double mach)
-{
-    // PerfectGas::ComputePTotal, API/Physics/src/PerfectGas.cpp:1609-1640
-    double p = 1.0 / (gama * mach * mach);
-    double m12 = mach * mach, gp1 = gama + 1.0, gm1 = gama - 1.0;
-    double c1 = 2.0 / gm1 + m12;
-    double c2 = 2.0 * gama / gm1 * m12 - 1.0;
-    double cc = gama / (gama - 1.0);
-    double t0t = 1.0 + 0.5 * gm1 * c1 / c2;
-    if (mach > 1.0) p *= (2.0 * gama / gp1 * m12 - gm1 / gp1);
-    return p * std::pow(t0t, cc);
-}
-
-static bool limiter_zeroed(int bcType)
-{
-    // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775
-    return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW;
-}
-
 int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out)
 {
     if (!out) return PHX_ERR_ARG;
@@ -323,7 +391,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         !gd->right_cell || !gd->cell_nnode || !gd->cell2node || !gd->region_type || (gd->n_bface > 0 && !gd->bface_region))
         return PHX_ERR_ARG;
     if (gd->n_cell <= 0 || gd->n_face <= 0 || gd->n_bface < 0 || gd->n_bface > gd->n_face || gd->n_node <= 0 ||
-        gd->n_cell + gd->n_bface > 0x7fffffffLL || gd->n_face > 0x7fffffffLL)
+        gd->n_cell + gd->n_bface > 0x3fffffffLL || gd->n_face > 0x3fffffffLL)
         return PHX_ERR_ARG;
     if (prm->precision != PHX_FP64 && prm->precision != PHX_MIXED) return PHX_ERR_ARG;
     if (prm->viscousType != 0) return PHX_ERR_ARG;   // viscous paths are attached by later releases
@@ -352,20 +420,26 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     h.left.assign(gd->left_cell, gd->left_cell + nf);
     h.right.assign(gd->right_cell, gd->right_cell + nf);
     for (int f = 0; f < nb; ++f) h.right[f] = nc + f;
-    for (int f = 0; f < nf; ++f) {
+    for (int f = 0; f < nf; ++f)
         if (h.left[f] < 0 || h.left[f] >= nc || (f >= nb && (h.right[f] < 0 || h.right[f] >= nc))) {
             delete ctx;
             return PHX_ERR_ARG;
         }
-    }
     for (int i = 0; i < h.foff[nf]; ++i)
         if (h.f2n[i] < 0 || h.f2n[i] >= h.nNode) { delete ctx; return PHX_ERR_ARG; }
     h.coff.resize(nc + 1);
     h.coff[0] = 0;
-    for (int c = 0; c < nc; ++c) h.coff[c + 1] = h.coff[c] + gd->cell_nnode[c];
+    for (int c = 0; c < nc; ++c) {
+        if (gd->cell_nnode[c] < 4) { delete ctx; return PHX_ERR_ARG; }
+        h.coff[c + 1] = h.coff[c] + gd->cell_nnode[c];
+    }
     h.c2n.assign(gd->cell2node, gd->cell2node + h.coff[nc]);
+    for (int i = 0; i < h.coff[nc]; ++i)
+        if (h.c2n[i] < 0 || h.c2n[i] >= h.nNode) { delete ctx; return PHX_ERR_ARG; }
+    for (int f = 0; f < nb; ++f)
+        if (gd->bface_region[f] < 0 || gd->bface_region[f] >= gd->n_region) { delete ctx; return PHX_ERR_ARG; }
 
-    // metrics
+    // FP64 metrics in the reference's order
     for (int k = 0; k < 7; ++k) ctx->geom[k].assign(nf, 0.0);
     for (int k = 7; k < 11; ++k) ctx->geom[k].assign(nt, 0.0);
     ctx->geom[11].assign(nc, 0.0);
@@ -376,7 +450,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     for (int c = 0; c < nc; ++c) vsum += ctx->geom[10][c];
     const double avgVol = vsum / (double)nc;   // Region::ComputeGlobalGridSize, Region.cpp:2655-2734
 
-    // cell -> face lists in ascending face order (UnstructGrid::ComputeCell2Face, :1246-1290)
+    // cell -> face lists in the reference's face order (UnstructGrid::ComputeCell2Face, :1246-1290)
     std::vector<int> c2f_off(nc + 1, 0), c2f;
     for (int f = 0; f < nf; ++f) { c2f_off[h.left[f] + 1]++; if (f >= nb) c2f_off[h.right[f] + 1]++; }
     for (int c = 0; c < nc; ++c) c2f_off[c + 1] += c2f_off[c];
@@ -385,8 +459,27 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         std::vector<int> fill(c2f_off.begin(), c2f_off.end() - 1);
         for (int f = 0; f < nf; ++f) { c2f[fill[h.left[f]]++] = f; if (f >= nb) c2f[fill[h.right[f]]++] = f; }
     }
+    for (int c = 0; c < nc; ++c)
+        if (c2f_off[c + 1] - c2f_off[c] > 8) { delete ctx; return PHX_ERR_ARG; }  // sweep lane groups hold 8 faces
 
-    // LU-SGS level schedules from the reference's cell order
+    // storage order
+    const std::vector<int> ord = morton_order(nc, ctx->geom[7].data(), ctx->geom[8].data(), ctx->geom[9].data());
+    std::vector<int> rank(nc);
+    for (int i = 0; i < nc; ++i) rank[ord[i]] = i;
+    std::vector<int> forder(nf);   // storage face -> reference face
+    for (int f = 0; f < nf; ++f) forder[f] = f;
+    std::stable_sort(forder.begin(), forder.begin() + nb, [&](int a, int b) { return rank[h.left[a]] < rank[h.left[b]]; });
+    std::stable_sort(forder.begin() + nb, forder.end(), [&](int a, int b) {
+        const int ma = std::min(rank[h.left[a]], rank[h.right[a]]), mb = std::min(rank[h.left[b]], rank[h.right[b]]);
+        if (ma != mb) return ma < mb;
+        return std::max(rank[h.left[a]], rank[h.right[a]]) < std::max(rank[h.left[b]], rank[h.right[b]]);
+    });
+    std::vector<int> fpos(nf);
+    for (int i = 0; i < nf; ++i) fpos[forder[i]] = i;
+    // storage index of any reference cell or ghost (ghost of reference boundary face f: nc + f)
+    auto sidx = [&](int c) { return c < nc ? rank[c] : nc + fpos[c - nc]; };
+
+    // LU-SGS level schedules from the reference's cell numbers
     std::vector<int> lev(nc, 0);
     int nfl = 0;
     for (int c = 0; c < nc; ++c) {
@@ -425,54 +518,82 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         nbl = std::max(nbl, l + 1);
     }
     bucket(nbl, bwd_cells, bwd_off, false);
+    int maxw = 1;
+    for (int l = 0; l < nfl; ++l) maxw = std::max(maxw, fwd_off[l + 1] - fwd_off[l]);
+    for (int l = 0; l < nbl; ++l) maxw = std::max(maxw, bwd_off[l + 1] - bwd_off[l]);
 
-    // sweep entry tables in schedule order
-    auto entries = [&](const std::vector<int> &cells, bool forward, std::vector<int> &eoff, std::vector<int> &enb,
-                       std::vector<int> &ef, std::vector<int> &ej) {
+    // sweep entry tables (storage indices), in schedule order and the cell's face order
+    auto entries = [&](std::vector<int> &cells, bool forward, std::vector<int> &eoff, std::vector<int> &enb,
+                       std::vector<int> &ef, std::vector<int> &ec) {
         eoff.assign(nc + 1, 0);
-        enb.clear(); ef.clear(); ej.clear();
+        enb.clear(); ef.clear(); ec.clear();
         for (int i = 0; i < nc; ++i) {
             const int c = cells[i];
             for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
                 const int f = c2f[j];
                 int nbr = -1;
-                bool inward = false;
+                bool isLeft = true;
                 if (f < nb) {
                     if (!forward) nbr = nc + f;
                 } else {
-                    const bool isLeft = h.left[f] == c;
+                    isLeft = h.left[f] == c;
                     const int o = isLeft ? h.right[f] : h.left[f];
                     if (forward ? (o < c) : (o > c)) nbr = o;
-                    inward = !isLeft;
                 }
                 if (nbr < 0) continue;
-                enb.push_back(nbr);
-                ef.push_back(inward ? (int)(f | 0x80000000u) : f);
-                ej.push_back(j);
+                enb.push_back(sidx(nbr));
+                ef.push_back(isLeft ? fpos[f] : (int)((unsigned)fpos[f] | 0x80000000u));
+                ec.push_back(2 * fpos[f] + (isLeft ? 0 : 1));
             }
             eoff[i + 1] = (int)enb.size();
+            cells[i] = rank[c];
         }
     };
-    std::vector<int> fe_off, fe_nb, fe_f, fe_j, be_off, be_nb, be_f, be_j;
-    entries(fwd_cells, true, fe_off, fe_nb, fe_f, fe_j);
-    entries(bwd_cells, false, be_off, be_nb, be_f, be_j);
+    std::vector<int> fe_off, fe_nb, fe_f, fe_c, be_off, be_nb, be_f, be_c;
+    entries(fwd_cells, true, fe_off, fe_nb, fe_f, fe_c);
+    entries(bwd_cells, false, be_off, be_nb, be_f, be_c);
 
-    // boundary classification
+    // boundary classification (storage face order)
     std::vector<int32_t> bkind(nb), btype(nb);
     std::vector<uint8_t> ffadj(nc, 0);
-    for (int f = 0; f < nb; ++f) {
-        const int r = gd->bface_region[f];
-        if (r < 0 || r >= gd->n_region) { delete ctx; return PHX_ERR_ARG; }
-        const int t = gd->region_type[r];
-        btype[f] = t;
-        if (t == PHX_BC_SOLID_SURFACE) bkind[f] = prm->viscousType ? BK_WALL : BK_SYMMETRY;
-        else if (t == PHX_BC_SYMMETRY) bkind[f] = BK_SYMMETRY;
-        else if (t == PHX_BC_FARFIELD) bkind[f] = BK_FARFIELD;
+    std::vector<double> limInit(nt, 1.0);
+    for (int fs = 0; fs < nb; ++fs) {
+        const int f = forder[fs];
+        const int t = gd->region_type[gd->bface_region[f]];
+        btype[fs] = t;
+        if (t == PHX_BC_SOLID_SURFACE) bkind[fs] = prm->viscousType ? BK_WALL : BK_SYMMETRY;
+        else if (t == PHX_BC_SYMMETRY) bkind[fs] = BK_SYMMETRY;
+        else if (t == PHX_BC_FARFIELD) bkind[fs] = BK_FARFIELD;
         else { delete ctx; return PHX_ERR_ARG; }
-        if (limiter_zeroed(t)) ffadj[h.left[f]] = 1;
+        if (limiter_zeroed(t)) { ffadj[rank[h.left[f]]] = 1; limInit[nc + fs] = 0.0; }
     }
-    std::vector<double> volpow(nc);
-    for (int c = 0; c < nc; ++c) volpow[c] = std::pow(std::pow(ctx->geom[10][c], 1.0 / 3.0), 3.0);
+
+    // records in storage order
+    std::vector<int2> lr(nf);
+    std::vector<double> frec((size_t)nf * kF), xrec((size_t)nt * kX);
+    for (int fs = 0; fs < nf; ++fs) {
+        const int f = forder[fs];
+        lr[fs] = make_int2(rank[h.left[f]], f < nb ? nc + fs : rank[h.right[f]]);
+        for (int k = 0; k < 7; ++k) frec[(size_t)fs * kF + k] = ctx->geom[k][f];
+        frec[(size_t)fs * kF + 7] = 0.0;
+    }
+    std::vector<int> origv(nt);
+    for (int i = 0; i < nt; ++i) {
+        const int c = i < nc ? ord[i] : nc + forder[i - nc];
+        origv[i] = c;
+        for (int k = 0; k < 4; ++k) xrec[(size_t)i * kX + k] = ctx->geom[7 + k][c];
+    }
+    std::vector<double> skew(nc), volpow(nc);
+    for (int i = 0; i < nc; ++i) {
+        skew[i] = ctx->geom[11][ord[i]];
+        volpow[i] = std::pow(std::pow(ctx->geom[10][ord[i]], 1.0 / 3.0), 3.0);
+    }
+    std::vector<int> sc2f_off(nc + 1, 0), sc2f(c2f.size());
+    for (int i = 0; i < nc; ++i) sc2f_off[i + 1] = sc2f_off[i] + (c2f_off[ord[i] + 1] - c2f_off[ord[i]]);
+    for (int i = 0; i < nc; ++i) {
+        const int c = ord[i];
+        for (int j = c2f_off[c], k = sc2f_off[i]; j < c2f_off[c + 1]; ++j, ++k) sc2f[k] = fpos[c2f[j]];
+    }
 
     // constants
     NsConst &k = ctx->nc;
@@ -487,7 +608,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     k.primInf[3] = std::sin(sid);
     k.primInf[4] = k.coefState;
     k.acoustic = k.convective = entropy_fix_coefficient(prm->refMachNumber, prm->roeEntropyScale);
-    double K = prm->venkatCoeff;
+    const double K = prm->venkatCoeff;
     double kt = K * K * K;
     kt *= 1.0 / std::pow(std::pow(avgVol, 1.0 / 3.0), 3.0);
     k.venkatK3 = kt;
@@ -504,76 +625,44 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     DevGrid &g = ctx->g;
     g.nCell = nc; g.nBFace = nb; g.nFace = nf; g.nTotal = nt;
     g.avgVol = avgVol;
+    g.nFwdLevels = nfl; g.nBwdLevels = nbl; g.maxLevelWidth = maxw;
+    g.walldist = nullptr;
     int rc = 0;
-    rc |= upload(ctx, &g.left, h.left);
-    rc |= upload(ctx, &g.right, h.right);
-    const double **gp[12] = {&g.xfn, &g.yfn, &g.zfn, &g.area, &g.xfc, &g.yfc, &g.zfc, &g.xcc, &g.ycc, &g.zcc, &g.vol, &g.skew};
-    for (int i = 0; i < 12; ++i) rc |= upload(ctx, gp[i], ctx->geom[i]);
+    rc |= upload(ctx, &g.lr, lr);
+    rc |= upload(ctx, &g.frec, frec);
+    rc |= upload(ctx, &g.xrec, xrec);
+    rc |= upload(ctx, &g.skew, skew);
     rc |= upload(ctx, &g.volpow, volpow);
-    rc |= upload(ctx, &g.c2f_off, c2f_off);
-    rc |= upload(ctx, &g.c2f, c2f);
+    rc |= upload(ctx, &g.c2f_off, sc2f_off);
+    rc |= upload(ctx, &g.c2f, sc2f);
+    rc |= upload(ctx, &g.orig, origv);
     rc |= upload(ctx, &g.bkind, bkind);
     rc |= upload(ctx, &g.btype, btype);
     rc |= upload(ctx, &g.farfield_adj, ffadj);
     rc |= upload(ctx, &g.fwd_cells, fwd_cells);
     rc |= upload(ctx, &g.fwd_off, fwd_off);
-    rc |= upload(ctx, &g.bwd_cells, bwd_cells);
-    rc |= upload(ctx, &g.bwd_off, bwd_off);
     rc |= upload(ctx, &g.fwd_eoff, fe_off);
     rc |= upload(ctx, &g.fwd_enb, fe_nb);
     rc |= upload(ctx, &g.fwd_ef, fe_f);
-    rc |= upload(ctx, &g.fwd_ej, fe_j);
+    rc |= upload(ctx, &g.fwd_ec, fe_c);
+    rc |= upload(ctx, &g.bwd_cells, bwd_cells);
+    rc |= upload(ctx, &g.bwd_off, bwd_off);
     rc |= upload(ctx, &g.bwd_eoff, be_off);
     rc |= upload(ctx, &g.bwd_enb, be_nb);
     rc |= upload(ctx, &g.bwd_ef, be_f);
-    rc |= upload(ctx, &g.bwd_ej, be_j);
-    g.nFwdLevels = nfl; g.nBwdLevels = nbl;
-    g.c2fLen = (int)c2f.size();
-    g.maxLevelWidth = 1;
-    for (int l = 0; l < nfl; ++l) g.maxLevelWidth = std::max(g.maxLevelWidth, fwd_off[l + 1] - fwd_off[l]);
-    for (int l = 0; l < nbl; ++l) g.maxLevelWidth = std::max(g.maxLevelWidth, bwd_off[l + 1] - bwd_off[l]);
-    for (int cc = 0; cc < nc; ++cc)
-        if (c2f_off[cc + 1] - c2f_off[cc] > 8) { phx_ctx_destroy(ctx); return PHX_ERR_ARG; }
-    g.walldist = nullptr;
-    if (rc) { std::string e = ctx->err; phx_ctx_destroy(ctx); (void)e; return PHX_ERR_CUDA; }
-
-    // state and work arrays
+    rc |= upload(ctx, &g.bwd_ec, be_c);
     rc |= dalloc(ctx, &ctx->q64[0], (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->q64[1], (size_t)5 * nt);
+    rc |= dalloc(ctx, &ctx->tmp, (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->red, 1);
     rc |= dalloc(ctx, &ctx->neglist, 1 << 16);
-    auto make_work = [&](auto &w, auto *tag) -> int {
-        using T = std::remove_pointer_t<decltype(tag)>;
-        int r = 0;
-        if (std::is_same<T, double>::value) w.qw = (T *)ctx->q64[0];
-        else r |= dalloc(ctx, &w.qw, (size_t)5 * nt);
-        r |= dalloc(ctx, &w.grad, (size_t)15 * nc);
-        r |= dalloc(ctx, &w.limit, (size_t)nt);
-        r |= dalloc(ctx, &w.res, (size_t)5 * nc);
-        r |= dalloc(ctx, &w.invspec, (size_t)nc);
-        r |= dalloc(ctx, &w.visspec, (size_t)nc);
-        r |= dalloc(ctx, &w.dtraw, (size_t)nc);
-        r |= dalloc(ctx, &w.dq, (size_t)5 * nt);
-        r |= dalloc(ctx, &w.dflux, (size_t)5 * nc);
-        r |= dalloc(ctx, &w.diag, (size_t)nc);
-        r |= dalloc(ctx, &w.coef, (size_t)3 * c2f.size());
-        r |= dalloc(ctx, &w.c2, (size_t)nt);
-        r |= dalloc(ctx, &w.hm, (size_t)nt);
-        if (!r) {
-            // ghost limiter: 1 next to walls / symmetry, 0 next to far field (SetLimitBoundary)
-            std::vector<T> gl(nt, T(1));
-            for (int f = 0; f < nb; ++f) if (limiter_zeroed(btype[f])) gl[nc + f] = T(0);
-            if (cudaMemcpy(w.limit, gl.data(), sizeof(T) * nt, cudaMemcpyHostToDevice) != cudaSuccess) r = PHX_ERR_CUDA;
-            if (cudaMemset(w.dq, 0, sizeof(T) * 5 * (size_t)nt) != cudaSuccess) r = PHX_ERR_CUDA;
-            if (cudaMemset(w.visspec, 0, sizeof(T) * (size_t)nc) != cudaSuccess) r = PHX_ERR_CUDA;
-        }
-        return r;
-    };
-    if (ctx->mixed) rc |= make_work(ctx->w32, (float *)nullptr);
-    else rc |= make_work(ctx->w64, (double *)nullptr);
-    if (rc) { phx_ctx_destroy(ctx); return PHX_ERR_CUDA; }
-    if (cudaMemset(ctx->red, 0, sizeof(Reduce)) != cudaSuccess) { phx_ctx_destroy(ctx); return PHX_ERR_CUDA; }
-
+    if (!rc) rc = ctx->mixed ? make_work(ctx, ctx->w32, limInit) : make_work(ctx, ctx->w64, limInit);
+    if (!rc && cudaMemset(ctx->red, 0, sizeof(Reduce)) != cudaSuccess) rc = PHX_ERR_CUDA;
+    if (rc) {
+        const int code = rc < 0 ? rc : PHX_ERR_CUDA;
+        phx_ctx_destroy(ctx);
+        return code;
+    }
     // free-stream initial state (NSSolverUnstruct::InitFlow), ghosts included
     std::vector<double> q0((size_t)5 * nt);
     for (int m = 0; m < 5; ++m) std::fill(q0.begin() + (size_t)m * nt, q0.begin() + (size_t)(m + 1) * nt, k.primInf[m]);
@@ -584,6 +673,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
 int phx_ctx_destroy(phx_ctx *ctx)
 {
     if (!ctx) return PHX_OK;
+    cudaStreamSynchronize(ctx->stream);
     for (void *p : ctx->allocs) cudaFree(p);
     delete ctx;
     return PHX_OK;
@@ -608,146 +698,111 @@ int64_t phx_launch_count(const phx_ctx *ctx) { return ctx ? ctx->launches : -1; 
 
 namespace {
 
-struct Sel {
-    void *ptr;         // device pointer
-    bool isFloat;      // element type of the device array
-    int rows;          // variables
-    int stride;        // device elements per row
-    int hostLen;       // host elements per row (nTotal or nCell)
-    bool writable;
-};
-
-template <class T>
-Sel select_work(phx_ctx *ctx, const Work<T> &w, int which)
+int check_launch(phx_ctx *ctx, int n = 1)
 {
-    const bool f = std::is_same<T, float>::value;
-    const int nt = ctx->nTotal, nc = ctx->nCell;
-    switch (which) {
-    case PHX_RES: return {w.res, f, 5, nc, nt, true};
-    case PHX_LIMIT: return {w.limit, f, 1, nt, nt, true};
-    case PHX_GRADX: return {w.grad, f, 5, nc, nt, true};
-    case PHX_GRADY: return {w.grad + (size_t)5 * nc, f, 5, nc, nt, true};
-    case PHX_GRADZ: return {w.grad + (size_t)10 * nc, f, 5, nc, nt, true};
-    case PHX_DQ: return {w.dq, f, 5, nt, nt, true};
-    case PHX_INVSPEC: return {w.invspec, f, 1, nc, nc, true};
-    case PHX_VISSPEC: return {w.visspec, f, 1, nc, nc, true};
-    default: return {nullptr, false, 0, 0, 0, false};
-    }
+    ctx->launches += n;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, PHX_ERR_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+    return PHX_OK;
 }
 
-Sel select_state(phx_ctx *ctx, int which)
+// Fills ctx->tmp with the selected array in the reference's order; returns the
+// number of rows and the row length (elements per row).
+template <class T>
+int export_work(phx_ctx *ctx, const Work<T> &w, int which, int &rows, int &len)
 {
-    if (which == PHX_Q) return {ctx->q64[ctx->cur], false, 5, ctx->nTotal, ctx->nTotal, true};
-    return ctx->mixed ? select_work(ctx, ctx->w32, which) : select_work(ctx, ctx->w64, which);
+    const DevGrid &g = ctx->g;
+    const int nt = ctx->nTotal, nc = ctx->nCell;
+    cudaStream_t s = ctx->stream;
+    PHX_CUDA(ctx, cudaMemsetAsync(ctx->tmp, 0, sizeof(double) * 5 * (size_t)nt, s));
+    switch (which) {
+    case PHX_RES: rows = 5; len = nt; launch_export<T>(g, w.crec, kC, 0, 5, 1, nc, ctx->tmp, nt, s); break;
+    case PHX_LIMIT: rows = 1; len = nt; launch_export<T>(g, w.qrec, kQ, 7, 1, 1, nt, ctx->tmp, nt, s); break;
+    case PHX_GRADX: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 0, 5, 3, nc, ctx->tmp, nt, s); break;
+    case PHX_GRADY: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 1, 5, 3, nc, ctx->tmp, nt, s); break;
+    case PHX_GRADZ: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 2, 5, 3, nc, ctx->tmp, nt, s); break;
+    case PHX_DQ: rows = 5; len = nt; launch_export<T>(g, w.dqrec, kD, 0, 5, 1, nt, ctx->tmp, nt, s); break;
+    case PHX_INVSPEC: rows = 1; len = nc; launch_export<T>(g, w.crec, kC, 6, 1, 1, nc, ctx->tmp, nc, s); break;
+    case PHX_VISSPEC: rows = 1; len = nc; launch_export<T>(g, w.crec, kC, 7, 1, 1, nc, ctx->tmp, nc, s); break;
+    case PHX_DT: rows = 1; len = nt; launch_export<T>(g, w.dtraw, 1, 0, 1, 1, nc, ctx->tmp, nt, s); break;
+    default: return fail(ctx, PHX_ERR_ARG, "unknown or unavailable state selector");
+    }
+    return check_launch(ctx, 2);
 }
 
 }  // namespace
 
 extern "C" {
 
-static int copy_state(phx_ctx *ctx, int which, const double *src, double *dst, int64_t n, bool toDevice, bool hostSide)
+static int get_state_impl(phx_ctx *ctx, int which, double *dst, int64_t n, bool hostSide)
 {
-    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx || !dst) return PHX_ERR_ARG;
+    const int nt = ctx->nTotal, nc = ctx->nCell;
+    int rows = 0, len = 0, rc;
+    if (which == PHX_Q) {
+        rows = 5; len = nt;
+        launch_export_q(ctx->g, ctx->q64[ctx->cur], ctx->tmp, ctx->stream);
+        rc = check_launch(ctx);
+    } else {
+        rc = ctx->mixed ? export_work(ctx, ctx->w32, which, rows, len) : export_work(ctx, ctx->w64, which, rows, len);
+    }
+    if (rc) return rc;
+    if (n != (int64_t)rows * len) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
     if (which == PHX_DT) {
-        if (toDevice) return fail(ctx, PHX_ERR_ARG, "dt is derived; it cannot be set");
-        // the reference's dt after ReduceMaxTimeStep: min(dt, ktmax * min dt) / vol, ghosts copied
-        const int nc = ctx->nCell, nt = ctx->nTotal;
-        if (n != nt) return fail(ctx, PHX_ERR_ARG, "dt holds nTotal values");
-        std::vector<double> raw(nc);
+        // the reference's dt after ReduceMaxTimeStep (NSSolverUnstruct.cpp:5717-5745):
+        // min(dt, ktmax min dt) / vol, ghosts copied from their owners
+        std::vector<double> raw(nt);
         Reduce red;
+        PHX_CUDA(ctx, cudaMemcpyAsync(raw.data(), ctx->tmp, sizeof(double) * nt, cudaMemcpyDeviceToHost, ctx->stream));
+        PHX_CUDA(ctx, cudaMemcpyAsync(&red, ctx->red, sizeof(Reduce), cudaMemcpyDeviceToHost, ctx->stream));
         PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        PHX_CUDA(ctx, cudaMemcpy(&red, ctx->red, sizeof(Reduce), cudaMemcpyDeviceToHost));
-        if (ctx->mixed) {
-            std::vector<float> t(nc);
-            PHX_CUDA(ctx, cudaMemcpy(t.data(), ctx->w32.dtraw, sizeof(float) * nc, cudaMemcpyDeviceToHost));
-            for (int i = 0; i < nc; ++i) raw[i] = t[i];
-        } else {
-            PHX_CUDA(ctx, cudaMemcpy(raw.data(), ctx->w64.dtraw, sizeof(double) * nc, cudaMemcpyDeviceToHost));
-        }
         double mindt;
         std::memcpy(&mindt, &red.mindt_bits, sizeof(double));
-        std::vector<double> out(nt);
-        for (int i = 0; i < nc; ++i) {
-            double d = raw[i];
+        for (int c = 0; c < nc; ++c) {
+            double d = raw[c];
             if (ctx->nc.ktmax > 0) d = std::min(d, ctx->nc.ktmax * mindt);
-            out[i] = d / ctx->geom[10][i];
+            raw[c] = d / ctx->geom[10][c];
         }
-        {
-            std::vector<int> left(ctx->nBFace);
-            if (ctx->nBFace)
-                PHX_CUDA(ctx, cudaMemcpy(left.data(), ctx->g.left, sizeof(int) * ctx->nBFace, cudaMemcpyDeviceToHost));
-            for (int f = 0; f < ctx->nBFace; ++f) out[nc + f] = out[left[f]];
+        for (int f = 0; f < ctx->nBFace; ++f) raw[nc + f] = 0.0;
+        // ghost dt: the owner's value (SetGhostCell)
+        std::vector<int2> lr(ctx->nBFace);
+        std::vector<int> orig(ctx->nTotal);
+        if (ctx->nBFace) {
+            PHX_CUDA(ctx, cudaMemcpy(lr.data(), ctx->g.lr, sizeof(int2) * ctx->nBFace, cudaMemcpyDeviceToHost));
+            PHX_CUDA(ctx, cudaMemcpy(orig.data(), ctx->g.orig, sizeof(int) * ctx->nTotal, cudaMemcpyDeviceToHost));
+            for (int fs = 0; fs < ctx->nBFace; ++fs) raw[orig[nc + fs]] = raw[orig[lr[fs].x]];
         }
-        if (hostSide) std::memcpy(dst, out.data(), sizeof(double) * nt);
-        else PHX_CUDA(ctx, cudaMemcpy(dst, out.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
+        if (hostSide) std::memcpy(dst, raw.data(), sizeof(double) * nt);
+        else PHX_CUDA(ctx, cudaMemcpy(dst, raw.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
         return PHX_OK;
     }
-    Sel s = select_state(ctx, which);
-    if (!s.ptr) return fail(ctx, PHX_ERR_ARG, "unknown or unavailable state selector");
-    if (n != (int64_t)s.rows * s.hostLen) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
-    const cudaMemcpyKind kin = hostSide ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    const cudaMemcpyKind kout = hostSide ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    PHX_CUDA(ctx, cudaMemcpyAsync(dst, ctx->tmp, sizeof(double) * n, hostSide ? cudaMemcpyDeviceToHost
+                                                                             : cudaMemcpyDeviceToDevice, ctx->stream));
     PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    const int cols = std::min(s.stride, s.hostLen);
-    if (!s.isFloat) {
-        for (int r = 0; r < s.rows; ++r) {
-            double *d = (double *)s.ptr + (size_t)r * s.stride;
-            if (toDevice) {
-                PHX_CUDA(ctx, cudaMemcpy(d, src + (size_t)r * s.hostLen, sizeof(double) * cols, kin));
-            } else {
-                PHX_CUDA(ctx, cudaMemcpy(dst + (size_t)r * s.hostLen, d, sizeof(double) * cols, kout));
-                if (s.hostLen > cols) {
-                    if (hostSide) std::fill(dst + (size_t)r * s.hostLen + cols, dst + (size_t)(r + 1) * s.hostLen, 0.0);
-                    else PHX_CUDA(ctx, cudaMemset(dst + (size_t)r * s.hostLen + cols, 0, sizeof(double) * (s.hostLen - cols)));
-                }
-            }
-        }
-    } else {
-        if (!hostSide) return fail(ctx, PHX_ERR_ARG, "device-pointer copies of mixed-precision arrays are not supported");
-        std::vector<float> t(cols);
-        for (int r = 0; r < s.rows; ++r) {
-            float *d = (float *)s.ptr + (size_t)r * s.stride;
-            if (toDevice) {
-                for (int i = 0; i < cols; ++i) t[i] = (float)src[(size_t)r * s.hostLen + i];
-                PHX_CUDA(ctx, cudaMemcpy(d, t.data(), sizeof(float) * cols, cudaMemcpyHostToDevice));
-            } else {
-                PHX_CUDA(ctx, cudaMemcpy(t.data(), d, sizeof(float) * cols, cudaMemcpyDeviceToHost));
-                for (int i = 0; i < cols; ++i) dst[(size_t)r * s.hostLen + i] = t[i];
-                for (int i = cols; i < s.hostLen; ++i) dst[(size_t)r * s.hostLen + i] = 0.0;
-            }
-        }
-    }
-    if (toDevice && which == PHX_Q && ctx->mixed) {
-        // keep the FP32 working copy in step with the FP64 master state
-        std::vector<float> t((size_t)5 * ctx->nTotal);
-        std::vector<double> h((size_t)5 * ctx->nTotal);
-        PHX_CUDA(ctx, cudaMemcpy(h.data(), ctx->q64[ctx->cur], sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < h.size(); ++i) t[i] = (float)h[i];
-        PHX_CUDA(ctx, cudaMemcpy(ctx->w32.qw, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
-    }
     return PHX_OK;
 }
 
-int phx_set_state(phx_ctx *ctx, int which, const double *host, int64_t n)
+static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n, bool hostSide)
 {
-    if (!host) return fail(ctx, PHX_ERR_ARG, "null host pointer");
-    return copy_state(ctx, which, host, nullptr, n, true, true);
+    if (!ctx || !src) return PHX_ERR_ARG;
+    if (which != PHX_Q) return fail(ctx, PHX_ERR_ARG, "only the primitive state (PHX_Q) can be set");
+    const int nt = ctx->nTotal;
+    if (n != (int64_t)5 * nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
+    PHX_CUDA(ctx, cudaMemcpyAsync(ctx->tmp, src, sizeof(double) * n, hostSide ? cudaMemcpyHostToDevice
+                                                                             : cudaMemcpyDeviceToDevice, ctx->stream));
+    launch_import_q(ctx->g, ctx->tmp, ctx->q64[ctx->cur], ctx->stream);
+    if (ctx->mixed) launch_sync_qrec<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->stream);
+    else launch_sync_qrec<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->stream);
+    int rc = check_launch(ctx, 2);
+    if (rc) return rc;
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PHX_OK;
 }
-int phx_get_state(phx_ctx *ctx, int which, double *host, int64_t n)
-{
-    if (!host) return fail(ctx, PHX_ERR_ARG, "null host pointer");
-    return copy_state(ctx, which, nullptr, host, n, false, true);
-}
-int phx_set_state_device(phx_ctx *ctx, int which, const double *dev, int64_t n)
-{
-    if (!dev) return fail(ctx, PHX_ERR_ARG, "null device pointer");
-    return copy_state(ctx, which, dev, nullptr, n, true, false);
-}
-int phx_get_state_device(phx_ctx *ctx, int which, double *dev, int64_t n)
-{
-    if (!dev) return fail(ctx, PHX_ERR_ARG, "null device pointer");
-    return copy_state(ctx, which, nullptr, dev, n, false, false);
-}
+
+int phx_set_state(phx_ctx *ctx, int which, const double *host, int64_t n) { return set_state_impl(ctx, which, host, n, true); }
+int phx_get_state(phx_ctx *ctx, int which, double *host, int64_t n) { return get_state_impl(ctx, which, host, n, true); }
+int phx_set_state_device(phx_ctx *ctx, int which, const double *dev, int64_t n) { return set_state_impl(ctx, which, dev, n, false); }
+int phx_get_state_device(phx_ctx *ctx, int which, double *dev, int64_t n) { return get_state_impl(ctx, which, dev, n, false); }
 
 int phx_get_geometry(phx_ctx *ctx, const char *name, double *host, int64_t n)
 {
@@ -764,33 +819,11 @@ int phx_get_geometry(phx_ctx *ctx, const char *name, double *host, int64_t n)
 
 // --- phases ----------------------------------------------------------------
 
-static __global__ void reset_reduce_kernel(Reduce *r)
-{
-    r->mindt_bits = 0x7FEFFFFFFFFFFFFFULL;  // largest finite double
-    for (int k = 0; k < 5; ++k) r->resnorm[k] = 0.0;
-    r->negcount = 0;
-}
-
-static __global__ void finish_step_kernel(Reduce *r, double *hist, int i, double ncell)
-{
-    double v = sqrt(r->resnorm[0] / ncell);
-    if (!(v == v) || v > 1.0e300) r->error = PHX_ERR_NUMERIC;
-    if (hist) hist[i] = v;
-}
-
 static double cfl_at(const NsConst &c, int step)
 {
     // NSSolver::ComputeCFL, CFD/NSSolver/src/NSSolver.cpp:595-668 (cflMethod 0)
     if (step >= c.cflVaryStep) return c.cflEnd;
     return c.cflStart + (c.cflEnd - c.cflStart) * step / c.cflVaryStep;
-}
-
-static int check_launch(phx_ctx *ctx, int n = 1)
-{
-    ctx->launches += n;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(ctx, PHX_ERR_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
-    return PHX_OK;
 }
 
 int phx_ns_boundary(phx_ctx *ctx)
@@ -812,22 +845,22 @@ int phx_ns_gradient_limiter(phx_ctx *ctx)
 int phx_ns_residual(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
-    reset_reduce_kernel<<<1, 1, 0, ctx->stream>>>(ctx->red);
+    launch_reset_reduce(ctx->red, ctx->stream);
     const double cfl = cfl_at(ctx->nc, ctx->step);
     if (ctx->mixed) launch_residual<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, cfl, ctx->stream);
     else launch_residual<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, cfl, ctx->stream);
     ctx->haveResidual = true;
-    return check_launch(ctx, 2);
+    return check_launch(ctx, 3);
 }
 
 int phx_ns_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
     if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs needs phx_ns_residual first");
-    int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->q64[ctx->cur], ctx->red, ctx->numSMs, ctx->stream)
-                       : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->q64[ctx->cur], ctx->red, ctx->numSMs, ctx->stream);
+    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->numSMs, ctx->stream)
+                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->numSMs, ctx->stream);
     if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx);
+    return check_launch(ctx, 2);
 }
 
 int phx_ns_update(phx_ctx *ctx)
@@ -836,12 +869,11 @@ int phx_ns_update(phx_ctx *ctx)
     const int nxt = 1 - ctx->cur;
     double *qo = ctx->q64[ctx->cur], *qn = ctx->q64[nxt];
     if (ctx->mixed) {
-        launch_update<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->w32.qw, ctx->red, ctx->neglist, ctx->stream);
-        launch_solution_fix<float>(ctx->g, ctx->nc, qo, qn, ctx->w32.qw, ctx->red, ctx->neglist, ctx->stream);
+        launch_update<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->red, ctx->neglist, ctx->stream);
+        launch_solution_fix<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->red, ctx->neglist, ctx->stream);
     } else {
-        launch_update<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, qn, ctx->red, ctx->neglist, ctx->stream);
-        launch_solution_fix<double>(ctx->g, ctx->nc, qo, qn, qn, ctx->red, ctx->neglist, ctx->stream);
-        ctx->w64.qw = qn;
+        launch_update<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->stream);
+        launch_solution_fix<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->stream);
     }
     ctx->cur = nxt;
     return check_launch(ctx, 2);
@@ -856,7 +888,7 @@ static int relax_one(phx_ctx *ctx, double *dhist, int i)
     if ((rc = phx_ns_residual(ctx))) return rc;
     if ((rc = phx_ns_lusgs(ctx))) return rc;
     if ((rc = phx_ns_update(ctx))) return rc;
-    finish_step_kernel<<<1, 1, 0, ctx->stream>>>(ctx->red, dhist, i, (double)ctx->nCell);
+    launch_finish_step(ctx->red, dhist, i, (double)ctx->nCell, ctx->stream);
     return check_launch(ctx);
 }
 
@@ -865,13 +897,13 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
     if (!ctx || nsteps < 0) return PHX_ERR_ARG;
     if (nsteps > ctx->histCap) {
         double *h = nullptr;
-        int rc = dalloc(ctx, &h, (size_t)nsteps);
+        const int rc = dalloc(ctx, &h, (size_t)nsteps);
         if (rc) return rc;
         ctx->hist = h;
         ctx->histCap = nsteps;
     }
     for (int i = 0; i < nsteps; ++i) {
-        int rc = relax_one(ctx, ctx->hist, i);
+        const int rc = relax_one(ctx, ctx->hist, i);
         if (rc) return rc;
     }
     Reduce red;
@@ -889,7 +921,7 @@ int phx_residual_norm(phx_ctx *ctx, double out[5])
     if (!ctx || !out) return PHX_ERR_ARG;
     const int nc = ctx->nCell;
     std::vector<double> r((size_t)5 * ctx->nTotal);
-    int rc = phx_get_state(ctx, PHX_RES, r.data(), (int64_t)r.size());
+    const int rc = phx_get_state(ctx, PHX_RES, r.data(), (int64_t)r.size());
     if (rc) return rc;
     for (int m = 0; m < 5; ++m) {
         double s = 0.0;

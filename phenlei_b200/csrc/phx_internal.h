@@ -1,5 +1,15 @@
 // Internal definitions of the phx library: the device-side grid, the
 // working arrays of one precision, and the kernel launchers.
+//
+// Storage layout.  The API speaks the reference's layout (original cell and
+// face numbers, structure-of-arrays).  On the device, cells are stored in a
+// space-filling-curve (Morton) order of their centroids and faces grouped by
+// their storage owner, so that face neighbours lie close in memory; gathered
+// per-cell and per-face data are array-of-structs records read with vector
+// loads.  The reference's numbering is kept wherever it decides an order:
+// every cell's face list is sorted by the reference face number (the order
+// LoadFlux and the Green-Gauss loop accumulate in), and the LU-SGS level
+// schedules come from the reference cell numbers.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -23,37 +33,38 @@ enum BcKind : int32_t {
     BK_EXTRAP = 3,     // OutflowBCRegion / extrapolation
 };
 
-// Per-boundary-face flags used by BoundaryQlQrFix / SetLimitBoundary / ghost dq.
-struct BFaceInfo {
-    int32_t kind;       // BcKind
-    int32_t bcType;     // the reference bcType
-};
+// Record strides (elements).
+constexpr int kQ = 8;      // qrec: rho u v w p | c2 hm | limiter
+constexpr int kG = 16;     // grec: (d/dx, d/dy, d/dz) of var k at 3k..3k+2 | pad
+constexpr int kC = 8;      // crec: res0..4 | diag | inviscid | viscous spectral radius
+constexpr int kD = 8;      // dqrec / dflux: 5 values | pad
+constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | pad
+constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
+constexpr int kFlux = 8;   // face flux record: F0..4 (times area) | inviscid spectral part | pad
+constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | pad
 
-// Read-only device grid (FP64 metrics, connectivity, schedules).
+// Read-only device grid (FP64 metrics, connectivity, schedules), storage order.
 struct DevGrid {
     int nCell, nBFace, nFace, nTotal;
-    const int *left, *right;                 // right of boundary face f = nCell + f
-    const double *xfn, *yfn, *zfn, *area;    // [nFace]
-    const double *xfc, *yfc, *zfc;           // [nFace]
-    const double *xcc, *ycc, *zcc, *vol;     // [nTotal]
-    const double *skew;                      // [nCell]
-    const double *volpow;                    // [nCell] pow(pow(vol, 1/3), 3) as VencatLimiter7 forms it
-    const double *walldist;                  // [nCell]
-    const int *c2f_off, *c2f;                // ascending face lists per cell
-    const int32_t *bkind;                    // [nBFace] BcKind
-    const int32_t *btype;                    // [nBFace] bcType
-    const uint8_t *farfield_adj;             // [nCell] 1 if the cell touches a limiter-zeroing boundary
-    const int *fwd_cells, *fwd_off;          // LU-SGS forward schedule: cells by level
-    const int *bwd_cells, *bwd_off;          // backward schedule
-    // Per sweep, in schedule order: for position i the neighbours on the
-    // sweep's side, in the cell's face order, as entries eoff[i]..eoff[i+1]:
-    // neighbour cell, face (sign bit set when the normal points into the
-    // cell), and the slot j of the face in the cell's face list.
-    const int *fwd_eoff, *fwd_enb, *fwd_ef, *fwd_ej;
-    const int *bwd_eoff, *bwd_enb, *bwd_ef, *bwd_ej;
+    const int2 *lr;              // [nFace] left, right (boundary face f: right = nCell + f)
+    const double *frec;          // [nFace][kF]
+    const double *xrec;          // [nTotal][kX]
+    const double *skew;          // [nCell]
+    const double *volpow;        // [nCell] pow(pow(vol, 1/3), 3) as VencatLimiter7 forms it
+    const double *walldist;      // [nCell]
+    const int *c2f_off, *c2f;    // faces of each cell, ordered by the reference face number
+    const int *orig;             // [nTotal] reference number of each cell (ghost: nCell + reference face)
+    const int32_t *bkind;        // [nBFace] BcKind
+    const int32_t *btype;        // [nBFace] bcType
+    const uint8_t *farfield_adj; // [nCell] 1 if the cell touches a limiter-zeroing boundary
+    // LU-SGS schedules: cells by level, and per schedule position the
+    // neighbours on the sweep's side (in the cell's face order) as entries
+    // eoff[i]..eoff[i+1]: neighbour, face (sign bit set when the normal points
+    // into the cell), and the index of the face use's factors (2 f + side).
+    const int *fwd_cells, *fwd_off, *fwd_eoff, *fwd_enb, *fwd_ef, *fwd_ec;
+    const int *bwd_cells, *bwd_off, *bwd_eoff, *bwd_enb, *bwd_ef, *bwd_ec;
     int nFwdLevels, nBwdLevels;
-    int c2fLen;                              // c2f_off[nCell]
-    int maxLevelWidth;                       // widest LU-SGS level (cells)
+    int maxLevelWidth;           // widest LU-SGS level (cells)
     double avgVol;
 };
 
@@ -75,26 +86,17 @@ struct NsConst {
     double reynolds;
 };
 
-// Working arrays of one precision T.  In FP64 mode qw aliases q64.
+// Working arrays of one precision T (double: FP64 path, float: mixed path).
 template <class T>
 struct Work {
-    T *qw;          // [5][nTotal] working primitive state
-    T *grad;        // [15][nCell]: d/dx of 5 vars, then d/dy, then d/dz
-    T *limit;       // [nTotal]
-    T *res;         // [5][nCell]
-    T *invspec;     // [nCell] inviscid spectral radius ("invSpectralRadius")
-    T *visspec;     // [nCell] viscous spectral radius ("visSpectralRadius"), viscous runs only
-    T *dtraw;       // [nCell] CFL * vol / spec before the ktmax clamp
-    T *dq;          // [5][nTotal]
-    T *dflux;       // [5][nCell] LU-SGS delta flux carried between sweeps
-    T *diag;        // [nCell]
-    // LU-SGS coefficients that do not depend on dq, filled by the residual
-    // pass: per (cell, face slot) of the cell-to-face list the split
-    // eigenvalue l1 and the MXDQ weights x1, x2 of the neighbour across that
-    // face; per cell the squared sound speed and total enthalpy.
-    T *coef;        // [3][c2fLen]
-    T *c2;          // [nTotal]
-    T *hm;          // [nTotal]
+    T *qrec;        // [nTotal][kQ] working state, c2 = |gamma p / rho|, total enthalpy, limiter
+    T *grec;        // [nCell][kG] primitive gradients
+    T *flux;        // [nFace][kFlux] face flux times area and inviscid spectral radius term
+    T *coef;        // [2 nFace][kCoef] LU-SGS factors of each face use (side 0: the left cell's view)
+    T *crec;        // [nCell][kC] residual, diagonal, spectral radii
+    T *dtraw;       // [nCell] CFL * vol / spectral radius, before the ktmax clamp
+    T *dqrec;       // [nTotal][kD] LU-SGS dq
+    T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep
 };
 
 struct Reduce {
@@ -102,8 +104,7 @@ struct Reduce {
     double resnorm[5];
     int negcount;
     unsigned int barrier;           // monotonic arrival counter of the LU-SGS grid barrier
-    int error;                      // PHX_ERR_TIMEOUT when a bounded wait gave up
-    int step;                       // outer step (CFL ramp)
+    int error;                      // PHX_ERR_TIMEOUT / PHX_ERR_NUMERIC
 };
 
 // Kernel launchers (phx_kernels.cu).
@@ -114,13 +115,25 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s);
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, Reduce *red,
-                 int numSMs, cudaStream_t s);
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s);
 template <class T>
-void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new, T *qw_out,
+void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                    Reduce *red, int *neglist, cudaStream_t s);
 template <class T>
-void launch_solution_fix(const DevGrid &g, const NsConst &c, const double *q64, double *q64_new, T *qw_out,
+void launch_solution_fix(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                          Reduce *red, int *neglist, cudaStream_t s);
+// Refreshes qrec (state, c2, hm) of all cells and ghosts from the FP64 master state.
+template <class T>
+void launch_sync_qrec(const DevGrid &g, const NsConst &c, const double *q64, const Work<T> &w, cudaStream_t s);
+// Export of record fields into reference-order SoA: out[k * outLen +
+// orig[i]] = rec[i * stride + first + k * step] for k < count, i < n.
+template <class T>
+void launch_export(const DevGrid &g, const T *rec, int stride, int first, int count, int step, int n, double *out,
+                   int outLen, cudaStream_t s);
+// q64[k][i] = in[k][orig[i]] and the inverse.
+void launch_import_q(const DevGrid &g, const double *in, double *q64, cudaStream_t s);
+void launch_export_q(const DevGrid &g, const double *q64, double *out, cudaStream_t s);
+void launch_reset_reduce(Reduce *r, cudaStream_t s);
+void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s);
 
 }  // namespace phx

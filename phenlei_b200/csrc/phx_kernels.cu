@@ -1,9 +1,9 @@
-// sm_100a kernels of the NS per-iteration path.
+// sm_100a kernels of the NS per-iteration path (storage layout: see
+// phx_internal.h).
 //
-// Every kernel is owner-computes over cells: a cell gathers from its faces in
-// ascending face order (the order LoadFlux and the Green-Gauss loop of the
-// reference accumulate in), so no atomics touch the state and the FP64 path
-// reproduces the reference's summation order.  Face metrics stay FP64; the
+// Per-cell sums are owner-computes gathers over the cell's faces in the
+// reference's face order, so no atomics touch the state and the FP64 path
+// keeps the reference's accumulation order.  Face metrics stay FP64; the
 // working state T is double (FP64 path) or float (mixed path).
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -20,6 +20,60 @@ template <class T> __device__ __forceinline__ T ld(const T *p) { return __ldg(p)
 // Loads of data written earlier in the same kernel by other blocks: bypass L1.
 template <class T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
 
+// Vector loads of 4- or 8-element records (16-byte aligned).
+__device__ __forceinline__ void ld4(const double *p, double *o)
+{
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const float *p, float *o)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+template <class T>
+__device__ __forceinline__ void ld8(const T *p, T *o) { ld4(p, o); ld4(p + 4, o + 4); }
+__device__ __forceinline__ void ld4cg(const double *p, double *o)
+{
+    const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void ld4cg(const float *p, float *o)
+{
+    const float4 a = __ldcg(reinterpret_cast<const float4 *>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+template <class T>
+__device__ __forceinline__ void ld8cg(const T *p, T *o) { ld4cg(p, o); ld4cg(p + 4, o + 4); }
+__device__ __forceinline__ void st4(double *p, const double *v)
+{
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(float *p, const float *v)
+{
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+}
+template <class T>
+__device__ __forceinline__ void st8(T *p, const T *v) { st4(p, v); st4(p + 4, v + 4); }
+
+// Writes state, c2 = |gamma p / rho| and total enthalpy of a cell record
+// (slot 7, the limiter, is left untouched).  c2 and the enthalpy are the
+// per-cell factors MXDQ_STD forms (Jacobian.cpp:22-23, PerfectGas.cpp:384-394).
+template <class T>
+__device__ __forceinline__ void put_state(T *rec, const T *q, T gm)
+{
+    const T c2 = fabs(gm * q[4] / q[0]);
+    const T hm = (gm / (gm - T(1))) * (q[4] / q[0]) + T(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    T v[4] = {q[0], q[1], q[2], q[3]};
+    st4(rec, v);
+    rec[4] = q[4];
+    rec[5] = c2;
+    rec[6] = hm;
+}
+
 // ---------------------------------------------------------------------------
 // Boundary: ghost-cell state per boundary face (NSSolverUnstruct::Boundary,
 // NSSolverUnstruct.cpp:13404-13515): SymmetryBCRegion (:19413),
@@ -27,49 +81,51 @@ template <class T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg
 // Computed in FP64 from the FP64 master state.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, T *qw, T *c2o, T *hmo)
+__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, Work<T> w)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nBFace) return;
     const int nt = g.nTotal;
-    const int le = g.left[f], re = g.nCell + f;
-    double r = q[le], u = q[nt + le], v = q[2 * nt + le], w = q[3 * nt + le], p = q[4 * nt + le];
-    double xn = g.xfn[f], yn = g.yfn[f], zn = g.zfn[f];
-    double o[5] = {r, u, v, w, p};
-    int kind = g.bkind[f];
+    const int le = g.lr[f].x, re = g.nCell + f;
+    const double r = q[le], u = q[nt + le], v = q[2 * nt + le], wv = q[3 * nt + le], p = q[4 * nt + le];
+    double fr[4];
+    ld4(g.frec + (size_t)f * kF, fr);
+    const double xn = fr[0], yn = fr[1], zn = fr[2];
+    double o[5] = {r, u, v, wv, p};
+    const int kind = g.bkind[f];
     if (kind == BK_SYMMETRY) {
-        double vn = xn * u + yn * v + zn * w;
+        const double vn = xn * u + yn * v + zn * wv;
         o[1] = u - 2.0 * xn * vn;
         o[2] = v - 2.0 * yn * vn;
-        o[3] = w - 2.0 * zn * vn;
+        o[3] = wv - 2.0 * zn * vn;
     } else if (kind == BK_WALL) {
-        o[1] = -u; o[2] = -v; o[3] = -w;
+        o[1] = -u; o[2] = -v; o[3] = -wv;
     } else if (kind == BK_FARFIELD) {
         const double *pi = c.primInf;
-        double rO = pi[0], uO = pi[1], vO = pi[2], wO = pi[3], pO = pi[4];
-        double gl = c.gama;
-        double cO = sqrt(fabs(gl * pO / rO));
-        double vnO = xn * uO + yn * vO + zn * wO;
-        double vnI = xn * u + yn * v + zn * w;
-        double cI = sqrt(fabs(gl * p / r));
-        double gm1 = gl - 1.0;
-        double velI = sqrt(u * u + v * v + w * w);
+        const double rO = pi[0], uO = pi[1], vO = pi[2], wO = pi[3], pO = pi[4];
+        const double gl = c.gama;
+        const double cO = sqrt(fabs(gl * pO / rO));
+        const double vnO = xn * uO + yn * vO + zn * wO;
+        const double vnI = xn * u + yn * v + zn * wv;
+        const double cI = sqrt(fabs(gl * p / r));
+        const double gm1 = gl - 1.0;
+        const double velI = sqrt(u * u + v * v + wv * wv);
         if (velI > cI) {
             if (vnI < 0.0) { for (int k = 0; k < 5; ++k) o[k] = pi[k]; }
         } else {
-            double Rp = vnI + 2.0 * cI / gm1;
-            double Rm = vnO - 2.0 * cO / gm1;
-            double vnB = 0.5 * (Rp + Rm);
-            double cB = 0.25 * (Rp - Rm) * gm1;
+            const double Rp = vnI + 2.0 * cI / gm1;
+            const double Rm = vnO - 2.0 * cO / gm1;
+            const double vnB = 0.5 * (Rp + Rm);
+            const double cB = 0.25 * (Rp - Rm) * gm1;
             double s, vtx, vty, vtz;
             if (vnB >= 0.0) {
                 s = p / pow(r, gl);
-                vtx = u - xn * vnI; vty = v - yn * vnI; vtz = w - zn * vnI;
+                vtx = u - xn * vnI; vty = v - yn * vnI; vtz = wv - zn * vnI;
             } else {
                 s = pO / pow(rO, gl);
                 vtx = uO - xn * vnO; vty = vO - yn * vnO; vtz = wO - zn * vnO;
             }
-            double rB = pow((cB * cB / (s * gl)), 1.0 / gm1);
+            const double rB = pow((cB * cB / (s * gl)), 1.0 / gm1);
             o[0] = rB;
             o[1] = vtx + xn * vnB;
             o[2] = vty + yn * vnB;
@@ -81,354 +137,314 @@ __global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c
     for (int k = 0; k < 5; ++k) {
         q[k * nt + re] = o[k];
         t[k] = (T)o[k];
-        if ((void *)qw != (void *)q) qw[k * nt + re] = t[k];
     }
-    // squared sound speed and total enthalpy of the ghost for the LU-SGS sweep
-    const T gm = (T)c.gama;
-    c2o[re] = fabs(gm * t[4] / t[0]);
-    hmo[re] = (gm / (gm - T(1))) * (t[4] / t[0]) + T(0.5) * (t[1] * t[1] + t[2] * t[2] + t[3] * t[3]);
+    put_state<T>(w.qrec + (size_t)re * kQ, t, (T)c.gama);
 }
 
 template <class T>
 void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s)
 {
     if (g.nBFace == 0) return;
-    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w.qw, w.c2, w.hm);
+    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) sync_qrec_kernel(DevGrid g, NsConst c, const double *q, Work<T> w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nTotal) return;
+    const int nt = g.nTotal;
+    T t[5];
+    for (int k = 0; k < 5; ++k) t[k] = (T)q[k * nt + i];
+    put_state<T>(w.qrec + (size_t)i * kQ, t, (T)c.gama);
+}
+
+template <class T>
+void launch_sync_qrec(const DevGrid &g, const NsConst &c, const double *q64, const Work<T> &w, cudaStream_t s)
+{
+    sync_qrec_kernel<T><<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w);
 }
 
 // ---------------------------------------------------------------------------
 // Gradient + limiter, fused per cell:
 //  Green-Gauss cell gradient (UnstructGrid::CompGradientGGCell,
-//  Geo_UnstructGrid.cpp:3220-3284) of the 5 primitives; then the scalar
-//  Venkatakrishnan limiter from rho and p (Limiter::VencatLimiter7,
-//  Limiter.cpp:1091-1200, neighbour min/max of Limiter::MinMaxDiff
-//  :1202-1252 over interior faces), zeroed next to far-field boundaries
-//  (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
+//  Geo_UnstructGrid.cpp:3220-3284) of the 5 primitives, accumulated in the
+//  reference's face order; then the scalar Venkatakrishnan limiter from rho
+//  and p (Limiter::VencatLimiter7, Limiter.cpp:1091-1200, neighbour min/max of
+//  Limiter::MinMaxDiff :1202-1252 over interior faces), zeroed next to
+//  far-field boundaries (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
 // ---------------------------------------------------------------------------
-// Cells are processed by groups of kLanes lanes; lane k takes the k-th face of
-// the cell's ascending face list, and lane 0 adds the lanes' terms in face
-// order, so sums keep the reference's accumulation order.
-static constexpr int kLanes = 8;
-
 template <class T>
 __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, NsConst c, Work<T> w)
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cell = tid / kLanes, lane = tid % kLanes;
-    const int base = (threadIdx.x & 31) & ~(kLanes - 1);
-    const unsigned full = 0xffffffffu;
-    const int nt = g.nTotal, nc = g.nCell;
-    const bool valid = cell < nc;
-    const T *q = w.qw;
-    int j0 = 0, j1 = 0;
-    if (valid) { j0 = g.c2f_off[cell]; j1 = g.c2f_off[cell + 1]; }
-    const int j = j0 + lane;
-    const bool act = valid && j < j1;
-    T qc[5] = {0, 0, 0, 0, 0};
-    if (valid) {
-#pragma unroll
-        for (int k = 0; k < 5; ++k) qc[k] = q[k * nt + cell];
-    }
-    // this lane's face: signed contributions qf * n A, neighbour rho and p
-    T cx[5] = {0, 0, 0, 0, 0}, cy[5] = {0, 0, 0, 0, 0}, cz[5] = {0, 0, 0, 0, 0};
-    T rn = qc[0], pn = qc[4];
-    int f = 0;
-    bool interior = false, isLeft = true;
-    if (act) {
-        f = ld(g.c2f + j);
-        const int le = ld(g.left + f);
-        isLeft = (le == cell);
-        const int nb = isLeft ? (f < g.nBFace ? nc + f : ld(g.right + f)) : le;
-        const double a = ld(g.area + f);
-        const T nx = (T)(ld(g.xfn + f) * a), ny = (T)(ld(g.yfn + f) * a), nz = (T)(ld(g.zfn + f) * a);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            const T qn = q[k * nt + nb];
-            const T qf = T(0.5) * (isLeft ? (qc[k] + qn) : (qn + qc[k]));
-            cx[k] = qf * nx; cy[k] = qf * ny; cz[k] = qf * nz;
-        }
-        interior = f >= g.nBFace;
-        if (interior) { rn = q[nb]; pn = q[4 * nt + nb]; }
-    }
-    const unsigned actm = __ballot_sync(full, act);
-    const unsigned leftm = __ballot_sync(full, isLeft);
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= g.nCell) return;
+    T qc[8];
+    ld8(w.qrec + (size_t)cell * kQ, qc);
     T gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < kLanes; ++k) {
-        const int src = base + k;
-        const bool on = (actm >> src) & 1u;
-        const bool lf = (leftm >> src) & 1u;
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-            const T vx = __shfl_sync(full, cx[m], src), vy = __shfl_sync(full, cy[m], src), vz = __shfl_sync(full, cz[m], src);
-            if (on) {
-                if (lf) { gx[m] += vx; gy[m] += vy; gz[m] += vz; }
-                else { gx[m] -= vx; gy[m] -= vy; gz[m] -= vz; }
-            }
-        }
-    }
-    // neighbour min / max of rho and p over interior faces (order-free)
-    T rmin = interior ? rn : qc[0], rmax = rmin, pmin = interior ? pn : qc[4], pmax = pmin;
-#pragma unroll
-    for (int o = kLanes / 2; o > 0; o >>= 1) {
-        rmin = tmin(rmin, __shfl_xor_sync(full, rmin, o));
-        rmax = tmax(rmax, __shfl_xor_sync(full, rmax, o));
-        pmin = tmin(pmin, __shfl_xor_sync(full, pmin, o));
-        pmax = tmax(pmax, __shfl_xor_sync(full, pmax, o));
-    }
-    rmin = tmin(rmin, qc[0]); rmax = tmax(rmax, qc[0]);
-    pmin = tmin(pmin, qc[4]); pmax = tmax(pmax, qc[4]);
-    T ovol = T(1);
-    if (valid) ovol = T(1) / (T)ld(g.vol + cell);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) { gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol; }
-    if (valid && lane == 0) {
+    T rmin = qc[0], rmax = qc[0], pmin = qc[4], pmax = qc[4];
+    const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+    for (int j = j0; j < j1; ++j) {
+        const int f = ld(g.c2f + j);
+        const int2 lr = ld(g.lr + f);
+        const bool isLeft = (lr.x == cell);
+        const int nb = isLeft ? lr.y : lr.x;
+        double fr[4];
+        ld4(g.frec + (size_t)f * kF, fr);
+        T qn[8];
+        ld8(w.qrec + (size_t)nb * kQ, qn);
+        const double a = fr[3];
+        const T nx = (T)(fr[0] * a), ny = (T)(fr[1] * a), nz = (T)(fr[2] * a);
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            w.grad[(0 * 5 + k) * nc + cell] = gx[k];
-            w.grad[(1 * 5 + k) * nc + cell] = gy[k];
-            w.grad[(2 * 5 + k) * nc + cell] = gz[k];
+            const T qf = T(0.5) * (isLeft ? (qc[k] + qn[k]) : (qn[k] + qc[k]));
+            if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
+            else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+        }
+        if (f >= g.nBFace) {
+            rmin = tmin(rmin, qn[0]); rmax = tmax(rmax, qn[0]);
+            pmin = tmin(pmin, qn[4]); pmax = tmax(pmax, qn[4]);
         }
     }
-    // Venkatakrishnan limiter: every lane holds the group's gradient (each lane
-    // accumulated the same terms in the same order)
+    double xc[4];
+    ld4(g.xrec + (size_t)cell * kX, xc);
+    const T ovol = T(1) / (T)xc[3];
+    T gr[16];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol;
+        gr[3 * k] = gx[k]; gr[3 * k + 1] = gy[k]; gr[3 * k + 2] = gz[k];
+    }
+    gr[15] = T(0);
+    T *go = w.grec + (size_t)cell * kG;
+    st8(go, gr);
+    st8(go + 8, gr + 8);
     T lim = T(1);
-    if (c.limiter == 1 && act) {
+    if (c.limiter == 1) {
         const T vp = (T)ld(g.volpow + cell);
         T er = (T)c.venkatK3 * qc[0]; er = er * qc[0]; er = er * vp;
         T ep = (T)c.venkatK3 * qc[4]; ep = ep * qc[4]; ep = ep * vp;
         const T dminr = rmin - qc[0], dmaxr = rmax - qc[0];
         const T dminp = pmin - qc[4], dmaxp = pmax - qc[4];
-        const double xc = ld(g.xcc + cell), yc = ld(g.ycc + cell), zc = ld(g.zcc + cell);
         const T small = (T)kSmall;
-        const T dx = (T)(ld(g.xfc + f) - xc), dy = (T)(ld(g.yfc + f) - yc), dz = (T)(ld(g.zfc + f) - zc);
-        T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
-        if (d > small) lim = tmin(lim, venfun(dmaxr, d, er));
-        else if (d < -small) lim = tmin(lim, venfun(dminr, d, er));
-        d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
-        if (d > small) lim = tmin(lim, venfun(dmaxp, d, ep));
-        else if (d < -small) lim = tmin(lim, venfun(dminp, d, ep));
+        for (int j = j0; j < j1; ++j) {
+            const int f = ld(g.c2f + j);
+            double fc[4];
+            ld4(g.frec + (size_t)f * kF + 4, fc);
+            const T dx = (T)(fc[0] - xc[0]), dy = (T)(fc[1] - xc[1]), dz = (T)(fc[2] - xc[2]);
+            T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
+            if (d > small) lim = tmin(lim, venfun(dmaxr, d, er));
+            else if (d < -small) lim = tmin(lim, venfun(dminr, d, er));
+            d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
+            if (d > small) lim = tmin(lim, venfun(dmaxp, d, ep));
+            else if (d < -small) lim = tmin(lim, venfun(dminp, d, ep));
+        }
+        if (g.farfield_adj[cell]) lim = T(0);
     }
-#pragma unroll
-    for (int o = kLanes / 2; o > 0; o >>= 1) lim = tmin(lim, __shfl_xor_sync(full, lim, o));
-    if (valid && lane == 0) {
-        if (c.limiter == 1 && g.farfield_adj[cell]) lim = T(0);
-        w.limit[cell] = lim;
-    }
+    w.qrec[(size_t)cell * kQ + 7] = lim;
 }
 
 template <class T>
 void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s)
 {
-    const long long threads = (long long)g.nCell * kLanes;
-    gradient_limiter_kernel<T><<<(unsigned)((threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(g, c, w);
+    gradient_limiter_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
 }
 
 // ---------------------------------------------------------------------------
-// Residual: for every face of the cell, the MUSCL face states
-// (GetQlQr / ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193),
-// the wall / symmetry face fix (BoundaryQlQrFix, :13725-13951), the Roe flux
-// times the face area (InviscidFluxWrap, :14466-14488), gathered into res with
-// the sign LoadFlux applies (:6435-6495); the inviscid spectral radius
-// (SpectrumRadiusInviscid, :5749-5850); and in the epilogue the local time
-// step (LocalTimeStep / LimitCFL, :5999-6118) with its device-wide minimum
-// (Controller::ComputeMinTimeStep, Controller.cpp:706-752).
+// Residual, pass 1 (one thread per face): MUSCL face states (GetQlQr /
+// ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193), the wall /
+// symmetry face fix (BoundaryQlQrFix, :13725-13951), the Roe flux times the
+// face area (InviscidFluxWrap, :14466-14488), the face term of the inviscid
+// spectral radius (SpectrumRadiusInviscid, :5749-5850), and the dq-independent
+// LU-SGS factors of both face uses (RoeAveragedVariables + GetRad +
+// MXDQ_STD, :15097-15116, Jacobian.cpp:27-47).
 // ---------------------------------------------------------------------------
+
+// dq-independent part of the neighbour's MXDQ_STD term for the use (cell ->
+// neighbour, normal pointing from cell to neighbour).
 template <class T>
-__device__ __forceinline__ void load_side(const DevGrid &g, const Work<T> &w, int cell, int face, T lim, T *qo)
+__device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny, T nz, T area, T gm, T *o)
 {
-    const int nt = g.nTotal, nc = g.nCell;
-    T qs[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) qs[k] = w.qw[k * nt + cell];
-    if (cell < nc) {
-        const T dx = (T)(ld(g.xfc + face) - ld(g.xcc + cell));
-        const T dy = (T)(ld(g.yfc + face) - ld(g.ycc + cell));
-        const T dz = (T)(ld(g.zfc + face) - ld(g.zcc + cell));
-        T tr[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-            tr[k] = qs[k] + lim * (w.grad[(0 * 5 + k) * nc + cell] * dx + w.grad[(1 * 5 + k) * nc + cell] * dy +
-                                   w.grad[(2 * 5 + k) * nc + cell] * dz);
-        if (tr[0] > T(0) && tr[4] > T(0)) {
-#pragma unroll
-            for (int k = 0; k < 5; ++k) qs[k] = tr[k];
-        }
-    }
-    // ghost cells carry a zero gradient (CompGradientGGCell never writes them),
-    // so their reconstruction returns the ghost state itself
+    T fp[5];
+    roe_average<T>(qc, gm, qn, gm, fp);
+    const T vn = nx * fp[1] + ny * fp[2] + nz * fp[3];
+    const T rad = (fabs(vn) + sqrt(gm * fp[4] / fp[0])) * area;
+    const T c2 = fabs(gm * qn[4] / qn[0]);
+    const T cm = sqrt(c2);
+    const T cits = nx * qn[1] + ny * qn[2] + nz * qn[3];
+    const T ipnrad = -rad / tmax(T(kSmall), area);
+    const T a1 = T(0.5) * (cits + ipnrad);
+    const T a2 = T(0.5) * (cits + cm + ipnrad);
+    const T a3 = T(0.5) * (cits - cm + ipnrad);
+    o[0] = a1;
+    o[1] = (a1 + a1 - a2 - a3) / (c2 + c2);
+    o[2] = (a2 - a3) / (cm + cm);
+    o[3] = T(0);
+}
+
+// MUSCL state of one side (ghost cells carry a zero gradient, so their state
+// is used as is).
+template <class T>
+__device__ __forceinline__ void reconstruct(const DevGrid &g, const Work<T> &w, int cell, const double *fc, T lim,
+                                            const T *qs, T *qo)
+{
 #pragma unroll
     for (int k = 0; k < 5; ++k) qo[k] = qs[k];
+    if (cell >= g.nCell) return;
+    double xc[4];
+    ld4(g.xrec + (size_t)cell * kX, xc);
+    const T dx = (T)(fc[0] - xc[0]), dy = (T)(fc[1] - xc[1]), dz = (T)(fc[2] - xc[2]);
+    T gr[16];
+    const T *gp = w.grec + (size_t)cell * kG;
+    ld8(gp, gr);
+    ld8(gp + 8, gr + 8);
+    T tr[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) tr[k] = qs[k] + lim * (gr[3 * k] * dx + gr[3 * k + 1] * dy + gr[3 * k + 2] * dz);
+    if (tr[0] > T(0) && tr[4] > T(0)) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qo[k] = tr[k];
+    }
 }
 
 template <class T>
-__device__ __forceinline__ void face_flux(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, T *fa)
+__global__ void __launch_bounds__(kThreads) face_flux_kernel(DevGrid g, NsConst c, Work<T> w)
 {
-    const int nc = g.nCell, nt = g.nTotal;
-    const int le = ld(g.left + f);
-    const int re = f < g.nBFace ? nc + f : ld(g.right + f);
-    T limL = w.limit[le], limR = w.limit[re];
-    if (c.reconMethod == 1) { T m = tmin(limL, limR); limL = limR = m; }
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= g.nFace) return;
+    const int2 lr = ld(g.lr + f);
+    const int le = lr.x, re = lr.y;
+    double fr[8];
+    ld8(g.frec + (size_t)f * kF, fr);
+    T qL[8], qR[8];
+    ld8(w.qrec + (size_t)le * kQ, qL);
+    ld8(w.qrec + (size_t)re * kQ, qR);
+    T limL = qL[7], limR = qR[7];
+    if (c.reconMethod == 1) { const T m = tmin(limL, limR); limL = limR = m; }
     T ql[5], qr[5];
-    load_side(g, w, le, f, limL, ql);
-    load_side(g, w, re, f, limR, qr);
-    const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
+    reconstruct<T>(g, w, le, fr + 4, limL, qL, ql);
+    reconstruct<T>(g, w, re, fr + 4, limR, qR, qr);
+    const T xn = (T)fr[0], yn = (T)fr[1], zn = (T)fr[2], area = (T)fr[3];
     if (f < g.nBFace) {
-        const int kind = g.bkind[f];
         const int bt = g.btype[f];
         if (bt == PHX_BC_SOLID_SURFACE || bt == PHX_BC_SYMMETRY) {
 #pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                T a = T(0.5) * (w.qw[k * nt + le] + w.qw[k * nt + re]);
-                ql[k] = a; qr[k] = a;
-            }
+            for (int k = 0; k < 5; ++k) { const T a = T(0.5) * (qL[k] + qR[k]); ql[k] = a; qr[k] = a; }
             if (bt == PHX_BC_SYMMETRY) {
-                T vn = T(2) * (xn * ql[1] + yn * ql[2] + zn * ql[3]);
+                const T vn = T(2) * (xn * ql[1] + yn * ql[2] + zn * ql[3]);
                 qr[1] = ql[1] - vn * xn; qr[2] = ql[2] - vn * yn; qr[3] = ql[3] - vn * zn;
-            } else if (kind == BK_WALL) {
+            } else if (g.bkind[f] == BK_WALL) {
                 ql[1] = ql[2] = ql[3] = T(0);
                 qr[1] = qr[2] = qr[3] = T(0);
             }
         }
     }
     const T gm = (T)c.gama;
-    roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fa);
-    const T a = (T)ld(g.area + f);
+    T fl[8];
+    roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) fa[k] *= a;
+    for (int k = 0; k < 5; ++k) fl[k] *= area;
+    // inviscid spectral radius term from the face-mean state
+    {
+        const T vnl = xn * qL[1] + yn * qL[2] + zn * qL[3];
+        const T vnr = xn * qR[1] + yn * qR[2] + zn * qR[3];
+        const T gmm = T(0.5) * (gm + gm);
+        const T pm = T(0.5) * (qL[4] + qR[4]);
+        const T rm = T(0.5) * (qL[0] + qR[0]);
+        const T vn = T(0.5) * (vnl + vnr);
+        const T cm = sqrt(gmm * pm / rm);
+        fl[5] = T(0.5) * area * (fabs(vn) + cm);
+    }
+    fl[6] = fl[7] = T(0);
+    st8(w.flux + (size_t)f * kFlux, fl);
+    // LU-SGS factors: side 0 = the left cell's view, side 1 = the right cell's
+    T cf[4];
+    lusgs_coef<T>(qL, qR, xn, yn, zn, area, gm, cf);
+    st4(w.coef + (size_t)(2 * f) * kCoef, cf);
+    if (f >= g.nBFace) {
+        lusgs_coef<T>(qR, qL, -xn, -yn, -zn, area, gm, cf);
+        st4(w.coef + (size_t)(2 * f + 1) * kCoef, cf);
+    }
 }
 
-template <class T>
-__device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny, T nz, T area, T gm, T *l1, T *x1,
-                                           T *x2);
-
+// Residual, pass 2 (one thread per cell): res gathered from the face fluxes
+// in the reference's face order with the sign LoadFlux applies
+// (NSSolverUnstruct.cpp:6435-6495), the inviscid spectral radius, and the
+// local time step (LocalTimeStep / LimitCFL, :5999-6118) with its device-wide
+// minimum (Controller::ComputeMinTimeStep, Controller.cpp:706-752).
 __device__ __forceinline__ void atomic_min_pos_double(unsigned long long *addr, double v)
 {
     atomicMin(addr, (unsigned long long)__double_as_longlong(v));
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) residual_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red, double cfl)
+__global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red, double cfl)
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cell = tid / kLanes, lane = tid % kLanes;
-    const int base = (threadIdx.x & 31) & ~(kLanes - 1);
-    const unsigned full = 0xffffffffu;
-    const int nt = g.nTotal, nc = g.nCell;
-    const bool valid = cell < nc;
-    int j0 = 0, j1 = 0;
-    if (valid) { j0 = g.c2f_off[cell]; j1 = g.c2f_off[cell + 1]; }
-    const int j = j0 + lane;
-    const bool act = valid && j < j1;
-    T fa[5] = {0, 0, 0, 0, 0};
-    T sp = T(0);
-    bool isLeft = true;
-    if (act) {
-        const int f = ld(g.c2f + j);
-        const int le = ld(g.left + f);
-        isLeft = (le == cell);
-        face_flux<T>(g, c, w, f, fa);
-        // inviscid spectral radius from the face-mean state
-        const int re = f < g.nBFace ? nc + f : ld(g.right + f);
-        const T xn = (T)ld(g.xfn + f), yn = (T)ld(g.yfn + f), zn = (T)ld(g.zfn + f);
-        const T *q = w.qw;
-        T vnl = xn * q[nt + le] + yn * q[2 * nt + le] + zn * q[3 * nt + le];
-        T vnr = xn * q[nt + re] + yn * q[2 * nt + re] + zn * q[3 * nt + re];
-        T gm = T(0.5) * ((T)c.gama + (T)c.gama);
-        T pm = T(0.5) * (q[4 * nt + le] + q[4 * nt + re]);
-        T rm = T(0.5) * (q[le] + q[re]);
-        T vn = T(0.5) * (vnl + vnr);
-        T cm = sqrt(gm * pm / rm);
-        const T area = (T)ld(g.area + f);
-        sp = T(0.5) * area * (fabs(vn) + cm);
-        // LU-SGS factors of the neighbour across this face, as seen from this cell
-        const int nbr = isLeft ? re : le;
-        const T sg = isLeft ? T(1) : T(-1);
-        T qc[5], qn[5];
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    double mydt = kLarge;
+    if (cell < g.nCell) {
+        T res[5] = {0, 0, 0, 0, 0};
+        T spec = T(0);
+        const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
+        for (int j = j0; j < j1; ++j) {
+            const int f = ld(g.c2f + j);
+            const bool isLeft = ld(&g.lr[f].x) == cell;
+            T fl[8];
+            ld8(w.flux + (size_t)f * kFlux, fl);
+            if (isLeft) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) { qc[k] = q[k * nt + cell]; qn[k] = q[k * nt + nbr]; }
-        T l1, x1, x2;
-        lusgs_coef<T>(qc, qn, sg * xn, sg * yn, sg * zn, area, (T)c.gama, &l1, &x1, &x2);
-        w.coef[j] = l1;
-        w.coef[g.c2fLen + j] = x1;
-        w.coef[2 * g.c2fLen + j] = x2;
-    }
-    // LoadFlux order: lane 0 adds the faces in ascending face order
-    const unsigned actm = __ballot_sync(full, act);
-    const unsigned leftm = __ballot_sync(full, isLeft);
-    T res[5] = {0, 0, 0, 0, 0};
-    T spec = T(0);
-#pragma unroll
-    for (int k = 0; k < kLanes; ++k) {
-        const int src = base + k;
-        const bool on = (actm >> src) & 1u;
-        const bool lf = (leftm >> src) & 1u;
-        T v[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(full, fa[m], src);
-        const T vs = __shfl_sync(full, sp, src);
-        if (on) {
-            if (lf) {
-#pragma unroll
-                for (int m = 0; m < 5; ++m) res[m] -= v[m];
+                for (int k = 0; k < 5; ++k) res[k] -= fl[k];
             } else {
 #pragma unroll
-                for (int m = 0; m < 5; ++m) res[m] += v[m];
+                for (int k = 0; k < 5; ++k) res[k] += fl[k];
             }
-            spec += vs;
+            spec += fl[5];
         }
-    }
-    double mydt = kLarge;
-    if (valid && lane == 0) {
-#pragma unroll
-        for (int k = 0; k < 5; ++k) w.res[k * nc + cell] = res[k];
-        w.invspec[cell] = spec;
-        if (c.viscous) spec += w.visspec[cell];
-        const T *q = w.qw;
-        const T gm = (T)c.gama;
-        const T r = q[cell], u = q[nt + cell], v = q[2 * nt + cell], ww = q[3 * nt + cell], p = q[4 * nt + cell];
-        w.c2[cell] = fabs(gm * p / r);
-        w.hm[cell] = (gm / (gm - T(1))) * (p / r) + T(0.5) * (u * u + v * v + ww * ww);
-        // LimitCFL: pressure- and skewness-based CFL of the cell
+        T *cr = w.crec + (size_t)cell * kC;
+        const T vis = c.viscous ? cr[7] : T(0);
+        T out[8] = {res[0], res[1], res[2], res[3], res[4], T(0), spec, vis};
+        st8(cr, out);
+        T tot = spec;
+        if (c.viscous) tot += vis;
         double cc = cfl;
-        const double pc = (double)p;
+        const double pc = (double)w.qrec[(size_t)cell * kQ + 4];
         const double plo = 0.001 * c.pTotal, phi = 0.02 * c.pTotal;
         if (pc < plo) cc = c.cflStart;
         else if (pc < phi) cc = (pc - phi) * (cfl - c.cflStart) / (phi - plo) + cfl;
         const double sk = ld(g.skew + cell);
         if (sk < 0.1) cc *= 0.1;
         else if (sk < 10.0) cc *= (1.0 - exp(0.0 - sk));
-        T dt = (T)cc * (T)ld(g.vol + cell) / spec;
+        const T dt = (T)cc * (T)ld(&g.xrec[(size_t)cell * kX + 3]) / tot;
         w.dtraw[cell] = dt;
         mydt = (double)dt;
     }
-    // device-wide minimum of dt (positive doubles order like unsigned integers)
-    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(full, mydt, o));
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
     if ((threadIdx.x & 31) == 0 && mydt < kLarge) atomic_min_pos_double(&red->mindt_bits, mydt);
 }
 
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
 {
-    const long long threads = (long long)g.nCell * kLanes;
-    residual_kernel<T><<<(unsigned)((threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(g, c, w, red, cfl);
+    face_flux_kernel<T><<<(g.nFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
+    cell_residual_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, red, cfl);
 }
 
 // ---------------------------------------------------------------------------
 // LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955): one persistent
 // cooperative kernel runs the diagonal, the forward sweep level by level, the
 // ghost-cell dq and the backward sweep level by level.  Levels come from the
-// reference's own cell order (a cell depends on its face neighbours of lower
-// index in the forward sweep, higher index in the backward sweep), so every
-// cell sees exactly the neighbour values the sequential sweep of the
-// reference sees.  The dq-independent factors of MXDQ_STD (Roe-averaged
-// spectral radius, split eigenvalue, weights) were computed by the residual
-// pass, so the sequential critical path is multiply-adds only.  Between levels
-// a device-wide barrier on a monotonic counter; every wait is bounded (a
+// reference's own cell numbers (a cell depends on its face neighbours of
+// lower number in the forward sweep, higher number in the backward sweep),
+// so every cell sees exactly the neighbour values the sequential sweep of the
+// reference sees.  The dq-independent factors of MXDQ_STD were computed by
+// the residual pass; the next level's loads are issued before the barrier,
+// so after it only the neighbours' dq are read.  Between levels a
+// device-wide barrier on a monotonic counter; every wait is bounded (a
 // timeout sets Reduce::error and the kernel returns).
 // ---------------------------------------------------------------------------
 static constexpr long long kSpinLimit = 50000000LL;  // a few seconds of polling
 static constexpr int kSweepThreads = 512;
+static constexpr int kGroup = 8;                      // lanes per cell
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
 {
@@ -461,118 +477,58 @@ __device__ __forceinline__ bool grid_sync(Reduce *red, unsigned int &target, int
     return ok != 0;
 }
 
-// dq-independent part of the neighbour's MXDQ_STD term for the use (cell ->
-// neighbour across face f): Roe-averaged spectral radius (RoeAveragedVariables
-// + GetRad, NSSolverUnstruct.cpp:15097-15116, 15297-15313) and the split
-// eigenvalue l1 and weights x1, x2 of MXDQ_STD (Jacobian.cpp:27-47).
-template <class T>
-__device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny, T nz, T area, T gm, T *l1, T *x1,
-                                           T *x2)
-{
-    T fp[5];
-    roe_average<T>(qc, gm, qn, gm, fp);
-    T vn = nx * fp[1] + ny * fp[2] + nz * fp[3];
-    T rad = (fabs(vn) + sqrt(gm * fp[4] / fp[0])) * area;
-    T c2 = fabs(gm * qn[4] / qn[0]);
-    T cm = sqrt(c2);
-    T cits = nx * qn[1] + ny * qn[2] + nz * qn[3];
-    T ipnrad = -rad / tmax(T(kSmall), area);
-    T a1 = T(0.5) * (cits + ipnrad);
-    T a2 = T(0.5) * (cits + cm + ipnrad);
-    T a3 = T(0.5) * (cits - cm + ipnrad);
-    *l1 = a1;
-    *x1 = (a1 + a1 - a2 - a3) / (c2 + c2);
-    *x2 = (a2 - a3) / (cm + cm);
-}
-
-// MXDQ_STD (Jacobian.cpp:48-86) with the precomputed factors.
-template <class T>
-__device__ __forceinline__ void mxdq_apply(const Work<T> &w, int nt, int nb, T nx, T ny, T nz, T area, T gm, T l1,
-                                           T x1, T x2, const T *dq, T *f)
-{
-    const T um = w.qw[nt + nb], vm = w.qw[2 * nt + nb], wm = w.qw[3 * nt + nb];
-    const T c2 = w.c2[nb], hm = w.hm[nb];
-    const T cits = nx * um + ny * vm + nz * wm;
-    const T dc = cits * dq[0] - nx * dq[1] - ny * dq[2] - nz * dq[3];
-    const T c2dc = c2 * dc;
-    const T v2 = um * um + vm * vm + wm * wm;
-    const T g1 = gm - T(1);
-    T dh = -g1 * (um * dq[1] + vm * dq[2] + wm * dq[3] - dq[4]);
-    dh += T(0.5) * g1 * v2 * dq[0];
-    const T a = dh * x1 + dc * x2;
-    const T b = c2dc * x1 + dh * x2;
-    f[0] = (l1 * dq[0] - a) * area;
-    f[1] = (l1 * dq[1] - um * a + nx * b) * area;
-    f[2] = (l1 * dq[2] - vm * a + ny * b) * area;
-    f[3] = (l1 * dq[3] - wm * a + nz * b) * area;
-    f[4] = (l1 * dq[4] - hm * a + cits * b) * area;
-}
-
 // Ghost-cell dq between the sweeps (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810;
 // SetSymmBCGhostDQLUSGS :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).
 template <class T>
 __device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, int f)
 {
-    const int nt = g.nTotal, nc = g.nCell;
-    const int le = g.left[f], re = nc + f;
+    const int le = g.lr[f].x, re = g.nCell + f;
     const int kind = g.bkind[f];
-    T *dq = w.dq;
-    T dl[5];
-    for (int k = 0; k < 5; ++k) dl[k] = ldcg(dq + k * nt + le);
+    T dl[8];
+    ld8cg(w.dqrec + (size_t)le * kD, dl);
+    T o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (kind == BK_SYMMETRY) {
-        const T *q = w.qw;
-        T r = q[le], u = q[nt + le], v = q[2 * nt + le], ww = q[3 * nt + le], pp = q[4 * nt + le];
-        T gm = (T)c.gama;
-        T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
+        T ql[8], qg[8];
+        ld8(w.qrec + (size_t)le * kQ, ql);
+        ld8(w.qrec + (size_t)re * kQ, qg);
+        const T r = ql[0], u = ql[1], v = ql[2], ww = ql[3], pp = ql[4];
+        const T gm = (T)c.gama;
+        const T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
         T Q[5] = {r, r * u, r * v, r * ww, r * em};
         for (int k = 0; k < 5; ++k) Q[k] += dl[k];
-        T rm = q[re], um = q[nt + re], vm = q[2 * nt + re], wm = q[3 * nt + re], pm = q[4 * nt + re];
-        T xn = (T)g.xfn[f], yn = (T)g.yfn[f], zn = (T)g.zfn[f];
-        dq[re] = dl[0];
+        const T rm = qg[0], um = qg[1], vm = qg[2], wm = qg[3], pm = qg[4];
+        double fr[4];
+        ld4(g.frec + (size_t)f * kF, fr);
+        const T xn = (T)fr[0], yn = (T)fr[1], zn = (T)fr[2];
+        o[0] = dl[0];
         T rvn = T(2) * (xn * dl[1] + yn * dl[2] + zn * dl[3]);
-        dq[nt + re] = dl[1] - xn * rvn;
-        dq[2 * nt + re] = dl[2] - yn * rvn;
-        dq[3 * nt + re] = dl[3] - zn * rvn;
+        o[1] = dl[1] - xn * rvn;
+        o[2] = dl[2] - yn * rvn;
+        o[3] = dl[3] - zn * rvn;
         rvn = T(2) * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
-        T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
-        T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
-        T g1 = gm - T(1);
-        dq[4 * nt + re] = pnew - pm / g1 + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - rm * (um * um + vm * vm + wm * wm));
+        const T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
+        const T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
+        const T g1 = gm - T(1);
+        o[4] = pnew - pm / g1 + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - rm * (um * um + vm * vm + wm * wm));
     } else if (kind == BK_WALL) {
-        dq[re] = dl[0];
-        dq[nt + re] = -dl[1];
-        dq[2 * nt + re] = -dl[2];
-        dq[3 * nt + re] = -dl[3];
-        dq[4 * nt + re] = dl[4];
-    } else {
-        for (int k = 0; k < 5; ++k) dq[k * nt + re] = T(0);
+        o[0] = dl[0]; o[1] = -dl[1]; o[2] = -dl[2]; o[3] = -dl[3]; o[4] = dl[4];
     }
+    st8(w.dqrec + (size_t)re * kD, o);
 }
-
-// A sweep is processed by groups of kGroup lanes, one cell per group: lane k
-// takes the k-th face of the cell, computes the neighbour's delta flux if the
-// neighbour is on the sweep's side, and lane 0 adds the lanes' terms in face
-// order (the reference's order).  All loads that do not depend on dq are
-// issued for the next level before the barrier (Slot), so after the barrier
-// only the neighbours' dq are read.
-static constexpr int kGroup = 8;
 
 template <class T>
 struct Slot {
     int cell;          // -1: no cell for this group at this position
-    int nb;            // neighbour index, -1 if this lane has no entry
+    int nb;            // neighbour, -1 if this lane has no entry
     T nx, ny, nz, area, l1, x1, x2, um, vm, wm, c2, hm;
     T r[5];            // lane 0: res (forward) or res - carried delta flux (backward)
     T diag;            // lane 0
 };
 
-// Loads everything the position needs except the neighbours' dq (which the
-// previous level produces): issued one level ahead, before the barrier.
 template <class T, bool kForward>
 __device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, int level_pos_end, int pos, int lane,
                                           Slot<T> &s)
 {
-    const int nt = g.nTotal, nc = g.nCell, len = g.c2fLen;
     s.cell = -1;
     s.nb = -1;
     if (pos >= level_pos_end) return;
@@ -584,46 +540,48 @@ __device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, in
     if (e < eoff[pos + 1]) {
         const int nb = (kForward ? g.fwd_enb : g.bwd_enb)[e];
         const int fs = (kForward ? g.fwd_ef : g.bwd_ef)[e];
-        const int j = (kForward ? g.fwd_ej : g.bwd_ej)[e];
+        const int ec = (kForward ? g.fwd_ec : g.bwd_ec)[e];
         const int f = fs & 0x7fffffff;
         const T sgn = fs < 0 ? T(-1) : T(1);
+        double fr[4];
+        ld4(g.frec + (size_t)f * kF, fr);
+        T cf[4];
+        ld4(w.coef + (size_t)ec * kCoef, cf);
+        T qn[8];
+        ld8(w.qrec + (size_t)nb * kQ, qn);
         s.nb = nb;
-        s.nx = sgn * (T)ld(g.xfn + f);
-        s.ny = sgn * (T)ld(g.yfn + f);
-        s.nz = sgn * (T)ld(g.zfn + f);
-        s.area = (T)ld(g.area + f);
-        s.l1 = w.coef[j];
-        s.x1 = w.coef[len + j];
-        s.x2 = w.coef[2 * len + j];
-        s.um = w.qw[nt + nb];
-        s.vm = w.qw[2 * nt + nb];
-        s.wm = w.qw[3 * nt + nb];
-        s.c2 = w.c2[nb];
-        s.hm = w.hm[nb];
+        s.nx = sgn * (T)fr[0];
+        s.ny = sgn * (T)fr[1];
+        s.nz = sgn * (T)fr[2];
+        s.area = (T)fr[3];
+        s.l1 = cf[0]; s.x1 = cf[1]; s.x2 = cf[2];
+        s.um = qn[1]; s.vm = qn[2]; s.wm = qn[3]; s.c2 = qn[5]; s.hm = qn[6];
     }
     if (lane == 0) {
-        s.diag = ldcg(w.diag + cell);
+        T cr[8];
+        ld8cg(w.crec + (size_t)cell * kC, cr);
+        s.diag = cr[5];
+        if (kForward) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            T rv = w.res[k * nc + cell];
-            if (!kForward) rv = rv - ldcg(w.dflux + k * nc + cell);
-            s.r[k] = kForward ? (rv - T(0)) : rv;
+            for (int k = 0; k < 5; ++k) s.r[k] = cr[k] - T(0);
+        } else {
+            T df[8];
+            ld8cg(w.dflux + (size_t)cell * kD, df);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) s.r[k] = cr[k] - df[k];
         }
     }
 }
 
 template <class T, bool kForward>
-__device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c, const Work<T> &w, const Slot<T> &s,
-                                             int lane)
+__device__ __forceinline__ void process_slot(const NsConst &c, const Work<T> &w, const Slot<T> &s, int lane)
 {
     const unsigned full = 0xffffffffu;
-    const int nt = g.nTotal, nc = g.nCell;
     T df[5] = {0, 0, 0, 0, 0};
     const bool active = s.cell >= 0 && s.nb >= 0;
     if (active) {
-        T dq[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) dq[k] = ldcg(w.dq + k * nt + s.nb);
+        T dq[8];
+        ld8cg(w.dqrec + (size_t)s.nb * kD, dq);
         const T gm = (T)c.gama;
         const T cits = s.nx * s.um + s.ny * s.vm + s.nz * s.wm;
         const T dc = cits * dq[0] - s.nx * dq[1] - s.ny * dq[2] - s.nz * dq[3];
@@ -640,13 +598,13 @@ __device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c,
         df[3] = (s.l1 * dq[3] - s.wm * a + s.nz * b) * s.area;
         df[4] = (s.l1 * dq[4] - s.hm * a + cits * b) * s.area;
     }
-    // In-order accumulation on lane 0 of the group.  Entries are compact and in
-    // face order, so the active lanes of a group are 0..n-1; the trip count is
-    // the warp's maximum (uniform across the warp).
+    // In-order accumulation on lane 0 of the group: entries are compact and in
+    // face order (active lanes are 0..n-1); the trip count is the warp maximum
+    // so the shuffles stay warp-uniform.
     const unsigned act = __ballot_sync(full, active);
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
     const int ncnt = __popc((act >> base) & ((1u << kGroup) - 1u));
-    const int wmax = __reduce_max_sync(full, (unsigned)ncnt);
+    const int wmax = (int)__reduce_max_sync(full, (unsigned)ncnt);
     T rhs0[5] = {0, 0, 0, 0, 0};
     for (int k = 0; k < wmax; ++k) {
         T v[5];
@@ -658,11 +616,17 @@ __device__ __forceinline__ void process_slot(const DevGrid &g, const NsConst &c,
         }
     }
     if (lane == 0 && s.cell >= 0) {
-        const int cell = s.cell;
+        T o[8];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            w.dq[k * nt + cell] = (s.r[k] - rhs0[k]) / s.diag;
-            if (kForward) w.dflux[k * nc + cell] = T(0) + rhs0[k];
+        for (int k = 0; k < 5; ++k) o[k] = (s.r[k] - rhs0[k]) / s.diag;
+        o[5] = o[6] = o[7] = T(0);
+        st8(w.dqrec + (size_t)s.cell * kD, o);
+        if (kForward) {
+            T d[8];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) d[k] = T(0) + rhs0[k];
+            d[5] = d[6] = d[7] = T(0);
+            st8(w.dflux + (size_t)s.cell * kD, d);
         }
     }
 }
@@ -678,15 +642,14 @@ __device__ __forceinline__ bool run_sweep(const DevGrid &g, const NsConst &c, co
     load_slot<T, kForward>(g, w, off[1], off[0] + group, lane, cur);
     for (int L = 0; L < nlev; ++L) {
         const int b = off[L], e = off[L + 1];
-        // next level's dq-independent data, in flight while this level runs
         if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, nxt);
-        process_slot<T, kForward>(g, c, w, cur, lane);
-        // Levels wider than the grid: further rounds, warp-uniform trip count
-        // (process_slot uses full-warp collectives).
+        process_slot<T, kForward>(c, w, cur, lane);
+        // Levels wider than the grid: further rounds with a warp-uniform trip
+        // count (process_slot uses full-warp collectives).
         for (int round = b + ngroups; round + warpGroup0 < e; round += ngroups) {
             Slot<T> extra;
             load_slot<T, kForward>(g, w, e, round + group, lane, extra);
-            process_slot<T, kForward>(g, c, w, extra, lane);
+            process_slot<T, kForward>(c, w, extra, lane);
         }
         if (!grid_sync(red, target, gridDim.x)) return false;
         cur = nxt;
@@ -703,18 +666,19 @@ __global__ void __launch_bounds__(kSweepThreads, 1) lusgs_kernel(DevGrid g, NsCo
     const int group = tid / kGroup, lane = tid % kGroup, ngroups = stride / kGroup;
     unsigned int target = 0;
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
-
-    // Diagonal (NSSolverUnstruct.cpp:15867-15935); single sweep: dq starts
-    // from res, the carried delta flux from zero (LUSGSInitialization,
-    // Controller.cpp:1765-1777).
+    // Diagonal (NSSolverUnstruct.cpp:15867-15935): D = vol / dt' + spectral
+    // radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep, :5717-5745);
+    // single sweep: dq starts from res and the carried delta flux from zero
+    // (LUSGSInitialization, Controller.cpp:1765-1777).
     for (int cell = tid; cell < nc; cell += stride) {
         T dt = w.dtraw[cell];
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
-        dt /= (T)g.vol[cell];
+        dt /= (T)g.xrec[(size_t)cell * kX + 3];
+        T *cr = w.crec + (size_t)cell * kC;
         T d = T(1) / dt;
-        d += w.invspec[cell];
-        if (c.viscous) d += w.visspec[cell];
-        w.diag[cell] = d;
+        d += cr[6];
+        if (c.viscous) d += cr[7];
+        cr[5] = d;
     }
     if (!grid_sync(red, target, gridDim.x)) return;
     if (!run_sweep<T, true>(g, c, w, red, target, group, ngroups, lane)) return;
@@ -726,17 +690,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1) lusgs_kernel(DevGrid g, NsCo
 static __global__ void reset_barrier_kernel(Reduce *r) { r->barrier = 0u; }
 
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, Reduce *red, int numSMs,
-                 cudaStream_t s)
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s)
 {
-    (void)q64;
     static int perSMcache[2] = {-1, -1};
     int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
     if (perSM < 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kSweepThreads, 0);
         if (perSM < 1) perSM = 1;
     }
-    // one group per cell of the widest level; never more blocks than can be co-resident
+    // one lane group per cell of the widest level, never more blocks than can be co-resident
     const long long threads = (long long)g.maxLevelWidth * kGroup;
     int blocks = (int)((threads + kSweepThreads - 1) / kSweepThreads);
     if (blocks > numSMs * perSM) blocks = numSMs * perSM;
@@ -762,47 +724,53 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const dou
 // Q_cons (FP64, from the FP64 master primitive state) += dq, back to
 // primitive.  Cells whose density or pressure drop below 1e-6 of the free
 // stream are listed for the ordered SolutionFix pass.  Also reduces the
-// residual monitor sum res_m^2 in FP64 (Residual.cpp:534-600).
-// q_old is read, q_new written (ghosts copied), so the repair pass can see
-// the pre-update state of higher-index neighbours as the in-place sequential
-// loop of the reference does.
+// residual monitor sum res_m^2 in FP64 (Residual.cpp:534-600).  q_old is read
+// and q_new written (ghosts copied), so the repair pass can see the
+// pre-update state of neighbours that come later in the reference's order,
+// as the in-place sequential loop of the reference does.
 // ---------------------------------------------------------------------------
 static constexpr int kMaxNeg = 1 << 16;
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) update_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo,
-                                                          double *qn, T *qw_out, Reduce *red, int *neglist)
+                                                          double *qn, Reduce *red, int *neglist)
 {
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     const int nt = g.nTotal, nc = g.nCell;
     double rs[5] = {0, 0, 0, 0, 0};
     if (cell < nc) {
-        double r = qo[cell], u = qo[nt + cell], v = qo[2 * nt + cell], ww = qo[3 * nt + cell], p = qo[4 * nt + cell];
+        const double r = qo[cell], u = qo[nt + cell], v = qo[2 * nt + cell], ww = qo[3 * nt + cell], p = qo[4 * nt + cell];
         const double gm = c.gama;
-        double em = (p / r) / (gm - 1.0) + 0.5 * (u * u + v * v + ww * ww);
+        const double em = (p / r) / (gm - 1.0) + 0.5 * (u * u + v * v + ww * ww);
         double Q[5] = {r, r * u, r * v, r * ww, r * em};
+        T dq[8];
+        ld8(w.dqrec + (size_t)cell * kD, dq);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) Q[k] += (double)w.dq[k * nt + cell];
+        for (int k = 0; k < 5; ++k) Q[k] += (double)dq[k];
         double prim[5];
         if (Q[0] <= 0.0) {
             prim[0] = Q[0]; prim[1] = u; prim[2] = v; prim[3] = ww; prim[4] = p;
         } else {
-            double od = 1.0 / Q[0];
-            double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
-            double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
+            const double od = 1.0 / Q[0];
+            const double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
+            const double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
             prim[0] = Q[0]; prim[1] = um; prim[2] = vm; prim[3] = wm; prim[4] = (gm - 1.0) * ie;
         }
         if (prim[0] < 1.0e-6 * c.primInf[0] || prim[4] < 1.0e-6 * c.primInf[4]) {
-            int slot = atomicAdd(&red->negcount, 1);
+            const int slot = atomicAdd(&red->negcount, 1);
             if (slot < kMaxNeg) neglist[slot] = cell;
         }
+        T t[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
             qn[k * nt + cell] = prim[k];
-            if ((void *)qw_out != (void *)qn) qw_out[k * nt + cell] = (T)prim[k];
-            double rv = (double)w.res[k * nc + cell];
-            rs[k] = rv * rv;
+            t[k] = (T)prim[k];
         }
+        put_state<T>(w.qrec + (size_t)cell * kQ, t, (T)gm);
+        T cr[8];
+        ld8(w.crec + (size_t)cell * kC, cr);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) rs[k] = (double)cr[k] * (double)cr[k];
     }
     if (cell < g.nBFace) {
         const int gc = nc + cell;
@@ -818,40 +786,44 @@ __global__ void __launch_bounds__(kThreads) update_kernel(DevGrid g, NsConst c, 
 }
 
 template <class T>
-void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new, T *qw_out,
+void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                    Reduce *red, int *neglist, cudaStream_t s)
 {
-    int n = g.nCell > g.nBFace ? g.nCell : g.nBFace;
-    update_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, q64, q64_new, qw_out, red, neglist);
+    const int n = g.nCell > g.nBFace ? g.nCell : g.nBFace;
+    update_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
 }
 
-// SolutionFix (NSSolverUnstruct.cpp:14509-14585) for the listed cells, in
-// ascending cell order: neighbour averages of rho,u,v,w,p (|rho|, |p|),
-// lower-index neighbours taken after their update, higher-index ones before.
-// One thread: the list is empty in healthy runs and short otherwise.
+// SolutionFix (NSSolverUnstruct.cpp:14509-14585) for the listed cells, in the
+// reference's cell order: neighbour averages of rho,u,v,w,p (|rho|, |p|),
+// neighbours earlier in the reference's order taken after their update,
+// later ones before.  One thread: the list is empty in healthy runs and short
+// otherwise.
 template <class T>
-__global__ void solution_fix_kernel(DevGrid g, NsConst c, const double *qo, double *qn, T *qw_out, Reduce *red,
+__global__ void solution_fix_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo, double *qn, Reduce *red,
                                     int *neglist)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int n = red->negcount;
     if (n <= 0) return;
     if (n > kMaxNeg) { red->error = PHX_ERR_NUMERIC; n = kMaxNeg; }
-    for (int i = 1; i < n; ++i) {  // insertion sort (short list)
-        int v = neglist[i], j = i - 1;
-        while (j >= 0 && neglist[j] > v) { neglist[j + 1] = neglist[j]; --j; }
+    for (int i = 1; i < n; ++i) {  // insertion sort by reference number (short list)
+        const int v = neglist[i];
+        const int ov = g.orig[v];
+        int j = i - 1;
+        while (j >= 0 && g.orig[neglist[j]] > ov) { neglist[j + 1] = neglist[j]; --j; }
         neglist[j + 1] = v;
     }
-    const int nt = g.nTotal, nc = g.nCell;
+    const int nt = g.nTotal;
     const double rlim = 1.0e-6 * c.primInf[0], plim = 1.0e-6 * c.primInf[4];
     for (int i = 0; i < n; ++i) {
         const int cell = neglist[i];
+        const int oc = g.orig[cell];
         double acc[5] = {0, 0, 0, 0, 0}, wsum = 0.0;
         for (int j = g.c2f_off[cell]; j < g.c2f_off[cell + 1]; ++j) {
             const int f = g.c2f[j];
-            const int le = g.left[f], re = f < g.nBFace ? nc + f : g.right[f];
-            const int nb = (cell == le) ? re : le;
-            const double *src = (nb < cell) ? qn : qo;
+            const int2 lr = g.lr[f];
+            const int nb = (cell == lr.x) ? lr.y : lr.x;
+            const double *src = (g.orig[nb] < oc) ? qn : qo;
             if (src[nb] < rlim || src[4 * nt + nb] < plim) continue;
             wsum += 1.0;
             for (int k = 0; k < 5; ++k) {
@@ -861,34 +833,102 @@ __global__ void solution_fix_kernel(DevGrid g, NsConst c, const double *qo, doub
             }
         }
         double prim[5];
-        if (wsum > 0.0) { double o = 1.0 / wsum; for (int k = 0; k < 5; ++k) prim[k] = acc[k] * o; }
+        if (wsum > 0.0) { const double o = 1.0 / wsum; for (int k = 0; k < 5; ++k) prim[k] = acc[k] * o; }
         else for (int k = 0; k < 5; ++k) prim[k] = c.primInf[k];
-        for (int k = 0; k < 5; ++k) {
-            qn[k * nt + cell] = prim[k];
-            if ((void *)qw_out != (void *)qn) qw_out[k * nt + cell] = (T)prim[k];
-        }
+        T t[5];
+        for (int k = 0; k < 5; ++k) { qn[k * nt + cell] = prim[k]; t[k] = (T)prim[k]; }
+        put_state<T>(w.qrec + (size_t)cell * kQ, t, (T)c.gama);
     }
 }
 
 template <class T>
-void launch_solution_fix(const DevGrid &g, const NsConst &c, const double *q64, double *q64_new, T *qw_out,
+void launch_solution_fix(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                          Reduce *red, int *neglist, cudaStream_t s)
 {
-    solution_fix_kernel<T><<<1, 32, 0, s>>>(g, c, q64, q64_new, qw_out, red, neglist);
+    solution_fix_kernel<T><<<1, 32, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference order (API) and storage order.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void export_kernel(DevGrid g, const T *rec, int stride, int first, int count, int step, int n, double *out,
+                              int outLen)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = g.orig[i];
+    for (int k = 0; k < count; ++k) out[(size_t)k * outLen + o] = (double)rec[(size_t)i * stride + first + k * step];
+}
+
+template <class T>
+void launch_export(const DevGrid &g, const T *rec, int stride, int first, int count, int step, int n, double *out,
+                   int outLen, cudaStream_t s)
+{
+    export_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, rec, stride, first, count, step, n, out,
+                                                                       outLen);
+}
+
+__global__ void import_q_kernel(DevGrid g, const double *in, double *q)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nTotal) return;
+    const int o = g.orig[i], nt = g.nTotal;
+    for (int k = 0; k < 5; ++k) q[(size_t)k * nt + i] = in[(size_t)k * nt + o];
+}
+
+__global__ void export_q_kernel(DevGrid g, const double *q, double *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nTotal) return;
+    const int o = g.orig[i], nt = g.nTotal;
+    for (int k = 0; k < 5; ++k) out[(size_t)k * nt + o] = q[(size_t)k * nt + i];
+}
+
+void launch_import_q(const DevGrid &g, const double *in, double *q64, cudaStream_t s)
+{
+    import_q_kernel<<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, in, q64);
+}
+
+void launch_export_q(const DevGrid &g, const double *q64, double *out, cudaStream_t s)
+{
+    export_q_kernel<<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, q64, out);
+}
+
+static __global__ void reset_reduce_kernel(Reduce *r)
+{
+    r->mindt_bits = 0x7FEFFFFFFFFFFFFFULL;  // largest finite double
+    for (int k = 0; k < 5; ++k) r->resnorm[k] = 0.0;
+    r->negcount = 0;
+}
+
+static __global__ void finish_step_kernel(Reduce *r, double *hist, int i, double ncell)
+{
+    const double v = sqrt(r->resnorm[0] / ncell);
+    if (!(v == v) || v > 1.0e300) r->error = PHX_ERR_NUMERIC;
+    if (hist) hist[i] = v;
+}
+
+void launch_reset_reduce(Reduce *r, cudaStream_t s) { reset_reduce_kernel<<<1, 1, 0, s>>>(r); }
+void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s)
+{
+    finish_step_kernel<<<1, 1, 0, s>>>(r, hist, i, ncell);
 }
 
 // Explicit instantiations for the FP64 and mixed paths.
-#define PHX_INSTANTIATE(T)                                                                                      \
-    template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, const Work<T> &, cudaStream_t);\
-    template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);   \
-    template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,        \
-                                     cudaStream_t);                                                              \
-    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, Reduce *, int, \
-                                 cudaStream_t);                                                                  \
-    template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *, T *, \
-                                   Reduce *, int *, cudaStream_t);                                               \
-    template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const double *, double *, T *, Reduce *, \
-                                         int *, cudaStream_t);
+#define PHX_INSTANTIATE(T)                                                                                         \
+    template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, const Work<T> &, cudaStream_t);   \
+    template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);      \
+    template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,           \
+                                     cudaStream_t);                                                                 \
+    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t);   \
+    template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \
+                                   Reduce *, int *, cudaStream_t);                                                  \
+    template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *,         \
+                                         double *, Reduce *, int *, cudaStream_t);                                  \
+    template void launch_sync_qrec<T>(const DevGrid &, const NsConst &, const double *, const Work<T> &,            \
+                                      cudaStream_t);                                                                \
+    template void launch_export<T>(const DevGrid &, const T *, int, int, int, int, int, double *, int, cudaStream_t);
 PHX_INSTANTIATE(double)
 PHX_INSTANTIATE(float)
 
