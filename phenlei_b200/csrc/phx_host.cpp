@@ -36,6 +36,8 @@ struct phx_ctx {
     Reduce *red = nullptr;
     int *neglist = nullptr;
     double *tmp = nullptr;                // [5][nTotal] staging buffer in the reference's order
+    int *flagF = nullptr, *flagB = nullptr;  // LU-SGS per-cell completion flags (epoch of the solve)
+    int epoch = 0;
     double *hist = nullptr;
     int histCap = 0;
     int step = 0;
@@ -656,6 +658,10 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= dalloc(ctx, &ctx->tmp, (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->red, 1);
     rc |= dalloc(ctx, &ctx->neglist, 1 << 16);
+    rc |= dalloc(ctx, &ctx->flagF, (size_t)nc);
+    rc |= dalloc(ctx, &ctx->flagB, (size_t)nc);
+    if (!rc && (cudaMemset(ctx->flagF, 0, sizeof(int) * nc) != cudaSuccess ||
+                cudaMemset(ctx->flagB, 0, sizeof(int) * nc) != cudaSuccess)) rc = PHX_ERR_CUDA;
     if (!rc) rc = ctx->mixed ? make_work(ctx, ctx->w32, limInit) : make_work(ctx, ctx->w64, limInit);
     if (!rc && cudaMemset(ctx->red, 0, sizeof(Reduce)) != cudaSuccess) rc = PHX_ERR_CUDA;
     if (rc) {
@@ -857,10 +863,13 @@ int phx_ns_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
     if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs needs phx_ns_residual first");
-    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->numSMs, ctx->stream)
-                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->numSMs, ctx->stream);
+    ctx->epoch += 1;
+    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->flagF, ctx->flagB,
+                                                   ctx->epoch, ctx->numSMs, ctx->stream)
+                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->flagF, ctx->flagB,
+                                                    ctx->epoch, ctx->numSMs, ctx->stream);
     if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx, 2);
+    return check_launch(ctx, 1);
 }
 
 int phx_ns_update(phx_ctx *ctx)

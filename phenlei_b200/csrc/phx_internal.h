@@ -115,7 +115,8 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s);
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s);
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int *flagF, int *flagB, int epoch,
+                 int numSMs, cudaStream_t s);
 template <class T>
 void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                    Reduce *red, int *neglist, cudaStream_t s);

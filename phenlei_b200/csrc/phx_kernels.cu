@@ -430,63 +430,62 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 }
 
 // ---------------------------------------------------------------------------
-// LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955): one persistent
-// cooperative kernel runs the diagonal, the forward sweep level by level, the
-// ghost-cell dq and the backward sweep level by level.  Levels come from the
-// reference's own cell numbers (a cell depends on its face neighbours of
-// lower number in the forward sweep, higher number in the backward sweep),
-// so every cell sees exactly the neighbour values the sequential sweep of the
-// reference sees.  The dq-independent factors of MXDQ_STD were computed by
-// the residual pass; the next level's loads are issued before the barrier,
-// so after it only the neighbours' dq are read.  Between levels a
-// device-wide barrier on a monotonic counter; every wait is bounded (a
-// timeout sets Reduce::error and the kernel returns).
+// LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955) as a dataflow
+// computation.  The forward sweep of the reference visits cells in
+// increasing number and uses the just-updated dq of lower-numbered face
+// neighbours; the backward sweep the reverse.  Here every cell publishes
+// "forward done" and "backward done" flags (the solve's epoch number) after
+// its dq; a cell waits only on the flags of the neighbours it reads, so it
+// sees exactly the values the sequential sweep of the reference sees, with
+// no device-wide barrier.  Lane groups (one per cell) take schedule
+// positions in level order (forward positions, then backward positions);
+// a group only waits on cells of earlier positions, and all groups are
+// co-resident (cooperative launch), so the wait graph cannot cycle.  Every
+// wait is bounded: a timeout sets Reduce::error and the kernel gives up.
+// The dq-independent MXDQ_STD factors were computed by the residual pass.
 // ---------------------------------------------------------------------------
-static constexpr long long kSpinLimit = 50000000LL;  // a few seconds of polling
-static constexpr int kSweepThreads = 512;
+static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
+static constexpr int kSweepThreads = 256;
 static constexpr int kGroup = 8;                      // lanes per cell
 
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
+__device__ __forceinline__ int ld_acquire(const int *p)
 {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ bool grid_sync(Reduce *red, unsigned int &target, int nblocks)
+__device__ __forceinline__ void st_release(int *p, int v)
 {
-    if (nblocks == 1) { __syncthreads(); return true; }
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        target += (unsigned int)nblocks;
-        __threadfence();
-        atomicAdd(&red->barrier, 1u);
-        long long spins = 0;
-        while (ld_acquire(&red->barrier) < target) {
-            __nanosleep(20);
-            if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
-                atomicExch(&red->error, PHX_ERR_TIMEOUT);
-                ok = 0;
-                break;
-            }
-        }
-    }
-    __syncthreads();
-    return ok != 0;
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Ghost-cell dq between the sweeps (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810;
-// SetSymmBCGhostDQLUSGS :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).
+// Bounded wait for flag == epoch; false on timeout (sets the error flag).
+__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, Reduce *red)
+{
+    if (ld_acquire(flag) == epoch) return true;
+    long long spins = 0;
+    while (ld_acquire(flag) != epoch) {
+        __nanosleep(32);
+        if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
+            atomicExch(&red->error, PHX_ERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+// Ghost-cell dq of boundary face f from the owner's forward dq
+// (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810; SetSymmBCGhostDQLUSGS
+// :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).
 template <class T>
-__device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, int f)
+__device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, const T *dl,
+                                         T *o)
 {
     const int le = g.lr[f].x, re = g.nCell + f;
     const int kind = g.bkind[f];
-    T dl[8];
-    ld8cg(w.dqrec + (size_t)le * kD, dl);
-    T o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) o[k] = T(0);
     if (kind == BK_SYMMETRY) {
         T ql[8], qg[8];
         ld8(w.qrec + (size_t)le * kQ, ql);
@@ -513,184 +512,132 @@ __device__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, i
     } else if (kind == BK_WALL) {
         o[0] = dl[0]; o[1] = -dl[1]; o[2] = -dl[2]; o[3] = -dl[3]; o[4] = dl[4];
     }
-    st8(w.dqrec + (size_t)re * kD, o);
 }
 
-template <class T>
-struct Slot {
-    int cell;          // -1: no cell for this group at this position
-    int nb;            // neighbour, -1 if this lane has no entry
-    T nx, ny, nz, area, l1, x1, x2, um, vm, wm, c2, hm;
-    T r[5];            // lane 0: res (forward) or res - carried delta flux (backward)
-    T diag;            // lane 0
-};
-
+// One schedule position of a sweep, processed by a lane group.
 template <class T, bool kForward>
-__device__ __forceinline__ void load_slot(const DevGrid &g, const Work<T> &w, int level_pos_end, int pos, int lane,
-                                          Slot<T> &s)
-{
-    s.cell = -1;
-    s.nb = -1;
-    if (pos >= level_pos_end) return;
-    const int *cells = kForward ? g.fwd_cells : g.bwd_cells;
-    const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
-    const int cell = cells[pos];
-    s.cell = cell;
-    const int e = eoff[pos] + lane;
-    if (e < eoff[pos + 1]) {
-        const int nb = (kForward ? g.fwd_enb : g.bwd_enb)[e];
-        const int fs = (kForward ? g.fwd_ef : g.bwd_ef)[e];
-        const int ec = (kForward ? g.fwd_ec : g.bwd_ec)[e];
-        const int f = fs & 0x7fffffff;
-        const T sgn = fs < 0 ? T(-1) : T(1);
-        double fr[4];
-        ld4(g.frec + (size_t)f * kF, fr);
-        T cf[4];
-        ld4(w.coef + (size_t)ec * kCoef, cf);
-        T qn[8];
-        ld8(w.qrec + (size_t)nb * kQ, qn);
-        s.nb = nb;
-        s.nx = sgn * (T)fr[0];
-        s.ny = sgn * (T)fr[1];
-        s.nz = sgn * (T)fr[2];
-        s.area = (T)fr[3];
-        s.l1 = cf[0]; s.x1 = cf[1]; s.x2 = cf[2];
-        s.um = qn[1]; s.vm = qn[2]; s.wm = qn[3]; s.c2 = qn[5]; s.hm = qn[6];
-    }
-    if (lane == 0) {
-        T cr[8];
-        ld8cg(w.crec + (size_t)cell * kC, cr);
-        s.diag = cr[5];
-        if (kForward) {
-#pragma unroll
-            for (int k = 0; k < 5; ++k) s.r[k] = cr[k] - T(0);
-        } else {
-            T df[8];
-            ld8cg(w.dflux + (size_t)cell * kD, df);
-#pragma unroll
-            for (int k = 0; k < 5; ++k) s.r[k] = cr[k] - df[k];
-        }
-    }
-}
-
-template <class T, bool kForward>
-__device__ __forceinline__ void process_slot(const NsConst &c, const Work<T> &w, const Slot<T> &s, int lane)
-{
-    const unsigned full = 0xffffffffu;
-    T df[5] = {0, 0, 0, 0, 0};
-    const bool active = s.cell >= 0 && s.nb >= 0;
-    if (active) {
-        T dq[8];
-        ld8cg(w.dqrec + (size_t)s.nb * kD, dq);
-        const T gm = (T)c.gama;
-        const T cits = s.nx * s.um + s.ny * s.vm + s.nz * s.wm;
-        const T dc = cits * dq[0] - s.nx * dq[1] - s.ny * dq[2] - s.nz * dq[3];
-        const T c2dc = s.c2 * dc;
-        const T v2 = s.um * s.um + s.vm * s.vm + s.wm * s.wm;
-        const T g1 = gm - T(1);
-        T dh = -g1 * (s.um * dq[1] + s.vm * dq[2] + s.wm * dq[3] - dq[4]);
-        dh += T(0.5) * g1 * v2 * dq[0];
-        const T a = dh * s.x1 + dc * s.x2;
-        const T b = c2dc * s.x1 + dh * s.x2;
-        df[0] = (s.l1 * dq[0] - a) * s.area;
-        df[1] = (s.l1 * dq[1] - s.um * a + s.nx * b) * s.area;
-        df[2] = (s.l1 * dq[2] - s.vm * a + s.ny * b) * s.area;
-        df[3] = (s.l1 * dq[3] - s.wm * a + s.nz * b) * s.area;
-        df[4] = (s.l1 * dq[4] - s.hm * a + cits * b) * s.area;
-    }
-    // In-order accumulation on lane 0 of the group: entries are compact and in
-    // face order (active lanes are 0..n-1); the trip count is the warp maximum
-    // so the shuffles stay warp-uniform.
-    const unsigned act = __ballot_sync(full, active);
-    const int base = (threadIdx.x & 31) & ~(kGroup - 1);
-    const int ncnt = __popc((act >> base) & ((1u << kGroup) - 1u));
-    const int wmax = (int)__reduce_max_sync(full, (unsigned)ncnt);
-    T rhs0[5] = {0, 0, 0, 0, 0};
-    for (int k = 0; k < wmax; ++k) {
-        T v[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) v[m] = __shfl_sync(full, df[m], base + k);
-        if (k < ncnt) {
-#pragma unroll
-            for (int m = 0; m < 5; ++m) rhs0[m] += v[m];
-        }
-    }
-    if (lane == 0 && s.cell >= 0) {
-        T o[8];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) o[k] = (s.r[k] - rhs0[k]) / s.diag;
-        o[5] = o[6] = o[7] = T(0);
-        st8(w.dqrec + (size_t)s.cell * kD, o);
-        if (kForward) {
-            T d[8];
-#pragma unroll
-            for (int k = 0; k < 5; ++k) d[k] = T(0) + rhs0[k];
-            d[5] = d[6] = d[7] = T(0);
-            st8(w.dflux + (size_t)s.cell * kD, d);
-        }
-    }
-}
-
-template <class T, bool kForward>
-__device__ __forceinline__ bool run_sweep(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
-                                          unsigned &target, int group, int ngroups, int lane)
-{
-    const int nlev = kForward ? g.nFwdLevels : g.nBwdLevels;
-    const int *off = kForward ? g.fwd_off : g.bwd_off;
-    const int warpGroup0 = group - ((threadIdx.x & 31) / kGroup);
-    Slot<T> cur, nxt;
-    load_slot<T, kForward>(g, w, off[1], off[0] + group, lane, cur);
-    for (int L = 0; L < nlev; ++L) {
-        const int b = off[L], e = off[L + 1];
-        if (L + 1 < nlev) load_slot<T, kForward>(g, w, off[L + 2], off[L + 1] + group, lane, nxt);
-        process_slot<T, kForward>(c, w, cur, lane);
-        // Levels wider than the grid: further rounds with a warp-uniform trip
-        // count (process_slot uses full-warp collectives).
-        for (int round = b + ngroups; round + warpGroup0 < e; round += ngroups) {
-            Slot<T> extra;
-            load_slot<T, kForward>(g, w, e, round + group, lane, extra);
-            process_slot<T, kForward>(c, w, extra, lane);
-        }
-        if (!grid_sync(red, target, gridDim.x)) return false;
-        cur = nxt;
-    }
-    return true;
-}
-
-template <class T>
-__global__ void __launch_bounds__(kSweepThreads, 1) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+__device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
+                                               int *flagF, int *flagB, int epoch, double mindt, int pos, int lane,
+                                               unsigned gmask, int base)
 {
     const int nc = g.nCell;
-    const int stride = gridDim.x * blockDim.x;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int group = tid / kGroup, lane = tid % kGroup, ngroups = stride / kGroup;
-    unsigned int target = 0;
-    const double mindt = __longlong_as_double((long long)red->mindt_bits);
-    // Diagonal (NSSolverUnstruct.cpp:15867-15935): D = vol / dt' + spectral
-    // radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep, :5717-5745);
-    // single sweep: dq starts from res and the carried delta flux from zero
-    // (LUSGSInitialization, Controller.cpp:1765-1777).
-    for (int cell = tid; cell < nc; cell += stride) {
-        T dt = w.dtraw[cell];
+    const int cell = (kForward ? g.fwd_cells : g.bwd_cells)[pos];
+    const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
+    const int e0 = eoff[pos], e1 = eoff[pos + 1];
+    const int e = e0 + lane;
+    const bool has = e < e1;
+    // dq-independent loads first: they overlap the waits below
+    int nb = -1, f = 0;
+    T sgn = T(1), nx = 0, ny = 0, nz = 0, area = 0, cf[4] = {0, 0, 0, 0}, qn[8];
+    if (has) {
+        nb = (kForward ? g.fwd_enb : g.bwd_enb)[e];
+        const int fs = (kForward ? g.fwd_ef : g.bwd_ef)[e];
+        const int ec = (kForward ? g.fwd_ec : g.bwd_ec)[e];
+        f = fs & 0x7fffffff;
+        sgn = fs < 0 ? T(-1) : T(1);
+        double fr[4];
+        ld4(g.frec + (size_t)f * kF, fr);
+        nx = sgn * (T)fr[0]; ny = sgn * (T)fr[1]; nz = sgn * (T)fr[2]; area = (T)fr[3];
+        ld4(w.coef + (size_t)ec * kCoef, cf);
+        ld8(w.qrec + (size_t)nb * kQ, qn);
+    }
+    T cr[8], dt = T(0);
+    if (lane == 0) {
+        ld8(w.crec + (size_t)cell * kC, cr);
+        dt = w.dtraw[cell];
+    }
+    // wait for the neighbours' dq (a ghost's dq comes from this cell's forward value)
+    bool ok = true;
+    const bool ghost = has && nb >= nc;
+    if (has && !ghost) ok = wait_flag((kForward ? flagF : flagB) + nb, epoch, red);
+    if (!kForward && (lane == 0 || ghost)) ok = wait_flag(flagF + cell, epoch, red) && ok;
+    T df[5] = {0, 0, 0, 0, 0};
+    if (has && ok) {
+        T dq[8];
+        if (ghost) {
+            T dl[8];
+            ld8cg(w.dqrec + (size_t)cell * kD, dl);
+            ghost_dq<T>(g, c, w, nb - nc, dl, dq);
+        } else {
+            ld8cg(w.dqrec + (size_t)nb * kD, dq);
+        }
+        const T gm = (T)c.gama;
+        const T um = qn[1], vm = qn[2], wm = qn[3], c2 = qn[5], hm = qn[6];
+        const T cits = nx * um + ny * vm + nz * wm;
+        const T dc = cits * dq[0] - nx * dq[1] - ny * dq[2] - nz * dq[3];
+        const T c2dc = c2 * dc;
+        const T v2 = um * um + vm * vm + wm * wm;
+        const T g1 = gm - T(1);
+        T dh = -g1 * (um * dq[1] + vm * dq[2] + wm * dq[3] - dq[4]);
+        dh += T(0.5) * g1 * v2 * dq[0];
+        const T a = dh * cf[1] + dc * cf[2];
+        const T b = c2dc * cf[1] + dh * cf[2];
+        df[0] = (cf[0] * dq[0] - a) * area;
+        df[1] = (cf[0] * dq[1] - um * a + nx * b) * area;
+        df[2] = (cf[0] * dq[2] - vm * a + ny * b) * area;
+        df[3] = (cf[0] * dq[3] - wm * a + nz * b) * area;
+        df[4] = (cf[0] * dq[4] - hm * a + cits * b) * area;
+    }
+    // in-order accumulation on lane 0 (entries are in the cell's face order)
+    const int n = e1 - e0;
+    T rhs0[5] = {0, 0, 0, 0, 0};
+    for (int k = 0; k < n; ++k) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) rhs0[m] += __shfl_sync(gmask, df[m], base + k);
+    }
+    const bool allok = __all_sync(gmask, ok);
+    if (lane == 0) {
+        // Diagonal (NSSolverUnstruct.cpp:15867-15935): 1 / (dt' / vol) + spectral
+        // radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep, :5717-5745)
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
         dt /= (T)g.xrec[(size_t)cell * kX + 3];
-        T *cr = w.crec + (size_t)cell * kC;
         T d = T(1) / dt;
         d += cr[6];
         if (c.viscous) d += cr[7];
-        cr[5] = d;
+        T o[8];
+        if (kForward) {
+            // dq = (res - Ux - L dq) / D, Ux = 0 for a single sweep
+            // (LUSGSInitialization, Controller.cpp:1765-1777)
+            T fl[8];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) { o[k] = (cr[k] - T(0) - rhs0[k]) / d; fl[k] = T(0) + rhs0[k]; }
+            o[5] = o[6] = o[7] = T(0);
+            fl[5] = fl[6] = fl[7] = T(0);
+            st8(w.dflux + (size_t)cell * kD, fl);
+        } else {
+            T fl[8];
+            ld8cg(w.dflux + (size_t)cell * kD, fl);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) o[k] = (cr[k] - fl[k] - rhs0[k]) / d;
+            o[5] = o[6] = o[7] = T(0);
+        }
+        st8(w.dqrec + (size_t)cell * kD, o);
+        __threadfence();
+        st_release((kForward ? flagF : flagB) + cell, epoch);
     }
-    if (!grid_sync(red, target, gridDim.x)) return;
-    if (!run_sweep<T, true>(g, c, w, red, target, group, ngroups, lane)) return;
-    for (int f = tid; f < g.nBFace; f += stride) ghost_dq<T>(g, c, w, f);
-    if (!grid_sync(red, target, gridDim.x)) return;
-    run_sweep<T, false>(g, c, w, red, target, group, ngroups, lane);
+    return allok;
 }
 
-static __global__ void reset_barrier_kernel(Reduce *r) { r->barrier = 0u; }
+template <class T>
+__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red,
+                                                              int *flagF, int *flagB, int epoch)
+{
+    const int nc = g.nCell;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int group = tid / kGroup, lane = tid % kGroup;
+    const int ngroups = (gridDim.x * blockDim.x) / kGroup;
+    const int base = (threadIdx.x & 31) & ~(kGroup - 1);
+    const unsigned gmask = ((1u << kGroup) - 1u) << base;
+    const double mindt = __longlong_as_double((long long)red->mindt_bits);
+    for (int pos = group; pos < nc; pos += ngroups)
+        if (!sweep_position<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, pos, lane, gmask, base)) return;
+    for (int pos = group; pos < nc; pos += ngroups)
+        if (!sweep_position<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, pos, lane, gmask, base)) return;
+}
 
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s)
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int *flagF, int *flagB, int epoch,
+                 int numSMs, cudaStream_t s)
 {
     static int perSMcache[2] = {-1, -1};
     int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
@@ -698,24 +645,24 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kSweepThreads, 0);
         if (perSM < 1) perSM = 1;
     }
-    // one lane group per cell of the widest level, never more blocks than can be co-resident
-    const long long threads = (long long)g.maxLevelWidth * kGroup;
-    int blocks = (int)((threads + kSweepThreads - 1) / kSweepThreads);
-    if (blocks > numSMs * perSM) blocks = numSMs * perSM;
-    // PHX_LUSGS_MAX_BLOCKS caps the sweep grid (tuning, and tests of levels
-    // wider than the grid on small meshes)
+    int blocks = numSMs * perSM;
+    const int need = (int)(((long long)g.nCell * kGroup + kSweepThreads - 1) / kSweepThreads);
+    if (blocks > need) blocks = need;
+    // PHX_LUSGS_MAX_BLOCKS caps the grid (tuning; tests of many positions per group)
     if (const char *cap = getenv("PHX_LUSGS_MAX_BLOCKS")) {
         const int v = atoi(cap);
         if (v > 0 && blocks > v) blocks = v;
     }
     if (blocks < 1) blocks = 1;
-    reset_barrier_kernel<<<1, 1, 0, s>>>(red);
     DevGrid gg = g;
     NsConst cc = c;
     Work<T> ww = w;
     Reduce *rr = red;
-    void *args[] = {&gg, &cc, &ww, &rr};
-    cudaError_t e = cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
+    int *ff = flagF, *fb = flagB;
+    int ep = epoch;
+    void *args[] = {&gg, &cc, &ww, &rr, &ff, &fb, &ep};
+    const cudaError_t e =
+        cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
 }
 
@@ -921,7 +868,8 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
     template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);      \
     template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,           \
                                      cudaStream_t);                                                                 \
-    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t);   \
+    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int *, int *, int,    \
+                                 int, cudaStream_t);                                                                \
     template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \
                                    Reduce *, int *, cudaStream_t);                                                  \
     template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *,         \
