@@ -29,7 +29,8 @@ class _Grid(C.Structure):
 class _Metrics(C.Structure):
     _fields_ = [("xfn", _dp), ("yfn", _dp), ("zfn", _dp), ("area", _dp), ("xfc", _dp), ("yfc", _dp),
                 ("zfc", _dp), ("xcc", _dp), ("ycc", _dp), ("zcc", _dp), ("vol", _dp), ("skew", _dp),
-                ("walldist", _dp), ("avg_vol", C.c_double), ("c2f_off", _ip), ("c2f", _ip)]
+                ("walldist", _dp), ("avg_vol", C.c_double), ("c2f_off", _ip), ("c2f", _ip),
+                ("iwt", _dp), ("ixx", _dp), ("iyy", _dp), ("izz", _dp), ("ixy", _dp), ("ixz", _dp), ("iyz", _dp)]
 
 
 class _Params(C.Structure):
@@ -177,6 +178,10 @@ class Oracle:
             setattr(m, k, _p(v))
         m.walldist = _dp()
         m.c2f_off, m.c2f = _p(self.c2f_off, _ip), _p(self.c2f, _ip)
+        self.lsq = {"iwt": np.zeros(nf)}
+        self.lsq.update({k: np.zeros(nc) for k in ("ixx", "iyy", "izz", "ixy", "ixz", "iyz")})
+        for k, v in self.lsq.items():
+            setattr(m, k, _p(v))
         lib().ox_compute_metrics(C.byref(g), C.byref(m))
         self.m = m
         self.params = dict(params)

@@ -183,11 +183,54 @@ static void skewness(const ox_grid *g, ox_metrics *m)
     }
 }
 
+/* UnstructGrid::ComputeWeight, Geo_UnstructGrid.cpp:3761-3935 (3-D, every
+ * face mark 1): per face the inverse squared centre distance, per cell the
+ * inverse of sum_f w d d^T (zeroed when its determinant is below SMALL).
+ * Boundary faces use the ghost centre. */
+static void lsq_weights(const ox_grid *g, ox_metrics *m)
+{
+    int nc = g->n_cell, nb = g->n_bface;
+    for (int c = 0; c < nc; ++c) m->ixx[c] = m->iyy[c] = m->izz[c] = m->ixy[c] = m->ixz[c] = m->iyz[c] = 0.0;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double dx = (m->xcc[re] - m->xcc[le]) * 1.0;
+        double dy = (m->ycc[re] - m->ycc[le]) * 1.0;
+        double dz = (m->zcc[re] - m->zcc[le]) * 1.0;
+        double ods = 1.0 / (dx * dx + dy * dy + dz * dz + OX_SMALL);
+        double txx = ods * dx * dx, tyy = ods * dy * dy, tzz = ods * dz * dz;
+        double txy = ods * dx * dy, txz = ods * dx * dz, tyz = ods * dy * dz;
+        m->iwt[f] = ods;
+        m->ixx[le] += txx; m->iyy[le] += tyy; m->izz[le] += tzz;
+        m->ixy[le] += txy; m->ixz[le] += txz; m->iyz[le] += tyz;
+        if (f >= nb) {
+            m->ixx[re] += txx; m->iyy[re] += tyy; m->izz[re] += tzz;
+            m->ixy[re] += txy; m->ixz[re] += txz; m->iyz[re] += tyz;
+        }
+    }
+    for (int c = 0; c < nc; ++c) {
+        double txx = m->ixx[c], tyy = m->iyy[c], tzz = m->izz[c];
+        double txy = m->ixy[c], txz = m->ixz[c], tyz = m->iyz[c];
+        double delt = (txx * tyy * tzz + 2.0 * txy * txz * tyz - txx * tyz * tyz - tyy * txz * txz - tzz * txy * txy);
+        if (fabs(delt) < OX_SMALL) {
+            m->ixx[c] = m->iyy[c] = m->izz[c] = m->ixy[c] = m->ixz[c] = m->iyz[c] = 0.0;
+        } else {
+            double od = 1.0 / delt;
+            m->ixx[c] = (tyy * tzz - tyz * tyz) * od;
+            m->iyy[c] = (txx * tzz - txz * txz) * od;
+            m->izz[c] = (txx * tyy - txy * txy) * od;
+            m->ixy[c] = (txz * tyz - txy * tzz) * od;
+            m->ixz[c] = (txy * tyz - txz * tyy) * od;
+            m->iyz[c] = (txy * txz - tyz * txx) * od;
+        }
+    }
+}
+
 void ox_compute_metrics(const ox_grid *g, ox_metrics *m)
 {
     face_metrics(g, m);
     cell_metrics(g, m);
     skewness(g, m);
+    if (m->iwt) lsq_weights(g, m);
     double s = 0.0;
     for (int c = 0; c < g->n_cell; ++c) s += m->vol[c];
     m->avg_vol = s / (double)g->n_cell;
@@ -341,11 +384,39 @@ static void gradient_ggcell(const ox_grid *g, const ox_metrics *m, const double 
     }
 }
 
+/* UnstructGrid::CompGradientLSQ, Geo_UnstructGrid.cpp:3996-4085: weighted
+ * differences to face neighbours (ghosts for boundary faces) times the
+ * cell's inverse normal matrix; ghost gradients copy the owner's. */
+static void gradient_lsq(const ox_grid *g, const ox_metrics *m, const double *q, double *dx, double *dy,
+                         double *dz)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int c = 0; c < nt; ++c) dx[c] = dy[c] = dz[c] = 0.0;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double ddx = m->xcc[re] - m->xcc[le], ddy = m->ycc[re] - m->ycc[le], ddz = m->zcc[re] - m->zcc[le];
+        double dq = m->iwt[f] * (q[re] - q[le]) * 1.0;
+        double tx = dq * ddx, ty = dq * ddy, tz = dq * ddz;
+        dx[le] += tx; dy[le] += ty; dz[le] += tz;
+        if (f >= nb) { dx[re] += tx; dy[re] += ty; dz[re] += tz; }
+    }
+    for (int c = 0; c < nc; ++c) {
+        double tx = dx[c], ty = dy[c], tz = dz[c];
+        dx[c] = m->ixx[c] * tx + m->ixy[c] * ty + m->ixz[c] * tz;
+        dy[c] = m->ixy[c] * tx + m->iyy[c] * ty + m->iyz[c] * tz;
+        dz[c] = m->ixz[c] * tx + m->iyz[c] * ty + m->izz[c] * tz;
+    }
+    for (int f = 0; f < nb; ++f) {
+        int le = g->left[f], re = nc + f;
+        dx[re] = dx[le]; dy[re] = dy[le]; dz[re] = dz[le];
+    }
+}
+
 void ox_gradient(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *f,
                  double *dfdx, double *dfdy, double *dfdz)
 {
-    (void)p;
-    gradient_ggcell(g, m, f, dfdx, dfdy, dfdz);
+    if (p->gradient == 1) gradient_lsq(g, m, f, dfdx, dfdy, dfdz);
+    else gradient_ggcell(g, m, f, dfdx, dfdy, dfdz);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -547,6 +618,144 @@ void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Viscous terms                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* ComputeViscousCoefficientWithoutChemical, NSSolverUnstruct.cpp:6722-6747
+ * (Sutherland, every cell and ghost); laminar runs have zero eddy viscosity. */
+void ox_viscosity(const ox_grid *g, const ox_params *p, const double *t, double *visl, double *vist)
+{
+    int nt = ntot(g);
+    double s = p->tsuth_nd;
+    for (int c = 0; c < nt; ++c) {
+        visl[c] = t[c] * sqrt(t[c]) * (1.0 + s) / (t[c] + s);
+        if (p->viscous == 1) vist[c] = 0.0;
+    }
+}
+
+/* NSSolverUnstruct::ViscousFlux (7058-7110) per face, in face order:
+ * UnstructGrid::FaceWeight (Geo_UnstructGrid.cpp:2420-2478), GetVisFaceValue
+ * (NSSolverUnstruct.cpp:7126-7375; static adiabatic walls), ComputeVisflux
+ * (12977-13378; perfect gas, no Reynolds-stress model), LoadFlux.  res is
+ * accumulated after the inviscid flux. */
+void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *t,
+                     const double *visl, const double *vist, const double *dqdx, const double *dqdy,
+                     const double *dqdz, const double *dtdx, const double *dtdy, const double *dtdz, double *res)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    double ore = 1.0 / p->reynolds;
+    double oprl = 1.0 / p->prandtl, oprt = 1.0 / p->prandtl_turb;
+    double cp = 1.0 / ((p->gama - 1.0) * (p->mach * p->mach));
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        int bt = f < nb ? g->region_type[g->bface_region[f]] : 0;
+        int wall = f < nb && is_wall(bt);
+        /* FaceWeight */
+        double dxl = m->xfc[f] - m->xcc[le], dyl = m->yfc[f] - m->ycc[le], dzl = m->zfc[f] - m->zcc[le];
+        double dxr = m->xfc[f] - m->xcc[re], dyr = m->yfc[f] - m->ycc[re], dzr = m->zfc[f] - m->zcc[re];
+        double d1 = sqrt(dxl * dxl + dyl * dyl + dzl * dzl), d2 = sqrt(dxr * dxr + dyr * dyr + dzr * dzr);
+        double dlt = 1.0 / (d1 + d2 + OX_SMALL);
+        double dwl = d2 * dlt, dwr = d1 * dlt;
+        if (f < nb) { dwl = 1.0; dwr = 0.0; }
+        /* GetVisFaceValue */
+        double mul = 0.5 * (visl[le] + visl[re]);
+        double mut = 0.5 * (vist[le] + vist[re]);
+        double pf[5];
+        for (int k = 0; k < 5; ++k) pf[k] = 0.5 * (q[k * nt + le] + q[k * nt + re]);
+        double tmf = 0.5 * (t[le] + t[re]);
+        double kcp = (mul * oprl + mut * oprt) * cp;
+        if (wall) pf[1] = pf[2] = pf[3] = 0.0;
+        /* ComputeVisflux */
+        double nxs = m->xfn[f], nys = m->yfn[f], nzs = m->zfn[f];
+        double t1x, t1y, t1z;
+        if (fabs(nxs) > OX_SMALL) { t1x = nys; t1y = -nxs; t1z = 0.0; }
+        else if (fabs(nys) > OX_SMALL) { t1x = -nys; t1y = nxs; t1z = 0.0; }
+        else if (fabs(nzs) > OX_SMALL) { t1x = 0.0; t1y = -nzs; t1z = nys; }
+        else continue;  /* zero flux */
+        double on = 1.0 / sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+        t1x *= on; t1y *= on; t1z *= on;
+        double t2x = nys * t1z - nzs * t1y, t2y = nzs * t1x - nxs * t1z, t2z = nxs * t1y - nys * t1x;
+        double dxL = m->xcc[le] - m->xfc[f], dyL = m->ycc[le] - m->yfc[f], dzL = m->zcc[le] - m->zfc[f];
+        double dxR = m->xcc[re] - m->xfc[f], dyR = m->ycc[re] - m->yfc[f], dzR = m->zcc[re] - m->zfc[f];
+        double dL = nxs * dxL + nys * dyL + nzs * dzL;
+        double dR = nxs * dxR + nys * dyR + nzs * dzR;
+        double tmp = -dL / (sqrt(dxL * dxL + dyL * dyL + dzL * dzL) + OX_SMALL);
+        tmp = omin(tmp, 1.0); tmp = omax(tmp, -1.0);
+        double a1 = asin(tmp) * 180.0 / OX_PI;
+        tmp = dR / (sqrt(dxR * dxR + dyR * dyR + dzR * dzR) + OX_SMALL);
+        tmp = omin(tmp, 1.0); tmp = omax(tmp, -1.0);
+        double a2 = asin(tmp) * 180.0 / OX_PI;
+        double dxnL = nxs * dL - dxL, dynL = nys * dL - dyL, dznL = nzs * dL - dzL;
+        double dxnR = nxs * dR - dxR, dynR = nys * dR - dyR, dznR = nzs * dR - dzR;
+        double f1[5], f2[5], fm[5];
+        for (int k = 0; k < 5; ++k) { f1[k] = q[k * nt + le]; f2[k] = q[k * nt + re]; }
+        double tL = t[le], tR = t[re];
+        for (int k = 0; k < 5; ++k) fm[k] = 0.5 * (f1[k] + f2[k]);
+        double tM = 0.5 * (tL + tR);
+        if (wall) {
+            tM = tmf;
+            fm[0] = fm[4] / (p->coef_state * tM);
+        }
+        if (a1 > p->skewness_angle && a2 > p->skewness_angle) {
+            for (int k = 0; k < 5; ++k) {
+                f1[k] += dqdx[k * nt + le] * dxnL + dqdy[k * nt + le] * dynL + dqdz[k * nt + le] * dznL;
+                f2[k] += dqdx[k * nt + re] * dxnR + dqdy[k * nt + re] * dynR + dqdz[k * nt + re] * dznR;
+            }
+            tL += dtdx[le] * dxnL + dtdy[le] * dynL + dtdz[le] * dznL;
+            tR += dtdx[re] * dxnR + dtdy[re] * dynR + dtdz[re] * dznR;
+            if (tL < OX_SMALL) tL = t[le];
+            if (tR < OX_SMALL) tR = t[re];
+            for (int k = 0; k < 5; ++k) fm[k] = pf[k];
+            tM = tmf;
+        }
+        double dfdn[5] = {0, 0, 0, 0, 0}, dtdn = 0.0;
+        if (a1 > 0.0 && a2 > 0.0 && fabs(dL) > OX_TINY && fabs(dR) > OX_TINY) {
+            double dtmp = dL * dL + dR * dR;
+            double wL = dL * dL / dtmp;
+            double wR = 1.0 - wL;
+            if (f < nb) { wL = 1.0; wR = 0.0; }
+            for (int k = 0; k < 5; ++k) {
+                double e1 = (f1[k] - fm[k]) / dL, e2 = (f2[k] - fm[k]) / dR;
+                dfdn[k] = wL * e1 + wR * e2;
+            }
+            double dtd1 = (tL - tM) / dL, dtd2 = (tR - tM) / dR;
+            dtdn = dtd1 * wL + dtd2 * wR;
+        }
+        double gx[5], gy[5], gz[5];
+        for (int k = 1; k <= 3; ++k) {
+            double fx = dwl * dqdx[k * nt + le] + dwr * dqdx[k * nt + re];
+            double fy = dwl * dqdy[k * nt + le] + dwr * dqdy[k * nt + re];
+            double fz = dwl * dqdz[k * nt + le] + dwr * dqdz[k * nt + re];
+            double dt1 = t1x * fx + t1y * fy + t1z * fz;
+            double dt2 = t2x * fx + t2y * fy + t2z * fz;
+            gx[k] = nxs * dfdn[k] + t1x * dt1 + t2x * dt2;
+            gy[k] = nys * dfdn[k] + t1y * dt1 + t2y * dt2;
+            gz[k] = nzs * dfdn[k] + t1z * dt1 + t2z * dt2;
+        }
+        double dudx = gx[1], dudy = gy[1], dudz = gz[1];
+        double dvdx = gx[2], dvdy = gy[2], dvdz = gz[2];
+        double dwdx = gx[3], dwdy = gy[3], dwdz = gz[3];
+        double qn = 0.0;
+        qn += kcp * dtdn;
+        double div = (2.0 / 3.0) * (dudx + dvdy + dwdz);
+        double vis = mul + mut;
+        double txx = vis * (2.0 * dudx - div), tyy = vis * (2.0 * dvdy - div), tzz = vis * (2.0 * dwdz - div);
+        double txy = vis * (dudy + dvdx), txz = vis * (dudz + dwdx), tyz = vis * (dvdz + dwdy);
+        double fv[5];
+        fv[0] = 0.0;
+        fv[1] = nxs * txx + nys * txy + nzs * txz;
+        fv[2] = nxs * txy + nys * tyy + nzs * tyz;
+        fv[3] = nxs * txz + nys * tyz + nzs * tzz;
+        fv[4] = fm[1] * fv[1] + fm[2] * fv[2] + fm[3] * fv[3] + qn;
+        for (int k = 0; k < 5; ++k) {
+            double fl = -ore * m->area[f] * fv[k];
+            res[k * nt + le] -= fl;
+            if (f >= nb) res[k * nt + re] += fl;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Spectral radius and time step                                             */
 /* ------------------------------------------------------------------------ */
 
@@ -571,7 +780,20 @@ void ox_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, cons
         inv_spec[le] += s;
         if (re < nc) inv_spec[re] += s;
     }
-    (void)p; (void)visl; (void)vist;
+    if (!p->viscous || !vis_spec) return;
+    /* visSpetrumMethod 2 (5930-5960): 2 mu / (rho |n.dr| Re) * A/2 */
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double dx = m->xcc[re] - m->xcc[le], dy = m->ycc[re] - m->ycc[le], dz = m->zcc[re] - m->zcc[le];
+        double ds = fabs(m->xfn[f] * dx + m->yfn[f] * dy + m->zfn[f] * dz);
+        double mul = 0.5 * (visl[le] + visl[re]);
+        double mut = 0.5 * (vist[le] + vist[re]);
+        double rho = 0.5 * (q[le] + q[re]);
+        double vs = 2.0 * (mul + mut) / (rho * ds * p->reynolds + OX_SMALL);
+        vs *= 0.5 * m->area[f];
+        vis_spec[le] += vs;
+        if (re < nc) vis_spec[re] += vs;
+    }
 }
 
 /* NSSolver::ComputeCFL, CFD/NSSolver/src/NSSolver.cpp:595-668 (cflMethod 0,
@@ -877,11 +1099,16 @@ void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
     ox_gamma_temperature(g, p, q, w->gama, w->t);  /* gama of the ghosts is needed by the far field */
     ox_ns_boundary(g, m, p, q, w->gama);
     ox_gamma_temperature(g, p, q, w->gama, w->t);
+    if (p->viscous) ox_viscosity(g, p, w->t, w->visl, w->vist);
     for (int k = 0; k < 5; ++k)
         ox_gradient(g, m, p, q + (size_t)k * nt, w->dqdx + (size_t)k * nt, w->dqdy + (size_t)k * nt, w->dqdz + (size_t)k * nt);
+    if (p->viscous) ox_gradient(g, m, p, w->t, w->dtdx, w->dtdy, w->dtdz);
     ox_limiter(g, m, p, q, w->dqdx, w->dqdy, w->dqdz, w->limit);
     memset(w->res, 0, sizeof(double) * 5 * nt);
     ox_inviscid_flux(g, m, p, q, w->gama, w->dqdx, w->dqdy, w->dqdz, w->limit, w->res);
+    if (p->viscous)
+        ox_viscous_flux(g, m, p, q, w->t, w->visl, w->vist, w->dqdx, w->dqdy, w->dqdz, w->dtdx, w->dtdy, w->dtdz,
+                        w->res);
     ox_spectrum(g, m, p, q, w->gama, w->visl, w->vist, w->inv_spec, w->vis_spec);
     ox_timestep(g, m, p, step, q, w->inv_spec, w->vis_spec, w->dt);
     ox_lusgs(g, m, p, q, w->gama, w->t, w->visl, w->vist, w->res, w->dt, w->inv_spec, w->vis_spec, w->dq);

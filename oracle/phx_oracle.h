@@ -40,6 +40,10 @@ typedef struct {
     double avg_vol;
     /* cell -> face lists in ascending face order, [n_cell+1] offsets */
     int *c2f_off, *c2f;
+    /* least-squares weights (UnstructGrid::ComputeWeight,
+     * Geo_UnstructGrid.cpp:3761-3935): iwt [n_face], inverse normal matrix
+     * ixx..iyz [n_cell]; filled when non-NULL */
+    double *iwt, *ixx, *iyy, *izz, *ixy, *ixz, *iyz;
 } ox_metrics;
 
 typedef struct {
@@ -115,6 +119,10 @@ void ox_lusgs(const ox_grid *g, const ox_metrics *m, const ox_params *p, const d
 int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double *q, const double *gama,
               const double *dq);
 double ox_residual_norm(const ox_grid *g, const double *res);
+void ox_viscosity(const ox_grid *g, const ox_params *p, const double *t, double *visl, double *vist);
+void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *t,
+                     const double *visl, const double *vist, const double *dqdx, const double *dqdy,
+                     const double *dqdz, const double *dtdx, const double *dtdy, const double *dtdz, double *res);
 
 #ifdef __cplusplus
 }

@@ -30,6 +30,10 @@ EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "v
               "nLUSGSSweeps": 1, "CFLStart": 0.01, "CFLEnd": 10.0, "CFLVaryStep": 500, "refMachNumber": 0.5,
               "attackd": 0.0, "refGama": 1.4}
 
+# Laminar NS: viscous adiabatic walls on the bump, Sutherland viscosity, Re 1e4.
+LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, refDimensionalTemperature=288.15,
+               prl=0.72, wallTemperature=-1.0)
+
 
 def mesh_spec(m, kind, args):
     return {"kind": kind, "args": args}
@@ -43,6 +47,10 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02)
         state = perturbed_state(m, params, seed=perturb_seed, amplitude=amplitude)
     dumps = [("q", 5, nt), ("res", 5, nt), ("dt", 0, nt), ("limit2D", 5, nt), ("gradPrimtiveVarX", 5, nt),
              ("gradPrimtiveVarY", 5, nt), ("gradPrimtiveVarZ", 5, nt), ("invSpectralRadius", 0, nc)]
+    viscous = params.get("viscousType", 0) > 0
+    if viscous:
+        dumps += [("visl", 0, nt), ("visSpectralRadius", 0, nc), ("gradTemperatureX", 1, nt),
+                  ("gradTemperatureY", 1, nt), ("gradTemperatureZ", 1, nt)]
     r = run_reference(m, params, nsteps, dumps=dumps, state=state)
     out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}),
            "nsteps": nsteps, "res_hist": r["res_hist"]}
@@ -51,6 +59,11 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02)
     for k in ("q", "res", "dt", "gradPrimtiveVarX", "gradPrimtiveVarY", "gradPrimtiveVarZ", "invSpectralRadius",
               "xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol"):
         out[k] = r[k]
+    if viscous:
+        for k in ("visl", "visSpectralRadius"):
+            out[k] = r[k]
+        for k in ("gradTemperatureX", "gradTemperatureY", "gradTemperatureZ"):
+            out[k] = r[k].reshape(-1)[:nt]
     out["limit"] = r["limit2D"][0]
     path = os.path.join(OUT, name + ".npz")
     np.savez_compressed(path, **out)
@@ -58,6 +71,13 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02)
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]
+    if only:
+        _fixture = fixture
+
+        def fixture(name, *a, **k):  # noqa: F811 - regenerate the named fixtures only
+            if name in only:
+                _fixture(name, *a, **k)
     # Euler bump, seeded perturbation, one iteration: every intermediate array.
     fixture("euler_bump_16x8x2_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, EULER_BUMP, 1, perturb_seed=7)
     # Euler bump from the free stream, 40 iterations through the CFL ramp.
@@ -65,3 +85,11 @@ if __name__ == "__main__":
     # Euler on a jittered tetrahedral cube (all far field), perturbed, 3 iterations.
     fixture("euler_tetcube_4_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
             dict(EULER_BUMP, refMachNumber=0.3), 3, perturb_seed=11)
+    # Laminar bump (no-slip adiabatic walls), LSQ gradient, perturbed, one iteration.
+    fixture("laminar_bump_16x8x2_lsq_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(LAMINAR, gradientName="lsq"), 1, perturb_seed=7)
+    # Laminar bump, GG-cell gradient, 20 iterations from the free stream.
+    fixture("laminar_bump_16x8x2_step20", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, LAMINAR, 20)
+    # Laminar jittered tetrahedra (config-2 element type), LSQ, perturbed, 3 iterations.
+    fixture("laminar_tetcube_4_lsq_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
+            dict(LAMINAR, gradientName="lsq"), 3, perturb_seed=11)

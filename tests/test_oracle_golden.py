@@ -30,6 +30,29 @@ def test_oracle_matches_reference(golden, name):
     assert rel_err(o.work("inv_spec"), d["invSpectralRadius"]) <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["laminar_bump_16x8x2_lsq_step1", "laminar_bump_16x8x2_step20",
+                                  "laminar_tetcube_4_lsq_step3"])
+def test_oracle_matches_reference_laminar(golden, name):
+    """Laminar NS: Sutherland viscosity, temperature gradient, viscous flux and
+    spectral radius, no-slip adiabatic walls, GG-cell and LSQ gradients."""
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    o = Oracle(m, d["params_dict"])
+    if "state_in" in d:
+        o.set_state(d["state_in"][:, :nc])
+    hist = o.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(o.q[:, :nc], d["q"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("res")[:, :nc], d["res"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dt")[:nc], d["dt"][:nc]) <= 1e-12
+    assert rel_err(o.work("visl")[:nc], d["visl"][:nc]) <= 1e-12
+    assert rel_err(o.work("vis_spec"), d["visSpectralRadius"]) <= 1e-12
+    assert rel_err(o.work("dqdy")[:, :nc], d["gradPrimtiveVarY"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dtdx")[:nc], d["gradTemperatureX"][:nc]) <= 1e-12
+    assert rel_err(o.work("dtdz")[:nc], d["gradTemperatureZ"][:nc]) <= 1e-12
+
+
 def test_oracle_detects_planted_error(golden):
     """A mistake planted in the oracle's input shows up in the comparison."""
     d = golden("euler_bump_16x8x2_step1")
