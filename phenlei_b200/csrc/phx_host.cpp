@@ -495,11 +495,14 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         lev[c] = l;
         nfl = std::max(nfl, l + 1);
     }
+    // Each level is padded with idle positions (-1) to a multiple of
+    // kSweepPad, the lane groups of one warp, so that the positions one warp
+    // takes together always lie in one level and never depend on each other.
     auto bucket = [&](int nlev, std::vector<int> &cells, std::vector<int> &off, bool ascending) {
         off.assign(nlev + 1, 0);
         for (int c = 0; c < nc; ++c) off[lev[c] + 1]++;
-        for (int l = 0; l < nlev; ++l) off[l + 1] += off[l];
-        cells.resize(nc);
+        for (int l = 0; l < nlev; ++l) off[l + 1] = off[l] + (off[l + 1] + kSweepPad - 1) / kSweepPad * kSweepPad;
+        cells.assign(off[nlev], -1);
         std::vector<int> fill(off.begin(), off.end() - 1);
         if (ascending) for (int c = 0; c < nc; ++c) cells[fill[lev[c]]++] = c;
         else for (int c = nc - 1; c >= 0; --c) cells[fill[lev[c]]++] = c;
@@ -527,10 +530,12 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     // sweep entry tables (storage indices), in schedule order and the cell's face order
     auto entries = [&](std::vector<int> &cells, bool forward, std::vector<int> &eoff, std::vector<int> &enb,
                        std::vector<int> &ef, std::vector<int> &ec) {
-        eoff.assign(nc + 1, 0);
+        const int npos = (int)cells.size();
+        eoff.assign(npos + 1, 0);
         enb.clear(); ef.clear(); ec.clear();
-        for (int i = 0; i < nc; ++i) {
+        for (int i = 0; i < npos; ++i) {
             const int c = cells[i];
+            if (c < 0) { eoff[i + 1] = eoff[i]; continue; }
             for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
                 const int f = c2f[j];
                 int nbr = -1;
@@ -628,6 +633,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     g.nCell = nc; g.nBFace = nb; g.nFace = nf; g.nTotal = nt;
     g.avgVol = avgVol;
     g.nFwdLevels = nfl; g.nBwdLevels = nbl; g.maxLevelWidth = maxw;
+    g.nFwdPos = (int)fwd_cells.size(); g.nBwdPos = (int)bwd_cells.size();
     g.walldist = nullptr;
     int rc = 0;
     rc |= upload(ctx, &g.lr, lr);
@@ -878,10 +884,10 @@ int phx_ns_update(phx_ctx *ctx)
     const int nxt = 1 - ctx->cur;
     double *qo = ctx->q64[ctx->cur], *qn = ctx->q64[nxt];
     if (ctx->mixed) {
-        launch_update<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->red, ctx->neglist, ctx->stream);
+        launch_update<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->red, ctx->neglist, ctx->numSMs, ctx->stream);
         launch_solution_fix<float>(ctx->g, ctx->nc, ctx->w32, qo, qn, ctx->red, ctx->neglist, ctx->stream);
     } else {
-        launch_update<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->stream);
+        launch_update<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->numSMs, ctx->stream);
         launch_solution_fix<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->stream);
     }
     ctx->cur = nxt;
@@ -920,7 +926,7 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
     if (res_hist && nsteps > 0)
         PHX_CUDA(ctx, cudaMemcpyAsync(res_hist, ctx->hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
     PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS level barrier timed out");
+    if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
     if (red.error == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
     return PHX_OK;
 }

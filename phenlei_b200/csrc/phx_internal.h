@@ -42,6 +42,7 @@ constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | pad
 constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
 constexpr int kFlux = 8;   // face flux record: F0..4 (times area) | inviscid spectral part | pad
 constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | pad
+constexpr int kSweepPad = 4; // LU-SGS lane groups per warp: schedule levels are padded to this multiple
 
 // Read-only device grid (FP64 metrics, connectivity, schedules), storage order.
 struct DevGrid {
@@ -64,6 +65,7 @@ struct DevGrid {
     const int *fwd_cells, *fwd_off, *fwd_eoff, *fwd_enb, *fwd_ef, *fwd_ec;
     const int *bwd_cells, *bwd_off, *bwd_eoff, *bwd_enb, *bwd_ef, *bwd_ec;
     int nFwdLevels, nBwdLevels;
+    int nFwdPos, nBwdPos;        // schedule positions incl. idle padding (-1 cells)
     int maxLevelWidth;           // widest LU-SGS level (cells)
     double avgVol;
 };
@@ -119,7 +121,7 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
                  int numSMs, cudaStream_t s);
 template <class T>
 void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
-                   Reduce *red, int *neglist, cudaStream_t s);
+                   Reduce *red, int *neglist, int numSMs, cudaStream_t s);
 template <class T>
 void launch_solution_fix(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                          Reduce *red, int *neglist, cudaStream_t s);

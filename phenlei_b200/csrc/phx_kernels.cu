@@ -418,8 +418,18 @@ __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsCo
         w.dtraw[cell] = dt;
         mydt = (double)dt;
     }
+    // block minimum, then one atomic per block, skipped when it cannot lower
+    // the running minimum (positive doubles order like their bit patterns)
     for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
-    if ((threadIdx.x & 31) == 0 && mydt < kLarge) atomic_min_pos_double(&red->mindt_bits, mydt);
+    __shared__ double wmin[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = mydt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = wmin[0];
+        for (int i = 1; i < kThreads / 32; ++i) m = fmin(m, wmin[i]);
+        const unsigned long long cur = *(volatile unsigned long long *)&red->mindt_bits;
+        if (m < kLarge && (unsigned long long)__double_as_longlong(m) < cur) atomic_min_pos_double(&red->mindt_bits, m);
+    }
 }
 
 template <class T>
@@ -438,15 +448,19 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 // its dq; a cell waits only on the flags of the neighbours it reads, so it
 // sees exactly the values the sequential sweep of the reference sees, with
 // no device-wide barrier.  Lane groups (one per cell) take schedule
-// positions in level order (forward positions, then backward positions);
-// a group only waits on cells of earlier positions, and all groups are
-// co-resident (cooperative launch), so the wait graph cannot cycle.  Every
+// positions in level order (forward positions, then backward positions),
+// the four groups of a warp four consecutive positions of one level (levels
+// are padded to multiples of four), so a warp only waits on cells of earlier
+// levels, held by other warps or by its own earlier rounds.  All warps are
+// co-resident (cooperative launch), so the wait graph cannot cycle: the warp
+// holding the lowest unfinished position always has its inputs.  Every
 // wait is bounded: a timeout sets Reduce::error and the kernel gives up.
 // The dq-independent MXDQ_STD factors were computed by the residual pass.
 // ---------------------------------------------------------------------------
 static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
 static constexpr int kSweepThreads = 256;
 static constexpr int kGroup = 8;                      // lanes per cell
+static_assert(kGroup * kSweepPad == 32, "one warp holds kSweepPad lane groups");
 
 __device__ __forceinline__ int ld_acquire(const int *p)
 {
@@ -458,21 +472,6 @@ __device__ __forceinline__ int ld_acquire(const int *p)
 __device__ __forceinline__ void st_release(int *p, int v)
 {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Bounded wait for flag == epoch; false on timeout (sets the error flag).
-__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, Reduce *red)
-{
-    if (ld_acquire(flag) == epoch) return true;
-    long long spins = 0;
-    while (ld_acquire(flag) != epoch) {
-        __nanosleep(32);
-        if (++spins > kSpinLimit || ((volatile int *)&red->error)[0] != 0) {
-            atomicExch(&red->error, PHX_ERR_TIMEOUT);
-            return false;
-        }
-    }
-    return true;
 }
 
 // Ghost-cell dq of boundary face f from the owner's forward dq
@@ -514,18 +513,28 @@ __device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, con
     }
 }
 
-// One schedule position of a sweep, processed by a lane group.
+// One schedule position of a sweep, processed by a lane group of kGroup
+// lanes (one lane per neighbour entry).  The four groups of a warp run in
+// lockstep: the warp polls until every lane's flags are set, so no group ever
+// spins while a sibling in the same warp is ready to work, and every shuffle
+// uses the full warp mask.  pos >= nCell marks an idle group (the warp's trip
+// count is uniform).
 template <class T, bool kForward>
 __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
                                                int *flagF, int *flagB, int epoch, double mindt, int pos, int lane,
-                                               unsigned gmask, int base)
+                                               int base)
 {
     const int nc = g.nCell;
-    const int cell = (kForward ? g.fwd_cells : g.bwd_cells)[pos];
-    const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
-    const int e0 = eoff[pos], e1 = eoff[pos + 1];
+    int cell = -1, e0 = 0, e1 = 0;
+    if (pos < (kForward ? g.nFwdPos : g.nBwdPos)) {
+        cell = (kForward ? g.fwd_cells : g.bwd_cells)[pos];
+        const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
+        e0 = eoff[pos];
+        e1 = eoff[pos + 1];
+    }
+    const bool live = cell >= 0;
     const int e = e0 + lane;
-    const bool has = e < e1;
+    const bool has = live && e < e1;
     // dq-independent loads first: they overlap the waits below
     int nb = -1, f = 0;
     T sgn = T(1), nx = 0, ny = 0, nz = 0, area = 0, cf[4] = {0, 0, 0, 0}, qn[8];
@@ -542,17 +551,28 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         ld8(w.qrec + (size_t)nb * kQ, qn);
     }
     T cr[8], dt = T(0);
-    if (lane == 0) {
+    if (live && lane == 0) {
         ld8(w.crec + (size_t)cell * kC, cr);
         dt = w.dtraw[cell];
     }
     // wait for the neighbours' dq (a ghost's dq comes from this cell's forward value)
-    bool ok = true;
     const bool ghost = has && nb >= nc;
-    if (has && !ghost) ok = wait_flag((kForward ? flagF : flagB) + nb, epoch, red);
-    if (!kForward && (lane == 0 || ghost)) ok = wait_flag(flagF + cell, epoch, red) && ok;
+    const int *w1 = (has && !ghost) ? (kForward ? flagF : flagB) + nb : nullptr;
+    const int *w2 = (!kForward && live && (lane == 0 || ghost)) ? flagF + cell : nullptr;
+    bool ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+    long long spins = 0;
+    while (!__all_sync(0xffffffffu, ready)) {
+        ++spins;
+        if (spins > kSpinLimit) {
+            if ((threadIdx.x & 31) == 0) atomicExch(&red->error, PHX_ERR_TIMEOUT);
+            return false;
+        }
+        if ((spins & 1023) == 0 && __any_sync(0xffffffffu, ((volatile int *)&red->error)[0] != 0)) return false;
+        if (spins > 8) __nanosleep(20);
+        if (!ready) ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+    }
     T df[5] = {0, 0, 0, 0, 0};
-    if (has && ok) {
+    if (has) {
         T dq[8];
         if (ghost) {
             T dl[8];
@@ -578,15 +598,18 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         df[3] = (cf[0] * dq[3] - wm * a + nz * b) * area;
         df[4] = (cf[0] * dq[4] - hm * a + cits * b) * area;
     }
-    // in-order accumulation on lane 0 (entries are in the cell's face order)
-    const int n = e1 - e0;
+    // in-order accumulation (entries are in the cell's face order; lanes
+    // past the cell's entry count contribute exact zeros)
     T rhs0[5] = {0, 0, 0, 0, 0};
-    for (int k = 0; k < n; ++k) {
 #pragma unroll
-        for (int m = 0; m < 5; ++m) rhs0[m] += __shfl_sync(gmask, df[m], base + k);
+    for (int k = 0; k < kGroup; ++k) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            const T v = __shfl_sync(0xffffffffu, df[m], base + k);
+            if (k < e1 - e0) rhs0[m] += v;
+        }
     }
-    const bool allok = __all_sync(gmask, ok);
-    if (lane == 0) {
+    if (live && lane == 0) {
         // Diagonal (NSSolverUnstruct.cpp:15867-15935): 1 / (dt' / vol) + spectral
         // radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep, :5717-5745)
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
@@ -612,27 +635,28 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
             o[5] = o[6] = o[7] = T(0);
         }
         st8(w.dqrec + (size_t)cell * kD, o);
-        __threadfence();
+        // release orders this thread's dq / dflux stores before the flag
         st_release((kForward ? flagF : flagB) + cell, epoch);
     }
-    return allok;
+    return true;
 }
 
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red,
                                                               int *flagF, int *flagB, int epoch)
 {
-    const int nc = g.nCell;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kGroup, lane = tid % kGroup;
     const int ngroups = (gridDim.x * blockDim.x) / kGroup;
+    const int wgroup0 = group & ~(32 / kGroup - 1);   // first group of this warp
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
-    const unsigned gmask = ((1u << kGroup) - 1u) << base;
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
-    for (int pos = group; pos < nc; pos += ngroups)
-        if (!sweep_position<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, pos, lane, gmask, base)) return;
-    for (int pos = group; pos < nc; pos += ngroups)
-        if (!sweep_position<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, pos, lane, gmask, base)) return;
+    for (int p0 = wgroup0; p0 < g.nFwdPos; p0 += ngroups)
+        if (!sweep_position<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, p0 + (group - wgroup0), lane, base))
+            return;
+    for (int p0 = wgroup0; p0 < g.nBwdPos; p0 += ngroups)
+        if (!sweep_position<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, p0 + (group - wgroup0), lane, base))
+            return;
 }
 
 template <class T>
@@ -646,7 +670,8 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
         if (perSM < 1) perSM = 1;
     }
     int blocks = numSMs * perSM;
-    const int need = (int)(((long long)g.nCell * kGroup + kSweepThreads - 1) / kSweepThreads);
+    const int npos = g.nFwdPos > g.nBwdPos ? g.nFwdPos : g.nBwdPos;
+    const int need = (int)(((long long)npos * kGroup + kSweepThreads - 1) / kSweepThreads);
     if (blocks > need) blocks = need;
     // PHX_LUSGS_MAX_BLOCKS caps the grid (tuning; tests of many positions per group)
     if (const char *cap = getenv("PHX_LUSGS_MAX_BLOCKS")) {
@@ -682,62 +707,76 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) update_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo,
                                                           double *qn, Reduce *red, int *neglist)
 {
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     const int nt = g.nTotal, nc = g.nCell;
+    const int n = nc > g.nBFace ? nc : g.nBFace;
+    const double gm = c.gama;
     double rs[5] = {0, 0, 0, 0, 0};
-    if (cell < nc) {
-        const double r = qo[cell], u = qo[nt + cell], v = qo[2 * nt + cell], ww = qo[3 * nt + cell], p = qo[4 * nt + cell];
-        const double gm = c.gama;
-        const double em = (p / r) / (gm - 1.0) + 0.5 * (u * u + v * v + ww * ww);
-        double Q[5] = {r, r * u, r * v, r * ww, r * em};
-        T dq[8];
-        ld8(w.dqrec + (size_t)cell * kD, dq);
+    for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n; cell += gridDim.x * blockDim.x) {
+        if (cell < nc) {
+            const double r = qo[cell], u = qo[nt + cell], v = qo[2 * nt + cell], ww = qo[3 * nt + cell],
+                         p = qo[4 * nt + cell];
+            const double em = (p / r) / (gm - 1.0) + 0.5 * (u * u + v * v + ww * ww);
+            double Q[5] = {r, r * u, r * v, r * ww, r * em};
+            T dq[8];
+            ld8(w.dqrec + (size_t)cell * kD, dq);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) Q[k] += (double)dq[k];
-        double prim[5];
-        if (Q[0] <= 0.0) {
-            prim[0] = Q[0]; prim[1] = u; prim[2] = v; prim[3] = ww; prim[4] = p;
-        } else {
-            const double od = 1.0 / Q[0];
-            const double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
-            const double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
-            prim[0] = Q[0]; prim[1] = um; prim[2] = vm; prim[3] = wm; prim[4] = (gm - 1.0) * ie;
-        }
-        if (prim[0] < 1.0e-6 * c.primInf[0] || prim[4] < 1.0e-6 * c.primInf[4]) {
-            const int slot = atomicAdd(&red->negcount, 1);
-            if (slot < kMaxNeg) neglist[slot] = cell;
-        }
-        T t[5];
+            for (int k = 0; k < 5; ++k) Q[k] += (double)dq[k];
+            double prim[5];
+            if (Q[0] <= 0.0) {
+                prim[0] = Q[0]; prim[1] = u; prim[2] = v; prim[3] = ww; prim[4] = p;
+            } else {
+                const double od = 1.0 / Q[0];
+                const double um = Q[1] * od, vm = Q[2] * od, wm = Q[3] * od;
+                const double ie = Q[4] - 0.5 * Q[0] * (um * um + vm * vm + wm * wm);
+                prim[0] = Q[0]; prim[1] = um; prim[2] = vm; prim[3] = wm; prim[4] = (gm - 1.0) * ie;
+            }
+            if (prim[0] < 1.0e-6 * c.primInf[0] || prim[4] < 1.0e-6 * c.primInf[4]) {
+                const int slot = atomicAdd(&red->negcount, 1);
+                if (slot < kMaxNeg) neglist[slot] = cell;
+            }
+            T t[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            qn[k * nt + cell] = prim[k];
-            t[k] = (T)prim[k];
-        }
-        put_state<T>(w.qrec + (size_t)cell * kQ, t, (T)gm);
-        T cr[8];
-        ld8(w.crec + (size_t)cell * kC, cr);
+            for (int k = 0; k < 5; ++k) {
+                qn[k * nt + cell] = prim[k];
+                t[k] = (T)prim[k];
+            }
+            put_state<T>(w.qrec + (size_t)cell * kQ, t, (T)gm);
+            T cr[8];
+            ld8(w.crec + (size_t)cell * kC, cr);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) rs[k] = (double)cr[k] * (double)cr[k];
+            for (int k = 0; k < 5; ++k) rs[k] += (double)cr[k] * (double)cr[k];
+        }
+        if (cell < g.nBFace) {
+            const int gc = nc + cell;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) qn[k * nt + gc] = qo[k * nt + gc];
+        }
     }
-    if (cell < g.nBFace) {
-        const int gc = nc + cell;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) qn[k * nt + gc] = qo[k * nt + gc];
-    }
+    // residual monitor sums: warp shuffle, then one FP64 atomic per block and variable
+    __shared__ double part[kThreads / 32][5];
+    const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         double v = rs[k];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&red->resnorm[k], v);
+        if (ln == 0) part[wid][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int i = 0; i < kThreads / 32; ++i) v += part[i][threadIdx.x];
+        if (v != 0.0) atomicAdd(&red->resnorm[threadIdx.x], v);
     }
 }
 
 template <class T>
 void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
-                   Reduce *red, int *neglist, cudaStream_t s)
+                   Reduce *red, int *neglist, int numSMs, cudaStream_t s)
 {
     const int n = g.nCell > g.nBFace ? g.nCell : g.nBFace;
-    update_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
+    int blocks = (n + kThreads - 1) / kThreads;
+    if (blocks > numSMs * 8) blocks = numSMs * 8;
+    update_kernel<T><<<blocks, kThreads, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
 }
 
 // SolutionFix (NSSolverUnstruct.cpp:14509-14585) for the listed cells, in the
@@ -871,7 +910,7 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
     template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int *, int *, int,    \
                                  int, cudaStream_t);                                                                \
     template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \
-                                   Reduce *, int *, cudaStream_t);                                                  \
+                                   Reduce *, int *, int, cudaStream_t);                                             \
     template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *,         \
                                          double *, Reduce *, int *, cudaStream_t);                                  \
     template void launch_sync_qrec<T>(const DevGrid &, const NsConst &, const double *, const Work<T> &,            \
