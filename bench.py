@@ -63,6 +63,16 @@ def workloads():
             mesh=lambda: M.channel_bump(256, 128, 32),
             params=dict(cases.EULER_BUMP),
             desc="Euler channel bump 256x128x32 hex (1.05M cells), M=0.5"),
+        # Config 2: 100^3 hexes x 6 jittered tetrahedra, laminar, least squares.
+        "laminar_cube_6M": dict(
+            mesh=lambda: M.tet_cube(100, jitter=0.15, seed=1),
+            params=dict(cases.LAMINAR, gradientName="lsq"),
+            desc="config 2: laminar cube, 100^3 hexes x 6 jittered tets (6.0M cells), M=0.3, Re=1e4, LSQ, "
+                 "Roe+Venkat, LU-SGS"),
+        "laminar_bump_1M": dict(
+            mesh=lambda: M.channel_bump(256, 128, 32),
+            params=dict(cases.LAMINAR),
+            desc="laminar channel bump 256x128x32 hex (1.05M cells), no-slip walls, M=0.3, Re=1e4, GG-cell"),
     }
 
 

@@ -23,6 +23,11 @@ EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "v
               "tscheme": 4, "nLUSGSSweeps": 1, "CFLStart": 0.01, "CFLEnd": 10.0, "CFLVaryStep": 500,
               "refMachNumber": 0.5, "attackd": 0.0, "refGama": 1.4}
 
+# Laminar NS (config 2 keys): Sutherland viscosity, Re 1e4 per unit length,
+# adiabatic no-slip walls.
+LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, refDimensionalTemperature=288.15,
+               prl=0.72, wallTemperature=-1.0)
+
 
 def freestream(params: dict) -> np.ndarray:
     """Non-dimensional free-stream primitive state (PerfectGas::ComputeReferencePrimitive,

@@ -263,6 +263,74 @@ uint64_t spread3(uint64_t v)
     return v;
 }
 
+// Least-squares weights (UnstructGrid::ComputeWeight, Geo_UnstructGrid.cpp:3761-3935,
+// 3-D, every face mark 1): per face the inverse squared centre distance (ghost
+// centre for boundary faces), per cell the inverse of sum_f w d d^T, zeroed
+// when its determinant is below SMALL.  Reference order; m6 is [nCell][6].
+void lsq_weights(const HostGrid &h, const std::vector<double> *G, std::vector<double> &iwt, std::vector<double> &m6)
+{
+    const int nc = h.nCell, nb = h.nBFace, nf = h.nFace;
+    const double *xcc = G[7].data(), *ycc = G[8].data(), *zcc = G[9].data();
+    iwt.assign(nf, 0.0);
+    m6.assign((size_t)nc * 6, 0.0);
+    for (int f = 0; f < nf; ++f) {
+        const int le = h.left[f], re = f < nb ? nc + f : h.right[f];
+        const double dx = (xcc[re] - xcc[le]) * 1.0, dy = (ycc[re] - ycc[le]) * 1.0, dz = (zcc[re] - zcc[le]) * 1.0;
+        const double ods = 1.0 / (dx * dx + dy * dy + dz * dz + kSmall);
+        const double t[6] = {ods * dx * dx, ods * dy * dy, ods * dz * dz, ods * dx * dy, ods * dx * dz, ods * dy * dz};
+        iwt[f] = ods;
+        for (int k = 0; k < 6; ++k) m6[(size_t)le * 6 + k] += t[k];
+        if (f >= nb)
+            for (int k = 0; k < 6; ++k) m6[(size_t)re * 6 + k] += t[k];
+    }
+    for (int c = 0; c < nc; ++c) {
+        double *m = &m6[(size_t)c * 6];
+        const double txx = m[0], tyy = m[1], tzz = m[2], txy = m[3], txz = m[4], tyz = m[5];
+        const double delt = (txx * tyy * tzz + 2.0 * txy * txz * tyz - txx * tyz * tyz - tyy * txz * txz - tzz * txy * txy);
+        if (std::fabs(delt) < kSmall) {
+            for (int k = 0; k < 6; ++k) m[k] = 0.0;
+        } else {
+            const double od = 1.0 / delt;
+            m[0] = (tyy * tzz - tyz * tyz) * od;
+            m[1] = (txx * tzz - txz * txz) * od;
+            m[2] = (txx * tyy - txy * txy) * od;
+            m[3] = (txz * tyz - txy * tzz) * od;
+            m[4] = (txy * tyz - txz * tyy) * od;
+            m[5] = (txy * txz - tyz * txx) * od;
+        }
+    }
+}
+
+// Geometry switches of ComputeVisflux (NSSolverUnstruct.cpp:13147-13236) per
+// reference face: bit 0 when both centre angles exceed skewnessAngle, bit 1
+// when both are positive and |dL|, |dR| > TINY.
+std::vector<uint8_t> viscous_flags(const HostGrid &h, const std::vector<double> *G, double skewAngle)
+{
+    const int nc = h.nCell, nb = h.nBFace, nf = h.nFace;
+    std::vector<uint8_t> vf(nf, 0);
+    for (int f = 0; f < nf; ++f) {
+        const int le = h.left[f], re = f < nb ? nc + f : h.right[f];
+        const double nxs = G[0][f], nys = G[1][f], nzs = G[2][f];
+        const double dxL = G[7][le] - G[4][f], dyL = G[8][le] - G[5][f], dzL = G[9][le] - G[6][f];
+        const double dxR = G[7][re] - G[4][f], dyR = G[8][re] - G[5][f], dzR = G[9][re] - G[6][f];
+        const double dL = nxs * dxL + nys * dyL + nzs * dzL;
+        const double dR = nxs * dxR + nys * dyR + nzs * dzR;
+        double t = -dL / (std::sqrt(dxL * dxL + dyL * dyL + dzL * dzL) + kSmall);
+        t = std::min(t, 1.0);
+        t = std::max(t, -1.0);
+        const double a1 = std::asin(t) * 180.0 / 3.141592653589793;
+        t = dR / (std::sqrt(dxR * dxR + dyR * dyR + dzR * dzR) + kSmall);
+        t = std::min(t, 1.0);
+        t = std::max(t, -1.0);
+        const double a2 = std::asin(t) * 180.0 / 3.141592653589793;
+        uint8_t b = 0;
+        if (a1 > skewAngle && a2 > skewAngle) b |= 1;
+        if (a1 > 0.0 && a2 > 0.0 && std::fabs(dL) > kSmall && std::fabs(dR) > kSmall) b |= 2;
+        vf[f] = b;
+    }
+    return vf;
+}
+
 std::vector<int> morton_order(int n, const double *x, const double *y, const double *z)
 {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -396,8 +464,10 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         gd->n_cell + gd->n_bface > 0x3fffffffLL || gd->n_face > 0x3fffffffLL)
         return PHX_ERR_ARG;
     if (prm->precision != PHX_FP64 && prm->precision != PHX_MIXED) return PHX_ERR_ARG;
-    if (prm->viscousType != 0) return PHX_ERR_ARG;   // viscous paths are attached by later releases
-    if (prm->gradientName != 0 || prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
+    // inviscid and laminar; laminar with adiabatic walls (wallTemperature <= 0)
+    if (prm->viscousType != 0 && prm->viscousType != 1) return PHX_ERR_ARG;
+    if (prm->viscousType == 1 && (prm->wallTemperature > 0.0 || prm->refReNumber <= 0.0)) return PHX_ERR_ARG;
+    if ((prm->gradientName != 0 && prm->gradientName != 1) || prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
 
@@ -575,6 +645,9 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         if (limiter_zeroed(t)) { ffadj[rank[h.left[f]]] = 1; limInit[nc + fs] = 0.0; }
     }
 
+    std::vector<double> iwt, m6;
+    if (prm->gradientName == 1) lsq_weights(h, ctx->geom, iwt, m6);
+
     // records in storage order
     std::vector<int2> lr(nf);
     std::vector<double> frec((size_t)nf * kF), xrec((size_t)nt * kX);
@@ -582,8 +655,17 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         const int f = forder[fs];
         lr[fs] = make_int2(rank[h.left[f]], f < nb ? nc + fs : rank[h.right[f]]);
         for (int k = 0; k < 7; ++k) frec[(size_t)fs * kF + k] = ctx->geom[k][f];
-        frec[(size_t)fs * kF + 7] = 0.0;
+        frec[(size_t)fs * kF + 7] = prm->gradientName == 1 ? iwt[f] : 0.0;
     }
+    std::vector<uint8_t> vflag(nf, 0);
+    if (prm->viscousType) {
+        const std::vector<uint8_t> vref = viscous_flags(h, ctx->geom, prm->skewnessAngle);
+        for (int fs = 0; fs < nf; ++fs) vflag[fs] = vref[forder[fs]];
+    }
+    std::vector<double> lsqs(prm->gradientName == 1 ? (size_t)nc * 8 : 8, 0.0);
+    if (prm->gradientName == 1)
+        for (int i = 0; i < nc; ++i)
+            for (int k = 0; k < 6; ++k) lsqs[(size_t)i * 8 + k] = m6[(size_t)ord[i] * 6 + k];
     std::vector<int> origv(nt);
     for (int i = 0; i < nt; ++i) {
         const int c = i < nc ? ord[i] : nc + forder[i - nc];
@@ -627,6 +709,16 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     k.nSweeps = prm->nLUSGSSweeps;
     k.lusgsTol = prm->LUSGSTolerance;
     k.reynolds = prm->refReNumber;
+    k.gradient = prm->gradientName;
+    // Param_NSSolverUnstruct getters; the Sutherland constant (110.4 K) over the
+    // reference temperature (PerfectGas::ComputeReferenceViscosityDimensional,
+    // PerfectGas.cpp:1486-1494)
+    k.oRe = prm->viscousType ? 1.0 / prm->refReNumber : 0.0;
+    k.oPrl = 1.0 / prm->prl;
+    k.oPrt = 1.0 / prm->prt;
+    k.cp = 1.0 / ((prm->refGama - 1.0) * (prm->refMachNumber * prm->refMachNumber));
+    k.tsuth = prm->tsuth / prm->refDimensionalTemperature;
+    k.skewAngle = prm->skewnessAngle;
 
     // device grid
     DevGrid &g = ctx->g;
@@ -638,6 +730,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     int rc = 0;
     rc |= upload(ctx, &g.lr, lr);
     rc |= upload(ctx, &g.frec, frec);
+    rc |= upload(ctx, &g.vflag, vflag);
+    rc |= upload(ctx, &g.lsq, lsqs);
     rc |= upload(ctx, &g.xrec, xrec);
     rc |= upload(ctx, &g.skew, skew);
     rc |= upload(ctx, &g.volpow, volpow);

@@ -35,13 +35,14 @@ enum BcKind : int32_t {
 
 // Record strides (elements).
 constexpr int kQ = 8;      // qrec: rho u v w p | c2 hm | limiter
-constexpr int kG = 16;     // grec: (d/dx, d/dy, d/dz) of var k at 3k..3k+2 | pad
+constexpr int kG = 20;     // grec: (d/dx, d/dy, d/dz) of var k at 3k..3k+2 | pad | temperature gradient 16..18 | pad
 constexpr int kC = 8;      // crec: res0..4 | diag | inviscid | viscous spectral radius
 constexpr int kD = 8;      // dqrec / dflux: 5 values | pad
-constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | pad
+constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | least-squares face weight
 constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
-constexpr int kFlux = 8;   // face flux record: F0..4 (times area) | inviscid spectral part | pad
-constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | pad
+constexpr int kFlux = 16;  // face flux record: inviscid F0..4 (times area) | inviscid and viscous
+                           // spectral parts | pad | viscous F1..4 (times area; F0 is zero) | pad
+constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | viscous spectral term
 constexpr int kSweepPad = 4; // LU-SGS lane groups per warp: schedule levels are padded to this multiple
 
 // Read-only device grid (FP64 metrics, connectivity, schedules), storage order.
@@ -53,6 +54,12 @@ struct DevGrid {
     const double *skew;          // [nCell]
     const double *volpow;        // [nCell] pow(pow(vol, 1/3), 3) as VencatLimiter7 forms it
     const double *walldist;      // [nCell]
+    const double *lsq;           // [nCell][8] inverse least-squares matrix ixx iyy izz ixy ixz iyz | pad (lsq only)
+    // [nFace] viscous-flux geometry switches of ComputeVisflux: bit 0 = both
+    // centre angles above skewnessAngle (project the cell values onto the
+    // normal line), bit 1 = both angles positive and |dL|, |dR| > TINY (form
+    // the normal derivative); pure geometry, decided on the host
+    const uint8_t *vflag;
     const int *c2f_off, *c2f;    // faces of each cell, ordered by the reference face number
     const int *orig;             // [nTotal] reference number of each cell (ghost: nCell + reference face)
     const int32_t *bkind;        // [nBFace] BcKind
@@ -86,6 +93,11 @@ struct NsConst {
     int nSweeps;
     double lusgsTol;
     double reynolds;
+    int gradient;                  // 0 Green-Gauss cell, 1 least squares
+    // viscous terms (Param_NSSolverUnstruct / PerfectGas): 1/Re, 1/Pr, 1/Pr_t,
+    // cp = 1 / ((gamma - 1) M^2), Sutherland constant over the reference
+    // temperature, skewness switch of the viscous flux (degrees)
+    double oRe, oPrl, oPrt, cp, tsuth, skewAngle;
 };
 
 // Working arrays of one precision T (double: FP64 path, float: mixed path).

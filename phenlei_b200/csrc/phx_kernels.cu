@@ -165,23 +165,44 @@ void launch_sync_qrec(const DevGrid &g, const NsConst &c, const double *q64, con
     sync_qrec_kernel<T><<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w);
 }
 
+// Temperature (ComputeGamaAndTemperature, NSSolverUnstruct.cpp:4717-4730) and
+// Sutherland viscosity (ComputeViscousCoefficientWithoutChemical, :6722-6747),
+// formed on the fly from a cell record wherever they are needed.
+template <class T>
+__device__ __forceinline__ T temperature(const T *q, T coef) { return q[4] / (coef * q[0]); }
+template <class T>
+__device__ __forceinline__ T sutherland(T t, T s) { return t * sqrt(t) * (T(1) + s) / (t + s); }
+
 // ---------------------------------------------------------------------------
 // Gradient + limiter, fused per cell:
 //  Green-Gauss cell gradient (UnstructGrid::CompGradientGGCell,
-//  Geo_UnstructGrid.cpp:3220-3284) of the 5 primitives, accumulated in the
-//  reference's face order; then the scalar Venkatakrishnan limiter from rho
-//  and p (Limiter::VencatLimiter7, Limiter.cpp:1091-1200, neighbour min/max of
+//  Geo_UnstructGrid.cpp:3220-3284) or least-squares gradient
+//  (CompGradientLSQ, :3996-4085, weights of ComputeWeight :3761-3935) of the 5
+//  primitives, and for viscous runs of the temperature (GetGradientField,
+//  NSSolverUnstruct.cpp:18244-18330), accumulated in the reference's face
+//  order; then the scalar Venkatakrishnan limiter from rho and p
+//  (Limiter::VencatLimiter7, Limiter.cpp:1091-1200, neighbour min/max of
 //  Limiter::MinMaxDiff :1202-1252 over interior faces), zeroed next to
 //  far-field boundaries (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, bool kTemp, bool kLsq>
 __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, NsConst c, Work<T> w)
 {
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= g.nCell) return;
+    constexpr int NV = kTemp ? 6 : 5;   // variable 5: temperature
     T qc[8];
     ld8(w.qrec + (size_t)cell * kQ, qc);
-    T gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
+    const T coef = (T)c.coefState;
+    T vc[NV];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) vc[k] = qc[k];
+    if (kTemp) vc[NV - 1] = temperature(qc, coef);
+    double xc[4];
+    ld4(g.xrec + (size_t)cell * kX, xc);
+    T gx[NV], gy[NV], gz[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) gx[k] = gy[k] = gz[k] = T(0);
     T rmin = qc[0], rmax = qc[0], pmin = qc[4], pmax = qc[4];
     const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
     for (int j = j0; j < j1; ++j) {
@@ -189,36 +210,70 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
         const int2 lr = ld(g.lr + f);
         const bool isLeft = (lr.x == cell);
         const int nb = isLeft ? lr.y : lr.x;
-        double fr[4];
-        ld4(g.frec + (size_t)f * kF, fr);
         T qn[8];
         ld8(w.qrec + (size_t)nb * kQ, qn);
-        const double a = fr[3];
-        const T nx = (T)(fr[0] * a), ny = (T)(fr[1] * a), nz = (T)(fr[2] * a);
+        T vn[NV];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            const T qf = T(0.5) * (isLeft ? (qc[k] + qn[k]) : (qn[k] + qc[k]));
-            if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
-            else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+        for (int k = 0; k < 5; ++k) vn[k] = qn[k];
+        if (kTemp) vn[NV - 1] = temperature(qn, coef);
+        if (kLsq) {
+            // (q[re] - q[le]) (x[re] - x[le]) iwt in the face's own orientation,
+            // added to both sides
+            double xn[4];
+            ld4(g.xrec + (size_t)nb * kX, xn);
+            const double iw = ld(g.frec + (size_t)f * kF + 7);
+            const T dx = (T)(isLeft ? xn[0] - xc[0] : xc[0] - xn[0]);
+            const T dy = (T)(isLeft ? xn[1] - xc[1] : xc[1] - xn[1]);
+            const T dz = (T)(isLeft ? xn[2] - xc[2] : xc[2] - xn[2]);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const T dq = (T)iw * (isLeft ? vn[k] - vc[k] : vc[k] - vn[k]);
+                gx[k] += dq * dx; gy[k] += dq * dy; gz[k] += dq * dz;
+            }
+        } else {
+            double fr[4];
+            ld4(g.frec + (size_t)f * kF, fr);
+            const double a = fr[3];
+            const T nx = (T)(fr[0] * a), ny = (T)(fr[1] * a), nz = (T)(fr[2] * a);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const T qf = T(0.5) * (isLeft ? (vc[k] + vn[k]) : (vn[k] + vc[k]));
+                if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
+                else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+            }
         }
         if (f >= g.nBFace) {
             rmin = tmin(rmin, qn[0]); rmax = tmax(rmax, qn[0]);
             pmin = tmin(pmin, qn[4]); pmax = tmax(pmax, qn[4]);
         }
     }
-    double xc[4];
-    ld4(g.xrec + (size_t)cell * kX, xc);
-    const T ovol = T(1) / (T)xc[3];
-    T gr[16];
+    if (kLsq) {
+        double m6[8];
+        ld8(g.lsq + (size_t)cell * 8, m6);
+        const T ixx = (T)m6[0], iyy = (T)m6[1], izz = (T)m6[2], ixy = (T)m6[3], ixz = (T)m6[4], iyz = (T)m6[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol;
-        gr[3 * k] = gx[k]; gr[3 * k + 1] = gy[k]; gr[3 * k + 2] = gz[k];
+        for (int k = 0; k < NV; ++k) {
+            const T tx = gx[k], ty = gy[k], tz = gz[k];
+            gx[k] = ixx * tx + ixy * ty + ixz * tz;
+            gy[k] = ixy * tx + iyy * ty + iyz * tz;
+            gz[k] = ixz * tx + iyz * ty + izz * tz;
+        }
+    } else {
+        const T ovol = T(1) / (T)xc[3];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) { gx[k] *= ovol; gy[k] *= ovol; gz[k] *= ovol; }
     }
+    T gr[kG];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { gr[3 * k] = gx[k]; gr[3 * k + 1] = gy[k]; gr[3 * k + 2] = gz[k]; }
     gr[15] = T(0);
     T *go = w.grec + (size_t)cell * kG;
     st8(go, gr);
     st8(go + 8, gr + 8);
+    if (kTemp) {
+        gr[16] = gx[NV - 1]; gr[17] = gy[NV - 1]; gr[18] = gz[NV - 1]; gr[19] = T(0);
+        st4(go + 16, gr + 16);
+    }
     T lim = T(1);
     if (c.limiter == 1) {
         const T vp = (T)ld(g.volpow + cell);
@@ -247,7 +302,14 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
 template <class T>
 void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s)
 {
-    gradient_limiter_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
+    const int blocks = (g.nCell + kThreads - 1) / kThreads;
+    if (c.viscous) {
+        if (c.gradient == 1) gradient_limiter_kernel<T, true, true><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else gradient_limiter_kernel<T, true, false><<<blocks, kThreads, 0, s>>>(g, c, w);
+    } else {
+        if (c.gradient == 1) gradient_limiter_kernel<T, false, true><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else gradient_limiter_kernel<T, false, false><<<blocks, kThreads, 0, s>>>(g, c, w);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -307,7 +369,151 @@ __device__ __forceinline__ void reconstruct(const DevGrid &g, const Work<T> &w, 
     }
 }
 
+// Gradients of u, v, w (9 values) and of the temperature (3) of one side of
+// a face; a ghost has the owner's gradient (least squares) or none
+// (Green-Gauss), as the reference's gradient routines leave them.
 template <class T>
+__device__ __forceinline__ void side_gradients(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell,
+                                               int owner, T *gv, T *gt)
+{
+    const int src = cell < g.nCell ? cell : (c.gradient == 1 ? owner : -1);
+    if (src < 0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gv[k] = T(0);
+        gt[0] = gt[1] = gt[2] = T(0);
+        return;
+    }
+    const T *gp = w.grec + (size_t)src * kG;
+    T a[16];
+    ld8(gp, a);
+    ld8(gp + 8, a + 8);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gv[k] = a[3 + k];
+    T b[4];
+    ld4(gp + 16, b);
+    gt[0] = b[0]; gt[1] = b[1]; gt[2] = b[2];
+}
+
+// Viscous flux of one face times the area, F1..F4 (F0 is zero), and the
+// face's viscous spectral-radius term, which is also the LU-SGS viscous
+// factor of both face uses (SpectrumRadiusViscous method 2,
+// NSSolverUnstruct.cpp:5930-5960; SolveLUSGSForward :15339-15357).
+// FaceWeight (Geo_UnstructGrid.cpp:2420-2478), GetVisFaceValue
+// (NSSolverUnstruct.cpp:7126-7375, static adiabatic walls) and ComputeVisflux
+// (:12977-13378, perfect gas).  Geometry is formed in FP64.
+template <class T>
+__device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, int le,
+                                             int re, const double *fr, const T *qL, const T *qR, T *fv, T &vspec)
+{
+    const bool bnd = f < g.nBFace;
+    const bool wall = bnd && g.bkind[f] == BK_WALL;
+    double xl[4], xr[4];
+    ld4(g.xrec + (size_t)le * kX, xl);
+    ld4(g.xrec + (size_t)re * kX, xr);
+    const double nxs = fr[0], nys = fr[1], nzs = fr[2], area = fr[3];
+    const T coef = (T)c.coefState, S = (T)c.tsuth;
+    const T tl0 = temperature(qL, coef), tr0 = temperature(qR, coef);
+    const T mul = T(0.5) * (sutherland(tl0, S) + sutherland(tr0, S));
+    const T mut = T(0);
+    // spectral radius / LU-SGS viscous factor
+    {
+        const double ds = fabs(nxs * (xr[0] - xl[0]) + nys * (xr[1] - xl[1]) + nzs * (xr[2] - xl[2]));
+        const T rho = T(0.5) * (qL[0] + qR[0]);
+        T vs = T(2) * (mul + mut) / (rho * (T)ds * (T)c.reynolds + (T)kSmall);
+        vs *= T(0.5) * (T)area;
+        vspec = vs;
+    }
+    // FaceWeight
+    double dwl = 1.0, dwr = 0.0;
+    if (!bnd) {
+        const double ax = fr[4] - xl[0], ay = fr[5] - xl[1], az = fr[6] - xl[2];
+        const double bx = fr[4] - xr[0], by = fr[5] - xr[1], bz = fr[6] - xr[2];
+        const double d1 = sqrt(ax * ax + ay * ay + az * az), d2 = sqrt(bx * bx + by * by + bz * bz);
+        const double dl = 1.0 / (d1 + d2 + kSmall);
+        dwl = d2 * dl;
+        dwr = d1 * dl;
+    }
+    // tangents
+    double t1x, t1y, t1z;
+    if (fabs(nxs) > kSmall) { t1x = nys; t1y = -nxs; t1z = 0.0; }
+    else if (fabs(nys) > kSmall) { t1x = -nys; t1y = nxs; t1z = 0.0; }
+    else if (fabs(nzs) > kSmall) { t1x = 0.0; t1y = -nzs; t1z = nys; }
+    else { fv[0] = fv[1] = fv[2] = fv[3] = T(0); return; }
+    const double on = 1.0 / sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    t1x *= on; t1y *= on; t1z *= on;
+    const double t2x = nys * t1z - nzs * t1y, t2y = nzs * t1x - nxs * t1z, t2z = nxs * t1y - nys * t1x;
+    const double dxL = xl[0] - fr[4], dyL = xl[1] - fr[5], dzL = xl[2] - fr[6];
+    const double dxR = xr[0] - fr[4], dyR = xr[1] - fr[5], dzR = xr[2] - fr[6];
+    const double dL = nxs * dxL + nys * dyL + nzs * dzL;
+    const double dR = nxs * dxR + nys * dyR + nzs * dzR;
+    const int vf = g.vflag[f];
+    T gvl[9], gtl[3], gvr[9], gtr[3];
+    side_gradients<T>(g, c, w, le, le, gvl, gtl);
+    side_gradients<T>(g, c, w, re, le, gvr, gtr);
+    T f1[3] = {qL[1], qL[2], qL[3]}, f2[3] = {qR[1], qR[2], qR[3]};
+    T tL = tl0, tR = tr0;
+    T fm[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) fm[k] = T(0.5) * (f1[k] + f2[k]);
+    const T tmf = T(0.5) * (tl0 + tr0);
+    T tM = tmf;
+    if (vf & 1) {
+        const T xnl = (T)(nxs * dL - dxL), ynl = (T)(nys * dL - dyL), znl = (T)(nzs * dL - dzL);
+        const T xnr = (T)(nxs * dR - dxR), ynr = (T)(nys * dR - dyR), znr = (T)(nzs * dR - dzR);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            f1[k] += gvl[3 * k] * xnl + gvl[3 * k + 1] * ynl + gvl[3 * k + 2] * znl;
+            f2[k] += gvr[3 * k] * xnr + gvr[3 * k + 1] * ynr + gvr[3 * k + 2] * znr;
+        }
+        tL += gtl[0] * xnl + gtl[1] * ynl + gtl[2] * znl;
+        tR += gtr[0] * xnr + gtr[1] * ynr + gtr[2] * znr;
+        if (tL < (T)kSmall) tL = tl0;
+        if (tR < (T)kSmall) tR = tr0;
+        // face values of GetVisFaceValue: the mean, no-slip at walls
+#pragma unroll
+        for (int k = 0; k < 3; ++k) fm[k] = wall ? T(0) : T(0.5) * (qL[k + 1] + qR[k + 1]);
+        tM = tmf;
+    }
+    T dfdn[3] = {0, 0, 0}, dtdn = T(0);
+    if (vf & 2) {
+        const T dLt = (T)dL, dRt = (T)dR;
+        T wL = dLt * dLt / (dLt * dLt + dRt * dRt);
+        T wR = T(1) - wL;
+        if (bnd) { wL = T(1); wR = T(0); }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) dfdn[k] = wL * ((f1[k] - fm[k]) / dLt) + wR * ((f2[k] - fm[k]) / dRt);
+        dtdn = ((tL - tM) / dLt) * wL + ((tR - tM) / dRt) * wR;
+    }
+    T gx[3], gy[3], gz[3];
+    const T wl = (T)dwl, wr = (T)dwr;
+    const T n1 = (T)nxs, n2 = (T)nys, n3 = (T)nzs;
+    const T a1 = (T)t1x, a2 = (T)t1y, a3 = (T)t1z, b1 = (T)t2x, b2 = (T)t2y, b3 = (T)t2z;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const T fx = wl * gvl[3 * k] + wr * gvr[3 * k];
+        const T fy = wl * gvl[3 * k + 1] + wr * gvr[3 * k + 1];
+        const T fz = wl * gvl[3 * k + 2] + wr * gvr[3 * k + 2];
+        const T d1 = a1 * fx + a2 * fy + a3 * fz;
+        const T d2 = b1 * fx + b2 * fy + b3 * fz;
+        gx[k] = n1 * dfdn[k] + a1 * d1 + b1 * d2;
+        gy[k] = n2 * dfdn[k] + a2 * d1 + b2 * d2;
+        gz[k] = n3 * dfdn[k] + a3 * d1 + b3 * d2;
+    }
+    const T kcp = (mul * (T)c.oPrl + mut * (T)c.oPrt) * (T)c.cp;
+    const T qn = kcp * dtdn;
+    const T div = T(2.0 / 3.0) * (gx[0] + gy[1] + gz[2]);
+    const T vis = mul + mut;
+    const T txx = vis * (T(2) * gx[0] - div), tyy = vis * (T(2) * gy[1] - div), tzz = vis * (T(2) * gz[2] - div);
+    const T txy = vis * (gy[0] + gx[1]), txz = vis * (gz[0] + gx[2]), tyz = vis * (gz[1] + gy[2]);
+    const T v1 = n1 * txx + n2 * txy + n3 * txz;
+    const T v2 = n1 * txy + n2 * tyy + n3 * tyz;
+    const T v3 = n1 * txz + n2 * tyz + n3 * tzz;
+    const T v4 = fm[0] * v1 + fm[1] * v2 + fm[2] * v3 + qn;
+    const T sc = -(T)c.oRe * (T)area;
+    fv[0] = sc * v1; fv[1] = sc * v2; fv[2] = sc * v3; fv[3] = sc * v4;
+}
+
+template <class T, bool kVisc>
 __global__ void __launch_bounds__(kThreads) face_flux_kernel(DevGrid g, NsConst c, Work<T> w)
 {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -355,14 +561,24 @@ __global__ void __launch_bounds__(kThreads) face_flux_kernel(DevGrid g, NsConst 
         const T cm = sqrt(gmm * pm / rm);
         fl[5] = T(0.5) * area * (fabs(vn) + cm);
     }
-    fl[6] = fl[7] = T(0);
+    T vspec = T(0);
+    if (kVisc) {
+        T fv[4];
+        viscous_face<T>(g, c, w, f, le, re, fr, qL, qR, fv, vspec);
+        T vr[8] = {fv[0], fv[1], fv[2], fv[3], T(0), T(0), T(0), T(0)};
+        st8(w.flux + (size_t)f * kFlux + 8, vr);
+    }
+    fl[6] = vspec;
+    fl[7] = T(0);
     st8(w.flux + (size_t)f * kFlux, fl);
     // LU-SGS factors: side 0 = the left cell's view, side 1 = the right cell's
     T cf[4];
     lusgs_coef<T>(qL, qR, xn, yn, zn, area, gm, cf);
+    cf[3] = vspec;
     st4(w.coef + (size_t)(2 * f) * kCoef, cf);
     if (f >= g.nBFace) {
         lusgs_coef<T>(qR, qL, -xn, -yn, -zn, area, gm, cf);
+        cf[3] = vspec;
         st4(w.coef + (size_t)(2 * f + 1) * kCoef, cf);
     }
 }
@@ -377,14 +593,14 @@ __device__ __forceinline__ void atomic_min_pos_double(unsigned long long *addr, 
     atomicMin(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-template <class T>
+template <class T, bool kVisc>
 __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red, double cfl)
 {
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     double mydt = kLarge;
     if (cell < g.nCell) {
         T res[5] = {0, 0, 0, 0, 0};
-        T spec = T(0);
+        T spec = T(0), vis = T(0);
         const int j0 = g.c2f_off[cell], j1 = g.c2f_off[cell + 1];
         for (int j = j0; j < j1; ++j) {
             const int f = ld(g.c2f + j);
@@ -399,9 +615,26 @@ __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsCo
                 for (int k = 0; k < 5; ++k) res[k] += fl[k];
             }
             spec += fl[5];
+            if (kVisc) vis += fl[6];
+        }
+        if (kVisc) {
+            // ViscousFlux is loaded after InviscidFlux (NSSolver::UpdateResiduals,
+            // NSSolver.cpp:71-80): a second pass in the same face order
+            for (int j = j0; j < j1; ++j) {
+                const int f = ld(g.c2f + j);
+                const bool isLeft = ld(&g.lr[f].x) == cell;
+                T fv[4];
+                ld4(w.flux + (size_t)f * kFlux + 8, fv);
+                if (isLeft) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) res[k + 1] -= fv[k];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) res[k + 1] += fv[k];
+                }
+            }
         }
         T *cr = w.crec + (size_t)cell * kC;
-        const T vis = c.viscous ? cr[7] : T(0);
         T out[8] = {res[0], res[1], res[2], res[3], res[4], T(0), spec, vis};
         st8(cr, out);
         T tot = spec;
@@ -435,8 +668,14 @@ __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsCo
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
 {
-    face_flux_kernel<T><<<(g.nFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w);
-    cell_residual_kernel<T><<<(g.nCell + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, red, cfl);
+    const int fb = (g.nFace + kThreads - 1) / kThreads, cb = (g.nCell + kThreads - 1) / kThreads;
+    if (c.viscous) {
+        face_flux_kernel<T, true><<<fb, kThreads, 0, s>>>(g, c, w);
+        cell_residual_kernel<T, true><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
+    } else {
+        face_flux_kernel<T, false><<<fb, kThreads, 0, s>>>(g, c, w);
+        cell_residual_kernel<T, false><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -597,6 +836,11 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         df[2] = (cf[0] * dq[2] - vm * a + ny * b) * area;
         df[3] = (cf[0] * dq[3] - wm * a + nz * b) * area;
         df[4] = (cf[0] * dq[4] - hm * a + cits * b) * area;
+        if (c.viscous) {
+            // viscous part of the delta flux (SolveLUSGSForward, :15339-15357)
+#pragma unroll
+            for (int m = 0; m < 5; ++m) df[m] -= cf[3] * dq[m];
+        }
     }
     // in-order accumulation (entries are in the cell's face order; lanes
     // past the cell's entry count contribute exact zeros)
