@@ -43,14 +43,17 @@ class _Params(C.Structure):
                 ("entropy_acoustic", C.c_double), ("entropy_convective", C.c_double),
                 ("cfl_start", C.c_double), ("cfl_end", C.c_double), ("cfl_vary_step", C.c_int),
                 ("ktmax", C.c_double), ("n_sweeps", C.c_int), ("lusgs_tol", C.c_double),
-                ("skewness_angle", C.c_double)]
+                ("skewness_angle", C.c_double), ("nut_inf", C.c_double), ("vist_inf", C.c_double),
+                ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double)]
 
 
 class _Work(C.Structure):
     _fields_ = [("gama", _dp), ("t", _dp), ("dqdx", _dp), ("dqdy", _dp), ("dqdz", _dp), ("limit", _dp),
                 ("res", _dp), ("inv_spec", _dp), ("vis_spec", _dp), ("dt", _dp), ("dq", _dp),
                 ("visl", _dp), ("vist", _dp), ("dtdx", _dp), ("dtdy", _dp), ("dtdz", _dp),
-                ("res_norm", C.c_double), ("n_negative", C.c_int)]
+                ("res_norm", C.c_double), ("n_negative", C.c_int),
+                ("qt", _dp), ("res_t", _dp), ("spec_t", _dp), ("dqt", _dp), ("matl", _dp), ("matr", _dp),
+                ("dntx", _dp), ("dnty", _dp), ("dntz", _dp)]
 
 
 _lib = None
@@ -139,13 +142,18 @@ def make_params(**kw) -> _Params:
     p.n_sweeps = kw.get("nLUSGSSweeps", 1)
     p.lusgs_tol = kw.get("LUSGSTolerance", 0.01)
     p.skewness_angle = kw.get("skewnessAngle", 60.0)
+    # Param_TurbSolver::Init: freeStreamTurbVar[ISA] = muoo / (rho_inf * 1 + SMALL)
+    p.nut_inf = kw.get("muoo", 3.0) / (1.0 * 1.0 + 1e-40)
+    p.vist_inf = kw.get("freeStreamViscosity", 1.0e-3)
+    p.turb_cfl_scale = kw.get("turbCFLScale", 1.0)
+    p.turb_skew_angle = kw.get("turbSkewnessAngle", 0.0)
     return p
 
 
 class Oracle:
     """Oracle state for one mesh: grid, metrics and the primitive field."""
 
-    def __init__(self, mesh, params: dict):
+    def __init__(self, mesh, params: dict, wall_dist=None):
         self.mesh = mesh
         self.keep = []
         nf, nc, nb = mesh.n_face, mesh.n_cell, mesh.n_bface
@@ -176,7 +184,12 @@ class Oracle:
         m = _Metrics()
         for k, v in self.geo.items():
             setattr(m, k, _p(v))
-        m.walldist = _dp()
+        self.walldist = None
+        if wall_dist is not None:
+            self.walldist = np.ascontiguousarray(wall_dist, np.float64)
+            m.walldist = _p(self.walldist)
+        else:
+            m.walldist = _dp()
         m.c2f_off, m.c2f = _p(self.c2f_off, _ip), _p(self.c2f, _ip)
         self.lsq = {"iwt": np.zeros(nf)}
         self.lsq.update({k: np.zeros(nc) for k in ("ixx", "iyy", "izz", "ixy", "ixz", "iyz")})
@@ -193,19 +206,27 @@ class Oracle:
         for name, shape in [("gama", (nt,)), ("t", (nt,)), ("dqdx", (5, nt)), ("dqdy", (5, nt)),
                             ("dqdz", (5, nt)), ("limit", (nt,)), ("res", (5, nt)), ("inv_spec", (nc,)),
                             ("vis_spec", (nc,)), ("dt", (nt,)), ("dq", (5, nt)), ("visl", (nt,)),
-                            ("vist", (nt,)), ("dtdx", (nt,)), ("dtdy", (nt,)), ("dtdz", (nt,))]:
+                            ("vist", (nt,)), ("dtdx", (nt,)), ("dtdy", (nt,)), ("dtdz", (nt,)),
+                            ("qt", (nt,)), ("res_t", (nt,)), ("spec_t", (nt,)), ("dqt", (nt,)),
+                            ("matl", (nf,)), ("matr", (nf,)), ("dntx", (nt,)), ("dnty", (nt,)), ("dntz", (nt,))]:
             a = np.zeros(shape)
             self.w_arrays[name] = a
             setattr(w, name, _p(a))
         self.w = w
         self.step = 0
+        if self.p.viscous == 3:
+            if self.walldist is None:
+                raise ValueError("the SA model needs the wall distance of every cell")
+            self.w_arrays["qt"][:] = self.p.nut_inf
 
     @property
     def avg_vol(self):
         return self.m.avg_vol
 
-    def set_state(self, q_cells: np.ndarray):
+    def set_state(self, q_cells: np.ndarray, qt_cells=None):
         self.q[:, : self.mesh.n_cell] = q_cells
+        if qt_cells is not None:
+            self.w_arrays["qt"][: self.mesh.n_cell] = qt_cells
 
     def iterate(self, nsteps: int = 1):
         hist = []

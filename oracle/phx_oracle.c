@@ -1114,4 +1114,369 @@ void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
     ox_lusgs(g, m, p, q, w->gama, w->t, w->visl, w->vist, w->res, w->dt, w->inv_spec, w->vis_spec, w->dq);
     w->n_negative = ox_update(g, m, p, q, w->gama, w->dq);
     w->res_norm = ox_residual_norm(g, w->res);
+    /* Controller::PostSolve (Controller.cpp:5063-5090): ghost states of the
+     * updated field, which the turbulence step reads */
+    ox_ns_boundary(g, m, p, q, w->gama);
+    if (p->viscous == 3) ox_sa_step(g, m, p, q, w);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Spalart-Allmaras (TurbSolverUnstr, NSMB formation, RANS, no wall function) */
+/* ------------------------------------------------------------------------ */
+
+/* PositiveSA, CFD/TurbSolver/include/TurbSolver.h:103-116. */
+static double positive_sa(double nue, double visl, double rho)
+{
+    if (nue < 0.0) {
+        double xsi = nue / (visl / rho);
+        double xsi3 = xsi * xsi * xsi;
+        return nue * (16.0 + xsi3) / (16.0 - xsi3);
+    }
+    return nue;
+}
+
+/* TurbSolverUnstr::Boundary (TurbSolverUnstr.cpp:5919-6019): OutflowBCRegion
+ * (copy; symmetry too), WallBCRegion (6116-6160, reflection), FarfieldBCRegion
+ * (6546-6640: Riemann-invariant direction picks copy or free stream). */
+void ox_sa_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
+                    double *qt, double *vist)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    const double *pi = p->prim_inf;
+    for (int f = 0; f < g->n_bface; ++f) {
+        int t = g->region_type[g->bface_region[f]];
+        int le = g->left[f], re = nc + f;
+        if (t == OX_BC_EXTRAPOLATION || t == OX_BC_SYMMETRY || t == OX_BC_OUTFLOW) {
+            vist[re] = vist[le];
+            qt[re] = qt[le];
+        } else if (is_wall(t)) {
+            vist[re] = -vist[le];
+            qt[re] = -qt[le];
+        } else if (t == OX_BC_FARFIELD) {
+            double rin = q[le], uin = q[nt + le], vin = q[2 * nt + le], win = q[3 * nt + le], pin = q[4 * nt + le];
+            double vno = m->xfn[f] * pi[1] + m->yfn[f] * pi[2] + m->zfn[f] * pi[3] - 0.0;
+            double vni = m->xfn[f] * uin + m->yfn[f] * vin + m->zfn[f] * win - 0.0;
+            double vei = sqrt(uin * uin + vin * vin + win * win);
+            double ga = gama[le];
+            double coo = sqrt(fabs(p->gama * pi[4] / pi[0]));
+            double cin = sqrt(fabs(ga * pin / rin));
+            int exit_;
+            if (vei > cin) {
+                exit_ = vni >= 0.0;
+            } else {
+                double riemp = vni + 2.0 * cin / (ga - 1.0);
+                double riemm = vno - 2.0 * coo / (p->gama - 1.0);
+                double vnb = 0.5 * (riemp + riemm);
+                exit_ = vnb >= 0.0;
+            }
+            if (exit_) { vist[re] = vist[le]; qt[re] = qt[le]; }
+            else { vist[re] = p->vist_inf; qt[re] = p->nut_inf; }
+        }
+    }
+}
+
+/* TurbSolverUnstr::Viscosity, 1eq-sa branch (TurbSolverUnstr.cpp:6910-6960):
+ * interior cells only. */
+static void sa_viscosity(const ox_grid *g, const double *q, const double *qt, const double *visl, double *vist)
+{
+    const double cv13 = 7.1 * 7.1 * 7.1;
+    for (int c = 0; c < g->n_cell; ++c) {
+        double nue = qt[c];
+        if (nue > 0.0) {
+            double ld = nue * q[c] / (visl[c] + OX_SMALL);
+            double ld3 = ld * ld * ld;
+            double fv1 = ld3 / (ld3 + cv13);
+            vist[c] = q[c] * fv1 * nue;
+        } else {
+            vist[c] = 0.0;
+        }
+    }
+}
+
+/* SourceFluxOneEquationOriginal (TurbSolverUnstr.cpp:2702-2916), NSMB
+ * formation (the cb2 gradient term is carried by the diffusion flux), RANS
+ * length scale = wall distance.  Velocity gradients are those of the NS step. */
+static void sa_source(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    int nt = ntot(g);
+    /* (the divergence term cmachfix is computed and zeroed by the reference) */
+    const double *dudy = w->dqdy + nt, *dudz = w->dqdz + nt;
+    const double *dvdx = w->dqdx + 2 * nt, *dvdz = w->dqdz + 2 * nt;
+    const double *dwdx = w->dqdx + 3 * nt, *dwdy = w->dqdy + 3 * nt;
+    const double ore = 1.0 / p->reynolds;
+    const double karm = 0.41, cb1 = 0.1355, cb2 = 0.622, cv1 = 7.1, cw2 = 0.3, cw3 = 2.0;
+    const double sigma = 2.0 / 3.0, sdilim = 1.0e9;
+    double kap2 = karm * karm, okap2 = 1.0 / kap2;
+    double osigma = 1.0 / sigma;
+    double cw1 = cb1 * okap2 + (1.0 + cb2) / sigma;
+    double cv13 = cv1 * cv1 * cv1;
+    double cw36 = pow(cw3, 6);
+    double or6 = 1.0 / 6.0;
+    double ct3 = 1.2;
+    double saC2 = 0.7, saC3 = 0.9;
+    double cb2s = osigma * cb2;
+    double cw1kap2 = cw1 * kap2;
+    for (int c = 0; c < g->n_cell; ++c) {
+        double nue = w->qt[c];
+        double omega = sqrt((dwdy[c] - dvdz[c]) * (dwdy[c] - dvdz[c]) + (dudz[c] - dwdx[c]) * (dudz[c] - dwdx[c]) +
+                            (dvdx[c] - dudy[c]) * (dvdx[c] - dudy[c]));
+        double volume = m->vol[c];
+        double olam = q[c] / (w->visl[c] + OX_SMALL);
+        double dist2 = m->walldist[c] * m->walldist[c];
+        double odist2 = 1.0 / dist2;
+        double xsi = nue * olam + OX_SMALL;
+        double xsi3 = xsi * xsi * xsi;
+        double fv1 = xsi3 / (xsi3 + cv13);
+        double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
+        double rs = nue * okap2 * odist2 * ore;
+        double nuetrs = nue * rs;
+        double sbar = rs * fv2;
+        double std_;
+        if (sbar >= -saC2 * omega) std_ = omega + sbar;
+        else std_ = omega + omega * (saC2 * saC2 * omega + saC3 * sbar) / ((saC3 - 2 * saC2) * omega - sbar);
+        double ostd = 1.0 / (std_ + OX_SMALL);
+        double r = rs * ostd;
+        r = omin(r, 10.0);
+        double r5 = pow(r, 5);
+        double gg = r + cw2 * (r5 * r - r);
+        double g6 = pow(gg, 6);
+        double fw = gg * pow((1.0 + cw36) / (g6 + cw36), or6);
+        double ft2 = 0.0;
+        double grd2 = w->dntx[c] * w->dntx[c] + w->dnty[c] * w->dnty[c] + w->dntz[c] * w->dntz[c];
+        double production = cb1 * (1.0 - ft2) * std_ * nue;
+        double diffsource = cb2s * grd2 * ore;
+        double walldest = (cw1kap2 * fw - cb1 * ft2) * nuetrs;
+        double destr_alpha = 50.0;
+        if (nue < 0.0) {
+            production = cb1 * (1.0 - ct3) * omega * nue;
+            walldest = -destr_alpha * cw1kap2 * nuetrs;
+        }
+        diffsource = omin(sdilim * production, diffsource);
+        (void)diffsource;
+        double source = production - walldest;
+        w->res_t[c] += (source) * volume;
+        double dfv2dk = (3.0 * cv13 * pow(fv1 / (xsi + OX_SMALL), 2) - 1.0) / pow(1.0 + xsi * fv1, 2);
+        double dsdnu = ore * okap2 * odist2 * (fv2 + xsi * dfv2dk);
+        double dfwdg = fw / (gg + OX_SMALL) * (1.0 - g6 / (g6 + cw36));
+        double dgdr = 1.0 + cw2 * (6.0 * r5 - 1.0);
+        double drdnu = ore * okap2 * odist2 * ostd * (1.0 - nue * ostd * dsdnu);
+        double dfwdnu = dfwdg * dgdr * drdnu;
+        double prod = cb1 * (1.0 - ft2) * std_;
+        double dest = (cw1 * fw - cb1 * ft2 * okap2) * nue * odist2 * ore;
+        double prodp = cb1 * ((1.0 - ft2) * dsdnu);
+        double destp = (cw1 * (fw + dfwdnu * nue) - cb1 * ft2 * okap2) * odist2 * ore;
+        if (nue < 0.0) {
+            prod = cb1 * (1.0 - ct3) * omega;
+            dest = -destr_alpha * cw1 * nue * odist2 * ore;
+            prodp = cb1 * ((1.0 - ct3) * dsdnu);
+            destp = -destr_alpha * cw1 * odist2 * ore;
+        }
+        double prde = prod - dest;
+        double prdep = prodp - destp;
+        double part1 = -0.5 * (prde - fabs(prde));
+        double part2 = -0.5 * (prdep - fabs(prdep)) * nue;
+        w->spec_t[c] += (part1 + part2) * volume;
+    }
+}
+
+/* InviscidFlux: GetQlQrTurbulence / GetQlQrNS (TurbSolverUnstr.cpp:4978-5140,
+ * boundary faces averaged; symmetry copies the left nu~) and NNDFlux
+ * (5721-5805, first-order upwind, rhoFlag = 0), LoadFlux (2205-2260). */
+static void sa_convection(const ox_grid *g, const ox_metrics *m, const double *q, ox_ns_work *w)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double ql = w->qt[le], qr = w->qt[re];
+        double pl[4], pr[4];
+        for (int k = 0; k < 4; ++k) { pl[k] = q[k * nt + le]; pr[k] = q[k * nt + re]; }
+        if (f < nb) {
+            int t = g->region_type[g->bface_region[f]];
+            if (t == OX_BC_SYMMETRY) qr = ql;
+            else { double a = 0.5 * (qr + ql); qr = a; ql = a; }
+            for (int k = 0; k < 4; ++k) { double a = 0.5 * (pr[k] + pl[k]); pr[k] = a; pl[k] = a; }
+        }
+        double vnl = m->xfn[f] * pl[1] + m->yfn[f] * pl[2] + m->zfn[f] * pl[3] - 0.0;
+        double vnr = m->xfn[f] * pr[1] + m->yfn[f] * pr[2] + m->zfn[f] * pr[3] - 0.0;
+        double vnll = 0.5 * (vnl + fabs(vnl));
+        double vnrr = 0.5 * (vnr - fabs(vnr));
+        double fl = (vnll * ql + vnrr * qr) * m->area[f];
+        w->res_t[le] -= fl;
+        if (f >= nb) w->res_t[re] += fl;
+    }
+}
+
+/* ViscousFlux: GetVisFaceValue (TurbSolverUnstr.cpp:3893-3990, mlt of the
+ * one-equation branch) and ComputeVisflux, NSMB branch (4438-4674). */
+static void sa_diffusion(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    int nb = g->n_bface, nc = g->n_cell;
+    const double ore = 1.0 / p->reynolds;
+    const double cb2 = 0.622, sigma = 2.0 / 3.0, osigma = 1.0 / sigma;
+    const double kw_osigma = 1.0 / (2.0 / 3.0);
+    const double *qt = w->qt, *visl = w->visl;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        int t = f < nb ? g->region_type[g->bface_region[f]] : 0;
+        /* mlt */
+        double nl = qt[le], vl = visl[le], rl = q[le];
+        double nr = qt[re], vr = visl[re], rr = q[re];
+        if (f < nb) {
+            if (nl < 0.0) {
+                nl = positive_sa(nl, vl, rl);
+                if (is_wall(t)) nr = -nl;
+            }
+        } else {
+            nl = positive_sa(nl, vl, rl);
+            nr = positive_sa(nr, vr, rr);
+        }
+        double mlt = kw_osigma * 0.5 * (vl / rl + vr / rr + nl + nr);
+        /* normal derivative */
+        double nxs = m->xfn[f], nys = m->yfn[f], nzs = m->zfn[f];
+        double dxL = m->xcc[le] - m->xfc[f], dyL = m->ycc[le] - m->yfc[f], dzL = m->zcc[le] - m->zfc[f];
+        double dxR = m->xcc[re] - m->xfc[f], dyR = m->ycc[re] - m->yfc[f], dzR = m->zcc[re] - m->zfc[f];
+        double dL = nxs * dxL + nys * dyL + nzs * dzL;
+        double dR = nxs * dxR + nys * dyR + nzs * dzR;
+        double tmp = -dL / (sqrt(dxL * dxL + dyL * dyL + dzL * dzL) + OX_SMALL);
+        tmp = omin(tmp, 1.0); tmp = omax(tmp, -1.0);
+        double a1 = asin(tmp) * 180.0 / OX_PI;
+        tmp = dR / (sqrt(dxR * dxR + dyR * dyR + dzR * dzR) + OX_SMALL);
+        tmp = omin(tmp, 1.0); tmp = omax(tmp, -1.0);
+        double a2 = asin(tmp) * 180.0 / OX_PI;
+        double f1 = qt[le], f2 = qt[re];
+        double fm = 0.5 * (f1 + f2);
+        double dfdn = 0.0;
+        if (a1 > p->turb_skew_angle && a2 > p->turb_skew_angle && fabs(dL) > OX_TINY && fabs(dR) > OX_TINY) {
+            double d1 = (f1 - fm) / dL, d2 = (f2 - fm) / dR;
+            double dtmp = dL * dL + dR * dR;
+            double wl = dL * dL / dtmp;
+            double wr = 1.0 - wl;
+            dfdn = wl * d1 + wr * d2;
+            if (f < nb && t != OX_BC_SYMMETRY) {
+                double nd = (m->xcc[re] - m->xcc[le]) * nxs + (m->ycc[re] - m->ycc[le]) * nys +
+                            (m->zcc[re] - m->zcc[le]) * nzs;
+                dfdn = (f2 - f1) / nd;
+            }
+        }
+        double flux1 = -ore * (1.0 + cb2) * mlt * dfdn * m->area[f];
+        double flux2 = ore * cb2 * osigma * dfdn * m->area[f];
+        double nuel = positive_sa(qt[le], visl[le], q[le]);
+        double nuer = positive_sa(qt[re], visl[re], q[re]);
+        w->res_t[le] -= flux1;
+        w->res_t[le] -= flux2 * (visl[le] / q[le] + nuel);
+        if (f >= nb) {
+            w->res_t[re] += flux1;
+            w->res_t[re] += flux2 * (visl[re] / q[re] + nuer);
+        }
+    }
+}
+
+/* SpectrumRadiusOfOneEquation, NSMB branch (TurbSolverUnstr.cpp:4690-4855):
+ * upwind convective Jacobians and the diffusion term into spec_turb and the
+ * face matrices mat_turbl / mat_turbr (called by Diagonal before the sweeps). */
+static void sa_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    const double ore = 1.0 / p->reynolds;
+    const double sigma = 2.0 / 3.0, osigma = 1.0 / sigma, cb2 = 0.622;
+    const double *qt = w->qt, *visl = w->visl;
+    double *spec = w->spec_t;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double rl = q[le], ul = q[nt + le], vl = q[2 * nt + le], wl = q[3 * nt + le];
+        double vnl = m->xfn[f] * ul + m->yfn[f] * vl + m->zfn[f] * wl - 0.0;
+        double ijl = vnl > 0.0 ? rl * vnl * m->area[f] : 0.0;
+        double rr = q[re], ur = q[nt + re], vr = q[2 * nt + re], wr = q[3 * nt + re];
+        double vnr = m->xfn[f] * ur + m->yfn[f] * vr + m->zfn[f] * wr - 0.0;
+        double ijr = vnr < 0.0 ? rr * vnr * m->area[f] : 0.0;
+        spec[le] += ijl;
+        spec[re] -= ijr;
+        w->matr[f] = ijr;
+        w->matl[f] = -ijl;
+        double orl = 1.0 / (rl + OX_SMALL), orr = 1.0 / (rr + OX_SMALL);
+        double nuel = positive_sa(qt[le], visl[le], rl);
+        double nuer = positive_sa(qt[re], visl[re], rr);
+        if (f < nb && is_wall(g->region_type[g->bface_region[f]])) nuer = -nuel;
+        double effl = visl[le] * orl + fabs(nuel);
+        double effr = visl[re] * orr + fabs(nuer);
+        double eff = 0.5 * (effl + effr);
+        double volume = 0.5 * (m->vol[le] + m->vol[re]);
+        double ovol = 1.0 / volume;
+        double ns2 = m->area[f] * m->area[f];
+        spec[le] += ore * ovol * (1.0 + cb2) * (osigma * eff * ns2);
+        spec[re] += ore * ovol * (1.0 + cb2) * (osigma * eff * ns2);
+        w->matl[f] += -ore * ovol * (1.0 + cb2) * (osigma * eff * ns2);
+        w->matr[f] += -ore * ovol * (1.0 + cb2) * (osigma * eff * ns2);
+        double cl = cb2 * osigma * effl, cr = cb2 * osigma * effr;
+        w->matl[f] += ore * ovol * ns2 * cl;
+        w->matr[f] += ore * ovol * ns2 * cr;
+    }
+}
+
+/* Scalar LU-SGS (SolveLUSGSForward / Backward, TurbSolverUnstr.cpp:1400-1638)
+ * with dq initialised by res (Controller::LUSGSInitialization); ghost dq keep
+ * the (zero) ghost residual.  Then UpdateFlowField (1180-1230, RANS, no
+ * clipping). */
+static void sa_lusgs_update(const ox_grid *g, const ox_metrics *m, ox_ns_work *w)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    double *dq = w->dqt;
+    double *dfl = calloc((size_t)nt, sizeof(double));
+    for (int i = 0; i < nt; ++i) dq[i] = w->res_t[i];
+    for (int c = 0; c < nc; ++c) {
+        double rhs0 = 0.0;
+        double ux = dfl[c];
+        dfl[c] = 0.0;
+        double d = w->res_t[c];
+        for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+            int f = m->c2f[j];
+            int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+            if (le > c || re > c) continue;
+            double df = (re == c) ? w->matl[f] * dq[le] : w->matr[f] * dq[re];
+            rhs0 += df;
+        }
+        dq[c] = (d - ux - rhs0) / w->spec_t[c];
+        dfl[c] += rhs0;
+    }
+    for (int c = nc - 1; c >= 0; --c) {
+        double rhs0 = 0.0;
+        double lx = dfl[c];
+        dfl[c] = 0.0;
+        double d = w->res_t[c];
+        for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+            int f = m->c2f[j];
+            int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+            if (le < c || re < c) continue;
+            double df = (re == c) ? w->matl[f] * dq[le] : w->matr[f] * dq[re];
+            rhs0 += df;
+        }
+        dq[c] = (d - lx - rhs0) / w->spec_t[c];
+        dfl[c] += rhs0;
+    }
+    free(dfl);
+    for (int c = 0; c < nc; ++c) w->qt[c] += dq[c];
+}
+
+void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    /* LoadResiduals: res = -rhs = -0 */
+    for (int i = 0; i < nt; ++i) w->res_t[i] = -0.0;
+    /* Controller::UpdateResiduals: SetBoundaryValueOfField, UpdateIndependentField
+     * (Viscosity, gradient of nu~) */
+    ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
+    sa_viscosity(g, q, w->qt, w->visl, w->vist);
+    ox_gradient(g, m, p, w->qt, w->dntx, w->dnty, w->dntz);
+    /* TurbSolver::UpdateResiduals (TurbSolver.cpp:316-346) */
+    ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
+    for (int i = 0; i < nt; ++i) w->spec_t[i] = 0.0;
+    for (int c = 0; c < nc; ++c) w->spec_t[c] = 0.0 * m->vol[c] + 1.0 / (p->turb_cfl_scale * w->dt[c] + OX_SMALL);
+    sa_source(g, m, p, q, w);
+    sa_convection(g, m, q, w);
+    sa_diffusion(g, m, p, q, w);
+    /* Controller::LUSGS: Diagonal, sweeps, UpdateFlowField */
+    sa_spectrum(g, m, p, q, w);
+    sa_lusgs_update(g, m, w);
+    /* PostSolve: SetBoundaryValueOfField */
+    ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
 }

@@ -70,6 +70,11 @@ typedef struct {
     int n_sweeps;           /* nLUSGSSweeps */
     double lusgs_tol;
     double skewness_angle;  /* viscous-flux skewness switch, degrees */
+    /* Spalart-Allmaras (viscous == 3; Param_TurbSolver.cpp:20-280) */
+    double nut_inf;         /* freeStreamTurbVar[ISA] = muoo / (rho_inf + SMALL) */
+    double vist_inf;        /* freeStreamViscosity (far-field inflow ghost eddy viscosity) */
+    double turb_cfl_scale;  /* turbCFLScale */
+    double turb_skew_angle; /* turbSkewnessAngle, degrees */
 } ox_params;
 
 /* Grid metrics: API/Geometry/src/Geo_UnstructGrid.cpp:5911-6156 (faces),
@@ -93,6 +98,10 @@ typedef struct {
     double *dtdx, *dtdy, *dtdz;  /* [nTotal] temperature gradient */
     double res_norm;             /* sqrt(sum res_rho^2 / nCell) */
     int n_negative;              /* cells repaired by SolutionFix */
+    /* Spalart-Allmaras working variable nu~ and its solver arrays */
+    double *qt, *res_t, *spec_t, *dqt;  /* [nTotal] */
+    double *matl, *matr;                /* [n_face] mat_turbl / mat_turbr */
+    double *dntx, *dnty, *dntz;         /* [nTotal] gradient of nu~ */
 } ox_ns_work;
 
 void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p,
@@ -120,6 +129,12 @@ int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double 
               const double *dq);
 double ox_residual_norm(const ox_grid *g, const double *res);
 void ox_viscosity(const ox_grid *g, const ox_params *p, const double *t, double *visl, double *vist);
+/* One outer step of TurbSolverUnstr (SA, NSMB formation), run after the NS
+ * step of the same outer iteration (Simulation::SolveSteady,
+ * Main/src/Simulation.cpp:1527-1560). */
+void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w);
+void ox_sa_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
+                    double *qt, double *vist);
 void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *t,
                      const double *visl, const double *vist, const double *dqdx, const double *dqdy,
                      const double *dqdz, const double *dtdx, const double *dtdy, const double *dtdz, double *res);

@@ -34,23 +34,44 @@ EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "v
 LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, refDimensionalTemperature=288.15,
                prl=0.72, wallTemperature=-1.0)
 
+# Spalart-Allmaras (NSMB formation), adiabatic no-slip walls, Re 1e5.
+SA = dict(LAMINAR, viscousType=3, viscousName="1eq-sa", refReNumber=1.0e5, muoo=3.0)
+
+
+def turb_state(m, params, seed):
+    """Seeded nu~ field around the free-stream value, about 10% of the cells negative."""
+    rng = np.random.default_rng(seed)
+    nu = params.get("muoo", 3.0) * (0.2 + 1.5 * rng.random(m.n_cell))
+    neg = rng.random(m.n_cell) < 0.1
+    nu[neg] = -0.5 * rng.random(int(neg.sum()))
+    return nu
+
 
 def mesh_spec(m, kind, args):
     return {"kind": kind, "args": args}
 
 
-def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02):
+def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02, turb_seed=None):
     m = getattr(M, kind)(**args)
     nc, nt = m.n_cell, m.n_cell + m.n_bface
     state = None
     if perturb_seed is not None:
         state = perturbed_state(m, params, seed=perturb_seed, amplitude=amplitude)
+    sa = params.get("viscousType", 0) == 3
+    if sa and turb_seed is not None:
+        if state is None:
+            from phenlei_b200.cases import freestream
+            state = np.repeat(freestream(params)[:, None], nc, axis=1)
+        state = np.vstack([state, turb_state(m, params, turb_seed)[None, :]])
     dumps = [("q", 5, nt), ("res", 5, nt), ("dt", 0, nt), ("limit2D", 5, nt), ("gradPrimtiveVarX", 5, nt),
              ("gradPrimtiveVarY", 5, nt), ("gradPrimtiveVarZ", 5, nt), ("invSpectralRadius", 0, nc)]
     viscous = params.get("viscousType", 0) > 0
     if viscous:
         dumps += [("visl", 0, nt), ("visSpectralRadius", 0, nc), ("gradTemperatureX", 1, nt),
                   ("gradTemperatureY", 1, nt), ("gradTemperatureZ", 1, nt)]
+    if sa:
+        dumps += [("vist", 0, nt), ("q_turb", 1, nt), ("res_turb", 1, nt), ("spec_turb", 1, nt),
+                  ("gradTurbulenceX", 1, nt)]
     r = run_reference(m, params, nsteps, dumps=dumps, state=state)
     out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}),
            "nsteps": nsteps, "res_hist": r["res_hist"]}
@@ -63,6 +84,11 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02)
         for k in ("visl", "visSpectralRadius"):
             out[k] = r[k]
         for k in ("gradTemperatureX", "gradTemperatureY", "gradTemperatureZ"):
+            out[k] = r[k].reshape(-1)[:nt]
+    if sa:
+        out["vist"] = r["vist"]
+        out["walldist"] = r["walldist"]
+        for k in ("q_turb", "res_turb", "spec_turb", "gradTurbulenceX"):
             out[k] = r[k].reshape(-1)[:nt]
     out["limit"] = r["limit2D"][0]
     path = os.path.join(OUT, name + ".npz")
@@ -93,3 +119,11 @@ if __name__ == "__main__":
     # Laminar jittered tetrahedra (config-2 element type), LSQ, perturbed, 3 iterations.
     fixture("laminar_tetcube_4_lsq_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
             dict(LAMINAR, gradientName="lsq"), 3, perturb_seed=11)
+    # SA bump, perturbed flow and nu~ (negative cells included), one iteration.
+    fixture("sa_bump_16x8x2_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 1, perturb_seed=7,
+            turb_seed=5)
+    # SA bump, LSQ, perturbed, 3 iterations.
+    fixture("sa_bump_16x8x2_lsq_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(SA, gradientName="lsq"), 3, perturb_seed=9, turb_seed=6)
+    # SA bump from the free stream, 30 iterations.
+    fixture("sa_bump_16x8x2_step30", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 30)

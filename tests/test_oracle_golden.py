@@ -53,6 +53,28 @@ def test_oracle_matches_reference_laminar(golden, name):
     assert rel_err(o.work("dtdz")[:nc], d["gradTemperatureZ"][:nc]) <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_16x8x2_step30"])
+def test_oracle_matches_reference_sa(golden, name):
+    """Spalart-Allmaras (NSMB formation) coupled to the NS step: boundary
+    values, eddy viscosity, source (negative-nu~ branch included), upwind
+    convection, diffusion, spectral radius, scalar LU-SGS."""
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    o = Oracle(m, d["params_dict"], wall_dist=d["walldist"])
+    if "state_in" in d:
+        o.set_state(d["state_in"][:5, :nc], d["state_in"][5, :nc])
+    hist = o.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(o.q[:, :nc], d["q"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("res")[:, :nc], d["res"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("qt")[:nc], d["q_turb"][:nc]) <= 1e-12
+    assert rel_err(o.work("vist"), d["vist"]) <= 1e-12
+    assert rel_err(o.work("res_t")[:nc], d["res_turb"][:nc]) <= 1e-12
+    assert rel_err(o.work("spec_t")[:nc], d["spec_turb"][:nc]) <= 1e-12
+    assert rel_err(o.work("dntx")[:nc], d["gradTurbulenceX"][:nc]) <= 1e-12
+
+
 def test_oracle_detects_planted_error(golden):
     """A mistake planted in the oracle's input shows up in the comparison."""
     d = golden("euler_bump_16x8x2_step1")
