@@ -239,3 +239,9 @@ class Oracle:
 
     def work(self, name):
         return self.w_arrays[name]
+
+    def forces(self):
+        """Wall force sums of AirForceCoefParts (16 values) from the current state."""
+        out = np.zeros(16)
+        lib().ox_forces(C.byref(self.g), C.byref(self.m), C.byref(self.p), _p(self.q), C.byref(self.w), _p(out))
+        return out

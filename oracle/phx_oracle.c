@@ -1480,3 +1480,69 @@ void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     /* PostSolve: SetBoundaryValueOfField */
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
 }
+
+/* CorrectGradient, API/Physics/src/GradientOperation.cpp:21-31. */
+static void correct_gradient(double fl, double fr, double *dfdx, double *dfdy, double *dfdz, double dx, double dy,
+                             double dz, double ods)
+{
+    double fold = *dfdx * dx + *dfdy * dy + *dfdz * dz;
+    double fnew = (fr - fl) * ods;
+    double df = fnew - fold;
+    *dfdx += df * dx;
+    *dfdy += df * dy;
+    *dfdz += df * dz;
+}
+
+void ox_forces(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const ox_ns_work *w,
+               double *out)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    double ca_f = 0, ca_p = 0, cn_f = 0, cn_p = 0, cz_f = 0, cz_p = 0, cpx = 0, cpy = 0, cpz = 0;
+    double cl_f = 0, cl_p = 0, cnm_f = 0, cnm_p = 0, cm_f = 0, cm_p = 0;
+    double poo = p->prim_inf[4];
+    double ore = p->viscous ? 1.0 / p->reynolds : 0.0;
+    /* regions in order, faces of a region in face order */
+    for (int r = 0; r < g->n_region; ++r) {
+        if (g->region_type[r] != OX_BC_SOLID_SURFACE) continue;
+        for (int f = 0; f < g->n_bface; ++f) {
+            if (g->bface_region[f] != r) continue;
+            int le = g->left[f], re = nc + f;
+            double nx = m->xfn[f] * m->area[f], ny = m->yfn[f] * m->area[f], nz = m->zfn[f] * m->area[f];
+            double pw = q[4 * nt + le];
+            double cp = 2.0 * (pw - poo);
+            double dpx = nx * cp, dpy = ny * cp, dpz = nz * cp;
+            ca_p += dpx; cn_p += dpy; cz_p += dpz;
+            double xc = m->xfc[f], yc = m->yfc[f], zc = m->zfc[f];
+            if (p->viscous) {
+                double dudx = w->dqdx[nt + le], dudy = w->dqdy[nt + le], dudz = w->dqdz[nt + le];
+                double dvdx = w->dqdx[2 * nt + le], dvdy = w->dqdy[2 * nt + le], dvdz = w->dqdz[2 * nt + le];
+                double dwdx = w->dqdx[3 * nt + le], dwdy = w->dqdy[3 * nt + le], dwdz = w->dqdz[3 * nt + le];
+                double dx = m->xcc[re] - m->xcc[le], dy = m->ycc[re] - m->ycc[le], dz = m->zcc[re] - m->zcc[le];
+                double ods = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+                dx = dx * ods; dy = dy * ods; dz = dz * ods;
+                correct_gradient(q[nt + le], q[nt + re], &dudx, &dudy, &dudz, dx, dy, dz, ods);
+                correct_gradient(q[2 * nt + le], q[2 * nt + re], &dvdx, &dvdy, &dvdz, dx, dy, dz, ods);
+                correct_gradient(q[3 * nt + le], q[3 * nt + re], &dwdx, &dwdy, &dwdz, dx, dy, dz, ods);
+                double vis = w->visl[le];
+                const double c23 = 2.0 / 3.0;
+                double txx = vis * c23 * (2.0 * dudx - dvdy - dwdz);
+                double tyy = vis * c23 * (2.0 * dvdy - dwdz - dudx);
+                double tzz = vis * c23 * (2.0 * dwdz - dudx - dvdy);
+                double txy = vis * (dudy + dvdx), txz = vis * (dudz + dwdx), tyz = vis * (dvdz + dwdy);
+                double fvsx = -2.0 * (nx * txx + ny * txy + nz * txz) * ore;
+                double fvsy = -2.0 * (nx * txy + ny * tyy + nz * tyz) * ore;
+                double fvsz = -2.0 * (nx * txz + ny * tyz + nz * tzz) * ore;
+                ca_f += fvsx; cn_f += fvsy; cz_f += fvsz;
+                cl_f += yc * fvsz - zc * fvsy;
+                cnm_f += zc * fvsx - xc * fvsz;
+                cm_f += xc * fvsy - yc * fvsx;
+            }
+            cl_p += yc * dpz - zc * dpy;
+            cnm_p += zc * dpx - xc * dpz;
+            cm_p += xc * dpy - yc * dpx;
+            cpx += dpx; cpy += dpy; cpz += dpz;
+        }
+    }
+    double v[16] = {ca_f, ca_p, cn_f, cn_p, cz_f, cz_p, cpx, cpy, cpz, cl_f, cl_p, cnm_f, cnm_p, cm_f, cm_p, 0.0};
+    for (int k = 0; k < 16; ++k) out[k] = v[k];
+}

@@ -129,6 +129,12 @@ int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double 
               const double *dq);
 double ox_residual_norm(const ox_grid *g, const double *res);
 void ox_viscosity(const ox_grid *g, const ox_params *p, const double *t, double *visl, double *vist);
+/* Wall force sums of NSSolverUnstruct::AirForceCoefParts (NSSolverUnstruct.cpp:
+ * 16026-16240, all solid-wall faces, torque reference at the origin): out[16] =
+ * CA_f CA_p CN_f CN_p CZ_f CZ_p cpx cpy cpz Cl_f Cl_p Cn_f Cn_p Cm_f Cm_p 0,
+ * from the current state, the NS step's gradients and laminar viscosity. */
+void ox_forces(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const ox_ns_work *w,
+               double *out);
 /* One outer step of TurbSolverUnstr (SA, NSMB formation), run after the NS
  * step of the same outer iteration (Simulation::SolveSteady,
  * Main/src/Simulation.cpp:1527-1560). */

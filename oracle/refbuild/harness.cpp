@@ -444,6 +444,20 @@ int main(int argc, char **argv)
     WriteRaw(outdir + "/zcc.bin", grid->GetCellCenterZ(), nTotal);
     WriteRaw(outdir + "/vol.bin", grid->GetCellVolume(), nTotal);
     if (grid->GetWallDist()) WriteRaw(outdir + "/walldist.bin", grid->GetWallDist(), nTotalCell);
+    // Wall force sums of NSSolverUnstruct::AirForceCoefParts (all parts): CA_f CA_p
+    // CN_f CN_p CZ_f CZ_p cpx cpy cpz Cl_f Cl_p Cn_f Cn_p Cm_f Cm_p hingeMoment.
+    {
+        NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(0, 0));
+        ActionKey *ak = new ActionKey();
+        ak->level = 0;
+        ns->AirForceCoefParts(ak, -1);
+        DataContainer *cd = ak->GetData();
+        cd->MoveToBegin();
+        std::vector<RDouble> f(16, 0.0);
+        for (int k = 0; k < 16; ++k) cd->Read(&f[k], sizeof(RDouble));
+        WriteRaw(outdir + "/forces.bin", f.data(), f.size());
+        delete ak;
+    }
     fprintf(stdout, "ref_harness: done %d steps, nTotalCell=%d nBoundFace=%d\n", nSteps, nTotalCell, nBoundFace);
     return 0;
 }

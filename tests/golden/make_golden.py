@@ -91,6 +91,7 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
         for k in ("q_turb", "res_turb", "spec_turb", "gradTurbulenceX"):
             out[k] = r[k].reshape(-1)[:nt]
     out["limit"] = r["limit2D"][0]
+    out["forces"] = r["forces"]
     path = os.path.join(OUT, name + ".npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path))

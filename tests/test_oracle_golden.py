@@ -28,6 +28,7 @@ def test_oracle_matches_reference(golden, name):
     assert rel_err(o.work("dqdx")[:, :nc], d["gradPrimtiveVarX"][:, :nc]) <= 1e-12
     assert rel_err(o.work("dqdz")[:, :nc], d["gradPrimtiveVarZ"][:, :nc]) <= 1e-12
     assert rel_err(o.work("inv_spec"), d["invSpectralRadius"]) <= 1e-12
+    assert rel_err(o.forces(), d["forces"]) <= 1e-12
 
 
 @pytest.mark.parametrize("name", ["laminar_bump_16x8x2_lsq_step1", "laminar_bump_16x8x2_step20",
@@ -51,6 +52,7 @@ def test_oracle_matches_reference_laminar(golden, name):
     assert rel_err(o.work("dqdy")[:, :nc], d["gradPrimtiveVarY"][:, :nc]) <= 1e-12
     assert rel_err(o.work("dtdx")[:nc], d["gradTemperatureX"][:nc]) <= 1e-12
     assert rel_err(o.work("dtdz")[:nc], d["gradTemperatureZ"][:nc]) <= 1e-12
+    assert rel_err(o.forces(), d["forces"]) <= 1e-12
 
 
 @pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_16x8x2_step30"])
@@ -73,6 +75,7 @@ def test_oracle_matches_reference_sa(golden, name):
     assert rel_err(o.work("res_t")[:nc], d["res_turb"][:nc]) <= 1e-12
     assert rel_err(o.work("spec_t")[:nc], d["spec_turb"][:nc]) <= 1e-12
     assert rel_err(o.work("dntx")[:nc], d["gradTurbulenceX"][:nc]) <= 1e-12
+    assert rel_err(o.forces(), d["forces"]) <= 1e-12
 
 
 def test_oracle_detects_planted_error(golden):
