@@ -75,6 +75,30 @@ class Mesh:
         return off
 
 
+def wall_distance(m: Mesh) -> np.ndarray:
+    """Distance of each cell's node-average centre to the nearest node-average
+    centre of a solid-wall face (k-d tree).  A stand-in for the reference's
+    wall-distance preprocessing (Pre_WalldistCompute) for generated meshes; the
+    SA path takes the wall distance as an input, and parity tests give both
+    sides the reference's own values."""
+    from scipy.spatial import cKDTree
+
+    fo = m.face_offsets()
+    walls = np.array([t == BC_SOLID_SURFACE for t, _ in m.regions])
+    wf = np.flatnonzero(walls[m.bface_region[: m.n_bface]])
+    if wf.size == 0:
+        raise ValueError("the mesh has no solid-wall faces")
+    xyz = np.stack([m.x, m.y, m.z], axis=1)
+    nb_end = int(fo[m.n_bface])
+    bsum = np.add.reduceat(xyz[m.face2node[:nb_end]], fo[: m.n_bface], axis=0)
+    fc = (bsum / m.face_nnode[: m.n_bface, None])[wf]
+    co = m.cell_offsets()
+    csum = np.add.reduceat(xyz[m.cell2node[: co[-1]]], co[:-1], axis=0)
+    cc = csum / m.cell_nnode[:, None]
+    d, _ = cKDTree(fc).query(cc, workers=-1)
+    return d
+
+
 def write_mesh(path: str, m: Mesh) -> None:
     """Raw little-endian file read by the oracle's reference harness."""
     with open(path, "wb") as f:
@@ -183,6 +207,175 @@ def _hex_block(X: np.ndarray, side_region: dict, regions: list) -> Mesh:
         n_bface=int(bnodes.shape[0]), bface_region=breg.astype(np.int32), regions=regions)
 
 
+def _hex_prism_block(X: np.ndarray, jp: int, side_region: dict, regions: list) -> Mesh:
+    """Structured block with its first `jp` j-layers split into prisms.
+
+    Each hexahedron (i, j, k) with j < jp becomes two prisms with triangles
+    (i,k)(i+1,k)(i+1,k+1) [A] and (i,k)(i+1,k+1)(i,k+1) [B] in the x-z plane,
+    extruded in j.  The hexahedra of layer jp see the prism layer's top as two
+    triangular faces (7 faces per cell).  Cells are numbered k slowest, then j,
+    then i (prism pairs A, B adjacent); boundary faces come first, grouped by
+    region, then interior faces ordered by (left, right).  Faces are oriented
+    from the left cell to the right cell (outward on the boundary).
+    """
+    ni, nj, nk = (s_ - 1 for s_ in X.shape[:3])
+    jp = max(0, min(jp, nj))
+    xyz = X.transpose(2, 1, 0, 3).reshape(-1, 3)
+
+    def nid(i, j, k):
+        return (i + (ni + 1) * (j + (nj + 1) * k)).astype(np.int64)
+
+    S = jp * 2 * ni + (nj - jp) * ni
+
+    def cA(i, j, k):
+        return k * S + j * 2 * ni + 2 * i
+
+    def cH(i, j, k):
+        return k * S + jp * 2 * ni + (j - jp) * ni + i
+
+    def grid(*shape_ranges):
+        return np.meshgrid(*[np.arange(a, b, dtype=np.int64) for a, b in shape_ranges], indexing="ij")
+
+    F, L, R, SIDE = [], [], [], []   # face node arrays, left, right (-1 boundary), boundary side
+
+    def add(nodes, left, right, side=None):
+        F.append(nodes); L.append(left.ravel()); R.append(right.ravel())
+        SIDE.append(np.full(left.size, -1 if side is None else side, np.int8))
+
+    sides = ["imin", "imax", "jmin", "jmax", "kmin", "kmax"]
+    # i-faces
+    for lo_j, hi_j, prism in ((0, jp, True), (jp, nj, False)):
+        if hi_j <= lo_j:
+            continue
+        ii, j, k = grid((0, ni + 1), (lo_j, hi_j), (0, nk))
+        q = np.stack([nid(ii, j, k), nid(ii, j + 1, k), nid(ii, j + 1, k + 1), nid(ii, j, k + 1)], -1).reshape(-1, 4)
+        minus = (cA(ii - 1, j, k) if prism else cH(ii - 1, j, k)).ravel()       # A has the +x side
+        plus = (cA(ii, j, k) + 1 if prism else cH(ii, j, k)).ravel()           # B has the -x side
+        iiv = ii.ravel()
+        inner = (iiv > 0) & (iiv < ni)
+        add(q[inner], minus[inner], plus[inner])
+        add(q[iiv == 0], plus[iiv == 0], np.full(int((iiv == 0).sum()), -1), 0)
+        add(q[iiv == ni], minus[iiv == ni], np.full(int((iiv == ni).sum()), -1), 1)
+    # k-faces
+    for lo_j, hi_j, prism in ((0, jp, True), (jp, nj, False)):
+        if hi_j <= lo_j:
+            continue
+        i, j, kk = grid((0, ni), (lo_j, hi_j), (0, nk + 1))
+        q = np.stack([nid(i, j, kk), nid(i + 1, j, kk), nid(i + 1, j + 1, kk), nid(i, j + 1, kk)], -1).reshape(-1, 4)
+        minus = (cA(i, j, kk - 1) + 1 if prism else cH(i, j, kk - 1)).ravel()  # B has the +z side
+        plus = (cA(i, j, kk) if prism else cH(i, j, kk)).ravel()               # A has the -z side
+        kv = kk.ravel()
+        inner = (kv > 0) & (kv < nk)
+        add(q[inner], minus[inner], plus[inner])
+        add(q[kv == 0], plus[kv == 0], np.full(int((kv == 0).sum()), -1), 4)
+        add(q[kv == nk], minus[kv == nk], np.full(int((kv == nk).sum()), -1), 5)
+    # j-faces: triangles up to and including the interface jp, quads above
+    if jp > 0:
+        i, jj, k = grid((0, ni), (0, jp + 1), (0, nk))
+        n00, n10, n11, n01 = nid(i, jj, k), nid(i + 1, jj, k), nid(i + 1, jj, k + 1), nid(i, jj, k + 1)
+        for tri, off in ((np.stack([n00, n10, n11], -1), 0), (np.stack([n00, n11, n01], -1), 1)):
+            t = tri.reshape(-1, 3)
+            jv = jj.ravel()
+            below = (cA(i, jj - 1, k) + off).ravel()
+            above = np.where(jj < jp, cA(i, jj, k) + off, cH(i, np.minimum(jj, nj - 1), k) if jp < nj else -1).ravel()
+            inner = (jv > 0) & ((jv < jp) | ((jv == jp) & (jp < nj)))
+            add(t[inner], below[inner], above[inner])
+            add(t[jv == 0], above[jv == 0], np.full(int((jv == 0).sum()), -1), 2)
+            if jp == nj:
+                add(t[jv == nj], below[jv == nj], np.full(int((jv == nj).sum()), -1), 3)
+    if jp < nj:
+        i, jj, k = grid((0, ni), (jp if jp > 0 else 0, nj + 1), (0, nk))
+        q = np.stack([nid(i, jj, k), nid(i, jj, k + 1), nid(i + 1, jj, k + 1), nid(i + 1, jj, k)], -1).reshape(-1, 4)
+        jv = jj.ravel()
+        below = cH(i, np.maximum(jj - 1, jp), k).ravel()
+        above = cH(i, np.minimum(jj, nj - 1), k).ravel()
+        inner = (jv > jp) & (jv < nj)
+        add(q[inner], below[inner], above[inner])
+        if jp == 0:
+            add(q[jv == 0], above[jv == 0], np.full(int((jv == 0).sum()), -1), 2)
+        add(q[jv == nj], below[jv == nj], np.full(int((jv == nj).sum()), -1), 3)
+    # diagonal faces inside the prism pairs
+    if jp > 0:
+        i, j, k = grid((0, ni), (0, jp), (0, nk))
+        q = np.stack([nid(i, j, k), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k)], -1).reshape(-1, 4)
+        add(q, cA(i, j, k).ravel(), (cA(i, j, k) + 1).ravel())
+    # cells
+    cells = []
+    if jp > 0:
+        i, j, k = grid((0, ni), (0, jp), (0, nk))
+        a = np.stack([nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j, k + 1),
+                      nid(i, j + 1, k), nid(i + 1, j + 1, k), nid(i + 1, j + 1, k + 1)], -1)
+        b = np.stack([nid(i, j, k), nid(i + 1, j, k + 1), nid(i, j, k + 1),
+                      nid(i, j + 1, k), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)], -1)
+        cells.append((cA(i, j, k).ravel(), a.reshape(-1, 6)))
+        cells.append(((cA(i, j, k) + 1).ravel(), b.reshape(-1, 6)))
+    if jp < nj:
+        i, j, k = grid((0, ni), (jp, nj), (0, nk))
+        h = np.stack([nid(i, j, k), nid(i + 1, j, k), nid(i, j + 1, k), nid(i + 1, j + 1, k),
+                      nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i, j + 1, k + 1), nid(i + 1, j + 1, k + 1)], -1)
+        cells.append((cH(i, j, k).ravel(), h.reshape(-1, 8)))
+    ncell = sum(c.size for c, _ in cells)
+    cnn = np.zeros(ncell, np.int32)
+    for ids, nodes in cells:
+        cnn[ids] = nodes.shape[1]
+    coff = np.zeros(ncell + 1, np.int64)
+    np.cumsum(cnn, out=coff[1:])
+    c2n = np.zeros(int(coff[-1]), np.int64)
+    cen = np.zeros((ncell, 3))
+    for ids, nodes in cells:
+        w = nodes.shape[1]
+        c2n[(coff[ids][:, None] + np.arange(w)[None, :]).ravel()] = np.sort(nodes, axis=1).ravel()
+        cen[ids] = xyz[nodes].mean(axis=1)
+    # orient faces left -> right (outward on the boundary), order, flatten
+    out_nodes, out_left, out_right, out_side = [], [], [], []
+    for nodes, le, re, sd in zip(F, L, R, SIDE):
+        if nodes.shape[0] == 0:
+            continue
+        p = xyz[nodes]
+        if nodes.shape[1] == 4:
+            nrm = np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 1])
+        else:
+            nrm = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+        tgt = np.where((re >= 0)[:, None], cen[np.maximum(re, 0)], p.mean(axis=1)) - cen[le]
+        flip = np.einsum("ij,ij->i", nrm, tgt) < 0.0
+        nodes = nodes.copy()
+        nodes[flip] = nodes[flip][:, ::-1]
+        out_nodes.append(nodes); out_left.append(le); out_right.append(re); out_side.append(sd)
+    left = np.concatenate(out_left)
+    right = np.concatenate(out_right)
+    side = np.concatenate(out_side)
+    nnode = np.concatenate([np.full(n.shape[0], n.shape[1], np.int32) for n in out_nodes])
+    # region of each boundary face
+    breg = np.full(left.size, -1, np.int64)
+    fcen = np.concatenate([xyz[n].mean(axis=1) for n in out_nodes])
+    for sidx, name in enumerate(sides):
+        m_ = side == sidx
+        if not m_.any():
+            continue
+        r = side_region[name]
+        breg[m_] = np.asarray(r(fcen[m_]), np.int64) if callable(r) else r
+    bnd = right < 0
+    bidx = np.flatnonzero(bnd)
+    bidx = bidx[np.lexsort((left[bidx], breg[bidx]))]
+    iidx = np.flatnonzero(~bnd)
+    iidx = iidx[np.lexsort((right[iidx], left[iidx]))]
+    order = np.concatenate([bidx, iidx])
+    # flatten face2node in the new order
+    offs = np.zeros(nnode.size + 1, np.int64)
+    np.cumsum(nnode, out=offs[1:])
+    flat = np.concatenate([n.ravel() for n in out_nodes])
+    nn_o = nnode[order]
+    starts = offs[order]
+    idx = np.repeat(starts, nn_o) + (np.arange(int(nn_o.sum())) - np.repeat(np.cumsum(nn_o) - nn_o, nn_o))
+    f2n = flat[idx]
+    return Mesh(
+        x=np.ascontiguousarray(xyz[:, 0]), y=np.ascontiguousarray(xyz[:, 1]), z=np.ascontiguousarray(xyz[:, 2]),
+        face_nnode=nn_o.astype(np.int32), face2node=f2n.astype(np.int32),
+        left=left[order].astype(np.int32), right=np.where(bnd[order], -1, right[order]).astype(np.int32),
+        cell_nnode=cnn, cell2node=c2n.astype(np.int32),
+        n_bface=int(bidx.size), bface_region=breg[bidx].astype(np.int32), regions=regions)
+
+
 def tanh_one_sided(n: int, first: float) -> np.ndarray:
     """n+1 points on [0,1] clustered at 0 with first spacing `first` (tanh law)."""
     if first * n >= 1.0:
@@ -205,7 +398,7 @@ def tanh_one_sided(n: int, first: float) -> np.ndarray:
 
 
 def channel_bump(nx=64, ny=32, nz=4, thickness=0.10, length=3.0, height=1.0,
-                 wall_spacing=0.01, dz=None, lower_region="Wall", upper_region="Wall") -> Mesh:
+                 wall_spacing=0.01, dz=None, lower_region="Wall", upper_region="Wall", prism_layers=0) -> Mesh:
     """3-D channel with a circular-arc bump of chord 1 on x in [1,2] of the lower wall.
 
     x and z are uniform (dz defaults to dx), y is tanh-stretched from the lower
@@ -227,6 +420,8 @@ def channel_bump(nx=64, ny=32, nz=4, thickness=0.10, length=3.0, height=1.0,
     regions = [(BC_SOLID_SURFACE, "LowerWall"), (BC_SOLID_SURFACE, "UpperWall"),
                (BC_FARFIELD, "Farfield"), (BC_SYMMETRY, "Symmetry")]
     side = {"jmin": 0, "jmax": 1, "imin": 2, "imax": 2, "kmin": 3, "kmax": 3}
+    if prism_layers > 0:
+        return _hex_prism_block(X, prism_layers, side, regions)
     return _hex_block(X, side, regions)
 
 

@@ -126,5 +126,8 @@ if __name__ == "__main__":
     # SA bump, LSQ, perturbed, 3 iterations.
     fixture("sa_bump_16x8x2_lsq_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
             dict(SA, gradientName="lsq"), 3, perturb_seed=9, turb_seed=6)
+    # SA bump on the mixed hex / prism mesh (3 prism layers at the walls), perturbed, 2 iterations.
+    fixture("sa_bump_prism_16x8x2_step2", "channel_bump", {"nx": 16, "ny": 8, "nz": 2, "prism_layers": 3}, SA, 2,
+            perturb_seed=8, turb_seed=4)
     # SA bump from the free stream, 30 iterations.
     fixture("sa_bump_16x8x2_step30", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 30)
