@@ -55,6 +55,20 @@ def workloads():
             params=dict(cases.EULER_BUMP, refMachNumber=0.8, CFLEnd=20.0),
             desc="3-D transonic channel bump 8% thick, 1024x92x128 hex (12.06M cells), M=0.8, Roe+Venkat, "
                  "GG-cell, LU-SGS CFL 20, inviscid"),
+        # Config 5: mixed hex / prism bump, 1024x92x128 with the 30 wall-adjacent
+        # layers as prisms (15,990,784 cells), M=0.8, Re=1e7, SA, Roe + Venkat, CFL 20.
+        "transonic_bump_sa_16M": dict(
+            mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001,
+                                        prism_layers=30),
+            params=dict(cases.SA_BUMP),
+            wall_dist=True,
+            desc="config 5: 3-D transonic channel bump 8% thick, 1024x92x128 with 30 prism layers at the walls "
+                 "(15.99M hex+prism cells), M=0.8, Re=1e7, Spalart-Allmaras, Roe+Venkat, GG-cell, LU-SGS CFL 20"),
+        "sa_bump_1M": dict(
+            mesh=lambda: M.channel_bump(256, 92, 32, thickness=0.08, wall_spacing=0.001, prism_layers=30),
+            params=dict(cases.SA_BUMP),
+            wall_dist=True,
+            desc="SA channel bump 256x92x32 with 30 prism layers (1.0M hex+prism cells), M=0.8, Re=1e7"),
         "euler_bump_8k": dict(
             mesh=lambda: M.channel_bump(64, 32, 4),
             params=dict(cases.EULER_BUMP),
@@ -76,7 +90,7 @@ def workloads():
     }
 
 
-DEFAULT_WORKLOAD = "transonic_bump_euler_16M"
+DEFAULT_WORKLOAD = "transonic_bump_sa_16M"
 
 
 class ClockSampler:
@@ -139,34 +153,65 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def kernel_bytes(m, precision: str) -> dict:
-    """Algorithmic bytes per launch of each kernel (compulsory-byte rule)."""
+def kernel_bytes(m, precision: str, viscous: int = 0, gradient: str = "ggcell") -> dict:
+    """Algorithmic bytes per launch of each phase under the compulsory-byte rule
+    (each array element counted once per pass that reads or writes it; cell
+    values gathered through faces counted once per cell; face arrays once per
+    face per pass; indices 4 B, FP64 metrics and master state 8 B, working
+    state E = 8 B (FP64) or 4 B (mixed)).  Derivation in DESIGN.md."""
     nc, nb, nf = m.n_cell, m.n_bface, m.n_face
     nt = nc + nb
-    ni = nf - nb
-    lc2f = 2 * ni + nb
-    t = 8 if precision == "fp64" else 4
-    face_geo = 7 * 8          # normal (3), area, centre (3), FP64
-    idx = 8                   # left, right
+    L = 2 * (nf - nb) + nb          # cell -> face entries
+    E = 8 if precision == "fp64" else 4
+    vis = viscous > 0
+    sa = viscous == 3
+    lsq = gradient == "lsq"
     out = {}
-    # boundary: read owner state (FP64 master) + normal, write ghost state (+ working copy) + c2, hm
-    out["boundary"] = nb * (5 * 8 + 3 * 8 + 4 + 5 * 8 + (5 * t if t == 4 else 0) + 2 * t)
-    # gradient+limiter: read q (5), c2f, face normal/area/centre per face, cell centre/vol/volpow; write grad (15) + limiter
-    out["gradient_limiter"] = nt * 5 * t + (lc2f + nc + 1) * 4 + nf * (face_geo + idx) + nc * 5 * 8 + nc * 16 * t
-    # residual: read q, grad, limiter, cell centres, face geometry, c2f; write res (5), invspec, dtraw, coef (3 per slot), c2, hm
-    out["residual"] = (nt * 5 * t + nc * 15 * t + nt * t + nt * 3 * 8 + nf * (face_geo + idx + 4)
-                       + (lc2f + nc + 1) * 4 + nc * 2 * 8 + nc * (5 + 2 + 2) * t + 3 * lc2f * t)
-    # LU-SGS: read res, dtraw, spec, vol, q (u,v,w), c2, hm, coef, normals/area, c2f, schedules; write dq, dflux, diag;
-    # dq of every cell read back by its neighbours (counted once per sweep)
-    out["lusgs"] = (nc * (5 + 3) * t + nc * 8 + nt * 5 * t + 2 * nt * t + 2 * 3 * lc2f * t + 2 * nf * (4 * 8 + idx)
-                    + 2 * (lc2f + nc + 1) * 4 + 2 * nc * 4 + nc * (5 + 5 + 1) * t + 2 * nt * 5 * t + nc * 5 * t)
-    # update: read q (FP64), dq, res; write q (FP64) (+ working copy)
-    out["update"] = nc * (5 * 8 + 5 * t + 5 * t + 5 * 8 + (5 * t if t == 4 else 0)) + nb * 10 * 8
+    # NS boundary: owner master state + normal -> ghost master state + working record (5 + c2, hm)
+    bnd = nb * (5 * 8 + 3 * 8 + 4 + 5 * 8 + 7 * E) + (nb * E if sa else 0)
+    out["boundary"] = bnd
+    # gradient + limiter: working state of cells and ghosts, per face normal*area (GG) or weight + centres (LSQ),
+    # face centre (limiter), lr, c2f; cell centre, volume, volpow (+ LSQ matrix); writes gradients + limiter
+    nvar = 6 if vis else 5
+    g = nt * (5 * E) + nf * (4 * 8 + 3 * 8 + 8) + (L + nc + 1) * 4 + nc * (4 * 8 + 8) + nc * (3 * nvar * E + E)
+    if lsq:
+        g += nt * 3 * 8 + nc * 6 * 8 + nf * 8
+    if sa:
+        g += nc * E
+    out["gradient_limiter"] = g
+    # face pass: state + limiter of both sides (once per cell), gradients, cell centres, face geometry and lr;
+    # writes face flux (5 + spectral parts) and the MXDQ factors of each face use (3 + viscous term)
+    fp = nt * 6 * E + nc * 15 * E + nt * 3 * 8 + nf * (7 * 8 + 8) + nf * 6 * E + L * (3 + (1 if vis else 0)) * E
+    if vis:
+        fp += nc * 3 * E + nf * (4 + 1) * E + nf * 1
+    if sa:
+        fp += nt * E
+    # cell pass: face fluxes through c2f + lr, skew, volume, pressure; writes residual, spectral radii, dt
+    cp = nf * 6 * E + (L + nc + 1) * 4 + nf * 4 + nc * (8 + 8 + E) + nc * (8 * E)
+    if vis:
+        cp += nf * 5 * E
+    out["residual"] = fp + cp
+    # LU-SGS, two sweeps: per entry neighbour / face / factor indices and the factors, face normal + area,
+    # neighbour state (u v w c2 hm) and dq once per cell per sweep, own res + spectral radii + dt + volume,
+    # dq / delta-flux writes, completion flags
+    lu = (L * 3 * 4 + L * 4 * E + 2 * nf * 4 * 8 + 2 * nc * 5 * E + 2 * nc * 5 * E
+          + 2 * nc * (7 * E + E + 8) + 2 * nc * 5 * E + 2 * nc * 5 * E + 2 * 2 * nc * 4)
+    out["lusgs"] = lu
+    # update: FP64 master state in and out (ghosts copied), dq, residual (monitor); working record out
+    out["update"] = nc * (5 * 8 + 5 * E + 5 * E + 5 * 8 + 7 * E) + nb * 2 * 5 * 8 + bnd
+    if sa:
+        sb = nb * (8 + 2 * E + 5 * 8 + 3 * 8 + 4 + 8 + 2 * E)
+        vg = nt * E + nc * (2 * E + E) + nf * (4 * 8 + 8) + (L + nc + 1) * 4 + nc * 4 * 8 + nc * (E + 3 * E)
+        sf = nt * (4 * E + 3 * E + 4 * 8) + nf * (7 * 8 + 8) + nf * 6 * E + L * E
+        sc = nc * (6 * E + 3 * E + 3 * E + E + 8 + E + 8) + nf * 6 * E + (L + nc + 1) * 4 + nf * 4 + nc * 2 * E
+        out["sa_residual"] = 2 * sb + vg + sf + sc
+        out["sa_lusgs"] = L * 2 * 4 + L * E + 2 * nc * 2 * E + 2 * nc * E + 2 * nc * E + 2 * nc * E + 2 * 2 * nc * 4
+        out["sa_update"] = nc * (8 + E + 8 + E) + sb
     out["iteration"] = sum(out.values())
     return out
 
 
-def run_phx(args, rank, world):
+def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=False):
     import torch
 
     from phenlei_b200 import solver as S
@@ -175,8 +220,12 @@ def run_phx(args, rank, world):
     torch.cuda.set_device(dev)
     wl = workloads()[args.workload]
     t0 = time.time()
-    m = wl["mesh"]()
-    s = S.NSSolverUnstruct(m, precision=args.precision, **wl["params"])
+    params = dict(wl["params"])
+    if mlp_blob is not None:
+        params["sa_source"] = "mlp_fallback"
+    s = S.NSSolverUnstruct(m, precision=precision, wall_dist=wd, **params)
+    if mlp_blob is not None:
+        s.set_mlp_blob(mlp_blob)
     stream = torch.cuda.current_stream()
     s.set_stream(stream.cuda_stream)
     setup_s = time.time() - t0
@@ -203,6 +252,9 @@ def run_phx(args, rank, world):
     phase_ms = {}
     names = [("boundary", s.Boundary), ("gradient_limiter", s.ComputeGradientAndLimiter),
              ("residual", s.UpdateResiduals), ("lusgs", s.LUSGS), ("update", s.UpdateFlowField)]
+    if wl["params"].get("viscousType", 0) == 3:
+        names += [("sa_residual", s.TurbUpdateResiduals), ("sa_lusgs", s.TurbLUSGS),
+                  ("sa_update", s.TurbUpdateFlowField)]
     reps = max(1, min(args.steps, 10))
     acc = {n: 0.0 for n, _ in names}
     for _ in range(reps):
@@ -215,6 +267,28 @@ def run_phx(args, rank, world):
             b.synchronize()
             acc[n] += a.elapsed_time(b)
     phase_ms = {n: v / reps for n, v in acc.items()}
+    forces = s.AirForceCoef() if params.get("viscousType", 0) > 0 else None
+    mlp_info = None
+    if mlp_blob is not None:
+        mlp_info = {"cells_learned": s.mlp_cells()}
+    if train:
+        # training set of the learned SA source: features and exact targets of
+        # this run's current state, a seeded subsample of 2M cells, 20 epochs,
+        # batch 8192, Adam lr 1e-3 (the trainer runs on this GPU)
+        f, t, _, _ = s.capture_sa_samples()
+        rng = np.random.default_rng(0)
+        if len(t) > 2_000_000:
+            sel = rng.choice(len(t), 2_000_000, replace=False)
+            f, t = f[sel], t[sel]
+        t1 = time.perf_counter()
+        loss = s.train_sa_mlp(f, t, epochs=20, batch=8192, lr=1e-3, seed=0)
+        mlp_info = {"samples": int(len(t)), "epochs": 20, "batch": 8192, "final_loss": loss,
+                    "train_s": round(time.perf_counter() - t1, 2), "blob": s.mlp_blob()}
+    if not e2e:
+        res = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=None, nc=nc, mesh=m,
+                   hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info)
+        s.close()
+        return res
     # end-to-end through the C ABI with pinned host buffers
     qh = torch.empty((5, s.nt), dtype=torch.float64).pin_memory()
     qh.copy_(torch.from_numpy(s.get(S.PHX_Q)))
@@ -231,7 +305,7 @@ def run_phx(args, rank, world):
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t1) / e2e_steps
     res = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=e2e_s, nc=nc, mesh=m,
-               hist=hist, setup_s=setup_s, nt=s.nt)
+               hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info)
     s.close()
     return res
 
@@ -244,8 +318,9 @@ def cpu_baseline(args, wl_name, sample_budget_s=20.0):
     from phenlei_b200 import mesh as M
 
     wl = workloads()[wl_name]
-    m = M.channel_bump(128, 46, 32, thickness=0.08, wall_spacing=0.001) if "16M" in wl_name else wl["mesh"]()
-    o = Oracle(m, wl["params"])
+    m = (M.channel_bump(128, 46, 32, thickness=0.08, wall_spacing=0.001, prism_layers=15 if "sa" in wl_name else 0)
+         if "16M" in wl_name else wl["mesh"]())
+    o = Oracle(m, wl["params"], wall_dist=M.wall_distance(m) if wl.get("wall_dist") else None)
     o.iterate(1)
     n = 0
     t0 = time.perf_counter()
@@ -264,7 +339,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="phx", choices=["phx", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison run of a mixed run")
+    ap.add_argument("--exact-source", action="store_true", help="mixed SA runs keep the exact SA source")
+    ap.add_argument("--save-mlp", default=None, help="write the trained learned-source model (.npy)")
+    ap.add_argument("--mlp-blob", default=None, help="use this learned-source model (.npy) instead of training one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -289,7 +368,30 @@ def main():
         import datetime
 
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
-    r = run_phx(args, rank, world)
+    from phenlei_b200 import mesh as M
+
+    if world == 1:
+        import torch
+
+        torch.cuda.set_device(0)
+    m = wl["mesh"]()
+    wd = M.wall_distance(m) if wl.get("wall_dist") else None
+    sa = wl["params"].get("viscousType", 0) == 3
+    r64 = None
+    blob = None
+    if args.mlp_blob:
+        blob = np.load(args.mlp_blob).astype(np.float32)
+    if args.precision == "mixed" and not args.no_fp64_arm:
+        # the headline ratio: mixed path (with the learned SA source on SA
+        # workloads) against the plain FP64 path on the same mesh; the FP64
+        # arm runs first and its final state trains the learned source
+        r64 = run_phx(args, rank, world, "fp64", m, wd, e2e=False,
+                      train=sa and not args.exact_source and blob is None)
+        if r64["mlp"]:
+            blob = r64["mlp"].pop("blob")
+            if args.save_mlp and rank == 0:
+                np.save(args.save_mlp, blob)
+    r = run_phx(args, rank, world, args.precision, m, wd, mlp_blob=blob)
     ms = r["ms"]
     if world > 1:
         import torch
@@ -302,7 +404,8 @@ def main():
     per_gpu = nc * args.steps / (ms / 1e3) / 1e6
     value = per_gpu * world
     peak, peak_kind = measured_peaks()
-    kb = kernel_bytes(r["mesh"], args.precision)
+    kb = kernel_bytes(r["mesh"], args.precision, wl["params"].get("viscousType", 0),
+                      wl["params"].get("gradientName", "ggcell"))
     phase = r["phase_ms"]
     dom = max(phase, key=phase.get)
     achieved = kb[dom] / (phase[dom] / 1e3) / 1e9
@@ -327,6 +430,22 @@ def main():
                 "h2d_bytes_per_step": 5 * 8 * r["nt"], "d2h_bytes_per_step": 5 * 8 * r["nt"] + 8},
         "residual_last": float(r["hist"][-1]) if len(r["hist"]) else None,
     }
+    if r64 is not None:
+        v64 = nc * args.steps / (r64["ms"] / 1e3) / 1e6 * world
+        line["fp64_arm"] = {"value": round(v64, 3), "ms_per_step": round(r64["ms"] / args.steps, 4),
+                            "phase_ms": {k: round(v, 4) for k, v in r64["phase_ms"].items()},
+                            "residual_last": float(r64["hist"][-1]) if len(r64["hist"]) else None}
+        line["speedup_vs_fp64"] = round(value / v64, 3)
+        if r["forces"] and r64["forces"]:
+            line["accuracy_vs_fp64"] = {"dCL": abs(r["forces"]["CL"] - r64["forces"]["CL"]),
+                                        "dCD": abs(r["forces"]["CD"] - r64["forces"]["CD"]),
+                                        "CL_fp64": r64["forces"]["CL"], "CD_fp64": r64["forces"]["CD"],
+                                        "after_iterations": args.warmup + args.steps}
+    line["config"]["sa_source"] = (("learned (MLP, exact outside its hull)" if blob is not None else "exact")
+                                   if sa else None)
+    if blob is not None:
+        line["mlp"] = dict((r64 or {}).get("mlp") or {"loaded": args.mlp_blob}, cells_learned_per_iteration=round(
+            r["mlp"]["cells_learned"] / (args.warmup + args.steps + max(1, min(args.steps, 10))), 1))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.workload)
     if rank == 0:

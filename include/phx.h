@@ -64,6 +64,7 @@ extern "C" {
 #define PHX_VIST 12      /* eddy viscosity [nTotal] ("vist") */
 #define PHX_RES_TURB 13  /* SA residual [nTotal] */
 #define PHX_GEOM 14      /* geometry, see phx_get_geometry */
+#define PHX_SA_SRC 15    /* SA source per unit volume used by the last SA residual [nCell] (learned-source runs) */
 
 typedef struct phx_ctx phx_ctx;
 
@@ -114,6 +115,8 @@ typedef struct {
     double muoo;                /* SA free-stream nu~ / nu */
     double turbCFLScale;
     int32_t sa_source;          /* 0 exact SA source, 1 MLP, 2 MLP with exact fallback */
+    double turbSkewnessAngle;   /* SA diffusion skewness switch, degrees */
+    double freeStreamViscosity; /* eddy viscosity of far-field inflow ghosts (SA) */
 } phx_params;
 
 /* Fills `p` with the reference's defaults for every key. */
@@ -174,6 +177,46 @@ int phx_ns_lusgs(phx_ctx *ctx);
  * Replaces NSSolverUnstruct::UpdateFlowField (:14587) and SolutionFix (:14509). */
 int phx_ns_update(phx_ctx *ctx);
 
+/* Spalart-Allmaras step (viscousType = 3), run after phx_ns_update of the
+ * same outer iteration, as Simulation::SolveSteady orders the solvers
+ * (Main/src/Simulation.cpp:1527-1560).
+ * phx_sa_boundary replaces TurbSolverUnstr::Boundary
+ * (CFD/TurbSolver/src/TurbSolverUnstr.cpp:5919), after the NS PostSolve
+ * boundary of the updated NS state (Controller::PostSolve,
+ * CFD/Solver/src/Controller.cpp:5063).
+ * phx_sa_residual replaces Controller::UpdateResiduals for TURB_SOLVER:
+ * Viscosity (:6910), GetGradientField (:8652), TurbSolver::UpdateResiduals
+ * (CFD/TurbSolver/src/TurbSolver.cpp:316: InitSpectrum :1025, SourceFlux
+ * :2342, InviscidFlux :5187, ViscousFlux :3856) and Diagonal (:4675).
+ * phx_sa_lusgs replaces SolveLUSGSForward / Backward (:1400, :1521).
+ * phx_sa_update replaces UpdateFlowField (:1180) and the PostSolve boundary. */
+int phx_sa_boundary(phx_ctx *ctx);
+int phx_sa_residual(phx_ctx *ctx);
+int phx_sa_lusgs(phx_ctx *ctx);
+int phx_sa_update(phx_ctx *ctx);
+
+/* Learned SA source (sa_source = 1: the MLP for every cell with nu~ > 0;
+ * 2: the MLP inside its training hull, the exact source outside; the exact
+ * source is always used for nu~ <= 0).  The MLP replaces production - wall
+ * destruction of SourceFluxOneEquationOriginal (TurbSolverUnstr.cpp:2702);
+ * the implicit part of the source stays exact.
+ * phx_sa_capture writes, for every cell with nu~ > 0 after an SA residual,
+ * the 6 raw input features ([count][6]) and the target of the exact source,
+ * and optionally (non-NULL) each sample's reference cell number and the scale
+ * that turns a network output into a source (source = target * scale).
+ * phx_mlp_train trains the 6-64-64-64-1 SiLU network on the GPU (Adam, MSE;
+ * seeded) and installs it; phx_mlp_get / phx_mlp_set move the model as a flat
+ * float blob of phx_mlp_blob_size() values (weights, normalisation, hull).
+ * phx_mlp_cells returns the running count of cells that used the MLP. */
+int phx_sa_capture(phx_ctx *ctx, float *features, float *targets, int32_t *cells, float *scales, int64_t capacity,
+                   int64_t *count);
+int phx_mlp_train(phx_ctx *ctx, const float *features, const float *targets, int64_t n, int epochs, int batch,
+                  double lr, uint64_t seed, double *final_loss);
+int phx_mlp_get(phx_ctx *ctx, float *blob, int64_t n);
+int phx_mlp_set(phx_ctx *ctx, const float *blob, int64_t n);
+int64_t phx_mlp_blob_size(void);
+int phx_mlp_cells(phx_ctx *ctx, uint64_t *count);
+
 /* nsteps outer iterations of the NS solver (and the SA solver when
  * viscousType = 3): the sequence of Controller::Relaxation with tscheme =
  * LU_SGS (Controller.cpp:549-587), driven as Simulation::SolveSteady
@@ -181,6 +224,14 @@ int phx_ns_update(phx_ctx *ctx);
  * step, the residual monitor of NSSolverUnstruct::GetResidual (:14258,
  * API/Physics/src/Residual.cpp:534): sqrt(sum res_rho^2 / nCell). */
 int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist);
+
+/* Wall force sums of the current state (NSSolverUnstruct::AirForceCoefParts,
+ * CFD/NSSolver/src/NSSolverUnstruct.cpp:16026, all solid walls, torque
+ * reference at the origin): out = CA_f CA_p CN_f CN_p CZ_f CZ_p cpx cpy cpz
+ * Cl_f Cl_p Cn_f Cn_p Cm_f Cm_p 0, FP64 device reduction.  CL and CD follow
+ * as in Force.cpp:441-536: scale by 1 / forceReferenceArea, then
+ * CL = -sin(a) CFx + cos(a) CFy, CD = cos(a) cos(b) CFx + sin(a) cos(b) CFy + sin(b) CFz. */
+int phx_forces(phx_ctx *ctx, double out[16]);
 
 /* Residual monitor of the current res, per equation: out[m] =
  * sqrt(sum res_m^2 / nCell) (FP64 device reduction). */

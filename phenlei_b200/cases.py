@@ -28,6 +28,10 @@ EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "v
 LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, refDimensionalTemperature=288.15,
                prl=0.72, wallTemperature=-1.0)
 
+# Config 5 flow: transonic bump, Spalart-Allmaras, Re 1e7 per unit length.
+SA_BUMP = dict(EULER_BUMP, viscousType=3, refMachNumber=0.8, refReNumber=1.0e7, refDimensionalTemperature=288.15,
+               prl=0.72, prt=0.9, wallTemperature=-1.0, muoo=3.0, CFLEnd=20.0)
+
 
 def freestream(params: dict) -> np.ndarray:
     """Non-dimensional free-stream primitive state (PerfectGas::ComputeReferencePrimitive,

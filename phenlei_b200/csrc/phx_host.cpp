@@ -12,8 +12,22 @@
 #include <vector>
 
 #include "phx_internal.h"
+#include "phx_mlp.h"
+
+namespace phx {
+int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch, float lr, unsigned long long seed,
+              MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float &tscale, double &lastLoss,
+              cudaStream_t s);
+void mlp_pack(const MlpHostWeights &w, std::vector<uint16_t> &w1c, std::vector<uint16_t> &w2c,
+              std::vector<uint16_t> &w3c);
+}  // namespace phx
 
 using namespace phx;
+
+// Flat model blob of phx_mlp_get / phx_mlp_set: weights (w1 b1 w2 b2 w3 b3 w4
+// b4, row-major [out][in]), then mean, 1/std, hull lo, hull hi (6 each), target scale.
+static constexpr int kMlpWeightFloats = sizeof(MlpHostWeights) / sizeof(float);
+static constexpr int kMlpBlobFloats = kMlpWeightFloats + 4 * kMlpIn + 1;
 
 struct phx_ctx {
     int device = 0;
@@ -33,6 +47,17 @@ struct phx_ctx {
     int cur = 0;
     Work<double> w64{};
     Work<float> w32{};
+    TurbWork<double> t64{};
+    TurbWork<float> t32{};
+    bool sa = false;
+    // learned SA source
+    bool mlpReady = false;
+    MlpDev mlp{};
+    std::vector<float> mlpBlob;
+    __nv_bfloat16 *mlpW = nullptr;          // w1c | w2c | w3c
+    float *mlpF = nullptr;                  // b1 | b2 | b3 | w4
+    unsigned long long *nmlp = nullptr;     // cells that used the learned source (running count)
+    double *forces = nullptr;               // [16] wall force sums
     Reduce *red = nullptr;
     int *neglist = nullptr;
     double *tmp = nullptr;                // [5][nTotal] staging buffer in the reference's order
@@ -303,8 +328,11 @@ void lsq_weights(const HostGrid &h, const std::vector<double> *G, std::vector<do
 
 // Geometry switches of ComputeVisflux (NSSolverUnstruct.cpp:13147-13236) per
 // reference face: bit 0 when both centre angles exceed skewnessAngle, bit 1
-// when both are positive and |dL|, |dR| > TINY.
-std::vector<uint8_t> viscous_flags(const HostGrid &h, const std::vector<double> *G, double skewAngle)
+// when both are positive and |dL|, |dR| > TINY; bit 2 for the SA diffusion
+// (TurbSolverUnstr::ComputeVisflux, TurbSolverUnstr.cpp:4520-4530): both above
+// turbSkewnessAngle and |dL|, |dR| > TINY.
+std::vector<uint8_t> viscous_flags(const HostGrid &h, const std::vector<double> *G, double skewAngle,
+                                   double turbSkewAngle)
 {
     const int nc = h.nCell, nb = h.nBFace, nf = h.nFace;
     std::vector<uint8_t> vf(nf, 0);
@@ -326,6 +354,7 @@ std::vector<uint8_t> viscous_flags(const HostGrid &h, const std::vector<double> 
         uint8_t b = 0;
         if (a1 > skewAngle && a2 > skewAngle) b |= 1;
         if (a1 > 0.0 && a2 > 0.0 && std::fabs(dL) > kSmall && std::fabs(dR) > kSmall) b |= 2;
+        if (a1 > turbSkewAngle && a2 > turbSkewAngle && std::fabs(dL) > kSmall && std::fabs(dR) > kSmall) b |= 4;
         vf[f] = b;
     }
     return vf;
@@ -384,6 +413,57 @@ bool limiter_zeroed(int bcType)
 {
     // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775
     return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW;
+}
+
+// Viscosity record of a laminar run: eddy viscosity 0, laminar viscosity of the
+// NS step (read by the wall forces).
+template <class T>
+int make_visc(phx_ctx *ctx, Work<T> &w)
+{
+    const size_t nt = ctx->nTotal;
+    int r = dalloc(ctx, &w.trec, nt * kTr);
+    if (r) return r;
+    std::vector<T> rec(nt * kTr, T(0));
+    for (size_t i = 0; i < nt; ++i) rec[i * kTr + 2] = T(1);
+    PHX_CUDA(ctx, cudaMemcpy(w.trec, rec.data(), sizeof(T) * nt * kTr, cudaMemcpyHostToDevice));
+    return PHX_OK;
+}
+
+// Spalart-Allmaras arrays: nu~ of the free stream everywhere (TurbSolverUnstr::
+// InitFlowAsRestart, TurbSolverUnstr.cpp:910-930), eddy viscosity 0 and laminar
+// viscosity 1 until the first NS step forms it (NSSolverUnstruct.cpp:685-695).
+template <class T>
+int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
+{
+    const size_t nt = ctx->nTotal, nc = ctx->nCell, nf = ctx->nFace;
+    int r = 0;
+    r |= dalloc(ctx, &w.trec, nt * kTr);
+    r |= dalloc(ctx, &t.qt64, nt);
+    r |= dalloc(ctx, &t.tgrad, nc * kTg);
+    r |= dalloc(ctx, &t.tcrec, nc * kTc);
+    r |= dalloc(ctx, &t.tface, nf * kTf);
+    r |= dalloc(ctx, &t.tcoef, 2 * nf);
+    r |= dalloc(ctx, &t.tdq, nc);
+    r |= dalloc(ctx, &t.tdfl, nc);
+    r |= dalloc(ctx, &t.tsrc, nc);
+    r |= dalloc(ctx, &ctx->nmlp, 1);
+    r |= dalloc(ctx, &ctx->mlpW, (size_t)kMlpH * kMlpK1 + 2 * (size_t)kMlpH * kMlpH);
+    r |= dalloc(ctx, &ctx->mlpF, 4 * (size_t)kMlpH);
+    if (r) return r;
+    PHX_CUDA(ctx, cudaMemset(ctx->nmlp, 0, sizeof(unsigned long long)));
+    const double nu = ctx->nc.nutInf;
+    std::vector<double> q(nt, nu);
+    std::vector<T> rec(nt * kTr);
+    for (size_t i = 0; i < nt; ++i) {
+        rec[i * kTr] = (T)nu;
+        rec[i * kTr + 1] = T(0);
+        rec[i * kTr + 2] = T(1);
+        rec[i * kTr + 3] = T(0);
+    }
+    PHX_CUDA(ctx, cudaMemcpy(t.qt64, q.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, cudaMemcpy(w.trec, rec.data(), sizeof(T) * nt * kTr, cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, cudaMemset(t.tcoef, 0, sizeof(T) * 2 * nf));
+    return PHX_OK;
 }
 
 template <class T>
@@ -451,6 +531,8 @@ void phx_default_params(phx_params *p)
     p->muoo = 3.0;
     p->turbCFLScale = 1.0;
     p->sa_source = 0;
+    p->turbSkewnessAngle = 0.0;
+    p->freeStreamViscosity = 1.0e-3;
 }
 
 int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out)
@@ -464,9 +546,13 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         gd->n_cell + gd->n_bface > 0x3fffffffLL || gd->n_face > 0x3fffffffLL)
         return PHX_ERR_ARG;
     if (prm->precision != PHX_FP64 && prm->precision != PHX_MIXED) return PHX_ERR_ARG;
-    // inviscid and laminar; laminar with adiabatic walls (wallTemperature <= 0)
-    if (prm->viscousType != 0 && prm->viscousType != 1) return PHX_ERR_ARG;
-    if (prm->viscousType == 1 && (prm->wallTemperature > 0.0 || prm->refReNumber <= 0.0)) return PHX_ERR_ARG;
+    // inviscid, laminar and Spalart-Allmaras; adiabatic walls (wallTemperature <= 0);
+    // SA needs the wall distance of every cell
+    if (prm->viscousType != 0 && prm->viscousType != 1 && prm->viscousType != 3) return PHX_ERR_ARG;
+    if (prm->viscousType != 0 && (prm->wallTemperature > 0.0 || prm->refReNumber <= 0.0)) return PHX_ERR_ARG;
+    if (prm->viscousType == 3 && (!gd->wall_dist || prm->sa_source < 0 || prm->sa_source > 2 ||
+                                  prm->turbCFLScale <= 0.0))
+        return PHX_ERR_ARG;
     if ((prm->gradientName != 0 && prm->gradientName != 1) || prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
@@ -474,6 +560,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     phx_ctx *ctx = new phx_ctx();
     ctx->prm = *prm;
     ctx->mixed = prm->precision == PHX_MIXED;
+    ctx->sa = prm->viscousType == 3;
     cudaGetDevice(&ctx->device);
     cudaDeviceGetAttribute(&ctx->numSMs, cudaDevAttrMultiProcessorCount, ctx->device);
 
@@ -629,6 +716,28 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     std::vector<int> fe_off, fe_nb, fe_f, fe_c, be_off, be_nb, be_f, be_c;
     entries(fwd_cells, true, fe_off, fe_nb, fe_f, fe_c);
     entries(bwd_cells, false, be_off, be_nb, be_f, be_c);
+    // per position {cell, entry count} and the entries padded to one lane group
+    // (kSweepGroup slots; neighbour -1 on unused slots), so a lane reads its
+    // entry with one load and no offset lookup
+    auto pack = [&](const std::vector<int> &cells, const std::vector<int> &eoff, const std::vector<int> &enb,
+                    const std::vector<int> &ef, const std::vector<int> &ec, std::vector<int2> &pinfo,
+                    std::vector<int4> &ent) {
+        const size_t npos = cells.size();
+        pinfo.resize(npos);
+        ent.assign(npos * kSweepGroup, make_int4(-1, 0, 0, 0));
+        for (size_t i = 0; i < npos; ++i) {
+            const int n = eoff[i + 1] - eoff[i];
+            pinfo[i] = make_int2(cells[i], n);
+            for (int k = 0; k < n; ++k) {
+                const int e = eoff[i] + k;
+                ent[i * kSweepGroup + k] = make_int4(enb[e], ef[e], ec[e], 0);
+            }
+        }
+    };
+    std::vector<int2> fwd_pinfo, bwd_pinfo;
+    std::vector<int4> fwd_ent, bwd_ent;
+    pack(fwd_cells, fe_off, fe_nb, fe_f, fe_c, fwd_pinfo, fwd_ent);
+    pack(bwd_cells, be_off, be_nb, be_f, be_c, bwd_pinfo, bwd_ent);
 
     // boundary classification (storage face order)
     std::vector<int32_t> bkind(nb), btype(nb);
@@ -659,7 +768,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     }
     std::vector<uint8_t> vflag(nf, 0);
     if (prm->viscousType) {
-        const std::vector<uint8_t> vref = viscous_flags(h, ctx->geom, prm->skewnessAngle);
+        const std::vector<uint8_t> vref = viscous_flags(h, ctx->geom, prm->skewnessAngle, prm->turbSkewnessAngle);
         for (int fs = 0; fs < nf; ++fs) vflag[fs] = vref[forder[fs]];
     }
     std::vector<double> lsqs(prm->gradientName == 1 ? (size_t)nc * 8 : 8, 0.0);
@@ -719,6 +828,12 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     k.cp = 1.0 / ((prm->refGama - 1.0) * (prm->refMachNumber * prm->refMachNumber));
     k.tsuth = prm->tsuth / prm->refDimensionalTemperature;
     k.skewAngle = prm->skewnessAngle;
+    // Param_TurbSolver::Init (CFD/TurbSolver/src/Param_TurbSolver.cpp:249-256):
+    // nu~ of the free stream = muoo / (rho_inf * turb_cmu + SMALL), turb_cmu = 1
+    k.nutInf = prm->muoo / (k.primInf[0] * 1.0 + kSmall);
+    k.vistInf = prm->freeStreamViscosity;
+    k.turbCflScale = prm->turbCFLScale;
+    k.saSource = prm->viscousType == 3 ? prm->sa_source : 0;
 
     // device grid
     DevGrid &g = ctx->g;
@@ -728,6 +843,11 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     g.nFwdPos = (int)fwd_cells.size(); g.nBwdPos = (int)bwd_cells.size();
     g.walldist = nullptr;
     int rc = 0;
+    if (ctx->sa) {
+        std::vector<double> wd(nc);
+        for (int i = 0; i < nc; ++i) wd[i] = gd->wall_dist[ord[i]];
+        rc |= upload(ctx, &g.walldist, wd);
+    }
     rc |= upload(ctx, &g.lr, lr);
     rc |= upload(ctx, &g.frec, frec);
     rc |= upload(ctx, &g.vflag, vflag);
@@ -741,18 +861,10 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= upload(ctx, &g.bkind, bkind);
     rc |= upload(ctx, &g.btype, btype);
     rc |= upload(ctx, &g.farfield_adj, ffadj);
-    rc |= upload(ctx, &g.fwd_cells, fwd_cells);
-    rc |= upload(ctx, &g.fwd_off, fwd_off);
-    rc |= upload(ctx, &g.fwd_eoff, fe_off);
-    rc |= upload(ctx, &g.fwd_enb, fe_nb);
-    rc |= upload(ctx, &g.fwd_ef, fe_f);
-    rc |= upload(ctx, &g.fwd_ec, fe_c);
-    rc |= upload(ctx, &g.bwd_cells, bwd_cells);
-    rc |= upload(ctx, &g.bwd_off, bwd_off);
-    rc |= upload(ctx, &g.bwd_eoff, be_off);
-    rc |= upload(ctx, &g.bwd_enb, be_nb);
-    rc |= upload(ctx, &g.bwd_ef, be_f);
-    rc |= upload(ctx, &g.bwd_ec, be_c);
+    rc |= upload(ctx, &g.fwd_pinfo, fwd_pinfo);
+    rc |= upload(ctx, &g.fwd_ent, fwd_ent);
+    rc |= upload(ctx, &g.bwd_pinfo, bwd_pinfo);
+    rc |= upload(ctx, &g.bwd_ent, bwd_ent);
     rc |= dalloc(ctx, &ctx->q64[0], (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->q64[1], (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->tmp, (size_t)5 * nt);
@@ -763,6 +875,9 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     if (!rc && (cudaMemset(ctx->flagF, 0, sizeof(int) * nc) != cudaSuccess ||
                 cudaMemset(ctx->flagB, 0, sizeof(int) * nc) != cudaSuccess)) rc = PHX_ERR_CUDA;
     if (!rc) rc = ctx->mixed ? make_work(ctx, ctx->w32, limInit) : make_work(ctx, ctx->w64, limInit);
+    if (!rc && ctx->sa) rc = ctx->mixed ? make_turb(ctx, ctx->w32, ctx->t32) : make_turb(ctx, ctx->w64, ctx->t64);
+    else if (!rc && prm->viscousType) rc = ctx->mixed ? make_visc(ctx, ctx->w32) : make_visc(ctx, ctx->w64);
+    if (!rc) rc = dalloc(ctx, &ctx->forces, 16);
     if (!rc && cudaMemset(ctx->red, 0, sizeof(Reduce)) != cudaSuccess) rc = PHX_ERR_CUDA;
     if (rc) {
         const int code = rc < 0 ? rc : PHX_ERR_CUDA;
@@ -812,6 +927,10 @@ int check_launch(phx_ctx *ctx, int n = 1)
     return PHX_OK;
 }
 
+template <class T> const TurbWork<T> &turb_of(const phx_ctx *ctx);
+template <> const TurbWork<double> &turb_of<double>(const phx_ctx *ctx) { return ctx->t64; }
+template <> const TurbWork<float> &turb_of<float>(const phx_ctx *ctx) { return ctx->t32; }
+
 // Fills ctx->tmp with the selected array in the reference's order; returns the
 // number of rows and the row length (elements per row).
 template <class T>
@@ -831,6 +950,24 @@ int export_work(phx_ctx *ctx, const Work<T> &w, int which, int &rows, int &len)
     case PHX_INVSPEC: rows = 1; len = nc; launch_export<T>(g, w.crec, kC, 6, 1, 1, nc, ctx->tmp, nc, s); break;
     case PHX_VISSPEC: rows = 1; len = nc; launch_export<T>(g, w.crec, kC, 7, 1, 1, nc, ctx->tmp, nc, s); break;
     case PHX_DT: rows = 1; len = nt; launch_export<T>(g, w.dtraw, 1, 0, 1, 1, nc, ctx->tmp, nt, s); break;
+    case PHX_SA_SRC:
+        if (!ctx->sa || !ctx->nc.saSource) return fail(ctx, PHX_ERR_ARG, "PHX_SA_SRC needs the learned SA source");
+        rows = 1; len = nc;
+        launch_export<T>(g, turb_of<T>(ctx).tsrc, 1, 0, 1, 1, nc, ctx->tmp, nc, s);
+        break;
+    case PHX_Q_TURB:
+    case PHX_VISL:
+    case PHX_VIST:
+    case PHX_RES_TURB: {
+        if (!ctx->sa) return fail(ctx, PHX_ERR_ARG, "SA state selector on a context without the SA model");
+        const TurbWork<T> &t = turb_of<T>(ctx);
+        rows = 1; len = nt;
+        if (which == PHX_Q_TURB) launch_export<double>(g, t.qt64, 1, 0, 1, 1, nt, ctx->tmp, nt, s);
+        else if (which == PHX_VISL) launch_export<T>(g, w.trec, kTr, 2, 1, 1, nt, ctx->tmp, nt, s);
+        else if (which == PHX_VIST) launch_export<T>(g, w.trec, kTr, 1, 1, 1, nt, ctx->tmp, nt, s);
+        else launch_export<T>(g, t.tcrec, kTc, 0, 1, 1, nc, ctx->tmp, nt, s);
+        break;
+    }
     default: return fail(ctx, PHX_ERR_ARG, "unknown or unavailable state selector");
     }
     return check_launch(ctx, 2);
@@ -891,8 +1028,20 @@ static int get_state_impl(phx_ctx *ctx, int which, double *dst, int64_t n, bool 
 static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n, bool hostSide)
 {
     if (!ctx || !src) return PHX_ERR_ARG;
-    if (which != PHX_Q) return fail(ctx, PHX_ERR_ARG, "only the primitive state (PHX_Q) can be set");
     const int nt = ctx->nTotal;
+    if (which == PHX_Q_TURB) {
+        if (!ctx->sa) return fail(ctx, PHX_ERR_ARG, "SA state selector on a context without the SA model");
+        if (n != (int64_t)nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
+        PHX_CUDA(ctx, cudaMemcpyAsync(ctx->tmp, src, sizeof(double) * n, hostSide ? cudaMemcpyHostToDevice
+                                                                                 : cudaMemcpyDeviceToDevice, ctx->stream));
+        if (ctx->mixed) launch_import_turb<float>(ctx->g, ctx->tmp, ctx->t32, ctx->w32, ctx->stream);
+        else launch_import_turb<double>(ctx->g, ctx->tmp, ctx->t64, ctx->w64, ctx->stream);
+        int rc = check_launch(ctx);
+        if (rc) return rc;
+        PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return PHX_OK;
+    }
+    if (which != PHX_Q) return fail(ctx, PHX_ERR_ARG, "only PHX_Q and PHX_Q_TURB can be set");
     if (n != (int64_t)5 * nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
     PHX_CUDA(ctx, cudaMemcpyAsync(ctx->tmp, src, sizeof(double) * n, hostSide ? cudaMemcpyHostToDevice
                                                                              : cudaMemcpyDeviceToDevice, ctx->stream));
@@ -985,7 +1134,61 @@ int phx_ns_update(phx_ctx *ctx)
         launch_solution_fix<double>(ctx->g, ctx->nc, ctx->w64, qo, qn, ctx->red, ctx->neglist, ctx->stream);
     }
     ctx->cur = nxt;
-    return check_launch(ctx, 2);
+    // Controller::PostSolve (Controller.cpp:5063-5090): ghost states of the
+    // updated field (the SA step and exported states read them)
+    if (ctx->mixed) launch_boundary_post<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->stream);
+    else launch_boundary_post<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->stream);
+    return check_launch(ctx, 3);
+}
+
+int phx_sa_boundary(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (ctx->mixed) launch_sa_boundary<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->t32, ctx->stream);
+    else launch_sa_boundary<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->t64, ctx->stream);
+    return check_launch(ctx);
+}
+
+int phx_sa_residual(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_sa_residual needs the NS time step (phx_ns_residual)");
+    if (ctx->nc.saSource && !ctx->mlpReady)
+        return fail(ctx, PHX_ERR_STATE, "sa_source selects the learned source but no model is set (phx_mlp_train / phx_mlp_set)");
+    const MlpDev *mlp = ctx->nc.saSource ? &ctx->mlp : nullptr;
+    if (ctx->mixed)
+        launch_sa_residual<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->t32, ctx->red, mlp, ctx->nmlp,
+                                  ctx->numSMs, ctx->stream);
+    else
+        launch_sa_residual<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->t64, ctx->red, mlp, ctx->nmlp,
+                                   ctx->numSMs, ctx->stream);
+    return check_launch(ctx, mlp ? 6 : 5);
+}
+
+int phx_sa_lusgs(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    ctx->epoch += 1;
+    const int e = ctx->mixed ? launch_sa_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->red, ctx->flagF,
+                                                      ctx->flagB, ctx->epoch, ctx->numSMs, ctx->stream)
+                             : launch_sa_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->red, ctx->flagF,
+                                                       ctx->flagB, ctx->epoch, ctx->numSMs, ctx->stream);
+    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
+    return check_launch(ctx, 1);
+}
+
+int phx_sa_update(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (ctx->mixed) launch_sa_update<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->stream);
+    else launch_sa_update<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->stream);
+    int rc = check_launch(ctx);
+    if (rc) return rc;
+    return phx_sa_boundary(ctx);   // TURB PostSolve
 }
 
 static int relax_one(phx_ctx *ctx, double *dhist, int i)
@@ -998,6 +1201,11 @@ static int relax_one(phx_ctx *ctx, double *dhist, int i)
     if ((rc = phx_ns_lusgs(ctx))) return rc;
     if ((rc = phx_ns_update(ctx))) return rc;
     launch_finish_step(ctx->red, dhist, i, (double)ctx->nCell, ctx->stream);
+    if (ctx->sa) {
+        if ((rc = phx_sa_residual(ctx))) return rc;
+        if ((rc = phx_sa_lusgs(ctx))) return rc;
+        if ((rc = phx_sa_update(ctx))) return rc;
+    }
     return check_launch(ctx);
 }
 
@@ -1022,6 +1230,145 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
     PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
     if (red.error == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
+    return PHX_OK;
+}
+
+// --- learned SA source ----------------------------------------------------
+
+static int mlp_install(phx_ctx *ctx, const float *blob)
+{
+    MlpHostWeights w;
+    std::memcpy(&w, blob, sizeof(MlpHostWeights));
+    const float *norm = blob + kMlpWeightFloats;
+    std::vector<uint16_t> w1c, w2c, w3c;
+    mlp_pack(w, w1c, w2c, w3c);
+    std::vector<uint16_t> wall(w1c);
+    wall.insert(wall.end(), w2c.begin(), w2c.end());
+    wall.insert(wall.end(), w3c.begin(), w3c.end());
+    std::vector<float> fall;
+    fall.insert(fall.end(), w.b1, w.b1 + kMlpH);
+    fall.insert(fall.end(), w.b2, w.b2 + kMlpH);
+    fall.insert(fall.end(), w.b3, w.b3 + kMlpH);
+    fall.insert(fall.end(), w.w4, w.w4 + kMlpH);
+    PHX_CUDA(ctx, cudaMemcpy(ctx->mlpW, wall.data(), sizeof(uint16_t) * wall.size(), cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, cudaMemcpy(ctx->mlpF, fall.data(), sizeof(float) * fall.size(), cudaMemcpyHostToDevice));
+    MlpDev &m = ctx->mlp;
+    m.w1c = ctx->mlpW;
+    m.w2c = ctx->mlpW + kMlpH * kMlpK1;
+    m.w3c = ctx->mlpW + kMlpH * kMlpK1 + kMlpH * kMlpH;
+    m.b1 = ctx->mlpF;
+    m.b2 = ctx->mlpF + kMlpH;
+    m.b3 = ctx->mlpF + 2 * kMlpH;
+    m.w4 = ctx->mlpF + 3 * kMlpH;
+    m.b4 = w.b4;
+    for (int k = 0; k < kMlpIn; ++k) {
+        m.mean[k] = norm[k];
+        m.rstd[k] = norm[kMlpIn + k];
+        m.lo[k] = norm[2 * kMlpIn + k];
+        m.hi[k] = norm[3 * kMlpIn + k];
+    }
+    m.tscale = norm[4 * kMlpIn];
+    ctx->mlpBlob.assign(blob, blob + kMlpBlobFloats);
+    ctx->mlpReady = true;
+    return PHX_OK;
+}
+
+int phx_sa_capture(phx_ctx *ctx, float *features, float *targets, int32_t *cells, float *scales, int64_t capacity,
+                   int64_t *count)
+{
+    if (!ctx || !features || !targets || !count || capacity < 0) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_sa_capture needs a completed SA residual");
+    const int nc = ctx->nCell;
+    float *df = nullptr, *dt = nullptr, *dsc = nullptr;
+    int *dcl = nullptr;
+    unsigned long long *dn = nullptr;
+    int rc = 0;
+    rc |= dalloc(ctx, &df, (size_t)nc * kMlpIn);
+    rc |= dalloc(ctx, &dt, (size_t)nc);
+    rc |= dalloc(ctx, &dsc, (size_t)nc);
+    rc |= dalloc(ctx, &dcl, (size_t)nc);
+    rc |= dalloc(ctx, &dn, 1);
+    if (rc) return rc;
+    PHX_CUDA(ctx, cudaMemsetAsync(dn, 0, sizeof(unsigned long long), ctx->stream));
+    if (ctx->mixed) launch_mlp_capture<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, df, dt, dcl, dsc, nc, dn, ctx->stream);
+    else launch_mlp_capture<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, df, dt, dcl, dsc, nc, dn, ctx->stream);
+    rc = check_launch(ctx);
+    if (rc) return rc;
+    unsigned long long n = 0;
+    PHX_CUDA(ctx, cudaMemcpyAsync(&n, dn, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int64_t m = std::min<int64_t>((int64_t)n, capacity);
+    PHX_CUDA(ctx, cudaMemcpy(features, df, sizeof(float) * kMlpIn * (size_t)m, cudaMemcpyDeviceToHost));
+    PHX_CUDA(ctx, cudaMemcpy(targets, dt, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
+    if (cells) PHX_CUDA(ctx, cudaMemcpy(cells, dcl, sizeof(int) * (size_t)m, cudaMemcpyDeviceToHost));
+    if (scales) PHX_CUDA(ctx, cudaMemcpy(scales, dsc, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
+    // the staging buffers are released at once (they are not part of the context's resident state)
+    for (void *p : {(void *)df, (void *)dt, (void *)dsc, (void *)dcl, (void *)dn}) {
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), p));
+        cudaFree(p);
+    }
+    *count = m;
+    return PHX_OK;
+}
+
+int phx_mlp_train(phx_ctx *ctx, const float *features, const float *targets, int64_t n, int epochs, int batch,
+                  double lr, uint64_t seed, double *final_loss)
+{
+    if (!ctx || !features || !targets || n < 2 || epochs < 1 || batch < 1 || !(lr > 0.0)) return PHX_ERR_ARG;
+    std::vector<float> blob(kMlpBlobFloats);
+    MlpHostWeights w;
+    float *norm = blob.data() + kMlpWeightFloats;
+    float tscale = 1.0f;
+    double loss = 0.0;
+    const int e = mlp_train(features, targets, n, epochs, batch, (float)lr, seed, w, norm, norm + kMlpIn,
+                            norm + 2 * kMlpIn, norm + 3 * kMlpIn, tscale, loss, ctx->stream);
+    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("MLP training failed: ") + cudaGetErrorString((cudaError_t)e));
+    norm[4 * kMlpIn] = tscale;
+    std::memcpy(blob.data(), &w, sizeof(MlpHostWeights));
+    if (final_loss) *final_loss = loss;
+    return mlp_install(ctx, blob.data());
+}
+
+int phx_mlp_get(phx_ctx *ctx, float *blob, int64_t n)
+{
+    if (!ctx || !blob) return PHX_ERR_ARG;
+    if (!ctx->mlpReady) return fail(ctx, PHX_ERR_STATE, "no learned source model is set");
+    if (n != kMlpBlobFloats) return fail(ctx, PHX_ERR_ARG, "model blob size mismatch");
+    std::memcpy(blob, ctx->mlpBlob.data(), sizeof(float) * kMlpBlobFloats);
+    return PHX_OK;
+}
+
+int phx_mlp_set(phx_ctx *ctx, const float *blob, int64_t n)
+{
+    if (!ctx || !blob) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (n != kMlpBlobFloats) return fail(ctx, PHX_ERR_ARG, "model blob size mismatch");
+    return mlp_install(ctx, blob);
+}
+
+int64_t phx_mlp_blob_size(void) { return kMlpBlobFloats; }
+
+int phx_mlp_cells(phx_ctx *ctx, uint64_t *count)
+{
+    if (!ctx || !count) return PHX_ERR_ARG;
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    unsigned long long n = 0;
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    PHX_CUDA(ctx, cudaMemcpy(&n, ctx->nmlp, sizeof(n), cudaMemcpyDeviceToHost));
+    *count = n;
+    return PHX_OK;
+}
+
+int phx_forces(phx_ctx *ctx, double out[16])
+{
+    if (!ctx || !out) return PHX_ERR_ARG;
+    if (ctx->mixed) launch_forces<float>(ctx->g, ctx->nc, ctx->w32, ctx->q64[ctx->cur], ctx->forces, ctx->stream);
+    else launch_forces<double>(ctx->g, ctx->nc, ctx->w64, ctx->q64[ctx->cur], ctx->forces, ctx->stream);
+    int rc = check_launch(ctx);
+    if (rc) return rc;
+    PHX_CUDA(ctx, cudaMemcpyAsync(out, ctx->forces, sizeof(double) * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return PHX_OK;
 }
 

@@ -44,6 +44,13 @@ constexpr int kFlux = 16;  // face flux record: inviscid F0..4 (times area) | in
                            // spectral parts | pad | viscous F1..4 (times area; F0 is zero) | pad
 constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | viscous spectral term
 constexpr int kSweepPad = 4; // LU-SGS lane groups per warp: schedule levels are padded to this multiple
+constexpr int kSweepGroup = 8; // lanes (neighbour entries) per cell in the LU-SGS sweeps
+// Spalart-Allmaras records
+constexpr int kTr = 4;     // trec: nu~ | eddy viscosity | laminar viscosity of the NS step | pad
+constexpr int kTg = 4;     // tgrad: d nu~ / dx, dy, dz | pad
+constexpr int kTc = 4;     // tcrec: res_turb | spec_turb | pad
+constexpr int kTf = 8;     // tface: convective flux | diffusion flux1, flux2 | upwind Jacobians L, R |
+                           // diffusion spectral term | pad
 
 // Read-only device grid (FP64 metrics, connectivity, schedules), storage order.
 struct DevGrid {
@@ -58,19 +65,22 @@ struct DevGrid {
     // [nFace] viscous-flux geometry switches of ComputeVisflux: bit 0 = both
     // centre angles above skewnessAngle (project the cell values onto the
     // normal line), bit 1 = both angles positive and |dL|, |dR| > TINY (form
-    // the normal derivative); pure geometry, decided on the host
+    // the normal derivative), bit 2 = both angles above turbSkewnessAngle and
+    // |dL|, |dR| > TINY (the SA diffusion's normal derivative); pure geometry,
+    // decided on the host
     const uint8_t *vflag;
     const int *c2f_off, *c2f;    // faces of each cell, ordered by the reference face number
     const int *orig;             // [nTotal] reference number of each cell (ghost: nCell + reference face)
     const int32_t *bkind;        // [nBFace] BcKind
     const int32_t *btype;        // [nBFace] bcType
     const uint8_t *farfield_adj; // [nCell] 1 if the cell touches a limiter-zeroing boundary
-    // LU-SGS schedules: cells by level, and per schedule position the
-    // neighbours on the sweep's side (in the cell's face order) as entries
-    // eoff[i]..eoff[i+1]: neighbour, face (sign bit set when the normal points
-    // into the cell), and the index of the face use's factors (2 f + side).
-    const int *fwd_cells, *fwd_off, *fwd_eoff, *fwd_enb, *fwd_ef, *fwd_ec;
-    const int *bwd_cells, *bwd_off, *bwd_eoff, *bwd_enb, *bwd_ef, *bwd_ec;
+    // LU-SGS schedules, positions in level order (levels padded with idle
+    // positions): pinfo = {storage cell or -1, entry count}; ent = kSweepGroup
+    // slots per position, the neighbours on the sweep's side in the cell's face
+    // order: {neighbour (-1: unused slot), face (sign bit set when the normal
+    // points into the cell), index of the face use's factors (2 f + side), 0}.
+    const int2 *fwd_pinfo, *bwd_pinfo;
+    const int4 *fwd_ent, *bwd_ent;
     int nFwdLevels, nBwdLevels;
     int nFwdPos, nBwdPos;        // schedule positions incl. idle padding (-1 cells)
     int maxLevelWidth;           // widest LU-SGS level (cells)
@@ -98,6 +108,11 @@ struct NsConst {
     // cp = 1 / ((gamma - 1) M^2), Sutherland constant over the reference
     // temperature, skewness switch of the viscous flux (degrees)
     double oRe, oPrl, oPrt, cp, tsuth, skewAngle;
+    // Spalart-Allmaras (viscousType 3): free-stream nu~ and eddy viscosity of
+    // far-field inflow ghosts, turbCFLScale
+    double nutInf, vistInf, turbCflScale;
+    int saSource;                  // 0 exact source, 1 learned source (exact for nu~ <= 0), 2 learned inside its
+                                   // training hull, exact outside
 };
 
 // Working arrays of one precision T (double: FP64 path, float: mixed path).
@@ -111,6 +126,20 @@ struct Work {
     T *dtraw;       // [nCell] CFL * vol / spectral radius, before the ktmax clamp
     T *dqrec;       // [nTotal][kD] LU-SGS dq
     T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep
+    T *trec;        // [nTotal][kTr] SA variable, eddy and laminar viscosity (SA runs; else null)
+};
+
+// Spalart-Allmaras working arrays (one precision T; the FP64 master nu~ is qt64).
+template <class T>
+struct TurbWork {
+    double *qt64;   // [nTotal] master nu~
+    T *tgrad;       // [nCell][kTg] gradient of nu~
+    T *tcrec;       // [nCell][kTc] residual and spectral radius
+    T *tface;       // [nFace][kTf] face terms
+    T *tcoef;       // [2 nFace] LU-SGS matrix of each face use (side 0: left cell's view = mat_turbr)
+    T *tdq;         // [nCell] LU-SGS dq
+    T *tdfl;        // [nCell] forward delta flux
+    T *tsrc;        // [nCell] source computed by the learned-source kernel (sa_source != 0)
 };
 
 struct Reduce {
@@ -149,6 +178,39 @@ void launch_export(const DevGrid &g, const T *rec, int stride, int first, int co
 void launch_import_q(const DevGrid &g, const double *in, double *q64, cudaStream_t s);
 void launch_export_q(const DevGrid &g, const double *q64, double *out, cudaStream_t s);
 void launch_reset_reduce(Reduce *r, cudaStream_t s);
+// NS boundary after the update (Controller::PostSolve): ghost states only,
+// the laminar viscosity of the ghosts keeps its value of the NS step.
+template <class T>
+void launch_boundary_post(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s);
+// Spalart-Allmaras step (phx_sa.cu).
+template <class T>
+void launch_sa_boundary(const DevGrid &g, const NsConst &c, const double *q64, const Work<T> &w,
+                        const TurbWork<T> &t, cudaStream_t s);
+struct MlpDev;
+template <class T>
+void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, const Work<T> &w,
+                        const TurbWork<T> &t, Reduce *red, const MlpDev *mlp, unsigned long long *nmlp, int numSMs,
+                        cudaStream_t s);
+// Learned SA source (phx_mlp.cu): source of every cell into t.tsrc; training-sample capture.
+template <class T>
+void launch_mlp_source(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t,
+                       const MlpDev &mlp, Reduce *red, unsigned long long *nmlp, int numSMs, cudaStream_t s);
+template <class T>
+void launch_mlp_capture(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, float *feat,
+                        float *targ, int *cells, float *scales, long long cap, unsigned long long *count,
+                        cudaStream_t s);
+template <class T>
+int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
+                    int *flagF, int *flagB, int epoch, int numSMs, cudaStream_t s);
+template <class T>
+void launch_sa_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s);
+// Wall force sums (16 doubles, the last zero) of the current state.
+template <class T>
+void launch_forces(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *out,
+                   cudaStream_t s);
+// qt64[i] = in[orig[i]] and the working copy in trec, cells and ghosts.
+template <class T>
+void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t, const Work<T> &w, cudaStream_t s);
 void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s);
 
 }  // namespace phx

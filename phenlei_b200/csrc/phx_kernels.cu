@@ -10,69 +10,10 @@
 #include <stdlib.h>
 
 #include "phx_internal.h"
+#include "phx_device.cuh"
 #include "phx_physics.cuh"
 
 namespace phx {
-
-static constexpr int kThreads = 256;
-
-template <class T> __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
-// Loads of data written earlier in the same kernel by other blocks: bypass L1.
-template <class T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
-
-// Vector loads of 4- or 8-element records (16-byte aligned).
-__device__ __forceinline__ void ld4(const double *p, double *o)
-{
-    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
-    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-}
-__device__ __forceinline__ void ld4(const float *p, float *o)
-{
-    const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
-    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-}
-template <class T>
-__device__ __forceinline__ void ld8(const T *p, T *o) { ld4(p, o); ld4(p + 4, o + 4); }
-__device__ __forceinline__ void ld4cg(const double *p, double *o)
-{
-    const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
-    const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-}
-__device__ __forceinline__ void ld4cg(const float *p, float *o)
-{
-    const float4 a = __ldcg(reinterpret_cast<const float4 *>(p));
-    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-}
-template <class T>
-__device__ __forceinline__ void ld8cg(const T *p, T *o) { ld4cg(p, o); ld4cg(p + 4, o + 4); }
-__device__ __forceinline__ void st4(double *p, const double *v)
-{
-    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
-    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
-}
-__device__ __forceinline__ void st4(float *p, const float *v)
-{
-    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
-}
-template <class T>
-__device__ __forceinline__ void st8(T *p, const T *v) { st4(p, v); st4(p + 4, v + 4); }
-
-// Writes state, c2 = |gamma p / rho| and total enthalpy of a cell record
-// (slot 7, the limiter, is left untouched).  c2 and the enthalpy are the
-// per-cell factors MXDQ_STD forms (Jacobian.cpp:22-23, PerfectGas.cpp:384-394).
-template <class T>
-__device__ __forceinline__ void put_state(T *rec, const T *q, T gm)
-{
-    const T c2 = fabs(gm * q[4] / q[0]);
-    const T hm = (gm / (gm - T(1))) * (q[4] / q[0]) + T(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-    T v[4] = {q[0], q[1], q[2], q[3]};
-    st4(rec, v);
-    rec[4] = q[4];
-    rec[5] = c2;
-    rec[6] = hm;
-}
 
 // ---------------------------------------------------------------------------
 // Boundary: ghost-cell state per boundary face (NSSolverUnstruct::Boundary,
@@ -81,7 +22,8 @@ __device__ __forceinline__ void put_state(T *rec, const T *q, T gm)
 // Computed in FP64 from the FP64 master state.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, Work<T> w)
+__global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, Work<T> w,
+                                                            bool writeVisl)
 {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nBFace) return;
@@ -139,13 +81,23 @@ __global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c
         t[k] = (T)o[k];
     }
     put_state<T>(w.qrec + (size_t)re * kQ, t, (T)c.gama);
+    // laminar viscosity of the ghost for the SA step (NS ComputeViscousCoeff
+    // covers the ghosts, NSSolverUnstruct.cpp:6733-6745)
+    if (w.trec && writeVisl) w.trec[(size_t)re * kTr + 2] = sutherland(temperature(t, (T)c.coefState), (T)c.tsuth);
 }
 
 template <class T>
 void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s)
 {
     if (g.nBFace == 0) return;
-    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w);
+    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w, true);
+}
+
+template <class T>
+void launch_boundary_post(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s)
+{
+    if (g.nBFace == 0) return;
+    boundary_kernel<T><<<(g.nBFace + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w, false);
 }
 
 template <class T>
@@ -164,14 +116,6 @@ void launch_sync_qrec(const DevGrid &g, const NsConst &c, const double *q64, con
 {
     sync_qrec_kernel<T><<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, q64, w);
 }
-
-// Temperature (ComputeGamaAndTemperature, NSSolverUnstruct.cpp:4717-4730) and
-// Sutherland viscosity (ComputeViscousCoefficientWithoutChemical, :6722-6747),
-// formed on the fly from a cell record wherever they are needed.
-template <class T>
-__device__ __forceinline__ T temperature(const T *q, T coef) { return q[4] / (coef * q[0]); }
-template <class T>
-__device__ __forceinline__ T sutherland(T t, T s) { return t * sqrt(t) * (T(1) + s) / (t + s); }
 
 // ---------------------------------------------------------------------------
 // Gradient + limiter, fused per cell:
@@ -273,6 +217,8 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
     if (kTemp) {
         gr[16] = gx[NV - 1]; gr[17] = gy[NV - 1]; gr[18] = gz[NV - 1]; gr[19] = T(0);
         st4(go + 16, gr + 16);
+        // laminar viscosity of this NS step, read by the SA step after the update
+        if (w.trec) w.trec[(size_t)cell * kTr + 2] = sutherland(vc[NV - 1], (T)c.tsuth);
     }
     T lim = T(1);
     if (c.limiter == 1) {
@@ -414,7 +360,7 @@ __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c,
     const T coef = (T)c.coefState, S = (T)c.tsuth;
     const T tl0 = temperature(qL, coef), tr0 = temperature(qR, coef);
     const T mul = T(0.5) * (sutherland(tl0, S) + sutherland(tr0, S));
-    const T mut = T(0);
+    const T mut = w.trec ? T(0.5) * (w.trec[(size_t)le * kTr + 1] + w.trec[(size_t)re * kTr + 1]) : T(0);
     // spectral radius / LU-SGS viscous factor
     {
         const double ds = fabs(nxs * (xr[0] - xl[0]) + nys * (xr[1] - xl[1]) + nzs * (xr[2] - xl[2]));
@@ -696,22 +642,6 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 // wait is bounded: a timeout sets Reduce::error and the kernel gives up.
 // The dq-independent MXDQ_STD factors were computed by the residual pass.
 // ---------------------------------------------------------------------------
-static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
-static constexpr int kSweepThreads = 256;
-static constexpr int kGroup = 8;                      // lanes per cell
-static_assert(kGroup * kSweepPad == 32, "one warp holds kSweepPad lane groups");
-
-__device__ __forceinline__ int ld_acquire(const int *p)
-{
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(int *p, int v)
-{
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // Ghost-cell dq of boundary face f from the owner's forward dq
 // (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810; SetSymmBCGhostDQLUSGS
@@ -758,29 +688,26 @@ __device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, con
 // spins while a sibling in the same warp is ready to work, and every shuffle
 // uses the full warp mask.  pos >= nCell marks an idle group (the warp's trip
 // count is uniform).
+// The position's {cell, count} and this lane's entry were loaded one round
+// ahead by the caller (info, en); the next round's (ninfo, nen) are known here,
+// so their records are prefetched into L2 while this position waits.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
-                                               int *flagF, int *flagB, int epoch, double mindt, int pos, int lane,
-                                               int base)
+                                               int *flagF, int *flagB, int epoch, double mindt, int2 info, int4 en,
+                                               int2 ninfo, int4 nen, int lane, int base)
 {
     const int nc = g.nCell;
-    int cell = -1, e0 = 0, e1 = 0;
-    if (pos < (kForward ? g.nFwdPos : g.nBwdPos)) {
-        cell = (kForward ? g.fwd_cells : g.bwd_cells)[pos];
-        const int *eoff = kForward ? g.fwd_eoff : g.bwd_eoff;
-        e0 = eoff[pos];
-        e1 = eoff[pos + 1];
-    }
+    const int cell = info.x;
     const bool live = cell >= 0;
-    const int e = e0 + lane;
-    const bool has = live && e < e1;
+    const int e0 = 0, e1 = live ? info.y : 0;
+    const bool has = live && en.x >= 0;
     // dq-independent loads first: they overlap the waits below
     int nb = -1, f = 0;
     T sgn = T(1), nx = 0, ny = 0, nz = 0, area = 0, cf[4] = {0, 0, 0, 0}, qn[8];
     if (has) {
-        nb = (kForward ? g.fwd_enb : g.bwd_enb)[e];
-        const int fs = (kForward ? g.fwd_ef : g.bwd_ef)[e];
-        const int ec = (kForward ? g.fwd_ec : g.bwd_ec)[e];
+        nb = en.x;
+        const int fs = en.y;
+        const int ec = en.z;
         f = fs & 0x7fffffff;
         sgn = fs < 0 ? T(-1) : T(1);
         double fr[4];
@@ -809,6 +736,16 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         if ((spins & 1023) == 0 && __any_sync(0xffffffffu, ((volatile int *)&red->error)[0] != 0)) return false;
         if (spins > 8) __nanosleep(20);
         if (!ready) ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+    }
+    // next round's records into L2 (their entries arrived during the wait)
+    if (nen.x >= 0) {
+        prefetch_l2(g.frec + (size_t)(nen.y & 0x7fffffff) * kF);
+        prefetch_l2(w.coef + (size_t)nen.z * kCoef);
+        prefetch_l2(w.qrec + (size_t)nen.x * kQ);
+    }
+    if (lane == 0 && ninfo.x >= 0) {
+        prefetch_l2(w.crec + (size_t)ninfo.x * kC);
+        prefetch_l2(w.dtraw + ninfo.x);
     }
     T df[5] = {0, 0, 0, 0, 0};
     if (has) {
@@ -885,6 +822,34 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     return true;
 }
 
+// One sweep over the schedule: rounds of ngroups positions, the loads of
+// {cell, count} and of this lane's entry issued one round ahead.
+template <class T, bool kForward>
+__device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
+                                          int *flagF, int *flagB, int epoch, double mindt, int group, int wgroup0,
+                                          int ngroups, int lane, int base)
+{
+    const int npos = kForward ? g.nFwdPos : g.nBwdPos;
+    const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
+    const int4 *ent = kForward ? g.fwd_ent : g.bwd_ent;
+    int p = group;
+    int2 info = make_int2(-1, 0);
+    int4 en = make_int4(-1, 0, 0, 0);
+    if (p < npos) { info = __ldg(pinfo + p); en = __ldg(ent + (size_t)p * kGroup + lane); }
+    for (int p0 = wgroup0; p0 < npos; p0 += ngroups) {
+        const int pn = p + ngroups;
+        int2 ninfo = make_int2(-1, 0);
+        int4 nen = make_int4(-1, 0, 0, 0);
+        if (pn < npos) { ninfo = __ldg(pinfo + pn); nen = __ldg(ent + (size_t)pn * kGroup + lane); }
+        if (!sweep_position<T, kForward>(g, c, w, red, flagF, flagB, epoch, mindt, info, en, ninfo, nen, lane, base))
+            return false;
+        info = ninfo;
+        en = nen;
+        p = pn;
+    }
+    return true;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red,
                                                               int *flagF, int *flagB, int epoch)
@@ -895,12 +860,8 @@ __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst
     const int wgroup0 = group & ~(32 / kGroup - 1);   // first group of this warp
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
-    for (int p0 = wgroup0; p0 < g.nFwdPos; p0 += ngroups)
-        if (!sweep_position<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, p0 + (group - wgroup0), lane, base))
-            return;
-    for (int p0 = wgroup0; p0 < g.nBwdPos; p0 += ngroups)
-        if (!sweep_position<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, p0 + (group - wgroup0), lane, base))
-            return;
+    if (!sweep_all<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, group, wgroup0, ngroups, lane, base)) return;
+    sweep_all<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, group, wgroup0, ngroups, lane, base);
 }
 
 template <class T>
@@ -945,7 +906,9 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
 // pre-update state of neighbours that come later in the reference's order,
 // as the in-place sequential loop of the reference does.
 // ---------------------------------------------------------------------------
-static constexpr int kMaxNeg = 1 << 16;
+// Cells the ordered repair pass takes per iteration; more than that means the
+// run has diverged: the pass sets PHX_ERR_NUMERIC and leaves the state alone.
+static constexpr int kMaxNeg = 4096;
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) update_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo,
@@ -1026,28 +989,51 @@ void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const d
 // SolutionFix (NSSolverUnstruct.cpp:14509-14585) for the listed cells, in the
 // reference's cell order: neighbour averages of rho,u,v,w,p (|rho|, |p|),
 // neighbours earlier in the reference's order taken after their update,
-// later ones before.  One thread: the list is empty in healthy runs and short
-// otherwise.
+// later ones before.  One block: the list (at most kMaxNeg cells; empty in
+// healthy runs) is sorted by reference number with a bitonic sort in shared
+// memory, then one thread repairs the cells in that order.
+static constexpr int kFixThreads = 1024;
+
 template <class T>
-__global__ void solution_fix_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo, double *qn, Reduce *red,
-                                    int *neglist)
+__global__ void __launch_bounds__(kFixThreads) solution_fix_kernel(DevGrid g, NsConst c, Work<T> w, const double *qo,
+                                                                   double *qn, Reduce *red, int *neglist)
 {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    int n = red->negcount;
+    __shared__ int key[kMaxNeg], val[kMaxNeg];
+    const int n = red->negcount;
     if (n <= 0) return;
-    if (n > kMaxNeg) { red->error = PHX_ERR_NUMERIC; n = kMaxNeg; }
-    for (int i = 1; i < n; ++i) {  // insertion sort by reference number (short list)
-        const int v = neglist[i];
-        const int ov = g.orig[v];
-        int j = i - 1;
-        while (j >= 0 && g.orig[neglist[j]] > ov) { neglist[j + 1] = neglist[j]; --j; }
-        neglist[j + 1] = v;
+    if (n > kMaxNeg) {
+        if (threadIdx.x == 0) red->error = PHX_ERR_NUMERIC;
+        return;
     }
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int v = i < n ? neglist[i] : -1;
+        key[i] = i < n ? g.orig[v] : 0x7fffffff;
+        val[i] = v;
+    }
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    if ((key[i] > key[l]) == up) {
+                        const int tk = key[i]; key[i] = key[l]; key[l] = tk;
+                        const int tv = val[i]; val[i] = val[l]; val[l] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x != 0) return;
     const int nt = g.nTotal;
     const double rlim = 1.0e-6 * c.primInf[0], plim = 1.0e-6 * c.primInf[4];
     for (int i = 0; i < n; ++i) {
-        const int cell = neglist[i];
-        const int oc = g.orig[cell];
+        const int cell = val[i];
+        const int oc = key[i];
         double acc[5] = {0, 0, 0, 0, 0}, wsum = 0.0;
         for (int j = g.c2f_off[cell]; j < g.c2f_off[cell + 1]; ++j) {
             const int f = g.c2f[j];
@@ -1075,7 +1061,7 @@ template <class T>
 void launch_solution_fix(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                          Reduce *red, int *neglist, cudaStream_t s)
 {
-    solution_fix_kernel<T><<<1, 32, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
+    solution_fix_kernel<T><<<1, kFixThreads, 0, s>>>(g, c, w, q64, q64_new, red, neglist);
 }
 
 // ---------------------------------------------------------------------------
@@ -1153,6 +1139,8 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
                                      cudaStream_t);                                                                 \
     template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int *, int *, int,    \
                                  int, cudaStream_t);                                                                \
+    template void launch_boundary_post<T>(const DevGrid &, const NsConst &, double *, const Work<T> &,           \
+                                          cudaStream_t);                                                            \
     template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \
                                    Reduce *, int *, int, cudaStream_t);                                             \
     template void launch_solution_fix<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *,         \

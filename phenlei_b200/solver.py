@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libphx.so")
 PHX_FP64, PHX_MIXED = 0, 1
 PHX_Q, PHX_RES, PHX_DT, PHX_LIMIT, PHX_GRADX, PHX_GRADY, PHX_GRADZ, PHX_DQ, PHX_INVSPEC, PHX_VISSPEC = range(10)
 PHX_Q_TURB, PHX_VISL, PHX_VIST, PHX_RES_TURB = 10, 11, 12, 13
+PHX_SA_SRC = 15
 ERRORS = {-1: "PHX_ERR_ARG", -2: "PHX_ERR_CUDA", -3: "PHX_ERR_TIMEOUT", -4: "PHX_ERR_NUMERIC", -5: "PHX_ERR_STATE"}
 
 _dp = C.POINTER(C.c_double)
@@ -45,7 +46,8 @@ class Params(C.Structure):
                 ("roeEntropyFixMethod", C.c_int32), ("roeEntropyScale", C.c_double), ("CFLStart", C.c_double),
                 ("CFLEnd", C.c_double), ("CFLVaryStep", C.c_int32), ("ktmax", C.c_double),
                 ("nLUSGSSweeps", C.c_int32), ("LUSGSTolerance", C.c_double), ("skewnessAngle", C.c_double),
-                ("muoo", C.c_double), ("turbCFLScale", C.c_double), ("sa_source", C.c_int32)]
+                ("muoo", C.c_double), ("turbCFLScale", C.c_double), ("sa_source", C.c_int32),
+                ("turbSkewnessAngle", C.c_double), ("freeStreamViscosity", C.c_double)]
 
 
 _STRING_KEYS = {
@@ -75,10 +77,20 @@ def lib() -> C.CDLL:
         _lib.phx_ns_relaxation.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         _lib.phx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         for name in ("phx_ns_boundary", "phx_ns_gradient_limiter", "phx_ns_residual", "phx_ns_lusgs",
-                     "phx_ns_update", "phx_ctx_destroy", "phx_launch_count", "phx_get_step"):
+                     "phx_ns_update", "phx_ctx_destroy", "phx_launch_count", "phx_get_step", "phx_sa_boundary",
+                     "phx_sa_residual", "phx_sa_lusgs", "phx_sa_update"):
             getattr(_lib, name).argtypes = [C.c_void_p]
         _lib.phx_set_step.argtypes = [C.c_void_p, C.c_int]
         _lib.phx_residual_norm.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.phx_forces.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.phx_sa_capture.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                        C.POINTER(C.c_int64)]
+        _lib.phx_mlp_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
+                                       C.c_uint64, C.POINTER(C.c_double)]
+        _lib.phx_mlp_get.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        _lib.phx_mlp_set.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        _lib.phx_mlp_blob_size.restype = C.c_int64
+        _lib.phx_mlp_cells.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
     return _lib
 
 
@@ -102,7 +114,9 @@ def make_params(**keys) -> Params:
 class NSSolverUnstruct:
     """One phx context: a grid, its FP64 metrics and the device-resident flow state."""
 
-    def __init__(self, mesh, precision="fp64", **params):
+    def __init__(self, mesh, precision="fp64", wall_dist=None, **params):
+        """wall_dist: distance of every cell centre to the nearest wall (reference
+        order, [n_cell]); required by the SA model (viscousType 3)."""
         self.mesh = mesh
         self._keep = []
         nb, nc = mesh.n_bface, mesh.n_cell
@@ -122,7 +136,14 @@ class NSSolverUnstruct:
         g.face_nnode, g.face2node, g.left_cell, g.right_cell = i(a["fnn"]), i(a["f2n"]), i(a["left"]), i(a["right"])
         g.cell_nnode, g.cell2node = i(a["cnn"]), i(a["c2n"])
         g.n_region, g.region_type, g.bface_region = len(mesh.regions), i(a["rtype"]), i(a["breg"])
-        g.wall_dist = _dp()
+        if wall_dist is not None:
+            wd = np.ascontiguousarray(wall_dist, dtype=np.float64)
+            if wd.shape != (nc,):
+                raise ValueError("wall_dist must hold one value per cell")
+            self._keep.append(wd)
+            g.wall_dist = wd.ctypes.data_as(_dp)
+        else:
+            g.wall_dist = _dp()
         self.params = make_params(precision=precision, **params)
         h = C.c_void_p()
         rc = lib().phx_ctx_create(C.byref(g), C.byref(self.params), C.byref(h))
@@ -155,7 +176,8 @@ class NSSolverUnstruct:
         return int(lib().phx_launch_count(self.h))
 
     _SHAPES = {PHX_Q: 5, PHX_RES: 5, PHX_DT: 1, PHX_LIMIT: 1, PHX_GRADX: 5, PHX_GRADY: 5, PHX_GRADZ: 5,
-               PHX_DQ: 5, PHX_INVSPEC: -1, PHX_VISSPEC: -1}
+               PHX_DQ: 5, PHX_INVSPEC: -1, PHX_VISSPEC: -1, PHX_Q_TURB: 1, PHX_VISL: 1, PHX_VIST: 1,
+               PHX_RES_TURB: 1, PHX_SA_SRC: -1}
 
     def get(self, which) -> np.ndarray:
         rows = self._SHAPES[which]
@@ -175,6 +197,12 @@ class NSSolverUnstruct:
         q = self.get(PHX_Q)
         q[:, : self.mesh.n_cell] = q_cells
         self.set(PHX_Q, q)
+
+    def set_qt_cells(self, qt_cells: np.ndarray):
+        """Set the SA variable nu~ of the interior cells (ghosts are set by the SA boundary)."""
+        qt = self.get(PHX_Q_TURB)
+        qt[: self.mesh.n_cell] = qt_cells
+        self.set(PHX_Q_TURB, qt)
 
     def geometry(self, name: str) -> np.ndarray:
         n = self.mesh.n_face if name in ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc") else (
@@ -208,11 +236,75 @@ class NSSolverUnstruct:
     def UpdateFlowField(self):
         self._check(lib().phx_ns_update(self.h), "phx_ns_update")
 
+    # -- the reference's TurbSolverUnstr methods (SA) --------------------------
+    def TurbBoundary(self):
+        self._check(lib().phx_sa_boundary(self.h), "phx_sa_boundary")
+
+    def TurbUpdateResiduals(self):
+        """Viscosity, gradient of nu~, source, convection, diffusion, Diagonal."""
+        self._check(lib().phx_sa_residual(self.h), "phx_sa_residual")
+
+    def TurbLUSGS(self):
+        self._check(lib().phx_sa_lusgs(self.h), "phx_sa_lusgs")
+
+    def TurbUpdateFlowField(self):
+        self._check(lib().phx_sa_update(self.h), "phx_sa_update")
+
+    # -- learned SA source --------------------------------------------------------
+    def capture_sa_samples(self):
+        """Features [n, 6], targets [n], reference cell numbers [n], scales [n] of
+        every cell with nu~ > 0, from the last SA residual."""
+        nc = self.mesh.n_cell
+        f = np.empty((nc, 6), np.float32)
+        t = np.empty(nc, np.float32)
+        cells = np.empty(nc, np.int32)
+        sc = np.empty(nc, np.float32)
+        n = C.c_int64()
+        self._check(lib().phx_sa_capture(self.h, f.ctypes.data, t.ctypes.data, cells.ctypes.data, sc.ctypes.data,
+                                         nc, C.byref(n)), "phx_sa_capture")
+        k = n.value
+        return f[:k].copy(), t[:k].copy(), cells[:k].copy(), sc[:k].copy()
+
+    def train_sa_mlp(self, features, targets, epochs=20, batch=8192, lr=1e-3, seed=0) -> float:
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        loss = C.c_double()
+        self._check(lib().phx_mlp_train(self.h, f.ctypes.data, t.ctypes.data, len(t), epochs, batch, lr, seed,
+                                        C.byref(loss)), "phx_mlp_train")
+        return loss.value
+
+    def mlp_blob(self) -> np.ndarray:
+        b = np.empty(int(lib().phx_mlp_blob_size()), np.float32)
+        self._check(lib().phx_mlp_get(self.h, b.ctypes.data, b.size), "phx_mlp_get")
+        return b
+
+    def set_mlp_blob(self, blob):
+        b = np.ascontiguousarray(blob, np.float32)
+        self._check(lib().phx_mlp_set(self.h, b.ctypes.data, b.size), "phx_mlp_set")
+
+    def mlp_cells(self) -> int:
+        n = C.c_uint64()
+        self._check(lib().phx_mlp_cells(self.h, C.byref(n)), "phx_mlp_cells")
+        return int(n.value)
+
     def Relaxation(self, nsteps: int = 1) -> np.ndarray:
         """nsteps outer iterations; returns the residual monitor per step."""
         hist = np.zeros(max(nsteps, 1))
         self._check(lib().phx_ns_relaxation(self.h, nsteps, hist.ctypes.data), "phx_ns_relaxation")
         return hist[:nsteps]
+
+    def AirForceCoef(self, reference_area: float = 1.0) -> dict:
+        """Wall force sums (AirForceCoefParts) and CL / CD (Force.cpp:441-536)."""
+        out = np.zeros(16)
+        self._check(lib().phx_forces(self.h, out.ctypes.data), "phx_forces")
+        import math
+
+        a = math.radians(self.params.attackd)
+        b = math.radians(self.params.angleSlide)
+        cf = (out[0:6:2] + out[1:6:2]) / reference_area
+        cl = -math.sin(a) * cf[0] + math.cos(a) * cf[1]
+        cd = math.cos(a) * math.cos(b) * cf[0] + math.sin(a) * math.cos(b) * cf[1] + math.sin(b) * cf[2]
+        return {"sums": out, "CL": cl, "CD": cd}
 
     def GetResidual(self) -> np.ndarray:
         out = np.zeros(5)

@@ -40,6 +40,7 @@ def test_fp64_laminar_matches_reference_golden(golden, name):
     assert rel_err(s.get(S.PHX_DT)[:nc], d["dt"][:nc]) <= FP64_TOL
     assert rel_err(s.get(S.PHX_VISSPEC), d["visSpectralRadius"]) <= FP64_TOL
     assert rel_err(s.get(S.PHX_GRADY)[:, :nc], d["gradPrimtiveVarY"][:, :nc]) <= FP64_TOL
+    assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= FP64_TOL
 
 
 def test_fp64_laminar_history_matches_reference_golden(golden):

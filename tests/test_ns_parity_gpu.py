@@ -41,6 +41,7 @@ def test_fp64_matches_reference_golden(golden, name):
     assert rel_err(s.get(S.PHX_GRADX)[:, :nc], d["gradPrimtiveVarX"][:, :nc]) <= FP64_TOL
     assert rel_err(s.get(S.PHX_GRADY)[:, :nc], d["gradPrimtiveVarY"][:, :nc]) <= FP64_TOL
     assert rel_err(s.get(S.PHX_INVSPEC), d["invSpectralRadius"]) <= FP64_TOL
+    assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= FP64_TOL
 
 
 def test_fp64_residual_history_matches_reference_golden(golden):

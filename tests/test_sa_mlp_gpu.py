@@ -1,0 +1,139 @@
+"""Learned SA source (MLP 6-64-64-64-1, SiLU) on the GPU: tcgen05 inference
+against a NumPy forward pass with the same BF16 rounding of the tensor-core
+operands, GPU training, the exact fallback outside the training hull, and a
+coupled SA run with the learned source.
+
+Tolerances: inference 2e-3 (norm-wise; FP32 accumulation order and the
+SiLU's fast exponential differ); fallback 1e-12 (the same exact source);
+coupled runs 2e-2 on the residual history (a learned source is not the exact
+source)."""
+import numpy as np
+import pytest
+
+from phenlei_b200 import cases
+from phenlei_b200 import mesh as M
+from phenlei_b200 import solver as S
+from tests.conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+SA = dict(cases.LAMINAR, viscousType=3, refReNumber=1.0e5, muoo=3.0)
+H = 64
+
+
+def bf16(a):
+    """Round float32 values to bfloat16 (nearest even) and back."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def unpack(blob):
+    o = 0
+
+    def take(n):
+        nonlocal o
+        v = blob[o:o + n]
+        o += n
+        return v
+
+    w1 = take(H * 6).reshape(H, 6); b1 = take(H)
+    w2 = take(H * H).reshape(H, H); b2 = take(H)
+    w3 = take(H * H).reshape(H, H); b3 = take(H)
+    w4 = take(H); b4 = take(1)[0]
+    mean, rstd, lo, hi = take(6), take(6), take(6), take(6)
+    tscale = take(1)[0]
+    return dict(w1=w1, b1=b1, w2=w2, b2=b2, w3=w3, b3=b3, w4=w4, b4=b4, mean=mean, rstd=rstd, lo=lo, hi=hi,
+                tscale=tscale)
+
+
+def forward_bf16(p, f):
+    silu = lambda z: z / (1.0 + np.exp(-z))  # noqa: E731
+    x = bf16((f - p["mean"]) * p["rstd"])
+    h = silu(x @ bf16(p["w1"]).T + p["b1"])
+    h = silu(bf16(h) @ bf16(p["w2"]).T + p["b2"])
+    h = silu(bf16(h) @ bf16(p["w3"]).T + p["b3"])
+    return h @ p["w4"] + p["b4"]
+
+
+def _trained_blob(m, wd, epochs=8):
+    a = S.NSSolverUnstruct(m, wall_dist=wd, **SA)
+    a.Relaxation(3)
+    f, t, _, _ = a.capture_sa_samples()
+    assert len(t) > m.n_cell // 2
+    loss = a.train_sa_mlp(f, t, epochs=epochs, batch=512, lr=2e-3, seed=1)
+    assert np.isfinite(loss)
+    return a.mlp_blob(), f, t
+
+
+def _step_to_sa_residual(s):
+    s.step = s.step + 1
+    s.Boundary()
+    s.ComputeGradientAndLimiter()
+    s.UpdateResiduals()
+    s.LUSGS()
+    s.UpdateFlowField()
+    s.TurbUpdateResiduals()
+
+
+def test_tcgen05_inference_matches_numpy():
+    m = M.channel_bump(32, 16, 4)
+    wd = M.wall_distance(m)
+    blob, _, _ = _trained_blob(m, wd, epochs=3)
+    p = unpack(blob)
+    b = S.NSSolverUnstruct(m, wall_dist=wd, sa_source="mlp", **SA)
+    b.set_mlp_blob(blob)
+    b.Relaxation(2)
+    _step_to_sa_residual(b)
+    f, _, cells, sc = b.capture_sa_samples()
+    src = b.get(S.PHX_SA_SRC)[cells]
+    want = forward_bf16(p, f) * p["tscale"] * sc
+    assert rel_err(src, want) <= 2e-3
+    assert b.mlp_cells() > 0
+
+
+def test_training_reduces_loss_and_fits_exact_source():
+    m = M.channel_bump(32, 16, 4)
+    wd = M.wall_distance(m)
+    a = S.NSSolverUnstruct(m, wall_dist=wd, **SA)
+    a.Relaxation(3)
+    f, t, _, _ = a.capture_sa_samples()
+    l1 = a.train_sa_mlp(f, t, epochs=1, batch=512, lr=2e-3, seed=3)
+    lmany = a.train_sa_mlp(f, t, epochs=300, batch=512, lr=2e-3, seed=3)
+    assert lmany < 0.2 * l1
+    p = unpack(a.mlp_blob())
+    pred = forward_bf16(p, f) * p["tscale"]
+    assert rel_err(pred, t) <= 0.1
+
+
+def test_fallback_outside_hull_is_the_exact_source():
+    m = M.channel_bump(16, 8, 2)
+    wd = M.wall_distance(m)
+    blob, _, _ = _trained_blob(m, wd, epochs=1)
+    nowhere = blob.copy()
+    k = H * 6 + H + 2 * (H * H + H) + H + 1 + 12     # hull lo
+    nowhere[k:k + 6] = 1e30                           # lo > every feature: no cell inside the hull
+    q0 = cases.perturbed_state(m, SA, seed=5)
+    ex = S.NSSolverUnstruct(m, wall_dist=wd, **SA)
+    fb = S.NSSolverUnstruct(m, wall_dist=wd, sa_source="mlp_fallback", **SA)
+    fb.set_mlp_blob(nowhere)
+    for s in (ex, fb):
+        s.set_q_cells(q0)
+        s.Relaxation(2)
+    assert fb.mlp_cells() == 0
+    assert rel_err(fb.get(S.PHX_Q_TURB)[: m.n_cell], ex.get(S.PHX_Q_TURB)[: m.n_cell]) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_coupled_run_with_learned_source(precision):
+    m = M.channel_bump(32, 16, 4)
+    wd = M.wall_distance(m)
+    blob, _, _ = _trained_blob(m, wd, epochs=300)
+    ex = S.NSSolverUnstruct(m, wall_dist=wd, precision=precision, **SA)
+    ml = S.NSSolverUnstruct(m, wall_dist=wd, precision=precision, sa_source="mlp_fallback", **SA)
+    ml.set_mlp_blob(blob)
+    he = ex.Relaxation(30)
+    hm = ml.Relaxation(30)
+    assert np.all(np.isfinite(hm))
+    assert rel_err(hm, he) <= 2e-2
+    assert ml.mlp_cells() > 0
