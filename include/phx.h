@@ -237,6 +237,18 @@ int phx_forces(phx_ctx *ctx, double out[16]);
  * sqrt(sum res_m^2 / nCell) (FP64 device reduction). */
 int phx_residual_norm(phx_ctx *ctx, double out[5]);
 
+/* Allocation-free residual monitor (no counterpart in the reference, whose
+ * GetResidual reduces on the host): out_host[m] = sqrt(sum_{c < n_cell}
+ * res_dev[m * n_total + c]^2 / n_cell) for m < nvar, over a device residual in
+ * the reference's SoA layout, on `stream` (NULL: the default stream).  Needs no
+ * context and allocates nothing: the partial sums live in a fixed 64 KiB
+ * device array of the library (at most 8 variables; larger nvar is rejected
+ * with PHX_ERR_ARG; any n_cell).  The first call on a device looks the array
+ * up, so make it before any stream capture.  Calls that overlap on one device
+ * share the array and race: serialise them. */
+int phx_residual_norm_noalloc(const double *res_dev, int64_t n_cell, int64_t n_total, int nvar, double *out_host,
+                              void *stream);
+
 /* Outer step counter (drives the CFL ramp of NSSolver::ComputeCFL). */
 int phx_set_step(phx_ctx *ctx, int step);
 int phx_get_step(const phx_ctx *ctx);

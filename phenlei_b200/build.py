@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libphx.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["phx_kernels.cu", "phx_sa.cu", "phx_mlp.cu", "phx_host.cpp"]
+SOURCES = ["phx_kernels.cu", "phx_sa.cu", "phx_mlp.cu", "phx_noalloc.cu", "phx_host.cpp"]
 
 
 def _run(cmd):
