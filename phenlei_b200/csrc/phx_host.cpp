@@ -1375,15 +1375,15 @@ int phx_forces(phx_ctx *ctx, double out[16])
 int phx_residual_norm(phx_ctx *ctx, double out[5])
 {
     if (!ctx || !out) return PHX_ERR_ARG;
-    const int nc = ctx->nCell;
-    std::vector<double> r((size_t)5 * ctx->nTotal);
-    const int rc = phx_get_state(ctx, PHX_RES, r.data(), (int64_t)r.size());
+    double *d = ctx->forces;   // 16-double device scratch of the context, free between calls
+    if (ctx->mixed) launch_resnorm<float>(ctx->g, ctx->w32, d, ctx->numSMs, ctx->stream);
+    else launch_resnorm<double>(ctx->g, ctx->w64, d, ctx->numSMs, ctx->stream);
+    const int rc = check_launch(ctx);
     if (rc) return rc;
-    for (int m = 0; m < 5; ++m) {
-        double s = 0.0;
-        for (int c = 0; c < nc; ++c) s += r[(size_t)m * ctx->nTotal + c] * r[(size_t)m * ctx->nTotal + c];
-        out[m] = std::sqrt(s / nc);
-    }
+    double s[5];
+    PHX_CUDA(ctx, cudaMemcpyAsync(s, d, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int m = 0; m < 5; ++m) out[m] = std::sqrt(s[m] / ctx->nCell);
     return PHX_OK;
 }
 

@@ -178,6 +178,9 @@ void launch_export(const DevGrid &g, const T *rec, int stride, int first, int co
 void launch_import_q(const DevGrid &g, const double *in, double *q64, cudaStream_t s);
 void launch_export_q(const DevGrid &g, const double *q64, double *out, cudaStream_t s);
 void launch_reset_reduce(Reduce *r, cudaStream_t s);
+// out[m] = sum over cells of res_m^2 (FP64 device reduction of the residual record).
+template <class T>
+void launch_resnorm(const DevGrid &g, const Work<T> &w, double *out, int numSMs, cudaStream_t s);
 // NS boundary after the update (Controller::PostSolve): ghost states only,
 // the laminar viscosity of the ghosts keeps its value of the NS step.
 template <class T>

@@ -1125,6 +1125,45 @@ static __global__ void finish_step_kernel(Reduce *r, double *hist, int i, double
     if (hist) hist[i] = v;
 }
 
+// Residual monitor of the current residual record: out[m] += sum_c res_m^2
+// (FP64; block sums, one atomic per block and equation; out zeroed first).
+template <class T>
+__global__ void __launch_bounds__(kThreads) resnorm_kernel(DevGrid g, Work<T> w, double *out)
+{
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.nCell; c += gridDim.x * blockDim.x) {
+        T cr[8];
+        ld8(w.crec + (size_t)c * kC, cr);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s[k] += (double)cr[k] * (double)cr[k];
+    }
+    __shared__ double part[kThreads / 32][5];
+    const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double v = s[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (ln == 0) part[wid][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int i = 0; i < kThreads / 32; ++i) v += part[i][threadIdx.x];
+        if (v != 0.0) atomicAdd(out + threadIdx.x, v);
+    }
+}
+
+template <class T>
+void launch_resnorm(const DevGrid &g, const Work<T> &w, double *out, int numSMs, cudaStream_t s)
+{
+    cudaMemsetAsync(out, 0, sizeof(double) * 5, s);
+    int blocks = (g.nCell + kThreads - 1) / kThreads;
+    if (blocks > numSMs * 8) blocks = numSMs * 8;
+    resnorm_kernel<T><<<blocks, kThreads, 0, s>>>(g, w, out);
+}
+template void launch_resnorm<double>(const DevGrid &, const Work<double> &, double *, int, cudaStream_t);
+template void launch_resnorm<float>(const DevGrid &, const Work<float> &, double *, int, cudaStream_t);
+
 void launch_reset_reduce(Reduce *r, cudaStream_t s) { reset_reduce_kernel<<<1, 1, 0, s>>>(r); }
 void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s)
 {
