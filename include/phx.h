@@ -64,7 +64,8 @@ extern "C" {
 #define PHX_VIST 12      /* eddy viscosity [nTotal] ("vist") */
 #define PHX_RES_TURB 13  /* SA residual [nTotal] */
 #define PHX_GEOM 14      /* geometry, see phx_get_geometry */
-#define PHX_SA_SRC 15    /* SA source per unit volume used by the last SA residual [nCell] (learned-source runs) */
+#define PHX_SA_SRC 15    /* learned SA source per unit volume of the last SA residual [nCell] (learned-source runs;
+                            NaN where the cell took the exact source) */
 
 typedef struct phx_ctx phx_ctx;
 

@@ -77,24 +77,104 @@ __device__ __forceinline__ T sutherland(T t, T s) { return t * sqrt(t) * (T(1) +
 
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// Per-cell completion flags of the LU-SGS dataflow sweeps (release / acquire at
-// device scope), and the sweep geometry: a lane group of kGroup lanes per cell,
-// kSweepPad groups per warp.
+// Sweep geometry of the LU-SGS dataflow sweeps: a lane group of kGroup lanes
+// per cell, kSweepPad groups per warp.
 static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
 static constexpr int kSweepThreads = 256;
 static constexpr int kGroup = kSweepGroup;            // lanes per cell
 static_assert(kGroup * kSweepPad == 32, "one warp holds kSweepPad lane groups");
 
-__device__ __forceinline__ int ld_acquire(const int *p)
+// Write-once sweep records.  Before a sweep every element of its output
+// records holds the sentinel, a NaN whose sign and payload no arithmetic
+// result carries (the GPU's NaN results are the positive canonical NaN, and
+// producers map the sentinel pattern itself to that NaN).  During the sweep
+// each element is stored once, so a reader that sees anything but the
+// sentinel sees the final value: the data is its own completion flag, and
+// neither a fence between the producer's stores nor a second load after the
+// wait sits on the sweep's critical path.  Stores and polling loads are
+// relaxed at device scope (coherent in L2, not cached in L1).
+static constexpr unsigned kSentinelF = 0xffc0e1a5u;
+static constexpr unsigned long long kSentinelD = 0xfff80000d0e1a5c3ull;
+
+template <class T> __device__ __forceinline__ T sweep_sentinel();
+template <> __device__ __forceinline__ float sweep_sentinel<float>() { return __uint_as_float(kSentinelF); }
+template <> __device__ __forceinline__ double sweep_sentinel<double>()
 {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
+    return __longlong_as_double((long long)kSentinelD);
+}
+__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_uint(v) == kSentinelF; }
+__device__ __forceinline__ bool is_sentinel(double v)
+{
+    return (unsigned long long)__double_as_longlong(v) == kSentinelD;
+}
+// a computed value as stored: the sentinel pattern becomes the canonical NaN
+__device__ __forceinline__ float unsentinel(float v) { return is_sentinel(v) ? __int_as_float(0x7fffffff) : v; }
+__device__ __forceinline__ double unsentinel(double v)
+{
+    return is_sentinel(v) ? __longlong_as_double(0x7fffffffffffffffLL) : v;
 }
 
-__device__ __forceinline__ void st_release(int *p, int v)
+__device__ __forceinline__ float ld_poll(const float *p)
 {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ double ld_poll(const double *p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(float *p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(double *p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
+// Polls the first five elements of an 8-element record; true once none of
+// them is the sentinel (o then holds the final values).
+__device__ __forceinline__ bool poll5(const float *p, float *o)
+{
+    asm volatile("ld.relaxed.gpu.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
+                 : "l"(p)
+                 : "memory");
+    o[4] = ld_poll(p + 4);
+    return !(is_sentinel(o[0]) | is_sentinel(o[1]) | is_sentinel(o[2]) | is_sentinel(o[3]) | is_sentinel(o[4]));
+}
+__device__ __forceinline__ bool poll5(const double *p, double *o)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.f64 {%0, %1}, [%2];" : "=d"(o[0]), "=d"(o[1]) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.v2.f64 {%0, %1}, [%2];" : "=d"(o[2]), "=d"(o[3]) : "l"(p + 2) : "memory");
+    o[4] = ld_poll(p + 4);
+    return !(is_sentinel(o[0]) | is_sentinel(o[1]) | is_sentinel(o[2]) | is_sentinel(o[3]) | is_sentinel(o[4]));
+}
+
+// Publishes the five values of an 8-element record (slots 5-7 zero).
+__device__ __forceinline__ void publish5(float *p, const float *v)
+{
+    asm volatile("st.relaxed.gpu.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(unsentinel(v[0])),
+                 "f"(unsentinel(v[1])), "f"(unsentinel(v[2])), "f"(unsentinel(v[3]))
+                 : "memory");
+    asm volatile("st.relaxed.gpu.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p + 4), "f"(unsentinel(v[4])),
+                 "f"(0.0f), "f"(0.0f), "f"(0.0f)
+                 : "memory");
+}
+__device__ __forceinline__ void publish5(double *p, const double *v)
+{
+    asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(unsentinel(v[0])),
+                 "d"(unsentinel(v[1]))
+                 : "memory");
+    asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1, %2};" ::"l"(p + 2), "d"(unsentinel(v[2])),
+                 "d"(unsentinel(v[3]))
+                 : "memory");
+    asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1, %2};" ::"l"(p + 4), "d"(unsentinel(v[4])), "d"(0.0)
+                 : "memory");
+    asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1, %2};" ::"l"(p + 6), "d"(0.0), "d"(0.0) : "memory");
 }
 
 }  // namespace phx

@@ -61,8 +61,6 @@ struct phx_ctx {
     Reduce *red = nullptr;
     int *neglist = nullptr;
     double *tmp = nullptr;                // [5][nTotal] staging buffer in the reference's order
-    int *flagF = nullptr, *flagB = nullptr;  // LU-SGS per-cell completion flags (epoch of the solve)
-    int epoch = 0;
     double *hist = nullptr;
     int histCap = 0;
     int step = 0;
@@ -444,6 +442,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     r |= dalloc(ctx, &t.tface, nf * kTf);
     r |= dalloc(ctx, &t.tcoef, 2 * nf);
     r |= dalloc(ctx, &t.tdq, nc);
+    r |= dalloc(ctx, &t.tdqf, nc);
     r |= dalloc(ctx, &t.tdfl, nc);
     r |= dalloc(ctx, &t.tsrc, nc);
     r |= dalloc(ctx, &ctx->nmlp, 1);
@@ -478,6 +477,7 @@ int make_work(phx_ctx *ctx, Work<T> &w, const std::vector<double> &limInit)
     r |= dalloc(ctx, &w.crec, nc * kC);
     r |= dalloc(ctx, &w.dtraw, nc);
     r |= dalloc(ctx, &w.dqrec, nt * kD);
+    r |= dalloc(ctx, &w.dqfwd, nc * kD);
     r |= dalloc(ctx, &w.dflux, nc * kD);
     if (r) return r;
     std::vector<T> q(nt * kQ, T(0));
@@ -870,10 +870,6 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= dalloc(ctx, &ctx->tmp, (size_t)5 * nt);
     rc |= dalloc(ctx, &ctx->red, 1);
     rc |= dalloc(ctx, &ctx->neglist, 1 << 16);
-    rc |= dalloc(ctx, &ctx->flagF, (size_t)nc);
-    rc |= dalloc(ctx, &ctx->flagB, (size_t)nc);
-    if (!rc && (cudaMemset(ctx->flagF, 0, sizeof(int) * nc) != cudaSuccess ||
-                cudaMemset(ctx->flagB, 0, sizeof(int) * nc) != cudaSuccess)) rc = PHX_ERR_CUDA;
     if (!rc) rc = ctx->mixed ? make_work(ctx, ctx->w32, limInit) : make_work(ctx, ctx->w64, limInit);
     if (!rc && ctx->sa) rc = ctx->mixed ? make_turb(ctx, ctx->w32, ctx->t32) : make_turb(ctx, ctx->w64, ctx->t64);
     else if (!rc && prm->viscousType) rc = ctx->mixed ? make_visc(ctx, ctx->w32) : make_visc(ctx, ctx->w64);
@@ -1112,13 +1108,10 @@ int phx_ns_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
     if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs needs phx_ns_residual first");
-    ctx->epoch += 1;
-    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->flagF, ctx->flagB,
-                                                   ctx->epoch, ctx->numSMs, ctx->stream)
-                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->flagF, ctx->flagB,
-                                                    ctx->epoch, ctx->numSMs, ctx->stream);
+    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->numSMs, ctx->stream)
+                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->numSMs, ctx->stream);
     if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx, 1);
+    return check_launch(ctx, 2);
 }
 
 int phx_ns_update(phx_ctx *ctx)
@@ -1171,13 +1164,12 @@ int phx_sa_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
     if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
-    ctx->epoch += 1;
-    const int e = ctx->mixed ? launch_sa_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->red, ctx->flagF,
-                                                      ctx->flagB, ctx->epoch, ctx->numSMs, ctx->stream)
-                             : launch_sa_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->red, ctx->flagF,
-                                                       ctx->flagB, ctx->epoch, ctx->numSMs, ctx->stream);
+    const int e = ctx->mixed ? launch_sa_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->red, ctx->numSMs,
+                                                      ctx->stream)
+                             : launch_sa_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->red, ctx->numSMs,
+                                                       ctx->stream);
     if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx, 1);
+    return check_launch(ctx, 2);
 }
 
 int phx_sa_update(phx_ctx *ctx)

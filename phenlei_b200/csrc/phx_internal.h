@@ -124,8 +124,9 @@ struct Work {
     T *coef;        // [2 nFace][kCoef] LU-SGS factors of each face use (side 0: the left cell's view)
     T *crec;        // [nCell][kC] residual, diagonal, spectral radii
     T *dtraw;       // [nCell] CFL * vol / spectral radius, before the ktmax clamp
-    T *dqrec;       // [nTotal][kD] LU-SGS dq
-    T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep
+    T *dqrec;       // [nTotal][kD] LU-SGS dq (backward sweep; write-once per sweep)
+    T *dqfwd;       // [nCell][kD] forward-sweep dq (write-once per sweep)
+    T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep (write-once)
     T *trec;        // [nTotal][kTr] SA variable, eddy and laminar viscosity (SA runs; else null)
 };
 
@@ -137,8 +138,9 @@ struct TurbWork {
     T *tcrec;       // [nCell][kTc] residual and spectral radius
     T *tface;       // [nFace][kTf] face terms
     T *tcoef;       // [2 nFace] LU-SGS matrix of each face use (side 0: left cell's view = mat_turbr)
-    T *tdq;         // [nCell] LU-SGS dq
-    T *tdfl;        // [nCell] forward delta flux
+    T *tdq;         // [nCell] LU-SGS dq (backward sweep; write-once per sweep)
+    T *tdqf;        // [nCell] forward-sweep dq (write-once per sweep)
+    T *tdfl;        // [nCell] forward delta flux (write-once per sweep)
     T *tsrc;        // [nCell] source computed by the learned-source kernel (sa_source != 0)
 };
 
@@ -146,7 +148,6 @@ struct Reduce {
     unsigned long long mindt_bits;  // min over cells of dtraw (positive doubles order as integers)
     double resnorm[5];
     int negcount;
-    unsigned int barrier;           // monotonic arrival counter of the LU-SGS grid barrier
     int error;                      // PHX_ERR_TIMEOUT / PHX_ERR_NUMERIC
 };
 
@@ -158,8 +159,7 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s);
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int *flagF, int *flagB, int epoch,
-                 int numSMs, cudaStream_t s);
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s);
 template <class T>
 void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                    Reduce *red, int *neglist, int numSMs, cudaStream_t s);
@@ -204,7 +204,7 @@ void launch_mlp_capture(const DevGrid &g, const NsConst &c, const Work<T> &w, co
                         cudaStream_t s);
 template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
-                    int *flagF, int *flagB, int epoch, int numSMs, cudaStream_t s);
+                    int numSMs, cudaStream_t s);
 template <class T>
 void launch_sa_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s);
 // Wall force sums (16 doubles, the last zero) of the current state.

@@ -9,6 +9,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 #include "phx_internal.h"
 #include "phx_device.cuh"
 #include "phx_physics.cuh"
@@ -628,19 +630,22 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 // LU-SGS (Controller::LUSGS, Controller.cpp:1878-1955) as a dataflow
 // computation.  The forward sweep of the reference visits cells in
 // increasing number and uses the just-updated dq of lower-numbered face
-// neighbours; the backward sweep the reverse.  Here every cell publishes
-// "forward done" and "backward done" flags (the solve's epoch number) after
-// its dq; a cell waits only on the flags of the neighbours it reads, so it
-// sees exactly the values the sequential sweep of the reference sees, with
-// no device-wide barrier.  Lane groups (one per cell) take schedule
-// positions in level order (forward positions, then backward positions),
-// the four groups of a warp four consecutive positions of one level (levels
-// are padded to multiples of four), so a warp only waits on cells of earlier
-// levels, held by other warps or by its own earlier rounds.  All warps are
-// co-resident (cooperative launch), so the wait graph cannot cycle: the warp
-// holding the lowest unfinished position always has its inputs.  Every
-// wait is bounded: a timeout sets Reduce::error and the kernel gives up.
-// The dq-independent MXDQ_STD factors were computed by the residual pass.
+// neighbours; the backward sweep the reverse.  Here the forward sweep writes
+// each cell's dq and delta flux into write-once records (dqfwd, dflux) and
+// the backward sweep writes the final dq into dqrec; all three are filled
+// with the sentinel before the sweep (sweep_reset_kernel), so a cell waits
+// only on the records of the neighbours it reads, polling the data itself,
+// and sees exactly the values the sequential sweep of the reference sees,
+// with no device-wide barrier and no completion flags.  Lane groups (one per
+// cell) take schedule positions in level order (forward positions, then
+// backward positions), the four groups of a warp four consecutive positions
+// of one level (levels are padded to multiples of four), so a warp only
+// waits on cells of earlier levels, held by other warps or by its own
+// earlier rounds.  All warps are co-resident (cooperative launch), so the
+// wait graph cannot cycle: the warp holding the lowest unfinished position
+// always has its inputs.  Every wait is bounded: a timeout sets
+// Reduce::error and the kernel gives up.  The dq-independent MXDQ_STD
+// factors were computed by the residual pass.
 // ---------------------------------------------------------------------------
 
 // Ghost-cell dq of boundary face f from the owner's forward dq
@@ -684,17 +689,17 @@ __device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, con
 
 // One schedule position of a sweep, processed by a lane group of kGroup
 // lanes (one lane per neighbour entry).  The four groups of a warp run in
-// lockstep: the warp polls until every lane's flags are set, so no group ever
-// spins while a sibling in the same warp is ready to work, and every shuffle
-// uses the full warp mask.  pos >= nCell marks an idle group (the warp's trip
-// count is uniform).
+// lockstep: the warp polls until every lane's inputs are final, so no group
+// ever spins while a sibling in the same warp is ready to work, and every
+// shuffle uses the full warp mask.  info.x < 0 marks an idle group (the
+// warp's trip count is uniform).
 // The position's {cell, count} and this lane's entry were loaded one round
 // ahead by the caller (info, en); the next round's (ninfo, nen) are known here,
 // so their records are prefetched into L2 while this position waits.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
-                                               int *flagF, int *flagB, int epoch, double mindt, int2 info, int4 en,
-                                               int2 ninfo, int4 nen, int lane, int base)
+                                               double mindt, int2 info, int4 en, int2 ninfo, int4 nen, int lane,
+                                               int base)
 {
     const int nc = g.nCell;
     const int cell = info.x;
@@ -721,13 +726,19 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         ld8(w.crec + (size_t)cell * kC, cr);
         dt = w.dtraw[cell];
     }
-    // wait for the neighbours' dq (a ghost's dq comes from this cell's forward value)
-    const bool ghost = has && nb >= nc;
-    const int *w1 = (has && !ghost) ? (kForward ? flagF : flagB) + nb : nullptr;
-    const int *w2 = (!kForward && live && (lane == 0 || ghost)) ? flagF + cell : nullptr;
-    bool ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+    // wait for the inputs other positions write: the neighbour's dq (forward:
+    // its forward dq; backward: its final dq; a ghost's comes from this cell's
+    // forward dq) and, backward, this cell's forward delta flux
+    const bool ghost = !kForward && has && nb >= nc;
+    const T *src1 = !has ? nullptr
+                         : ghost ? w.dqfwd + (size_t)cell * kD
+                                 : (kForward ? w.dqfwd : w.dqrec) + (size_t)nb * kD;
+    const T *src2 = (!kForward && live && lane == 0) ? w.dflux + (size_t)cell * kD : nullptr;
+    T v1[5], fl[5];
+    bool r1 = !src1 || poll5(src1, v1);
+    bool r2 = !src2 || poll5(src2, fl);
     long long spins = 0;
-    while (!__all_sync(0xffffffffu, ready)) {
+    while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
         if (spins > kSpinLimit) {
             if ((threadIdx.x & 31) == 0) atomicExch(&red->error, PHX_ERR_TIMEOUT);
@@ -735,7 +746,8 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         }
         if ((spins & 1023) == 0 && __any_sync(0xffffffffu, ((volatile int *)&red->error)[0] != 0)) return false;
         if (spins > 8) __nanosleep(20);
-        if (!ready) ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+        if (!r1) r1 = poll5(src1, v1);
+        if (!r2) r2 = poll5(src2, fl);
     }
     // next round's records into L2 (their entries arrived during the wait)
     if (nen.x >= 0) {
@@ -751,11 +763,10 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     if (has) {
         T dq[8];
         if (ghost) {
-            T dl[8];
-            ld8cg(w.dqrec + (size_t)cell * kD, dl);
-            ghost_dq<T>(g, c, w, nb - nc, dl, dq);
+            ghost_dq<T>(g, c, w, nb - nc, v1, dq);
         } else {
-            ld8cg(w.dqrec + (size_t)nb * kD, dq);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) dq[k] = v1[k];
         }
         const T gm = (T)c.gama;
         const T um = qn[1], vm = qn[2], wm = qn[3], c2 = qn[5], hm = qn[6];
@@ -798,26 +809,20 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         T d = T(1) / dt;
         d += cr[6];
         if (c.viscous) d += cr[7];
-        T o[8];
+        T o[5];
         if (kForward) {
             // dq = (res - Ux - L dq) / D, Ux = 0 for a single sweep
             // (LUSGSInitialization, Controller.cpp:1765-1777)
-            T fl[8];
+            T fo[5];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) { o[k] = (cr[k] - T(0) - rhs0[k]) / d; fl[k] = T(0) + rhs0[k]; }
-            o[5] = o[6] = o[7] = T(0);
-            fl[5] = fl[6] = fl[7] = T(0);
-            st8(w.dflux + (size_t)cell * kD, fl);
+            for (int k = 0; k < 5; ++k) { o[k] = (cr[k] - T(0) - rhs0[k]) / d; fo[k] = T(0) + rhs0[k]; }
+            publish5(w.dflux + (size_t)cell * kD, fo);
+            publish5(w.dqfwd + (size_t)cell * kD, o);
         } else {
-            T fl[8];
-            ld8cg(w.dflux + (size_t)cell * kD, fl);
 #pragma unroll
             for (int k = 0; k < 5; ++k) o[k] = (cr[k] - fl[k] - rhs0[k]) / d;
-            o[5] = o[6] = o[7] = T(0);
+            publish5(w.dqrec + (size_t)cell * kD, o);
         }
-        st8(w.dqrec + (size_t)cell * kD, o);
-        // release orders this thread's dq / dflux stores before the flag
-        st_release((kForward ? flagF : flagB) + cell, epoch);
     }
     return true;
 }
@@ -826,8 +831,7 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
 // {cell, count} and of this lane's entry issued one round ahead.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
-                                          int *flagF, int *flagB, int epoch, double mindt, int group, int wgroup0,
-                                          int ngroups, int lane, int base)
+                                          double mindt, int group, int wgroup0, int ngroups, int lane, int base)
 {
     const int npos = kForward ? g.nFwdPos : g.nBwdPos;
     const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
@@ -841,8 +845,7 @@ __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, co
         int2 ninfo = make_int2(-1, 0);
         int4 nen = make_int4(-1, 0, 0, 0);
         if (pn < npos) { ninfo = __ldg(pinfo + pn); nen = __ldg(ent + (size_t)pn * kGroup + lane); }
-        if (!sweep_position<T, kForward>(g, c, w, red, flagF, flagB, epoch, mindt, info, en, ninfo, nen, lane, base))
-            return false;
+        if (!sweep_position<T, kForward>(g, c, w, red, mindt, info, en, ninfo, nen, lane, base)) return false;
         info = ninfo;
         en = nen;
         p = pn;
@@ -851,8 +854,7 @@ __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, co
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red,
-                                                              int *flagF, int *flagB, int epoch)
+__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kGroup, lane = tid % kGroup;
@@ -860,18 +862,33 @@ __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst
     const int wgroup0 = group & ~(32 / kGroup - 1);   // first group of this warp
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
-    if (!sweep_all<T, true>(g, c, w, red, flagF, flagB, epoch, mindt, group, wgroup0, ngroups, lane, base)) return;
-    sweep_all<T, false>(g, c, w, red, flagF, flagB, epoch, mindt, group, wgroup0, ngroups, lane, base);
+    if (!sweep_all<T, true>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base)) return;
+    sweep_all<T, false>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base);
 }
 
+// Fills the sweep's output records (forward dq, forward delta flux, final dq)
+// with the sentinel: 8-element records, 16-byte stores.
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int *flagF, int *flagB, int epoch,
-                 int numSMs, cudaStream_t s)
+__global__ void __launch_bounds__(kThreads) sweep_reset_kernel(int n, T *a, T *b, T *c)
 {
-    static int perSMcache[2] = {-1, -1};
-    int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
+    const T s = sweep_sentinel<T>();
+    const long long tot = (long long)n * kD;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i * 4 < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const T v[4] = {s, s, s, s};
+        st4(a + i * 4, v);
+        st4(b + i * 4, v);
+        st4(c + i * 4, v);
+    }
+}
+
+// Grid of the sweeps: every resident lane group (cooperative launch), at most
+// one group per schedule position.
+template <class K>
+static int sweep_blocks(K kernel, int &perSM, const DevGrid &g, int numSMs)
+{
     if (perSM < 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, lusgs_kernel<T>, kSweepThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kSweepThreads, 0);
         if (perSM < 1) perSM = 1;
     }
     int blocks = numSMs * perSM;
@@ -883,14 +900,22 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
         const int v = atoi(cap);
         if (v > 0 && blocks > v) blocks = v;
     }
-    if (blocks < 1) blocks = 1;
+    return blocks < 1 ? 1 : blocks;
+}
+
+template <class T>
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s)
+{
+    static int perSMcache[2] = {-1, -1};
+    const int blocks = sweep_blocks(lusgs_kernel<T>, perSMcache[sizeof(T) == 8 ? 0 : 1], g, numSMs);
+    const long long quads = (long long)g.nCell * kD / 4;
+    const int rb = (int)std::min<long long>((quads + kThreads - 1) / kThreads, (long long)numSMs * 16);
+    sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, w.dqfwd, w.dflux, w.dqrec);
     DevGrid gg = g;
     NsConst cc = c;
     Work<T> ww = w;
     Reduce *rr = red;
-    int *ff = flagF, *fb = flagB;
-    int ep = epoch;
-    void *args[] = {&gg, &cc, &ww, &rr, &ff, &fb, &ep};
+    void *args[] = {&gg, &cc, &ww, &rr};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
@@ -1176,8 +1201,7 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
     template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);      \
     template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,           \
                                      cudaStream_t);                                                                 \
-    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int *, int *, int,    \
-                                 int, cudaStream_t);                                                                \
+    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t);   \
     template void launch_boundary_post<T>(const DevGrid &, const NsConst &, double *, const Work<T> &,           \
                                           cudaStream_t);                                                            \
     template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \

@@ -121,7 +121,7 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v)
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu(float x) { return x / (1.0f + __expf(-x)); }
+__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
 
 // ---------------------------------------------------------------------------
 // Features and target of the learned source, for a cell with nu~ > 0.
@@ -243,19 +243,16 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
     const int ntiles = (g.nCell + kMlpTile - 1) / kMlpTile;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int cell = tile * kMlpTile + tid;
-        // inputs, exact source (fallback), features
+        // inputs and features (the exact source of fallback cells is formed by the SA cell pass)
         float x[kMlpK1];
 #pragma unroll
         for (int k = 0; k < kMlpK1; ++k) x[k] = 0.0f;
-        T srcExact = T(0);
         float scale = 0.0f;
         bool useMlp = false;
         if (cell < g.nCell) {
             T nue, omega, smag, gradn2, olam;
             double d;
             sa_cell_inputs<T>(g, w, t, cell, nue, omega, smag, gradn2, olam, d);
-            T sspec;
-            sa_source_exact<T>(nue, omega, olam, T(1) / ((T)d * (T)d), gradn2, (T)c.oRe, srcExact, sspec);
             if (nue > T(0) && c.saSource) {
                 float f[kMlpIn];
                 sa_features((float)nue, (float)omega, (float)smag, sqrtf((float)gradn2), (float)olam, (float)d,
@@ -310,7 +307,8 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
 #pragma unroll
         for (int k = 0; k < kMlpH; ++k) out += __ldg(mlp.w4 + k) * h[k];
         if (cell < g.nCell) {
-            t.tsrc[cell] = useMlp ? (T)(out * mlp.tscale * scale) : srcExact;
+            // NaN marks a cell that takes the exact source
+            t.tsrc[cell] = useMlp ? (T)(out * mlp.tscale * scale) : (T)__int_as_float(0x7fc00000);
             used += useMlp ? 1 : 0;
         }
         tc_fence_before();

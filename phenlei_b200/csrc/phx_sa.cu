@@ -11,6 +11,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 #include "phx_device.cuh"
 #include "phx_internal.h"
 #include "phx_physics.cuh"
@@ -300,7 +302,11 @@ __global__ void __launch_bounds__(kThreads) sa_cell_kernel(DevGrid g, NsConst c,
     const T odist2 = T(1) / ((T)d * (T)d);
     T src, sspec;
     sa_source_exact<T>(nue, omega, olam, odist2, grd2, (T)c.oRe, src, sspec);
-    if (c.saSource) src = t.tsrc[cell];   // learned source (exact where it falls back)
+    if (c.saSource) {
+        // learned source; NaN marks the cells that take the exact source
+        const T s = t.tsrc[cell];
+        if (s == s) src = s;
+    }
     // NS dt after ReduceMaxTimeStep: min(dt, ktmax dt_min) / vol
     T dt = w.dtraw[cell];
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
@@ -361,15 +367,15 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
 // ---------------------------------------------------------------------------
 // Scalar LU-SGS of the SA equation (SolveLUSGSForward / Backward,
 // TurbSolverUnstr.cpp:1400-1638): dq = (res - L/U dq - rhs0) / spec_turb with
-// the face matrices of each face use.  Same dataflow schedule, flags and
-// bounded waits as the NS sweep (phx_kernels.cu), with its own epoch.  dq of
-// the ghosts is the ghost residual, which is zero, so ghost entries of the
-// backward sweep add nothing and are skipped.
+// the face matrices of each face use.  Same dataflow schedule, write-once
+// records and bounded waits as the NS sweep (phx_kernels.cu): tdqf (forward
+// dq), tdfl (forward delta flux) and tdq (final dq) hold the sentinel until
+// written.  dq of the ghosts is the ghost residual, which is zero, so ghost
+// entries of the backward sweep add nothing and are skipped.
 // ---------------------------------------------------------------------------
 template <class T, bool kForward>
-__device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int *flagF,
-                                                  int *flagB, int epoch, int2 info, int4 en, int2 ninfo, int4 nen,
-                                                  int lane, int base)
+__device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int2 info,
+                                                  int4 en, int2 ninfo, int4 nen, int lane, int base)
 {
     const int nc = g.nCell;
     const int cell = info.x;
@@ -383,13 +389,18 @@ __device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWo
         if (nb >= nc) has = false;
         else mat = t.tcoef[en.z];
     }
-    T cr[4] = {0, 0, 0, 0}, fl = T(0);
+    T cr[4] = {0, 0, 0, 0};
     if (live && lane == 0) ld4(t.tcrec + (size_t)cell * kTc, cr);
-    const int *w1 = has ? (kForward ? flagF : flagB) + nb : nullptr;
-    const int *w2 = (!kForward && live && lane == 0) ? flagF + cell : nullptr;
-    bool ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+    // the neighbour's dq (forward: its forward dq; backward: its final dq)
+    // and, backward, this cell's forward delta flux
+    const T *src1 = has ? (kForward ? t.tdqf : t.tdq) + nb : nullptr;
+    const T *src2 = (!kForward && live && lane == 0) ? t.tdfl + cell : nullptr;
+    T v1 = T(0), fl = T(0);
+    bool r1 = true, r2 = true;
+    if (src1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
+    if (src2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
     long long spins = 0;
-    while (!__all_sync(0xffffffffu, ready)) {
+    while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
         if (spins > kSpinLimit) {
             if ((threadIdx.x & 31) == 0) atomicExch(&red->error, PHX_ERR_TIMEOUT);
@@ -397,17 +408,12 @@ __device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWo
         }
         if ((spins & 1023) == 0 && __any_sync(0xffffffffu, ((volatile int *)&red->error)[0] != 0)) return false;
         if (spins > 8) __nanosleep(20);
-        if (!ready) ready = (!w1 || ld_acquire(w1) == epoch) && (!w2 || ld_acquire(w2) == epoch);
+        if (!r1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
+        if (!r2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
     }
-    if (nen.x >= 0 && nen.x < nc) {
-        prefetch_l2(t.tcoef + nen.z);
-        prefetch_l2(t.tdq + nen.x);
-    }
+    if (nen.x >= 0 && nen.x < nc) prefetch_l2(t.tcoef + nen.z);
     if (lane == 0 && ninfo.x >= 0) prefetch_l2(t.tcrec + (size_t)ninfo.x * kTc);
-    // the forward delta flux of this cell, written by the forward sweep (flagF)
-    if (!kForward && live && lane == 0) fl = __ldcg(t.tdfl + cell);
-    T df = T(0);
-    if (has) df = mat * __ldcg(t.tdq + nb);
+    const T df = has ? mat * v1 : T(0);
     T rhs0 = T(0);
 #pragma unroll
     for (int k = 0; k < kGroup; ++k) {
@@ -415,23 +421,19 @@ __device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWo
         if (k < e1 - e0) rhs0 += v;
     }
     if (live && lane == 0) {
-        T dq;
         if (kForward) {
-            dq = (cr[0] - T(0) - rhs0) / cr[1];
-            t.tdfl[cell] = T(0) + rhs0;
+            st_relaxed(t.tdfl + cell, unsentinel(T(0) + rhs0));
+            st_relaxed(t.tdqf + cell, unsentinel((cr[0] - T(0) - rhs0) / cr[1]));
         } else {
-            dq = (cr[0] - fl - rhs0) / cr[1];
+            st_relaxed(t.tdq + cell, unsentinel((cr[0] - fl - rhs0) / cr[1]));
         }
-        t.tdq[cell] = dq;
-        st_release((kForward ? flagF : flagB) + cell, epoch);
     }
     return true;
 }
 
 template <class T, bool kForward>
-__device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int *flagF,
-                                             int *flagB, int epoch, int group, int wgroup0, int ngroups, int lane,
-                                             int base)
+__device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int group,
+                                             int wgroup0, int ngroups, int lane, int base)
 {
     const int npos = kForward ? g.nFwdPos : g.nBwdPos;
     const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
@@ -445,8 +447,7 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
         int2 ninfo = make_int2(-1, 0);
         int4 nen = make_int4(-1, 0, 0, 0);
         if (pn < npos) { ninfo = __ldg(pinfo + pn); nen = __ldg(ent + (size_t)pn * kGroup + lane); }
-        if (!sa_sweep_position<T, kForward>(g, t, red, flagF, flagB, epoch, info, en, ninfo, nen, lane, base))
-            return false;
+        if (!sa_sweep_position<T, kForward>(g, t, red, info, en, ninfo, nen, lane, base)) return false;
         info = ninfo;
         en = nen;
         p = pn;
@@ -455,21 +456,32 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red, int *flagF,
-                                                                 int *flagB, int epoch)
+__global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kGroup, lane = tid % kGroup;
     const int ngroups = (gridDim.x * blockDim.x) / kGroup;
     const int wgroup0 = group & ~(32 / kGroup - 1);
     const int base = (threadIdx.x & 31) & ~(kGroup - 1);
-    if (!sa_sweep_all<T, true>(g, t, red, flagF, flagB, epoch, group, wgroup0, ngroups, lane, base)) return;
-    sa_sweep_all<T, false>(g, t, red, flagF, flagB, epoch, group, wgroup0, ngroups, lane, base);
+    if (!sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base)) return;
+    sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base);
+}
+
+// Fills the SA sweep's output records with the sentinel.
+template <class T>
+__global__ void __launch_bounds__(kThreads) sa_sweep_reset_kernel(int n, T *a, T *b, T *c)
+{
+    const T s = sweep_sentinel<T>();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        a[i] = s;
+        b[i] = s;
+        c[i] = s;
+    }
 }
 
 template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
-                    int *flagF, int *flagB, int epoch, int numSMs, cudaStream_t s)
+                    int numSMs, cudaStream_t s)
 {
     (void)c; (void)w;
     static int perSMcache[2] = {-1, -1};
@@ -487,12 +499,12 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
         if (v > 0 && blocks > v) blocks = v;
     }
     if (blocks < 1) blocks = 1;
+    const int rb = std::min((g.nCell + kThreads - 1) / kThreads, numSMs * 16);
+    sa_sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, t.tdqf, t.tdfl, t.tdq);
     DevGrid gg = g;
     TurbWork<T> tt = t;
     Reduce *rr = red;
-    int *ff = flagF, *fb = flagB;
-    int ep = epoch;
-    void *args[] = {&gg, &tt, &rr, &ff, &fb, &ep};
+    void *args[] = {&gg, &tt, &rr};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((void *)sa_lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
@@ -540,7 +552,7 @@ void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t
                                         const TurbWork<T> &, Reduce *, const MlpDev *, unsigned long long *, int, \
                                         cudaStream_t);                                                            \
     template int launch_sa_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, const TurbWork<T> &,       \
-                                    Reduce *, int *, int *, int, int, cudaStream_t);                              \
+                                    Reduce *, int, cudaStream_t);                                                 \
     template void launch_sa_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const TurbWork<T> &,     \
                                       cudaStream_t);                                                              \
     template void launch_import_turb<T>(const DevGrid &, const double *, const TurbWork<T> &, const Work<T> &,    \
