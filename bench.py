@@ -233,6 +233,9 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
     # warm-up
     s.Relaxation(args.warmup)
     torch.cuda.synchronize()
+    # the learned source's training set also holds the early, near-uniform
+    # flow: samples after the warm-up (untimed) join those of the final state
+    early = s.capture_sa_samples()[:2] if train else None
     # timed region (device): K iterations
     sampler = ClockSampler(dev)
     sampler.start()
@@ -267,15 +270,25 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
             b.synchronize()
             acc[n] += a.elapsed_time(b)
     phase_ms = {n: v / reps for n, v in acc.items()}
+    iters = s.step
     forces = s.AirForceCoef() if params.get("viscousType", 0) > 0 else None
+    vist = None
+    if params.get("viscousType", 0) == 3:
+        # a number measured on a diverged turbulence field is no number
+        vist = s.get(S.PHX_VIST)[:nc]
+        if not (np.all(np.isfinite(s.get(S.PHX_Q_TURB)[:nc])) and np.all(np.isfinite(vist))):
+            raise RuntimeError(f"{precision} run: the SA field is not finite after {s.step} iterations")
     mlp_info = None
     if mlp_blob is not None:
         mlp_info = {"cells_learned": s.mlp_cells()}
     if train:
         # training set of the learned SA source: features and exact targets of
-        # this run's current state, a seeded subsample of 2M cells, 20 epochs,
-        # batch 8192, Adam lr 1e-3 (the trainer runs on this GPU)
+        # this run's state after the warm-up and its current state, a seeded
+        # subsample of 2M cells, 20 epochs, batch 8192, Adam lr 1e-3 (the
+        # trainer runs on this GPU)
         f, t, _, _ = s.capture_sa_samples()
+        f, t = np.concatenate([early[0], f]), np.concatenate([early[1], t])
+        early = None
         rng = np.random.default_rng(0)
         if len(t) > 2_000_000:
             sel = rng.choice(len(t), 2_000_000, replace=False)
@@ -286,7 +299,7 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
                     "train_s": round(time.perf_counter() - t1, 2), "blob": s.mlp_blob()}
     if not e2e:
         res = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=None, nc=nc, mesh=m,
-                   hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info)
+                   hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info, vist=vist, iters=iters)
         s.close()
         return res
     # end-to-end through the C ABI with pinned host buffers
@@ -305,7 +318,7 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t1) / e2e_steps
     res = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=e2e_s, nc=nc, mesh=m,
-               hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info)
+               hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info, vist=vist, iters=iters)
     s.close()
     return res
 
@@ -440,12 +453,19 @@ def main():
             line["accuracy_vs_fp64"] = {"dCL": abs(r["forces"]["CL"] - r64["forces"]["CL"]),
                                         "dCD": abs(r["forces"]["CD"] - r64["forces"]["CD"]),
                                         "CL_fp64": r64["forces"]["CL"], "CD_fp64": r64["forces"]["CD"],
-                                        "after_iterations": args.warmup + args.steps}
+                                        "after_iterations": r["iters"]}
+            if r["vist"] is not None and r64["vist"] is not None:
+                # eddy viscosity, max-norm relative difference over all cells
+                line["accuracy_vs_fp64"]["dVIST_rel"] = float(np.max(np.abs(r["vist"] - r64["vist"]))
+                                                             / np.max(np.abs(r64["vist"])))
+                line["accuracy_vs_fp64"]["dVIST_rms_rel"] = float(np.sqrt(np.mean((r["vist"] - r64["vist"]) ** 2))
+                                                                 / np.sqrt(np.mean(r64["vist"] ** 2)))
+                line["accuracy_vs_fp64"]["VIST_max_fp64"] = float(np.max(r64["vist"]))
     line["config"]["sa_source"] = (("learned (MLP, exact outside its hull)" if blob is not None else "exact")
                                    if sa else None)
     if blob is not None:
         line["mlp"] = dict((r64 or {}).get("mlp") or {"loaded": args.mlp_blob}, cells_learned_per_iteration=round(
-            r["mlp"]["cells_learned"] / (args.warmup + args.steps + max(1, min(args.steps, 10))), 1))
+            r["mlp"]["cells_learned"] / r["iters"], 1), cells=nc)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.workload)
     if rank == 0:

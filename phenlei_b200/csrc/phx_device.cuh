@@ -77,12 +77,12 @@ __device__ __forceinline__ T sutherland(T t, T s) { return t * sqrt(t) * (T(1) +
 
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// Sweep geometry of the LU-SGS dataflow sweeps: a lane group of kGroup lanes
-// per cell, kSweepPad groups per warp.
+// Sweep geometry of the LU-SGS dataflow sweeps: a slot of kSweepLanes lanes
+// per schedule position, kSweepSlots slots per warp.
 static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
 static constexpr int kSweepThreads = 256;
-static constexpr int kGroup = kSweepGroup;            // lanes per cell
-static_assert(kGroup * kSweepPad == 32, "one warp holds kSweepPad lane groups");
+static_assert(kSweepLanes * kSweepSlots == 32, "one warp holds kSweepSlots slots");
+static_assert(kSweepMaxEntries == 2 * kSweepLanes, "a cell spans at most two adjacent slots");
 
 // Write-once sweep records.  Before a sweep every element of its output
 // records holds the sentinel, a NaN whose sign and payload no arithmetic

@@ -16,8 +16,8 @@
 
 namespace phx {
 int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch, float lr, unsigned long long seed,
-              MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float &tscale, double &lastLoss,
-              cudaStream_t s);
+              MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float *occ, float &tscale,
+              double &lastLoss, cudaStream_t s);
 void mlp_pack(const MlpHostWeights &w, std::vector<uint16_t> &w1c, std::vector<uint16_t> &w2c,
               std::vector<uint16_t> &w3c);
 }  // namespace phx
@@ -25,9 +25,10 @@ void mlp_pack(const MlpHostWeights &w, std::vector<uint16_t> &w1c, std::vector<u
 using namespace phx;
 
 // Flat model blob of phx_mlp_get / phx_mlp_set: weights (w1 b1 w2 b2 w3 b3 w4
-// b4, row-major [out][in]), then mean, 1/std, hull lo, hull hi (6 each), target scale.
+// b4, row-major [out][in]), then mean, 1/std, hull lo, hull hi (6 each), target
+// scale, and the hull's occupied (ln chi, ln s) bins (kMlpGrid x kMlpGrid, 0 / 1).
 static constexpr int kMlpWeightFloats = sizeof(MlpHostWeights) / sizeof(float);
-static constexpr int kMlpBlobFloats = kMlpWeightFloats + 4 * kMlpIn + 1;
+static constexpr int kMlpBlobFloats = kMlpWeightFloats + 4 * kMlpIn + 1 + kMlpGrid * kMlpGrid;
 
 struct phx_ctx {
     int device = 0;
@@ -56,6 +57,7 @@ struct phx_ctx {
     std::vector<float> mlpBlob;
     __nv_bfloat16 *mlpW = nullptr;          // w1c | w2c | w3c
     float *mlpF = nullptr;                  // b1 | b2 | b3 | w4
+    uint8_t *mlpOcc = nullptr;              // occupied hull bins
     unsigned long long *nmlp = nullptr;     // cells that used the learned source (running count)
     double *forces = nullptr;               // [16] wall force sums
     Reduce *red = nullptr;
@@ -448,6 +450,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     r |= dalloc(ctx, &ctx->nmlp, 1);
     r |= dalloc(ctx, &ctx->mlpW, (size_t)kMlpH * kMlpK1 + 2 * (size_t)kMlpH * kMlpH);
     r |= dalloc(ctx, &ctx->mlpF, 4 * (size_t)kMlpH);
+    r |= dalloc(ctx, &ctx->mlpOcc, (size_t)kMlpGrid * kMlpGrid);
     if (r) return r;
     PHX_CUDA(ctx, cudaMemset(ctx->nmlp, 0, sizeof(unsigned long long)));
     const double nu = ctx->nc.nutInf;
@@ -619,7 +622,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         for (int f = 0; f < nf; ++f) { c2f[fill[h.left[f]]++] = f; if (f >= nb) c2f[fill[h.right[f]]++] = f; }
     }
     for (int c = 0; c < nc; ++c)
-        if (c2f_off[c + 1] - c2f_off[c] > 8) { delete ctx; return PHX_ERR_ARG; }  // sweep lane groups hold 8 faces
+        if (c2f_off[c + 1] - c2f_off[c] > kSweepMaxEntries) { delete ctx; return PHX_ERR_ARG; }  // two sweep slots
 
     // storage order
     const std::vector<int> ord = morton_order(nc, ctx->geom[7].data(), ctx->geom[8].data(), ctx->geom[9].data());
@@ -638,34 +641,57 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     // storage index of any reference cell or ghost (ghost of reference boundary face f: nc + f)
     auto sidx = [&](int c) { return c < nc ? rank[c] : nc + fpos[c - nc]; };
 
-    // LU-SGS level schedules from the reference's cell numbers
-    std::vector<int> lev(nc, 0);
+    // LU-SGS level schedules from the reference's cell numbers, with each
+    // cell's entry count (neighbours on the sweep's side; the backward sweep
+    // also reads the ghosts of the cell's boundary faces)
+    std::vector<int> lev(nc, 0), cntF(nc, 0), cntB(nc, 0);
     int nfl = 0;
     for (int c = 0; c < nc; ++c) {
         int l = 0;
         for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
             const int f = c2f[j];
-            if (f < nb) continue;
+            if (f < nb) { cntB[c]++; continue; }
             const int o = h.left[f] == c ? h.right[f] : h.left[f];
-            if (o < c) l = std::max(l, lev[o] + 1);
+            if (o < c) { l = std::max(l, lev[o] + 1); cntF[c]++; }
+            else cntB[c]++;
         }
         lev[c] = l;
         nfl = std::max(nfl, l + 1);
     }
-    // Each level is padded with idle positions (-1) to a multiple of
-    // kSweepPad, the lane groups of one warp, so that the positions one warp
-    // takes together always lie in one level and never depend on each other.
-    auto bucket = [&](int nlev, std::vector<int> &cells, std::vector<int> &off, bool ascending) {
-        off.assign(nlev + 1, 0);
-        for (int c = 0; c < nc; ++c) off[lev[c] + 1]++;
-        for (int l = 0; l < nlev; ++l) off[l + 1] = off[l] + (off[l + 1] + kSweepPad - 1) / kSweepPad * kSweepPad;
+    // Positions are slots of kSweepLanes lanes.  A cell with more entries
+    // than one slot holds takes two adjacent slots (the second continues its
+    // entries).  In each level the two-slot cells come first, so their slot
+    // pairs start at even slot numbers and never straddle a warp, and each
+    // level is padded with idle slots (-1) to a multiple of kSweepSlots, the
+    // slots of one warp, so that the slots one warp takes together always lie
+    // in one level and never depend on each other.
+    auto bucket = [&](int nlev, const std::vector<int> &cnt, std::vector<int> &cells, std::vector<uint8_t> &cont,
+                      bool ascending) {
+        std::vector<int> nbig(nlev, 0), nsmall(nlev, 0), off(nlev + 1, 0);
+        for (int c = 0; c < nc; ++c) (cnt[c] > kSweepLanes ? nbig : nsmall)[lev[c]]++;
+        for (int l = 0; l < nlev; ++l)
+            off[l + 1] = off[l] + (2 * nbig[l] + nsmall[l] + kSweepSlots - 1) / kSweepSlots * kSweepSlots;
         cells.assign(off[nlev], -1);
-        std::vector<int> fill(off.begin(), off.end() - 1);
-        if (ascending) for (int c = 0; c < nc; ++c) cells[fill[lev[c]]++] = c;
-        else for (int c = nc - 1; c >= 0; --c) cells[fill[lev[c]]++] = c;
+        cont.assign(off[nlev], 0);
+        std::vector<int> fbig(off.begin(), off.end() - 1), fsmall(nlev);
+        for (int l = 0; l < nlev; ++l) fsmall[l] = off[l] + 2 * nbig[l];
+        auto put = [&](int c) {
+            const int l = lev[c];
+            if (cnt[c] > kSweepLanes) {
+                cells[fbig[l]] = c;
+                cells[fbig[l] + 1] = c;
+                cont[fbig[l] + 1] = 1;
+                fbig[l] += 2;
+            } else {
+                cells[fsmall[l]++] = c;
+            }
+        };
+        if (ascending) for (int c = 0; c < nc; ++c) put(c);
+        else for (int c = nc - 1; c >= 0; --c) put(c);
     };
-    std::vector<int> fwd_cells, fwd_off, bwd_cells, bwd_off;
-    bucket(nfl, fwd_cells, fwd_off, true);
+    std::vector<int> fwd_cells, bwd_cells;
+    std::vector<uint8_t> fwd_cont, bwd_cont;
+    bucket(nfl, cntF, fwd_cells, fwd_cont, true);
     std::fill(lev.begin(), lev.end(), 0);
     int nbl = 0;
     for (int c = nc - 1; c >= 0; --c) {
@@ -679,65 +705,52 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         lev[c] = l;
         nbl = std::max(nbl, l + 1);
     }
-    bucket(nbl, bwd_cells, bwd_off, false);
-    int maxw = 1;
-    for (int l = 0; l < nfl; ++l) maxw = std::max(maxw, fwd_off[l + 1] - fwd_off[l]);
-    for (int l = 0; l < nbl; ++l) maxw = std::max(maxw, bwd_off[l + 1] - bwd_off[l]);
+    bucket(nbl, cntB, bwd_cells, bwd_cont, false);
 
-    // sweep entry tables (storage indices), in schedule order and the cell's face order
-    auto entries = [&](std::vector<int> &cells, bool forward, std::vector<int> &eoff, std::vector<int> &enb,
-                       std::vector<int> &ef, std::vector<int> &ec) {
-        const int npos = (int)cells.size();
-        eoff.assign(npos + 1, 0);
-        enb.clear(); ef.clear(); ec.clear();
-        for (int i = 0; i < npos; ++i) {
-            const int c = cells[i];
-            if (c < 0) { eoff[i + 1] = eoff[i]; continue; }
-            for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
-                const int f = c2f[j];
-                int nbr = -1;
-                bool isLeft = true;
-                if (f < nb) {
-                    if (!forward) nbr = nc + f;
-                } else {
-                    isLeft = h.left[f] == c;
-                    const int o = isLeft ? h.right[f] : h.left[f];
-                    if (forward ? (o < c) : (o > c)) nbr = o;
-                }
-                if (nbr < 0) continue;
-                enb.push_back(sidx(nbr));
-                ef.push_back(isLeft ? fpos[f] : (int)((unsigned)fpos[f] | 0x80000000u));
-                ec.push_back(2 * fpos[f] + (isLeft ? 0 : 1));
+    // sweep entries (storage indices) of each cell in the cell's face order:
+    // {neighbour, face (sign bit set when the normal points into the cell),
+    // index of the face use's factors (2 f + side), 0}
+    auto cell_entries = [&](int c, bool forward, std::vector<int4> &e) {
+        e.clear();
+        for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+            const int f = c2f[j];
+            int nbr = -1;
+            bool isLeft = true;
+            if (f < nb) {
+                if (!forward) nbr = nc + f;
+            } else {
+                isLeft = h.left[f] == c;
+                const int o = isLeft ? h.right[f] : h.left[f];
+                if (forward ? (o < c) : (o > c)) nbr = o;
             }
-            eoff[i + 1] = (int)enb.size();
-            cells[i] = rank[c];
+            if (nbr < 0) continue;
+            e.push_back(make_int4(sidx(nbr), isLeft ? fpos[f] : (int)((unsigned)fpos[f] | 0x80000000u),
+                                  2 * fpos[f] + (isLeft ? 0 : 1), 0));
         }
     };
-    std::vector<int> fe_off, fe_nb, fe_f, fe_c, be_off, be_nb, be_f, be_c;
-    entries(fwd_cells, true, fe_off, fe_nb, fe_f, fe_c);
-    entries(bwd_cells, false, be_off, be_nb, be_f, be_c);
-    // per position {cell, entry count} and the entries padded to one lane group
-    // (kSweepGroup slots; neighbour -1 on unused slots), so a lane reads its
-    // entry with one load and no offset lookup
-    auto pack = [&](const std::vector<int> &cells, const std::vector<int> &eoff, const std::vector<int> &enb,
-                    const std::vector<int> &ef, const std::vector<int> &ec, std::vector<int2> &pinfo,
-                    std::vector<int4> &ent) {
+    // per slot {storage cell, entry count} ({cell, -1} on the second slot of a
+    // two-slot cell) and kSweepLanes entries (neighbour -1 on unused lanes), so
+    // a lane reads its entry with one load and no offset lookup
+    auto pack = [&](const std::vector<int> &cells, const std::vector<uint8_t> &cont, bool forward,
+                    std::vector<int2> &pinfo, std::vector<int4> &ent) {
         const size_t npos = cells.size();
         pinfo.resize(npos);
-        ent.assign(npos * kSweepGroup, make_int4(-1, 0, 0, 0));
+        ent.assign(npos * kSweepLanes, make_int4(-1, 0, 0, 0));
+        std::vector<int4> e;
         for (size_t i = 0; i < npos; ++i) {
-            const int n = eoff[i + 1] - eoff[i];
-            pinfo[i] = make_int2(cells[i], n);
-            for (int k = 0; k < n; ++k) {
-                const int e = eoff[i] + k;
-                ent[i * kSweepGroup + k] = make_int4(enb[e], ef[e], ec[e], 0);
-            }
+            const int c = cells[i];
+            if (c < 0) { pinfo[i] = make_int2(-1, 0); continue; }
+            cell_entries(c, forward, e);
+            const int n = (int)e.size();
+            pinfo[i] = make_int2(rank[c], cont[i] ? -1 : n);
+            const int k0 = cont[i] ? kSweepLanes : 0;
+            for (int k = k0; k < std::min(n, k0 + kSweepLanes); ++k) ent[i * kSweepLanes + (k - k0)] = e[k];
         }
     };
     std::vector<int2> fwd_pinfo, bwd_pinfo;
     std::vector<int4> fwd_ent, bwd_ent;
-    pack(fwd_cells, fe_off, fe_nb, fe_f, fe_c, fwd_pinfo, fwd_ent);
-    pack(bwd_cells, be_off, be_nb, be_f, be_c, bwd_pinfo, bwd_ent);
+    pack(fwd_cells, fwd_cont, true, fwd_pinfo, fwd_ent);
+    pack(bwd_cells, bwd_cont, false, bwd_pinfo, bwd_ent);
 
     // boundary classification (storage face order)
     std::vector<int32_t> bkind(nb), btype(nb);
@@ -839,7 +852,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     DevGrid &g = ctx->g;
     g.nCell = nc; g.nBFace = nb; g.nFace = nf; g.nTotal = nt;
     g.avgVol = avgVol;
-    g.nFwdLevels = nfl; g.nBwdLevels = nbl; g.maxLevelWidth = maxw;
+    g.nFwdLevels = nfl; g.nBwdLevels = nbl;
     g.nFwdPos = (int)fwd_cells.size(); g.nBwdPos = (int)bwd_cells.size();
     g.walldist = nullptr;
     int rc = 0;
@@ -1260,6 +1273,10 @@ static int mlp_install(phx_ctx *ctx, const float *blob)
         m.hi[k] = norm[3 * kMlpIn + k];
     }
     m.tscale = norm[4 * kMlpIn];
+    std::vector<uint8_t> occ(kMlpGrid * kMlpGrid);
+    for (int b = 0; b < kMlpGrid * kMlpGrid; ++b) occ[b] = norm[4 * kMlpIn + 1 + b] != 0.0f ? 1 : 0;
+    PHX_CUDA(ctx, cudaMemcpy(ctx->mlpOcc, occ.data(), occ.size(), cudaMemcpyHostToDevice));
+    m.occ = ctx->mlpOcc;
     ctx->mlpBlob.assign(blob, blob + kMlpBlobFloats);
     ctx->mlpReady = true;
     return PHX_OK;
@@ -1314,7 +1331,7 @@ int phx_mlp_train(phx_ctx *ctx, const float *features, const float *targets, int
     float tscale = 1.0f;
     double loss = 0.0;
     const int e = mlp_train(features, targets, n, epochs, batch, (float)lr, seed, w, norm, norm + kMlpIn,
-                            norm + 2 * kMlpIn, norm + 3 * kMlpIn, tscale, loss, ctx->stream);
+                            norm + 2 * kMlpIn, norm + 3 * kMlpIn, norm + 4 * kMlpIn + 1, tscale, loss, ctx->stream);
     if (e) return fail(ctx, PHX_ERR_CUDA, std::string("MLP training failed: ") + cudaGetErrorString((cudaError_t)e));
     norm[4 * kMlpIn] = tscale;
     std::memcpy(blob.data(), &w, sizeof(MlpHostWeights));

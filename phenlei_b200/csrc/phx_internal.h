@@ -43,8 +43,9 @@ constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
 constexpr int kFlux = 16;  // face flux record: inviscid F0..4 (times area) | inviscid and viscous
                            // spectral parts | pad | viscous F1..4 (times area; F0 is zero) | pad
 constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | viscous spectral term
-constexpr int kSweepPad = 4; // LU-SGS lane groups per warp: schedule levels are padded to this multiple
-constexpr int kSweepGroup = 8; // lanes (neighbour entries) per cell in the LU-SGS sweeps
+constexpr int kSweepLanes = 4;   // LU-SGS lanes (neighbour entries) per schedule slot
+constexpr int kSweepSlots = 8;   // slots per warp: schedule levels are padded to this multiple
+constexpr int kSweepMaxEntries = 2 * kSweepLanes;   // entries of a cell: one slot, or two adjacent slots
 // Spalart-Allmaras records
 constexpr int kTr = 4;     // trec: nu~ | eddy viscosity | laminar viscosity of the NS step | pad
 constexpr int kTg = 4;     // tgrad: d nu~ / dx, dy, dz | pad
@@ -74,16 +75,16 @@ struct DevGrid {
     const int32_t *bkind;        // [nBFace] BcKind
     const int32_t *btype;        // [nBFace] bcType
     const uint8_t *farfield_adj; // [nCell] 1 if the cell touches a limiter-zeroing boundary
-    // LU-SGS schedules, positions in level order (levels padded with idle
-    // positions): pinfo = {storage cell or -1, entry count}; ent = kSweepGroup
-    // slots per position, the neighbours on the sweep's side in the cell's face
-    // order: {neighbour (-1: unused slot), face (sign bit set when the normal
-    // points into the cell), index of the face use's factors (2 f + side), 0}.
+    // LU-SGS schedules, slots in level order (levels padded with idle slots):
+    // pinfo = {storage cell or -1, entry count}, {cell, -1} on the second slot
+    // of a cell with more than kSweepLanes entries; ent = kSweepLanes entries
+    // per slot, the neighbours on the sweep's side in the cell's face order:
+    // {neighbour (-1: unused lane), face (sign bit set when the normal points
+    // into the cell), index of the face use's factors (2 f + side), 0}.
     const int2 *fwd_pinfo, *bwd_pinfo;
     const int4 *fwd_ent, *bwd_ent;
     int nFwdLevels, nBwdLevels;
-    int nFwdPos, nBwdPos;        // schedule positions incl. idle padding (-1 cells)
-    int maxLevelWidth;           // widest LU-SGS level (cells)
+    int nFwdPos, nBwdPos;        // schedule slots incl. idle padding (-1 cells)
     double avgVol;
 };
 

@@ -648,30 +648,38 @@ void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduc
 // factors were computed by the residual pass.
 // ---------------------------------------------------------------------------
 
-// Ghost-cell dq of boundary face f from the owner's forward dq
+// Ghost-cell dq of a boundary face from the owner's forward dq dl
 // (SetGhostDQLUSGS, NSSolverUnstruct.cpp:14767-14810; SetSymmBCGhostDQLUSGS
-// :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).
+// :14812-14915; SetWallBCGhostDQLUSGS :14917-15006; far field 0).  The
+// dq-independent terms of the symmetry ghost (the owner's conservative state
+// Q, p_ghost / (gamma - 1), rho |u|^2 of the ghost) were formed before the
+// wait by ghost_static.
 template <class T>
-__device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, const T *dl,
-                                         T *o)
+struct GhostStatic {
+    T Q[5];
+    T pmg, rmu2;
+};
+
+template <class T>
+__device__ __forceinline__ void ghost_static(const T *ql, const T *qg, T gm, GhostStatic<T> &s)
 {
-    const int le = g.lr[f].x, re = g.nCell + f;
-    const int kind = g.bkind[f];
+    const T r = ql[0], u = ql[1], v = ql[2], ww = ql[3], pp = ql[4];
+    const T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
+    s.Q[0] = r; s.Q[1] = r * u; s.Q[2] = r * v; s.Q[3] = r * ww; s.Q[4] = r * em;
+    const T rm = qg[0], um = qg[1], vm = qg[2], wm = qg[3], pm = qg[4];
+    s.pmg = pm / (gm - T(1));
+    s.rmu2 = rm * (um * um + vm * vm + wm * wm);
+}
+
+template <class T>
+__device__ __forceinline__ void ghost_dq(int kind, T xn, T yn, T zn, const GhostStatic<T> &s, const T *dl, T *o)
+{
 #pragma unroll
     for (int k = 0; k < 5; ++k) o[k] = T(0);
     if (kind == BK_SYMMETRY) {
-        T ql[8], qg[8];
-        ld8(w.qrec + (size_t)le * kQ, ql);
-        ld8(w.qrec + (size_t)re * kQ, qg);
-        const T r = ql[0], u = ql[1], v = ql[2], ww = ql[3], pp = ql[4];
-        const T gm = (T)c.gama;
-        const T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
-        T Q[5] = {r, r * u, r * v, r * ww, r * em};
-        for (int k = 0; k < 5; ++k) Q[k] += dl[k];
-        const T rm = qg[0], um = qg[1], vm = qg[2], wm = qg[3], pm = qg[4];
-        double fr[4];
-        ld4(g.frec + (size_t)f * kF, fr);
-        const T xn = (T)fr[0], yn = (T)fr[1], zn = (T)fr[2];
+        T Q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) Q[k] = s.Q[k] + dl[k];
         o[0] = dl[0];
         T rvn = T(2) * (xn * dl[1] + yn * dl[2] + zn * dl[3]);
         o[1] = dl[1] - xn * rvn;
@@ -680,63 +688,106 @@ __device__ __forceinline__ void ghost_dq(const DevGrid &g, const NsConst &c, con
         rvn = T(2) * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
         const T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
         const T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
-        const T g1 = gm - T(1);
-        o[4] = pnew - pm / g1 + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - rm * (um * um + vm * vm + wm * wm));
+        o[4] = pnew - s.pmg + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - s.rmu2);
     } else if (kind == BK_WALL) {
         o[0] = dl[0]; o[1] = -dl[1]; o[2] = -dl[2]; o[3] = -dl[3]; o[4] = dl[4];
     }
 }
 
-// One schedule position of a sweep, processed by a lane group of kGroup
-// lanes (one lane per neighbour entry).  The four groups of a warp run in
-// lockstep: the warp polls until every lane's inputs are final, so no group
-// ever spins while a sibling in the same warp is ready to work, and every
-// shuffle uses the full warp mask.  info.x < 0 marks an idle group (the
-// warp's trip count is uniform).
-// The position's {cell, count} and this lane's entry were loaded one round
-// ahead by the caller (info, en); the next round's (ninfo, nen) are known here,
-// so their records are prefetched into L2 while this position waits.
+// Static inputs of one schedule slot for one lane: the slot, this lane's
+// neighbour entry with its face, MXDQ factors and the neighbour's record,
+// and (lane 0 of the cell's first slot) the cell's residual record, time step
+// and volume.  Loaded into registers one round before the slot is processed,
+// so that only the neighbours' dq are waited for.
+template <class T>
+struct SweepIn {
+    int cell, count;   // cell < 0: idle slot; count < 0: second slot of a two-slot cell
+    int nb, kind;      // neighbour storage index (-1: no entry); boundary kind of a ghost entry
+    T nx, ny, nz, area;
+    T cf[4];
+    T qn[8];
+    T ql[5];           // ghost entries: the owner cell's state
+    T cr[8];
+    T dt, vol;
+};
+
 template <class T, bool kForward>
-__device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
-                                               double mindt, int2 info, int4 en, int2 ninfo, int4 nen, int lane,
-                                               int base)
+__device__ __forceinline__ void sweep_load(const DevGrid &g, const Work<T> &w, int2 info, int4 en, int lane,
+                                           SweepIn<T> &s)
 {
+    s.cell = info.x;
+    s.count = info.y;
+    s.nb = -1;
+    s.kind = -1;
     const int nc = g.nCell;
-    const int cell = info.x;
-    const bool live = cell >= 0;
-    const int e0 = 0, e1 = live ? info.y : 0;
-    const bool has = live && en.x >= 0;
-    // dq-independent loads first: they overlap the waits below
-    int nb = -1, f = 0;
-    T sgn = T(1), nx = 0, ny = 0, nz = 0, area = 0, cf[4] = {0, 0, 0, 0}, qn[8];
-    if (has) {
-        nb = en.x;
-        const int fs = en.y;
-        const int ec = en.z;
-        f = fs & 0x7fffffff;
-        sgn = fs < 0 ? T(-1) : T(1);
+    if (info.x >= 0 && en.x >= 0) {
+        s.nb = en.x;
+        const int f = en.y & 0x7fffffff;
+        const T sgn = en.y < 0 ? T(-1) : T(1);
         double fr[4];
         ld4(g.frec + (size_t)f * kF, fr);
-        nx = sgn * (T)fr[0]; ny = sgn * (T)fr[1]; nz = sgn * (T)fr[2]; area = (T)fr[3];
-        ld4(w.coef + (size_t)ec * kCoef, cf);
-        ld8(w.qrec + (size_t)nb * kQ, qn);
+        s.nx = sgn * (T)fr[0]; s.ny = sgn * (T)fr[1]; s.nz = sgn * (T)fr[2]; s.area = (T)fr[3];
+        ld4(w.coef + (size_t)en.z * kCoef, s.cf);
+        ld8(w.qrec + (size_t)en.x * kQ, s.qn);
+        if (!kForward && en.x >= nc) {
+            s.kind = ld(g.bkind + (en.x - nc));
+            T q8[8];
+            ld8(w.qrec + (size_t)info.x * kQ, q8);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) s.ql[k] = q8[k];
+        }
     }
-    T cr[8], dt = T(0);
-    if (live && lane == 0) {
-        ld8(w.crec + (size_t)cell * kC, cr);
-        dt = w.dtraw[cell];
+    if (info.x >= 0 && info.y >= 0 && lane == 0) {
+        ld8(w.crec + (size_t)info.x * kC, s.cr);
+        s.dt = w.dtraw[info.x];
+        s.vol = (T)g.xrec[(size_t)info.x * kX + 3];
     }
+}
+
+// One schedule slot of a sweep, processed by kSweepLanes lanes (one lane per
+// neighbour entry; a cell with more entries spans two adjacent slots, whose
+// first slot's lane 0 sums all of them).  The eight slots of a warp run in
+// lockstep: the warp polls until every lane's inputs are final, so no slot
+// ever spins while a sibling in the same warp is ready to work, and every
+// shuffle uses the full warp mask.  s.cell < 0 marks an idle slot (the
+// warp's trip count is uniform).
+template <class T, bool kForward>
+__device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
+                                               double mindt, const SweepIn<T> &s, int lane, int base)
+{
+    const int nc = g.nCell;
+    const int cell = s.cell;
+    const bool live = cell >= 0;
+    const bool lead = live && s.count >= 0;   // the cell's first slot
+    const int e1 = lead ? s.count : 0;
+    const bool has = live && s.nb >= 0;
     // wait for the inputs other positions write: the neighbour's dq (forward:
     // its forward dq; backward: its final dq; a ghost's comes from this cell's
     // forward dq) and, backward, this cell's forward delta flux
-    const bool ghost = !kForward && has && nb >= nc;
+    const bool ghost = !kForward && has && s.nb >= nc;
     const T *src1 = !has ? nullptr
                          : ghost ? w.dqfwd + (size_t)cell * kD
-                                 : (kForward ? w.dqfwd : w.dqrec) + (size_t)nb * kD;
-    const T *src2 = (!kForward && live && lane == 0) ? w.dflux + (size_t)cell * kD : nullptr;
+                                 : (kForward ? w.dqfwd : w.dqrec) + (size_t)s.nb * kD;
+    const T *src2 = (!kForward && lead && lane == 0) ? w.dflux + (size_t)cell * kD : nullptr;
     T v1[5], fl[5];
     bool r1 = !src1 || poll5(src1, v1);
     bool r2 = !src2 || poll5(src2, fl);
+    const T gm = (T)c.gama;
+    // dq-independent terms, formed while the first poll is in flight:
+    // the diagonal (NSSolverUnstruct.cpp:15867-15935), 1 / (dt' / vol) +
+    // spectral radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep,
+    // :5717-5745), and the symmetry ghost's static terms
+    T d = T(1);
+    if (lead && lane == 0) {
+        T dt = s.dt;
+        if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
+        dt /= s.vol;
+        d = T(1) / dt;
+        d += s.cr[6];
+        if (c.viscous) d += s.cr[7];
+    }
+    GhostStatic<T> gs;
+    if (ghost && s.kind == BK_SYMMETRY) ghost_static<T>(s.ql, s.qn, gm, gs);
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
@@ -749,27 +800,18 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         if (!r1) r1 = poll5(src1, v1);
         if (!r2) r2 = poll5(src2, fl);
     }
-    // next round's records into L2 (their entries arrived during the wait)
-    if (nen.x >= 0) {
-        prefetch_l2(g.frec + (size_t)(nen.y & 0x7fffffff) * kF);
-        prefetch_l2(w.coef + (size_t)nen.z * kCoef);
-        prefetch_l2(w.qrec + (size_t)nen.x * kQ);
-    }
-    if (lane == 0 && ninfo.x >= 0) {
-        prefetch_l2(w.crec + (size_t)ninfo.x * kC);
-        prefetch_l2(w.dtraw + ninfo.x);
-    }
     T df[5] = {0, 0, 0, 0, 0};
     if (has) {
-        T dq[8];
+        T dq[5];
         if (ghost) {
-            ghost_dq<T>(g, c, w, nb - nc, v1, dq);
+            ghost_dq<T>(s.kind, s.nx, s.ny, s.nz, gs, v1, dq);
         } else {
 #pragma unroll
             for (int k = 0; k < 5; ++k) dq[k] = v1[k];
         }
-        const T gm = (T)c.gama;
-        const T um = qn[1], vm = qn[2], wm = qn[3], c2 = qn[5], hm = qn[6];
+        const T nx = s.nx, ny = s.ny, nz = s.nz, area = s.area;
+        const T um = s.qn[1], vm = s.qn[2], wm = s.qn[3], c2 = s.qn[5], hm = s.qn[6];
+        const T *cf = s.cf;
         const T cits = nx * um + ny * vm + nz * wm;
         const T dc = cits * dq[0] - nx * dq[1] - ny * dq[2] - nz * dq[3];
         const T c2dc = c2 * dc;
@@ -791,44 +833,50 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
         }
     }
     // in-order accumulation (entries are in the cell's face order; lanes
-    // past the cell's entry count contribute exact zeros)
+    // past the cell's entry count are skipped); the second slot's lanes only
+    // when the warp holds a two-slot cell
     T rhs0[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < kGroup; ++k) {
+    for (int k = 0; k < kSweepLanes; ++k) {
 #pragma unroll
         for (int m = 0; m < 5; ++m) {
             const T v = __shfl_sync(0xffffffffu, df[m], base + k);
-            if (k < e1 - e0) rhs0[m] += v;
+            if (k < e1) rhs0[m] += v;
         }
     }
-    if (live && lane == 0) {
-        // Diagonal (NSSolverUnstruct.cpp:15867-15935): 1 / (dt' / vol) + spectral
-        // radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep, :5717-5745)
-        if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
-        dt /= (T)g.xrec[(size_t)cell * kX + 3];
-        T d = T(1) / dt;
-        d += cr[6];
-        if (c.viscous) d += cr[7];
+    if (__any_sync(0xffffffffu, e1 > kSweepLanes)) {
+#pragma unroll
+        for (int k = kSweepLanes; k < kSweepMaxEntries; ++k) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                const T v = __shfl_sync(0xffffffffu, df[m], (base + k) & 31);
+                if (k < e1) rhs0[m] += v;
+            }
+        }
+    }
+    if (lead && lane == 0) {
         T o[5];
         if (kForward) {
             // dq = (res - Ux - L dq) / D, Ux = 0 for a single sweep
             // (LUSGSInitialization, Controller.cpp:1765-1777)
             T fo[5];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) { o[k] = (cr[k] - T(0) - rhs0[k]) / d; fo[k] = T(0) + rhs0[k]; }
+            for (int k = 0; k < 5; ++k) { o[k] = (s.cr[k] - T(0) - rhs0[k]) / d; fo[k] = T(0) + rhs0[k]; }
             publish5(w.dflux + (size_t)cell * kD, fo);
             publish5(w.dqfwd + (size_t)cell * kD, o);
         } else {
 #pragma unroll
-            for (int k = 0; k < 5; ++k) o[k] = (cr[k] - fl[k] - rhs0[k]) / d;
+            for (int k = 0; k < 5; ++k) o[k] = (s.cr[k] - fl[k] - rhs0[k]) / d;
             publish5(w.dqrec + (size_t)cell * kD, o);
         }
     }
     return true;
 }
 
-// One sweep over the schedule: rounds of ngroups positions, the loads of
-// {cell, count} and of this lane's entry issued one round ahead.
+// One sweep over the schedule: rounds of ngroups positions.  The entries
+// ({cell, count} and this lane's neighbour entry) are loaded two rounds
+// ahead and the records they point to one round ahead (into registers, and
+// into L2 a round before that), so a position starts by polling.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red,
                                           double mindt, int group, int wgroup0, int ngroups, int lane, int base)
@@ -836,19 +884,35 @@ __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, co
     const int npos = kForward ? g.nFwdPos : g.nBwdPos;
     const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
     const int4 *ent = kForward ? g.fwd_ent : g.bwd_ent;
+    auto entry = [&](int p, int2 &info, int4 &en) {
+        info = make_int2(-1, 0);
+        en = make_int4(-1, 0, 0, 0);
+        if (p < npos) { info = __ldg(pinfo + p); en = __ldg(ent + (size_t)p * kSweepLanes + lane); }
+    };
     int p = group;
-    int2 info = make_int2(-1, 0);
-    int4 en = make_int4(-1, 0, 0, 0);
-    if (p < npos) { info = __ldg(pinfo + p); en = __ldg(ent + (size_t)p * kGroup + lane); }
+    int2 info;
+    int4 en;
+    entry(p, info, en);
+    SweepIn<T> cur;
+    sweep_load<T, kForward>(g, w, info, en, lane, cur);
+    entry(p + ngroups, info, en);   // entries of the next round
     for (int p0 = wgroup0; p0 < npos; p0 += ngroups) {
-        const int pn = p + ngroups;
-        int2 ninfo = make_int2(-1, 0);
-        int4 nen = make_int4(-1, 0, 0, 0);
-        if (pn < npos) { ninfo = __ldg(pinfo + pn); nen = __ldg(ent + (size_t)pn * kGroup + lane); }
-        if (!sweep_position<T, kForward>(g, c, w, red, mindt, info, en, ninfo, nen, lane, base)) return false;
-        info = ninfo;
-        en = nen;
-        p = pn;
+        SweepIn<T> nxt;
+        sweep_load<T, kForward>(g, w, info, en, lane, nxt);
+        entry(p + 2 * ngroups, info, en);
+        if (!sweep_position<T, kForward>(g, c, w, red, mindt, cur, lane, base)) return false;
+        // the records of the round after next into L2 (its entries have arrived)
+        if (en.x >= 0) {
+            prefetch_l2(g.frec + (size_t)(en.y & 0x7fffffff) * kF);
+            prefetch_l2(w.coef + (size_t)en.z * kCoef);
+            prefetch_l2(w.qrec + (size_t)en.x * kQ);
+        }
+        if (lane == 0 && info.x >= 0 && info.y >= 0) {
+            prefetch_l2(w.crec + (size_t)info.x * kC);
+            prefetch_l2(w.dtraw + info.x);
+        }
+        cur = nxt;
+        p += ngroups;
     }
     return true;
 }
@@ -857,10 +921,10 @@ template <class T>
 __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int group = tid / kGroup, lane = tid % kGroup;
-    const int ngroups = (gridDim.x * blockDim.x) / kGroup;
-    const int wgroup0 = group & ~(32 / kGroup - 1);   // first group of this warp
-    const int base = (threadIdx.x & 31) & ~(kGroup - 1);
+    const int group = tid / kSweepLanes, lane = tid % kSweepLanes;   // slot lane group
+    const int ngroups = (gridDim.x * blockDim.x) / kSweepLanes;
+    const int wgroup0 = group & ~(kSweepSlots - 1);   // first group of this warp
+    const int base = (threadIdx.x & 31) & ~(kSweepLanes - 1);
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
     if (!sweep_all<T, true>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base)) return;
     sweep_all<T, false>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base);
@@ -893,7 +957,7 @@ static int sweep_blocks(K kernel, int &perSM, const DevGrid &g, int numSMs)
     }
     int blocks = numSMs * perSM;
     const int npos = g.nFwdPos > g.nBwdPos ? g.nFwdPos : g.nBwdPos;
-    const int need = (int)(((long long)npos * kGroup + kSweepThreads - 1) / kSweepThreads);
+    const int need = (int)(((long long)npos * kSweepLanes + kSweepThreads - 1) / kSweepThreads);
     if (blocks > need) blocks = need;
     // PHX_LUSGS_MAX_BLOCKS caps the grid (tuning; tests of many positions per group)
     if (const char *cap = getenv("PHX_LUSGS_MAX_BLOCKS")) {

@@ -125,32 +125,47 @@ __device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __e
 
 // ---------------------------------------------------------------------------
 // Features and target of the learned source, for a cell with nu~ > 0.
-// rate = nu~ / (d^2 Re) is the destruction rate scale: with it the exact NSMB
-// source depends on chi and Omega / rate only (src / (nu~ rate) =
-// cb1 (1 - ft2) S~ / rate - cw1 fw), and the target t = src / (nu~ rate (1 +
-// Omega / rate)) stays of order one.  Features (raw, before standardisation):
-//   f0 = ln chi, f1 = ln(Omega / rate), f2 = ln d, f3 = ln(|grad nu~| d / nu~),
-//   f4 = ln Omega, f5 = ln(|S| / rate)   (|S| = sqrt(2 S_ij S_ij))
+// rate = nu~ / (d^2 Re) is the destruction rate scale.  With ft2 = 0 the
+// NSMB source (TurbSolverUnstr.cpp:2790-2870) divided by nu~ rate is a
+// function of two variables only, chi = nu~ rho / mu and s = Omega / rate:
+// S~ / rate = s + fv2(chi) / kappa^2 (or its clipped form), r = 1 / (kappa^2
+// S~ / rate), src / (nu~ rate) = cb1 S~ / rate - cw1 fw(r).  The target
+// t = src / (nu~ rate (1 + s)) stays of order one, and the six inputs are
+// smooth functions of (chi, s), so the model learns that two-variable
+// function and nothing that varies between states or precisions at equal
+// (chi, s):
+//   f0 = ln chi, f1 = ln s, f2 = fv1(chi), f3 = s / (1 + s), f4 = 1 / (1 + chi),
+//   f5 = ln(1 + s).
+// s is floored at kRateFloor: below it the source is within 0.1 % of its
+// s = 0 value (S~ is clipped and r = 10 when fv2 < 0; S~ / rate moves by
+// 1e-3 otherwise), and a near-uniform region, where the velocity gradients of
+// an FP32 state are exactly zero and those of an FP64 state are round-off,
+// maps to one finite point in both precisions.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void sa_features(float nue, float omega, float smag, float gradn, float olam, float d,
-                                            float oRe, float *f, float &scale)
+constexpr float kRateFloor = 1e-3f;
+
+__device__ __forceinline__ void sa_features(float nue, float omega, float olam, float d, float oRe, float *f,
+                                            float &scale)
 {
     const float rate = nue * oRe / (d * d);
-    const float tiny = 1e-30f;
-    f[0] = __logf(nue * olam + tiny);
-    f[1] = __logf(omega / rate + tiny);
-    f[2] = __logf(d + tiny);
-    f[3] = __logf(gradn * d / nue + tiny);
-    f[4] = __logf(omega + tiny);
-    f[5] = __logf(smag / rate + tiny);
-    scale = nue * rate * (1.0f + omega / rate);
+    const float chi = nue * olam;
+    const float sr = omega / rate;
+    const float s = fmaxf(sr, kRateFloor);
+    const float chi3 = chi * chi * chi;
+    f[0] = __logf(chi);
+    f[1] = __logf(s);
+    f[2] = chi3 / (chi3 + 357.911f);   // fv1, cv1 = 7.1
+    f[3] = s / (1.0f + s);
+    f[4] = 1.0f / (1.0f + chi);
+    f[5] = log1pf(s);
+    scale = nue * rate * (1.0f + sr);
 }
 
-// Inputs of the source for one cell: NS velocity gradients (vorticity and
-// strain-rate magnitudes), nu~, its gradient, rho / mu, wall distance.
+// Inputs of the source for one cell: vorticity magnitude of the NS velocity
+// gradients, nu~, rho / mu, wall distance.
 template <class T>
-__device__ __forceinline__ void sa_cell_inputs(const DevGrid &g, const Work<T> &w, const TurbWork<T> &t, int cell,
-                                               T &nue, T &omega, T &smag, T &gradn2, T &olam, double &d)
+__device__ __forceinline__ void sa_cell_inputs(const DevGrid &g, const Work<T> &w, int cell, T &nue, T &omega,
+                                               T &olam, double &d)
 {
     T tr[4];
     ld4(w.trec + (size_t)cell * kTr, tr);
@@ -160,14 +175,8 @@ __device__ __forceinline__ void sa_cell_inputs(const DevGrid &g, const Work<T> &
     const T *gp = w.grec + (size_t)cell * kG;
     ld8(gp, gr);
     ld8(gp + 8, gr + 8);
-    const T dudx = gr[3], dudy = gr[4], dudz = gr[5], dvdx = gr[6], dvdy = gr[7], dvdz = gr[8];
-    const T dwdx = gr[9], dwdy = gr[10], dwdz = gr[11];
+    const T dudy = gr[4], dudz = gr[5], dvdx = gr[6], dvdz = gr[8], dwdx = gr[9], dwdy = gr[10];
     omega = sqrt((dwdy - dvdz) * (dwdy - dvdz) + (dudz - dwdx) * (dudz - dwdx) + (dvdx - dudy) * (dvdx - dudy));
-    const T sxy = T(0.5) * (dudy + dvdx), sxz = T(0.5) * (dudz + dwdx), syz = T(0.5) * (dvdz + dwdy);
-    smag = sqrt(T(2) * (dudx * dudx + dvdy * dvdy + dwdz * dwdz + T(2) * (sxy * sxy + sxz * sxz + syz * syz)));
-    T tg[4];
-    ld4(t.tgrad + (size_t)cell * kTg, tg);
-    gradn2 = tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2];
     olam = rho / (tr[2] + (T)kSmall);
     d = ld(g.walldist + cell);
 }
@@ -250,19 +259,22 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
         float scale = 0.0f;
         bool useMlp = false;
         if (cell < g.nCell) {
-            T nue, omega, smag, gradn2, olam;
+            T nue, omega, olam;
             double d;
-            sa_cell_inputs<T>(g, w, t, cell, nue, omega, smag, gradn2, olam, d);
+            sa_cell_inputs<T>(g, w, cell, nue, omega, olam, d);
             if (nue > T(0) && c.saSource) {
                 float f[kMlpIn];
-                sa_features((float)nue, (float)omega, (float)smag, sqrtf((float)gradn2), (float)olam, (float)d,
-                            (float)c.oRe, f, scale);
+                sa_features((float)nue, (float)omega, (float)olam, (float)d, (float)c.oRe, f, scale);
                 useMlp = true;
 #pragma unroll
                 for (int k = 0; k < kMlpIn; ++k) {
                     if (c.saSource == 2 && !(f[k] >= mlp.lo[k] && f[k] <= mlp.hi[k])) useMlp = false;
                     x[k] = (f[k] - mlp.mean[k]) * mlp.rstd[k];
                 }
+                // inside the box, the (chi, s) bin must hold training samples
+                if (c.saSource == 2 && useMlp)
+                    useMlp = __ldg(mlp.occ + mlp_bin(f[0], mlp.lo[0], mlp.hi[0]) * kMlpGrid +
+                                   mlp_bin(f[1], mlp.lo[1], mlp.hi[1])) != 0;
             }
         }
         store_row_bf16(sm + kMlpSmemA1, tid, kMlpK1 / 8, x);
@@ -350,15 +362,14 @@ __global__ void __launch_bounds__(kThreads) mlp_capture_kernel(DevGrid g, NsCons
 {
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= g.nCell) return;
-    T nue, omega, smag, gradn2, olam;
+    T nue, omega, olam;
     double d;
-    sa_cell_inputs<T>(g, w, t, cell, nue, omega, smag, gradn2, olam, d);
+    sa_cell_inputs<T>(g, w, cell, nue, omega, olam, d);
     if (!(nue > T(0))) return;
     T src, sspec;
-    sa_source_exact<T>(nue, omega, olam, T(1) / ((T)d * (T)d), gradn2, (T)c.oRe, src, sspec);
+    sa_source_fp64<T>(nue, omega, olam, d, T(0), c.oRe, src, sspec);
     float f[kMlpIn], scale;
-    sa_features((float)nue, (float)omega, (float)smag, sqrtf((float)gradn2), (float)olam, (float)d, (float)c.oRe, f,
-                scale);
+    sa_features((float)nue, (float)omega, (float)olam, (float)d, (float)c.oRe, f, scale);
     const unsigned long long slot = atomicAdd(count, 1ULL);
     if ((long long)slot >= cap) return;
 #pragma unroll
@@ -526,11 +537,11 @@ float uniform(uint64_t &x) { return (float)((splitmix(x) >> 11) * (1.0 / 9007199
 }  // namespace
 
 // Trains the MLP on n samples (raw features [n][6], targets [n]) with Adam and
-// mean-squared error; returns the weights, the normalisation and hull, and the
-// loss of the last epoch (normalised units).  0 on success, else a CUDA error.
+// mean-squared error; returns the weights, the normalisation, the hull (box
+// and occupied bins), and the loss of the last epoch (normalised units).  0 on success, else a CUDA error.
 int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch, float lr, unsigned long long seed,
-              MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float &tscale, double &lastLoss,
-              cudaStream_t s)
+              MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float *occ, float &tscale,
+              double &lastLoss, cudaStream_t s)
 {
     if (n < 2 || batch < 1) return -1;
     // normalisation and hull
@@ -550,6 +561,10 @@ int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch
         rstd[k] = (float)(1.0 / std::sqrt(var));
     }
     tscale = (float)std::sqrt(std::max(yq / n, 1e-30));
+    // occupied (ln chi, ln s) bins: the learned source is used only where training samples fell
+    for (int b = 0; b < kMlpGrid * kMlpGrid; ++b) occ[b] = 0.0f;
+    for (long long i = 0; i < n; ++i)
+        occ[mlp_bin(X[i * kMlpIn], lo[0], hi[0]) * kMlpGrid + mlp_bin(X[i * kMlpIn + 1], lo[1], hi[1])] = 1.0f;
     // initialisation (uniform, fan-in scaled)
     std::vector<float> prm(kNParam, 0.0f);
     uint64_t rs = seed * 0x2545F4914F6CDD1DULL + 1;

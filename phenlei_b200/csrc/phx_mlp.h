@@ -9,6 +9,16 @@ constexpr int kMlpIn = 6;       // input features
 constexpr int kMlpK1 = 16;      // first-layer K padded to one MMA
 constexpr int kMlpH = 64;       // hidden width
 constexpr int kMlpTile = 128;   // cells per CTA tile (MMA M)
+constexpr int kMlpGrid = 64;    // occupancy bins per axis over (f0, f1) = (ln chi, ln s) of the training hull
+
+// Occupancy bin of a feature value over [lo, hi] (host and device alike).
+__host__ __device__ inline int mlp_bin(float v, float lo, float hi)
+{
+    if (!(hi > lo)) return 0;
+    const float t = (v - lo) / (hi - lo) * (float)kMlpGrid;
+    if (!(t >= 0.0f)) return 0;
+    return t >= (float)(kMlpGrid - 1) ? kMlpGrid - 1 : (int)t;
+}
 
 // Weights in the canonical K-major core-matrix layout the MMA reads
 // (byte offset of (n, k) = (n / 8) * sbo + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2,
@@ -22,7 +32,8 @@ struct MlpDev {
     const float *w4;            // [64]
     float b4;
     float mean[kMlpIn], rstd[kMlpIn];  // feature standardisation
-    float lo[kMlpIn], hi[kMlpIn];      // training hull (raw features)
+    float lo[kMlpIn], hi[kMlpIn];      // training hull (raw features): the box
+    const uint8_t *occ;                // and the occupied (f0, f1) bins [kMlpGrid][kMlpGrid]
     float tscale;                      // target scale
 };
 

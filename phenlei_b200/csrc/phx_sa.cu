@@ -299,9 +299,8 @@ __global__ void __launch_bounds__(kThreads) sa_cell_kernel(DevGrid g, NsConst c,
     const T grd2 = tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2];
     const T olam = rho / (visl + (T)kSmall);
     const double d = ld(g.walldist + cell);
-    const T odist2 = T(1) / ((T)d * (T)d);
     T src, sspec;
-    sa_source_exact<T>(nue, omega, olam, odist2, grd2, (T)c.oRe, src, sspec);
+    sa_source_fp64<T>(nue, omega, olam, d, grd2, c.oRe, src, sspec);
     if (c.saSource) {
         // learned source; NaN marks the cells that take the exact source
         const T s = t.tsrc[cell];
@@ -373,28 +372,47 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
 // written.  dq of the ghosts is the ghost residual, which is zero, so ghost
 // entries of the backward sweep add nothing and are skipped.
 // ---------------------------------------------------------------------------
-template <class T, bool kForward>
-__device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int2 info,
-                                                  int4 en, int2 ninfo, int4 nen, int lane, int base)
+// Static inputs of one slot for one lane (loaded a round ahead): neighbour
+// (-1: none or a ghost), its face matrix, and (lane 0 of the cell's first
+// slot) the cell's residual and spectral radius.
+template <class T>
+struct SaSweepIn {
+    int cell, count, nb;
+    T mat, res, spec;
+};
+
+template <class T>
+__device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T> &t, int2 info, int4 en, int lane,
+                                              SaSweepIn<T> &s)
 {
-    const int nc = g.nCell;
-    const int cell = info.x;
-    const bool live = cell >= 0;
-    const int e0 = 0, e1 = live ? info.y : 0;
-    bool has = live && en.x >= 0;
-    int nb = -1;
-    T mat = T(0);
-    if (has) {
-        nb = en.x;
-        if (nb >= nc) has = false;
-        else mat = t.tcoef[en.z];
+    s.cell = info.x;
+    s.count = info.y;
+    s.nb = -1;
+    if (info.x >= 0 && en.x >= 0 && en.x < g.nCell) {
+        s.nb = en.x;
+        s.mat = t.tcoef[en.z];
     }
-    T cr[4] = {0, 0, 0, 0};
-    if (live && lane == 0) ld4(t.tcrec + (size_t)cell * kTc, cr);
+    if (info.x >= 0 && info.y >= 0 && lane == 0) {
+        T cr[4];
+        ld4(t.tcrec + (size_t)info.x * kTc, cr);
+        s.res = cr[0];
+        s.spec = cr[1];
+    }
+}
+
+template <class T, bool kForward>
+__device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *red, const SaSweepIn<T> &s, int lane,
+                                                  int base)
+{
+    const int cell = s.cell;
+    const bool live = cell >= 0;
+    const bool lead = live && s.count >= 0;   // the cell's first slot
+    const int e1 = lead ? s.count : 0;
+    const bool has = live && s.nb >= 0;
     // the neighbour's dq (forward: its forward dq; backward: its final dq)
     // and, backward, this cell's forward delta flux
-    const T *src1 = has ? (kForward ? t.tdqf : t.tdq) + nb : nullptr;
-    const T *src2 = (!kForward && live && lane == 0) ? t.tdfl + cell : nullptr;
+    const T *src1 = has ? (kForward ? t.tdqf : t.tdq) + s.nb : nullptr;
+    const T *src2 = (!kForward && lead && lane == 0) ? t.tdfl + cell : nullptr;
     T v1 = T(0), fl = T(0);
     bool r1 = true, r2 = true;
     if (src1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
@@ -411,26 +429,33 @@ __device__ __forceinline__ bool sa_sweep_position(const DevGrid &g, const TurbWo
         if (!r1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
         if (!r2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
     }
-    if (nen.x >= 0 && nen.x < nc) prefetch_l2(t.tcoef + nen.z);
-    if (lane == 0 && ninfo.x >= 0) prefetch_l2(t.tcrec + (size_t)ninfo.x * kTc);
-    const T df = has ? mat * v1 : T(0);
+    const T df = has ? s.mat * v1 : T(0);
     T rhs0 = T(0);
 #pragma unroll
-    for (int k = 0; k < kGroup; ++k) {
+    for (int k = 0; k < kSweepLanes; ++k) {
         const T v = __shfl_sync(0xffffffffu, df, base + k);
-        if (k < e1 - e0) rhs0 += v;
+        if (k < e1) rhs0 += v;
     }
-    if (live && lane == 0) {
+    if (__any_sync(0xffffffffu, e1 > kSweepLanes)) {
+#pragma unroll
+        for (int k = kSweepLanes; k < kSweepMaxEntries; ++k) {
+            const T v = __shfl_sync(0xffffffffu, df, (base + k) & 31);
+            if (k < e1) rhs0 += v;
+        }
+    }
+    if (lead && lane == 0) {
         if (kForward) {
             st_relaxed(t.tdfl + cell, unsentinel(T(0) + rhs0));
-            st_relaxed(t.tdqf + cell, unsentinel((cr[0] - T(0) - rhs0) / cr[1]));
+            st_relaxed(t.tdqf + cell, unsentinel((s.res - T(0) - rhs0) / s.spec));
         } else {
-            st_relaxed(t.tdq + cell, unsentinel((cr[0] - fl - rhs0) / cr[1]));
+            st_relaxed(t.tdq + cell, unsentinel((s.res - fl - rhs0) / s.spec));
         }
     }
     return true;
 }
 
+// Rounds of ngroups positions; entries loaded two rounds ahead, the face
+// matrices and residual records one round ahead.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int group,
                                              int wgroup0, int ngroups, int lane, int base)
@@ -438,19 +463,27 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
     const int npos = kForward ? g.nFwdPos : g.nBwdPos;
     const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
     const int4 *ent = kForward ? g.fwd_ent : g.bwd_ent;
+    auto entry = [&](int p, int2 &info, int4 &en) {
+        info = make_int2(-1, 0);
+        en = make_int4(-1, 0, 0, 0);
+        if (p < npos) { info = __ldg(pinfo + p); en = __ldg(ent + (size_t)p * kSweepLanes + lane); }
+    };
     int p = group;
-    int2 info = make_int2(-1, 0);
-    int4 en = make_int4(-1, 0, 0, 0);
-    if (p < npos) { info = __ldg(pinfo + p); en = __ldg(ent + (size_t)p * kGroup + lane); }
+    int2 info;
+    int4 en;
+    entry(p, info, en);
+    SaSweepIn<T> cur;
+    sa_sweep_load<T>(g, t, info, en, lane, cur);
+    entry(p + ngroups, info, en);
     for (int p0 = wgroup0; p0 < npos; p0 += ngroups) {
-        const int pn = p + ngroups;
-        int2 ninfo = make_int2(-1, 0);
-        int4 nen = make_int4(-1, 0, 0, 0);
-        if (pn < npos) { ninfo = __ldg(pinfo + pn); nen = __ldg(ent + (size_t)pn * kGroup + lane); }
-        if (!sa_sweep_position<T, kForward>(g, t, red, info, en, ninfo, nen, lane, base)) return false;
-        info = ninfo;
-        en = nen;
-        p = pn;
+        SaSweepIn<T> nxt;
+        sa_sweep_load<T>(g, t, info, en, lane, nxt);
+        entry(p + 2 * ngroups, info, en);
+        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base)) return false;
+        if (en.x >= 0 && en.x < g.nCell) prefetch_l2(t.tcoef + en.z);
+        if (lane == 0 && info.x >= 0 && info.y >= 0) prefetch_l2(t.tcrec + (size_t)info.x * kTc);
+        cur = nxt;
+        p += ngroups;
     }
     return true;
 }
@@ -459,10 +492,10 @@ template <class T>
 __global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int group = tid / kGroup, lane = tid % kGroup;
-    const int ngroups = (gridDim.x * blockDim.x) / kGroup;
-    const int wgroup0 = group & ~(32 / kGroup - 1);
-    const int base = (threadIdx.x & 31) & ~(kGroup - 1);
+    const int group = tid / kSweepLanes, lane = tid % kSweepLanes;
+    const int ngroups = (gridDim.x * blockDim.x) / kSweepLanes;
+    const int wgroup0 = group & ~(kSweepSlots - 1);
+    const int base = (threadIdx.x & 31) & ~(kSweepLanes - 1);
     if (!sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base)) return;
     sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base);
 }
@@ -492,7 +525,7 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
     }
     int blocks = numSMs * perSM;
     const int npos = g.nFwdPos > g.nBwdPos ? g.nFwdPos : g.nBwdPos;
-    const int need = (int)(((long long)npos * kGroup + kSweepThreads - 1) / kSweepThreads);
+    const int need = (int)(((long long)npos * kSweepLanes + kSweepThreads - 1) / kSweepThreads);
     if (blocks > need) blocks = need;
     if (const char *cap = getenv("PHX_LUSGS_MAX_BLOCKS")) {
         const int v = atoi(cap);

@@ -89,4 +89,17 @@ __device__ __forceinline__ void sa_source_exact(T nue, T omega, T olam, T odist2
     spec = part1 + part2;
 }
 
+// The exact source evaluated in FP64 for either working precision.  In the
+// free stream (Omega = 0) the implicit part multiplies d fw / dg = 0 by a
+// d r / d nu~ of order 1e48 / d^4, which overflows FP32 to 0 * inf = NaN; in
+// FP64 the product is the finite zero the reference computes.
+template <class T>
+__device__ __forceinline__ void sa_source_fp64(T nue, T omega, T olam, double d, T grd2, double oRe, T &src, T &spec)
+{
+    double s, p;
+    sa_source_exact<double>((double)nue, (double)omega, (double)olam, 1.0 / (d * d), (double)grd2, oRe, s, p);
+    src = (T)s;
+    spec = (T)p;
+}
+
 }  // namespace phx

@@ -130,6 +130,26 @@ def test_sa_residual_history_100_steps_vs_oracle():
     assert rel_err(s.get(S.PHX_Q_TURB)[: m.n_cell], o.work("qt")[: m.n_cell]) <= 1e-9
 
 
+def test_mixed_sa_from_free_stream_matches_fp64():
+    """Transonic bump parameters (M 0.8, Re 1e7) from the uniform free stream,
+    where the vorticity is exactly zero and the source's implicit part forms
+    products of order 1e48 that overflow FP32: the mixed path keeps nu~ and
+    the eddy viscosity finite and within 1e-3 of the FP64 path after five
+    iterations."""
+    m = M.channel_bump(32, 16, 4, thickness=0.08, wall_spacing=0.001, prism_layers=4)
+    wd = M.wall_distance(m)
+    nc = m.n_cell
+    a = _solver(m, cases.SA_BUMP, wd, "fp64")
+    b = _solver(m, cases.SA_BUMP, wd, "mixed")
+    a.Relaxation(5)
+    b.Relaxation(5)
+    qa, qb = a.get(S.PHX_Q_TURB)[:nc], b.get(S.PHX_Q_TURB)[:nc]
+    assert np.all(np.isfinite(qb))
+    assert rel_err(qb, qa) <= 1e-3
+    assert rel_err(b.get(S.PHX_VIST)[:nc], a.get(S.PHX_VIST)[:nc]) <= 1e-3
+    assert np.max(b.get(S.PHX_VIST)[:nc]) > 0.0
+
+
 def test_sa_requires_wall_distance():
     m = M.channel_bump(16, 8, 2)
     with pytest.raises(S.PhxError):
