@@ -10,6 +10,7 @@
 // tcgen05.ld.  The last layer (64 -> 1) is a dot product on the CUDA cores.
 // Training uses hand-written FP32 forward / backward / Adam kernels.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -121,7 +122,22 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v)
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
+// SiLU of a pair, x sigma(x) = x/2 + (x/2) tanh(x/2), with one
+// tanh.approx.f16x2 for both values: one special-function operation per two
+// activations instead of an exponential and a reciprocal per activation (the
+// special-function unit bounds this kernel).  The half-precision tanh of
+// x/2 (relative error ~2^-11) is below the BF16 rounding the activations get
+// next.
+__device__ __forceinline__ void silu2(float &a, float &b)
+{
+    const float ha = 0.5f * a, hb = 0.5f * b;
+    const __half2 h = __floats2half2_rn(ha, hb);
+    uint32_t t;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&h)));
+    const float2 tf = __half22float2(*reinterpret_cast<const __half2 *>(&t));
+    a = fmaf(ha, tf.x, ha);
+    b = fmaf(hb, tf.y, hb);
+}
 
 // ---------------------------------------------------------------------------
 // Features and target of the learned source, for a cell with nu~ > 0.
@@ -297,7 +313,11 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
             tmem_ld64(taddr, h);
             const float *b = layer == 0 ? mlp.b1 : (layer == 1 ? mlp.b2 : mlp.b3);
 #pragma unroll
-            for (int k = 0; k < kMlpH; ++k) h[k] = silu(h[k] + __ldg(b + k));
+            for (int k = 0; k < kMlpH; k += 2) {
+                h[k] += __ldg(b + k);
+                h[k + 1] += __ldg(b + k + 1);
+                silu2(h[k], h[k + 1]);
+            }
             if (layer == 2) break;
             store_row_bf16(sm + kMlpSmemAct, tid, kMlpH / 8, h);
             fence_async_smem();
@@ -347,7 +367,9 @@ void launch_mlp_source(const DevGrid &g, const NsConst &c, const Work<T> &w, con
         a = true;
     }
     const int ntiles = (g.nCell + kMlpTile - 1) / kMlpTile;
-    int blocks = numSMs * 4;   // 4 CTAs per SM: 4 x 64 TMEM columns, 4 x ~39 KB shared memory
+    // 5 CTAs per SM: 5 x 64 of the 512 TMEM columns, 5 x 39 KB shared memory,
+    // 5 x 128 threads x 96 registers
+    int blocks = numSMs * 5;
     if (blocks > ntiles) blocks = ntiles;
     if (blocks < 1) blocks = 1;
     mlp_source_kernel<T><<<blocks, kMlpTile, kMlpSmemBytes, s>>>(g, c, w, t, mlp, red, nmlp);

@@ -9,7 +9,7 @@ constexpr int kMlpIn = 6;       // input features
 constexpr int kMlpK1 = 16;      // first-layer K padded to one MMA
 constexpr int kMlpH = 64;       // hidden width
 constexpr int kMlpTile = 128;   // cells per CTA tile (MMA M)
-constexpr int kMlpGrid = 64;    // occupancy bins per axis over (f0, f1) = (ln chi, ln s) of the training hull
+constexpr int kMlpGrid = 256;   // occupancy bins per axis over (f0, f1) = (ln chi, ln s) of the training hull
 
 // Occupancy bin of a feature value over [lo, hi] (host and device alike).
 __host__ __device__ inline int mlp_bin(float v, float lo, float hi)

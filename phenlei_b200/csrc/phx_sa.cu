@@ -522,6 +522,10 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
     if (perSM < 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, sa_lusgs_kernel<T>, kSweepThreads, 0);
         if (perSM < 1) perSM = 1;
+        // at most two blocks per SM: the scalar sweep does little work per
+        // poll, and more polling slots only load L2 (16M cells: 4.1 ms at two
+        // blocks per SM against 4.5 ms at six)
+        if (perSM > 2) perSM = 2;
     }
     int blocks = numSMs * perSM;
     const int npos = g.nFwdPos > g.nBwdPos ? g.nFwdPos : g.nBwdPos;
