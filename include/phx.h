@@ -99,7 +99,7 @@ typedef struct {
     double prl, prt;            /* laminar / turbulent Prandtl numbers */
     double tsuth;               /* Sutherland constant, K */
     double wallTemperature;     /* <= 0: adiabatic wall */
-    int32_t gradientName;       /* 0 "ggcell", 1 "lsq" */
+    int32_t gradientName;       /* 0 "ggcell", 1 "lsq", 2 "ggnode" (inviscid and laminar) */
     int32_t uns_limiter_name;   /* 0 "nolim", 1 "vencat" */
     int32_t ivencat;            /* Venkatakrishnan variant (7 supported) */
     double venkatCoeff;

@@ -53,7 +53,8 @@ class _Work(C.Structure):
                 ("visl", _dp), ("vist", _dp), ("dtdx", _dp), ("dtdy", _dp), ("dtdz", _dp),
                 ("res_norm", C.c_double), ("n_negative", C.c_int),
                 ("qt", _dp), ("res_t", _dp), ("spec_t", _dp), ("dqt", _dp), ("matl", _dp), ("matr", _dp),
-                ("dntx", _dp), ("dnty", _dp), ("dntz", _dp)]
+                ("dntx", _dp), ("dnty", _dp), ("dntz", _dp), ("qnode", _dp), ("tnode_prev", _dp),
+                ("have_tnode_prev", C.c_int)]
 
 
 _lib = None
@@ -127,7 +128,7 @@ def make_params(**kw) -> _Params:
     p.prandtl_turb = kw.get("prt", 0.90)
     p.tsuth_nd = kw.get("tsuth_nd", 110.4 / kw.get("refDimensionalTemperature", 288.15))
     p.wall_temperature = kw.get("wallTemperature", -1.0)
-    p.gradient = {"ggcell": 0, "lsq": 1}[kw.get("gradientName", "ggcell")]
+    p.gradient = {"ggcell": 0, "lsq": 1, "ggnode": 2}[kw.get("gradientName", "ggcell")]
     p.limiter = {"nolim": 0, "vencat": 1}[kw.get("uns_limiter_name", "vencat")]
     p.venkat_coeff = kw.get("venkatCoeff", 5.0)
     p.recon_method = kw.get("reconmeth", 1)
@@ -208,7 +209,8 @@ class Oracle:
                             ("vis_spec", (nc,)), ("dt", (nt,)), ("dq", (5, nt)), ("visl", (nt,)),
                             ("vist", (nt,)), ("dtdx", (nt,)), ("dtdy", (nt,)), ("dtdz", (nt,)),
                             ("qt", (nt,)), ("res_t", (nt,)), ("spec_t", (nt,)), ("dqt", (nt,)),
-                            ("matl", (nf,)), ("matr", (nf,)), ("dntx", (nt,)), ("dnty", (nt,)), ("dntz", (nt,))]:
+                            ("matl", (nf,)), ("matr", (nf,)), ("dntx", (nt,)), ("dnty", (nt,)), ("dntz", (nt,)),
+                            ("qnode", (5, mesh.n_node)), ("tnode_prev", (mesh.n_node,))]:
             a = np.zeros(shape)
             self.w_arrays[name] = a
             setattr(w, name, _p(a))
@@ -225,6 +227,7 @@ class Oracle:
 
     def set_state(self, q_cells: np.ndarray, qt_cells=None):
         self.q[:, : self.mesh.n_cell] = q_cells
+        self.w.have_tnode_prev = 0
         if qt_cells is not None:
             self.w_arrays["qt"][: self.mesh.n_cell] = qt_cells
 
@@ -239,6 +242,21 @@ class Oracle:
 
     def work(self, name):
         return self.w_arrays[name]
+
+    def node_values(self):
+        """GG-node node values [5][n_node] and temperature node values [n_node] of
+        the current state, with its boundary values and temperature formed first
+        (what PostSolve hands the next iteration's gradient)."""
+        nn, nt = self.mesh.n_node, self.nt
+        q = self.q.copy()
+        gama, t = np.zeros(nt), np.zeros(nt)
+        L = lib()
+        L.ox_gamma_temperature(C.byref(self.g), C.byref(self.p), _p(q), _p(gama), _p(t))
+        L.ox_ns_boundary(C.byref(self.g), C.byref(self.m), C.byref(self.p), _p(q), _p(gama))
+        L.ox_gamma_temperature(C.byref(self.g), C.byref(self.p), _p(q), _p(gama), _p(t))
+        qn, tn = np.zeros((5, nn)), np.zeros(nn)
+        L.ox_node_values(C.byref(self.g), C.byref(self.m), _p(q), 5, _p(t), _p(qn), _p(tn))
+        return qn, tn
 
     def forces(self):
         """Wall force sums of AirForceCoefParts (16 values) from the current state."""

@@ -1082,6 +1082,142 @@ int ox_update(const ox_grid *g, const ox_metrics *m, const ox_params *p, double 
 
 /* Residual monitor, API/Physics/src/Residual.cpp:534-600 and 184-224 (unit
  * grid scale): sqrt(sum res_rho^2 / nCell). */
+/* Node values of nv cell fields f [nv][nTotal] and the temperature t
+ * (NSSolverUnstruct::ComputeNodeValue, NSSolverUnstruct.cpp:4734-5080, then
+ * ModifyNodeValue, :5083-5116): node boundary types by priority (solid wall,
+ * then far field, then other non-symmetry boundaries); boundary nodes take
+ * 1/distance-weighted face values 0.5 (f_L + f_ghost) of their boundary faces
+ * (solid wall faces, then far-field, then other non-symmetry faces, each
+ * skipping nodes of a higher-priority type); the other nodes, symmetry nodes
+ * included, take 1/distance-weighted values of the cells around them; then
+ * each node value is divided by its weight sum (0 where the sum is not
+ * above SMALL).  fn is [nv][n_node], tn [n_node]. */
+enum { OX_NODE_NO_BC = -1 };
+void ox_node_values(const ox_grid *g, const ox_metrics *m, const double *f, int nv, const double *t, double *fn,
+                    double *tn)
+{
+    int nn = g->n_node, nb = g->n_bface, nc = g->n_cell, nt = ntot(g);
+    int *nbc = malloc(sizeof(int) * nn);
+    double *w = calloc((size_t)nn, sizeof(double));
+    for (int i = 0; i < nn; ++i) nbc[i] = OX_NODE_NO_BC;
+    for (int k = 0; k < nv; ++k) memset(fn + (size_t)k * nn, 0, sizeof(double) * nn);
+    memset(tn, 0, sizeof(double) * nn);
+    /* node boundary types */
+    for (int r = 0; r < g->n_region; ++r) {
+        if (g->region_type[r] != OX_BC_SOLID_SURFACE) continue;
+        for (int fc = 0; fc < nb; ++fc) {
+            if (g->bface_region[fc] != r) continue;
+            for (int j = g->face_off[fc]; j < g->face_off[fc + 1]; ++j) nbc[g->face2node[j]] = OX_BC_SOLID_SURFACE;
+        }
+    }
+    for (int r = 0; r < g->n_region; ++r) {
+        if (g->region_type[r] != OX_BC_FARFIELD) continue;
+        for (int fc = 0; fc < nb; ++fc) {
+            if (g->bface_region[fc] != r) continue;
+            for (int j = g->face_off[fc]; j < g->face_off[fc + 1]; ++j) {
+                int pt = g->face2node[j];
+                if (nbc[pt] == OX_BC_SOLID_SURFACE) continue;
+                nbc[pt] = OX_BC_FARFIELD;
+            }
+        }
+    }
+    for (int r = 0; r < g->n_region; ++r) {
+        int bt = g->region_type[r];
+        for (int fc = 0; fc < nb; ++fc) {
+            if (g->bface_region[fc] != r) continue;
+            if (bt == OX_BC_SOLID_SURFACE || bt == OX_BC_FARFIELD || bt == OX_BC_SYMMETRY) continue;
+            for (int j = g->face_off[fc]; j < g->face_off[fc + 1]; ++j) {
+                int pt = g->face2node[j];
+                if (nbc[pt] == OX_BC_SOLID_SURFACE || nbc[pt] == OX_BC_FARFIELD) continue;
+                nbc[pt] = bt;
+            }
+        }
+    }
+    /* boundary nodes: steps 1 (solid wall), 2 (far field), 3 (others but symmetry) */
+    for (int step = 1; step <= 3; ++step) {
+        for (int r = 0; r < g->n_region; ++r) {
+            int bt = g->region_type[r];
+            int take = step == 1 ? bt == OX_BC_SOLID_SURFACE
+                     : step == 2 ? bt == OX_BC_FARFIELD
+                     : (bt != OX_BC_SOLID_SURFACE && bt != OX_BC_FARFIELD && bt != OX_BC_SYMMETRY);
+            if (!take) continue;
+            for (int fc = 0; fc < nb; ++fc) {
+                if (g->bface_region[fc] != r) continue;
+                int le = g->left[fc], re = nc + fc;
+                for (int j = g->face_off[fc]; j < g->face_off[fc + 1]; ++j) {
+                    int pt = g->face2node[j];
+                    if (step == 2 && nbc[pt] == OX_BC_SOLID_SURFACE) continue;
+                    if (step == 3 && (nbc[pt] == OX_BC_SOLID_SURFACE || nbc[pt] == OX_BC_FARFIELD)) continue;
+                    double dx = g->x[pt] - m->xfc[fc], dy = g->y[pt] - m->yfc[fc], dz = g->z[pt] - m->zfc[fc];
+                    double wt = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+                    for (int k = 0; k < nv; ++k) {
+                        const double *fk = f + (size_t)k * nt;
+                        double qf = 0.5 * (fk[le] + fk[re]);
+                        fn[(size_t)k * nn + pt] += qf * wt;
+                    }
+                    tn[pt] += 0.5 * (t[le] + t[re]) * wt;
+                    w[pt] += wt;
+                }
+            }
+        }
+    }
+    /* step 4: the other nodes from the cells around them */
+    for (int c = 0; c < nc; ++c) {
+        for (int j = g->cell_off[c]; j < g->cell_off[c + 1]; ++j) {
+            int pt = g->cell2node[j];
+            if (nbc[pt] != OX_NODE_NO_BC) continue;
+            double dx = g->x[pt] - m->xcc[c], dy = g->y[pt] - m->ycc[c], dz = g->z[pt] - m->zcc[c];
+            double wt = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+            for (int k = 0; k < nv; ++k) fn[(size_t)k * nn + pt] += f[(size_t)k * nt + c] * wt;
+            tn[pt] += t[c] * wt;
+            w[pt] += wt;
+        }
+    }
+    for (int i = 0; i < nn; ++i) {
+        if (w[i] > OX_SMALL) {
+            for (int k = 0; k < nv; ++k) fn[(size_t)k * nn + i] /= w[i];
+            tn[i] /= w[i];
+        } else {
+            for (int k = 0; k < nv; ++k) fn[(size_t)k * nn + i] = 0.0;
+            tn[i] = 0.0;
+        }
+    }
+    free(nbc);
+    free(w);
+}
+
+/* UnstructGrid::CompGradientGGNode_NEW, Geo_UnstructGrid.cpp:4202-4309: face
+ * values are the averages of the face's node values, except on boundary faces
+ * other than symmetry, which take 0.5 (f_L + f_ghost); divided by the volume;
+ * ghost gradients copy the owner's. */
+void ox_gradient_ggnode(const ox_grid *g, const ox_metrics *m, const double *q, const double *qn, double *dx,
+                        double *dy, double *dz)
+{
+    int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
+    for (int c = 0; c < nt; ++c) dx[c] = dy[c] = dz[c] = 0.0;
+    for (int f = 0; f < g->n_face; ++f) {
+        int le = g->left[f], re = f < nb ? nc + f : g->right[f];
+        double qf;
+        if (f >= nb || g->region_type[g->bface_region[f]] == OX_BC_SYMMETRY) {
+            qf = 0.0;
+            for (int j = g->face_off[f]; j < g->face_off[f + 1]; ++j) qf += qn[g->face2node[j]];
+            qf /= (g->face_off[f + 1] - g->face_off[f]);
+        } else {
+            qf = 0.5 * (q[le] + q[re]);
+        }
+        double nx = m->xfn[f] * m->area[f], ny = m->yfn[f] * m->area[f], nz = m->zfn[f] * m->area[f];
+        dx[le] += qf * nx; dy[le] += qf * ny; dz[le] += qf * nz;
+        if (f >= nb) { dx[re] -= qf * nx; dy[re] -= qf * ny; dz[re] -= qf * nz; }
+    }
+    for (int c = 0; c < nc; ++c) {
+        dx[c] /= m->vol[c]; dy[c] /= m->vol[c]; dz[c] /= m->vol[c];
+    }
+    for (int f = 0; f < nb; ++f) {
+        int le = g->left[f], re = nc + f;
+        dx[re] = dx[le]; dy[re] = dy[le]; dz[re] = dz[le];
+    }
+}
+
 double ox_residual_norm(const ox_grid *g, const double *res)
 {
     double s = 0.0;
@@ -1100,9 +1236,36 @@ void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
     ox_ns_boundary(g, m, p, q, w->gama);
     ox_gamma_temperature(g, p, q, w->gama, w->t);
     if (p->viscous) ox_viscosity(g, p, w->t, w->visl, w->vist);
-    for (int k = 0; k < 5; ++k)
-        ox_gradient(g, m, p, q + (size_t)k * nt, w->dqdx + (size_t)k * nt, w->dqdy + (size_t)k * nt, w->dqdz + (size_t)k * nt);
-    if (p->viscous) ox_gradient(g, m, p, w->t, w->dtdx, w->dtdy, w->dtdz);
+    if (p->gradient == 2) {
+        /* GG-node.  The reference forms node values in PostSolve, after the
+         * update and the boundary (Controller::PostSolve, Controller.cpp:
+         * 5063-5205), and SetBoundaryValueOfField (:1467-1491) applies the
+         * boundary without recomputing the temperature: the velocity / pressure
+         * node values are those of the current state, the temperature node
+         * values those of the previous iteration's temperature.  At
+         * initialisation (and after a state is loaded) both come from the same
+         * state (NSSolver::InitDependentVariables, NSSolver.cpp:757-790). */
+        int nn = g->n_node;
+        double *qn = malloc(sizeof(double) * 5 * (size_t)nn), *tn = malloc(sizeof(double) * (size_t)nn);
+        ox_node_values(g, m, q, 5, w->t, qn, tn);
+        const double *tnode = (w->tnode_prev && w->have_tnode_prev) ? w->tnode_prev : tn;
+        for (int k = 0; k < 5; ++k)
+            ox_gradient_ggnode(g, m, q + (size_t)k * nt, qn + (size_t)k * nn, w->dqdx + (size_t)k * nt,
+                               w->dqdy + (size_t)k * nt, w->dqdz + (size_t)k * nt);
+        if (p->viscous) ox_gradient_ggnode(g, m, w->t, tnode, w->dtdx, w->dtdy, w->dtdz);
+        if (w->qnode) memcpy(w->qnode, qn, sizeof(double) * 5 * (size_t)nn);
+        if (w->tnode_prev) {
+            memcpy(w->tnode_prev, tn, sizeof(double) * (size_t)nn);
+            w->have_tnode_prev = 1;
+        }
+        free(qn);
+        free(tn);
+    } else {
+        for (int k = 0; k < 5; ++k)
+            ox_gradient(g, m, p, q + (size_t)k * nt, w->dqdx + (size_t)k * nt, w->dqdy + (size_t)k * nt,
+                        w->dqdz + (size_t)k * nt);
+        if (p->viscous) ox_gradient(g, m, p, w->t, w->dtdx, w->dtdy, w->dtdz);
+    }
     ox_limiter(g, m, p, q, w->dqdx, w->dqdy, w->dqdz, w->limit);
     memset(w->res, 0, sizeof(double) * 5 * nt);
     ox_inviscid_flux(g, m, p, q, w->gama, w->dqdx, w->dqdy, w->dqdz, w->limit, w->res);

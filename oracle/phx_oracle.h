@@ -57,7 +57,7 @@ typedef struct {
     double prandtl, prandtl_turb;
     double tsuth_nd;        /* Sutherland constant / reference temperature */
     double wall_temperature;/* <= 0: adiabatic */
-    int gradient;           /* 0 ggcell, 1 lsq */
+    int gradient;           /* 0 ggcell, 1 lsq, 2 ggnode */
     int limiter;            /* 0 nolim, 1 vencat(ivencat=7, scalar from rho and p) */
     double venkat_coeff;
     int recon_method;       /* reconmeth: 0 own limiter, 1 min(L,R) */
@@ -102,6 +102,9 @@ typedef struct {
     double *qt, *res_t, *spec_t, *dqt;  /* [nTotal] */
     double *matl, *matr;                /* [n_face] mat_turbl / mat_turbr */
     double *dntx, *dnty, *dntz;         /* [nTotal] gradient of nu~ */
+    double *qnode;                      /* [5][n_node] GG-node node values of the last gradient, or NULL */
+    double *tnode_prev;                 /* [n_node] GG-node temperature node values for the next iteration */
+    int have_tnode_prev;                /* 0 after initialisation or a state load */
 } ox_ns_work;
 
 void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p,
@@ -112,6 +115,10 @@ void ox_ns_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, d
 void ox_gamma_temperature(const ox_grid *g, const ox_params *p, const double *q, double *gama, double *t);
 void ox_gradient(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *f,
                  double *dfdx, double *dfdy, double *dfdz);
+void ox_node_values(const ox_grid *g, const ox_metrics *m, const double *f, int nv, const double *t, double *fn,
+                    double *tn);
+void ox_gradient_ggnode(const ox_grid *g, const ox_metrics *m, const double *q, const double *qn, double *dx,
+                        double *dy, double *dz);
 void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
                 const double *dqdx, const double *dqdy, const double *dqdz, double *limit);
 void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,

@@ -367,6 +367,16 @@ int main(int argc, char **argv)
             }
         }
         fclose(f);
+        // GG-node gradients read node values that the solver forms at
+        // initialisation (NSSolver::InitDependentVariables, NSSolver.cpp:757-790,
+        // then Controller::Initialize's ModifyNodeValue) and in each PostSolve;
+        // a loaded state gets them the way an initialisation from a restart does.
+        if (GlobalDataBase::GetStrParaFromDB("gradientName") == "ggnode")
+        {
+            NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(0, 0));
+            ns->InitDependentVariables();
+            ns->ModifyNodeValue(grid);
+        }
     }
 
     // Outer loop: Simulation::SolveSimulation / SolveOneOuterStep without the

@@ -65,6 +65,7 @@ struct phx_ctx {
     double *tmp = nullptr;                // [5][nTotal] staging buffer in the reference's order
     double *hist = nullptr;
     int histCap = 0;
+    bool nodePrev = false;                // GG-node: node values of a previous state are in nrec (slot 5)
     int step = 0;
     bool haveResidual = false;
 };
@@ -125,6 +126,114 @@ struct HostGrid {
     const double *x, *y, *z;
     std::vector<int> foff, f2n, left, right, coff, c2n;
 };
+
+// GG-node schedule (NSSolverUnstruct::ComputeNodeValue, NSSolverUnstruct.cpp:
+// 4734-5080, with ModifyNodeValue :5083-5116).  Nodes are numbered in the order
+// the storage-ordered cells first touch them.  Per storage node: its
+// contributions in the reference's accumulation order (boundary nodes: the
+// faces of solid-wall regions, then far-field regions, then other
+// non-symmetry regions, each region's faces in face order, skipping nodes of a
+// higher-priority boundary type; the other nodes, symmetry nodes included:
+// the cells around them in cell order), each {storage cell, or storage
+// boundary face with the sign bit set} with its FP64 1/distance weight, and
+// the weight sum accumulated in the same order.  Per storage face: its nodes
+// in the face's node order, for the face averages of the gradient.
+struct NodeSchedule {
+    std::vector<int> off, src, foff, fidx;
+    std::vector<double> w, wsum;
+};
+
+static void node_schedule(const HostGrid &h, const phx_grid_desc *gd, const std::vector<double> *geom,
+                          const std::vector<int> &ord, const std::vector<int> &rank, const std::vector<int> &fpos,
+                          const std::vector<int> &forder, NodeSchedule &ns)
+{
+    const int nn = h.nNode, nc = h.nCell, nb = h.nBFace, nf = h.nFace;
+    enum { kNoBC = -1 };
+    std::vector<int> nodeOf(nn, -1);
+    int next = 0;
+    for (int i = 0; i < nc; ++i) {
+        const int c = ord[i];
+        for (int j = h.coff[c]; j < h.coff[c + 1]; ++j)
+            if (nodeOf[h.c2n[j]] < 0) nodeOf[h.c2n[j]] = next++;
+    }
+    for (int p = 0; p < nn; ++p)
+        if (nodeOf[p] < 0) nodeOf[p] = next++;
+    // node boundary types by priority: solid wall, far field, the other types but symmetry
+    std::vector<std::vector<int>> rfaces((size_t)gd->n_region);
+    for (int f = 0; f < nb; ++f) rfaces[gd->bface_region[f]].push_back(f);
+    std::vector<int> nbc(nn, kNoBC);
+    auto type = [&](int r) { return gd->region_type[r]; };
+    for (int r = 0; r < gd->n_region; ++r)
+        if (type(r) == PHX_BC_SOLID_SURFACE)
+            for (int f : rfaces[r])
+                for (int j = h.foff[f]; j < h.foff[f + 1]; ++j) nbc[h.f2n[j]] = PHX_BC_SOLID_SURFACE;
+    for (int r = 0; r < gd->n_region; ++r)
+        if (type(r) == PHX_BC_FARFIELD)
+            for (int f : rfaces[r])
+                for (int j = h.foff[f]; j < h.foff[f + 1]; ++j)
+                    if (nbc[h.f2n[j]] != PHX_BC_SOLID_SURFACE) nbc[h.f2n[j]] = PHX_BC_FARFIELD;
+    for (int r = 0; r < gd->n_region; ++r) {
+        const int bt = type(r);
+        if (bt == PHX_BC_SOLID_SURFACE || bt == PHX_BC_FARFIELD || bt == PHX_BC_SYMMETRY) continue;
+        for (int f : rfaces[r])
+            for (int j = h.foff[f]; j < h.foff[f + 1]; ++j) {
+                const int p = h.f2n[j];
+                if (nbc[p] != PHX_BC_SOLID_SURFACE && nbc[p] != PHX_BC_FARFIELD) nbc[p] = bt;
+            }
+    }
+    const double *xfc = geom[4].data(), *yfc = geom[5].data(), *zfc = geom[6].data();
+    const double *xcc = geom[7].data(), *ycc = geom[8].data(), *zcc = geom[9].data();
+    // every contribution in the reference's order: emit(reference node, source, weight)
+    auto visit = [&](auto &&emit) {
+        for (int step = 1; step <= 3; ++step)
+            for (int r = 0; r < gd->n_region; ++r) {
+                const int bt = type(r);
+                const bool take = step == 1 ? bt == PHX_BC_SOLID_SURFACE
+                                : step == 2 ? bt == PHX_BC_FARFIELD
+                                            : (bt != PHX_BC_SOLID_SURFACE && bt != PHX_BC_FARFIELD &&
+                                               bt != PHX_BC_SYMMETRY);
+                if (!take) continue;
+                for (int f : rfaces[r])
+                    for (int j = h.foff[f]; j < h.foff[f + 1]; ++j) {
+                        const int p = h.f2n[j];
+                        if (step == 2 && nbc[p] == PHX_BC_SOLID_SURFACE) continue;
+                        if (step == 3 && (nbc[p] == PHX_BC_SOLID_SURFACE || nbc[p] == PHX_BC_FARFIELD)) continue;
+                        const double dx = h.x[p] - xfc[f], dy = h.y[p] - yfc[f], dz = h.z[p] - zfc[f];
+                        emit(p, (int)((unsigned)fpos[f] | 0x80000000u), 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz));
+                    }
+            }
+        for (int c = 0; c < nc; ++c)
+            for (int j = h.coff[c]; j < h.coff[c + 1]; ++j) {
+                const int p = h.c2n[j];
+                if (nbc[p] != kNoBC) continue;
+                const double dx = h.x[p] - xcc[c], dy = h.y[p] - ycc[c], dz = h.z[p] - zcc[c];
+                emit(p, rank[c], 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz));
+            }
+    };
+    ns.off.assign(nn + 1, 0);
+    visit([&](int p, int, double) { ns.off[nodeOf[p] + 1]++; });
+    for (int i = 0; i < nn; ++i) ns.off[i + 1] += ns.off[i];
+    ns.src.resize(ns.off[nn]);
+    ns.w.resize(ns.off[nn]);
+    ns.wsum.assign(nn, 0.0);
+    std::vector<int> fill(ns.off.begin(), ns.off.end() - 1);
+    visit([&](int p, int src, double wt) {
+        const int i = nodeOf[p];
+        ns.src[fill[i]] = src;
+        ns.w[fill[i]++] = wt;
+        ns.wsum[i] += wt;
+    });
+    ns.foff.assign(nf + 1, 0);
+    for (int sf = 0; sf < nf; ++sf) {
+        const int f = forder[sf];
+        ns.foff[sf + 1] = ns.foff[sf] + (h.foff[f + 1] - h.foff[f]);
+    }
+    ns.fidx.resize(ns.foff[nf]);
+    for (int sf = 0; sf < nf; ++sf) {
+        const int f = forder[sf];
+        for (int j = h.foff[f], k = ns.foff[sf]; j < h.foff[f + 1]; ++j, ++k) ns.fidx[k] = nodeOf[h.f2n[j]];
+    }
+}
 
 void face_metrics(const HostGrid &h, std::vector<double> *G)
 {
@@ -482,7 +591,9 @@ int make_work(phx_ctx *ctx, Work<T> &w, const std::vector<double> &limInit)
     r |= dalloc(ctx, &w.dqrec, nt * kD);
     r |= dalloc(ctx, &w.dqfwd, nc * kD);
     r |= dalloc(ctx, &w.dflux, nc * kD);
+    if (ctx->prm.gradientName == 2) r |= dalloc(ctx, &w.nrec, (size_t)ctx->nNode * kN);
     if (r) return r;
+    if (w.nrec) PHX_CUDA(ctx, cudaMemset(w.nrec, 0, sizeof(T) * (size_t)ctx->nNode * kN));
     std::vector<T> q(nt * kQ, T(0));
     for (size_t i = 0; i < nt; ++i) q[i * kQ + 7] = (T)limInit[i];
     PHX_CUDA(ctx, cudaMemcpy(w.qrec, q.data(), sizeof(T) * q.size(), cudaMemcpyHostToDevice));
@@ -556,7 +667,10 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     if (prm->viscousType == 3 && (!gd->wall_dist || prm->sa_source < 0 || prm->sa_source > 2 ||
                                   prm->turbCFLScale <= 0.0))
         return PHX_ERR_ARG;
-    if ((prm->gradientName != 0 && prm->gradientName != 1) || prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
+    // gradientName 0 ggcell, 1 lsq, 2 ggnode; GG-node with SA is not built (the
+    // nu~ node values of TurbSolverUnstr::ComputeQTurbNodeValue are a separate routine)
+    if (prm->gradientName < 0 || prm->gradientName > 2 || (prm->gradientName == 2 && prm->viscousType == 3) ||
+        prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
 
@@ -874,6 +988,17 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     rc |= upload(ctx, &g.bkind, bkind);
     rc |= upload(ctx, &g.btype, btype);
     rc |= upload(ctx, &g.farfield_adj, ffadj);
+    g.nNode = h.nNode;
+    if (prm->gradientName == 2) {
+        NodeSchedule ns;
+        node_schedule(h, gd, ctx->geom, ord, rank, fpos, forder, ns);
+        rc |= upload(ctx, &g.node_off, ns.off);
+        rc |= upload(ctx, &g.node_src, ns.src);
+        rc |= upload(ctx, &g.node_w, ns.w);
+        rc |= upload(ctx, &g.node_wsum, ns.wsum);
+        rc |= upload(ctx, &g.fn_off, ns.foff);
+        rc |= upload(ctx, &g.fn_idx, ns.fidx);
+    }
     rc |= upload(ctx, &g.fwd_pinfo, fwd_pinfo);
     rc |= upload(ctx, &g.fwd_ent, fwd_ent);
     rc |= upload(ctx, &g.bwd_pinfo, bwd_pinfo);
@@ -1057,6 +1182,7 @@ static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n,
     launch_import_q(ctx->g, ctx->tmp, ctx->q64[ctx->cur], ctx->stream);
     if (ctx->mixed) launch_sync_qrec<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->stream);
     else launch_sync_qrec<double>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w64, ctx->stream);
+    ctx->nodePrev = false;   // GG-node: a loaded state starts its node values afresh, as a restart does
     int rc = check_launch(ctx, 2);
     if (rc) return rc;
     PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1101,8 +1227,10 @@ int phx_ns_boundary(phx_ctx *ctx)
 int phx_ns_gradient_limiter(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
-    if (ctx->mixed) launch_gradient_limiter<float>(ctx->g, ctx->nc, ctx->w32, ctx->stream);
-    else launch_gradient_limiter<double>(ctx->g, ctx->nc, ctx->w64, ctx->stream);
+    const int prev = ctx->nodePrev ? 1 : 0;
+    if (ctx->mixed) launch_gradient_limiter<float>(ctx->g, ctx->nc, ctx->w32, prev, ctx->stream);
+    else launch_gradient_limiter<double>(ctx->g, ctx->nc, ctx->w64, prev, ctx->stream);
+    ctx->nodePrev = true;
     return check_launch(ctx);
 }
 

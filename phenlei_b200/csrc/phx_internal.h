@@ -42,6 +42,8 @@ constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | least-squ
 constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
 constexpr int kFlux = 16;  // face flux record: inviscid F0..4 (times area) | inviscid and viscous
                            // spectral parts | pad | viscous F1..4 (times area; F0 is zero) | pad
+constexpr int kN = 8;      // nrec (GG-node): q node values (5), temperature node values of this
+                           // iteration's state, those the gradient uses (the previous state's), pad
 constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | viscous spectral term
 constexpr int kSweepLanes = 4;   // LU-SGS lanes (neighbour entries) per schedule slot
 constexpr int kSweepSlots = 8;   // slots per warp: schedule levels are padded to this multiple
@@ -83,6 +85,14 @@ struct DevGrid {
     // into the cell), index of the face use's factors (2 f + side), 0}.
     const int2 *fwd_pinfo, *bwd_pinfo;
     const int4 *fwd_ent, *bwd_ent;
+    // GG-node (gradientName 2): per storage node, its contributions {storage
+    // cell, or storage boundary face with the sign bit set} with 1/distance
+    // weights in the reference's order and their sum; per storage face, its
+    // storage nodes in the face's node order
+    int nNode;
+    const int *node_off, *node_src;
+    const double *node_w, *node_wsum;
+    const int *fn_off, *fn_idx;
     int nFwdLevels, nBwdLevels;
     int nFwdPos, nBwdPos;        // schedule slots incl. idle padding (-1 cells)
     double avgVol;
@@ -129,6 +139,7 @@ struct Work {
     T *dqfwd;       // [nCell][kD] forward-sweep dq (write-once per sweep)
     T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep (write-once)
     T *trec;        // [nTotal][kTr] SA variable, eddy and laminar viscosity (SA runs; else null)
+    T *nrec;        // [nNode][kN] GG-node node values (GG-node runs; else null)
 };
 
 // Spalart-Allmaras working arrays (one precision T; the FP64 master nu~ is qt64).
@@ -156,7 +167,7 @@ struct Reduce {
 template <class T>
 void launch_boundary(const DevGrid &g, const NsConst &c, double *q64, const Work<T> &w, cudaStream_t s);
 template <class T>
-void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s);
+void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, int nodePrev, cudaStream_t s);
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s);
 template <class T>

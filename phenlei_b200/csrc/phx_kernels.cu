@@ -131,9 +131,64 @@ void launch_sync_qrec(const DevGrid &g, const NsConst &c, const double *q64, con
 //  Limiter::MinMaxDiff :1202-1252 over interior faces), zeroed next to
 //  far-field boundaries (SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775).
 // ---------------------------------------------------------------------------
-template <class T, bool kTemp, bool kLsq>
+// GG-node node values (NSSolverUnstruct::ComputeNodeValue,
+// NSSolverUnstruct.cpp:4734-5080, and ModifyNodeValue :5083-5116) of the
+// current state: per node the 1/distance-weighted sum of its contributions in
+// the reference's order (a boundary face gives 0.5 (owner + ghost), a cell its
+// value) over the weight sum, 0 where the sum is not above SMALL.  The
+// reference forms node values in PostSolve after the update and the boundary
+// but without recomputing the temperature (Controller::PostSolve,
+// Controller.cpp:5063-5205; SetBoundaryValueOfField :1467-1491), so the
+// temperature node values its next gradient reads are those of the previous
+// state: slot 6 takes slot 5 of the previous call (havePrev), or this state's
+// after a state import, as at initialisation (NSSolver::InitDependentVariables,
+// NSSolver.cpp:757-790).
+template <class T>
+__global__ void __launch_bounds__(kThreads) node_value_kernel(DevGrid g, NsConst c, Work<T> w, int havePrev)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nNode) return;
+    const T coef = (T)c.coefState;
+    T acc[6] = {0, 0, 0, 0, 0, 0};
+    const int j1 = ld(g.node_off + n + 1);
+    for (int j = ld(g.node_off + n); j < j1; ++j) {
+        const int src = ld(g.node_src + j);
+        const T wt = (T)ld(g.node_w + j);
+        T v[6];
+        if (src < 0) {
+            const int fs = src & 0x7fffffff;
+            const int le = ld(&g.lr[fs].x), re = g.nCell + fs;
+            T ql[8], qg[8];
+            ld8(w.qrec + (size_t)le * kQ, ql);
+            ld8(w.qrec + (size_t)re * kQ, qg);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) v[k] = T(0.5) * (ql[k] + qg[k]);
+            v[5] = T(0.5) * (temperature(ql, coef) + temperature(qg, coef));
+        } else {
+            T qc[8];
+            ld8(w.qrec + (size_t)src * kQ, qc);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) v[k] = qc[k];
+            v[5] = temperature(qc, coef);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] += v[k] * wt;
+    }
+    const double ws = ld(g.node_wsum + n);
+    T o[8];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) o[k] = ws > kSmall ? acc[k] / (T)ws : T(0);
+    T *r = w.nrec + (size_t)n * kN;
+    o[6] = havePrev ? r[5] : o[5];
+    o[7] = T(0);
+    st8(r, o);
+}
+
+// kGrad: 0 GG-cell, 1 least squares, 2 GG-node.
+template <class T, bool kTemp, int kGrad>
 __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, NsConst c, Work<T> w)
 {
+    constexpr bool kLsq = kGrad == 1;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= g.nCell) return;
     constexpr int NV = kTemp ? 6 : 5;   // variable 5: temperature
@@ -181,11 +236,31 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
             ld4(g.frec + (size_t)f * kF, fr);
             const double a = fr[3];
             const T nx = (T)(fr[0] * a), ny = (T)(fr[1] * a), nz = (T)(fr[2] * a);
+            T qf[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) qf[k] = T(0.5) * (isLeft ? (vc[k] + vn[k]) : (vn[k] + vc[k]));
+            if (kGrad == 2 && (f >= g.nBFace || ld(g.btype + f) == PHX_BC_SYMMETRY)) {
+                // UnstructGrid::CompGradientGGNode_NEW (Geo_UnstructGrid.cpp:4202-4309):
+                // the average of the face's node values, in the face's node order
+                T sn[NV];
+#pragma unroll
+                for (int k = 0; k < NV; ++k) sn[k] = T(0);
+                const int a0 = ld(g.fn_off + f), a1 = ld(g.fn_off + f + 1);
+                for (int a = a0; a < a1; ++a) {
+                    T r[8];
+                    ld8(w.nrec + (size_t)ld(g.fn_idx + a) * kN, r);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) sn[k] += r[k];
+                    if (kTemp) sn[NV - 1] += r[6];
+                }
+                const T cnt = (T)(a1 - a0);
+#pragma unroll
+                for (int k = 0; k < NV; ++k) qf[k] = sn[k] / cnt;
+            }
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
-                const T qf = T(0.5) * (isLeft ? (vc[k] + vn[k]) : (vn[k] + vc[k]));
-                if (isLeft) { gx[k] += qf * nx; gy[k] += qf * ny; gz[k] += qf * nz; }
-                else { gx[k] -= qf * nx; gy[k] -= qf * ny; gz[k] -= qf * nz; }
+                if (isLeft) { gx[k] += qf[k] * nx; gy[k] += qf[k] * ny; gz[k] += qf[k] * nz; }
+                else { gx[k] -= qf[k] * nx; gy[k] -= qf[k] * ny; gz[k] -= qf[k] * nz; }
             }
         }
         if (f >= g.nBFace) {
@@ -204,6 +279,10 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
             gy[k] = ixy * tx + iyy * ty + iyz * tz;
             gz[k] = ixz * tx + iyz * ty + izz * tz;
         }
+    } else if (kGrad == 2) {
+        const T vol = (T)xc[3];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) { gx[k] /= vol; gy[k] /= vol; gz[k] /= vol; }
     } else {
         const T ovol = T(1) / (T)xc[3];
 #pragma unroll
@@ -248,15 +327,19 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
 }
 
 template <class T>
-void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, cudaStream_t s)
+void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, int nodePrev, cudaStream_t s)
 {
     const int blocks = (g.nCell + kThreads - 1) / kThreads;
+    if (c.gradient == 2)
+        node_value_kernel<T><<<(g.nNode + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, c, w, nodePrev);
     if (c.viscous) {
-        if (c.gradient == 1) gradient_limiter_kernel<T, true, true><<<blocks, kThreads, 0, s>>>(g, c, w);
-        else gradient_limiter_kernel<T, true, false><<<blocks, kThreads, 0, s>>>(g, c, w);
+        if (c.gradient == 1) gradient_limiter_kernel<T, true, 1><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else if (c.gradient == 2) gradient_limiter_kernel<T, true, 2><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else gradient_limiter_kernel<T, true, 0><<<blocks, kThreads, 0, s>>>(g, c, w);
     } else {
-        if (c.gradient == 1) gradient_limiter_kernel<T, false, true><<<blocks, kThreads, 0, s>>>(g, c, w);
-        else gradient_limiter_kernel<T, false, false><<<blocks, kThreads, 0, s>>>(g, c, w);
+        if (c.gradient == 1) gradient_limiter_kernel<T, false, 1><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else if (c.gradient == 2) gradient_limiter_kernel<T, false, 2><<<blocks, kThreads, 0, s>>>(g, c, w);
+        else gradient_limiter_kernel<T, false, 0><<<blocks, kThreads, 0, s>>>(g, c, w);
     }
 }
 
@@ -318,13 +401,13 @@ __device__ __forceinline__ void reconstruct(const DevGrid &g, const Work<T> &w, 
 }
 
 // Gradients of u, v, w (9 values) and of the temperature (3) of one side of
-// a face; a ghost has the owner's gradient (least squares) or none
-// (Green-Gauss), as the reference's gradient routines leave them.
+// a face; a ghost has the owner's gradient (least squares, GG-node) or none
+// (GG-cell), as the reference's gradient routines leave them.
 template <class T>
 __device__ __forceinline__ void side_gradients(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell,
                                                int owner, T *gv, T *gt)
 {
-    const int src = cell < g.nCell ? cell : (c.gradient == 1 ? owner : -1);
+    const int src = cell < g.nCell ? cell : (c.gradient != 0 ? owner : -1);
     if (src < 0) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) gv[k] = T(0);
@@ -1265,7 +1348,7 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
 // Explicit instantiations for the FP64 and mixed paths.
 #define PHX_INSTANTIATE(T)                                                                                         \
     template void launch_boundary<T>(const DevGrid &, const NsConst &, double *, const Work<T> &, cudaStream_t);   \
-    template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, cudaStream_t);      \
+    template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, int, cudaStream_t); \
     template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,           \
                                      cudaStream_t);                                                                 \
     template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t);   \

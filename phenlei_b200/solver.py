@@ -51,7 +51,7 @@ class Params(C.Structure):
 
 
 _STRING_KEYS = {
-    "gradientName": {"ggcell": 0, "lsq": 1},
+    "gradientName": {"ggcell": 0, "lsq": 1, "ggnode": 2},
     "uns_limiter_name": {"nolim": 0, "vencat": 1},
     "uns_scheme_name": {"roe": 0, "ausmpw+": 1},
     "precision": {"fp64": PHX_FP64, "mixed": PHX_MIXED},

@@ -72,6 +72,9 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
     if sa:
         dumps += [("vist", 0, nt), ("q_turb", 1, nt), ("res_turb", 1, nt), ("spec_turb", 1, nt),
                   ("gradTurbulenceX", 1, nt)]
+    ggnode = params.get("gradientName") == "ggnode"
+    if ggnode:
+        dumps += [("qnode", 5, m.n_node)]
     r = run_reference(m, params, nsteps, dumps=dumps, state=state)
     out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}),
            "nsteps": nsteps, "res_hist": r["res_hist"]}
@@ -90,6 +93,8 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
         out["walldist"] = r["walldist"]
         for k in ("q_turb", "res_turb", "spec_turb", "gradTurbulenceX"):
             out[k] = r[k].reshape(-1)[:nt]
+    if ggnode:
+        out["qnode"] = r["qnode"]
     out["limit"] = r["limit2D"][0]
     out["forces"] = r["forces"]
     path = os.path.join(OUT, name + ".npz")
@@ -129,5 +134,17 @@ if __name__ == "__main__":
     # SA bump on the mixed hex / prism mesh (3 prism layers at the walls), perturbed, 2 iterations.
     fixture("sa_bump_prism_16x8x2_step2", "channel_bump", {"nx": 16, "ny": 8, "nz": 2, "prism_layers": 3}, SA, 2,
             perturb_seed=8, turb_seed=4)
+    # GG-node gradient (the reference's default gradientName): Euler bump, perturbed, one iteration.
+    fixture("euler_bump_16x8x2_ggnode_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(EULER_BUMP, gradientName="ggnode"), 1, perturb_seed=7)
+    # GG-node, laminar bump (wall, far-field and symmetry nodes), perturbed, one iteration.
+    fixture("laminar_bump_16x8x2_ggnode_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(LAMINAR, gradientName="ggnode"), 1, perturb_seed=7)
+    # GG-node, laminar bump from the free stream, 20 iterations.
+    fixture("laminar_bump_16x8x2_ggnode_step20", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(LAMINAR, gradientName="ggnode"), 20)
+    # GG-node on jittered tetrahedra (all far field), perturbed, 3 iterations.
+    fixture("euler_tetcube_4_ggnode_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
+            dict(EULER_BUMP, refMachNumber=0.3, gradientName="ggnode"), 3, perturb_seed=11)
     # SA bump from the free stream, 30 iterations.
     fixture("sa_bump_16x8x2_step30", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 30)

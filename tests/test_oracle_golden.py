@@ -89,3 +89,32 @@ def test_oracle_detects_planted_error(golden):
     o.set_state(s)
     o.iterate(1)
     assert rel_err(o.work("res")[:, : m.n_cell], d["res"][:, : m.n_cell]) > 1e-10
+
+
+@pytest.mark.parametrize("name", ["euler_bump_16x8x2_ggnode_step1", "laminar_bump_16x8x2_ggnode_step1",
+                                  "laminar_bump_16x8x2_ggnode_step20", "euler_tetcube_4_ggnode_step3"])
+def test_oracle_matches_reference_ggnode(golden, name):
+    """GG-node gradient (the reference's default): node values with the
+    boundary-type priorities and 1/distance weights, face values from the face's
+    nodes (0.5 (L + ghost) on non-symmetry boundary faces), ghost gradients
+    copied from the owner; the node values the reference's PostSolve formed
+    after the last iteration against the oracle's node values of its final state."""
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    o = Oracle(m, d["params_dict"])
+    if "state_in" in d:
+        o.set_state(d["state_in"][:, :nc])
+    hist = o.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(o.q[:, :nc], d["q"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("res")[:, :nc], d["res"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dqdx")[:, :nc], d["gradPrimtiveVarX"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dqdy")[:, :nc], d["gradPrimtiveVarY"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("dqdz")[:, :nc], d["gradPrimtiveVarZ"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("limit"), d["limit"]) <= 1e-12
+    if "gradTemperatureX" in d:
+        assert rel_err(o.work("dtdx")[:nc], d["gradTemperatureX"][:nc]) <= 1e-12
+    qn, _ = o.node_values()
+    assert rel_err(qn, d["qnode"]) <= 1e-14
+    assert rel_err(o.forces(), d["forces"]) <= 1e-12

