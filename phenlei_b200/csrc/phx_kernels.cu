@@ -773,8 +773,9 @@ __device__ __forceinline__ void ghost_dq(int kind, T xn, T yn, T zn, const Ghost
         o[3] = dl[3] - zn * rvn;
         rvn = T(2) * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
         const T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
-        const T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
-        o[4] = pnew - s.pmg + T(0.5) * ((ru * ru + rv * rv + rw * rw) / Q[0] - s.rmu2);
+        const T rq0 = T(1) / Q[0];   // one division on the sweep's critical path, not two
+        const T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) * rq0;
+        o[4] = pnew - s.pmg + T(0.5) * ((ru * ru + rv * rv + rw * rw) * rq0 - s.rmu2);
     } else if (kind == BK_WALL) {
         o[0] = dl[0]; o[1] = -dl[1]; o[2] = -dl[2]; o[3] = -dl[3]; o[4] = dl[4];
     }
@@ -862,15 +863,19 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     // dq-independent terms, formed while the first poll is in flight:
     // the diagonal (NSSolverUnstruct.cpp:15867-15935), 1 / (dt' / vol) +
     // spectral radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep,
-    // :5717-5745), and the symmetry ghost's static terms
-    T d = T(1);
+    // :5717-5745), its reciprocal, and the symmetry ghost's static terms.
+    // dq is then (res - flux) times the reciprocal: IEEE divisions after the
+    // wait held the publishing lanes for up to 2 us (per-cell timestamps), on
+    // the critical path of every level.
+    T rd = T(1);
     if (lead && lane == 0) {
         T dt = s.dt;
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
         dt /= s.vol;
-        d = T(1) / dt;
+        T d = T(1) / dt;
         d += s.cr[6];
         if (c.viscous) d += s.cr[7];
+        rd = T(1) / d;
     }
     GhostStatic<T> gs;
     if (ghost && s.kind == BK_SYMMETRY) ghost_static<T>(s.ql, s.qn, gm, gs);
@@ -947,12 +952,12 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
             // (LUSGSInitialization, Controller.cpp:1765-1777)
             T fo[5];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) { o[k] = (s.cr[k] - T(0) - rhs0[k]) / d; fo[k] = T(0) + rhs0[k]; }
+            for (int k = 0; k < 5; ++k) { o[k] = (s.cr[k] - T(0) - rhs0[k]) * rd; fo[k] = T(0) + rhs0[k]; }
             publish5(w.dflux + (size_t)cell * kD, fo);
             publish5(w.dqfwd + (size_t)cell * kD, o);
         } else {
 #pragma unroll
-            for (int k = 0; k < 5; ++k) o[k] = (s.cr[k] - fl[k] - rhs0[k]) / d;
+            for (int k = 0; k < 5; ++k) o[k] = (s.cr[k] - fl[k] - rhs0[k]) * rd;
             publish5(w.dqrec + (size_t)cell * kD, o);
         }
     }

@@ -417,6 +417,9 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
     bool r1 = true, r2 = true;
     if (src1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
     if (src2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
+    // reciprocal of the spectral radius while the polls are in flight (an IEEE
+    // division after the wait sits on the critical path; see the NS sweep)
+    const T rspec = (live && lane == 0 && s.count >= 0) ? T(1) / s.spec : T(0);
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
@@ -446,9 +449,9 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
     if (lead && lane == 0) {
         if (kForward) {
             st_relaxed(t.tdfl + cell, unsentinel(T(0) + rhs0));
-            st_relaxed(t.tdqf + cell, unsentinel((s.res - T(0) - rhs0) / s.spec));
+            st_relaxed(t.tdqf + cell, unsentinel((s.res - T(0) - rhs0) * rspec));
         } else {
-            st_relaxed(t.tdq + cell, unsentinel((s.res - fl - rhs0) / s.spec));
+            st_relaxed(t.tdq + cell, unsentinel((s.res - fl - rhs0) * rspec));
         }
     }
     return true;
