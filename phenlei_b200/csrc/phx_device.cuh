@@ -77,6 +77,11 @@ __device__ __forceinline__ T sutherland(T t, T s) { return t * sqrt(t) * (T(1) +
 
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
+// IEEE division on both paths, for the LU-SGS sweeps: the files holding the
+// face and SA passes are compiled with approximate FP32 division.
+__device__ __forceinline__ float idiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double idiv(double a, double b) { return a / b; }
+
 // Sweep geometry of the LU-SGS dataflow sweeps: a slot of kSweepLanes lanes
 // per schedule position, kSweepSlots slots per warp.
 static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait

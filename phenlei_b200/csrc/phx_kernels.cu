@@ -750,10 +750,10 @@ template <class T>
 __device__ __forceinline__ void ghost_static(const T *ql, const T *qg, T gm, GhostStatic<T> &s)
 {
     const T r = ql[0], u = ql[1], v = ql[2], ww = ql[3], pp = ql[4];
-    const T em = (pp / r) / (gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
+    const T em = idiv(idiv(pp, r), gm - T(1)) + T(0.5) * (u * u + v * v + ww * ww);
     s.Q[0] = r; s.Q[1] = r * u; s.Q[2] = r * v; s.Q[3] = r * ww; s.Q[4] = r * em;
     const T rm = qg[0], um = qg[1], vm = qg[2], wm = qg[3], pm = qg[4];
-    s.pmg = pm / (gm - T(1));
+    s.pmg = idiv(pm, gm - T(1));
     s.rmu2 = rm * (um * um + vm * vm + wm * wm);
 }
 
@@ -773,7 +773,7 @@ __device__ __forceinline__ void ghost_dq(int kind, T xn, T yn, T zn, const Ghost
         o[3] = dl[3] - zn * rvn;
         rvn = T(2) * (xn * Q[1] + yn * Q[2] + zn * Q[3]);
         const T ru = Q[1] - xn * rvn, rv = Q[2] - yn * rvn, rw = Q[3] - zn * rvn;
-        const T rq0 = T(1) / Q[0];   // one division on the sweep's critical path, not two
+        const T rq0 = idiv(T(1), Q[0]);   // one division on the sweep's critical path, not two
         const T pnew = Q[4] - T(0.5) * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) * rq0;
         o[4] = pnew - s.pmg + T(0.5) * ((ru * ru + rv * rv + rw * rw) * rq0 - s.rmu2);
     } else if (kind == BK_WALL) {
@@ -871,11 +871,11 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     if (lead && lane == 0) {
         T dt = s.dt;
         if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
-        dt /= s.vol;
-        T d = T(1) / dt;
+        dt = idiv(dt, s.vol);
+        T d = idiv(T(1), dt);
         d += s.cr[6];
         if (c.viscous) d += s.cr[7];
-        rd = T(1) / d;
+        rd = idiv(T(1), d);
     }
     GhostStatic<T> gs;
     if (ghost && s.kind == BK_SYMMETRY) ghost_static<T>(s.ql, s.qn, gm, gs);

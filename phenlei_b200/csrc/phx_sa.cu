@@ -419,7 +419,7 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
     if (src2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
     // reciprocal of the spectral radius while the polls are in flight (an IEEE
     // division after the wait sits on the critical path; see the NS sweep)
-    const T rspec = (live && lane == 0 && s.count >= 0) ? T(1) / s.spec : T(0);
+    const T rspec = (live && lane == 0 && s.count >= 0) ? idiv(T(1), s.spec) : T(0);
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
