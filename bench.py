@@ -155,10 +155,10 @@ def measured_peaks():
 
 # DRAM bytes per cell of one launch of a sweep kernel, mixed precision:
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu --set full capture
-# of lusgs_kernel<float> on the 0.999M-cell SA bump (939.08 MB + 94.16 MB).
+# of lusgs_kernel<float> on the 0.999M-cell SA bump (940.16 MB + 95.03 MB).
 # Both sweeps read every cell's records once, so a launch's traffic at
 # another mesh size is this figure times the cells.
-MEASURED_TRAFFIC_PER_CELL = {("lusgs", "mixed"): (939.08e6 + 94.16e6) / 999424}
+MEASURED_TRAFFIC_PER_CELL = {("lusgs", "mixed"): (940.16e6 + 95.03e6) / 999424}
 
 
 def kernel_bytes(m, precision: str, viscous: int = 0, gradient: str = "ggcell") -> dict:

@@ -36,7 +36,7 @@ enum BcKind : int32_t {
 // Record strides (elements).
 constexpr int kQ = 8;      // qrec: rho u v w p | c2 hm | limiter
 constexpr int kG = 20;     // grec: (d/dx, d/dy, d/dz) of var k at 3k..3k+2 | pad | temperature gradient 16..18 | pad
-constexpr int kC = 8;      // crec: res0..4 | diag | inviscid | viscous spectral radius
+constexpr int kC = 8;      // crec: res0..4 | 1 / LU-SGS diagonal (unclamped dt) | inviscid | viscous spectral radius
 constexpr int kD = 8;      // dqrec / dflux: 5 values | pad
 constexpr int kF = 8;      // frec (FP64): nx ny nz area xfc yfc zfc | least-squares face weight
 constexpr int kX = 4;      // xrec (FP64): xcc ycc zcc vol
@@ -147,7 +147,7 @@ template <class T>
 struct TurbWork {
     double *qt64;   // [nTotal] master nu~
     T *tgrad;       // [nCell][kTg] gradient of nu~
-    T *tcrec;       // [nCell][kTc] residual and spectral radius
+    T *tcrec;       // [nCell][kTc] residual, spectral radius, its reciprocal, pad
     T *tface;       // [nFace][kTf] face terms
     T *tcoef;       // [2 nFace] LU-SGS matrix of each face use (side 0: left cell's view = mat_turbr)
     T *tdq;         // [nCell] LU-SGS dq (backward sweep; write-once per sweep)

@@ -668,9 +668,6 @@ __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsCo
                 }
             }
         }
-        T *cr = w.crec + (size_t)cell * kC;
-        T out[8] = {res[0], res[1], res[2], res[3], res[4], T(0), spec, vis};
-        st8(cr, out);
         T tot = spec;
         if (c.viscous) tot += vis;
         double cc = cfl;
@@ -681,9 +678,17 @@ __global__ void __launch_bounds__(kThreads) cell_residual_kernel(DevGrid g, NsCo
         const double sk = ld(g.skew + cell);
         if (sk < 0.1) cc *= 0.1;
         else if (sk < 10.0) cc *= (1.0 - exp(0.0 - sk));
-        const T dt = (T)cc * (T)ld(&g.xrec[(size_t)cell * kX + 3]) / tot;
+        const T vol = (T)ld(&g.xrec[(size_t)cell * kX + 3]);
+        const T dt = (T)cc * vol / tot;
         w.dtraw[cell] = dt;
         mydt = (double)dt;
+        // reciprocal of the LU-SGS diagonal for the unclamped time step, formed
+        // as the sweep forms it (the sweep recomputes it where ktmax clamps dt)
+        T dd = idiv(T(1), idiv(dt, vol));
+        dd += spec;
+        if (c.viscous) dd += vis;
+        T out[8] = {res[0], res[1], res[2], res[3], res[4], idiv(T(1), dd), spec, vis};
+        st8(w.crec + (size_t)cell * kC, out);
     }
     // block minimum, then one atomic per block, skipped when it cannot lower
     // the running minimum (positive doubles order like their bit patterns)
@@ -861,21 +866,26 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     bool r2 = !src2 || poll5(src2, fl);
     const T gm = (T)c.gama;
     // dq-independent terms, formed while the first poll is in flight:
-    // the diagonal (NSSolverUnstruct.cpp:15867-15935), 1 / (dt' / vol) +
-    // spectral radii, dt' = min(dt, ktmax min dt) (ReduceMaxTimeStep,
-    // :5717-5745), its reciprocal, and the symmetry ghost's static terms.
-    // dq is then (res - flux) times the reciprocal: IEEE divisions after the
-    // wait held the publishing lanes for up to 2 us (per-cell timestamps), on
-    // the critical path of every level.
+    // the reciprocal of the diagonal (NSSolverUnstruct.cpp:15867-15935),
+    // 1 / (dt' / vol) + spectral radii, dt' = min(dt, ktmax min dt)
+    // (ReduceMaxTimeStep, :5717-5745) -- formed by the residual pass for the
+    // raw dt, here only where the clamp applies -- and the symmetry ghost's
+    // static terms.  dq is then (res - flux) times the reciprocal: IEEE
+    // divisions after the wait held the publishing lanes for up to 2 us
+    // (per-cell timestamps), on the critical path of every level.
     T rd = T(1);
     if (lead && lane == 0) {
-        T dt = s.dt;
-        if (c.ktmax > 0) dt = tmin(dt, (T)(c.ktmax * mindt));
-        dt = idiv(dt, s.vol);
-        T d = idiv(T(1), dt);
-        d += s.cr[6];
-        if (c.viscous) d += s.cr[7];
-        rd = idiv(T(1), d);
+        const T clamp = (T)(c.ktmax * mindt);
+        if (c.ktmax > 0 && s.dt > clamp) {
+            // the clamp applies: the residual pass's reciprocal is for the raw dt
+            const T dt = idiv(clamp, s.vol);
+            T d = idiv(T(1), dt);
+            d += s.cr[6];
+            if (c.viscous) d += s.cr[7];
+            rd = idiv(T(1), d);
+        } else {
+            rd = s.cr[5];
+        }
     }
     GhostStatic<T> gs;
     if (ghost && s.kind == BK_SYMMETRY) ghost_static<T>(s.ql, s.qn, gm, gs);

@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kThreads) sa_cell_kernel(DevGrid g, NsConst c,
         else spec -= tf[4];
         spec += tf[5];
     }
-    T o[4] = {res, spec, T(0), T(0)};
+    T o[4] = {res, spec, idiv(T(1), spec), T(0)};   // the sweep multiplies by the reciprocal
     st4(t.tcrec + (size_t)cell * kTc, o);
 }
 
@@ -374,11 +374,11 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
 // ---------------------------------------------------------------------------
 // Static inputs of one slot for one lane (loaded a round ahead): neighbour
 // (-1: none or a ghost), its face matrix, and (lane 0 of the cell's first
-// slot) the cell's residual and spectral radius.
+// slot) the cell's residual and the reciprocal of its spectral radius.
 template <class T>
 struct SaSweepIn {
     int cell, count, nb;
-    T mat, res, spec;
+    T mat, res, rspec;
 };
 
 template <class T>
@@ -396,7 +396,7 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
         T cr[4];
         ld4(t.tcrec + (size_t)info.x * kTc, cr);
         s.res = cr[0];
-        s.spec = cr[1];
+        s.rspec = cr[2];
     }
 }
 
@@ -417,9 +417,9 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
     bool r1 = true, r2 = true;
     if (src1) { v1 = ld_poll(src1); r1 = !is_sentinel(v1); }
     if (src2) { fl = ld_poll(src2); r2 = !is_sentinel(fl); }
-    // reciprocal of the spectral radius while the polls are in flight (an IEEE
-    // division after the wait sits on the critical path; see the NS sweep)
-    const T rspec = (live && lane == 0 && s.count >= 0) ? idiv(T(1), s.spec) : T(0);
+    // the SA cell pass formed the reciprocal of the spectral radius (a division
+    // on the sweep's critical path costs up to microseconds; see the NS sweep)
+    const T rspec = s.rspec;
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
