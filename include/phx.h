@@ -64,6 +64,7 @@ extern "C" {
 #define PHX_VIST 12      /* eddy viscosity [nTotal] ("vist") */
 #define PHX_RES_TURB 13  /* SA residual [nTotal] */
 #define PHX_GEOM 14      /* geometry, see phx_get_geometry */
+#define PHX_GRAD_TURB 16 /* gradient of nu~ of the last SA residual [3][nTotal] (x, y, z; ghosts 0) */
 #define PHX_SA_SRC 15    /* learned SA source per unit volume of the last SA residual [nCell] (learned-source runs;
                             NaN where the cell took the exact source) */
 
@@ -99,7 +100,7 @@ typedef struct {
     double prl, prt;            /* laminar / turbulent Prandtl numbers */
     double tsuth;               /* Sutherland constant, K */
     double wallTemperature;     /* <= 0: adiabatic wall */
-    int32_t gradientName;       /* 0 "ggcell", 1 "lsq", 2 "ggnode" (inviscid and laminar) */
+    int32_t gradientName;       /* 0 "ggcell", 1 "lsq", 2 "ggnode" */
     int32_t uns_limiter_name;   /* 0 "nolim", 1 "vencat" */
     int32_t ivencat;            /* Venkatakrishnan variant (7 supported) */
     double venkatCoeff;

@@ -54,7 +54,7 @@ class _Work(C.Structure):
                 ("res_norm", C.c_double), ("n_negative", C.c_int),
                 ("qt", _dp), ("res_t", _dp), ("spec_t", _dp), ("dqt", _dp), ("matl", _dp), ("matr", _dp),
                 ("dntx", _dp), ("dnty", _dp), ("dntz", _dp), ("qnode", _dp), ("tnode_prev", _dp),
-                ("have_tnode_prev", C.c_int)]
+                ("have_tnode_prev", C.c_int), ("qtnode", _dp), ("have_qtnode", C.c_int)]
 
 
 _lib = None
@@ -163,11 +163,11 @@ class Oracle:
         co = mesh.cell_offsets().astype(np.int32)
         right = mesh.right.astype(np.int32).copy()
         right[:nb] = nc + np.arange(nb, dtype=np.int32)
-        rtype = np.array([t for t, _ in mesh.regions], dtype=np.int32)
+        rtype, breg = mesh.solver_regions()
         arrs = dict(x=np.ascontiguousarray(mesh.x, np.float64), y=np.ascontiguousarray(mesh.y, np.float64),
                     z=np.ascontiguousarray(mesh.z, np.float64), fo=fo, f2n=mesh.face2node.astype(np.int32),
                     left=mesh.left.astype(np.int32), right=right, co=co, c2n=mesh.cell2node.astype(np.int32),
-                    rtype=rtype, breg=mesh.bface_region.astype(np.int32))
+                    rtype=rtype, breg=breg)
         self.keep.append(arrs)
         g = _Grid()
         g.n_node, g.n_face, g.n_cell, g.n_bface = mesh.n_node, nf, nc, nb
@@ -210,7 +210,8 @@ class Oracle:
                             ("vist", (nt,)), ("dtdx", (nt,)), ("dtdy", (nt,)), ("dtdz", (nt,)),
                             ("qt", (nt,)), ("res_t", (nt,)), ("spec_t", (nt,)), ("dqt", (nt,)),
                             ("matl", (nf,)), ("matr", (nf,)), ("dntx", (nt,)), ("dnty", (nt,)), ("dntz", (nt,)),
-                            ("qnode", (5, mesh.n_node)), ("tnode_prev", (mesh.n_node,))]:
+                            ("qnode", (5, mesh.n_node)), ("tnode_prev", (mesh.n_node,)),
+                            ("qtnode", (mesh.n_node,))]:
             a = np.zeros(shape)
             self.w_arrays[name] = a
             setattr(w, name, _p(a))
@@ -228,6 +229,7 @@ class Oracle:
     def set_state(self, q_cells: np.ndarray, qt_cells=None):
         self.q[:, : self.mesh.n_cell] = q_cells
         self.w.have_tnode_prev = 0
+        self.w.have_qtnode = 0
         if qt_cells is not None:
             self.w_arrays["qt"][: self.mesh.n_cell] = qt_cells
 

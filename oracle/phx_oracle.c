@@ -1620,6 +1620,69 @@ static void sa_lusgs_update(const ox_grid *g, const ox_metrics *m, ox_ns_work *w
     for (int c = 0; c < nc; ++c) w->qt[c] += dq[c];
 }
 
+/* Node values of nu~ (TurbSolverUnstr::ComputeQTurbNodeValue,
+ * TurbSolverUnstr.cpp:3480-3814, then ModifyQTurbNodeValue :3816-3845): every
+ * face adds its owner's and its other side's value to each of its nodes
+ * (boundary faces region by region, reading the face-to-node list at a
+ * running position, then the interior faces); the nodes of symmetry, then
+ * far-field, then solid-wall faces are reset and take those faces' values
+ * only; each node divides by its number of values. */
+void ox_qturb_node_values(const ox_grid *g, const double *qt, double *qn)
+{
+    int nn = g->n_node, nb = g->n_bface, nc = g->n_cell, nf = g->n_face;
+    double *acc = calloc((size_t)nn, sizeof(double));
+    int *cnt = calloc((size_t)nn, sizeof(int));
+    int pos = 0;
+    for (int r = 0; r < g->n_region; ++r)
+        for (int f = 0; f < nb; ++f) {
+            if (g->bface_region[f] != r) continue;
+            int le = g->left[f], re = nc + f, n = g->face_off[f + 1] - g->face_off[f];
+            for (int j = 0; j < n; ++j) {
+                int pt = g->face2node[pos + j];
+                acc[pt] += qt[le]; cnt[pt] += 1;
+                acc[pt] += qt[re]; cnt[pt] += 1;
+            }
+            pos += n;
+        }
+    for (int f = nb; f < nf; ++f) {
+        int le = g->left[f], re = g->right[f], n = g->face_off[f + 1] - g->face_off[f];
+        for (int j = 0; j < n; ++j) {
+            int pt = g->face2node[pos + j];
+            acc[pt] += qt[le]; cnt[pt] += 1;
+            acc[pt] += qt[re]; cnt[pt] += 1;
+        }
+        pos += n;
+    }
+    const int order[3] = {OX_BC_SYMMETRY, OX_BC_FARFIELD, OX_BC_SOLID_SURFACE};
+    for (int k = 0; k < 3; ++k) {
+        pos = 0;
+        for (int r = 0; r < g->n_region; ++r)
+            for (int f = 0; f < nb; ++f) {
+                if (g->bface_region[f] != r) continue;
+                int n = g->face_off[f + 1] - g->face_off[f];
+                if (g->region_type[r] == order[k])
+                    for (int j = 0; j < n; ++j) { acc[g->face2node[pos + j]] = 0.0; cnt[g->face2node[pos + j]] = 0; }
+                pos += n;
+            }
+        pos = 0;
+        for (int r = 0; r < g->n_region; ++r)
+            for (int f = 0; f < nb; ++f) {
+                if (g->bface_region[f] != r) continue;
+                int le = g->left[f], re = nc + f, n = g->face_off[f + 1] - g->face_off[f];
+                if (g->region_type[r] == order[k])
+                    for (int j = 0; j < n; ++j) {
+                        int pt = g->face2node[pos + j];
+                        acc[pt] += qt[le]; cnt[pt] += 1;
+                        acc[pt] += qt[re]; cnt[pt] += 1;
+                    }
+                pos += n;
+            }
+    }
+    for (int i = 0; i < nn; ++i) qn[i] = cnt[i] != 0 ? acc[i] / cnt[i] : 0.0;
+    free(acc);
+    free(cnt);
+}
+
 void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
 {
     int nt = ntot(g), nc = g->n_cell;
@@ -1627,9 +1690,18 @@ void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     for (int i = 0; i < nt; ++i) w->res_t[i] = -0.0;
     /* Controller::UpdateResiduals: SetBoundaryValueOfField, UpdateIndependentField
      * (Viscosity, gradient of nu~) */
+    /* GG-node: the nu~ node values are those the previous PostSolve formed
+     * after the update and the boundary, or, first, those of the state as
+     * initialised or loaded, before any boundary (TurbSolver::
+     * InitDependentVariables, TurbSolver.cpp:46-56) */
+    if (p->gradient == 2 && w->qtnode && !w->have_qtnode) {
+        ox_qturb_node_values(g, w->qt, w->qtnode);
+        w->have_qtnode = 1;
+    }
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
     sa_viscosity(g, q, w->qt, w->visl, w->vist);
-    ox_gradient(g, m, p, w->qt, w->dntx, w->dnty, w->dntz);
+    if (p->gradient == 2) ox_gradient_ggnode(g, m, w->qt, w->qtnode, w->dntx, w->dnty, w->dntz);
+    else ox_gradient(g, m, p, w->qt, w->dntx, w->dnty, w->dntz);
     /* TurbSolver::UpdateResiduals (TurbSolver.cpp:316-346) */
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
     for (int i = 0; i < nt; ++i) w->spec_t[i] = 0.0;
@@ -1640,8 +1712,9 @@ void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     /* Controller::LUSGS: Diagonal, sweeps, UpdateFlowField */
     sa_spectrum(g, m, p, q, w);
     sa_lusgs_update(g, m, w);
-    /* PostSolve: SetBoundaryValueOfField */
+    /* PostSolve: SetBoundaryValueOfField, then the node values of nu~ */
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
+    if (p->gradient == 2 && w->qtnode) ox_qturb_node_values(g, w->qt, w->qtnode);
 }
 
 /* CorrectGradient, API/Physics/src/GradientOperation.cpp:21-31. */

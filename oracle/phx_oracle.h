@@ -105,6 +105,8 @@ typedef struct {
     double *qnode;                      /* [5][n_node] GG-node node values of the last gradient, or NULL */
     double *tnode_prev;                 /* [n_node] GG-node temperature node values for the next iteration */
     int have_tnode_prev;                /* 0 after initialisation or a state load */
+    double *qtnode;                     /* [n_node] GG-node node values of nu~ for the next SA gradient */
+    int have_qtnode;                    /* 0 after initialisation or a state load */
 } ox_ns_work;
 
 void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p,
@@ -119,6 +121,7 @@ void ox_node_values(const ox_grid *g, const ox_metrics *m, const double *f, int 
                     double *tn);
 void ox_gradient_ggnode(const ox_grid *g, const ox_metrics *m, const double *q, const double *qn, double *dx,
                         double *dy, double *dz);
+void ox_qturb_node_values(const ox_grid *g, const double *qt, double *qn);
 void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
                 const double *dqdx, const double *dqdy, const double *dqdz, double *limit);
 void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,

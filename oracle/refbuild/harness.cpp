@@ -376,6 +376,14 @@ int main(int argc, char **argv)
             NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(0, 0));
             ns->InitDependentVariables();
             ns->ModifyNodeValue(grid);
+            if (nTurb)
+            {
+                // the SA solver's node values of nu~ (TurbSolver::InitDependentVariables,
+                // TurbSolver.cpp:46-56, then ModifyQTurbNodeValue)
+                TurbSolverUnstr *turb = static_cast<TurbSolverUnstr *>(GlobalSolvers::GetSolver(0, 1));
+                turb->InitDependentVariables();
+                turb->ModifyQTurbNodeValue(grid);
+            }
         }
     }
 

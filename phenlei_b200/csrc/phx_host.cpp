@@ -66,6 +66,7 @@ struct phx_ctx {
     double *hist = nullptr;
     int histCap = 0;
     bool nodePrev = false;                // GG-node: node values of a previous state are in nrec (slot 5)
+    bool turbNodeValid = false;           // GG-node with SA: qtnode holds node values for the next SA gradient
     int step = 0;
     bool haveResidual = false;
 };
@@ -139,7 +140,7 @@ struct HostGrid {
 // the weight sum accumulated in the same order.  Per storage face: its nodes
 // in the face's node order, for the face averages of the gradient.
 struct NodeSchedule {
-    std::vector<int> off, src, foff, fidx;
+    std::vector<int> off, src, foff, fidx, nodeOf;
     std::vector<double> w, wsum;
 };
 
@@ -149,7 +150,8 @@ static void node_schedule(const HostGrid &h, const phx_grid_desc *gd, const std:
 {
     const int nn = h.nNode, nc = h.nCell, nb = h.nBFace, nf = h.nFace;
     enum { kNoBC = -1 };
-    std::vector<int> nodeOf(nn, -1);
+    std::vector<int> &nodeOf = ns.nodeOf;
+    nodeOf.assign(nn, -1);
     int next = 0;
     for (int i = 0; i < nc; ++i) {
         const int c = ord[i];
@@ -233,6 +235,68 @@ static void node_schedule(const HostGrid &h, const phx_grid_desc *gd, const std:
         const int f = forder[sf];
         for (int j = h.foff[f], k = ns.foff[sf]; j < h.foff[f + 1]; ++j, ++k) ns.fidx[k] = nodeOf[h.f2n[j]];
     }
+}
+
+// GG-node schedule of the SA variable (TurbSolverUnstr::ComputeQTurbNodeValue,
+// TurbSolverUnstr.cpp:3480-3814, and ModifyQTurbNodeValue :3816-3845): every
+// face adds its two sides' values to each of its nodes -- the boundary faces
+// region by region with the face-to-node list read at a running position, as
+// the reference reads it, then the interior faces -- and the nodes of
+// symmetry, then far-field, then solid-wall faces are reset and take those
+// faces only.  Per storage node: the pairs {storage owner, storage other
+// side} in that order (the node value is their sum over twice their count).
+struct TurbNodeSchedule {
+    std::vector<int> off;
+    std::vector<int2> pairs;
+};
+
+static void turb_node_schedule(const HostGrid &h, const phx_grid_desc *gd, const std::vector<int> &nodeOf,
+                               const std::vector<int> &rank, const std::vector<int> &fpos, TurbNodeSchedule &ts)
+{
+    const int nn = h.nNode, nc = h.nCell, nb = h.nBFace, nf = h.nFace;
+    std::vector<std::vector<int>> rfaces((size_t)gd->n_region);
+    for (int f = 0; f < nb; ++f) rfaces[gd->bface_region[f]].push_back(f);
+    // the running positions of the boundary faces' node blocks, regions in order
+    std::vector<int> bpos(nb);
+    int pos = 0;
+    for (int r = 0; r < gd->n_region; ++r)
+        for (int f : rfaces[r]) { bpos[f] = pos; pos += h.foff[f + 1] - h.foff[f]; }
+    // the last reset that reaches each node: 0 none, 1 symmetry, 2 far field, 3 solid wall
+    std::vector<uint8_t> cat(nn, 0);
+    const int kinds[3] = {PHX_BC_SYMMETRY, PHX_BC_FARFIELD, PHX_BC_SOLID_SURFACE};
+    for (int k = 0; k < 3; ++k)
+        for (int r = 0; r < gd->n_region; ++r)
+            if (gd->region_type[r] == kinds[k])
+                for (int f : rfaces[r])
+                    for (int j = 0; j < h.foff[f + 1] - h.foff[f]; ++j) cat[h.f2n[bpos[f] + j]] = (uint8_t)(k + 1);
+    auto other = [&](int f) { return f < nb ? nc + fpos[f] : rank[h.right[f]]; };
+    auto visit = [&](auto &&emit) {
+        for (int r = 0; r < gd->n_region; ++r)   // boundary faces: nodes outside the three kinds keep these
+            for (int f : rfaces[r])
+                for (int j = 0; j < h.foff[f + 1] - h.foff[f]; ++j) {
+                    const int p = h.f2n[bpos[f] + j];
+                    if (cat[p] == 0) emit(p, rank[h.left[f]], other(f));
+                }
+        for (int f = nb; f < nf; ++f)
+            for (int j = h.foff[f]; j < h.foff[f + 1]; ++j) {
+                const int p = h.f2n[j];
+                if (cat[p] == 0) emit(p, rank[h.left[f]], other(f));
+            }
+        for (int k = 0; k < 3; ++k)
+            for (int r = 0; r < gd->n_region; ++r)
+                if (gd->region_type[r] == kinds[k])
+                    for (int f : rfaces[r])
+                        for (int j = 0; j < h.foff[f + 1] - h.foff[f]; ++j) {
+                            const int p = h.f2n[bpos[f] + j];
+                            if (cat[p] == k + 1) emit(p, rank[h.left[f]], other(f));
+                        }
+    };
+    ts.off.assign(nn + 1, 0);
+    visit([&](int p, int, int) { ts.off[nodeOf[p] + 1]++; });
+    for (int i = 0; i < nn; ++i) ts.off[i + 1] += ts.off[i];
+    ts.pairs.resize(ts.off[nn]);
+    std::vector<int> fill(ts.off.begin(), ts.off.end() - 1);
+    visit([&](int p, int a, int b) { ts.pairs[fill[nodeOf[p]]++] = make_int2(a, b); });
 }
 
 void face_metrics(const HostGrid &h, std::vector<double> *G)
@@ -556,6 +620,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     r |= dalloc(ctx, &t.tdqf, nc);
     r |= dalloc(ctx, &t.tdfl, nc);
     r |= dalloc(ctx, &t.tsrc, nc);
+    if (ctx->prm.gradientName == 2) r |= dalloc(ctx, &t.qtnode, (size_t)ctx->nNode);
     r |= dalloc(ctx, &ctx->nmlp, 1);
     r |= dalloc(ctx, &ctx->mlpW, (size_t)kMlpH * kMlpK1 + 2 * (size_t)kMlpH * kMlpH);
     r |= dalloc(ctx, &ctx->mlpF, 4 * (size_t)kMlpH);
@@ -667,9 +732,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     if (prm->viscousType == 3 && (!gd->wall_dist || prm->sa_source < 0 || prm->sa_source > 2 ||
                                   prm->turbCFLScale <= 0.0))
         return PHX_ERR_ARG;
-    // gradientName 0 ggcell, 1 lsq, 2 ggnode; GG-node with SA is not built (the
-    // nu~ node values of TurbSolverUnstr::ComputeQTurbNodeValue are a separate routine)
-    if (prm->gradientName < 0 || prm->gradientName > 2 || (prm->gradientName == 2 && prm->viscousType == 3) ||
+    // gradientName 0 ggcell, 1 lsq, 2 ggnode
+    if (prm->gradientName < 0 || prm->gradientName > 2 ||
         prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
@@ -998,6 +1062,12 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         rc |= upload(ctx, &g.node_wsum, ns.wsum);
         rc |= upload(ctx, &g.fn_off, ns.foff);
         rc |= upload(ctx, &g.fn_idx, ns.fidx);
+        if (ctx->sa) {
+            TurbNodeSchedule ts;
+            turb_node_schedule(h, gd, ns.nodeOf, rank, fpos, ts);
+            rc |= upload(ctx, &g.tn_off, ts.off);
+            rc |= upload(ctx, &g.tn_pairs, ts.pairs);
+        }
     }
     rc |= upload(ctx, &g.fwd_pinfo, fwd_pinfo);
     rc |= upload(ctx, &g.fwd_ent, fwd_ent);
@@ -1089,6 +1159,11 @@ int export_work(phx_ctx *ctx, const Work<T> &w, int which, int &rows, int &len)
         rows = 1; len = nc;
         launch_export<T>(g, turb_of<T>(ctx).tsrc, 1, 0, 1, 1, nc, ctx->tmp, nc, s);
         break;
+    case PHX_GRAD_TURB:
+        if (!ctx->sa) return fail(ctx, PHX_ERR_ARG, "PHX_GRAD_TURB needs the SA model");
+        rows = 3; len = nt;
+        launch_export<T>(g, turb_of<T>(ctx).tgrad, kTg, 0, 3, 1, nc, ctx->tmp, nt, s);
+        break;
     case PHX_Q_TURB:
     case PHX_VISL:
     case PHX_VIST:
@@ -1170,6 +1245,7 @@ static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n,
                                                                                  : cudaMemcpyDeviceToDevice, ctx->stream));
         if (ctx->mixed) launch_import_turb<float>(ctx->g, ctx->tmp, ctx->t32, ctx->w32, ctx->stream);
         else launch_import_turb<double>(ctx->g, ctx->tmp, ctx->t64, ctx->w64, ctx->stream);
+        ctx->turbNodeValid = false;   // GG-node: a loaded nu~ forms its node values afresh
         int rc = check_launch(ctx);
         if (rc) return rc;
         PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1292,6 +1368,12 @@ int phx_sa_residual(phx_ctx *ctx)
     if (ctx->nc.saSource && !ctx->mlpReady)
         return fail(ctx, PHX_ERR_STATE, "sa_source selects the learned source but no model is set (phx_mlp_train / phx_mlp_set)");
     const MlpDev *mlp = ctx->nc.saSource ? &ctx->mlp : nullptr;
+    if (ctx->prm.gradientName == 2 && !ctx->turbNodeValid) {
+        // GG-node: the nu~ node values of the state as initialised or loaded, before any boundary
+        if (ctx->mixed) launch_turb_node_values<float>(ctx->g, ctx->w32, ctx->t32, ctx->stream);
+        else launch_turb_node_values<double>(ctx->g, ctx->w64, ctx->t64, ctx->stream);
+        ctx->turbNodeValid = true;
+    }
     if (ctx->mixed)
         launch_sa_residual<float>(ctx->g, ctx->nc, ctx->q64[ctx->cur], ctx->w32, ctx->t32, ctx->red, mlp, ctx->nmlp,
                                   ctx->numSMs, ctx->stream);
@@ -1321,7 +1403,14 @@ int phx_sa_update(phx_ctx *ctx)
     else launch_sa_update<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->stream);
     int rc = check_launch(ctx);
     if (rc) return rc;
-    return phx_sa_boundary(ctx);   // TURB PostSolve
+    rc = phx_sa_boundary(ctx);   // TURB PostSolve
+    if (rc || ctx->prm.gradientName != 2) return rc;
+    // GG-node: PostSolve forms the nu~ node values the next SA gradient reads
+    // (Controller::PostSolve, Controller.cpp:5063-5205)
+    if (ctx->mixed) launch_turb_node_values<float>(ctx->g, ctx->w32, ctx->t32, ctx->stream);
+    else launch_turb_node_values<double>(ctx->g, ctx->w64, ctx->t64, ctx->stream);
+    ctx->turbNodeValid = true;
+    return check_launch(ctx);
 }
 
 static int relax_one(phx_ctx *ctx, double *dhist, int i)

@@ -93,6 +93,10 @@ struct DevGrid {
     const int *node_off, *node_src;
     const double *node_w, *node_wsum;
     const int *fn_off, *fn_idx;
+    // GG-node of the SA variable: per storage node, the {owner, other side}
+    // pairs whose values it averages, in the reference's order
+    const int *tn_off;
+    const int2 *tn_pairs;
     int nFwdLevels, nBwdLevels;
     int nFwdPos, nBwdPos;        // schedule slots incl. idle padding (-1 cells)
     double avgVol;
@@ -154,6 +158,7 @@ struct TurbWork {
     T *tdqf;        // [nCell] forward-sweep dq (write-once per sweep)
     T *tdfl;        // [nCell] forward delta flux (write-once per sweep)
     T *tsrc;        // [nCell] source computed by the learned-source kernel (sa_source != 0)
+    T *qtnode;      // [nNode] GG-node node values of nu~ for the next SA gradient (GG-node runs; else null)
 };
 
 struct Reduce {
@@ -214,6 +219,8 @@ template <class T>
 void launch_mlp_capture(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, float *feat,
                         float *targ, int *cells, float *scales, long long cap, unsigned long long *count,
                         cudaStream_t s);
+template <class T>
+void launch_turb_node_values(const DevGrid &g, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s);
 template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
                     int numSMs, cudaStream_t s);

@@ -86,9 +86,36 @@ void launch_sa_boundary(const DevGrid &g, const NsConst &c, const double *q64, c
 // the gradient of nu~ (GetGradientField, :8652-8700: GG-cell or least
 // squares, as the NS gradient), fused per cell.
 // ---------------------------------------------------------------------------
-template <class T, bool kLsq>
+// GG-node node values of nu~ (TurbSolverUnstr::ComputeQTurbNodeValue,
+// TurbSolverUnstr.cpp:3480-3814, ModifyQTurbNodeValue :3816-3845): per node
+// the sum of its {owner, other side} pairs in the reference's order over twice
+// their number, 0 for a node without pairs.
+template <class T>
+__global__ void __launch_bounds__(kThreads) turb_node_kernel(DevGrid g, Work<T> w, TurbWork<T> t)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nNode) return;
+    const int j0 = ld(g.tn_off + n), j1 = ld(g.tn_off + n + 1);
+    T acc = T(0);
+    for (int j = j0; j < j1; ++j) {
+        const int2 pr = ld(g.tn_pairs + j);
+        acc += w.trec[(size_t)pr.x * kTr];
+        acc += w.trec[(size_t)pr.y * kTr];
+    }
+    t.qtnode[n] = j1 > j0 ? idiv(acc, (T)(2 * (j1 - j0))) : T(0);
+}
+
+template <class T>
+void launch_turb_node_values(const DevGrid &g, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s)
+{
+    turb_node_kernel<T><<<(g.nNode + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, w, t);
+}
+
+// kGrad: 0 GG-cell, 1 least squares, 2 GG-node.
+template <class T, int kGrad>
 __global__ void __launch_bounds__(kThreads) sa_visc_grad_kernel(DevGrid g, NsConst c, Work<T> w, TurbWork<T> t)
 {
+    constexpr bool kLsq = kGrad == 1;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= g.nCell) return;
     T tr[4];
@@ -128,7 +155,14 @@ __global__ void __launch_bounds__(kThreads) sa_visc_grad_kernel(DevGrid g, NsCon
             ld4(g.frec + (size_t)f * kF, fr);
             const double a = fr[3];
             const T nx = (T)(fr[0] * a), ny = (T)(fr[1] * a), nz = (T)(fr[2] * a);
-            const T qf = T(0.5) * (isLeft ? (nue + vn) : (vn + nue));
+            T qf = T(0.5) * (isLeft ? (nue + vn) : (vn + nue));
+            if (kGrad == 2 && (f >= g.nBFace || ld(g.btype + f) == PHX_BC_SYMMETRY)) {
+                // UnstructGrid::CompGradientGGNode_NEW (Geo_UnstructGrid.cpp:4202-4309)
+                const int a0 = ld(g.fn_off + f), a1 = ld(g.fn_off + f + 1);
+                T sn = T(0);
+                for (int k = a0; k < a1; ++k) sn += t.qtnode[ld(g.fn_idx + k)];
+                qf = sn / (T)(a1 - a0);
+            }
             if (isLeft) { gx += qf * nx; gy += qf * ny; gz += qf * nz; }
             else { gx -= qf * nx; gy -= qf * ny; gz -= qf * nz; }
         }
@@ -140,6 +174,9 @@ __global__ void __launch_bounds__(kThreads) sa_visc_grad_kernel(DevGrid g, NsCon
         gx = (T)m6[0] * tx + (T)m6[3] * ty + (T)m6[4] * tz;
         gy = (T)m6[3] * tx + (T)m6[1] * ty + (T)m6[5] * tz;
         gz = (T)m6[4] * tx + (T)m6[5] * ty + (T)m6[2] * tz;
+    } else if (kGrad == 2) {
+        const T vol = (T)xc[3];
+        gx /= vol; gy /= vol; gz /= vol;
     } else {
         const T ovol = T(1) / (T)xc[3];
         gx *= ovol; gy *= ovol; gz *= ovol;
@@ -355,8 +392,9 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
     // TurbSolver::UpdateResiduals repeats the boundary (ghost eddy viscosity of
     // the new interior values)
     launch_sa_boundary<T>(g, c, q64, w, t, s);
-    if (c.gradient == 1) sa_visc_grad_kernel<T, true><<<cb, kThreads, 0, s>>>(g, c, w, t);
-    else sa_visc_grad_kernel<T, false><<<cb, kThreads, 0, s>>>(g, c, w, t);
+    if (c.gradient == 1) sa_visc_grad_kernel<T, 1><<<cb, kThreads, 0, s>>>(g, c, w, t);
+    else if (c.gradient == 2) sa_visc_grad_kernel<T, 2><<<cb, kThreads, 0, s>>>(g, c, w, t);
+    else sa_visc_grad_kernel<T, 0><<<cb, kThreads, 0, s>>>(g, c, w, t);
     launch_sa_boundary<T>(g, c, q64, w, t, s);
     sa_face_kernel<T><<<fb, kThreads, 0, s>>>(g, c, w, t);
     if (c.saSource && mlp) launch_mlp_source<T>(g, c, w, t, *mlp, red, nmlp, numSMs, s);
@@ -595,6 +633,7 @@ void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t
                                     Reduce *, int, cudaStream_t);                                                 \
     template void launch_sa_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const TurbWork<T> &,     \
                                       cudaStream_t);                                                              \
+    template void launch_turb_node_values<T>(const DevGrid &, const Work<T> &, const TurbWork<T> &, cudaStream_t); \
     template void launch_import_turb<T>(const DevGrid &, const double *, const TurbWork<T> &, const Work<T> &,    \
                                         cudaStream_t);
 PHX_SA_INSTANTIATE(double)

@@ -52,6 +52,17 @@ class Mesh:
     bface_region: np.ndarray   # int32 [nBFace]
     regions: list              # [(bcType, name)]
 
+    def solver_regions(self):
+        """Boundary regions in the order the reference solver numbers them
+        (by name, as the std::set<string> of ReadUnstrBCName orders them,
+        Pre_HDF5File.cpp:1753-1940): their bcTypes, and each boundary face's
+        region in that numbering."""
+        order = sorted(range(len(self.regions)), key=lambda r: self.regions[r][1])
+        rank = np.empty(len(self.regions), np.int32)
+        rank[order] = np.arange(len(order), dtype=np.int32)
+        rtype = np.array([self.regions[r][0] for r in order], np.int32)
+        return rtype, rank[np.asarray(self.bface_region, np.int64)].astype(np.int32)
+
     @property
     def n_node(self) -> int:
         return int(self.x.size)

@@ -23,6 +23,7 @@ PHX_FP64, PHX_MIXED = 0, 1
 PHX_Q, PHX_RES, PHX_DT, PHX_LIMIT, PHX_GRADX, PHX_GRADY, PHX_GRADZ, PHX_DQ, PHX_INVSPEC, PHX_VISSPEC = range(10)
 PHX_Q_TURB, PHX_VISL, PHX_VIST, PHX_RES_TURB = 10, 11, 12, 13
 PHX_SA_SRC = 15
+PHX_GRAD_TURB = 16
 ERRORS = {-1: "PHX_ERR_ARG", -2: "PHX_ERR_CUDA", -3: "PHX_ERR_TIMEOUT", -4: "PHX_ERR_NUMERIC", -5: "PHX_ERR_STATE"}
 
 _dp = C.POINTER(C.c_double)
@@ -126,7 +127,7 @@ class NSSolverUnstruct:
                  fnn=arr(mesh.face_nnode, np.int32), f2n=arr(mesh.face2node, np.int32),
                  left=arr(mesh.left, np.int32), right=arr(mesh.right, np.int32),
                  cnn=arr(mesh.cell_nnode, np.int32), c2n=arr(mesh.cell2node, np.int32),
-                 rtype=arr([t for t, _ in mesh.regions], np.int32), breg=arr(mesh.bface_region, np.int32))
+                 rtype=arr(mesh.solver_regions()[0], np.int32), breg=arr(mesh.solver_regions()[1], np.int32))
         self._keep.append(a)
         g = GridDesc()
         g.n_node, g.n_face, g.n_cell, g.n_bface = mesh.n_node, mesh.n_face, nc, nb
@@ -177,7 +178,7 @@ class NSSolverUnstruct:
 
     _SHAPES = {PHX_Q: 5, PHX_RES: 5, PHX_DT: 1, PHX_LIMIT: 1, PHX_GRADX: 5, PHX_GRADY: 5, PHX_GRADZ: 5,
                PHX_DQ: 5, PHX_INVSPEC: -1, PHX_VISSPEC: -1, PHX_Q_TURB: 1, PHX_VISL: 1, PHX_VIST: 1,
-               PHX_RES_TURB: 1, PHX_SA_SRC: -1}
+               PHX_RES_TURB: 1, PHX_SA_SRC: -1, PHX_GRAD_TURB: 3}
 
     def get(self, which) -> np.ndarray:
         rows = self._SHAPES[which]

@@ -75,6 +75,8 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
     ggnode = params.get("gradientName") == "ggnode"
     if ggnode:
         dumps += [("qnode", 5, m.n_node)]
+        if sa:
+            dumps += [("qTurbNode", 1, m.n_node)]
     r = run_reference(m, params, nsteps, dumps=dumps, state=state)
     out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}),
            "nsteps": nsteps, "res_hist": r["res_hist"]}
@@ -95,6 +97,8 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
             out[k] = r[k].reshape(-1)[:nt]
     if ggnode:
         out["qnode"] = r["qnode"]
+        if sa:
+            out["qTurbNode"] = r["qTurbNode"].reshape(-1)[: m.n_node]
     out["limit"] = r["limit2D"][0]
     out["forces"] = r["forces"]
     path = os.path.join(OUT, name + ".npz")
@@ -146,5 +150,10 @@ if __name__ == "__main__":
     # GG-node on jittered tetrahedra (all far field), perturbed, 3 iterations.
     fixture("euler_tetcube_4_ggnode_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
             dict(EULER_BUMP, refMachNumber=0.3, gradientName="ggnode"), 3, perturb_seed=11)
+    # GG-node with SA: perturbed flow and nu~, one iteration; and 20 iterations from the free stream.
+    fixture("sa_bump_16x8x2_ggnode_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(SA, gradientName="ggnode"), 1, perturb_seed=7, turb_seed=5)
+    fixture("sa_bump_16x8x2_ggnode_step20", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(SA, gradientName="ggnode"), 20)
     # SA bump from the free stream, 30 iterations.
     fixture("sa_bump_16x8x2_step30", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 30)

@@ -1,8 +1,9 @@
 """GG-node gradient (the reference's default gradientName) on the CUDA path
 (through the C ABI): node values with the boundary-type priorities and
 1/distance weights, face values from the face's nodes, the temperature node
-values of the previous state, against golden vectors of the reference solver
-and against the oracle.
+values of the previous state, and with Spalart-Allmaras the node values of
+nu~ from the turbulence PostSolve, against golden vectors of the reference
+solver and against the oracle.
 
 Tolerances (norm-wise, max|a-b|/max|ref|): FP64 path 1e-12 per array after
 one to three iterations, 1e-10 over 20; the z gradients of the quasi-2-D
@@ -92,7 +93,24 @@ def test_ggnode_history_vs_oracle():
     assert rel_err(hs, ho) <= 1e-9
 
 
-def test_ggnode_with_sa_is_rejected():
-    m = M.channel_bump(16, 8, 2)
-    with pytest.raises(S.PhxError):
-        S.NSSolverUnstruct(m, wall_dist=M.wall_distance(m), **dict(cases.SA_BUMP, gradientName="ggnode"))
+@pytest.mark.parametrize("name", ["sa_bump_16x8x2_ggnode_step1", "sa_bump_16x8x2_ggnode_step20"])
+def test_fp64_sa_ggnode_matches_reference_golden(golden, name):
+    """GG-node with Spalart-Allmaras: the nu~ gradient from the node values the
+    turbulence PostSolve forms (face-based sums over a running face-to-node
+    position, symmetry / far-field / wall nodes rebuilt from those faces)."""
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    nsteps = int(d["nsteps"])
+    tol = FP64_TOL if nsteps == 1 else 1e-10
+    s = S.NSSolverUnstruct(m, wall_dist=d["walldist"], **d["params_dict"])
+    if "state_in" in d:
+        s.set_q_cells(d["state_in"][:5, :nc])
+        s.set_qt_cells(d["state_in"][5, :nc])
+    hist = s.Relaxation(nsteps)
+    assert rel_err(hist, d["res_hist"]) <= tol
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], d["q"][:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_Q_TURB)[:nc], d["q_turb"][:nc]) <= tol
+    assert rel_err(s.get(S.PHX_RES_TURB)[:nc], d["res_turb"][:nc]) <= tol
+    assert rel_err(s.get(S.PHX_GRAD_TURB)[0, :nc], d["gradTurbulenceX"][:nc]) <= tol
+    assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= tol

@@ -118,3 +118,26 @@ def test_oracle_matches_reference_ggnode(golden, name):
     qn, _ = o.node_values()
     assert rel_err(qn, d["qnode"]) <= 1e-14
     assert rel_err(o.forces(), d["forces"]) <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["sa_bump_16x8x2_ggnode_step1", "sa_bump_16x8x2_ggnode_step20"])
+def test_oracle_matches_reference_sa_ggnode(golden, name):
+    """GG-node with Spalart-Allmaras: the nu~ gradient from the node values the
+    turbulence PostSolve formed (face-based sums, symmetry / far-field / wall
+    nodes rebuilt from those faces only), checked with the node values the
+    reference formed after the last iteration."""
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    o = Oracle(m, d["params_dict"], wall_dist=d["walldist"])
+    if "state_in" in d:
+        o.set_state(d["state_in"][:5, :nc], d["state_in"][5, :nc])
+    hist = o.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(o.q[:, :nc], d["q"][:, :nc]) <= 1e-12
+    assert rel_err(o.work("qt")[:nc], d["q_turb"][:nc]) <= 1e-12
+    assert rel_err(o.work("vist"), d["vist"]) <= 1e-12
+    assert rel_err(o.work("res_t")[:nc], d["res_turb"][:nc]) <= 1e-12
+    assert rel_err(o.work("dntx")[:nc], d["gradTurbulenceX"][:nc]) <= 1e-12
+    assert rel_err(o.work("qtnode"), d["qTurbNode"]) <= 1e-14
+    assert rel_err(o.forces(), d["forces"]) <= 1e-12
