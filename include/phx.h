@@ -42,6 +42,15 @@ extern "C" {
 
 /* boundary condition codes: the reference's bcType values
  * (API/Geometry/include/Geo_SimpleBC.h:32-39) */
+/* Inviscid schemes (uns_scheme_name; GetSchemeID / GetINVScheme,
+ * API/Physics/src/Flux_Inviscid.cpp:16-134) */
+#define PHX_SCHEME_ROE 0          /* "roe" */
+#define PHX_SCHEME_AUSMPW_PLUS 1  /* "ausmpw+" */
+#define PHX_SCHEME_STEGER 2       /* "steger" */
+#define PHX_SCHEME_VANLEER 3      /* "vanleer" */
+#define PHX_SCHEME_HLLE 4         /* "hlle" */
+#define PHX_SCHEME_AUSMDV 5       /* "ausmdv" */
+
 #define PHX_BC_EXTRAPOLATION 1
 #define PHX_BC_SOLID_SURFACE 2
 #define PHX_BC_SYMMETRY 3
@@ -105,7 +114,7 @@ typedef struct {
     int32_t ivencat;            /* Venkatakrishnan variant (7 supported) */
     double venkatCoeff;
     int32_t reconmeth;          /* 0 own limiter, 1 min of both sides */
-    int32_t uns_scheme_name;    /* 0 "roe", 1 "ausmpw+" */
+    int32_t uns_scheme_name;    /* PHX_SCHEME_* */
     int32_t roeEntropyFixMethod;/* 3 (Harten) supported */
     double roeEntropyScale;
     double CFLStart, CFLEnd;
@@ -119,6 +128,7 @@ typedef struct {
     int32_t sa_source;          /* 0 exact SA source, 1 MLP, 2 MLP with exact fallback */
     double turbSkewnessAngle;   /* SA diffusion skewness switch, degrees */
     double freeStreamViscosity; /* eddy viscosity of far-field inflow ghosts (SA) */
+    double AusmpwPlusLimiter;   /* weight limiter of the AUSMPW+ scheme */
 } phx_params;
 
 /* Fills `p` with the reference's defaults for every key. */

@@ -44,7 +44,10 @@ class _Params(C.Structure):
                 ("cfl_start", C.c_double), ("cfl_end", C.c_double), ("cfl_vary_step", C.c_int),
                 ("ktmax", C.c_double), ("n_sweeps", C.c_int), ("lusgs_tol", C.c_double),
                 ("skewness_angle", C.c_double), ("nut_inf", C.c_double), ("vist_inf", C.c_double),
-                ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double)]
+                ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double), ("ausmpw_limiter", C.c_double)]
+
+# uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86)
+SCHEMES = {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5}
 
 
 class _Work(C.Structure):
@@ -132,7 +135,8 @@ def make_params(**kw) -> _Params:
     p.limiter = {"nolim": 0, "vencat": 1}[kw.get("uns_limiter_name", "vencat")]
     p.venkat_coeff = kw.get("venkatCoeff", 5.0)
     p.recon_method = kw.get("reconmeth", 1)
-    p.scheme = {"roe": 0, "ausmpw+": 1}[kw.get("uns_scheme_name", "roe")]
+    p.scheme = SCHEMES[kw.get("uns_scheme_name", "roe")]
+    p.ausmpw_limiter = kw.get("AusmpwPlusLimiter", 1.0)
     p.entropy_fix = kw.get("roeEntropyFixMethod", 3)
     e = entropy_fix_coefficient(mach, kw.get("roeEntropyScale", 1.0))
     p.entropy_acoustic = p.entropy_convective = e

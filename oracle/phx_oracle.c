@@ -564,6 +564,261 @@ static void roe_flux(const double *ql, const double *qr, double gl, double gr, d
     f[4] -= 0.5 * (e1 * dq4 + (theta * c2dc - hm * dh) * xi1 + (theta * dh - hm * dc) * xi2);
 }
 
+/* The other schemes of GetINVScheme (API/Physics/src/Flux_Inviscid.cpp:88-134)
+ * for a perfect gas on a static grid (face velocity 0), without
+ * preconditioning; each returns the flux per unit area in f[5]. */
+#define OX_SMALL 1.0e-40
+
+/* Steger_Scheme, Flux_Inviscid.cpp:12467-12694, entropy fix method 3 (none):
+ * positive eigenvalues of the left state plus negative ones of the right. */
+static void steger_side(const double *q, double g, double xsn, double ysn, double zsn, double sgn, double *f)
+{
+    double r = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
+    double v2 = u * u + v * v + w * w;
+    double h = (g / (g - 1.0)) * (p / r) + 0.5 * v2;
+    double e = h - p / (r + OX_SMALL);
+    double vn = xsn * u + ysn * v + zsn * w;
+    double c2 = g * p / r;
+    double c = sqrt(fabs(c2));
+    double l1 = vn, l2 = vn + c, l3 = vn - c;
+    l1 = 0.5 * (l1 + sgn * fabs(l1));
+    l2 = 0.5 * (l2 + sgn * fabs(l2));
+    l3 = 0.5 * (l3 + sgn * fabs(l3));
+    double c2g = c2 / g;
+    double xi1 = c2g * (l1 + l1 - l2 - l3) / (c2 + c2);
+    double xi2 = c2g * (l2 - l3) / (c + c);
+    double ex = l1 - xi1;
+    f[0] = r * ex;
+    f[1] = r * (ex * u + xi2 * xsn);
+    f[2] = r * (ex * v + xi2 * ysn);
+    f[3] = r * (ex * w + xi2 * zsn);
+    f[4] = r * (l1 * e - xi1 * h + xi2 * vn);
+}
+
+static void steger_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                        double zsn, double *f)
+{
+    double a[5], b[5];
+    steger_side(ql, gl, xsn, ysn, zsn, 1.0, a);
+    steger_side(qr, gr, xsn, ysn, zsn, -1.0, b);
+    for (int k = 0; k < 5; ++k) f[k] = a[k] + b[k];
+}
+
+/* Vanleer_Scheme, Flux_Inviscid.cpp:12697-12950 (nPrecondition = 0):
+ * Van Leer's Mach-number splitting, F+ of the left state plus F- of the right. */
+static void vanleer_side(const double *q, double g, double xsn, double ysn, double zsn, int left, double *f)
+{
+    double r = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
+    double v2 = u * u + v * v + w * w;
+    double h = (g / (g - 1.0)) * (p / r) + 0.5 * v2;
+    double vn = xsn * u + ysn * v + zsn * w;
+    double rvn = r * vn;
+    double c = sqrt(fabs(g * p / r));
+    double mach = vn / c;
+    int full = left ? mach > 1.0 : mach < -1.0;
+    int none = left ? mach < -1.0 : mach > 1.0;
+    if (full) {
+        f[0] = rvn;
+        f[1] = rvn * u + xsn * p;
+        f[2] = rvn * v + ysn * p;
+        f[3] = rvn * w + zsn * p;
+        f[4] = rvn * h;
+    } else if (none) {
+        for (int k = 0; k < 5; ++k) f[k] = 0.0;
+    } else {
+        double fm, t;
+        if (left) {
+            fm = 0.25 * r * c * (mach + 1.0) * (mach + 1.0);
+            t = (-vn + 2.0 * c) / g;
+        } else {
+            fm = -0.25 * r * c * (mach - 1.0) * (mach - 1.0);
+            t = (-vn - 2.0 * c) / g;
+        }
+        f[0] = fm;
+        f[1] = fm * (u + xsn * t);
+        f[2] = fm * (v + ysn * t);
+        f[3] = fm * (w + zsn * t);
+        f[4] = fm * h;
+    }
+}
+
+static void vanleer_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                         double zsn, double *f)
+{
+    double a[5], b[5];
+    vanleer_side(ql, gl, xsn, ysn, zsn, 1, a);
+    vanleer_side(qr, gr, xsn, ysn, zsn, 0, b);
+    for (int k = 0; k < 5; ++k) f[k] = a[k] + b[k];
+}
+
+/* Hlle_Scheme, Flux_Inviscid.cpp:13917-14077: the HLLE flux with signal
+ * speeds from the Roe average and both sides; the conserved jump from
+ * PerfectGas::Primitive2Conservative (PerfectGas.cpp:284-323). */
+static void hlle_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                      double zsn, double *f)
+{
+    double rl = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+    double rr = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+    double v2l = ul * ul + vl * vl + wl * wl;
+    double v2r = ur * ur + vr * vr + wr * wr;
+    double hl = (gl / (gl - 1.0)) * (pl / rl) + 0.5 * v2l;
+    double hr = (gr / (gr - 1.0)) * (pr / rr) + 0.5 * v2r;
+    double ratio = sqrt(rr / rl);
+    double coef = 1.0 / (1.0 + ratio);
+    double rm = sqrt(rl * rr);
+    double um = (ul + ur * ratio) * coef;
+    double vm = (vl + vr * ratio) * coef;
+    double wm = (wl + wr * ratio) * coef;
+    double pm = (pl + pr * ratio) * coef;
+    double gm = (gl + gr * ratio) * coef;
+    double vnl = xsn * ul + ysn * vl + zsn * wl;
+    double vnr = xsn * ur + ysn * vr + zsn * wr;
+    double rvnl = rl * vnl, rvnr = rr * vnr;
+    double vn = xsn * um + ysn * vm + zsn * wm;
+    double cl = sqrt(gl * pl / (rl + OX_SMALL));
+    double cr = sqrt(gr * pr / (rr + OX_SMALL));
+    double cm = sqrt(gm * pm / (rm + OX_SMALL));
+    double fl[5] = {rvnl, rvnl * ul + xsn * pl, rvnl * vl + ysn * pl, rvnl * wl + zsn * pl, rvnl * hl};
+    double fr[5] = {rvnr, rvnr * ur + xsn * pr, rvnr * vr + ysn * pr, rvnr * wr + zsn * pr, rvnr * hr};
+    double el = (pl / rl) / (gl - 1.0) + 0.5 * v2l;
+    double er = (pr / rr) / (gr - 1.0) + 0.5 * v2r;
+    double ul5[5] = {rl, rl * ul, rl * vl, rl * wl, rl * el};
+    double ur5[5] = {rr, rr * ur, rr * vr, rr * wr, rr * er};
+    double bm = omin(0.0, omin(vn - cm, vnl - cl));
+    double bp = omax(0.0, omax(vn + cm, vnr + cr));
+    double c1 = bp * bm / (bp - bm + OX_SMALL);
+    double c2 = -0.5 * (bp + bm) / (bp - bm + OX_SMALL);
+    for (int k = 0; k < 5; ++k) f[k] = 0.5 * (fl[k] + fr[k]) + c1 * (ur5[k] - ul5[k]) + c2 * (fr[k] - fl[k]);
+}
+
+/* Ausmdv_Scheme, Flux_Inviscid.cpp:13191-13461: AUSMD / AUSMV blended by the
+ * pressure jump, the Haenel / Van Leer flux at shocks, and its entropy fix. */
+static void ausmdv_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                        double zsn, double *f)
+{
+    double rl = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+    double rr = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+    double gama = 0.5 * (gl + gr);
+    double v2l = ul * ul + vl * vl + wl * wl;
+    double v2r = ur * ur + vr * vr + wr * wr;
+    double hl = (gl / (gl - 1.0)) * (pl / rl) + 0.5 * v2l;
+    double hr = (gr / (gr - 1.0)) * (pr / rr) + 0.5 * v2r;
+    double vnl = xsn * ul + ysn * vl + zsn * wl;
+    double vnr = xsn * ur + ysn * vr + zsn * wr;
+    double orl = 1.0 / (rl + OX_SMALL), orr = 1.0 / (rr + OX_SMALL);
+    double cl = sqrt(gama * pl * orl), cr = sqrt(gama * pr * orr);
+    double cm = omax(cl, cr);
+    double ocm = 1.0 / (cm + OX_SMALL);
+    double ssw = ((vnl > cl && vnr < cr) || (vnl > -cl && vnr < -cr)) ? 1.0 : 0.0;
+    double ssw_a = 1.0 - ssw;
+    /* Haenel / Van Leer with the side sound speeds */
+    double ml = vnl / cl, mr = vnr / cr;
+    double mla = fabs(ml), mra = fabs(mr);
+    double mpl, ppl, mmr, pmr;
+    if (mla >= 1.0) { mpl = 0.5 * (ml + mla); ppl = 0.5 * (1.0 + ml / (mla + OX_SMALL)); }
+    else { double t = 0.25 * ((ml + 1.0) * (ml + 1.0)); mpl = t; ppl = t * (2.0 - ml); }
+    if (mra >= 1.0) { mmr = 0.5 * (mr - mra); pmr = 0.5 * (1.0 - mr / (mra + OX_SMALL)); }
+    else { double t = 0.25 * ((mr - 1.0) * (mr - 1.0)); mmr = -t; pmr = t * (2.0 + mr); }
+    double p12 = ppl * pl + pmr * pr;
+    double rvnl_v = cl * rl * mpl, rvnr_v = cr * rr * mmr;
+    /* AUSMD / AUSMV with the common sound speed */
+    ml = vnl * ocm; mla = fabs(ml);
+    mr = vnr * ocm; mra = fabs(mr);
+    double r1 = pl * orl, r2 = pr * orr, r3 = 2.0 / (r1 + r2);
+    double al = r1 * r3, ar = r2 * r3;
+    if (mla >= 1.0) mpl = 0.5 * (ml + mla);
+    else { double t = 0.25 * ((ml + 1.0) * (ml + 1.0)); mpl = al * t + (1.0 - al) * (0.5 * (ml + mla)); }
+    if (mra >= 1.0) mmr = 0.5 * (mr - mra);
+    else { double t = 0.25 * ((mr - 1.0) * (mr - 1.0)); mmr = -ar * t + (1.0 - ar) * (0.5 * (mr - mra)); }
+    double rvnl_d = cm * rl * mpl, rvnr_d = cm * rr * mmr;
+    double rvn = rvnl_d + rvnr_d;
+    rvnl_d = 0.5 * (rvn + fabs(rvn));
+    rvnr_d = 0.5 * (rvn - fabs(rvn));
+    double rvnl = rvnl_v, rvnr = rvnr_v;
+    double s = 0.5 * omin(1.0, 10.0 * fabs(pr - pl) / omin(pl, pr));
+    double rvvn = ssw * (rvnl_v * vnl + rvnr_v * vnr);
+    rvvn += (0.5 - s) * ssw_a * (rvnl_d * vnl + rvnr_d * vnr) + (0.5 + s) * ssw_a * cm * (rl * mpl * vnl + rr * mmr * vnr);
+    int a = (vnl - cl) < 0.0 && (vnr - cr) > 0.0;
+    int b = (vnl + cl) < 0.0 && (vnr + cr) > 0.0;
+    if (a && !b) {
+        double t = ssw_a * 0.125 * ((vnr - cr) - (vnl - cl));
+        rvnl += t * rl; rvnr -= t * rr;
+    } else if (!a && b) {
+        double t = ssw_a * 0.125 * ((vnr + cr) - (vnl + cl));
+        rvnl += t * rl; rvnr -= t * rr;
+    }
+    double dul = ul - xsn * vnl, dvl = vl - ysn * vnl, dwl = wl - zsn * vnl;
+    double dur = ur - xsn * vnr, dvr = vr - ysn * vnr, dwr = wr - zsn * vnr;
+    rvvn += p12;
+    f[0] = rvnl + rvnr;
+    f[1] = rvnl * dul + rvnr * dur + rvvn * xsn;
+    f[2] = rvnl * dvl + rvnr * dvr + rvvn * ysn;
+    f[3] = rvnl * dwl + rvnr * dwr + rvvn * zsn;
+    f[4] = rvnl * hl + rvnr * hr;
+}
+
+/* FMmpn / FMppn, Flux_Inviscid.cpp:14079-14107: split Mach number and
+ * pressure polynomials (ipn = +1 for the left side, -1 for the right). */
+static double fm_mpn(double m, double ipn)
+{
+    if (fabs(m) >= 1.0) return 0.5 * (m + ipn * fabs(m));
+    return ipn * 0.25 * ((m + ipn) * (m + ipn));
+}
+
+static double fm_ppn(double m, double ipn)
+{
+    if (fabs(m) >= 1.0) return 0.5 * (m + ipn * fabs(m)) / m;
+    return ipn * 0.25 * ((m + ipn) * (m + ipn)) * (2.0 * ipn - m);
+}
+
+/* AusmpwPlus_Scheme, Flux_Inviscid.cpp:13628-13915: AUSMPW+ with the mean
+ * sound speed 0.5 (a_L + a_R) and the pressure-ratio weight
+ * 1 - min(p_L/p_R, p_R/p_L)^3 * AusmpwPlusLimiter. */
+static void ausmpwp_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                         double zsn, double lim, double *f)
+{
+    double rl = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+    double rr = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+    double v2l = ul * ul + vl * vl + wl * wl;
+    double v2r = ur * ur + vr * vr + wr * wr;
+    double hl = (gl / (gl - 1.0)) * (pl / rl) + 0.5 * v2l;
+    double hr = (gr / (gr - 1.0)) * (pr / rr) + 0.5 * v2r;
+    double al = sqrt(gl * (pl / (rl + OX_SMALL)));
+    double ar = sqrt(gr * (pr / (rr + OX_SMALL)));
+    double vnl = xsn * ul + ysn * vl + zsn * wl;
+    double vnr = xsn * ur + ysn * vr + zsn * wr;
+    double minplr = omin(pl / (pr + OX_SMALL), pr / (pl + OX_SMALL));
+    double c12 = 0.5 * (al + ar);
+    double ocm = 1.0 / c12;
+    double ml = vnl * ocm, mr = vnr * ocm;
+    double fm4l = fm_mpn(ml, 1.0), fm4r = fm_mpn(mr, -1.0);
+    double fp5l = fm_ppn(ml, 1.0), fp5r = fm_ppn(mr, -1.0);
+    double m12 = fm4l + fm4r;
+    double p12 = fp5l * pl + fp5r * pr;
+    double fw = 1.0 - minplr * minplr * minplr * lim;
+    double op12 = 1.0 / (p12 + OX_SMALL);
+    double fl = 0.0, fr = 0.0;
+    if (p12 != 0.0) {
+        if (fabs(ml) <= 1.0) fl = pl * op12 - 1.0;
+        if (fabs(mr) <= 1.0) fr = pr * op12 - 1.0;
+    }
+    double mpl, mmr;
+    if (m12 >= 0.0) {
+        double o = 1.0 + fr;
+        mpl = fm4l + fm4r * ((1.0 - fw) * o - fl);
+        mmr = fm4r * fw * o;
+    } else {
+        double o = 1.0 + fl;
+        mpl = fm4l * fw * o;
+        mmr = fm4r + fm4l * ((1.0 - fw) * o - fr);
+    }
+    f[0] = c12 * (mpl * rl + mmr * rr);
+    f[1] = c12 * (mpl * rl * ul + mmr * rr * ur) + p12 * xsn;
+    f[2] = c12 * (mpl * rl * vl + mmr * rr * vr) + p12 * ysn;
+    f[3] = c12 * (mpl * rl * wl + mmr * rr * wr) + p12 * zsn;
+    f[4] = c12 * (mpl * rl * hl + mmr * rr * hr);
+}
+
 /* PositiveCheckForDensityAndPressure: rho > 0 and p > 0. */
 static inline int positive(const double *q) { return q[0] > 0.0 && q[4] > 0.0; }
 
@@ -608,7 +863,14 @@ void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p,
             }
         }
         double fl[5];
-        roe_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->entropy_acoustic, p->entropy_convective, fl);
+        switch (p->scheme) {
+        case OX_SCHEME_AUSMPW_PLUS: ausmpwp_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->ausmpw_limiter, fl); break;
+        case OX_SCHEME_STEGER: steger_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        case OX_SCHEME_VANLEER: vanleer_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        case OX_SCHEME_HLLE: hlle_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        case OX_SCHEME_AUSMDV: ausmdv_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        default: roe_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->entropy_acoustic, p->entropy_convective, fl);
+        }
         for (int k = 0; k < 5; ++k) {
             double fa = fl[k] * m->area[f];
             res[k * nt + le] -= fa;

@@ -61,7 +61,7 @@ typedef struct {
     int limiter;            /* 0 nolim, 1 vencat(ivencat=7, scalar from rho and p) */
     double venkat_coeff;
     int recon_method;       /* reconmeth: 0 own limiter, 1 min(L,R) */
-    int scheme;             /* 0 roe, 1 ausmpw+ */
+    int scheme;             /* OX_SCHEME_*: uns_scheme_name */
     int entropy_fix;        /* roeEntropyFixMethod (3 supported) */
     double entropy_acoustic, entropy_convective;
     double cfl_start, cfl_end;
@@ -75,7 +75,12 @@ typedef struct {
     double vist_inf;        /* freeStreamViscosity (far-field inflow ghost eddy viscosity) */
     double turb_cfl_scale;  /* turbCFLScale */
     double turb_skew_angle; /* turbSkewnessAngle, degrees */
+    double ausmpw_limiter;  /* AusmpwPlusLimiter (Param_CFDSolver.cpp:116-120) */
 } ox_params;
+
+/* uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86) */
+enum { OX_SCHEME_ROE = 0, OX_SCHEME_AUSMPW_PLUS = 1, OX_SCHEME_STEGER = 2, OX_SCHEME_VANLEER = 3,
+       OX_SCHEME_HLLE = 4, OX_SCHEME_AUSMDV = 5 };
 
 /* Grid metrics: API/Geometry/src/Geo_UnstructGrid.cpp:5911-6156 (faces),
  * 6545-6819 (cells), 2206-2340 (skewness), Region.cpp:2655-2734 (avg volume),

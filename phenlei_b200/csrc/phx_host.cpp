@@ -712,6 +712,7 @@ void phx_default_params(phx_params *p)
     p->sa_source = 0;
     p->turbSkewnessAngle = 0.0;
     p->freeStreamViscosity = 1.0e-3;
+    p->AusmpwPlusLimiter = 1.0;
 }
 
 int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out)
@@ -734,7 +735,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         return PHX_ERR_ARG;
     // gradientName 0 ggcell, 1 lsq, 2 ggnode
     if (prm->gradientName < 0 || prm->gradientName > 2 ||
-        prm->uns_scheme_name != 0 || prm->roeEntropyFixMethod != 3 ||
+        prm->uns_scheme_name < PHX_SCHEME_ROE || prm->uns_scheme_name > PHX_SCHEME_AUSMDV ||
+        prm->roeEntropyFixMethod != 3 ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
 
@@ -997,6 +999,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     k.primInf[3] = std::sin(sid);
     k.primInf[4] = k.coefState;
     k.acoustic = k.convective = entropy_fix_coefficient(prm->refMachNumber, prm->roeEntropyScale);
+    k.scheme = prm->uns_scheme_name;
+    k.ausmpwLim = prm->AusmpwPlusLimiter;
     const double K = prm->venkatCoeff;
     double kt = K * K * K;
     kt *= 1.0 / std::pow(std::pow(avgVol, 1.0 / 3.0), 3.0);

@@ -346,8 +346,9 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 // ---------------------------------------------------------------------------
 // Residual, pass 1 (one thread per face): MUSCL face states (GetQlQr /
 // ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193), the wall /
-// symmetry face fix (BoundaryQlQrFix, :13725-13951), the Roe flux times the
-// face area (InviscidFluxWrap, :14466-14488), the face term of the inviscid
+// symmetry face fix (BoundaryQlQrFix, :13725-13951), the inviscid flux (Roe,
+// or with kRoe = false the scheme uns_scheme_name selects) times the face area
+// (InviscidFluxWrap, :14466-14488), the face term of the inviscid
 // spectral radius (SpectrumRadiusInviscid, :5749-5850), and the dq-independent
 // LU-SGS factors of both face uses (RoeAveragedVariables + GetRad +
 // MXDQ_STD, :15097-15116, Jacobian.cpp:27-47).
@@ -547,7 +548,7 @@ __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c,
 // Three blocks per SM on the mixed path (at most 85 registers): the face pass
 // is latency-bound on its arithmetic, and 16M cells take 5.3 ms against 6.2 ms
 // at the two blocks its natural 101 registers allow.
-template <class T, bool kVisc>
+template <class T, bool kVisc, bool kRoe>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_kernel(DevGrid g, NsConst c, Work<T> w)
 {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -581,7 +582,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     }
     const T gm = (T)c.gama;
     T fl[8];
-    roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
+    if (kRoe) roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
+    else other_flux<T>(c.scheme, ql, qr, gm, gm, xn, yn, zn, (T)c.ausmpwLim, fl);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fl[k] *= area;
     // inviscid spectral radius term from the face-mean state
@@ -708,11 +710,14 @@ template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
 {
     const int fb = (g.nFace + kThreads - 1) / kThreads, cb = (g.nCell + kThreads - 1) / kThreads;
+    const bool roe = c.scheme == PHX_SCHEME_ROE;
     if (c.viscous) {
-        face_flux_kernel<T, true><<<fb, kThreads, 0, s>>>(g, c, w);
+        if (roe) face_flux_kernel<T, true, true><<<fb, kThreads, 0, s>>>(g, c, w);
+        else face_flux_kernel<T, true, false><<<fb, kThreads, 0, s>>>(g, c, w);
         cell_residual_kernel<T, true><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
     } else {
-        face_flux_kernel<T, false><<<fb, kThreads, 0, s>>>(g, c, w);
+        if (roe) face_flux_kernel<T, false, true><<<fb, kThreads, 0, s>>>(g, c, w);
+        else face_flux_kernel<T, false, false><<<fb, kThreads, 0, s>>>(g, c, w);
         cell_residual_kernel<T, false><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
     }
 }

@@ -48,13 +48,14 @@ class Params(C.Structure):
                 ("CFLEnd", C.c_double), ("CFLVaryStep", C.c_int32), ("ktmax", C.c_double),
                 ("nLUSGSSweeps", C.c_int32), ("LUSGSTolerance", C.c_double), ("skewnessAngle", C.c_double),
                 ("muoo", C.c_double), ("turbCFLScale", C.c_double), ("sa_source", C.c_int32),
-                ("turbSkewnessAngle", C.c_double), ("freeStreamViscosity", C.c_double)]
+                ("turbSkewnessAngle", C.c_double), ("freeStreamViscosity", C.c_double),
+                ("AusmpwPlusLimiter", C.c_double)]
 
 
 _STRING_KEYS = {
     "gradientName": {"ggcell": 0, "lsq": 1, "ggnode": 2},
     "uns_limiter_name": {"nolim": 0, "vencat": 1},
-    "uns_scheme_name": {"roe": 0, "ausmpw+": 1},
+    "uns_scheme_name": {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5},
     "precision": {"fp64": PHX_FP64, "mixed": PHX_MIXED},
     "sa_source": {"exact": 0, "mlp": 1, "mlp_fallback": 2},
 }

@@ -157,3 +157,12 @@ if __name__ == "__main__":
             dict(SA, gradientName="ggnode"), 20)
     # SA bump from the free stream, 30 iterations.
     fixture("sa_bump_16x8x2_step30", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 30)
+    # The other inviscid schemes of the dispatcher (Flux_Inviscid.cpp:88-134): Euler bump, perturbed,
+    # 3 iterations; and a supersonic free stream (M = 1.6) through jittered tetrahedra, perturbed,
+    # 2 iterations, so the supersonic branches of each splitting run.
+    for scheme, tag in (("steger", "steger"), ("vanleer", "vanleer"), ("hlle", "hlle"), ("ausmdv", "ausmdv"),
+                        ("ausmpw+", "ausmpwp")):
+        fixture(f"euler_bump_16x8x2_{tag}_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+                dict(EULER_BUMP, uns_scheme_name=scheme), 3, perturb_seed=7)
+        fixture(f"euler_tetcube_4_{tag}_m16_step2", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
+                dict(EULER_BUMP, uns_scheme_name=scheme, refMachNumber=1.6), 2, perturb_seed=11, amplitude=0.1)

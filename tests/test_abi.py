@@ -36,3 +36,15 @@ def test_default_params_match_reference_defaults():
     p = solver.make_params()
     assert p.refGama == 1.4 and p.venkatCoeff == 5.0 and p.CFLVaryStep == 500
     assert p.nLUSGSSweeps == 1 and p.roeEntropyFixMethod == 3
+    assert p.uns_scheme_name == 0 and p.AusmpwPlusLimiter == 1.0
+
+
+def test_scheme_names_map_to_the_abi_ids():
+    """uns_scheme_name strings (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86)
+    map to the same ids in the solver mirror, the oracle and include/phx.h."""
+    from oracle.oracle import SCHEMES
+
+    assert solver._STRING_KEYS["uns_scheme_name"] == SCHEMES
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "phx.h")).read()
+    for name, sid in SCHEMES.items():
+        assert f'#define PHX_SCHEME_{name.upper().replace("+", "_PLUS")} {sid}' in hdr, name

@@ -9,7 +9,13 @@ from tests.conftest import rel_err
 GEOM = ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol")
 
 
-@pytest.mark.parametrize("name", ["euler_bump_16x8x2_step1", "euler_bump_16x8x2_step40", "euler_tetcube_4_step3"])
+SCHEME_TAGS = ("steger", "vanleer", "hlle", "ausmdv", "ausmpwp")
+SCHEME_CASES = [f"euler_bump_16x8x2_{t}_step3" for t in SCHEME_TAGS] + \
+    [f"euler_tetcube_4_{t}_m16_step2" for t in SCHEME_TAGS]
+
+
+@pytest.mark.parametrize("name", ["euler_bump_16x8x2_step1", "euler_bump_16x8x2_step40", "euler_tetcube_4_step3"]
+                         + SCHEME_CASES)
 def test_oracle_matches_reference(golden, name):
     d = golden(name)
     m = d["mesh_obj"]

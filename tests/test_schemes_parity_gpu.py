@@ -1,0 +1,84 @@
+"""The inviscid schemes besides Roe that the reference's dispatcher offers
+(GetINVScheme, API/Physics/src/Flux_Inviscid.cpp:88-134: Steger-Warming,
+Van Leer, HLLE, AUSMDV, AUSMPW+) on the CUDA path, through the C ABI: FP64
+against golden vectors of the reference solver (a subsonic bump and a
+supersonic stream through tetrahedra), and both precisions against the oracle
+on larger seeded cases, inviscid, laminar and with Spalart-Allmaras.
+
+Tolerances (norm-wise, max|a-b|/max|ref|): FP64 1e-12; mixed 1e-5.
+"""
+import pytest
+
+from phenlei_b200 import cases
+from phenlei_b200 import mesh as M
+from phenlei_b200 import solver as S
+from tests.conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-5
+SCHEMES = ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+")
+TAG = {"steger": "steger", "vanleer": "vanleer", "hlle": "hlle", "ausmdv": "ausmdv", "ausmpw+": "ausmpwp"}
+
+
+@pytest.mark.parametrize("name", [f"euler_bump_16x8x2_{TAG[s]}_step3" for s in SCHEMES]
+                         + [f"euler_tetcube_4_{TAG[s]}_m16_step2" for s in SCHEMES])
+def test_fp64_scheme_matches_reference_golden(golden, name):
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    s = S.NSSolverUnstruct(m, **d["params_dict"])
+    s.set_q_cells(d["state_in"][:, :nc])
+    hist = s.Relaxation(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], d["q"][:, :nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], d["res"][:, :nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_DT)[:nc], d["dt"][:nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_INVSPEC), d["invSpectralRadius"]) <= FP64_TOL
+    assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= FP64_TOL
+
+
+def _vs_oracle(m, params, precision, seed, nsteps=1, sa=False):
+    from oracle.oracle import Oracle
+
+    wd = M.wall_distance(m) if sa else None
+    o = Oracle(m, params, wall_dist=wd)
+    q0 = cases.perturbed_state(m, params, seed=seed)
+    o.set_state(q0)
+    o.iterate(nsteps)
+    s = S.NSSolverUnstruct(m, precision=precision, wall_dist=wd, **params)
+    s.set_q_cells(q0)
+    s.Relaxation(nsteps)
+    return o, s
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_scheme_vs_oracle_euler_bump_64x32x4(scheme, precision, tol):
+    m = M.channel_bump(64, 32, 4)
+    o, s = _vs_oracle(m, dict(cases.EULER_BUMP, uns_scheme_name=scheme), precision, seed=1)
+    nc = m.n_cell
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], o.work("res")[:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_DQ)[:, :nc], o.work("dq")[:, :nc]) <= tol * (10 if precision == "mixed" else 1)
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("scheme", ["hlle", "ausmpw+"])
+def test_scheme_vs_oracle_laminar(scheme, precision, tol):
+    """The viscous face-pass instantiation with a non-Roe scheme."""
+    m = M.channel_bump(32, 16, 2)
+    o, s = _vs_oracle(m, dict(cases.LAMINAR, uns_scheme_name=scheme), precision, seed=3, nsteps=2)
+    nc = m.n_cell
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], o.work("res")[:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= tol
+
+
+def test_scheme_vs_oracle_sa_fp64():
+    m = M.channel_bump(32, 16, 2)
+    params = dict(cases.SA_BUMP, uns_scheme_name="steger")
+    o, s = _vs_oracle(m, params, "fp64", seed=4, nsteps=2, sa=True)
+    nc = m.n_cell
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_Q_TURB)[:nc], o.work("qt")[:nc]) <= FP64_TOL
