@@ -129,6 +129,8 @@ typedef struct {
     double turbSkewnessAngle;   /* SA diffusion skewness switch, degrees */
     double freeStreamViscosity; /* eddy viscosity of far-field inflow ghosts (SA) */
     double AusmpwPlusLimiter;   /* weight limiter of the AUSMPW+ scheme */
+    int32_t flowInitStep;       /* outer steps 1..flowInitStep run first order with Van Leer's flux */
+    int32_t flowInitMethod;     /* 0 or 2 (1: boundary-layer start, 3: GMRES start, not supported) */
 } phx_params;
 
 /* Fills `p` with the reference's defaults for every key. */

@@ -44,7 +44,8 @@ class _Params(C.Structure):
                 ("cfl_start", C.c_double), ("cfl_end", C.c_double), ("cfl_vary_step", C.c_int),
                 ("ktmax", C.c_double), ("n_sweeps", C.c_int), ("lusgs_tol", C.c_double),
                 ("skewness_angle", C.c_double), ("nut_inf", C.c_double), ("vist_inf", C.c_double),
-                ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double), ("ausmpw_limiter", C.c_double)]
+                ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double), ("ausmpw_limiter", C.c_double),
+                ("flow_init_step", C.c_int), ("first_order", C.c_int)]
 
 # uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86)
 SCHEMES = {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5}
@@ -137,6 +138,9 @@ def make_params(**kw) -> _Params:
     p.recon_method = kw.get("reconmeth", 1)
     p.scheme = SCHEMES[kw.get("uns_scheme_name", "roe")]
     p.ausmpw_limiter = kw.get("AusmpwPlusLimiter", 1.0)
+    p.flow_init_step = kw.get("flowInitStep", 100)   # cfd_para.hypara:1290
+    if kw.get("flowInitMethod", 0) not in (0, 2):
+        raise ValueError("flowInitMethod 1 (boundary-layer start) and 3 (GMRES) are not on the path")
     p.entropy_fix = kw.get("roeEntropyFixMethod", 3)
     e = entropy_fix_coefficient(mach, kw.get("roeEntropyScale", 1.0))
     p.entropy_acoustic = p.entropy_convective = e

@@ -481,6 +481,10 @@ void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     int nt = ntot(g);
     for (int c = 0; c < nt; ++c) limit[c] = 1.0;
     if (p->limiter == 0) return;
+    if (p->first_order) {   /* NSSolverUnstruct::ComputeLimiter :18215-18224: zero, no limiter */
+        for (int c = 0; c < nt; ++c) limit[c] = 0.0;
+        return;
+    }
     vencat7(g, m, p, q, dqdx, dqdy, dqdz, limit);
     vencat7(g, m, p, q + 4 * nt, dqdx + 4 * nt, dqdy + 4 * nt, dqdz + 4 * nt, limit);
     for (int f = 0; f < g->n_bface; ++f) {
@@ -836,7 +840,7 @@ void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p,
         int le = g->left[f], re = f < nb ? nc + f : g->right[f];
         double ql[5], qr[5], tr[5];
         for (int k = 0; k < 5; ++k) { ql[k] = q[k * nt + le]; qr[k] = q[k * nt + re]; }
-        if (p->limiter != 0 || 1) {
+        if (!p->first_order) {   /* ReConstructFaceValue returns at once in first order (:14014-14021) */
             double lim_l = limit[le], lim_r = limit[re];
             if (p->recon_method == 1) lim_l = lim_r = omin(limit[le], limit[re]);
             double dx = m->xfc[f] - m->xcc[le], dy = m->yfc[f] - m->ycc[le], dz = m->zfc[f] - m->zcc[le];
@@ -1491,9 +1495,18 @@ double ox_residual_norm(const ox_grid *g, const double *res)
  * LoadResiduals, UpdateResiduals (boundary, gamma/T, viscosity, gradient,
  * limiter, inviscid and viscous flux), SpectrumRadius, TimeStep, LUSGS,
  * UpdateFlowField. */
-void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, double *q, ox_ns_work *w)
+void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p0, int step, double *q, ox_ns_work *w)
 {
     int nt = ntot(g);
+    /* Flow initialisation (Simulation::PreSolve, Main/src/Simulation.cpp:1190-1237):
+     * isInIniting holds for outer steps 1..flowInitStep.  Then the inviscid flux
+     * is Van Leer's (NSSolverUnstruct::ComputeInviscidFlux :14229-14235), the face
+     * states are the cell values (ReConstructFaceValue :14014-14021) and the
+     * limiter is zero (ComputeLimiter :18203-18224). */
+    ox_params pinit = *p0;
+    pinit.first_order = p0->flow_init_step > 0 && step <= p0->flow_init_step;
+    if (pinit.first_order) pinit.scheme = OX_SCHEME_VANLEER;
+    const ox_params *p = &pinit;
     ox_gamma_temperature(g, p, q, w->gama, w->t);  /* gama of the ghosts is needed by the far field */
     ox_ns_boundary(g, m, p, q, w->gama);
     ox_gamma_temperature(g, p, q, w->gama, w->t);

@@ -76,6 +76,8 @@ typedef struct {
     double turb_cfl_scale;  /* turbCFLScale */
     double turb_skew_angle; /* turbSkewnessAngle, degrees */
     double ausmpw_limiter;  /* AusmpwPlusLimiter (Param_CFDSolver.cpp:116-120) */
+    int flow_init_step;     /* flowInitStep: outer steps 1..flow_init_step run first order with Van Leer */
+    int first_order;        /* set by ox_ns_iteration on its copy while isInIniting holds */
 } ox_params;
 
 /* uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86) */

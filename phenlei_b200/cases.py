@@ -21,7 +21,7 @@ from . import mesh as M
 EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "vencat", "ivencat": 7,
               "venkatCoeff": 5.0, "gradientName": "ggcell", "reconmeth": 1, "roeEntropyFixMethod": 3,
               "tscheme": 4, "nLUSGSSweeps": 1, "CFLStart": 0.01, "CFLEnd": 10.0, "CFLVaryStep": 500,
-              "refMachNumber": 0.5, "attackd": 0.0, "refGama": 1.4}
+              "refMachNumber": 0.5, "attackd": 0.0, "refGama": 1.4, "flowInitStep": 0}
 
 # Laminar NS (config 2 keys): Sutherland viscosity, Re 1e4 per unit length,
 # adiabatic no-slip walls.

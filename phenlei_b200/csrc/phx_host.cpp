@@ -713,6 +713,8 @@ void phx_default_params(phx_params *p)
     p->turbSkewnessAngle = 0.0;
     p->freeStreamViscosity = 1.0e-3;
     p->AusmpwPlusLimiter = 1.0;
+    p->flowInitStep = 100;   // cfd_para.hypara:1290
+    p->flowInitMethod = 0;
 }
 
 int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out)
@@ -736,7 +738,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     // gradientName 0 ggcell, 1 lsq, 2 ggnode
     if (prm->gradientName < 0 || prm->gradientName > 2 ||
         prm->uns_scheme_name < PHX_SCHEME_ROE || prm->uns_scheme_name > PHX_SCHEME_AUSMDV ||
-        prm->roeEntropyFixMethod != 3 ||
+        prm->roeEntropyFixMethod != 3 || prm->flowInitStep < 0 ||
+        (prm->flowInitMethod != 0 && prm->flowInitMethod != 2) ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
 
@@ -944,7 +947,12 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         else if (t == PHX_BC_SYMMETRY) bkind[fs] = BK_SYMMETRY;
         else if (t == PHX_BC_FARFIELD) bkind[fs] = BK_FARFIELD;
         else { delete ctx; return PHX_ERR_ARG; }
-        if (limiter_zeroed(t)) { ffadj[rank[h.left[f]]] = 1; limInit[nc + fs] = 0.0; }
+        // SetLimitBoundary zeroes the far-field ghosts' limiter only when a limiter
+        // runs; with nolim every limit2D entry is 1 (ComputeLimiter :18213-18220)
+        if (limiter_zeroed(t)) {
+            ffadj[rank[h.left[f]]] = 1;
+            if (prm->uns_limiter_name == 1) limInit[nc + fs] = 0.0;
+        }
     }
 
     std::vector<double> iwt, m6;
@@ -1150,7 +1158,10 @@ int export_work(phx_ctx *ctx, const Work<T> &w, int which, int &rows, int &len)
     PHX_CUDA(ctx, cudaMemsetAsync(ctx->tmp, 0, sizeof(double) * 5 * (size_t)nt, s));
     switch (which) {
     case PHX_RES: rows = 5; len = nt; launch_export<T>(g, w.crec, kC, 0, 5, 1, nc, ctx->tmp, nt, s); break;
-    case PHX_LIMIT: rows = 1; len = nt; launch_export<T>(g, w.qrec, kQ, 7, 1, 1, nt, ctx->tmp, nt, s); break;
+    case PHX_LIMIT:   // first order with a limiter: zero on the ghosts too (ComputeLimiter :18215)
+        rows = 1; len = nt;
+        launch_export<T>(g, w.qrec, kQ, 7, 1, 1, ctx->nc.firstOrder && ctx->nc.limiter ? nc : nt, ctx->tmp, nt, s);
+        break;
     case PHX_GRADX: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 0, 5, 3, nc, ctx->tmp, nt, s); break;
     case PHX_GRADY: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 1, 5, 3, nc, ctx->tmp, nt, s); break;
     case PHX_GRADZ: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 2, 5, 3, nc, ctx->tmp, nt, s); break;
@@ -1304,9 +1315,22 @@ int phx_ns_boundary(phx_ctx *ctx)
     return check_launch(ctx);
 }
 
+// Flow initialisation (Simulation::PreSolve, Main/src/Simulation.cpp:1190-1237):
+// isInIniting holds for outer steps 1..flowInitStep.  Then the limiter is zero
+// (NSSolverUnstruct::ComputeLimiter, :18203-18224), the face states are the
+// cell values (ReConstructFaceValue, :14014-14021) and the inviscid flux is Van
+// Leer's (ComputeInviscidFlux, :14229-14235).
+static void init_phase(phx_ctx *ctx)
+{
+    const bool init = ctx->prm.flowInitStep > 0 && ctx->step <= ctx->prm.flowInitStep;
+    ctx->nc.firstOrder = init ? 1 : 0;
+    ctx->nc.scheme = init ? PHX_SCHEME_VANLEER : ctx->prm.uns_scheme_name;
+}
+
 int phx_ns_gradient_limiter(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
+    init_phase(ctx);
     const int prev = ctx->nodePrev ? 1 : 0;
     if (ctx->mixed) launch_gradient_limiter<float>(ctx->g, ctx->nc, ctx->w32, prev, ctx->stream);
     else launch_gradient_limiter<double>(ctx->g, ctx->nc, ctx->w64, prev, ctx->stream);
@@ -1317,6 +1341,7 @@ int phx_ns_gradient_limiter(phx_ctx *ctx)
 int phx_ns_residual(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
+    init_phase(ctx);
     launch_reset_reduce(ctx->red, ctx->stream);
     const double cfl = cfl_at(ctx->nc, ctx->step);
     if (ctx->mixed) launch_residual<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, cfl, ctx->stream);

@@ -108,7 +108,8 @@ struct NsConst {
     double gama, coefState, pTotal;
     double primInf[5];
     double acoustic, convective;   // Roe entropy-fix coefficients
-    int scheme;                    // PHX_SCHEME_* (uns_scheme_name)
+    int scheme;                    // PHX_SCHEME_* in use (Van Leer during the flow initialisation)
+    int firstOrder;                // flow initialisation: no reconstruction, zero limiter
     double ausmpwLim;              // AusmpwPlusLimiter
     double venkatK3;               // K^3 / (avgVol^(1/3))^3, as VencatLimiter7 forms it
     int viscous;                   // viscousType

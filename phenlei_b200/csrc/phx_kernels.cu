@@ -302,7 +302,9 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
         if (w.trec) w.trec[(size_t)cell * kTr + 2] = sutherland(vc[NV - 1], (T)c.tsuth);
     }
     T lim = T(1);
-    if (c.limiter == 1) {
+    if (c.limiter == 1 && c.firstOrder) {
+        lim = T(0);
+    } else if (c.limiter == 1) {
         const T vp = (T)ld(g.volpow + cell);
         T er = (T)c.venkatK3 * qc[0]; er = er * qc[0]; er = er * vp;
         T ep = (T)c.venkatK3 * qc[4]; ep = ep * qc[4]; ep = ep * vp;
@@ -563,8 +565,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     T limL = qL[7], limR = qR[7];
     if (c.reconMethod == 1) { const T m = tmin(limL, limR); limL = limR = m; }
     T ql[5], qr[5];
-    reconstruct<T>(g, w, le, fr + 4, limL, qL, ql);
-    reconstruct<T>(g, w, re, fr + 4, limR, qR, qr);
+    if (!kRoe && c.firstOrder) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) { ql[k] = qL[k]; qr[k] = qR[k]; }
+    } else {
+        reconstruct<T>(g, w, le, fr + 4, limL, qL, ql);
+        reconstruct<T>(g, w, re, fr + 4, limR, qR, qr);
+    }
     const T xn = (T)fr[0], yn = (T)fr[1], zn = (T)fr[2], area = (T)fr[3];
     if (f < g.nBFace) {
         const int bt = g.btype[f];

@@ -49,7 +49,7 @@ class Params(C.Structure):
                 ("nLUSGSSweeps", C.c_int32), ("LUSGSTolerance", C.c_double), ("skewnessAngle", C.c_double),
                 ("muoo", C.c_double), ("turbCFLScale", C.c_double), ("sa_source", C.c_int32),
                 ("turbSkewnessAngle", C.c_double), ("freeStreamViscosity", C.c_double),
-                ("AusmpwPlusLimiter", C.c_double)]
+                ("AusmpwPlusLimiter", C.c_double), ("flowInitStep", C.c_int32), ("flowInitMethod", C.c_int32)]
 
 
 _STRING_KEYS = {

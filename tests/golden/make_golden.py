@@ -166,3 +166,14 @@ if __name__ == "__main__":
                 dict(EULER_BUMP, uns_scheme_name=scheme), 3, perturb_seed=7)
         fixture(f"euler_tetcube_4_{tag}_m16_step2", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
                 dict(EULER_BUMP, uns_scheme_name=scheme, refMachNumber=1.6), 2, perturb_seed=11, amplitude=0.1)
+    # Flow initialisation (flowInitStep > 0: first order, zero limiter, Van Leer flux): inside the phase
+    # only; across its end (laminar); with no limiter (nolim keeps limit2D = 1 but still skips the
+    # reconstruction); and with SA.
+    fixture("euler_bump_16x8x2_init5_step2", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(EULER_BUMP, flowInitStep=5), 2, perturb_seed=7)
+    fixture("laminar_bump_16x8x2_init3_step5", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(LAMINAR, flowInitStep=3), 5, perturb_seed=7)
+    fixture("euler_bump_16x8x2_nolim_init2_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(EULER_BUMP, uns_limiter_name="nolim", flowInitStep=2), 3, perturb_seed=7)
+    fixture("sa_bump_16x8x2_init2_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(SA, flowInitStep=2), 3, perturb_seed=7, turb_seed=5)

@@ -37,6 +37,7 @@ def test_default_params_match_reference_defaults():
     assert p.refGama == 1.4 and p.venkatCoeff == 5.0 and p.CFLVaryStep == 500
     assert p.nLUSGSSweeps == 1 and p.roeEntropyFixMethod == 3
     assert p.uns_scheme_name == 0 and p.AusmpwPlusLimiter == 1.0
+    assert p.flowInitStep == 100 and p.flowInitMethod == 0
 
 
 def test_scheme_names_map_to_the_abi_ids():

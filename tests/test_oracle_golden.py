@@ -14,8 +14,11 @@ SCHEME_CASES = [f"euler_bump_16x8x2_{t}_step3" for t in SCHEME_TAGS] + \
     [f"euler_tetcube_4_{t}_m16_step2" for t in SCHEME_TAGS]
 
 
+INIT_CASES = ["euler_bump_16x8x2_init5_step2", "euler_bump_16x8x2_nolim_init2_step3"]
+
+
 @pytest.mark.parametrize("name", ["euler_bump_16x8x2_step1", "euler_bump_16x8x2_step40", "euler_tetcube_4_step3"]
-                         + SCHEME_CASES)
+                         + SCHEME_CASES + INIT_CASES)
 def test_oracle_matches_reference(golden, name):
     d = golden(name)
     m = d["mesh_obj"]
@@ -38,7 +41,7 @@ def test_oracle_matches_reference(golden, name):
 
 
 @pytest.mark.parametrize("name", ["laminar_bump_16x8x2_lsq_step1", "laminar_bump_16x8x2_step20",
-                                  "laminar_tetcube_4_lsq_step3"])
+                                  "laminar_tetcube_4_lsq_step3", "laminar_bump_16x8x2_init3_step5"])
 def test_oracle_matches_reference_laminar(golden, name):
     """Laminar NS: Sutherland viscosity, temperature gradient, viscous flux and
     spectral radius, no-slip adiabatic walls, GG-cell and LSQ gradients."""
@@ -62,7 +65,7 @@ def test_oracle_matches_reference_laminar(golden, name):
 
 
 @pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_16x8x2_step30",
-                                  "sa_bump_prism_16x8x2_step2"])
+                                  "sa_bump_prism_16x8x2_step2", "sa_bump_16x8x2_init2_step3"])
 def test_oracle_matches_reference_sa(golden, name):
     """Spalart-Allmaras (NSMB formation) coupled to the NS step: boundary
     values, eddy viscosity, source (negative-nu~ branch included), upwind

@@ -3,7 +3,9 @@
 Van Leer, HLLE, AUSMDV, AUSMPW+) on the CUDA path, through the C ABI: FP64
 against golden vectors of the reference solver (a subsonic bump and a
 supersonic stream through tetrahedra), and both precisions against the oracle
-on larger seeded cases, inviscid, laminar and with Spalart-Allmaras.
+on larger seeded cases, inviscid, laminar and with Spalart-Allmaras.  Also
+the flow initialisation phase (flowInitStep: first order, zero limiter, Van
+Leer's flux; Simulation::PreSolve, Main/src/Simulation.cpp:1190-1237).
 
 Tolerances (norm-wise, max|a-b|/max|ref|): FP64 1e-12; mixed 1e-5.
 """
@@ -82,3 +84,36 @@ def test_scheme_vs_oracle_sa_fp64():
     nc = m.n_cell
     assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= FP64_TOL
     assert rel_err(s.get(S.PHX_Q_TURB)[:nc], o.work("qt")[:nc]) <= FP64_TOL
+
+
+@pytest.mark.parametrize("name", ["euler_bump_16x8x2_init5_step2", "euler_bump_16x8x2_nolim_init2_step3",
+                                  "laminar_bump_16x8x2_init3_step5", "sa_bump_16x8x2_init2_step3"])
+def test_fp64_flow_initialisation_matches_reference_golden(golden, name):
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    sa = "walldist" in d
+    s = S.NSSolverUnstruct(m, wall_dist=d["walldist"] if sa else None, **d["params_dict"])
+    s.set_q_cells(d["state_in"][:5, :nc])
+    if sa:
+        s.set_qt_cells(d["state_in"][5, :nc])
+    hist = s.Relaxation(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], d["q"][:, :nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], d["res"][:, :nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_DT)[:nc], d["dt"][:nc]) <= FP64_TOL
+    assert rel_err(s.get(S.PHX_LIMIT), d["limit"]) <= FP64_TOL
+    assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= FP64_TOL
+    if sa:
+        assert rel_err(s.get(S.PHX_Q_TURB)[:nc], d["q_turb"][:nc]) <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_flow_initialisation_then_roe_vs_oracle(precision, tol):
+    """Two first-order Van Leer steps, then second-order Roe: the face pass
+    switches instantiation at the end of the phase."""
+    m = M.channel_bump(64, 32, 4)
+    o, s = _vs_oracle(m, dict(cases.EULER_BUMP, flowInitStep=2), precision, seed=1, nsteps=4)
+    nc = m.n_cell
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], o.work("res")[:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= tol
