@@ -51,6 +51,12 @@ extern "C" {
 #define PHX_SCHEME_HLLE 4         /* "hlle" */
 #define PHX_SCHEME_AUSMDV 5       /* "ausmdv" */
 
+/* Limiters (uns_limiter_name; GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300) */
+#define PHX_LIMITER_NOLIM 0       /* "nolim" */
+#define PHX_LIMITER_VENCAT 1      /* "vencat" (ivencat 7) */
+#define PHX_LIMITER_FIRST 2       /* "1st": first order */
+#define PHX_LIMITER_BARTH 3       /* "barth" */
+
 #define PHX_BC_EXTRAPOLATION 1
 #define PHX_BC_SOLID_SURFACE 2
 #define PHX_BC_SYMMETRY 3
@@ -110,7 +116,7 @@ typedef struct {
     double tsuth;               /* Sutherland constant, K */
     double wallTemperature;     /* <= 0: adiabatic wall */
     int32_t gradientName;       /* 0 "ggcell", 1 "lsq", 2 "ggnode" */
-    int32_t uns_limiter_name;   /* 0 "nolim", 1 "vencat" */
+    int32_t uns_limiter_name;   /* PHX_LIMITER_* (scalar limiter from rho and p) */
     int32_t ivencat;            /* Venkatakrishnan variant (7 supported) */
     double venkatCoeff;
     int32_t reconmeth;          /* 0 own limiter, 1 min of both sides */

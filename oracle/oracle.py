@@ -47,6 +47,8 @@ class _Params(C.Structure):
                 ("turb_cfl_scale", C.c_double), ("turb_skew_angle", C.c_double), ("ausmpw_limiter", C.c_double),
                 ("flow_init_step", C.c_int), ("first_order", C.c_int)]
 
+# uns_limiter_name (GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300)
+LIMITERS = {"nolim": 0, "vencat": 1, "1st": 2, "barth": 3}
 # uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86)
 SCHEMES = {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5}
 
@@ -133,7 +135,7 @@ def make_params(**kw) -> _Params:
     p.tsuth_nd = kw.get("tsuth_nd", 110.4 / kw.get("refDimensionalTemperature", 288.15))
     p.wall_temperature = kw.get("wallTemperature", -1.0)
     p.gradient = {"ggcell": 0, "lsq": 1, "ggnode": 2}[kw.get("gradientName", "ggcell")]
-    p.limiter = {"nolim": 0, "vencat": 1}[kw.get("uns_limiter_name", "vencat")]
+    p.limiter = LIMITERS[kw.get("uns_limiter_name", "vencat")]
     p.venkat_coeff = kw.get("venkatCoeff", 5.0)
     p.recon_method = kw.get("reconmeth", 1)
     p.scheme = SCHEMES[kw.get("uns_scheme_name", "roe")]

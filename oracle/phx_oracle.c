@@ -475,18 +475,57 @@ static void vencat7(const ox_grid *g, const ox_metrics *m, const ox_params *p, c
  * limitVector=0, Limiter.cpp:91-135), then SetLimitBoundary
  * (Geo_UnstructGrid.cpp:10744-10775): zero on both sides of far-field /
  * inflow faces.  `limit` holds nTotal values. */
+/* Limiter::BarthLimiter, API/Physics/src/Limiter.cpp:157-262: for each cell
+ * and each of its faces (boundary faces from the owner only), the face
+ * extrapolation dq = grad . (x_f - x_c) is limited to the neighbour min/max
+ * differences; a face whose centre lies behind the cell's outward normal
+ * zeroes the limiter. */
+static void barth_face(int c, double xn, double yn, double zn, double sgn, const ox_metrics *m, int f,
+                       const double *dqdx, const double *dqdy, const double *dqdz, const double *dmin,
+                       const double *dmax, double *limit)
+{
+    double dx = m->xfc[f] - m->xcc[c], dy = m->yfc[f] - m->ycc[c], dz = m->zfc[f] - m->zcc[c];
+    double dq = dqdx[c] * dx + dqdy[c] * dy + dqdz[c] * dz;
+    double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    double dot = sgn * (xn * dx + yn * dy + zn * dz) / (ds + OX_SMALL);
+    if (dot < 0.0) limit[c] = 0.0;
+    else if (dq > dmax[c]) limit[c] = omin(limit[c], dmax[c] / (dq + OX_SMALL));
+    else if (dq < dmin[c]) limit[c] = omin(limit[c], dmin[c] / (dq + OX_SMALL));
+}
+
+static void barth(const ox_grid *g, const ox_metrics *m, const double *q, const double *dqdx, const double *dqdy,
+                  const double *dqdz, double *limit)
+{
+    int nc = g->n_cell, nb = g->n_bface;
+    double *dmin = malloc(sizeof(double) * (size_t)nc), *dmax = malloc(sizeof(double) * (size_t)nc);
+    minmaxdiff(g, q, dmin, dmax);
+    for (int f = 0; f < g->n_face; ++f) {
+        barth_face(g->left[f], m->xfn[f], m->yfn[f], m->zfn[f], 1.0, m, f, dqdx, dqdy, dqdz, dmin, dmax, limit);
+        if (f >= nb)
+            barth_face(g->right[f], m->xfn[f], m->yfn[f], m->zfn[f], -1.0, m, f, dqdx, dqdy, dqdz, dmin, dmax,
+                       limit);
+    }
+    free(dmin);
+    free(dmax);
+}
+
 void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
                 const double *dqdx, const double *dqdy, const double *dqdz, double *limit)
 {
     int nt = ntot(g);
     for (int c = 0; c < nt; ++c) limit[c] = 1.0;
-    if (p->limiter == 0) return;
+    if (p->limiter == OX_LIMITER_NOLIM) return;
     if (p->first_order) {   /* NSSolverUnstruct::ComputeLimiter :18215-18224: zero, no limiter */
         for (int c = 0; c < nt; ++c) limit[c] = 0.0;
         return;
     }
-    vencat7(g, m, p, q, dqdx, dqdy, dqdz, limit);
-    vencat7(g, m, p, q + 4 * nt, dqdx + 4 * nt, dqdy + 4 * nt, dqdz + 4 * nt, limit);
+    if (p->limiter == OX_LIMITER_BARTH) {
+        barth(g, m, q, dqdx, dqdy, dqdz, limit);
+        barth(g, m, q + 4 * nt, dqdx + 4 * nt, dqdy + 4 * nt, dqdz + 4 * nt, limit);
+    } else {
+        vencat7(g, m, p, q, dqdx, dqdy, dqdz, limit);
+        vencat7(g, m, p, q + 4 * nt, dqdx + 4 * nt, dqdy + 4 * nt, dqdz + 4 * nt, limit);
+    }
     for (int f = 0; f < g->n_bface; ++f) {
         int t = g->region_type[g->bface_region[f]];
         if (t != OX_BC_SYMMETRY && !is_wall(t) && t != OX_BC_OUTFLOW) {
@@ -1504,8 +1543,10 @@ void ox_ns_iteration(const ox_grid *g, const ox_metrics *m, const ox_params *p0,
      * states are the cell values (ReConstructFaceValue :14014-14021) and the
      * limiter is zero (ComputeLimiter :18203-18224). */
     ox_params pinit = *p0;
-    pinit.first_order = p0->flow_init_step > 0 && step <= p0->flow_init_step;
-    if (pinit.first_order) pinit.scheme = OX_SCHEME_VANLEER;
+    const int init = p0->flow_init_step > 0 && step <= p0->flow_init_step;
+    /* the "1st" limiter is first order at every step, with the configured scheme */
+    pinit.first_order = init || p0->limiter == OX_LIMITER_FIRST;
+    if (init) pinit.scheme = OX_SCHEME_VANLEER;
     const ox_params *p = &pinit;
     ox_gamma_temperature(g, p, q, w->gama, w->t);  /* gama of the ghosts is needed by the far field */
     ox_ns_boundary(g, m, p, q, w->gama);

@@ -58,7 +58,7 @@ typedef struct {
     double tsuth_nd;        /* Sutherland constant / reference temperature */
     double wall_temperature;/* <= 0: adiabatic */
     int gradient;           /* 0 ggcell, 1 lsq, 2 ggnode */
-    int limiter;            /* 0 nolim, 1 vencat(ivencat=7, scalar from rho and p) */
+    int limiter;            /* OX_LIMITER_*: uns_limiter_name (scalar limiter from rho and p) */
     double venkat_coeff;
     int recon_method;       /* reconmeth: 0 own limiter, 1 min(L,R) */
     int scheme;             /* OX_SCHEME_*: uns_scheme_name */
@@ -79,6 +79,9 @@ typedef struct {
     int flow_init_step;     /* flowInitStep: outer steps 1..flow_init_step run first order with Van Leer */
     int first_order;        /* set by ox_ns_iteration on its copy while isInIniting holds */
 } ox_params;
+
+/* uns_limiter_name (GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300; vencat with ivencat 7) */
+enum { OX_LIMITER_NOLIM = 0, OX_LIMITER_VENCAT = 1, OX_LIMITER_FIRST = 2, OX_LIMITER_BARTH = 3 };
 
 /* uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86) */
 enum { OX_SCHEME_ROE = 0, OX_SCHEME_AUSMPW_PLUS = 1, OX_SCHEME_STEGER = 2, OX_SCHEME_VANLEER = 3,

@@ -739,6 +739,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     if (prm->gradientName < 0 || prm->gradientName > 2 ||
         prm->uns_scheme_name < PHX_SCHEME_ROE || prm->uns_scheme_name > PHX_SCHEME_AUSMDV ||
         prm->roeEntropyFixMethod != 3 || prm->flowInitStep < 0 ||
+        prm->uns_limiter_name < PHX_LIMITER_NOLIM || prm->uns_limiter_name > PHX_LIMITER_BARTH ||
         (prm->flowInitMethod != 0 && prm->flowInitMethod != 2) ||
         prm->nLUSGSSweeps != 1 || (prm->uns_limiter_name == 1 && prm->ivencat != 7))
         return PHX_ERR_ARG;
@@ -951,7 +952,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         // runs; with nolim every limit2D entry is 1 (ComputeLimiter :18213-18220)
         if (limiter_zeroed(t)) {
             ffadj[rank[h.left[f]]] = 1;
-            if (prm->uns_limiter_name == 1) limInit[nc + fs] = 0.0;
+            if (prm->uns_limiter_name == PHX_LIMITER_VENCAT || prm->uns_limiter_name == PHX_LIMITER_BARTH)
+                limInit[nc + fs] = 0.0;
         }
     }
 
@@ -1160,7 +1162,8 @@ int export_work(phx_ctx *ctx, const Work<T> &w, int which, int &rows, int &len)
     case PHX_RES: rows = 5; len = nt; launch_export<T>(g, w.crec, kC, 0, 5, 1, nc, ctx->tmp, nt, s); break;
     case PHX_LIMIT:   // first order with a limiter: zero on the ghosts too (ComputeLimiter :18215)
         rows = 1; len = nt;
-        launch_export<T>(g, w.qrec, kQ, 7, 1, 1, ctx->nc.firstOrder && ctx->nc.limiter ? nc : nt, ctx->tmp, nt, s);
+        launch_export<T>(g, w.qrec, kQ, 7, 1, 1, ctx->nc.firstOrder && ctx->nc.limiter != PHX_LIMITER_NOLIM ? nc : nt,
+                         ctx->tmp, nt, s);
         break;
     case PHX_GRADX: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 0, 5, 3, nc, ctx->tmp, nt, s); break;
     case PHX_GRADY: rows = 5; len = nt; launch_export<T>(g, w.grec, kG, 1, 5, 3, nc, ctx->tmp, nt, s); break;
@@ -1323,7 +1326,8 @@ int phx_ns_boundary(phx_ctx *ctx)
 static void init_phase(phx_ctx *ctx)
 {
     const bool init = ctx->prm.flowInitStep > 0 && ctx->step <= ctx->prm.flowInitStep;
-    ctx->nc.firstOrder = init ? 1 : 0;
+    // the "1st" limiter is first order at every step, with the configured scheme
+    ctx->nc.firstOrder = init || ctx->prm.uns_limiter_name == PHX_LIMITER_FIRST ? 1 : 0;
     ctx->nc.scheme = init ? PHX_SCHEME_VANLEER : ctx->prm.uns_scheme_name;
 }
 

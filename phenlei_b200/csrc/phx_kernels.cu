@@ -302,9 +302,36 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
         if (w.trec) w.trec[(size_t)cell * kTr + 2] = sutherland(vc[NV - 1], (T)c.tsuth);
     }
     T lim = T(1);
-    if (c.limiter == 1 && c.firstOrder) {
+    if (c.limiter != PHX_LIMITER_NOLIM && c.firstOrder) {
         lim = T(0);
-    } else if (c.limiter == 1) {
+    } else if (c.limiter == PHX_LIMITER_BARTH) {
+        // Limiter::BarthLimiter (Limiter.cpp:157-262) from rho and p: the face
+        // extrapolation clipped to the neighbour min/max difference; a face whose
+        // centre lies behind the cell's outward normal zeroes the limiter.  Each
+        // candidate is >= 0, so visiting rho and p per face gives the reference's
+        // two passes' minimum.
+        const T dminr = rmin - qc[0], dmaxr = rmax - qc[0];
+        const T dminp = pmin - qc[4], dmaxp = pmax - qc[4];
+        const T small = (T)kSmall;
+        for (int j = j0; j < j1; ++j) {
+            const int f = ld(g.c2f + j);
+            double fn[4], fc[4];
+            ld4(g.frec + (size_t)f * kF, fn);
+            ld4(g.frec + (size_t)f * kF + 4, fc);
+            const T dx = (T)(fc[0] - xc[0]), dy = (T)(fc[1] - xc[1]), dz = (T)(fc[2] - xc[2]);
+            const T ds = sqrt(dx * dx + dy * dy + dz * dz);
+            const T nd = (T)fn[0] * dx + (T)fn[1] * dy + (T)fn[2] * dz;
+            const T dot = (ld(g.lr + f).x == cell ? nd : -nd) / (ds + small);
+            if (dot < T(0)) { lim = T(0); continue; }
+            T d = gx[0] * dx + gy[0] * dy + gz[0] * dz;
+            if (d > dmaxr) lim = tmin(lim, dmaxr / (d + small));
+            else if (d < dminr) lim = tmin(lim, dminr / (d + small));
+            d = gx[4] * dx + gy[4] * dy + gz[4] * dz;
+            if (d > dmaxp) lim = tmin(lim, dmaxp / (d + small));
+            else if (d < dminp) lim = tmin(lim, dminp / (d + small));
+        }
+        if (g.farfield_adj[cell]) lim = T(0);
+    } else if (c.limiter == PHX_LIMITER_VENCAT) {
         const T vp = (T)ld(g.volpow + cell);
         T er = (T)c.venkatK3 * qc[0]; er = er * qc[0]; er = er * vp;
         T ep = (T)c.venkatK3 * qc[4]; ep = ep * qc[4]; ep = ep * vp;

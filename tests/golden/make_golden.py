@@ -177,3 +177,13 @@ if __name__ == "__main__":
             dict(EULER_BUMP, uns_limiter_name="nolim", flowInitStep=2), 3, perturb_seed=7)
     fixture("sa_bump_16x8x2_init2_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
             dict(SA, flowInitStep=2), 3, perturb_seed=7, turb_seed=5)
+    # The other unstructured limiters (GetLimiterID, Limiter.cpp:1279-1300): Barth-Jespersen from rho and p
+    # (bump, laminar LSQ bump, jittered tetrahedra), and "1st" (first order at every step, Roe flux).
+    fixture("euler_bump_16x8x2_barth_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(EULER_BUMP, uns_limiter_name="barth"), 3, perturb_seed=7)
+    fixture("laminar_bump_16x8x2_barth_lsq_step2", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(LAMINAR, uns_limiter_name="barth", gradientName="lsq"), 2, perturb_seed=7)
+    fixture("euler_tetcube_4_barth_step2", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
+            dict(EULER_BUMP, uns_limiter_name="barth", refMachNumber=0.3), 2, perturb_seed=11)
+    fixture("euler_bump_16x8x2_1st_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+            dict(EULER_BUMP, uns_limiter_name="1st"), 3, perturb_seed=7)

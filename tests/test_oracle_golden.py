@@ -15,10 +15,11 @@ SCHEME_CASES = [f"euler_bump_16x8x2_{t}_step3" for t in SCHEME_TAGS] + \
 
 
 INIT_CASES = ["euler_bump_16x8x2_init5_step2", "euler_bump_16x8x2_nolim_init2_step3"]
+LIMITER_CASES = ["euler_bump_16x8x2_barth_step3", "euler_tetcube_4_barth_step2", "euler_bump_16x8x2_1st_step3"]
 
 
 @pytest.mark.parametrize("name", ["euler_bump_16x8x2_step1", "euler_bump_16x8x2_step40", "euler_tetcube_4_step3"]
-                         + SCHEME_CASES + INIT_CASES)
+                         + SCHEME_CASES + INIT_CASES + LIMITER_CASES)
 def test_oracle_matches_reference(golden, name):
     d = golden(name)
     m = d["mesh_obj"]
@@ -41,7 +42,8 @@ def test_oracle_matches_reference(golden, name):
 
 
 @pytest.mark.parametrize("name", ["laminar_bump_16x8x2_lsq_step1", "laminar_bump_16x8x2_step20",
-                                  "laminar_tetcube_4_lsq_step3", "laminar_bump_16x8x2_init3_step5"])
+                                  "laminar_tetcube_4_lsq_step3", "laminar_bump_16x8x2_init3_step5",
+                                  "laminar_bump_16x8x2_barth_lsq_step2"])
 def test_oracle_matches_reference_laminar(golden, name):
     """Laminar NS: Sutherland viscosity, temperature gradient, viscous flux and
     spectral radius, no-slip adiabatic walls, GG-cell and LSQ gradients."""
