@@ -1,0 +1,138 @@
+"""Domain decomposition host logic (phenlei_b200.partition): cell partitions,
+interface faces (boundary faces of type INTERFACE whose ghost is the
+neighbouring part's cell, Geo_UnstructGrid.cpp:10806-10990), halo maps, and
+the halo exchange over torch.distributed with world_size-2 gloo ranks.  CPU
+only."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from phenlei_b200 import mesh as M
+from phenlei_b200 import partition as P
+from tests.conftest import rel_err
+
+MESHES = {"bump": lambda: M.channel_bump(16, 8, 2), "tets": lambda: M.tet_cube(4, jitter=0.15, seed=3),
+          "prism": lambda: M.channel_bump(16, 8, 2, prism_layers=3)}
+
+
+def _field(nc_global):
+    """A distinct value per global cell and variable: [5][nc]."""
+    return np.arange(5)[:, None] * 1000.0 + np.arange(nc_global)[None, :] + 0.5
+
+
+@pytest.mark.parametrize("kind", sorted(MESHES))
+@pytest.mark.parametrize("nparts", [2, 3, 5])
+def test_parts_cover_the_mesh_once(kind, nparts):
+    m = MESHES[kind]()
+    parts = P.split(m, P.slab_owner(m, nparts))
+    assert len(parts) == nparts
+    cells = np.concatenate([p.cells for p in parts])
+    assert np.array_equal(np.sort(cells), np.arange(m.n_cell))
+    count = np.zeros(m.n_face, int)
+    for p in parts:
+        np.add.at(count, p.faces, 1)
+        # boundary faces first, the interface faces contiguous after the original ones
+        assert p.mesh.n_bface == p.iface_first + p.n_iface
+        assert np.all(p.mesh.right[: p.mesh.n_bface] == -1) and np.all(p.mesh.right[p.mesh.n_bface:] >= 0)
+        rtype, _ = p.mesh.solver_regions()
+        assert (P.BC_INTERFACE in rtype) == (p.n_iface > 0)
+    cut = np.zeros(m.n_face, bool)
+    for p in parts:
+        cut[p.faces[p.iface_first:p.iface_first + p.n_iface]] = True
+    # original boundary and uncut interior faces once; cut faces once in each of their two parts
+    assert np.all(count[~cut] == 1) and np.all(count[cut] == 2)
+
+
+@pytest.mark.parametrize("kind", sorted(MESHES))
+def test_part_geometry_matches_the_global_mesh(kind):
+    """Cell volumes and centres, and face areas and centres, as the oracle's
+    metrics (UnstructGrid::ComputeMetrics) form them: the same in the part as
+    in the whole mesh; a flipped interface face has the opposite normal."""
+    m = MESHES[kind]()
+    g = Oracle(m, {"refMachNumber": 0.5}).geo
+    for p in P.split(m, P.slab_owner(m, 3)):
+        lg = Oracle(p.mesh, {"refMachNumber": 0.5}).geo
+        nc = p.mesh.n_cell
+        for k in ("vol", "xcc", "ycc", "zcc"):
+            assert rel_err(lg[k][:nc], g[k][p.cells]) <= 1e-14, k
+        for k in ("area", "xfc", "yfc", "zfc"):
+            assert rel_err(lg[k], g[k][p.faces]) <= 1e-14, k
+        sgn = np.where(p.flipped, -1.0, 1.0)
+        for k in ("xfn", "yfn", "zfn"):
+            assert rel_err(lg[k], sgn * g[k][p.faces]) <= 1e-14, k
+
+
+def _simulated_exchange(parts, values):
+    """Fill every part's interface ghosts from the halo maps alone (no
+    communication): what `exchange` moves between ranks."""
+    for p, part in enumerate(parts):
+        for q in part.halo.neighbors:
+            src = parts[q].halo.send[p]
+            values[p][:, part.halo.recv[q]] = values[q][:, src]
+
+
+@pytest.mark.parametrize("kind", sorted(MESHES))
+@pytest.mark.parametrize("nparts", [2, 4])
+def test_halo_maps_fill_ghosts_with_the_neighbour_cells(kind, nparts):
+    m = MESHES[kind]()
+    f = _field(m.n_cell)
+    parts = P.split(m, P.slab_owner(m, nparts))
+    vals = []
+    for p in parts:
+        v = np.full((5, p.mesh.n_cell + p.mesh.n_bface), np.nan)
+        v[:, : p.mesh.n_cell] = f[:, p.cells]
+        vals.append(v)
+    _simulated_exchange(parts, vals)
+    left, right = np.asarray(m.left), np.asarray(m.right)
+    for p, part in enumerate(parts):
+        sl = slice(part.iface_first, part.iface_first + part.n_iface)
+        gf = part.faces[sl]
+        nbr = np.where(part.flipped[sl], left[gf], right[gf])
+        ghosts = vals[p][:, part.mesh.n_cell + part.iface_first + np.arange(part.n_iface)]
+        assert np.array_equal(ghosts, f[:, nbr])
+        # the part's own side of each interface face is its owner (left) cell
+        own = np.where(part.flipped[sl], right[gf], left[gf])
+        assert np.array_equal(part.cells[part.mesh.left[sl]], own)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, kind, out):
+    import torch
+    import torch.distributed as dist
+    import datetime
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        m = MESHES[kind]()
+        part = P.split(m, P.slab_owner(m, world))[rank]
+        f = _field(m.n_cell)
+        nt = part.mesh.n_cell + part.mesh.n_bface
+        field = torch.full((5, nt), float("nan"), dtype=torch.float64)
+        field[:, : part.mesh.n_cell] = torch.from_numpy(f[:, part.cells])
+        P.exchange(part.halo, field)
+        sl = slice(part.iface_first, part.iface_first + part.n_iface)
+        gf = part.faces[sl]
+        nbr = np.where(part.flipped[sl], np.asarray(m.left)[gf], np.asarray(m.right)[gf])
+        got = field[:, part.mesh.n_cell + part.iface_first + np.arange(part.n_iface)].numpy()
+        ok = bool(np.array_equal(got, f[:, nbr])) and part.n_iface > 0
+        np.save(os.path.join(out, f"rank{rank}.npy"), np.array([ok]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind", ["bump", "tets"])
+def test_gloo_exchange_world_size_2(tmp_path, kind):
+    import torch.multiprocessing as mp
+
+    mp.spawn(_rank_main, args=(2, _free_port(), kind, str(tmp_path)), nprocs=2, join=True)
+    assert all(np.load(tmp_path / f"rank{r}.npy")[0] for r in range(2))
