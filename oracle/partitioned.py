@@ -1,0 +1,164 @@
+"""The oracle on a partitioned grid (test infrastructure, like the rest of
+oracle/): one Oracle per part of phenlei_b200.partition.split, stepped phase
+by phase with the reference's interface exchanges between the phases.
+
+The reference runs a partitioned grid as zones joined by INTERFACE faces
+(PHENGLEI::INTERFACE, API/Geometry/include/Geo_SimpleBC.h:32), and fills
+their ghosts from the neighbouring zone at these points:
+
+* set-up: the ghosts' cell centres, then the LSQ weights
+  (Region::SwapGeometry, API/Physics/src/Region.cpp:3257-3268), and one
+  average cell volume over all zones (Region::ComputeGlobalGridSize, :2655-2734);
+* after the update and at initialisation: q (NSSolver::PostSolve,
+  CFD/NSSolver/src/NSSolver.cpp:139-142);
+* after the gradient: the primitive and temperature gradients
+  (Controller::ComputeGradient, CFD/Solver/src/Controller.cpp:1288);
+* after the limiter: limit2D (Controller.cpp:1321);
+* between the forward and the backward LU-SGS sweep: dq (Controller.cpp:1917-1924).
+
+The residual norm is a sum over all zones (PH_AllReduce).  The exchanges here
+are plain array copies between the in-process parts; phenlei_b200.partition.exchange
+moves the same values between ranks.
+
+Covered: NS, inviscid and laminar, GG-cell or LSQ gradient, one LU-SGS
+sweep, no initialisation phase, ktmax inactive.  Not covered: GG-node (its
+node values need the interpoint exchange, Controller::PostSolve
+:5063-5205), Spalart-Allmaras, the global minimum time step of the ktmax
+clamp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from phenlei_b200 import partition as P
+
+from .oracle import Oracle, _p, lib
+
+
+class PartitionedOracle:
+    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None):
+        if params.get("gradientName", "ggcell") == "ggnode":
+            raise ValueError("GG-node across parts needs the interpoint exchange; not restated")
+        if params.get("viscousType", 0) not in (0, 1):
+            raise ValueError("inviscid and laminar runs only")
+        if params.get("flowInitStep", 100) != 0 or params.get("uns_limiter_name", "vencat") == "1st":
+            raise ValueError("second order from the first step only (flowInitStep = 0)")
+        if params.get("nLUSGSSweeps", 1) != 1 or params.get("ktmax", 1.0e10) < 1.0e10:
+            raise ValueError("one LU-SGS sweep and an inactive ktmax clamp only")
+        self.mesh = mesh
+        self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
+        self.parts = P.split(mesh, self.owner)
+        self.o = [Oracle(p.mesh, params) for p in self.parts]
+        self.viscous = params.get("viscousType", 0) > 0
+        self.step = 0
+        # SwapGeometry: the interface ghosts take the neighbouring cells' centres,
+        # and the least-squares weights are formed again from them
+        for k in ("xcc", "ycc", "zcc"):
+            self._exchange(lambda o, k=k: o.geo[k])
+        for o in self.o:
+            lib().ox_lsq_weights(C.byref(o.g), C.byref(o.m))
+        # Region::ComputeGlobalGridSize (API/Physics/src/Region.cpp:2655-2734): one
+        # average cell volume for all zones, each zone's sum added across the
+        # ranks (PH_AllReduce); the Venkatakrishnan limiter scales with it
+        tot, n = 0.0, 0
+        for o in self.o:
+            nc = o.mesh.n_cell
+            tot += float(np.cumsum(o.geo["vol"][:nc])[-1]) if nc else 0.0
+            n += nc
+        for o in self.o:
+            o.m.avg_vol = tot / n
+        self._exchange(lambda o: o.q)
+
+    def _exchange(self, get) -> None:
+        """Fill every part's interface ghosts of the array `get(oracle)`
+        ([..., n_total]) from the neighbouring parts' cells."""
+        arrs = [get(o) for o in self.o]
+        for p, part in enumerate(self.parts):
+            for q in part.halo.neighbors:
+                arrs[p][..., part.halo.recv[q]] = arrs[q][..., self.parts[q].halo.send[p]]
+
+    def set_state(self, q_cells: np.ndarray) -> None:
+        """Global cell state [5][n_cell] (reference numbering)."""
+        for part, o in zip(self.parts, self.o):
+            o.set_state(q_cells[:, part.cells])
+        self._exchange(lambda o: o.q)
+
+    def gather(self, name_or_array) -> np.ndarray:
+        """A per-cell work array (or 'q') of every part, in global cell order."""
+        first = self._cells(self.o[0], name_or_array)
+        out = np.zeros(first.shape[:-1] + (self.mesh.n_cell,))
+        for part, o in zip(self.parts, self.o):
+            out[..., part.cells] = self._cells(o, name_or_array)
+        return out
+
+    @staticmethod
+    def _cells(o, name):
+        a = o.q if name == "q" else o.work(name)
+        return a[..., : o.mesh.n_cell]
+
+    def iterate(self, nsteps: int = 1) -> np.ndarray:
+        """`nsteps` outer iterations (ox_ns_iteration phase by phase); returns
+        the global residual norms."""
+        L = lib()
+        hist = []
+        for _ in range(nsteps):
+            self.step += 1
+            for o in self.o:
+                w = o.w_arrays
+                g, m, p = C.byref(o.g), C.byref(o.m), C.byref(o.p)
+                L.ox_gamma_temperature(g, p, _p(o.q), _p(w["gama"]), _p(w["t"]))
+                L.ox_ns_boundary(g, m, p, _p(o.q), _p(w["gama"]))
+                L.ox_gamma_temperature(g, p, _p(o.q), _p(w["gama"]), _p(w["t"]))
+                if self.viscous:
+                    L.ox_viscosity(g, p, _p(w["t"]), _p(w["visl"]), _p(w["vist"]))
+                nt = o.nt
+                for k in range(5):
+                    off = k * nt * 8
+                    L.ox_gradient(g, m, p, C.cast(C.c_void_p(o.q.ctypes.data + off), C.POINTER(C.c_double)),
+                                  *[C.cast(C.c_void_p(w[d].ctypes.data + off), C.POINTER(C.c_double))
+                                    for d in ("dqdx", "dqdy", "dqdz")])
+                if self.viscous:
+                    L.ox_gradient(g, m, p, _p(w["t"]), _p(w["dtdx"]), _p(w["dtdy"]), _p(w["dtdz"]))
+            for d in ("dqdx", "dqdy", "dqdz") + (("dtdx", "dtdy", "dtdz") if self.viscous else ()):
+                self._exchange(lambda o, d=d: o.w_arrays[d])
+            for o in self.o:
+                w = o.w_arrays
+                L.ox_limiter(C.byref(o.g), C.byref(o.m), C.byref(o.p), _p(o.q), _p(w["dqdx"]), _p(w["dqdy"]),
+                             _p(w["dqdz"]), _p(w["limit"]))
+            self._exchange(lambda o: o.w_arrays["limit"])
+            for o in self.o:
+                w = o.w_arrays
+                g, m, p = C.byref(o.g), C.byref(o.m), C.byref(o.p)
+                w["res"][:] = 0.0
+                L.ox_inviscid_flux(g, m, p, _p(o.q), _p(w["gama"]), _p(w["dqdx"]), _p(w["dqdy"]), _p(w["dqdz"]),
+                                   _p(w["limit"]), _p(w["res"]))
+                if self.viscous:
+                    L.ox_viscous_flux(g, m, p, _p(o.q), _p(w["t"]), _p(w["visl"]), _p(w["vist"]), _p(w["dqdx"]),
+                                      _p(w["dqdy"]), _p(w["dqdz"]), _p(w["dtdx"]), _p(w["dtdy"]), _p(w["dtdz"]),
+                                      _p(w["res"]))
+                L.ox_spectrum(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["inv_spec"]),
+                              _p(w["vis_spec"]))
+                L.ox_timestep(g, m, p, self.step, _p(o.q), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dt"]))
+                o._dflux = np.zeros((5, o.nt))
+                L.ox_lusgs_forward(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["res"]),
+                                   _p(w["dt"]), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dq"]), _p(o._dflux))
+            self._exchange(lambda o: o.w_arrays["dq"])
+            s, n = 0.0, 0
+            for o in self.o:
+                w = o.w_arrays
+                g, m, p = C.byref(o.g), C.byref(o.m), C.byref(o.p)
+                L.ox_lusgs_backward(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["res"]),
+                                    _p(w["dt"]), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dq"]), _p(o._dflux))
+                L.ox_update(g, m, p, _p(o.q), _p(w["gama"]), _p(w["dq"]))
+                nc = o.mesh.n_cell
+                r = w["res"][0, :nc]
+                s += float(np.cumsum(r * r)[-1]) if nc else 0.0   # sequential, as ox_residual_norm sums
+                n += nc
+            hist.append(np.sqrt(s / n))
+            # PostSolve: interface ghosts of the updated state, then the boundary
+            self._exchange(lambda o: o.q)
+            for o in self.o:
+                L.ox_ns_boundary(C.byref(o.g), C.byref(o.m), C.byref(o.p), _p(o.q), _p(o.w_arrays["gama"]))
+        return np.array(hist)

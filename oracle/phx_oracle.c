@@ -225,6 +225,8 @@ static void lsq_weights(const ox_grid *g, ox_metrics *m)
     }
 }
 
+void ox_lsq_weights(const ox_grid *g, ox_metrics *m) { lsq_weights(g, m); }
+
 void ox_compute_metrics(const ox_grid *g, ox_metrics *m)
 {
     face_metrics(g, m);
@@ -342,6 +344,8 @@ void ox_ns_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, d
             bc_symmetry(g, m, f, q, nt);
         } else if (t == OX_BC_FARFIELD) {
             bc_farfield(g, m, p, f, q, gama, nt);
+        } else if (t == OX_BC_INTERFACE) {
+            /* NSSolverUnstruct::Boundary skips interface faces (:13474) */
         } else {
             /* extrapolation / outflow: ghost copies the owner */
             int le = g->left[f], re = g->n_cell + f;
@@ -430,11 +434,17 @@ static inline double venfun(double x, double y, double eps)
     return (x2 + eps + 2.0 * xy) / (x2 + 2.0 * y2 + xy + eps);
 }
 
-/* Limiter::MinMaxDiff, Limiter.cpp:1202-1252 (boundary faces excluded). */
+/* Limiter::MinMaxDiff, Limiter.cpp:1202-1252 (boundary faces excluded, but
+ * for interface faces). */
 static void minmaxdiff(const ox_grid *g, const double *q, double *dmin, double *dmax)
 {
     int nc = g->n_cell;
     for (int c = 0; c < nc; ++c) dmin[c] = dmax[c] = q[c];
+    for (int f = 0; f < g->n_bface; ++f) {   /* interface ghosts count as neighbours (:1219-1231) */
+        if (g->region_type[g->bface_region[f]] != OX_BC_INTERFACE) continue;
+        int le = g->left[f];
+        dmin[le] = omin(dmin[le], q[nc + f]); dmax[le] = omax(dmax[le], q[nc + f]);
+    }
     for (int f = g->n_bface; f < g->n_face; ++f) {
         int le = g->left[f], re = g->right[f];
         dmin[le] = omin(dmin[le], q[re]); dmax[le] = omax(dmax[le], q[re]);
@@ -528,7 +538,7 @@ void ox_limiter(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     }
     for (int f = 0; f < g->n_bface; ++f) {
         int t = g->region_type[g->bface_region[f]];
-        if (t != OX_BC_SYMMETRY && !is_wall(t) && t != OX_BC_OUTFLOW) {
+        if (t != OX_BC_INTERFACE && t != OX_BC_SYMMETRY && !is_wall(t) && t != OX_BC_OUTFLOW) {
             limit[g->left[f]] = 0.0;
             limit[g->n_cell + f] = 0.0;
         }
@@ -961,7 +971,7 @@ void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
         double d1 = sqrt(dxl * dxl + dyl * dyl + dzl * dzl), d2 = sqrt(dxr * dxr + dyr * dyr + dzr * dzr);
         double dlt = 1.0 / (d1 + d2 + OX_SMALL);
         double dwl = d2 * dlt, dwr = d1 * dlt;
-        if (f < nb) { dwl = 1.0; dwr = 0.0; }
+        if (f < nb && bt != OX_BC_INTERFACE) { dwl = 1.0; dwr = 0.0; }   /* FaceWeight, Geo_UnstructGrid.cpp:2475 */
         /* GetVisFaceValue */
         double mul = 0.5 * (visl[le] + visl[re]);
         double mut = 0.5 * (vist[le] + vist[re]);
@@ -1018,7 +1028,7 @@ void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
             double dtmp = dL * dL + dR * dR;
             double wL = dL * dL / dtmp;
             double wR = 1.0 - wL;
-            if (f < nb) { wL = 1.0; wR = 0.0; }
+            if (f < nb && bt != OX_BC_INTERFACE) { wL = 1.0; wR = 0.0; }   /* ComputeVisflux :13261 */
             for (int k = 0; k < 5; ++k) {
                 double e1 = (f1[k] - fm[k]) / dL, e2 = (f2[k] - fm[k]) / dR;
                 dfdn[k] = wL * e1 + wR * e2;
@@ -1257,81 +1267,129 @@ static void ghost_dq(const ox_grid *g, const ox_metrics *m, const ox_params *p, 
     }
 }
 
+static double *lusgs_diag(const ox_grid *g, const ox_params *p, const double *dt, const double *inv_spec,
+                          const double *vis_spec)
+{
+    double *diag = malloc(sizeof(double) * g->n_cell);
+    for (int c = 0; c < g->n_cell; ++c) {
+        diag[c] = 1.0 / dt[c] + inv_spec[c];
+        if (p->viscous) diag[c] += vis_spec[c];
+    }
+    return diag;
+}
+
+/* SolveLUSGSForward (NSSolverUnstruct.cpp:15118-15444): lower neighbours
+ * j < i over interior faces; then SetGhostDQLUSGS (:15428). */
+static double sweep_forward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                            const double *gama, const double *visl, const double *vist, const double *res,
+                            const double *diag, double *dq, double *dflux)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    double norm = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        double rhs0[5] = {0, 0, 0, 0, 0}, ux[5], old[5];
+        for (int k = 0; k < 5; ++k) {
+            old[k] = dq[k * nt + c];
+            dq[k * nt + c] = res[k * nt + c];
+            ux[k] = dflux[k * nt + c];
+            dflux[k * nt + c] = 0.0;
+        }
+        for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+            int f = m->c2f[j];
+            if (f < g->n_bface) continue;
+            int le = g->left[f], re = g->right[f];
+            if (le > c || re > c) continue;
+            double df[5];
+            lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
+            for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+        }
+        for (int k = 0; k < 5; ++k) {
+            double v = (dq[k * nt + c] - ux[k] - rhs0[k]) / diag[c];
+            dflux[k * nt + c] += rhs0[k];
+            dq[k * nt + c] = v;
+            norm += (v - old[k]) * (v - old[k]);
+        }
+    }
+    ghost_dq(g, m, p, q, gama, dq);
+    return norm;
+}
+
+/* SolveLUSGSBackward (NSSolverUnstruct.cpp:15446-15690): upper neighbours
+ * j > i, boundary ghosts included. */
+static double sweep_backward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                             const double *gama, const double *visl, const double *vist, const double *res,
+                             const double *diag, double *dq, double *dflux)
+{
+    int nt = ntot(g), nc = g->n_cell;
+    double norm = 0.0;
+    for (int c = nc - 1; c >= 0; --c) {
+        double rhs0[5] = {0, 0, 0, 0, 0}, lx[5], old[5];
+        for (int k = 0; k < 5; ++k) {
+            old[k] = dq[k * nt + c];
+            dq[k * nt + c] = res[k * nt + c];
+            lx[k] = dflux[k * nt + c];
+            dflux[k * nt + c] = 0.0;
+        }
+        for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
+            int f = m->c2f[j];
+            int le = g->left[f], re = f < g->n_bface ? nc + f : g->right[f];
+            if (le < c || re < c) continue;
+            double df[5];
+            lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
+            for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
+        }
+        for (int k = 0; k < 5; ++k) {
+            double v = (dq[k * nt + c] - lx[k] - rhs0[k]) / diag[c];
+            dflux[k * nt + c] += rhs0[k];
+            dq[k * nt + c] = v;
+            norm += (v - old[k]) * (v - old[k]);
+        }
+    }
+    return norm;
+}
+
 /* Controller::LUSGS (Controller.cpp:1878-1955), one or more symmetric sweeps:
- * Diagonal (NSSolverUnstruct.cpp:15867-15935), SolveLUSGSForward
- * (15118-15444, lower neighbours j < i, interior faces only),
- * SetGhostDQLUSGS, SolveLUSGSBackward (15446-15690, upper neighbours j > i,
- * boundary ghosts included).  dq [5][nTotal] is the output. */
+ * Diagonal (NSSolverUnstruct.cpp:15867-15935), the forward sweep with
+ * SetGhostDQLUSGS, the backward sweep.  dq [5][nTotal] is the output. */
 void ox_lusgs(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
               const double *t, const double *visl, const double *vist, const double *res, const double *dt,
               const double *inv_spec, const double *vis_spec, double *dq)
 {
     (void)t;
-    int nt = ntot(g), nc = g->n_cell;
-    double *diag = malloc(sizeof(double) * nc);
+    int nt = ntot(g);
+    double *diag = lusgs_diag(g, p, dt, inv_spec, vis_spec);
     double *dflux = calloc((size_t)5 * nt, sizeof(double));
-    for (int c = 0; c < nc; ++c) {
-        diag[c] = 1.0 / dt[c] + inv_spec[c];
-        if (p->viscous) diag[c] += vis_spec[c];
-    }
     /* LUSGSInitialization (Controller.cpp:1732-1785): dq = res for a single
      * sweep (ghost residuals are zero), zero otherwise. */
     for (int i = 0; i < 5 * nt; ++i) dq[i] = p->n_sweeps == 1 ? res[i] : 0.0;
     double norm0 = 0.0;
     for (int sweep = 0; sweep < p->n_sweeps; ++sweep) {
-        double norm = 0.0;
-        for (int c = 0; c < nc; ++c) {
-            double rhs0[5] = {0, 0, 0, 0, 0}, ux[5], old[5];
-            for (int k = 0; k < 5; ++k) {
-                old[k] = dq[k * nt + c];
-                dq[k * nt + c] = res[k * nt + c];
-                ux[k] = dflux[k * nt + c];
-                dflux[k * nt + c] = 0.0;
-            }
-            for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
-                int f = m->c2f[j];
-                if (f < g->n_bface) continue;
-                int le = g->left[f], re = g->right[f];
-                if (le > c || re > c) continue;
-                double df[5];
-                lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
-                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
-            }
-            for (int k = 0; k < 5; ++k) {
-                double v = (dq[k * nt + c] - ux[k] - rhs0[k]) / diag[c];
-                dflux[k * nt + c] += rhs0[k];
-                dq[k * nt + c] = v;
-                norm += (v - old[k]) * (v - old[k]);
-            }
-        }
-        ghost_dq(g, m, p, q, gama, dq);
-        for (int c = nc - 1; c >= 0; --c) {
-            double rhs0[5] = {0, 0, 0, 0, 0}, lx[5], old[5];
-            for (int k = 0; k < 5; ++k) {
-                old[k] = dq[k * nt + c];
-                dq[k * nt + c] = res[k * nt + c];
-                lx[k] = dflux[k * nt + c];
-                dflux[k * nt + c] = 0.0;
-            }
-            for (int j = m->c2f_off[c]; j < m->c2f_off[c + 1]; ++j) {
-                int f = m->c2f[j];
-                int le = g->left[f], re = f < g->n_bface ? nc + f : g->right[f];
-                if (le < c || re < c) continue;
-                double df[5];
-                lusgs_face(g, m, p, q, gama, visl, vist, dq, c, f, df);
-                for (int k = 0; k < 5; ++k) rhs0[k] += df[k];
-            }
-            for (int k = 0; k < 5; ++k) {
-                double v = (dq[k * nt + c] - lx[k] - rhs0[k]) / diag[c];
-                dflux[k * nt + c] += rhs0[k];
-                dq[k * nt + c] = v;
-                norm += (v - old[k]) * (v - old[k]);
-            }
-        }
+        double norm = sweep_forward(g, m, p, q, gama, visl, vist, res, diag, dq, dflux);
+        norm += sweep_backward(g, m, p, q, gama, visl, vist, res, diag, dq, dflux);
         if (sweep == 0) norm0 = norm;
         else if (norm / norm0 < p->lusgs_tol) break;
     }
     free(diag); free(dflux);
+}
+
+void ox_lusgs_forward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                      const double *gama, const double *visl, const double *vist, const double *res,
+                      const double *dt, const double *inv_spec, const double *vis_spec, double *dq, double *dflux)
+{
+    int nt = ntot(g);
+    double *diag = lusgs_diag(g, p, dt, inv_spec, vis_spec);
+    for (int i = 0; i < 5 * nt; ++i) { dq[i] = res[i]; dflux[i] = 0.0; }
+    sweep_forward(g, m, p, q, gama, visl, vist, res, diag, dq, dflux);
+    free(diag);
+}
+
+void ox_lusgs_backward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                       const double *gama, const double *visl, const double *vist, const double *res,
+                       const double *dt, const double *inv_spec, const double *vis_spec, double *dq, double *dflux)
+{
+    double *diag = lusgs_diag(g, p, dt, inv_spec, vis_spec);
+    sweep_backward(g, m, p, q, gama, visl, vist, res, diag, dq, dflux);
+    free(diag);
 }
 
 /* ------------------------------------------------------------------------ */

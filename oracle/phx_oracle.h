@@ -17,6 +17,10 @@ extern "C" {
 /* Boundary condition codes (API/Geometry/include/Geo_SimpleBC.h:32-39). */
 enum { OX_BC_EXTRAPOLATION = 1, OX_BC_SOLID_SURFACE = 2, OX_BC_SYMMETRY = 3,
        OX_BC_FARFIELD = 4, OX_BC_INFLOW = 5, OX_BC_OUTFLOW = 6 };
+/* PHENGLEI::INTERFACE (Geo_SimpleBC.h:32): a face cut by the partition; its
+ * ghost holds the neighbouring part's cell, filled by the caller's halo
+ * exchange (Geo_UnstructGrid.cpp:10806-10990). */
+enum { OX_BC_INTERFACE = -1 };
 
 typedef struct {
     int n_node, n_face, n_cell, n_bface;
@@ -91,6 +95,10 @@ enum { OX_SCHEME_ROE = 0, OX_SCHEME_AUSMPW_PLUS = 1, OX_SCHEME_STEGER = 2, OX_SC
  * 6545-6819 (cells), 2206-2340 (skewness), Region.cpp:2655-2734 (avg volume),
  * Geo_UnstructGrid.cpp:1246-1304 (cell2face). */
 void ox_compute_metrics(const ox_grid *g, ox_metrics *m);
+/* UnstructGrid::ComputeWeight again, after the caller has set the interface
+ * ghosts' centres to the neighbouring cells' (Region::SwapGeometry,
+ * API/Physics/src/Region.cpp:3257-3268). */
+void ox_lsq_weights(const ox_grid *g, ox_metrics *m);
 
 /* One full outer iteration of NSSolverUnstruct (Controller::Relaxation
  * tscheme=LU_SGS, CFD/Solver/src/Controller.cpp:549-587) at outer step
@@ -142,6 +150,18 @@ void ox_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, cons
 double ox_cfl(const ox_params *p, int step);
 void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
                  const double *inv_spec, const double *vis_spec, double *dt);
+/* The two halves of a single LU-SGS sweep, for a partitioned run
+ * (Controller::LUSGS, Controller.cpp:1917-1924): the forward sweep then
+ * SetGhostDQLUSGS (interface ghosts get dq = 0, its default branch); the
+ * caller fills the interface ghosts with the neighbours' forward dq
+ * (CommunicationDQ); then the backward sweep.  dflux [5][nTotal] carries the
+ * forward sweep's lower fluxes; both need n_sweeps == 1. */
+void ox_lusgs_forward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                      const double *gama, const double *visl, const double *vist, const double *res,
+                      const double *dt, const double *inv_spec, const double *vis_spec, double *dq, double *dflux);
+void ox_lusgs_backward(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q,
+                       const double *gama, const double *visl, const double *vist, const double *res,
+                       const double *dt, const double *inv_spec, const double *vis_spec, double *dq, double *dflux);
 void ox_lusgs(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
               const double *t, const double *visl, const double *vist, const double *res, const double *dt,
               const double *inv_spec, const double *vis_spec, double *dq);

@@ -136,3 +136,64 @@ def test_gloo_exchange_world_size_2(tmp_path, kind):
 
     mp.spawn(_rank_main, args=(2, _free_port(), kind, str(tmp_path)), nprocs=2, join=True)
     assert all(np.load(tmp_path / f"rank{r}.npy")[0] for r in range(2))
+
+
+# --- the oracle on a partitioned grid (oracle/partitioned.py) --------------------------------------
+
+def _global_and_parts(params, nparts, kind="bump", seed=3):
+    from phenlei_b200 import cases
+    from oracle.partitioned import PartitionedOracle
+
+    m = MESHES[kind]()
+    q0 = cases.perturbed_state(m, params, seed=seed)
+    o = Oracle(m, params)
+    o.set_state(q0)
+    po = PartitionedOracle(m, params, nparts)
+    po.set_state(q0)
+    return m, o, po
+
+
+def _case(name):
+    from phenlei_b200 import cases
+
+    return {"euler": cases.EULER_BUMP, "euler_lsq": dict(cases.EULER_BUMP, gradientName="lsq"),
+            "laminar": cases.LAMINAR, "laminar_lsq": dict(cases.LAMINAR, gradientName="lsq"),
+            "euler_barth": dict(cases.EULER_BUMP, uns_limiter_name="barth")}[name]
+
+
+def test_one_part_is_the_whole_mesh():
+    m, o, po = _global_and_parts(_case("laminar"), 1)
+    h0, h1 = o.iterate(3), po.iterate(3)
+    assert np.array_equal(h0, h1)
+    assert np.array_equal(po.gather("q"), o.q[:, : m.n_cell])
+
+
+@pytest.mark.parametrize("case", ["euler", "euler_lsq", "laminar", "laminar_lsq", "euler_barth"])
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_partitioned_explicit_operator_equals_the_whole_mesh(case, nparts):
+    """With the interface ghosts filled as the reference fills them, every
+    explicit quantity of an iteration (gradients, limiter, residual, spectral
+    radius, time step) is the whole mesh's, to rounding: only the LU-SGS
+    sweep (block-Jacobi across parts) differs."""
+    m, o, po = _global_and_parts(_case(case), nparts)
+    o.iterate(1)
+    po.iterate(1)
+    nc = m.n_cell
+    # the three gradient components together: on the quasi-2-D bump d/dz is round-off
+    grad = ("dqdx", "dqdy", "dqdz")
+    assert rel_err(np.stack([po.gather(k) for k in grad]), np.stack([o.work(k)[:, :nc] for k in grad])) <= 1e-12
+    for k in ("limit", "res", "inv_spec", "dt"):
+        assert rel_err(po.gather(k), o.work(k)[..., :nc]) <= 1e-12, k
+    if _case(case).get("viscousType", 0):
+        for k in ("dtdx", "dtdy", "vis_spec"):
+            assert rel_err(po.gather(k), o.work(k)[..., :nc]) <= 1e-12, k
+
+
+def test_block_jacobi_sweep_stays_close_to_the_whole_mesh():
+    """The partitioned LU-SGS couples the parts only through the forward dq
+    of the interface ghosts, so dq differs from the whole mesh's near the cut,
+    and the residual history follows the whole mesh's."""
+    m, o, po = _global_and_parts(_case("euler"), 2)
+    h0, h1 = o.iterate(10), po.iterate(10)
+    assert np.all(np.abs(h1 / h0 - 1.0) < 0.05)
+    assert not np.array_equal(po.gather("dq"), o.work("dq")[:, : m.n_cell])
