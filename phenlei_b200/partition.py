@@ -79,6 +79,15 @@ def slab_owner(m: Mesh, nparts: int, axis: int | None = None) -> np.ndarray:
     return owner
 
 
+def _ranks(counts: np.ndarray) -> np.ndarray:
+    """0, 1, .., n-1 for each run length n in `counts`, concatenated."""
+    counts = np.asarray(counts, np.int64)
+    if counts.size == 0:
+        return np.zeros(0, np.int64)
+    starts = np.repeat(np.cumsum(counts) - counts, counts)
+    return np.arange(int(counts.sum()), dtype=np.int64) - starts
+
+
 def split(m: Mesh, owner: np.ndarray) -> list:
     """The parts of `m` for the cell-to-part map `owner` (values 0..P-1)."""
     owner = np.asarray(owner, np.int32)
@@ -116,12 +125,12 @@ def split(m: Mesh, owner: np.ndarray) -> list:
         nbl = bfaces.size + ifaces.size
         # face nodes: a flipped face keeps its first node and reverses the rest
         fnn = np.asarray(m.face_nnode, np.int64)[faces]
-        f2n = []
-        for k, f in enumerate(faces):
-            nd = m.face2node[foff[f]:foff[f + 1]]
-            f2n.append(np.concatenate([nd[:1], nd[:0:-1]]) if flipped[k] else nd)
-        f2n = np.concatenate(f2n) if f2n else np.zeros(0, np.int32)
-        c2n = np.concatenate([m.cell2node[coff[c]:coff[c + 1]] for c in cells])
+        j = _ranks(fnn)                                   # position of each entry within its face
+        nn = np.repeat(fnn, fnn)
+        j = np.where(np.repeat(flipped, fnn) & (j > 0), nn - j, j)
+        f2n = np.asarray(m.face2node)[np.repeat(foff[faces], fnn) + j]
+        cnn = np.asarray(m.cell_nnode, np.int64)[cells]
+        c2n = np.asarray(m.cell2node)[np.repeat(coff[cells], cnn) + _ranks(cnn)]
         nodes = np.unique(np.concatenate([f2n, c2n]))
         node_local = np.full(m.n_node, -1, dtype=np.int64)
         node_local[nodes] = np.arange(nodes.size)
