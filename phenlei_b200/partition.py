@@ -42,6 +42,18 @@ class Halo:
     def n_send(self) -> int:
         return int(sum(len(v) for v in self.send.values()))
 
+    def index_tensors(self, device):
+        """{q: (send, recv)} as int64 tensors on `device`, made once per device."""
+        import torch
+
+        cache = self.__dict__.setdefault("_index", {})
+        key = str(device)
+        if key not in cache:
+            cache[key] = {q: (torch.as_tensor(self.send[q], dtype=torch.int64, device=device),
+                              torch.as_tensor(self.recv[q], dtype=torch.int64, device=device))
+                          for q in self.neighbors}
+        return cache[key]
+
 
 @dataclass
 class Part:
@@ -179,9 +191,9 @@ def exchange(halo: Halo, field, group=None) -> None:
     if not halo.neighbors:
         return
     ops, bufs = [], []
+    index = halo.index_tensors(field.device)
     for q in halo.neighbors:
-        idx = torch.as_tensor(halo.send[q], device=field.device)
-        out = field.index_select(1, idx).contiguous()
+        out = field.index_select(1, index[q][0]).contiguous()
         inb = torch.empty((field.shape[0], len(halo.recv[q])), dtype=field.dtype, device=field.device)
         ops.append(dist.P2POp(dist.isend, out, q, group))
         ops.append(dist.P2POp(dist.irecv, inb, q, group))
@@ -189,4 +201,4 @@ def exchange(halo: Halo, field, group=None) -> None:
     for r in dist.batch_isend_irecv(ops):
         r.wait()
     for q, inb, _ in bufs:
-        field[:, torch.as_tensor(halo.recv[q], device=field.device)] = inb
+        field[:, index[q][1]] = inb
