@@ -20,11 +20,16 @@ The residual norm is a sum over all zones (PH_AllReduce).  The exchanges here
 are plain array copies between the in-process parts; phenlei_b200.partition.exchange
 moves the same values between ranks.
 
-Covered: NS, inviscid and laminar, GG-cell or LSQ gradient, one LU-SGS
+With Spalart-Allmaras the turbulence step exchanges in the same places: the
+gradient of nu~, its dq between the sweeps (TurbSolverUnstr::SetGhostDQLUSGS
+leaves interface ghosts to that exchange, TurbSolverUnstr.cpp:1660), and
+q_turb with vist in its PostSolve (TurbSolverUnstr::UploadInterfaceValue,
+:7130-7145).  The wall distance of every part is the whole mesh's.
+
+Covered: NS, inviscid, laminar and SA, GG-cell or LSQ gradient, one LU-SGS
 sweep, no initialisation phase, ktmax inactive.  Not covered: GG-node (its
 node values need the interpoint exchange, Controller::PostSolve
-:5063-5205), Spalart-Allmaras, the global minimum time step of the ktmax
-clamp.
+:5063-5205), the global minimum time step of the ktmax clamp.
 """
 from __future__ import annotations
 
@@ -38,11 +43,14 @@ from .oracle import Oracle, _p, lib
 
 
 class PartitionedOracle:
-    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None):
+    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None):
         if params.get("gradientName", "ggcell") == "ggnode":
             raise ValueError("GG-node across parts needs the interpoint exchange; not restated")
-        if params.get("viscousType", 0) not in (0, 1):
-            raise ValueError("inviscid and laminar runs only")
+        if params.get("viscousType", 0) not in (0, 1, 3):
+            raise ValueError("inviscid, laminar and SA runs only")
+        self.sa = params.get("viscousType", 0) == 3
+        if self.sa and wall_dist is None:
+            raise ValueError("the SA model needs the wall distance of every cell")
         if params.get("flowInitStep", 100) != 0 or params.get("uns_limiter_name", "vencat") == "1st":
             raise ValueError("second order from the first step only (flowInitStep = 0)")
         if params.get("nLUSGSSweeps", 1) != 1 or params.get("ktmax", 1.0e10) < 1.0e10:
@@ -50,7 +58,8 @@ class PartitionedOracle:
         self.mesh = mesh
         self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
         self.parts = P.split(mesh, self.owner)
-        self.o = [Oracle(p.mesh, params) for p in self.parts]
+        self.o = [Oracle(p.mesh, params, wall_dist=None if wall_dist is None else np.asarray(wall_dist)[p.cells])
+                  for p in self.parts]
         self.viscous = params.get("viscousType", 0) > 0
         self.step = 0
         # SwapGeometry: the interface ghosts take the neighbouring cells' centres,
@@ -69,7 +78,15 @@ class PartitionedOracle:
             n += nc
         for o in self.o:
             o.m.avg_vol = tot / n
+        self._exchange_state()
+
+    def _exchange_state(self) -> None:
+        """The interface data of NSSolver / TurbSolver PostSolve: q, and with SA
+        q_turb and vist."""
         self._exchange(lambda o: o.q)
+        if self.sa:
+            self._exchange(lambda o: o.w_arrays["qt"])
+            self._exchange(lambda o: o.w_arrays["vist"])
 
     def _exchange(self, get) -> None:
         """Fill every part's interface ghosts of the array `get(oracle)`
@@ -79,11 +96,11 @@ class PartitionedOracle:
             for q in part.halo.neighbors:
                 arrs[p][..., part.halo.recv[q]] = arrs[q][..., self.parts[q].halo.send[p]]
 
-    def set_state(self, q_cells: np.ndarray) -> None:
-        """Global cell state [5][n_cell] (reference numbering)."""
+    def set_state(self, q_cells: np.ndarray, qt_cells=None) -> None:
+        """Global cell state [5][n_cell] (reference numbering), and nu~ [n_cell]."""
         for part, o in zip(self.parts, self.o):
-            o.set_state(q_cells[:, part.cells])
-        self._exchange(lambda o: o.q)
+            o.set_state(q_cells[:, part.cells], None if qt_cells is None else np.asarray(qt_cells)[part.cells])
+        self._exchange_state()
 
     def gather(self, name_or_array) -> np.ndarray:
         """A per-cell work array (or 'q') of every part, in global cell order."""
@@ -161,4 +178,27 @@ class PartitionedOracle:
             self._exchange(lambda o: o.q)
             for o in self.o:
                 L.ox_ns_boundary(C.byref(o.g), C.byref(o.m), C.byref(o.p), _p(o.q), _p(o.w_arrays["gama"]))
+            if self.sa:
+                self._sa_step()
         return np.array(hist)
+
+    def _sa_step(self) -> None:
+        """ox_sa_step phase by phase, with the turbulence solver's exchanges."""
+        L = lib()
+        args = [(C.byref(o.g), C.byref(o.m), C.byref(o.p), _p(o.q), C.byref(o.w)) for o in self.o]
+        for a in args:
+            L.ox_sa_gradient_phase(*a)
+        for d in ("dntx", "dnty", "dntz"):
+            self._exchange(lambda o, d=d: o.w_arrays[d])
+        for o, a in zip(self.o, args):
+            L.ox_sa_residual_phase(*a)
+            o._dfl = np.zeros(o.nt)
+            L.ox_sa_lusgs_forward(a[0], a[1], a[4], _p(o._dfl))
+        self._exchange(lambda o: o.w_arrays["dqt"])
+        for o, a in zip(self.o, args):
+            L.ox_sa_lusgs_backward(a[0], a[1], a[4], _p(o._dfl))
+        self._exchange(lambda o: o.w_arrays["qt"])
+        self._exchange(lambda o: o.w_arrays["vist"])
+        for a in args:
+            L.ox_sa_post_phase(*a)
+

@@ -1827,7 +1827,7 @@ static void sa_convection(const ox_grid *g, const ox_metrics *m, const double *q
         double ql = w->qt[le], qr = w->qt[re];
         double pl[4], pr[4];
         for (int k = 0; k < 4; ++k) { pl[k] = q[k * nt + le]; pr[k] = q[k * nt + re]; }
-        if (f < nb) {
+        if (f < nb && g->region_type[g->bface_region[f]] != OX_BC_INTERFACE) {   /* GetQlQr*: :5041, :5125 */
             int t = g->region_type[g->bface_region[f]];
             if (t == OX_BC_SYMMETRY) qr = ql;
             else { double a = 0.5 * (qr + ql); qr = a; ql = a; }
@@ -1858,7 +1858,7 @@ static void sa_diffusion(const ox_grid *g, const ox_metrics *m, const ox_params 
         /* mlt */
         double nl = qt[le], vl = visl[le], rl = q[le];
         double nr = qt[re], vr = visl[re], rr = q[re];
-        if (f < nb) {
+        if (f < nb && t != OX_BC_INTERFACE) {   /* GetVisFaceValue: interface faces as interior (:3950) */
             if (nl < 0.0) {
                 nl = positive_sa(nl, vl, rl);
                 if (is_wall(t)) nr = -nl;
@@ -1889,7 +1889,7 @@ static void sa_diffusion(const ox_grid *g, const ox_metrics *m, const ox_params 
             double wl = dL * dL / dtmp;
             double wr = 1.0 - wl;
             dfdn = wl * d1 + wr * d2;
-            if (f < nb && t != OX_BC_SYMMETRY) {
+            if (f < nb && t != OX_BC_SYMMETRY && t != OX_BC_INTERFACE) {   /* ComputeVisflux :4569 */
                 double nd = (m->xcc[re] - m->xcc[le]) * nxs + (m->ycc[re] - m->ycc[le]) * nys +
                             (m->zcc[re] - m->zcc[le]) * nzs;
                 dfdn = (f2 - f1) / nd;
@@ -1954,12 +1954,11 @@ static void sa_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *
  * with dq initialised by res (Controller::LUSGSInitialization); ghost dq keep
  * the (zero) ghost residual.  Then UpdateFlowField (1180-1230, RANS, no
  * clipping). */
-static void sa_lusgs_update(const ox_grid *g, const ox_metrics *m, ox_ns_work *w)
+static void sa_sweep_forward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl)
 {
     int nt = ntot(g), nb = g->n_bface, nc = g->n_cell;
     double *dq = w->dqt;
-    double *dfl = calloc((size_t)nt, sizeof(double));
-    for (int i = 0; i < nt; ++i) dq[i] = w->res_t[i];
+    for (int i = 0; i < nt; ++i) { dq[i] = w->res_t[i]; dfl[i] = 0.0; }
     for (int c = 0; c < nc; ++c) {
         double rhs0 = 0.0;
         double ux = dfl[c];
@@ -1975,6 +1974,12 @@ static void sa_lusgs_update(const ox_grid *g, const ox_metrics *m, ox_ns_work *w
         dq[c] = (d - ux - rhs0) / w->spec_t[c];
         dfl[c] += rhs0;
     }
+}
+
+static void sa_sweep_backward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl)
+{
+    int nb = g->n_bface, nc = g->n_cell;
+    double *dq = w->dqt;
     for (int c = nc - 1; c >= 0; --c) {
         double rhs0 = 0.0;
         double lx = dfl[c];
@@ -1990,8 +1995,17 @@ static void sa_lusgs_update(const ox_grid *g, const ox_metrics *m, ox_ns_work *w
         dq[c] = (d - lx - rhs0) / w->spec_t[c];
         dfl[c] += rhs0;
     }
-    free(dfl);
     for (int c = 0; c < nc; ++c) w->qt[c] += dq[c];
+}
+
+void ox_sa_lusgs_forward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl)
+{
+    sa_sweep_forward(g, m, w, dfl);
+}
+
+void ox_sa_lusgs_backward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl)
+{
+    sa_sweep_backward(g, m, w, dfl);
 }
 
 /* Node values of nu~ (TurbSolverUnstr::ComputeQTurbNodeValue,
@@ -2057,9 +2071,9 @@ void ox_qturb_node_values(const ox_grid *g, const double *qt, double *qn)
     free(cnt);
 }
 
-void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+void ox_sa_gradient_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
 {
-    int nt = ntot(g), nc = g->n_cell;
+    int nt = ntot(g);
     /* LoadResiduals: res = -rhs = -0 */
     for (int i = 0; i < nt; ++i) w->res_t[i] = -0.0;
     /* Controller::UpdateResiduals: SetBoundaryValueOfField, UpdateIndependentField
@@ -2076,6 +2090,11 @@ void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     sa_viscosity(g, q, w->qt, w->visl, w->vist);
     if (p->gradient == 2) ox_gradient_ggnode(g, m, w->qt, w->qtnode, w->dntx, w->dnty, w->dntz);
     else ox_gradient(g, m, p, w->qt, w->dntx, w->dnty, w->dntz);
+}
+
+void ox_sa_residual_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    int nt = ntot(g), nc = g->n_cell;
     /* TurbSolver::UpdateResiduals (TurbSolver.cpp:316-346) */
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
     for (int i = 0; i < nt; ++i) w->spec_t[i] = 0.0;
@@ -2083,12 +2102,27 @@ void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const
     sa_source(g, m, p, q, w);
     sa_convection(g, m, q, w);
     sa_diffusion(g, m, p, q, w);
-    /* Controller::LUSGS: Diagonal, sweeps, UpdateFlowField */
+    /* Controller::LUSGS: Diagonal */
     sa_spectrum(g, m, p, q, w);
-    sa_lusgs_update(g, m, w);
+}
+
+void ox_sa_post_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
     /* PostSolve: SetBoundaryValueOfField, then the node values of nu~ */
     ox_sa_boundary(g, m, p, q, w->gama, w->qt, w->vist);
     if (p->gradient == 2 && w->qtnode) ox_qturb_node_values(g, w->qt, w->qtnode);
+}
+
+void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w)
+{
+    double *dfl = malloc(sizeof(double) * (size_t)ntot(g));
+    ox_sa_gradient_phase(g, m, p, q, w);
+    ox_sa_residual_phase(g, m, p, q, w);
+    /* Controller::LUSGS: sweeps, UpdateFlowField */
+    sa_sweep_forward(g, m, w, dfl);
+    sa_sweep_backward(g, m, w, dfl);
+    free(dfl);
+    ox_sa_post_phase(g, m, p, q, w);
 }
 
 /* CorrectGradient, API/Physics/src/GradientOperation.cpp:21-31. */

@@ -179,6 +179,16 @@ void ox_forces(const ox_grid *g, const ox_metrics *m, const ox_params *p, const 
  * step of the same outer iteration (Simulation::SolveSteady,
  * Main/src/Simulation.cpp:1527-1560). */
 void ox_sa_step(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w);
+/* ox_sa_step in the phases a partitioned run exchanges between
+ * (Controller.cpp:1288 gradient of nu~, :1917-1924 dq between the sweeps,
+ * TurbSolver::PostSolve q_turb and vist; TurbSolverUnstr::SetGhostDQLUSGS
+ * leaves interface ghosts to that exchange, TurbSolverUnstr.cpp:1660).
+ * dfl [nTotal] carries the forward sweep's lower fluxes. */
+void ox_sa_gradient_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w);
+void ox_sa_residual_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w);
+void ox_sa_lusgs_forward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl);
+void ox_sa_lusgs_backward(const ox_grid *g, const ox_metrics *m, ox_ns_work *w, double *dfl);
+void ox_sa_post_phase(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, ox_ns_work *w);
 void ox_sa_boundary(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *gama,
                     double *qt, double *vist);
 void ox_viscous_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p, const double *q, const double *t,

@@ -146,10 +146,16 @@ def _global_and_parts(params, nparts, kind="bump", seed=3):
 
     m = MESHES[kind]()
     q0 = cases.perturbed_state(m, params, seed=seed)
-    o = Oracle(m, params)
-    o.set_state(q0)
-    po = PartitionedOracle(m, params, nparts)
-    po.set_state(q0)
+    sa = params.get("viscousType", 0) == 3
+    wd = M.wall_distance(m) if sa else None
+    qt0 = None
+    if sa:   # nu~ around its free-stream value, some cells negative
+        rng = np.random.default_rng(seed)
+        qt0 = params.get("muoo", 3.0) * (1.0 + 1.5 * rng.standard_normal(m.n_cell))
+    o = Oracle(m, params, wall_dist=wd)
+    o.set_state(q0, qt0)
+    po = PartitionedOracle(m, params, nparts, wall_dist=wd)
+    po.set_state(q0, qt0)
     return m, o, po
 
 
@@ -158,17 +164,22 @@ def _case(name):
 
     return {"euler": cases.EULER_BUMP, "euler_lsq": dict(cases.EULER_BUMP, gradientName="lsq"),
             "laminar": cases.LAMINAR, "laminar_lsq": dict(cases.LAMINAR, gradientName="lsq"),
-            "euler_barth": dict(cases.EULER_BUMP, uns_limiter_name="barth")}[name]
+            "euler_barth": dict(cases.EULER_BUMP, uns_limiter_name="barth"),
+            "sa": dict(cases.SA_BUMP, refReNumber=1.0e5), "sa_lsq": dict(cases.SA_BUMP, refReNumber=1.0e5,
+                                                                          gradientName="lsq")}[name]
 
 
-def test_one_part_is_the_whole_mesh():
-    m, o, po = _global_and_parts(_case("laminar"), 1)
+@pytest.mark.parametrize("case", ["laminar", "sa"])
+def test_one_part_is_the_whole_mesh(case):
+    m, o, po = _global_and_parts(_case(case), 1)
     h0, h1 = o.iterate(3), po.iterate(3)
     assert np.array_equal(h0, h1)
     assert np.array_equal(po.gather("q"), o.q[:, : m.n_cell])
+    if case == "sa":
+        assert np.array_equal(po.gather("qt"), o.work("qt")[: m.n_cell])
 
 
-@pytest.mark.parametrize("case", ["euler", "euler_lsq", "laminar", "laminar_lsq", "euler_barth"])
+@pytest.mark.parametrize("case", ["euler", "euler_lsq", "laminar", "laminar_lsq", "euler_barth", "sa", "sa_lsq"])
 @pytest.mark.parametrize("nparts", [2, 3])
 def test_partitioned_explicit_operator_equals_the_whole_mesh(case, nparts):
     """With the interface ghosts filled as the reference fills them, every
@@ -197,3 +208,12 @@ def test_block_jacobi_sweep_stays_close_to_the_whole_mesh():
     h0, h1 = o.iterate(10), po.iterate(10)
     assert np.all(np.abs(h1 / h0 - 1.0) < 0.05)
     assert not np.array_equal(po.gather("dq"), o.work("dq")[:, : m.n_cell])
+
+
+@pytest.mark.parametrize("case", ["laminar", "sa"])
+def test_partitioned_history_follows_the_whole_mesh(case):
+    m, o, po = _global_and_parts(_case(case), 3)
+    h0, h1 = o.iterate(10), po.iterate(10)
+    assert np.all(np.abs(h1 / h0 - 1.0) < 0.05)
+    if case == "sa":
+        assert rel_err(po.gather("qt"), o.work("qt")[: m.n_cell]) < 0.05
