@@ -57,7 +57,7 @@ class PartitionedOracle:
             raise ValueError("one LU-SGS sweep and an inactive ktmax clamp only")
         self.mesh = mesh
         self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
-        self.parts = P.split(mesh, self.owner)
+        self.parts = self._local(P.split(mesh, self.owner))
         self.o = [Oracle(p.mesh, params, wall_dist=None if wall_dist is None else np.asarray(wall_dist)[p.cells])
                   for p in self.parts]
         self.viscous = params.get("viscousType", 0) > 0
@@ -76,6 +76,7 @@ class PartitionedOracle:
             nc = o.mesh.n_cell
             tot += float(np.cumsum(o.geo["vol"][:nc])[-1]) if nc else 0.0
             n += nc
+        tot, n = self._allsum(tot, n)
         for o in self.o:
             o.m.avg_vol = tot / n
         self._exchange_state()
@@ -87,6 +88,14 @@ class PartitionedOracle:
         if self.sa:
             self._exchange(lambda o: o.w_arrays["qt"])
             self._exchange(lambda o: o.w_arrays["vist"])
+
+    def _local(self, parts):
+        """The parts this process steps (all of them in process)."""
+        return parts
+
+    def _allsum(self, s: float, n: int):
+        """The sums over all parts (PH_AllReduce); in process they are complete."""
+        return s, n
 
     def _exchange(self, get) -> None:
         """Fill every part's interface ghosts of the array `get(oracle)`
@@ -173,6 +182,7 @@ class PartitionedOracle:
                 r = w["res"][0, :nc]
                 s += float(np.cumsum(r * r)[-1]) if nc else 0.0   # sequential, as ox_residual_norm sums
                 n += nc
+            s, n = self._allsum(s, n)
             hist.append(np.sqrt(s / n))
             # PostSolve: interface ghosts of the updated state, then the boundary
             self._exchange(lambda o: o.q)
@@ -201,4 +211,39 @@ class PartitionedOracle:
         self._exchange(lambda o: o.w_arrays["vist"])
         for a in args:
             L.ox_sa_post_phase(*a)
+
+
+class DistributedOracle(PartitionedOracle):
+    """One rank's part of a PartitionedOracle run across processes: the same
+    phases, with the halos moved by phenlei_b200.partition.exchange over the
+    default torch.distributed group (gloo) and the global sums by all_reduce.
+    Every rank builds the same partition and calls the same steps."""
+
+    def __init__(self, mesh, params: dict, rank: int, world: int, owner=None, wall_dist=None):
+        self._rank = rank
+        self._world = world
+        super().__init__(mesh, params, world, owner=owner, wall_dist=wall_dist)
+
+    def _local(self, parts):
+        if len(parts) != self._world:
+            raise ValueError("one part per rank")
+        return [parts[self._rank]]
+
+    def _exchange(self, get) -> None:
+        import torch
+
+        a = get(self.o[0])
+        t = torch.from_numpy(a.reshape(-1, a.shape[-1]))   # shares memory with the array
+        P.exchange(self.parts[0].halo, t)
+
+    def _allsum(self, s: float, n: int):
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([s, float(n)], dtype=torch.float64)
+        dist.all_reduce(t)
+        return float(t[0]), int(round(float(t[1])))
+
+    def local_cells(self):
+        return self.parts[0].cells
 

@@ -217,3 +217,50 @@ def test_partitioned_history_follows_the_whole_mesh(case):
     assert np.all(np.abs(h1 / h0 - 1.0) < 0.05)
     if case == "sa":
         assert rel_err(po.gather("qt"), o.work("qt")[: m.n_cell]) < 0.05
+
+
+def _oracle_rank_main(rank, world, port, case, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    from oracle.partitioned import DistributedOracle
+    from phenlei_b200 import cases
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        params = _case(case)
+        m = MESHES["bump"]()
+        q0 = cases.perturbed_state(m, params, seed=3)
+        sa = params.get("viscousType", 0) == 3
+        wd = M.wall_distance(m) if sa else None
+        qt0 = params.get("muoo", 3.0) * (1.0 + 1.5 * np.random.default_rng(3).standard_normal(m.n_cell)) if sa else None
+        do = DistributedOracle(m, params, rank, world, wall_dist=wd)
+        do.set_state(q0, qt0)
+        hist = do.iterate(3)
+        np.savez(os.path.join(out, f"rank{rank}.npz"), hist=hist, cells=do.local_cells(), q=do.gather("q"),
+                 qt=do.gather("qt") if sa else np.zeros(1))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", ["laminar", "sa"])
+def test_distributed_oracle_world_size_2_equals_in_process(tmp_path, case):
+    """The partitioned oracle as two gloo ranks, each with its own part, halos
+    moved by partition.exchange and sums by all_reduce: the same residual
+    history and state as the in-process partitioned run, bit for bit."""
+    import torch.multiprocessing as mp
+
+    mp.spawn(_oracle_rank_main, args=(2, _free_port(), case, str(tmp_path)), nprocs=2, join=True)
+    m, _, po = _global_and_parts(_case(case), 2)
+    h = po.iterate(3)
+    q = po.gather("q")
+    for r in range(2):
+        d = np.load(tmp_path / f"rank{r}.npz")
+        assert np.array_equal(d["hist"], h)
+        cells = d["cells"]
+        assert np.array_equal(d["q"][:, cells], q[:, cells])
+        if case == "sa":
+            assert np.array_equal(d["qt"][cells], po.gather("qt")[cells])
