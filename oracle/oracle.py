@@ -75,6 +75,7 @@ def lib():
         _lib.ox_cfl.restype = C.c_double
         _lib.ox_residual_norm.restype = C.c_double
         _lib.ox_update.restype = C.c_int
+        _lib.ox_timestep_raw.restype = C.c_double
     return _lib
 
 

@@ -26,10 +26,12 @@ leaves interface ghosts to that exchange, TurbSolverUnstr.cpp:1660), and
 q_turb with vist in its PostSolve (TurbSolverUnstr::UploadInterfaceValue,
 :7130-7145).  The wall distance of every part is the whole mesh's.
 
+The ktmax clamp of the local time step takes the minimum over all zones
+(Controller::GetGlobalMinTimeStep, Controller.cpp:720-751).
+
 Covered: NS, inviscid, laminar and SA, GG-cell or LSQ gradient, one LU-SGS
-sweep, no initialisation phase, ktmax inactive.  Not covered: GG-node (its
-node values need the interpoint exchange, Controller::PostSolve
-:5063-5205), the global minimum time step of the ktmax clamp.
+sweep, no initialisation phase.  Not covered: GG-node (its node values need
+the interpoint exchange, Controller::PostSolve :5063-5205).
 """
 from __future__ import annotations
 
@@ -53,8 +55,8 @@ class PartitionedOracle:
             raise ValueError("the SA model needs the wall distance of every cell")
         if params.get("flowInitStep", 100) != 0 or params.get("uns_limiter_name", "vencat") == "1st":
             raise ValueError("second order from the first step only (flowInitStep = 0)")
-        if params.get("nLUSGSSweeps", 1) != 1 or params.get("ktmax", 1.0e10) < 1.0e10:
-            raise ValueError("one LU-SGS sweep and an inactive ktmax clamp only")
+        if params.get("nLUSGSSweeps", 1) != 1:
+            raise ValueError("one LU-SGS sweep only")
         self.mesh = mesh
         self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
         self.parts = self._local(P.split(mesh, self.owner))
@@ -96,6 +98,10 @@ class PartitionedOracle:
     def _allsum(self, s: float, n: int):
         """The sums over all parts (PH_AllReduce); in process they are complete."""
         return s, n
+
+    def _allmin(self, v: float) -> float:
+        """The minimum over all parts (PH_CompareMaxMin)."""
+        return v
 
     def _exchange(self, get) -> None:
         """Fill every part's interface ghosts of the array `get(oracle)`
@@ -166,7 +172,13 @@ class PartitionedOracle:
                                       _p(w["res"]))
                 L.ox_spectrum(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["inv_spec"]),
                               _p(w["vis_spec"]))
-                L.ox_timestep(g, m, p, self.step, _p(o.q), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dt"]))
+                o._mindt = L.ox_timestep_raw(g, m, p, self.step, _p(o.q), _p(w["inv_spec"]), _p(w["vis_spec"]),
+                                             _p(w["dt"]))
+            mindt = self._allmin(min(o._mindt for o in self.o))
+            for o in self.o:
+                w = o.w_arrays
+                g, m, p = C.byref(o.g), C.byref(o.m), C.byref(o.p)
+                L.ox_timestep_clamp(g, m, p, C.c_double(mindt), _p(w["dt"]))
                 o._dflux = np.zeros((5, o.nt))
                 L.ox_lusgs_forward(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["res"]),
                                    _p(w["dt"]), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dq"]), _p(o._dflux))
@@ -243,6 +255,14 @@ class DistributedOracle(PartitionedOracle):
         t = torch.tensor([s, float(n)], dtype=torch.float64)
         dist.all_reduce(t)
         return float(t[0]), int(round(float(t[1])))
+
+    def _allmin(self, v: float) -> float:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        return float(t[0])
 
     def local_cells(self):
         return self.parts[0].cells

@@ -1123,8 +1123,8 @@ double ox_cfl(const ox_params *p, int step)
  * Controller::ComputeMinTimeStep / ReduceMaxTimeStep (Controller.cpp:706-788,
  * NSSolverUnstruct.cpp:5696-5745): dt = CFL_cell vol / spec, clamped to
  * ktmax * min(dt), divided by vol; ghosts copy the owner. */
-void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
-                 const double *inv_spec, const double *vis_spec, double *dt)
+double ox_timestep_raw(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
+                       const double *inv_spec, const double *vis_spec, double *dt)
 {
     int nt = ntot(g), nc = g->n_cell;
     double cfl = ox_cfl(p, step);
@@ -1142,11 +1142,23 @@ void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int 
         dt[c] = cc * m->vol[c] / spec;
         mindt = omin(mindt, dt[c]);
     }
+    return mindt;
+}
+
+void ox_timestep_clamp(const ox_grid *g, const ox_metrics *m, const ox_params *p, double mindt, double *dt)
+{
+    int nc = g->n_cell;
     for (int c = 0; c < nc; ++c) {
         if (p->ktmax > 0) dt[c] = omin(dt[c], p->ktmax * mindt);
         dt[c] /= m->vol[c];
     }
     for (int f = 0; f < g->n_bface; ++f) dt[nc + f] = dt[g->left[f]];
+}
+
+void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
+                 const double *inv_spec, const double *vis_spec, double *dt)
+{
+    ox_timestep_clamp(g, m, p, ox_timestep_raw(g, m, p, step, q, inv_spec, vis_spec, dt), dt);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -150,6 +150,13 @@ void ox_spectrum(const ox_grid *g, const ox_metrics *m, const ox_params *p, cons
 double ox_cfl(const ox_params *p, int step);
 void ox_timestep(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
                  const double *inv_spec, const double *vis_spec, double *dt);
+/* ox_timestep in two halves for a partitioned run: the CFL-scaled
+ * vol / spectral radius of every cell, returning their minimum; then the
+ * ktmax clamp from the minimum over all zones (Controller::GetGlobalMinTimeStep,
+ * Controller.cpp:720-751, PH_CompareMaxMin) and the division by the volume. */
+double ox_timestep_raw(const ox_grid *g, const ox_metrics *m, const ox_params *p, int step, const double *q,
+                       const double *inv_spec, const double *vis_spec, double *dt);
+void ox_timestep_clamp(const ox_grid *g, const ox_metrics *m, const ox_params *p, double mindt, double *dt);
 /* The two halves of a single LU-SGS sweep, for a partitioned run
  * (Controller::LUSGS, Controller.cpp:1917-1924): the forward sweep then
  * SetGhostDQLUSGS (interface ghosts get dq = 0, its default branch); the

@@ -165,6 +165,7 @@ def _case(name):
     return {"euler": cases.EULER_BUMP, "euler_lsq": dict(cases.EULER_BUMP, gradientName="lsq"),
             "laminar": cases.LAMINAR, "laminar_lsq": dict(cases.LAMINAR, gradientName="lsq"),
             "euler_barth": dict(cases.EULER_BUMP, uns_limiter_name="barth"),
+            "euler_ktmax": dict(cases.EULER_BUMP, ktmax=1.5),
             "sa": dict(cases.SA_BUMP, refReNumber=1.0e5), "sa_lsq": dict(cases.SA_BUMP, refReNumber=1.0e5,
                                                                           gradientName="lsq")}[name]
 
@@ -179,7 +180,8 @@ def test_one_part_is_the_whole_mesh(case):
         assert np.array_equal(po.gather("qt"), o.work("qt")[: m.n_cell])
 
 
-@pytest.mark.parametrize("case", ["euler", "euler_lsq", "laminar", "laminar_lsq", "euler_barth", "sa", "sa_lsq"])
+@pytest.mark.parametrize("case", ["euler", "euler_lsq", "laminar", "laminar_lsq", "euler_barth", "euler_ktmax", "sa",
+                                  "sa_lsq"])
 @pytest.mark.parametrize("nparts", [2, 3])
 def test_partitioned_explicit_operator_equals_the_whole_mesh(case, nparts):
     """With the interface ghosts filled as the reference fills them, every
