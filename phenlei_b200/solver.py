@@ -299,16 +299,25 @@ class NSSolverUnstruct:
         """Wall force sums (AirForceCoefParts) and CL / CD (Force.cpp:441-536)."""
         out = np.zeros(16)
         self._check(lib().phx_forces(self.h, out.ctypes.data), "phx_forces")
-        import math
-
-        a = math.radians(self.params.attackd)
-        b = math.radians(self.params.angleSlide)
-        cf = (out[0:6:2] + out[1:6:2]) / reference_area
-        cl = -math.sin(a) * cf[0] + math.cos(a) * cf[1]
-        cd = math.cos(a) * math.cos(b) * cf[0] + math.sin(a) * math.cos(b) * cf[1] + math.sin(b) * cf[2]
-        return {"sums": out, "CL": cl, "CD": cd}
+        return force_coefficients(out, self.params.attackd, self.params.angleSlide, reference_area)
 
     def GetResidual(self) -> np.ndarray:
         out = np.zeros(5)
         self._check(lib().phx_residual_norm(self.h, out.ctypes.data), "phx_residual_norm")
         return out
+
+
+def force_coefficients(sums, attackd: float = 0.0, angleSlide: float = 0.0, reference_area: float = 1.0) -> dict:
+    """CL and CD from the 16 wall force sums of AirForceCoefParts
+    (CA_f CA_p CN_f CN_p CZ_f CZ_p ...): the body-axis force coefficients scaled
+    by 1 / forceReferenceArea and rotated by the angles of attack and sideslip
+    (degrees), as Force.cpp:441-536 does."""
+    import math
+
+    out = np.asarray(sums, dtype=np.float64)
+    a = math.radians(attackd)
+    b = math.radians(angleSlide)
+    cf = (out[0:6:2] + out[1:6:2]) / reference_area
+    cl = -math.sin(a) * cf[0] + math.cos(a) * cf[1]
+    cd = math.cos(a) * math.cos(b) * cf[0] + math.sin(a) * math.cos(b) * cf[1] + math.sin(b) * cf[2]
+    return {"sums": out, "CL": cl, "CD": cd}
