@@ -345,6 +345,85 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
     return res
 
 
+def converge(args, m, wd):
+    """The configuration's full iteration count for the three arms on one GPU
+    (FP64 exact source, mixed exact source, mixed learned source), from the
+    free stream.  The learned source is trained on FP64 states captured along
+    the FP64 run (early, middle and final), so it sees the flow it meets.
+    Reports CL, CD and the residual monitor of every arm at the end, the
+    differences of the mixed arms against FP64, and each arm's whole-run
+    throughput (CUDA events around the whole run)."""
+    import torch
+
+    from phenlei_b200 import solver as S
+
+    torch.cuda.set_device(0)
+    wl = workloads()[args.workload]
+    params = dict(wl["params"])
+    sa = params.get("viscousType", 0) == 3
+    n = args.iterations
+    nc = m.n_cell
+    out = {"workload": args.workload, "cells": nc, "iterations": n}
+
+    def run(precision, blob=None, capture_at=()):
+        p = dict(params)
+        if blob is not None:
+            p["sa_source"] = "mlp_fallback"
+        s = S.NSSolverUnstruct(m, precision=precision, wall_dist=wd, **p)
+        if blob is not None:
+            s.set_mlp_blob(blob)
+        stream = torch.cuda.current_stream()
+        s.set_stream(stream.cuda_stream)
+        caps, hist, done, ms = [], [], 0, 0.0
+        for stop in sorted(set([c for c in capture_at if 0 < c < n] + [n])):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            hist.append(s.Relaxation(stop - done))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            done = stop
+            if stop in capture_at or (capture_at and stop == n):
+                caps.append(s.capture_sa_samples()[:2])
+        h = np.concatenate(hist)
+        f = s.AirForceCoef()
+        r = {"CL": f["CL"], "CD": f["CD"], "res_first": float(h[0]), "res_last": float(h[-1]),
+             "res_drop_orders": round(float(np.log10(h[0] / h[-1])), 3), "ms_per_iter": round(ms / n, 4),
+             "mcell_iters_per_s": round(nc * n / (ms / 1e3) / 1e6, 3)}
+        if sa:
+            r["vist"] = s.get(S.PHX_VIST)[:nc]
+        if blob is not None:
+            r["cells_learned_per_iteration"] = round(s.mlp_cells() / n, 1)
+        blob_out = None
+        if caps:
+            f_, t_ = np.concatenate([c[0] for c in caps]), np.concatenate([c[1] for c in caps])
+            f_, t_ = balanced_subsample(f_, t_, 2_000_000, seed=0)
+            t1 = time.perf_counter()
+            loss = s.train_sa_mlp(f_, t_, epochs=60, batch=8192, lr=1e-3, seed=0)
+            r["mlp"] = {"samples": int(len(t_)), "epochs": 60, "final_loss": loss,
+                        "train_s": round(time.perf_counter() - t1, 2)}
+            blob_out = s.mlp_blob()
+        s.close()
+        return r, blob_out
+
+    r64, blob = run("fp64", capture_at=(30, n // 10, n) if sa else ())
+    arms = {"fp64": r64}
+    arms["mixed_exact"], _ = run("mixed")
+    if sa:
+        arms["mixed_learned"], _ = run("mixed", blob=blob)
+    for name, r in arms.items():
+        if name != "fp64":
+            r["dCL_vs_fp64"] = abs(r["CL"] - r64["CL"])
+            r["dCD_vs_fp64"] = abs(r["CD"] - r64["CD"])
+            if sa:
+                r["dVIST_rel_vs_fp64"] = float(np.max(np.abs(r["vist"] - r64["vist"])) / np.max(np.abs(r64["vist"])))
+            r["speedup_vs_fp64"] = round(r["mcell_iters_per_s"] / r64["mcell_iters_per_s"], 3)
+    for r in arms.values():
+        r.pop("vist", None)
+    out["arms"] = arms
+    return out
+
+
 def cpu_baseline(args, wl_name, sample_budget_s=20.0):
     """The oracle (single-threaded CPU restatement of the reference path) on a
     bounded sample of the workload: the same case kind at a size it finishes
@@ -370,8 +449,8 @@ def cpu_baseline(args, wl_name, sample_budget_s=20.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="phx", choices=["phx", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -380,6 +459,9 @@ def main():
     ap.add_argument("--save-mlp", default=None, help="write the trained learned-source model (.npy)")
     ap.add_argument("--mlp-blob", default=None, help="use this learned-source model (.npy) instead of training one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--converge", action="store_true",
+                    help="run the configuration's full iteration count for every arm and report converged CL/CD")
+    ap.add_argument("--iterations", type=int, default=3000, help="iterations of a --converge run")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -396,6 +478,14 @@ def main():
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-iters/s",
                                              "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return
+
+    if args.converge:
+        from phenlei_b200 import mesh as M
+
+        m = wl["mesh"]()
+        wd = M.wall_distance(m) if wl.get("wall_dist") else None
+        print(json.dumps({"converge": converge(args, m, wd)}))
         return
 
     if world > 1:

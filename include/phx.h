@@ -264,10 +264,26 @@ int phx_residual_norm(phx_ctx *ctx, double out[5]);
  * context and allocates nothing: the partial sums live in a fixed 64 KiB
  * device array of the library (at most 8 variables; larger nvar is rejected
  * with PHX_ERR_ARG; any n_cell).  The first call on a device looks the array
- * up, so make it before any stream capture.  Calls that overlap on one device
- * share the array and race: serialise them. */
+ * up, so make it before any stream capture.  Each call waits for `stream` to
+ * finish before it returns.  A CUDA error the calling thread left unchecked is
+ * reported as PHX_ERR_CUDA and left in place, with nothing launched.  Calls
+ * that overlap on one device share the array and race: serialise them. */
 int phx_residual_norm_noalloc(const double *res_dev, int64_t n_cell, int64_t n_total, int nvar, double *out_host,
                               void *stream);
+
+/* Bound on every device-side dependency wait of the LU-SGS sweeps, in polls
+ * (default 20,000,000, about one to two seconds).  A wait that runs out ends
+ * its sweep: the step's call returns PHX_ERR_TIMEOUT, the status is cleared,
+ * and the context stays usable (its state is then undefined until the next
+ * phx_set_state).  No counterpart in the reference, whose sweeps are
+ * sequential host loops (Controller::LUSGS, Controller.cpp:1878). */
+int phx_set_wait_limit(phx_ctx *ctx, int64_t polls);
+
+/* Failure-detection hook for tests: the forward LU-SGS result of reference
+ * cell `cell` never comes (-1: off), so the wait on it runs out and the step
+ * returns PHX_ERR_TIMEOUT instead of hanging.  Nothing faults: the sweep
+ * stops at its next level boundary.  No counterpart in the reference. */
+int phx_fault_hold_cell(phx_ctx *ctx, int32_t cell);
 
 /* Outer step counter (drives the CFL ramp of NSSolver::ComputeCFL). */
 int phx_set_step(phx_ctx *ctx, int step);

@@ -245,7 +245,12 @@ class DistributedOracle(PartitionedOracle):
         import torch
 
         a = get(self.o[0])
-        t = torch.from_numpy(a.reshape(-1, a.shape[-1]))   # shares memory with the array
+        # the received ghosts must land in the oracle's own array: a reshape of a
+        # non-contiguous array would be a copy, and they would be lost
+        if not a.flags.c_contiguous:
+            raise ValueError("halo exchange needs C-contiguous work arrays")
+        t = torch.from_numpy(a.reshape(-1, a.shape[-1]))
+        assert np.shares_memory(a, t.numpy())
         P.exchange(self.parts[0].halo, t)
 
     def _allsum(self, s: float, n: int):

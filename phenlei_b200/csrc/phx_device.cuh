@@ -83,8 +83,8 @@ __device__ __forceinline__ float idiv(float a, float b) { return __fdiv_rn(a, b)
 __device__ __forceinline__ double idiv(double a, double b) { return a / b; }
 
 // Sweep geometry of the LU-SGS dataflow sweeps: a slot of kSweepLanes lanes
-// per schedule position, kSweepSlots slots per warp.
-static constexpr long long kSpinLimit = 20000000LL;   // ~1-2 s of polling per wait
+// per schedule position, kSweepSlots slots per warp.  Every wait is bounded by
+// NsConst::spinLimit polls (phx_set_wait_limit).
 static constexpr int kSweepThreads = 256;
 static_assert(kSweepLanes * kSweepSlots == 32, "one warp holds kSweepSlots slots");
 static_assert(kSweepMaxEntries == 2 * kSweepLanes, "a cell spans at most two adjacent slots");

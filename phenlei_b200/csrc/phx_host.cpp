@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -69,6 +70,7 @@ struct phx_ctx {
     bool turbNodeValid = false;           // GG-node with SA: qtnode holds node values for the next SA gradient
     int step = 0;
     bool haveResidual = false;
+    std::vector<int> rankOf;              // storage index of each reference cell
 };
 
 namespace {
@@ -812,6 +814,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     const std::vector<int> ord = morton_order(nc, ctx->geom[7].data(), ctx->geom[8].data(), ctx->geom[9].data());
     std::vector<int> rank(nc);
     for (int i = 0; i < nc; ++i) rank[ord[i]] = i;
+    ctx->rankOf = rank;
     std::vector<int> forder(nf);   // storage face -> reference face
     for (int f = 0; f < nf; ++f) forder[f] = f;
     std::stable_sort(forder.begin(), forder.begin() + nb, [&](int a, int b) { return rank[h.left[a]] < rank[h.left[b]]; });
@@ -1039,6 +1042,8 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
     k.vistInf = prm->freeStreamViscosity;
     k.turbCflScale = prm->turbCFLScale;
     k.saSource = prm->viscousType == 3 ? prm->sa_source : 0;
+    k.spinLimit = kDefaultSpinLimit;
+    k.holdCell = -1;
 
     // device grid
     DevGrid &g = ctx->g;
@@ -1483,8 +1488,29 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
     if (res_hist && nsteps > 0)
         PHX_CUDA(ctx, cudaMemcpyAsync(res_hist, ctx->hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
     PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (red.error != 0) {
+        // reported once: the next call starts with a clear status
+        PHX_CUDA(ctx, cudaMemsetAsync(&ctx->red->error, 0, sizeof(int), ctx->stream));
+        PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
     if (red.error == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
+    return PHX_OK;
+}
+
+int phx_set_wait_limit(phx_ctx *ctx, int64_t polls)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (polls <= 0) return fail(ctx, PHX_ERR_ARG, "the wait limit must be positive");
+    ctx->nc.spinLimit = polls;
+    return PHX_OK;
+}
+
+int phx_fault_hold_cell(phx_ctx *ctx, int32_t cell)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    if (cell < -1 || cell >= ctx->nCell) return fail(ctx, PHX_ERR_ARG, "cell out of range");
+    ctx->nc.holdCell = cell < 0 ? -1 : ctx->rankOf[cell];
     return PHX_OK;
 }
 

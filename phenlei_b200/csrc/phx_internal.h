@@ -48,6 +48,7 @@ constexpr int kCoef = 4;   // LU-SGS factors per face use: l1 x1 x2 | viscous sp
 constexpr int kSweepLanes = 4;   // LU-SGS lanes (neighbour entries) per schedule slot
 constexpr int kSweepSlots = 8;   // slots per warp: schedule levels are padded to this multiple
 constexpr int kSweepMaxEntries = 2 * kSweepLanes;   // entries of a cell: one slot, or two adjacent slots
+constexpr long long kDefaultSpinLimit = 20000000LL;   // polls per dependency wait (~1-2 s)
 // Spalart-Allmaras records
 constexpr int kTr = 4;     // trec: nu~ | eddy viscosity | laminar viscosity of the NS step | pad
 constexpr int kTg = 4;     // tgrad: d nu~ / dx, dy, dz | pad
@@ -131,6 +132,9 @@ struct NsConst {
     double nutInf, vistInf, turbCflScale;
     int saSource;                  // 0 exact source, 1 learned source (exact for nu~ <= 0), 2 learned inside its
                                    // training hull, exact outside
+    long long spinLimit;           // polls per device-side dependency wait before PHX_ERR_TIMEOUT
+    int holdCell;                  // fault injection: storage cell whose forward LU-SGS result never comes (the
+                                   // wait on it runs out); -1 off
 };
 
 // Working arrays of one precision T (double: FP64 path, float: mixed path).

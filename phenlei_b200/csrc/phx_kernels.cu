@@ -928,17 +928,20 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     }
     GhostStatic<T> gs;
     if (ghost && s.kind == BK_SYMMETRY) ghost_static<T>(s.ql, s.qn, gm, gs);
+    // fault injection (phx_fault_hold_cell): the held cell's lead lane waits on
+    // nothing that is ever set, so its wait runs out
+    if (kForward && lead && lane == 0 && cell == c.holdCell) r2 = false;
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
-        if (spins > kSpinLimit) {
+        if (spins > c.spinLimit) {
             if ((threadIdx.x & 31) == 0) atomicExch(&red->error, PHX_ERR_TIMEOUT);
             return false;
         }
         if ((spins & 1023) == 0 && __any_sync(0xffffffffu, ((volatile int *)&red->error)[0] != 0)) return false;
         if (spins > 8) __nanosleep(20);
         if (!r1) r1 = poll5(src1, v1);
-        if (!r2) r2 = poll5(src2, fl);
+        if (!r2 && src2) r2 = poll5(src2, fl);
     }
     T df[5] = {0, 0, 0, 0, 0};
     if (has) {
@@ -1350,7 +1353,7 @@ static __global__ void reset_reduce_kernel(Reduce *r)
 static __global__ void finish_step_kernel(Reduce *r, double *hist, int i, double ncell)
 {
     const double v = sqrt(r->resnorm[0] / ncell);
-    if (!(v == v) || v > 1.0e300) r->error = PHX_ERR_NUMERIC;
+    if ((!(v == v) || v > 1.0e300) && r->error == 0) r->error = PHX_ERR_NUMERIC;
     if (hist) hist[i] = v;
 }
 

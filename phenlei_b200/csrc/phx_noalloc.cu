@@ -5,7 +5,9 @@
 // a context's cudaMalloc'd Reduce record.  This variant needs no context and
 // allocates nothing: its scratch is the file-scope device array below, whose
 // address is looked up once per device with cudaGetSymbolAddress (the first
-// call on a device does that set-up; make it before any stream capture).
+// call on a device does that set-up; make it before any stream capture).  Each
+// call waits for its stream before it returns: the result is copied to host
+// memory.
 //
 // Scratch contract:
 //  * capacity: kNoAllocMaxBlocks x kNoAllocMaxVars partial sums (64 KiB); the
@@ -84,20 +86,23 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_final_kernel(int nblo
     }
 }
 
-// Device address of the scratch, looked up once per device.
+// Device address of the scratch, looked up on the first call on a device (with
+// that device current) and kept; a failed lookup is not kept, so a later call
+// tries again.
 static double *g_noalloc_ptr[kNoAllocMaxDevices];
-static cudaError_t g_noalloc_err[kNoAllocMaxDevices];
-static std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mutex;
 
 static cudaError_t noalloc_scratch(int dev, double **ptr)
 {
-    std::call_once(g_noalloc_once[dev], [dev]() {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
-        g_noalloc_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
         g_noalloc_ptr[dev] = static_cast<double *>(p);
-    });
+    }
     *ptr = g_noalloc_ptr[dev];
-    return g_noalloc_err[dev];
+    return cudaSuccess;
 }
 
 }  // namespace phx
@@ -108,6 +113,9 @@ extern "C" int phx_residual_norm_noalloc(const double *res_dev, int64_t n_cell, 
     using namespace phx;
     if (!res_dev || !out_host || n_cell <= 0 || n_total < n_cell || nvar < 1) return PHX_ERR_ARG;
     if (nvar > kNoAllocMaxVars) return PHX_ERR_ARG;   // beyond the scratch's variable capacity
+    // an error the calling thread left unchecked is not taken for this call's
+    // own: it is reported (PHX_ERR_CUDA) and left in place, and nothing runs
+    if (cudaPeekAtLastError() != cudaSuccess) return PHX_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return PHX_ERR_CUDA;
     double *scratch = nullptr;

@@ -440,7 +440,7 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
 
 template <class T, bool kForward>
 __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *red, const SaSweepIn<T> &s, int lane,
-                                                  int base)
+                                                  int base, long long spinLimit)
 {
     const int cell = s.cell;
     const bool live = cell >= 0;
@@ -461,7 +461,7 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
     long long spins = 0;
     while (!__all_sync(0xffffffffu, r1 && r2)) {
         ++spins;
-        if (spins > kSpinLimit) {
+        if (spins > spinLimit) {
             if ((threadIdx.x & 31) == 0) atomicExch(&red->error, PHX_ERR_TIMEOUT);
             return false;
         }
@@ -499,7 +499,7 @@ __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *
 // matrices and residual records one round ahead.
 template <class T, bool kForward>
 __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T> &t, Reduce *red, int group,
-                                             int wgroup0, int ngroups, int lane, int base)
+                                             int wgroup0, int ngroups, int lane, int base, long long spinLimit)
 {
     const int npos = kForward ? g.nFwdPos : g.nBwdPos;
     const int2 *pinfo = kForward ? g.fwd_pinfo : g.bwd_pinfo;
@@ -520,7 +520,7 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
         SaSweepIn<T> nxt;
         sa_sweep_load<T>(g, t, info, en, lane, nxt);
         entry(p + 2 * ngroups, info, en);
-        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base)) return false;
+        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base, spinLimit)) return false;
         if (en.x >= 0 && en.x < g.nCell) prefetch_l2(t.tcoef + en.z);
         if (lane == 0 && info.x >= 0 && info.y >= 0) prefetch_l2(t.tcrec + (size_t)info.x * kTc);
         cur = nxt;
@@ -530,15 +530,16 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red)
+__global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red,
+                                                                 long long spinLimit)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kSweepLanes, lane = tid % kSweepLanes;
     const int ngroups = (gridDim.x * blockDim.x) / kSweepLanes;
     const int wgroup0 = group & ~(kSweepSlots - 1);
     const int base = (threadIdx.x & 31) & ~(kSweepLanes - 1);
-    if (!sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base)) return;
-    sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base);
+    if (!sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit)) return;
+    sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit);
 }
 
 // Fills the SA sweep's output records with the sentinel.
@@ -557,7 +558,7 @@ template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
                     int numSMs, cudaStream_t s)
 {
-    (void)c; (void)w;
+    (void)w;
     static int perSMcache[2] = {-1, -1};
     int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
     if (perSM < 0) {
@@ -582,7 +583,8 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
     DevGrid gg = g;
     TurbWork<T> tt = t;
     Reduce *rr = red;
-    void *args[] = {&gg, &tt, &rr};
+    long long lim = c.spinLimit;
+    void *args[] = {&gg, &tt, &rr, &lim};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((void *)sa_lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;

@@ -184,7 +184,8 @@ def exchange(halo: Halo, field, group=None) -> None:
     rank's part) from the neighbouring ranks, which call this in the same
     step.  One send and one receive per neighbour, posted together
     (torch.distributed.batch_isend_irecv): gloo for host tensors, NCCL for
-    device tensors."""
+    device tensors.  Part q is the rank q of `group` (default: the default
+    group); the peers are passed to torch.distributed as global ranks."""
     import torch
     import torch.distributed as dist
 
@@ -193,10 +194,11 @@ def exchange(halo: Halo, field, group=None) -> None:
     ops, bufs = [], []
     index = halo.index_tensors(field.device)
     for q in halo.neighbors:
+        peer = q if group is None else dist.get_global_rank(group, q)
         out = field.index_select(1, index[q][0]).contiguous()
         inb = torch.empty((field.shape[0], len(halo.recv[q])), dtype=field.dtype, device=field.device)
-        ops.append(dist.P2POp(dist.isend, out, q, group))
-        ops.append(dist.P2POp(dist.irecv, inb, q, group))
+        ops.append(dist.P2POp(dist.isend, out, peer, group))
+        ops.append(dist.P2POp(dist.irecv, inb, peer, group))
         bufs.append((q, inb, out))
     for r in dist.batch_isend_irecv(ops):
         r.wait()

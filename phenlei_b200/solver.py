@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
         _lib.phx_mlp_set.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         _lib.phx_mlp_blob_size.restype = C.c_int64
         _lib.phx_mlp_cells.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        _lib.phx_set_wait_limit.argtypes = [C.c_void_p, C.c_int64]
+        _lib.phx_fault_hold_cell.argtypes = [C.c_void_p, C.c_int32]
     return _lib
 
 
@@ -212,6 +214,15 @@ class NSSolverUnstruct:
         out = np.empty(n)
         self._check(lib().phx_get_geometry(self.h, name.encode(), out.ctypes.data, n), "phx_get_geometry")
         return out
+
+    def set_wait_limit(self, polls: int):
+        """Bound on every device-side dependency wait of the LU-SGS sweeps, in polls."""
+        self._check(lib().phx_set_wait_limit(self.h, int(polls)), "phx_set_wait_limit")
+
+    def fault_hold_cell(self, cell: int):
+        """Failure-detection hook: the forward LU-SGS result of reference cell
+        `cell` never comes (-1: off), so the step returns PHX_ERR_TIMEOUT."""
+        self._check(lib().phx_fault_hold_cell(self.h, int(cell)), "phx_fault_hold_cell")
 
     @property
     def step(self) -> int:

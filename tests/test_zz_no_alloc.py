@@ -46,6 +46,27 @@ def test_noalloc_residual_norm_matches_context_monitor():
             assert np.max(np.abs(out - ref)) <= TOL * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("n_cell,pad,nvar", [(300_000, 777, 8), (1, 0, 3), (1, 5, 8)])
+def test_noalloc_matches_numpy_on_a_random_array(n_cell, pad, nvar):
+    """Sizes past the partial-sum pass's 1024-block cap (its grid-stride loop),
+    the maximum number of variables, a row stride larger than the cell count,
+    and a single cell; two calls in a row."""
+    import torch
+
+    rng = np.random.default_rng(n_cell + pad + nvar)
+    n_total = n_cell + pad
+    x = rng.standard_normal((nvar, n_total))
+    res = torch.from_numpy(x).cuda()
+    torch.cuda.synchronize()
+    ref = np.sqrt(np.mean(x[:, :n_cell] ** 2, axis=1))
+    f = _noalloc()
+    for _ in range(2):
+        out = np.zeros(nvar)
+        rc = f(res.data_ptr(), n_cell, n_total, nvar, out.ctypes.data, None)
+        assert rc == 0
+        assert np.max(np.abs(out - ref) / ref) <= TOL
+
+
 def test_noalloc_rejects_more_variables_than_its_scratch_holds():
     import torch
 
