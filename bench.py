@@ -83,6 +83,20 @@ def workloads():
             params=dict(cases.LAMINAR, gradientName="lsq"),
             desc="config 2: laminar cube, 100^3 hexes x 6 jittered tets (6.0M cells), M=0.3, Re=1e4, LSQ, "
                  "Roe+Venkat, LU-SGS"),
+        # Config 3: SA flat plate 512x192x32 (3.1M hexes), first cell y+ about 1, M 0.2, Re 5e6, AUSMPW+, CFL 50,
+        # 5,000 iterations.  Config 4 trains the learned source on its states (2M samples, 20 epochs) and also
+        # runs the unseen flow M 0.3, Re 3e6.
+        "sa_plate_3M": dict(
+            mesh=lambda: M.flat_plate(512, 192, 32),
+            params=dict(cases.SA_PLATE),
+            wall_dist=True, iterations=5000, train_epochs=20, unseen=dict(cases.SA_PLATE_UNSEEN),
+            desc="config 3/4: SA flat plate 512x192x32 hex (3.15M cells), lead-in 0.33, plate 2, M=0.2, Re=5e6, "
+                 "T=300 K, AUSMPW+, Venkat, GG-cell, LU-SGS CFL 50; unseen flow M=0.3, Re=3e6"),
+        "sa_plate_200k": dict(
+            mesh=lambda: M.flat_plate(128, 96, 16, first_spacing=1e-5),
+            params=dict(cases.SA_PLATE),
+            wall_dist=True, iterations=5000, train_epochs=20, unseen=dict(cases.SA_PLATE_UNSEEN),
+            desc="SA flat plate 128x96x16 hex (197k cells), config-3 flow"),
         "laminar_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 128, 32),
             params=dict(cases.LAMINAR),
@@ -361,7 +375,7 @@ def converge(args, m, wd):
     wl = workloads()[args.workload]
     params = dict(wl["params"])
     sa = params.get("viscousType", 0) == 3
-    n = args.iterations
+    n = args.iterations or wl.get("iterations", 3000)
     nc = m.n_cell
     out = {"workload": args.workload, "cells": nc, "iterations": n}
 
@@ -387,8 +401,11 @@ def converge(args, m, wd):
                 caps.append(s.capture_sa_samples()[:2])
         h = np.concatenate(hist)
         f = s.AirForceCoef()
-        r = {"CL": f["CL"], "CD": f["CD"], "res_first": float(h[0]), "res_last": float(h[-1]),
-             "res_drop_orders": round(float(np.log10(h[0] / h[-1])), 3), "ms_per_iter": round(ms / n, 4),
+        # skin-friction drag: the viscous parts of the wall force sums, rotated as CD is
+        cdf = S.force_coefficients(np.where(np.arange(16) % 2 == 0, f["sums"], 0.0), s.params.attackd,
+                                   s.params.angleSlide)["CD"]
+        r = {"CL": f["CL"], "CD": f["CD"], "CD_friction": cdf, "res_max": float(np.max(h)), "res_last": float(h[-1]),
+             "res_drop_orders": round(float(np.log10(np.max(h) / h[-1])), 3), "ms_per_iter": round(ms / n, 4),
              "mcell_iters_per_s": round(nc * n / (ms / 1e3) / 1e6, 3)}
         if sa:
             r["vist"] = s.get(S.PHX_VIST)[:nc]
@@ -398,9 +415,10 @@ def converge(args, m, wd):
         if caps:
             f_, t_ = np.concatenate([c[0] for c in caps]), np.concatenate([c[1] for c in caps])
             f_, t_ = balanced_subsample(f_, t_, 2_000_000, seed=0)
+            epochs = wl.get("train_epochs", 60)
             t1 = time.perf_counter()
-            loss = s.train_sa_mlp(f_, t_, epochs=60, batch=8192, lr=1e-3, seed=0)
-            r["mlp"] = {"samples": int(len(t_)), "epochs": 60, "final_loss": loss,
+            loss = s.train_sa_mlp(f_, t_, epochs=epochs, batch=8192, lr=1e-3, seed=0)
+            r["mlp"] = {"samples": int(len(t_)), "epochs": epochs, "final_loss": loss,
                         "train_s": round(time.perf_counter() - t1, 2)}
             blob_out = s.mlp_blob()
         s.close()
@@ -411,39 +429,87 @@ def converge(args, m, wd):
     arms["mixed_exact"], _ = run("mixed")
     if sa:
         arms["mixed_learned"], _ = run("mixed", blob=blob)
-    for name, r in arms.items():
-        if name != "fp64":
-            r["dCL_vs_fp64"] = abs(r["CL"] - r64["CL"])
-            r["dCD_vs_fp64"] = abs(r["CD"] - r64["CD"])
+
+    def compare(arms, ref):
+        for name, r in arms.items():
+            if r is ref:
+                continue
+            r["dCL_vs_fp64"] = abs(r["CL"] - ref["CL"])
+            r["dCD_vs_fp64"] = abs(r["CD"] - ref["CD"])
+            r["dCDf_vs_fp64"] = abs(r["CD_friction"] - ref["CD_friction"])
             if sa:
-                r["dVIST_rel_vs_fp64"] = float(np.max(np.abs(r["vist"] - r64["vist"])) / np.max(np.abs(r64["vist"])))
-            r["speedup_vs_fp64"] = round(r["mcell_iters_per_s"] / r64["mcell_iters_per_s"], 3)
-    for r in arms.values():
-        r.pop("vist", None)
+                r["dVIST_rel_vs_fp64"] = float(np.max(np.abs(r["vist"] - ref["vist"])) / np.max(np.abs(ref["vist"])))
+            r["speedup_vs_fp64"] = round(r["mcell_iters_per_s"] / ref["mcell_iters_per_s"], 3)
+        for r in arms.values():
+            r.pop("vist", None)
+
+    compare(arms, r64)
     out["arms"] = arms
+    if sa and wl.get("unseen"):
+        # the learned source on a flow it was not trained on
+        params.clear()
+        params.update(wl["unseen"])
+        u64, _ = run("fp64")
+        unseen = {"fp64": u64}
+        unseen["mixed_learned"], _ = run("mixed", blob=blob)
+        compare(unseen, u64)
+        out["unseen"] = {"flow": {k: wl["unseen"][k] for k in ("refMachNumber", "refReNumber")}, "arms": unseen}
     return out
 
 
-def cpu_baseline(args, wl_name, sample_budget_s=20.0):
-    """The oracle (single-threaded CPU restatement of the reference path) on a
-    bounded sample of the workload: the same case kind at a size it finishes
-    in seconds, iterated until ~sample_budget_s."""
-    from oracle.oracle import Oracle
+def cpu_sample(wl_name):
+    """The mesh the CPU arms run on: the workload itself when it has about a
+    million cells or fewer, else a mesh of the same case kind with about one
+    million cells (the reference solves it at about a third of a million
+    cell-iterations per second on one core, so the full 16M-cell mesh would
+    take minutes per iteration), and a description of it."""
+    from phenlei_b200 import mesh as M
+
+    if wl_name == "transonic_bump_sa_16M":
+        return (M.channel_bump(256, 92, 32, thickness=0.08, length=3.0, wall_spacing=0.001, prism_layers=30),
+                "256x92x32 channel bump with 30 prism layers (999,424 cells): config 5's case kind and layer count")
+    if wl_name == "transonic_bump_euler_16M":
+        return (M.channel_bump(256, 92, 32, thickness=0.08, length=3.0, wall_spacing=0.001),
+                "256x92x32 hex channel bump (753,664 cells), the same case kind")
+    if wl_name == "sa_plate_3M":
+        return M.flat_plate(256, 96, 16), "256x96x16 flat plate (393,216 cells), the same case kind"
+    m = workloads()[wl_name]["mesh"]()
+    return m, "the workload's own mesh"
+
+
+def cpu_baseline(args, wl_name, budget_s=25.0):
+    """The reference's own CPU solver (oracle/_ref/ref_harness, built from its
+    sources: single zone, one core, its Controller relaxations) on a bounded
+    sample of the workload; the oracle port (single-threaded C restatement,
+    bit-exact with the reference) when the reference build is absent.  The
+    throughput is taken over the iteration loop alone."""
+    from oracle import refrun
     from phenlei_b200 import mesh as M
 
     wl = workloads()[wl_name]
-    m = (M.channel_bump(128, 46, 32, thickness=0.08, wall_spacing=0.001, prism_layers=15 if "sa" in wl_name else 0)
-         if "16M" in wl_name else wl["mesh"]())
-    o = Oracle(m, wl["params"], wall_dist=M.wall_distance(m) if wl.get("wall_dist") else None)
-    o.iterate(1)
-    n = 0
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < sample_budget_s:
+    m, what = cpu_sample(wl_name)
+    wd = M.wall_distance(m) if wl.get("wall_dist") else None
+    params = dict(wl["params"])
+    if refrun.available():
+        # about 0.35 Mcell-iterations/s: as many iterations as fit the budget, at least 2
+        n = int(max(2, min(args.steps, budget_s * 0.35e6 / m.n_cell)))
+        r = refrun.run_reference(m, params, n, wall_dist=wd)
+        sec = float(r["iter_seconds"][0])
+        kind, how = "reference", "the reference solver built from its own sources (oracle/_ref/ref_harness)"
+    else:
+        from oracle.oracle import Oracle
+
+        o = Oracle(m, params, wall_dist=wd)
         o.iterate(1)
-        n += 1
-    dt = time.perf_counter() - t0
-    return {"value": m.n_cell * n / dt / 1e6, "unit": "Mcell-iters/s", "cores": 1, "kind": "port",
-            "sample": f"{m.n_cell} cells of the same case kind, {n} iterations in {dt:.1f} s"}
+        n = int(max(2, min(args.steps, budget_s * 0.78e6 / m.n_cell)))
+        t0 = time.perf_counter()
+        o.iterate(n)
+        sec = time.perf_counter() - t0
+        kind, how = "port", "the oracle (single-threaded C restatement of the reference path)"
+    return {"value": round(m.n_cell * n / sec / 1e6, 4), "unit": "Mcell-iters/s", "cores": 1, "kind": kind,
+            "ms_per_step": round(sec / n * 1e3, 2), "iterations": n, "cells": m.n_cell,
+            "sample": f"{what}; {n} iterations in {sec:.1f} s by {how}; one zone on one core (the reference "
+                      "parallelises only across zones and MPI ranks)"}
 
 
 def main():
@@ -461,7 +527,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--converge", action="store_true",
                     help="run the configuration's full iteration count for every arm and report converged CL/CD")
-    ap.add_argument("--iterations", type=int, default=3000, help="iterations of a --converge run")
+    ap.add_argument("--iterations", type=int, default=0,
+                    help="iterations of a --converge run (default: the configuration's own count)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -472,9 +539,12 @@ def main():
             return
         cb = cpu_baseline(args, args.workload)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Mcell-iters/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "1 CPU core"},
+                "n_gpus": args.gpus, "steps": cb["iterations"], "warmup": 0, "ms_per_step": cb["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generated mesh, free-stream start)",
+                "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "1 CPU core",
+                           "same_config": cb["sample"].startswith("the workload's own mesh"),
+                           "sample": cb["sample"]},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-iters/s",
                                              "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -591,6 +661,18 @@ def main():
                 line["accuracy_vs_fp64"]["dVIST_rms_rel"] = float(np.sqrt(np.mean((r["vist"] - r64["vist"]) ** 2))
                                                                  / np.sqrt(np.mean(r64["vist"] ** 2)))
                 line["accuracy_vs_fp64"]["VIST_max_fp64"] = float(np.max(r64["vist"]))
+    if rx is not None and blob is not None:
+        # what the learned source buys against the exact source it replaces, on the same mixed path and steps
+        g = {"iteration_ms": {"learned": round(ms / args.steps, 4), "exact": round(rx["ms"] / args.steps, 4)},
+             "sa_residual_ms": {"learned": round(r["phase_ms"]["sa_residual"], 4),
+                                "exact": round(rx["phase_ms"]["sa_residual"], 4)},
+             "throughput_ratio_learned_over_exact": round(rx["ms"] / ms, 4)}
+        if r["forces"] and rx["forces"]:
+            g["dCL_vs_exact"] = abs(r["forces"]["CL"] - rx["forces"]["CL"])
+            g["dCD_vs_exact"] = abs(r["forces"]["CD"] - rx["forces"]["CD"])
+        if r["vist"] is not None and rx["vist"] is not None:
+            g["dVIST_rel_vs_exact"] = float(np.max(np.abs(r["vist"] - rx["vist"])) / np.max(np.abs(rx["vist"])))
+        line["mlp_gain"] = g
     line["config"]["sa_source"] = (("learned (MLP, exact outside its hull)" if blob is not None else "exact")
                                    if sa else None)
     if blob is not None:

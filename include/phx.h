@@ -235,6 +235,15 @@ int phx_mlp_train(phx_ctx *ctx, const float *features, const float *targets, int
 int phx_mlp_get(phx_ctx *ctx, float *blob, int64_t n);
 int phx_mlp_set(phx_ctx *ctx, const float *blob, int64_t n);
 int64_t phx_mlp_blob_size(void);
+/* One batch through the training kernels of phx_mlp_train, for checking them:
+ * params is the flat weight vector (w1 [64][6], b1 [64], w2 [64][64], b2, w3
+ * [64][64], b3, w4 [64], b4; phx_mlp_param_count() values, the first part of
+ * the model blob), x the standardised inputs [n][6], y the scaled targets [n];
+ * writes the mean squared error and its gradient with respect to params.  No
+ * counterpart in the reference (its SA source has no learned part). */
+int64_t phx_mlp_param_count(void);
+int phx_mlp_loss_grad(const float *params, int64_t nparam, const float *x, const float *y, int64_t n, float *grad,
+                      double *loss);
 int phx_mlp_cells(phx_ctx *ctx, uint64_t *count);
 
 /* nsteps outer iterations of the NS solver (and the SA solver when

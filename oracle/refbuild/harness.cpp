@@ -18,6 +18,7 @@
 //          for none
 //   name:rows:cols  grid data arrays to dump after the last step (rows=0 means
 //          a 1-D array of cols values)
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -326,7 +327,23 @@ int main(int argc, char **argv)
         if (viscousType != INVISCID)
         {
             AllocateWalldist();
-            ComputeWalldist();
+            // PHX_REF_WALLDIST names a file of nTotalCell doubles that replaces
+            // the reference's wall-distance search (its set-up cost grows with
+            // cells x wall faces); only the timing runs use it
+            const char *wdFile = getenv("PHX_REF_WALLDIST");
+            if (wdFile && *wdFile)
+            {
+                FILE *wf = fopen(wdFile, "rb");
+                if (!wf) Die("cannot open PHX_REF_WALLDIST");
+                RDouble *wd = grid->GetWallDist();
+                const size_t nread = fread(wd, sizeof(RDouble), grid->GetNTotalCell(), wf);
+                fclose(wf);
+                if ((int)nread != grid->GetNTotalCell()) Die("short PHX_REF_WALLDIST file");
+            }
+            else
+            {
+                ComputeWalldist();
+            }
         }
         if (viscousType > LAMINAR) WalldistStatics();
         int flowInitMethod = GlobalDataBase::GetIntParaFromDB("flowInitMethod");
@@ -391,6 +408,9 @@ int main(int argc, char **argv)
     // visual-file output of Simulation::PostSolve.
     int outIterStep = GlobalDataBase::GetIntParaFromDB("outnstep");
     std::vector<double> resHist;
+    // wall time of the iteration loop alone (set-up and output excluded): the
+    // reference's own throughput on this host, written to iter_seconds.bin
+    const auto loopStart = std::chrono::steady_clock::now();
     for (int step = 0; step < nSteps; ++step)
     {
         ++outIterStep;
@@ -424,6 +444,8 @@ int main(int argc, char **argv)
         for (int c = 0; c < nTotalCell; ++c) s += res[0][c] * res[0][c];
         resHist.push_back(sqrt(s / nTotalCell));
     }
+    const double loopSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - loopStart).count();
+    WriteRaw(outdir + "/iter_seconds.bin", &loopSeconds, 1);
     WriteRaw(outdir + "/res_hist.bin", resHist.data(), resHist.size());
 
     for (int a = 6; a < argc; ++a)

@@ -5,7 +5,8 @@ generate and check golden fixtures in the container that holds the
 reference sources; nothing on the product path imports it.
 
 Parameters are given as hypara key/value pairs on top of the reference's
-default parameter file (PHengLEI/examples/bin/cfd_para.hypara).
+default parameter file (PHengLEI/examples/bin/cfd_para.hypara in the reference
+project, staged as oracle/_ref/cfd_para.hypara by oracle/refbuild/Makefile).
 """
 from __future__ import annotations
 
@@ -17,8 +18,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "_ref", "ref_harness")
-REF_ROOT = os.environ.get("PHX_REFERENCE_ROOT", "/root/reference")
-DEFAULT_PARA = os.path.join(REF_ROOT, "PHengLEI", "examples", "bin", "cfd_para.hypara")
+# the reference's default parameter file, staged beside the harness by the build
+DEFAULT_PARA = os.path.join(HERE, "_ref", "cfd_para.hypara")
+
+
+def available() -> bool:
+    """True when the reference build (harness and its default parameter file) is present."""
+    return os.path.exists(HARNESS) and os.path.exists(DEFAULT_PARA)
 
 
 def _fmt(key, val):
@@ -41,19 +47,21 @@ BASE_PARAMS = {
 }
 
 
-def run_reference(mesh, params: dict, nsteps: int, dumps=(), state=None, workdir=None):
+def run_reference(mesh, params: dict, nsteps: int, dumps=(), state=None, workdir=None, wall_dist=None):
     """Run `nsteps` outer iterations of the reference solver.
 
     dumps: iterable of (name, rows, cols) grid arrays to return.
     state: optional primitive field [nEq, nCell] (plus turbulence rows) that
     replaces the reference's own initial field.
+    wall_dist: optional wall distance [nCell] that replaces the reference's
+    own wall-distance search (used by the timing runs, whose set-up it shortens).
     Returns a dict of numpy arrays (dumped arrays, geometry, residual history).
     """
     from phenlei_b200.mesh import write_mesh
 
-    if not os.path.exists(HARNESS):
-        raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle/refbuild harness)")
-    tmp = workdir or tempfile.mkdtemp(prefix="phx_ref_")
+    if not available():
+        raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle/refbuild REF=<root> all harness)")
+    tmp = os.path.abspath(workdir or tempfile.mkdtemp(prefix="phx_ref_"))
     os.makedirs(os.path.join(tmp, "bin"), exist_ok=True)
     os.makedirs(os.path.join(tmp, "grid"), exist_ok=True)
     os.makedirs(os.path.join(tmp, "results"), exist_ok=True)
@@ -78,7 +86,13 @@ def run_reference(mesh, params: dict, nsteps: int, dumps=(), state=None, workdir
         np.ascontiguousarray(state, dtype="<f8").tofile(spath)
     args = [HARNESS, mpath, tmp, os.path.join(tmp, "out"), str(nsteps), spath]
     args += [f"{n}:{r}:{c}" for (n, r, c) in dumps]
-    proc = subprocess.run(args, capture_output=True, text=True)
+    env = dict(os.environ)
+    env.pop("PHX_REF_WALLDIST", None)
+    if wall_dist is not None:
+        wpath = os.path.join(tmp, "grid", "walldist.bin")
+        np.ascontiguousarray(wall_dist, dtype="<f8").tofile(wpath)
+        env["PHX_REF_WALLDIST"] = wpath
+    proc = subprocess.run(args, capture_output=True, text=True, env=env)
     if proc.returncode != 0:
         raise RuntimeError(f"reference harness failed ({proc.returncode}):\n{proc.stdout[-4000:]}\n{proc.stderr[-4000:]}")
     out = {}

@@ -16,6 +16,9 @@
 #include "phx_mlp.h"
 
 namespace phx {
+int mlp_loss_grad(const float *params, const float *x, const float *y, int B, float *grad, double &lossOut,
+                  cudaStream_t s);
+int mlp_param_count();
 int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch, float lr, unsigned long long seed,
               MlpHostWeights &wts, float *mean, float *rstd, float *lo, float *hi, float *occ, float &tscale,
               double &lastLoss, cudaStream_t s);
@@ -1633,6 +1636,20 @@ int phx_mlp_set(phx_ctx *ctx, const float *blob, int64_t n)
 }
 
 int64_t phx_mlp_blob_size(void) { return kMlpBlobFloats; }
+
+int64_t phx_mlp_param_count(void) { return mlp_param_count(); }
+
+int phx_mlp_loss_grad(const float *params, int64_t nparam, const float *x, const float *y, int64_t n, float *grad,
+                      double *loss)
+{
+    if (!params || !x || !y || !grad || !loss || nparam != mlp_param_count() || n < 1 || n > (1 << 24))
+        return PHX_ERR_ARG;
+    double l = 0.0;
+    const int e = mlp_loss_grad(params, x, y, (int)n, grad, l, nullptr);
+    if (e) return PHX_ERR_CUDA;
+    *loss = l;
+    return PHX_OK;
+}
 
 int phx_mlp_cells(phx_ctx *ctx, uint64_t *count)
 {

@@ -473,8 +473,10 @@ __global__ void mlp_gather_kernel(int nb, const int *perm, int off, const float 
     y[b] = Y[r] * tinv;
 }
 
-// dy = 2 (y - t) / nb, and the summed squared error (for the loss).
-__global__ void mlp_loss_kernel(int nb, const float *y, const float *t, float *dy, float *loss)
+// dy = 2 (y - t) / nb, and the squared error summed per block into loss[blockIdx.x]
+// (fixed order: warp shuffles, then the block's warps in order; the host sums
+// the block partials in order, so the reported loss does not depend on timing).
+__global__ void __launch_bounds__(256) mlp_loss_kernel(int nb, const float *y, const float *t, float *dy, float *loss)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     float e = 0.0f;
@@ -484,7 +486,14 @@ __global__ void mlp_loss_kernel(int nb, const float *y, const float *t, float *d
         e = r * r;
     }
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, e);
+    __shared__ float part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float acc = 0.0f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) acc += part[i];
+        loss[blockIdx.x] += acc;
+    }
 }
 
 // Column sums of a [rows x cols] matrix (bias gradients).
@@ -558,6 +567,55 @@ float uniform(uint64_t &x) { return (float)((splitmix(x) >> 11) * (1.0 / 9007199
 
 }  // namespace
 
+// Flat parameter vector (w1 b1 w2 b2 w3 b3 w4 b4) and the activation buffers
+// of one batch of B rows.
+struct MlpBatch {
+    float *z1, *h1, *z2, *h2, *z3, *h3, *dh, *dz, *yp, *dy;
+};
+
+// Forward pass of one batch (x: standardised inputs [B][6], yt: scaled
+// targets [B]) and the gradient of the mean squared error into gp; the batch's
+// squared error is added to loss[0 .. ceil(B / 256)).
+void mlp_forward_backward(const float *p, float *gp, const float *x, const float *yt, int B, const MlpBatch &a,
+                          float *loss, cudaStream_t s)
+{
+    const int H = kMlpH;
+    // forward: z = a W^T + b (W row-major [out][in])
+    mlp_gemm(B, H, kMlpIn, x, kMlpIn, 1, p + kOffW1, 1, kMlpIn, a.z1, H, p + kOffB1, false, s);
+    mlp_silu((long long)B * H, a.z1, a.h1, nullptr, nullptr, s);
+    mlp_gemm(B, H, H, a.h1, H, 1, p + kOffW2, 1, H, a.z2, H, p + kOffB2, false, s);
+    mlp_silu((long long)B * H, a.z2, a.h2, nullptr, nullptr, s);
+    mlp_gemm(B, H, H, a.h2, H, 1, p + kOffW3, 1, H, a.z3, H, p + kOffB3, false, s);
+    mlp_silu((long long)B * H, a.z3, a.h3, nullptr, nullptr, s);
+    mlp_gemm(B, 1, H, a.h3, H, 1, p + kOffW4, 1, 1, a.yp, 1, p + kOffB4, false, s);
+    mlp_loss_kernel<<<(B + 255) / 256, 256, 0, s>>>(B, a.yp, yt, a.dy, loss);
+    // backward
+    mlp_gemm(1, H, B, a.dy, 1, 1, a.h3, H, 1, gp + kOffW4, H, nullptr, false, s);             // dW4 = dy^T h3
+    mlp_train_kernels_launch_silu_cols(B, 1, a.dy, gp + kOffB4, s);                           // db4
+    mlp_gemm(B, H, 1, a.dy, 1, 1, p + kOffW4, 1, 1, a.dh, H, nullptr, false, s);              // dH3 = dy w4
+    mlp_silu((long long)B * H, a.z3, nullptr, a.dh, a.dz, s);                                 // dZ3
+    mlp_gemm(H, H, B, a.dz, 1, H, a.h2, H, 1, gp + kOffW3, H, nullptr, false, s);             // dW3 = dZ3^T H2
+    mlp_train_kernels_launch_silu_cols(B, H, a.dz, gp + kOffB3, s);
+    mlp_gemm(B, H, H, a.dz, H, 1, p + kOffW3, H, 1, a.dh, H, nullptr, false, s);              // dH2 = dZ3 W3
+    mlp_silu((long long)B * H, a.z2, nullptr, a.dh, a.dz, s);
+    mlp_gemm(H, H, B, a.dz, 1, H, a.h1, H, 1, gp + kOffW2, H, nullptr, false, s);             // dW2
+    mlp_train_kernels_launch_silu_cols(B, H, a.dz, gp + kOffB2, s);
+    mlp_gemm(B, H, H, a.dz, H, 1, p + kOffW2, H, 1, a.dh, H, nullptr, false, s);              // dH1 = dZ2 W2
+    mlp_silu((long long)B * H, a.z1, nullptr, a.dh, a.dz, s);
+    mlp_gemm(H, kMlpIn, B, a.dz, 1, H, x, kMlpIn, 1, gp + kOffW1, kMlpIn, nullptr, false, s);  // dW1
+    mlp_train_kernels_launch_silu_cols(B, H, a.dz, gp + kOffB1, s);
+}
+
+// Device buffers of one batch of B rows (nullptr members if an allocation failed).
+static bool mlp_batch_alloc(DevBuf &db, int B, MlpBatch &a)
+{
+    const size_t bh = (size_t)B * kMlpH;
+    a.z1 = db.get<float>(bh); a.h1 = db.get<float>(bh); a.z2 = db.get<float>(bh); a.h2 = db.get<float>(bh);
+    a.z3 = db.get<float>(bh); a.h3 = db.get<float>(bh); a.dh = db.get<float>(bh); a.dz = db.get<float>(bh);
+    a.yp = db.get<float>(B); a.dy = db.get<float>(B);
+    return a.z1 && a.h1 && a.z2 && a.h2 && a.z3 && a.h3 && a.dh && a.dz && a.yp && a.dy;
+}
+
 // Trains the MLP on n samples (raw features [n][6], targets [n]) with Adam and
 // mean-squared error; returns the weights, the normalisation, the hull (box
 // and occupied bins), and the loss of the last epoch (normalised units).  0 on success, else a CUDA error.
@@ -605,14 +663,12 @@ int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch
     float *p = db.get<float>(kNParam), *gp = db.get<float>(kNParam), *m1 = db.get<float>(kNParam),
           *m2 = db.get<float>(kNParam);
     float *dmean = db.get<float>(kMlpIn), *drstd = db.get<float>(kMlpIn);
-    float *x = db.get<float>((size_t)B * kMlpIn), *yt = db.get<float>(B), *yp = db.get<float>(B), *dy = db.get<float>(B);
-    float *z1 = db.get<float>((size_t)B * kMlpH), *h1 = db.get<float>((size_t)B * kMlpH);
-    float *z2 = db.get<float>((size_t)B * kMlpH), *h2 = db.get<float>((size_t)B * kMlpH);
-    float *z3 = db.get<float>((size_t)B * kMlpH), *h3 = db.get<float>((size_t)B * kMlpH);
-    float *dh = db.get<float>((size_t)B * kMlpH), *dz = db.get<float>((size_t)B * kMlpH);
-    float *loss = db.get<float>(1);
-    if (!dX || !dY || !dperm || !p || !gp || !m1 || !m2 || !dmean || !drstd || !x || !yt || !yp || !dy || !z1 || !h1 ||
-        !z2 || !h2 || !z3 || !h3 || !dh || !dz || !loss)
+    float *x = db.get<float>((size_t)B * kMlpIn), *yt = db.get<float>(B);
+    const int nLoss = (B + 255) / 256;
+    float *loss = db.get<float>(nLoss);
+    MlpBatch act;
+    const bool actOk = mlp_batch_alloc(db, B, act);
+    if (!dX || !dY || !dperm || !p || !gp || !m1 || !m2 || !dmean || !drstd || !x || !yt || !loss || !actOk)
         return (int)cudaErrorMemoryAllocation;
     cudaMemcpyAsync(dX, X, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dY, Y, sizeof(float) * n, cudaMemcpyHostToDevice, s);
@@ -624,47 +680,26 @@ int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch
     std::vector<int> perm(n);
     for (long long i = 0; i < n; ++i) perm[i] = (int)i;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    long long stepCount = 0;
     const int H = kMlpH;
+    long long stepCount = 0;
+    std::vector<float> lossHost(nLoss);
     for (int ep = 0; ep < epochs; ++ep) {
         for (long long i = n - 1; i > 0; --i) std::swap(perm[i], perm[splitmix(rs) % (uint64_t)(i + 1)]);
         cudaMemcpyAsync(dperm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s);
-        cudaMemsetAsync(loss, 0, sizeof(float), s);
+        cudaMemsetAsync(loss, 0, sizeof(float) * nLoss, s);
         for (long long off = 0; off + B <= n; off += B) {
             mlp_gather_kernel<<<(B + 255) / 256, 256, 0, s>>>(B, dperm, (int)off, dX, dY, x, yt, dmean, drstd,
                                                               1.0f / tscale);
-            // forward: z = a W^T + b (W row-major [out][in])
-            mlp_gemm(B, H, kMlpIn, x, kMlpIn, 1, p + kOffW1, 1, kMlpIn, z1, H, p + kOffB1, false, s);
-            mlp_silu((long long)B * H, z1, h1, nullptr, nullptr, s);
-            mlp_gemm(B, H, H, h1, H, 1, p + kOffW2, 1, H, z2, H, p + kOffB2, false, s);
-            mlp_silu((long long)B * H, z2, h2, nullptr, nullptr, s);
-            mlp_gemm(B, H, H, h2, H, 1, p + kOffW3, 1, H, z3, H, p + kOffB3, false, s);
-            mlp_silu((long long)B * H, z3, h3, nullptr, nullptr, s);
-            mlp_gemm(B, 1, H, h3, H, 1, p + kOffW4, 1, 1, yp, 1, p + kOffB4, false, s);
-            mlp_loss_kernel<<<(B + 255) / 256, 256, 0, s>>>(B, yp, yt, dy, loss);
-            // backward
-            mlp_gemm(1, H, B, dy, 1, 1, h3, H, 1, gp + kOffW4, H, nullptr, false, s);           // dW4 = dy^T h3
-            mlp_train_kernels_launch_silu_cols(B, 1, dy, gp + kOffB4, s);                      // db4
-            mlp_gemm(B, H, 1, dy, 1, 1, p + kOffW4, 1, 1, dh, H, nullptr, false, s);            // dH3 = dy w4
-            mlp_silu((long long)B * H, z3, nullptr, dh, dz, s);                                 // dZ3
-            mlp_gemm(H, H, B, dz, 1, H, h2, H, 1, gp + kOffW3, H, nullptr, false, s);           // dW3 = dZ3^T H2
-            mlp_train_kernels_launch_silu_cols(B, H, dz, gp + kOffB3, s);
-            mlp_gemm(B, H, H, dz, H, 1, p + kOffW3, H, 1, dh, H, nullptr, false, s);            // dH2 = dZ3 W3
-            mlp_silu((long long)B * H, z2, nullptr, dh, dz, s);
-            mlp_gemm(H, H, B, dz, 1, H, h1, H, 1, gp + kOffW2, H, nullptr, false, s);           // dW2
-            mlp_train_kernels_launch_silu_cols(B, H, dz, gp + kOffB2, s);
-            mlp_gemm(B, H, H, dz, H, 1, p + kOffW2, H, 1, dh, H, nullptr, false, s);            // dH1 = dZ2 W2
-            mlp_silu((long long)B * H, z1, nullptr, dh, dz, s);
-            mlp_gemm(H, kMlpIn, B, dz, 1, H, x, kMlpIn, 1, gp + kOffW1, kMlpIn, nullptr, false, s);  // dW1
-            mlp_train_kernels_launch_silu_cols(B, H, dz, gp + kOffB1, s);
+            mlp_forward_backward(p, gp, x, yt, B, act, loss, s);
             ++stepCount;
             const float c1 = 1.0f - std::pow(b1, (float)stepCount), c2 = 1.0f - std::pow(b2, (float)stepCount);
             mlp_adam_kernel<<<(kNParam + 255) / 256, 256, 0, s>>>(kNParam, p, gp, m1, m2, lr, b1, b2, eps, c1, c2);
         }
-        float lh = 0.0f;
-        cudaMemcpyAsync(&lh, loss, sizeof(float), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(lossHost.data(), loss, sizeof(float) * nLoss, cudaMemcpyDeviceToHost, s);
         cudaStreamSynchronize(s);
-        lastLoss = (double)lh / (double)((n / B) * B);
+        double lh = 0.0;
+        for (int i = 0; i < nLoss; ++i) lh += lossHost[i];
+        lastLoss = lh / (double)((n / B) * B);
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
@@ -680,6 +715,38 @@ int mlp_train(const float *X, const float *Y, long long n, int epochs, int batch
     wts.b4 = prm[kOffB4];
     return 0;
 }
+
+// Mean squared error of one batch and its gradient with respect to the flat
+// parameter vector, by the training kernels above (x: standardised inputs,
+// y: scaled targets).  0 on success, else a CUDA error.
+int mlp_loss_grad(const float *params, const float *x, const float *y, int B, float *grad, double &lossOut,
+                  cudaStream_t s)
+{
+    if (B < 1) return -1;
+    DevBuf db;
+    const int nLoss = (B + 255) / 256;
+    float *p = db.get<float>(kNParam), *gp = db.get<float>(kNParam), *dx = db.get<float>((size_t)B * kMlpIn),
+          *dy = db.get<float>(B), *loss = db.get<float>(nLoss);
+    MlpBatch act;
+    if (!mlp_batch_alloc(db, B, act) || !p || !gp || !dx || !dy || !loss) return (int)cudaErrorMemoryAllocation;
+    cudaMemcpyAsync(p, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dx, x, sizeof(float) * B * kMlpIn, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dy, y, sizeof(float) * B, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(loss, 0, sizeof(float) * nLoss, s);
+    mlp_forward_backward(p, gp, dx, dy, B, act, loss, s);
+    std::vector<float> lh(nLoss);
+    cudaMemcpyAsync(grad, gp, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(lh.data(), loss, sizeof(float) * nLoss, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return (int)cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    double acc = 0.0;
+    for (int i = 0; i < nLoss; ++i) acc += lh[i];
+    lossOut = acc / B;
+    return 0;
+}
+
+int mlp_param_count() { return kNParam; }
 
 // Byte offset of element (n, k) of a K-major core-matrix tile with `kchunks`
 // 8-element K chunks.

@@ -93,6 +93,9 @@ def lib() -> C.CDLL:
         _lib.phx_mlp_set.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         _lib.phx_mlp_blob_size.restype = C.c_int64
         _lib.phx_mlp_cells.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        _lib.phx_mlp_param_count.restype = C.c_int64
+        _lib.phx_mlp_loss_grad.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                           C.POINTER(C.c_double)]
         _lib.phx_set_wait_limit.argtypes = [C.c_void_p, C.c_int64]
         _lib.phx_fault_hold_cell.argtypes = [C.c_void_p, C.c_int32]
     return _lib
@@ -276,7 +279,10 @@ class NSSolverUnstruct:
         self._check(lib().phx_sa_capture(self.h, f.ctypes.data, t.ctypes.data, cells.ctypes.data, sc.ctypes.data,
                                          nc, C.byref(n)), "phx_sa_capture")
         k = n.value
-        return f[:k].copy(), t[:k].copy(), cells[:k].copy(), sc[:k].copy()
+        # the device fills the arrays in the order its threads finish: sort by
+        # cell so that a capture (and a model trained on it) is reproducible
+        o = np.argsort(cells[:k], kind="stable")
+        return f[:k][o], t[:k][o], cells[:k][o], sc[:k][o]
 
     def train_sa_mlp(self, features, targets, epochs=20, batch=8192, lr=1e-3, seed=0) -> float:
         f = np.ascontiguousarray(features, np.float32)
@@ -332,3 +338,19 @@ def force_coefficients(sums, attackd: float = 0.0, angleSlide: float = 0.0, refe
     cl = -math.sin(a) * cf[0] + math.cos(a) * cf[1]
     cd = math.cos(a) * math.cos(b) * cf[0] + math.sin(a) * math.cos(b) * cf[1] + math.sin(b) * cf[2]
     return {"sums": out, "CL": cl, "CD": cd}
+
+
+def mlp_loss_grad(params, x, y):
+    """Mean squared error of one batch and its gradient with respect to the flat
+    weight vector, computed by the library's training kernels (see
+    phx_mlp_loss_grad)."""
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    yy = np.ascontiguousarray(y, np.float32)
+    g = np.empty_like(p)
+    loss = C.c_double()
+    rc = lib().phx_mlp_loss_grad(p.ctypes.data, p.size, xx.ctypes.data, yy.ctypes.data, yy.size, g.ctypes.data,
+                                 C.byref(loss))
+    if rc != 0:
+        raise PhxError(f"phx_mlp_loss_grad: {ERRORS.get(rc, rc)}")
+    return loss.value, g

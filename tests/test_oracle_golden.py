@@ -67,7 +67,8 @@ def test_oracle_matches_reference_laminar(golden, name):
 
 
 @pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_16x8x2_step30",
-                                  "sa_bump_prism_16x8x2_step2", "sa_bump_16x8x2_init2_step3"])
+                                  "sa_bump_prism_16x8x2_step2", "sa_bump_16x8x2_init2_step3",
+                                  "sa_plate_16x8x2_ausmpwp_step2", "sa_plate_16x8x2_ausmpwp_step20"])
 def test_oracle_matches_reference_sa(golden, name):
     """Spalart-Allmaras (NSMB formation) coupled to the NS step: boundary
     values, eddy viscosity, source (negative-nu~ branch included), upwind

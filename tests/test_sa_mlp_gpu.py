@@ -205,3 +205,89 @@ def test_learned_source_from_free_stream(precision):
     assert np.all(np.isfinite(qm))
     assert rel_err(qm, qe) <= 5e-2
     assert ml.mlp_cells() > nc
+
+
+def _silu64(z):
+    return z / (1.0 + np.exp(-z))
+
+
+def _dsilu64(z):
+    sg = 1.0 / (1.0 + np.exp(-z))
+    return sg * (1.0 + z * (1.0 - sg))
+
+
+def numpy_loss_grad(params, x, y):
+    """Float64 forward and backward pass of the 6-64-64-64-1 SiLU network with
+    the mean squared error, by hand: the CPU check of the training kernels."""
+    p = np.asarray(params, np.float64)
+    o = [0]
+
+    def take(n, shape=None):
+        v = p[o[0]:o[0] + n]
+        o[0] += n
+        return v.reshape(shape) if shape else v
+
+    w1, b1 = take(H * 6, (H, 6)), take(H)
+    w2, b2 = take(H * H, (H, H)), take(H)
+    w3, b3 = take(H * H, (H, H)), take(H)
+    w4, b4 = take(H), take(1)
+    x = np.asarray(x, np.float64)
+    t = np.asarray(y, np.float64)
+    z1 = x @ w1.T + b1
+    h1 = _silu64(z1)
+    z2 = h1 @ w2.T + b2
+    h2 = _silu64(z2)
+    z3 = h2 @ w3.T + b3
+    h3 = _silu64(z3)
+    out = h3 @ w4 + b4
+    n = len(t)
+    loss = np.mean((out - t) ** 2)
+    dy = 2.0 * (out - t) / n
+    g = {"w4": dy @ h3, "b4": np.array([dy.sum()])}
+    dz3 = np.outer(dy, w4) * _dsilu64(z3)
+    g["w3"], g["b3"] = dz3.T @ h2, dz3.sum(0)
+    dz2 = (dz3 @ w3) * _dsilu64(z2)
+    g["w2"], g["b2"] = dz2.T @ h1, dz2.sum(0)
+    dz1 = (dz2 @ w2) * _dsilu64(z1)
+    g["w1"], g["b1"] = dz1.T @ x, dz1.sum(0)
+    return loss, g
+
+
+def test_training_gradients_match_numpy_float64():
+    """The hand-written training kernels (strided GEMMs, SiLU and its
+    derivative, column sums) against a float64 NumPy backward pass: dW and db
+    of all four layers for a fixed seeded model and batch, 1e-4 relative
+    (norm-wise per array; the kernels run in FP32)."""
+    rng = np.random.default_rng(7)
+    n_par = int(S.lib().phx_mlp_param_count())
+    shapes = [("w1", H * 6), ("b1", H), ("w2", H * H), ("b2", H), ("w3", H * H), ("b3", H), ("w4", H), ("b4", 1)]
+    assert sum(n for _, n in shapes) == n_par
+    fan = {"w1": 6, "w2": H, "w3": H, "w4": H}
+    params = np.concatenate([rng.standard_normal(n) / np.sqrt(fan.get(k, 10.0)) for k, n in shapes]).astype(np.float32)
+    B = 1000   # not a multiple of the 16-row tiles or the 256-thread blocks
+    x = rng.standard_normal((B, 6)).astype(np.float32)
+    y = rng.standard_normal(B).astype(np.float32)
+    loss, grad = S.mlp_loss_grad(params, x, y)
+    lref, gref = numpy_loss_grad(params, x, y)
+    assert abs(loss - lref) <= 1e-5 * lref
+    off = 0
+    for k, n in shapes:
+        assert rel_err(grad[off:off + n], gref[k].ravel()) <= 1e-4, k
+        off += n
+
+
+def test_training_is_deterministic():
+    """Two trainings on the same captured samples with the same seed give the
+    same model bit for bit (fixed-order reductions; the capture is sorted by
+    cell)."""
+    m = M.channel_bump(32, 16, 4)
+    wd = M.wall_distance(m)
+    blobs, losses = [], []
+    for _ in range(2):
+        a = S.NSSolverUnstruct(m, wall_dist=wd, **SA)
+        a.Relaxation(3)
+        f, t, _, _ = a.capture_sa_samples()
+        losses.append(a.train_sa_mlp(f, t, epochs=5, batch=512, lr=2e-3, seed=4))
+        blobs.append(a.mlp_blob())
+    assert losses[0] == losses[1]
+    assert np.array_equal(blobs[0], blobs[1])

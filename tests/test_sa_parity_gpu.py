@@ -31,7 +31,8 @@ def _solver(m, params, wall_dist, precision="fp64"):
     return S.NSSolverUnstruct(m, precision=precision, wall_dist=wall_dist, **params)
 
 
-@pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_prism_16x8x2_step2"])
+@pytest.mark.parametrize("name", ["sa_bump_16x8x2_step1", "sa_bump_16x8x2_lsq_step3", "sa_bump_prism_16x8x2_step2",
+                                  "sa_plate_16x8x2_ausmpwp_step2"])
 def test_fp64_sa_matches_reference_golden(golden, name):
     d = golden(name)
     m = d["mesh_obj"]
@@ -50,8 +51,9 @@ def test_fp64_sa_matches_reference_golden(golden, name):
     assert rel_err(s.AirForceCoef()["sums"], d["forces"]) <= FP64_TOL
 
 
-def test_fp64_sa_history_matches_reference_golden(golden):
-    d = golden("sa_bump_16x8x2_step30")
+@pytest.mark.parametrize("name", ["sa_bump_16x8x2_step30", "sa_plate_16x8x2_ausmpwp_step20"])
+def test_fp64_sa_history_matches_reference_golden(golden, name):
+    d = golden(name)
     m = d["mesh_obj"]
     nc = m.n_cell
     s = _solver(m, d["params_dict"], d["walldist"])
@@ -154,3 +156,26 @@ def test_sa_requires_wall_distance():
     m = M.channel_bump(16, 8, 2)
     with pytest.raises(S.PhxError):
         S.NSSolverUnstruct(m, **SA)
+
+
+@pytest.mark.parametrize("precision,tol,turb_tol", [("fp64", FP64_TOL, FP64_TOL), ("mixed", MIXED_TOL, MIXED_TURB_TOL)])
+def test_plate_vs_oracle(precision, tol, turb_tol):
+    """Config-3 flow (SA, AUSMPW+, M 0.2, Re 5e6, CFL 50) on a 32x12x2 flat
+    plate, perturbed flow and nu~: one iteration, then 30 more."""
+    m = M.flat_plate(32, 12, 2, first_spacing=1e-4)
+    wd = M.wall_distance(m)
+    params = cases.SA_PLATE
+    o, q0, qt0 = _oracle(m, params, wd, seed=13)
+    s = _solver(m, params, wd, precision)
+    s.set_q_cells(q0)
+    s.set_qt_cells(qt0)
+    nc = m.n_cell
+    o.iterate(1)
+    s.Relaxation(1)
+    assert rel_err(s.get(S.PHX_RES)[:, :nc], o.work("res")[:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_Q)[:, :nc], o.q[:, :nc]) <= tol
+    assert rel_err(s.get(S.PHX_Q_TURB)[:nc], o.work("qt")[:nc]) <= turb_tol
+    ho = o.iterate(30)
+    hs = s.Relaxation(30)
+    assert rel_err(hs, ho) <= (1e-10 if precision == "fp64" else 1e-3)
+    assert rel_err(s.AirForceCoef()["sums"], o.forces()) <= (1e-10 if precision == "fp64" else 1e-3)
