@@ -59,7 +59,7 @@ struct phx_ctx {
     bool mlpReady = false;
     MlpDev mlp{};
     std::vector<float> mlpBlob;
-    __nv_bfloat16 *mlpW = nullptr;          // w1c | w2c | w3c
+    uint16_t *mlpW = nullptr;               // w1c | w2c | w3c (FP16 words)
     float *mlpF = nullptr;                  // b1 | b2 | b3 | w4
     uint8_t *mlpOcc = nullptr;              // occupied hull bins
     unsigned long long *nmlp = nullptr;     // cells that used the learned source (running count)

@@ -49,6 +49,7 @@ constexpr int kSweepLanes = 4;   // LU-SGS lanes (neighbour entries) per schedul
 constexpr int kSweepSlots = 8;   // slots per warp: schedule levels are padded to this multiple
 constexpr int kSweepMaxEntries = 2 * kSweepLanes;   // entries of a cell: one slot, or two adjacent slots
 constexpr long long kDefaultSpinLimit = 20000000LL;   // polls per dependency wait (~1-2 s)
+constexpr int kMaxDevices = 64;                       // per-device launch caches
 // Spalart-Allmaras records
 constexpr int kTr = 4;     // trec: nu~ | eddy viscosity | laminar viscosity of the NS step | pad
 constexpr int kTg = 4;     // tgrad: d nu~ / dx, dy, dz | pad

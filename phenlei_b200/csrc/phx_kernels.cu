@@ -1113,8 +1113,17 @@ static int sweep_blocks(K kernel, int &perSM, const DevGrid &g, int numSMs)
 template <class T>
 int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s)
 {
-    static int perSMcache[2] = {-1, -1};
-    const int blocks = sweep_blocks(lusgs_kernel<T>, perSMcache[sizeof(T) == 8 ? 0 : 1], g, numSMs);
+    // residency of the cooperative launch, per device (a process may drive several)
+    static int perSMcache[kMaxDevices][2];
+    static bool init = false;
+    if (!init) {
+        for (auto &d : perSMcache) d[0] = d[1] = -1;
+        init = true;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+    const int blocks = sweep_blocks(lusgs_kernel<T>, perSMcache[dev][sizeof(T) == 8 ? 0 : 1], g, numSMs);
     const long long quads = (long long)g.nCell * kD / 4;
     const int rb = (int)std::min<long long>((quads + kThreads - 1) / kThreads, (long long)numSMs * 16);
     sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, w.dqfwd, w.dflux, w.dqrec);

@@ -4,7 +4,7 @@
 // the exact source is used outside it and for nu~ <= 0.
 //
 // Inference runs on the 5th-generation tensor cores: per CTA a tile of 128
-// cells, BF16 operands in shared memory (canonical K-major layout, no
+// cells, FP16 operands in shared memory (canonical K-major layout, no
 // swizzle), FP32 accumulators in tensor memory (TMEM), tcgen05.mma issued by
 // one thread and completed through an mbarrier, results read back with
 // tcgen05.ld.  The last layer (64 -> 1) is a dot product on the CUDA cores.
@@ -48,15 +48,15 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
-// Instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
-// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N)
+// Instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B FP16
+// (bits 7-9 = 0, 10-12 = 0), both K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate)
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -124,10 +124,9 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v)
 
 // SiLU of a pair, x sigma(x) = x/2 + (x/2) tanh(x/2), with one
 // tanh.approx.f16x2 for both values: one special-function operation per two
-// activations instead of an exponential and a reciprocal per activation (the
-// special-function unit bounds this kernel).  The half-precision tanh of
-// x/2 (relative error ~2^-11) is below the BF16 rounding the activations get
-// next.
+// activations instead of an exponential and a reciprocal per activation.  The
+// last hidden layer uses it in FP32 (its outputs go to the CUDA-core dot
+// product); the half-precision tanh of x/2 has a relative error of ~2^-11.
 __device__ __forceinline__ void silu2(float &a, float &b)
 {
     const float ha = 0.5f * a, hb = 0.5f * b;
@@ -200,33 +199,61 @@ __device__ __forceinline__ void sa_cell_inputs(const DevGrid &g, const Work<T> &
 // ---------------------------------------------------------------------------
 // Inference: source of every cell into t.tsrc (the SA cell pass reads it).
 // One CTA = 128 threads = one row of the 128-cell tile each; persistent over
-// tiles.  Shared memory: W1 | W2 | W3 | A1 (128 x 16) | ACT (128 x 64) | mbarrier, TMEM address.
+// tiles.  Shared memory: W1 | W2 | W3 | A1 (128 x 16) | ACT (128 x 64) | b1, b2
+// in half precision | mbarrier, TMEM address.  Operands are FP16: the input
+// row, the weights, and the hidden activations, which the half-precision
+// epilogue writes as they are.
 // ---------------------------------------------------------------------------
 static constexpr int kMlpSmemW1 = 0;
 static constexpr int kMlpSmemW2 = kMlpSmemW1 + kMlpH * kMlpK1 * 2;
 static constexpr int kMlpSmemW3 = kMlpSmemW2 + kMlpH * kMlpH * 2;
 static constexpr int kMlpSmemA1 = kMlpSmemW3 + kMlpH * kMlpH * 2;
 static constexpr int kMlpSmemAct = kMlpSmemA1 + kMlpTile * kMlpK1 * 2;
-static constexpr int kMlpSmemBar = kMlpSmemAct + kMlpTile * kMlpH * 2;
+static constexpr int kMlpSmemBias = kMlpSmemAct + kMlpTile * kMlpH * 2;   // b1, b2 as half2 pairs
+static constexpr int kMlpSmemBar = kMlpSmemBias + 2 * kMlpH * 2;
 static constexpr int kMlpSmemBytes = kMlpSmemBar + 16;
 static constexpr uint32_t kMlpTmemCols = 64;
 
-// Row r of a K-major tile with `kchunks` 8-element K chunks (sbo = kchunks * 128).
-__device__ __forceinline__ void store_row_bf16(unsigned char *base, int r, int kchunks, const float *v)
+// Row r of a K-major FP16 tile with `kchunks` 8-element K chunks (sbo = kchunks * 128),
+// from FP32 values or from packed pairs.
+__device__ __forceinline__ void store_row_f16(unsigned char *base, int r, int kchunks, const float *v)
 {
     unsigned char *row = base + (r >> 3) * (kchunks * 128) + (r & 7) * 16;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         if (c >= kchunks) break;
-        __nv_bfloat162 p[4];
+        __half2 p[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
+        for (int i = 0; i < 4; ++i) p[i] = __floats2half2_rn(v[8 * c + 2 * i], v[8 * c + 2 * i + 1]);
         *reinterpret_cast<uint4 *>(row + c * 128) = *reinterpret_cast<uint4 *>(p);
+    }
+}
+__device__ __forceinline__ void store_row_h2(unsigned char *base, int r, const __half2 *v)
+{
+    unsigned char *row = base + (r >> 3) * ((kMlpH / 8) * 128) + (r & 7) * 16;
+#pragma unroll
+    for (int c = 0; c < kMlpH / 8; ++c) *reinterpret_cast<uint4 *>(row + c * 128) = *reinterpret_cast<const uint4 *>(v + 4 * c);
+}
+
+// Bias and SiLU of a hidden layer whose output feeds the next MMA, in half
+// precision: per pair of FP32 accumulators one pack, then the bias, x/2,
+// tanh(x/2) (one tanh.approx.f16x2) and x/2 + (x/2) tanh(x/2) in half2
+// arithmetic, so the result is the next layer's FP16 operand as it stands.
+__device__ __forceinline__ void bias_silu_h2(const float *acc, const __half2 *bias2, __half2 *out)
+{
+    const __half2 half = __float2half2_rn(0.5f);
+#pragma unroll
+    for (int k = 0; k < kMlpH / 2; ++k) {
+        const __half2 x = __hadd2(__floats2half2_rn(acc[2 * k], acc[2 * k + 1]), bias2[k]);
+        const __half2 hx = __hmul2(x, half);
+        uint32_t t;
+        asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&hx)));
+        out[k] = __hfma2(hx, *reinterpret_cast<const __half2 *>(&t), hx);
     }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst c, Work<T> w, TurbWork<T> t,
+__global__ void __launch_bounds__(kMlpTile, 5) mlp_source_kernel(DevGrid g, NsConst c, Work<T> w, TurbWork<T> t,
                                                                MlpDev mlp, Reduce *red, unsigned long long *nmlp)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -243,6 +270,12 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
         uint4 *d3 = reinterpret_cast<uint4 *>(sm + kMlpSmemW3);
         for (int i = tid; i < kMlpH * kMlpK1 * 2 / 16; i += blockDim.x) d1[i] = s1[i];
         for (int i = tid; i < kMlpH * kMlpH * 2 / 16; i += blockDim.x) { d2[i] = s2[i]; d3[i] = s3[i]; }
+        __half2 *bh = reinterpret_cast<__half2 *>(sm + kMlpSmemBias);
+        if (tid < kMlpH) {
+            const float *b = tid < kMlpH / 2 ? mlp.b1 : mlp.b2;
+            const int k = 2 * (tid % (kMlpH / 2));
+            bh[tid] = __floats2half2_rn(__ldg(b + k), __ldg(b + k + 1));
+        }
     }
     if (tid == 0) {
         mbar_init(mbar, 1);
@@ -259,7 +292,7 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);   // this warp's 32 lanes
-    const uint32_t idesc = umma_idesc_bf16(kMlpTile, kMlpH);
+    const uint32_t idesc = umma_idesc_f16(kMlpTile, kMlpH);
     const uint32_t sW1 = smem_u32(sm + kMlpSmemW1), sW2 = smem_u32(sm + kMlpSmemW2), sW3 = smem_u32(sm + kMlpSmemW3);
     const uint32_t sA1 = smem_u32(sm + kMlpSmemA1), sAct = smem_u32(sm + kMlpSmemAct);
     uint32_t phase = 0;
@@ -293,14 +326,25 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
                                    mlp_bin(f[1], mlp.lo[1], mlp.hi[1])) != 0;
             }
         }
-        store_row_bf16(sm + kMlpSmemA1, tid, kMlpK1 / 8, x);
+        // the next tile's cell records into L2 while this tile's MMAs run
+        {
+            const int nxt = cell + gridDim.x * kMlpTile;
+            if (nxt < g.nCell) {
+                prefetch_l2(w.grec + (size_t)nxt * kG);
+                prefetch_l2(w.grec + (size_t)nxt * kG + 8);
+                prefetch_l2(w.trec + (size_t)nxt * kTr);
+                prefetch_l2(w.qrec + (size_t)nxt * kQ);
+                prefetch_l2(g.walldist + nxt);
+            }
+        }
+        store_row_f16(sm + kMlpSmemA1, tid, kMlpK1 / 8, x);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
         // layer 1: [128 x 16] x [16 x 64]
         if (tid == 0) {
-            umma_bf16(tmem, umma_desc(sA1, 128, 256), umma_desc(sW1, 128, 256), idesc, 0u);
+            umma_f16(tmem, umma_desc(sA1, 128, 256), umma_desc(sW1, 128, 256), idesc, 0u);
             umma_commit(mbar);
         }
         float h[kMlpH];
@@ -311,15 +355,19 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
             phase ^= 1u;
             tc_fence_after();
             tmem_ld64(taddr, h);
-            const float *b = layer == 0 ? mlp.b1 : (layer == 1 ? mlp.b2 : mlp.b3);
+            if (layer == 2) {
+                // the last hidden layer feeds the CUDA-core dot product: FP32
 #pragma unroll
-            for (int k = 0; k < kMlpH; k += 2) {
-                h[k] += __ldg(b + k);
-                h[k + 1] += __ldg(b + k + 1);
-                silu2(h[k], h[k + 1]);
+                for (int k = 0; k < kMlpH; k += 2) {
+                    h[k] += __ldg(mlp.b3 + k);
+                    h[k + 1] += __ldg(mlp.b3 + k + 1);
+                    silu2(h[k], h[k + 1]);
+                }
+                break;
             }
-            if (layer == 2) break;
-            store_row_bf16(sm + kMlpSmemAct, tid, kMlpH / 8, h);
+            __half2 a2[kMlpH / 2];
+            bias_silu_h2(h, reinterpret_cast<const __half2 *>(sm + kMlpSmemBias) + layer * (kMlpH / 2), a2);
+            store_row_h2(sm + kMlpSmemAct, tid, a2);
             fence_async_smem();
             tc_fence_before();
             __syncthreads();
@@ -328,7 +376,7 @@ __global__ void __launch_bounds__(kMlpTile) mlp_source_kernel(DevGrid g, NsConst
                 const uint32_t sW = layer == 0 ? sW2 : sW3;
 #pragma unroll
                 for (int kk = 0; kk < kMlpH / 16; ++kk)
-                    umma_bf16(tmem, umma_desc(sAct + kk * 256, 128, 1024), umma_desc(sW + kk * 256, 128, 1024), idesc,
+                    umma_f16(tmem, umma_desc(sAct + kk * 256, 128, 1024), umma_desc(sW + kk * 256, 128, 1024), idesc,
                               kk > 0 ? 1u : 0u);
                 umma_commit(mbar);
             }
@@ -360,15 +408,13 @@ template <class T>
 void launch_mlp_source(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t,
                        const MlpDev &mlp, Reduce *red, unsigned long long *nmlp, int numSMs, cudaStream_t s)
 {
-    static bool attr[2] = {false, false};
-    bool &a = attr[sizeof(T) == 8 ? 0 : 1];
-    if (!a) {
-        cudaFuncSetAttribute(mlp_source_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmemBytes);
-        a = true;
-    }
+    // the attribute is per device: set on the current one at every launch
+    // (microseconds)
+    cudaFuncSetAttribute(mlp_source_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmemBytes);
     const int ntiles = (g.nCell + kMlpTile - 1) / kMlpTile;
-    // 5 CTAs per SM: 5 x 64 of the 512 TMEM columns, 5 x 39 KB shared memory,
-    // 5 x 128 threads x 96 registers
+    // persistent CTAs, every one resident: 5 per SM use 5 x 64 of the 512 TMEM
+    // columns, 5 x 39 KB shared memory and 5 x 128 threads x at most 102
+    // registers (the kernel's launch bounds)
     int blocks = numSMs * 5;
     if (blocks > ntiles) blocks = ntiles;
     if (blocks < 1) blocks = 1;
@@ -755,12 +801,12 @@ static size_t core_offset(int n, int k, int kchunks)
     return (size_t)(n >> 3) * (kchunks * 128) + (size_t)(k >> 3) * 128 + (size_t)(n & 7) * 16 + (size_t)(k & 7) * 2;
 }
 
-// BF16 weights in the MMA layout (w1: 64 x 16 with K 6..15 zero; w2, w3: 64 x 64).
+// FP16 weights in the MMA layout (w1: 64 x 16 with K 6..15 zero; w2, w3: 64 x 64).
 void mlp_pack(const MlpHostWeights &w, std::vector<uint16_t> &w1c, std::vector<uint16_t> &w2c,
               std::vector<uint16_t> &w3c)
 {
     auto bf = [](float f) {
-        const __nv_bfloat16 b = __float2bfloat16_rn(f);
+        const __half b = __float2half_rn(f);
         uint16_t u;
         std::memcpy(&u, &b, 2);
         return u;

@@ -20,14 +20,14 @@ __host__ __device__ inline int mlp_bin(float v, float lo, float hi)
     return t >= (float)(kMlpGrid - 1) ? kMlpGrid - 1 : (int)t;
 }
 
-// Weights in the canonical K-major core-matrix layout the MMA reads
-// (byte offset of (n, k) = (n / 8) * sbo + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2,
-// sbo = 256 for W1 (K = 16), 1024 for W2 and W3 (K = 64)), so a CTA copies
-// them to shared memory as they are.
+// Weights as FP16 words in the canonical K-major core-matrix layout the MMA
+// reads (byte offset of (n, k) = (n / 8) * sbo + (k / 8) * 128 + (n % 8) * 16 +
+// (k % 8) * 2, sbo = 256 for W1 (K = 16), 1024 for W2 and W3 (K = 64)), so a
+// CTA copies them to shared memory as they are.
 struct MlpDev {
-    const __nv_bfloat16 *w1c;   // [64 x 16]
-    const __nv_bfloat16 *w2c;   // [64 x 64]
-    const __nv_bfloat16 *w3c;   // [64 x 64]
+    const uint16_t *w1c;        // [64 x 16]
+    const uint16_t *w2c;        // [64 x 64]
+    const uint16_t *w3c;        // [64 x 64]
     const float *b1, *b2, *b3;  // [64]
     const float *w4;            // [64]
     float b4;

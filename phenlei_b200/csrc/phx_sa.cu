@@ -559,16 +559,28 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
                     int numSMs, cudaStream_t s)
 {
     (void)w;
-    static int perSMcache[2] = {-1, -1};
-    int &perSM = perSMcache[sizeof(T) == 8 ? 0 : 1];
-    if (perSM < 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, sa_lusgs_kernel<T>, kSweepThreads, 0);
-        if (perSM < 1) perSM = 1;
-        // at most two blocks per SM: the scalar sweep does little work per
-        // poll, and more polling slots only load L2 (16M cells: 4.1 ms at two
-        // blocks per SM against 4.5 ms at six)
-        if (perSM > 2) perSM = 2;
+    // residency of the cooperative launch, per device (a process may drive several)
+    static int perSMcache[kMaxDevices][2];
+    static bool init = false;
+    if (!init) {
+        for (auto &d : perSMcache) d[0] = d[1] = -1;
+        init = true;
     }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+    int &resident = perSMcache[dev][sizeof(T) == 8 ? 0 : 1];
+    if (resident < 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, sa_lusgs_kernel<T>, kSweepThreads, 0);
+        if (resident < 1) resident = 1;
+    }
+    // at most two blocks per SM: the scalar sweep does little work per poll,
+    // and more polling slots only load L2 (16M cells: 4.1 ms at two blocks per
+    // SM against 4.5 ms at six); PHX_SA_SWEEP_BLOCKS_PER_SM changes the cap
+    // (tuning)
+    int cap = 2;
+    if (const char *e = getenv("PHX_SA_SWEEP_BLOCKS_PER_SM")) cap = atoi(e) > 0 ? atoi(e) : cap;
+    const int perSM = resident < cap ? resident : cap;
     int blocks = numSMs * perSM;
     const int npos = g.nFwdPos > g.nBwdPos ? g.nFwdPos : g.nBwdPos;
     const int need = (int)(((long long)npos * kSweepLanes + kSweepThreads - 1) / kSweepThreads);
