@@ -38,6 +38,10 @@ struct phx_ctx {
     int device = 0;
     int numSMs = 148;
     cudaStream_t stream = nullptr;
+    // second stream of the fused driver: the next step's NS boundary and
+    // gradient run on it while the SA sweep runs (phx_ns_relaxation)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t evFork = nullptr, evHead = nullptr;
     std::string err;
     int64_t launches = 0;
     phx_params prm{};
@@ -1121,6 +1125,12 @@ int phx_ctx_destroy(phx_ctx *ctx)
 {
     if (!ctx) return PHX_OK;
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->aux) {
+        cudaStreamSynchronize(ctx->aux);
+        cudaStreamDestroy(ctx->aux);
+        cudaEventDestroy(ctx->evFork);
+        cudaEventDestroy(ctx->evHead);
+    }
     for (void *p : ctx->allocs) cudaFree(p);
     delete ctx;
     return PHX_OK;
@@ -1454,18 +1464,47 @@ int phx_sa_update(phx_ctx *ctx)
     return check_launch(ctx);
 }
 
-static int relax_one(phx_ctx *ctx, double *dhist, int i)
+// One outer step.  With `headDone` the step's NS boundary and gradient have
+// already run on the second stream (see below) and are only joined.  With
+// `prefetch` and SA, the next step's NS boundary and gradient are issued on
+// the second stream right after this step's SA residual, so that they run
+// while the latency-bound SA sweep runs.  They depend only on the updated NS
+// state, and they write nothing the SA sweep, SA update or SA boundary read:
+// ghost states, gradients, the limiter and the laminar viscosity slot; the SA
+// tail reads the SA records, the owner cells' FP64 state and the eddy
+// viscosity.  The next step's NS residual, which reads the new eddy
+// viscosity, waits for both streams.
+static int relax_one(phx_ctx *ctx, double *dhist, int i, bool headDone, bool prefetch, bool &prefetched)
 {
     ctx->step += 1;   // Simulation::UpdateOuterIterationStep
+    prefetched = false;
     int rc;
-    if ((rc = phx_ns_boundary(ctx))) return rc;
-    if ((rc = phx_ns_gradient_limiter(ctx))) return rc;
+    if (headDone) {
+        PHX_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->evHead, 0));
+    } else {
+        if ((rc = phx_ns_boundary(ctx))) return rc;
+        if ((rc = phx_ns_gradient_limiter(ctx))) return rc;
+    }
     if ((rc = phx_ns_residual(ctx))) return rc;
     if ((rc = phx_ns_lusgs(ctx))) return rc;
     if ((rc = phx_ns_update(ctx))) return rc;
     launch_finish_step(ctx->red, dhist, i, (double)ctx->nCell, ctx->stream);
     if (ctx->sa) {
         if ((rc = phx_sa_residual(ctx))) return rc;
+        if (prefetch) {
+            PHX_CUDA(ctx, cudaEventRecord(ctx->evFork, ctx->stream));
+            PHX_CUDA(ctx, cudaStreamWaitEvent(ctx->aux, ctx->evFork, 0));
+            cudaStream_t main = ctx->stream;
+            ctx->stream = ctx->aux;
+            ctx->step += 1;   // the next step's flow-initialisation phase
+            rc = phx_ns_boundary(ctx);
+            if (!rc) rc = phx_ns_gradient_limiter(ctx);
+            ctx->step -= 1;
+            ctx->stream = main;
+            if (rc) return rc;
+            PHX_CUDA(ctx, cudaEventRecord(ctx->evHead, ctx->aux));
+            prefetched = true;
+        }
         if ((rc = phx_sa_lusgs(ctx))) return rc;
         if ((rc = phx_sa_update(ctx))) return rc;
     }
@@ -1482,9 +1521,25 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
         ctx->hist = h;
         ctx->histCap = nsteps;
     }
+    // the overlap of the SA tail with the next step's NS head (relax_one);
+    // PHX_OVERLAP=0 runs every phase on the context's stream, in order
+    const char *ov = getenv("PHX_OVERLAP");
+    const bool overlap = ctx->sa && !(ov && atoi(ov) == 0);
+    if (overlap && !ctx->aux) {
+        PHX_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+        PHX_CUDA(ctx, cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming));
+        PHX_CUDA(ctx, cudaEventCreateWithFlags(&ctx->evHead, cudaEventDisableTiming));
+    }
+    bool headDone = false;
     for (int i = 0; i < nsteps; ++i) {
-        const int rc = relax_one(ctx, ctx->hist, i);
-        if (rc) return rc;
+        bool prefetched = false;
+        const int rc = relax_one(ctx, ctx->hist, i, headDone, overlap && i + 1 < nsteps, prefetched);
+        if (rc) {
+            // nothing of this call stays in flight on the second stream
+            if (prefetched) cudaStreamWaitEvent(ctx->stream, ctx->evHead, 0);
+            return rc;
+        }
+        headDone = prefetched;
     }
     Reduce red;
     PHX_CUDA(ctx, cudaMemcpyAsync(&red, ctx->red, sizeof(Reduce), cudaMemcpyDeviceToHost, ctx->stream));
