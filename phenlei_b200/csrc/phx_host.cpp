@@ -1464,16 +1464,20 @@ int phx_sa_update(phx_ctx *ctx)
     return check_launch(ctx);
 }
 
-// One outer step.  With `headDone` the step's NS boundary and gradient have
-// already run on the second stream (see below) and are only joined.  With
-// `prefetch` and SA, the next step's NS boundary and gradient are issued on
-// the second stream right after this step's SA residual, so that they run
-// while the latency-bound SA sweep runs.  They depend only on the updated NS
-// state, and they write nothing the SA sweep, SA update or SA boundary read:
-// ghost states, gradients, the limiter and the laminar viscosity slot; the SA
-// tail reads the SA records, the owner cells' FP64 state and the eddy
-// viscosity.  The next step's NS residual, which reads the new eddy
-// viscosity, waits for both streams.
+// One outer step.  With `headDone` the step's NS boundary, gradient and
+// residual have already run on the second stream (see below) and are only
+// joined, before the NS sweep.  With `prefetch` and SA, the next step's NS
+// boundary, gradient and residual are issued on the second stream right after
+// this step's SA residual, so that they run while the latency-bound SA sweep
+// and SA update run.  They need the updated NS state and the eddy viscosity,
+// which the SA residual has formed (the SA update changes nu~ only, and the SA
+// boundary after it writes the ghosts' eddy viscosity again with the same
+// values); they write ghost states, gradients, the limiter, the laminar
+// viscosity slot, the face fluxes and LU-SGS factors, the NS residual record,
+// the time step and the NS reduction fields, none of which the SA sweep, SA
+// update or SA boundary reads (they read the SA records, the owner cells'
+// FP64 state and the eddy viscosity).  The two cooperative sweeps never
+// overlap: the NS sweep waits for both streams.
 static int relax_one(phx_ctx *ctx, double *dhist, int i, bool headDone, bool prefetch, bool &prefetched)
 {
     ctx->step += 1;   // Simulation::UpdateOuterIterationStep
@@ -1484,8 +1488,8 @@ static int relax_one(phx_ctx *ctx, double *dhist, int i, bool headDone, bool pre
     } else {
         if ((rc = phx_ns_boundary(ctx))) return rc;
         if ((rc = phx_ns_gradient_limiter(ctx))) return rc;
+        if ((rc = phx_ns_residual(ctx))) return rc;
     }
-    if ((rc = phx_ns_residual(ctx))) return rc;
     if ((rc = phx_ns_lusgs(ctx))) return rc;
     if ((rc = phx_ns_update(ctx))) return rc;
     launch_finish_step(ctx->red, dhist, i, (double)ctx->nCell, ctx->stream);
@@ -1496,9 +1500,10 @@ static int relax_one(phx_ctx *ctx, double *dhist, int i, bool headDone, bool pre
             PHX_CUDA(ctx, cudaStreamWaitEvent(ctx->aux, ctx->evFork, 0));
             cudaStream_t main = ctx->stream;
             ctx->stream = ctx->aux;
-            ctx->step += 1;   // the next step's flow-initialisation phase
+            ctx->step += 1;   // the next step's flow-initialisation phase and CFL
             rc = phx_ns_boundary(ctx);
             if (!rc) rc = phx_ns_gradient_limiter(ctx);
+            if (!rc) rc = phx_ns_residual(ctx);
             ctx->step -= 1;
             ctx->stream = main;
             if (rc) return rc;
