@@ -39,9 +39,9 @@ METRIC = "Mcell-iters/s on 1 B200: mixed+MLP-SA vs plain FP64, at |Î”CL|,|Î”CD|â
 # Bytes each cell moves per iteration under the compulsory-byte rule (each
 # array element counted once per pass that reads or writes it; gathered
 # neighbour values counted once per cell; face arrays once per face per pass),
-# computed for the kernels below from their actual array traffic; see
-# DESIGN.md for the derivation.  Element sizes: FP64 metrics 8 B, working
-# state 8 B (FP64) or 4 B (mixed), indices 4 B.
+# computed for the kernels below from the arrays each pass reads and writes
+# (kernel_bytes lists them per phase).  Element sizes: FP64 metrics 8 B,
+# working state 8 B (FP64) or 4 B (mixed), indices 4 B.
 
 
 def workloads():
@@ -180,7 +180,8 @@ def kernel_bytes(m, precision: str, viscous: int = 0, gradient: str = "ggcell") 
     (each array element counted once per pass that reads or writes it; cell
     values gathered through faces counted once per cell; face arrays once per
     face per pass; indices 4 B, FP64 metrics and master state 8 B, working
-    state E = 8 B (FP64) or 4 B (mixed)).  Derivation in DESIGN.md."""
+    state E = 8 B (FP64) or 4 B (mixed)).  The comment above each term names
+    the arrays it counts."""
     nc, nb, nf = m.n_cell, m.n_bface, m.n_face
     nt = nc + nb
     L = 2 * (nf - nb) + nb          # cell -> face entries

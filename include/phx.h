@@ -11,8 +11,9 @@
  * Each entry point names the reference solver method(s) it replaces (file:line
  * in the reference project).  The reference's own accelerator hook pattern is
  * `#ifdef USE_CUDA CallGPUxxx(grid, ...); return; #endif` at the top of those
- * methods (e.g. CFD/NSSolver/src/NSSolverUnstruct.cpp:13406-13412); the
- * replacement binding is shown in INTEGRATION.md.
+ * methods (e.g. CFD/NSSolver/src/NSSolverUnstruct.cpp:13406-13412); a
+ * `#ifdef USE_PHX` block in the same place calls the entry point below that
+ * names the method, on the context the solver keeps for its grid.
  *
  * Layout conventions (the reference's, API/Geometry/include/Geo_UnstructGrid.h):
  *  - faces: boundary faces first (nBFace of them), then interior faces;
