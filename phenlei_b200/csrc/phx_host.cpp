@@ -565,6 +565,69 @@ std::vector<int> morton_order(int n, const double *x, const double *y, const dou
     return ord;
 }
 
+// Reverse Cuthill-McKee order of the cells over their interior faces: from a
+// pseudo-peripheral cell (the far end of a breadth-first search from a
+// minimum-degree cell), breadth-first, each cell's unvisited neighbours in
+// increasing degree, every connected component in turn, then reversed.
+std::vector<int> rcm_order(int nc, int nb, const std::vector<int> &c2f_off, const std::vector<int> &c2f,
+                           const std::vector<int> &left, const std::vector<int> &right)
+{
+    auto nbr = [&](int c, int j) {
+        const int f = c2f[j];
+        if (f < nb) return -1;
+        return left[f] == c ? right[f] : left[f];
+    };
+    std::vector<int> deg(nc, 0);
+    for (int c = 0; c < nc; ++c)
+        for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) deg[c] += nbr(c, j) >= 0;
+    std::vector<int> ord;
+    ord.reserve(nc);
+    std::vector<int> mark(nc, 0);   // 0 unvisited; BFS stamps
+    std::vector<int> q, tmp;
+    q.reserve(nc);
+    int stamp = 1;
+    // breadth-first from s over unvisited cells (mark != final); returns the last cell reached
+    auto far_end = [&](int s) {
+        ++stamp;
+        q.clear();
+        q.push_back(s);
+        mark[s] = stamp;
+        size_t h = 0;
+        int last = s;
+        while (h < q.size()) {
+            const int c = q[h++];
+            last = c;
+            for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+                const int o = nbr(c, j);
+                if (o >= 0 && mark[o] != -1 && mark[o] != stamp) { mark[o] = stamp; q.push_back(o); }
+            }
+        }
+        return last;
+    };
+    std::vector<int> byDeg(nc);
+    for (int c = 0; c < nc; ++c) byDeg[c] = c;
+    std::stable_sort(byDeg.begin(), byDeg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    for (int start : byDeg) {
+        if (mark[start] == -1) continue;
+        const int s = far_end(far_end(start));   // two searches: a pseudo-peripheral cell
+        const size_t first = ord.size();
+        ord.push_back(s);
+        mark[s] = -1;
+        for (size_t h = first; h < ord.size(); ++h) {
+            const int c = ord[h];
+            tmp.clear();
+            for (int j = c2f_off[c]; j < c2f_off[c + 1]; ++j) {
+                const int o = nbr(c, j);
+                if (o >= 0 && mark[o] != -1) { mark[o] = -1; tmp.push_back(o); }
+            }
+            std::stable_sort(tmp.begin(), tmp.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+            ord.insert(ord.end(), tmp.begin(), tmp.end());
+        }
+    }
+    std::reverse(ord.begin(), ord.end());
+    return ord;
+}
+
 double entropy_fix_coefficient(double mach, double scale)
 {
     // Param_NSSolver::SetEntropyFixCoefficients, CFD/NSSolver/src/Param_NSSolver.cpp:224-268
@@ -818,7 +881,12 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         if (c2f_off[c + 1] - c2f_off[c] > kSweepMaxEntries) { delete ctx; return PHX_ERR_ARG; }  // two sweep slots
 
     // storage order
-    const std::vector<int> ord = morton_order(nc, ctx->geom[7].data(), ctx->geom[8].data(), ctx->geom[9].data());
+    // storage order: Morton (Z-curve) order of the cell centres, or, with
+    // PHX_CELL_ORDER=rcm, reverse Cuthill-McKee over the faces
+    const char *co = getenv("PHX_CELL_ORDER");
+    const std::vector<int> ord = (co && std::strcmp(co, "rcm") == 0)
+                                     ? rcm_order(nc, nb, c2f_off, c2f, h.left, h.right)
+                                     : morton_order(nc, ctx->geom[7].data(), ctx->geom[8].data(), ctx->geom[9].data());
     std::vector<int> rank(nc);
     for (int i = 0; i < nc; ++i) rank[ord[i]] = i;
     ctx->rankOf = rank;
