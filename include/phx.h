@@ -51,6 +51,7 @@ extern "C" {
 #define PHX_SCHEME_VANLEER 3      /* "vanleer" */
 #define PHX_SCHEME_HLLE 4         /* "hlle" */
 #define PHX_SCHEME_AUSMDV 5       /* "ausmdv" */
+#define PHX_SCHEME_AUSMPW 6       /* "ausmpw" */
 
 /* Limiters (uns_limiter_name; GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300) */
 #define PHX_LIMITER_NOLIM 0       /* "nolim" */

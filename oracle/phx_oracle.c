@@ -872,6 +872,55 @@ static void ausmpwp_flux(const double *ql, const double *qr, double gl, double g
     f[4] = c12 * (mpl * rl * hl + mmr * rr * hr);
 }
 
+/* Ausmpw_Scheme, Flux_Inviscid.cpp:13463-13626: AUSMPW.  It differs from
+ * AUSMPW+ above in its sound speeds (gamma p (1 / (rho + SMALL)), mean
+ * 1 / (0.5 (a_L + a_R) + SMALL)), in a pressure weight without limiter, and in
+ * the pressure corrections, taken for |M| < 1 with no test of p12.  Its split
+ * polynomials FMSplit4 / FPSplit5 (:14109-14125) with beta = alpha = 0 are
+ * FMmpn / FMppn exactly. */
+static void ausmpw_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                        double zsn, double *f)
+{
+    double rl = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+    double rr = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+    double v2l = ul * ul + vl * vl + wl * wl;
+    double v2r = ur * ur + vr * vr + wr * wr;
+    double hl = (gl / (gl - 1.0)) * (pl / rl) + 0.5 * v2l;
+    double hr = (gr / (gr - 1.0)) * (pr / rr) + 0.5 * v2r;
+    double vnl = xsn * ul + ysn * vl + zsn * wl;
+    double vnr = xsn * ur + ysn * vr + zsn * wr;
+    double orl = 1.0 / (rl + OX_SMALL), orr = 1.0 / (rr + OX_SMALL);
+    double cl = sqrt(gl * pl * orl), cr = sqrt(gr * pr * orr);
+    double cm = 0.5 * (cl + cr);
+    double ocm = 1.0 / (cm + OX_SMALL);
+    double ml = vnl * ocm, mr = vnr * ocm;
+    double fm4l = fm_mpn(ml, 1.0), fm4r = fm_mpn(mr, -1.0);
+    double fp5l = fm_ppn(ml, 1.0), fp5r = fm_ppn(mr, -1.0);
+    double m12 = fm4l + fm4r;
+    double p12 = fp5l * pl + fp5r * pr;
+    double minplr = omin(pl / (pr + OX_SMALL), pr / (pl + OX_SMALL));
+    double fw = 1.0 - minplr * minplr * minplr;
+    double op12 = 1.0 / (p12 + OX_SMALL);
+    double fl = 0.0, fr = 0.0;
+    if (fabs(ml) < 1.0) fl = pl * op12 - 1.0;
+    if (fabs(mr) < 1.0) fr = pr * op12 - 1.0;
+    double mpl, mmr;
+    if (m12 >= 0.0) {
+        double o = 1.0 + fr;
+        mpl = fm4l + fm4r * ((1.0 - fw) * o - fl);
+        mmr = fm4r * fw * o;
+    } else {
+        double o = 1.0 + fl;
+        mpl = fm4l * fw * o;
+        mmr = fm4r + fm4l * ((1.0 - fw) * o - fr);
+    }
+    f[0] = cm * (mpl * rl + mmr * rr);
+    f[1] = cm * (mpl * rl * ul + mmr * rr * ur) + p12 * xsn;
+    f[2] = cm * (mpl * rl * vl + mmr * rr * vr) + p12 * ysn;
+    f[3] = cm * (mpl * rl * wl + mmr * rr * wr) + p12 * zsn;
+    f[4] = cm * (mpl * rl * hl + mmr * rr * hr);
+}
+
 /* PositiveCheckForDensityAndPressure: rho > 0 and p > 0. */
 static inline int positive(const double *q) { return q[0] > 0.0 && q[4] > 0.0; }
 
@@ -922,6 +971,7 @@ void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p,
         case OX_SCHEME_VANLEER: vanleer_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_HLLE: hlle_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_AUSMDV: ausmdv_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        case OX_SCHEME_AUSMPW: ausmpw_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         default: roe_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->entropy_acoustic, p->entropy_convective, fl);
         }
         for (int k = 0; k < 5; ++k) {

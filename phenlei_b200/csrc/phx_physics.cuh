@@ -311,6 +311,54 @@ __device__ __forceinline__ void ausmpwp_flux(const T *ql, const T *qr, T gl, T g
     f[4] = c12 * (mpl * rl * hl + mmr * rr * hr);
 }
 
+// Ausmpw_Scheme (Flux_Inviscid.cpp:13463-13626): AUSMPW.  It differs from
+// AUSMPW+ in its sound speeds (gamma p (1 / (rho + SMALL)), mean
+// 1 / (0.5 (a_L + a_R) + SMALL)), in a pressure weight without limiter, and in
+// the pressure corrections, taken for |M| < 1 with no test of p12.  Its split
+// polynomials (FMSplit4 / FPSplit5 with beta = alpha = 0) are FMmpn / FMppn.
+template <class T>
+__device__ __forceinline__ void ausmpw_flux(const T *ql, const T *qr, T gl, T gr, T xsn, T ysn, T zsn, T *f)
+{
+    const T rl = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+    const T rr = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+    const T v2l = ul * ul + vl * vl + wl * wl;
+    const T v2r = ur * ur + vr * vr + wr * wr;
+    const T hl = (gl / (gl - T(1))) * (pl / rl) + T(0.5) * v2l;
+    const T hr = (gr / (gr - T(1))) * (pr / rr) + T(0.5) * v2r;
+    const T vnl = xsn * ul + ysn * vl + zsn * wl;
+    const T vnr = xsn * ur + ysn * vr + zsn * wr;
+    const T orl = T(1) / (rl + T(kSmall)), orr = T(1) / (rr + T(kSmall));
+    const T cl = sqrt(gl * pl * orl), cr = sqrt(gr * pr * orr);
+    const T cm = T(0.5) * (cl + cr);
+    const T ocm = T(1) / (cm + T(kSmall));
+    const T ml = vnl * ocm, mr = vnr * ocm;
+    const T fm4l = fm_mpn(ml, T(1)), fm4r = fm_mpn(mr, T(-1));
+    const T fp5l = fm_ppn(ml, T(1)), fp5r = fm_ppn(mr, T(-1));
+    const T m12 = fm4l + fm4r;
+    const T p12 = fp5l * pl + fp5r * pr;
+    const T minplr = tmin(pl / (pr + T(kSmall)), pr / (pl + T(kSmall)));
+    const T fw = T(1) - minplr * minplr * minplr;
+    const T op12 = T(1) / (p12 + T(kSmall));
+    T fl = T(0), fr = T(0);
+    if (fabs(ml) < T(1)) fl = pl * op12 - T(1);
+    if (fabs(mr) < T(1)) fr = pr * op12 - T(1);
+    T mpl, mmr;
+    if (m12 >= T(0)) {
+        const T o = T(1) + fr;
+        mpl = fm4l + fm4r * ((T(1) - fw) * o - fl);
+        mmr = fm4r * fw * o;
+    } else {
+        const T o = T(1) + fl;
+        mpl = fm4l * fw * o;
+        mmr = fm4r + fm4l * ((T(1) - fw) * o - fr);
+    }
+    f[0] = cm * (mpl * rl + mmr * rr);
+    f[1] = cm * (mpl * rl * ul + mmr * rr * ur) + p12 * xsn;
+    f[2] = cm * (mpl * rl * vl + mmr * rr * vr) + p12 * ysn;
+    f[3] = cm * (mpl * rl * wl + mmr * rr * wr) + p12 * zsn;
+    f[4] = cm * (mpl * rl * hl + mmr * rr * hr);
+}
+
 // Non-Roe scheme selected by uns_scheme_name (PHX_SCHEME_*); uniform across a launch.
 template <class T>
 __device__ __forceinline__ void other_flux(int scheme, const T *ql, const T *qr, T gl, T gr, T xsn, T ysn, T zsn,
@@ -331,6 +379,8 @@ __device__ __forceinline__ void other_flux(int scheme, const T *ql, const T *qr,
         hlle_flux<T>(ql, qr, gl, gr, xsn, ysn, zsn, f);
     } else if (scheme == PHX_SCHEME_AUSMDV) {
         ausmdv_flux<T>(ql, qr, gl, gr, xsn, ysn, zsn, f);
+    } else if (scheme == PHX_SCHEME_AUSMPW) {
+        ausmpw_flux<T>(ql, qr, gl, gr, xsn, ysn, zsn, f);
     } else {
         ausmpwp_flux<T>(ql, qr, gl, gr, xsn, ysn, zsn, ausmpwLim, f);
     }

@@ -21,8 +21,9 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 MIXED_TOL = 1e-5
-SCHEMES = ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+")
-TAG = {"steger": "steger", "vanleer": "vanleer", "hlle": "hlle", "ausmdv": "ausmdv", "ausmpw+": "ausmpwp"}
+SCHEMES = ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+", "ausmpw")
+TAG = {"steger": "steger", "vanleer": "vanleer", "hlle": "hlle", "ausmdv": "ausmdv", "ausmpw+": "ausmpwp",
+       "ausmpw": "ausmpw"}
 
 
 @pytest.mark.parametrize("name", [f"euler_bump_16x8x2_{TAG[s]}_step3" for s in SCHEMES]
@@ -68,7 +69,7 @@ def test_scheme_vs_oracle_euler_bump_64x32x4(scheme, precision, tol):
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
-@pytest.mark.parametrize("scheme", ["hlle", "ausmpw+"])
+@pytest.mark.parametrize("scheme", ["hlle", "ausmpw+", "ausmpw"])
 def test_scheme_vs_oracle_laminar(scheme, precision, tol):
     """The viscous face-pass instantiation with a non-Roe scheme."""
     m = M.channel_bump(32, 16, 2)
