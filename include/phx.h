@@ -64,6 +64,21 @@ extern "C" {
 #define PHX_BC_SYMMETRY 3
 #define PHX_BC_FARFIELD 4
 #define PHX_BC_OUTFLOW 6
+/* PHENGLEI::INTERFACE (Geo_SimpleBC.h:32): the faces of a zone cut by a
+ * partition.  The ghost of such a face is the neighbouring zone's cell: its
+ * values come from halo exchanges (phx_set_halo / phx_halo_pack /
+ * phx_halo_unpack), never from the boundary pass, and every other pass treats
+ * the face as an interior face. */
+#define PHX_BC_INTERFACE -1
+
+/* Halo fields, the interface data the reference uploads between zones: */
+#define PHX_HALO_Q 0         /* FP64 state (NSSolver::PostSolve, CFD/NSSolver/src/NSSolver.cpp:139-142) */
+#define PHX_HALO_GRADIENT 1  /* primitive and temperature gradients with the limiter
+                                (Controller::ComputeGradient, CFD/Solver/src/Controller.cpp:1288, :1321) */
+#define PHX_HALO_DQ 2        /* forward-sweep dq between the LU-SGS sweeps (Controller::LUSGS, :1917-1924) */
+#define PHX_HALO_TURB 3      /* nu~ and eddy viscosity (TurbSolverUnstr::UploadInterfaceValue,
+                                CFD/TurbSolver/src/TurbSolverUnstr.cpp:7130-7145) */
+#define PHX_HALO_TURB_DQ 4   /* forward-sweep SA dq between the SA sweeps */
 
 /* state selectors for phx_set_state / phx_get_state */
 #define PHX_Q 0          /* primitive state [5][nTotal] */
@@ -295,6 +310,68 @@ int phx_set_wait_limit(phx_ctx *ctx, int64_t polls);
  * returns PHX_ERR_TIMEOUT instead of hanging.  Nothing faults: the sweep
  * stops at its next level boundary.  No counterpart in the reference. */
 int phx_fault_hold_cell(phx_ctx *ctx, int32_t cell);
+
+/* --- partitioned grids (zones joined by PHX_BC_INTERFACE faces) ------------
+ * One context per zone.  A partitioned step runs the phases one by one with
+ * the reference's exchanges between them (Controller::Relaxation,
+ * CFD/Solver/src/Controller.cpp:549-587; the interface communication of
+ * Controller::CommunicationInterfaceData, :3389): boundary, gradient and
+ * limiter, HALO GRADIENT, residual, the minimum time step over all zones,
+ * forward sweep, HALO DQ, backward sweep, update, HALO Q; with SA: SA
+ * residual, SA forward sweep, HALO TURB_DQ, SA backward sweep, SA update,
+ * HALO TURB.  The gradient of nu~ needs no exchange here: only its own cell
+ * reads it.  The fused
+ * phx_ns_relaxation, phx_ns_lusgs and phx_sa_lusgs refuse a context with
+ * interface faces (PHX_ERR_STATE).  GG-node gradients are not supported
+ * across zones (PHX_ERR_ARG at creation). */
+
+/* Region::SwapGeometry (API/Physics/src/Region.cpp:3257-3268) and
+ * Region::ComputeGlobalGridSize (:2655-2734): the cell centres and volumes of
+ * the neighbouring zones' cells behind n interface faces bfaces[] (this
+ * zone's boundary face numbers) become their ghosts' (UnstructGrid::
+ * TranslateCellCenter, API/Geometry/src/Geo_UnstructGrid.cpp:4500-4541), and
+ * the least-squares weights and viscous-flux switches are formed again;
+ * avg_vol > 0 replaces the average cell volume the Venkatakrishnan limiter
+ * scales with (the average over all zones).  Host arrays. */
+int phx_swap_geometry(phx_ctx *ctx, int64_t n, const int32_t *bfaces, const double *xcc, const double *ycc,
+                      const double *zcc, const double *vol, double avg_vol);
+
+/* The halo plan of this zone: the n_send cells (this zone's cell numbers)
+ * whose values the neighbouring zones receive, and the n_recv interface faces
+ * (boundary face numbers) whose ghosts receive, each in the caller's order
+ * (concatenated over the neighbours).  Host arrays, copied. */
+int phx_set_halo(phx_ctx *ctx, int64_t n_send, const int32_t *send_cells, int64_t n_recv,
+                 const int32_t *recv_bfaces);
+/* Bytes of one row of a halo field (it depends on the precision). */
+int64_t phx_halo_row_bytes(const phx_ctx *ctx, int field);
+/* Gathers the send cells' rows of `field` into buf_dev (n_send rows), or
+ * scatters buf_dev (n_recv rows) into the receiving ghosts, on the context's
+ * stream.  Device buffers; the caller moves the rows between the zones
+ * (peer copies, NCCL). */
+int phx_halo_pack(phx_ctx *ctx, int field, void *buf_dev);
+int phx_halo_unpack(phx_ctx *ctx, int field, const void *buf_dev);
+
+/* The two LU-SGS sweeps of phx_ns_lusgs / phx_sa_lusgs as separate calls,
+ * for the dq exchange between them (Controller::LUSGS, Controller.cpp:1917-1924;
+ * CommunicationDQ :2874).  The backward sweep reads the interface ghosts' dq
+ * from HALO DQ (TURB_DQ). */
+int phx_ns_lusgs_forward(phx_ctx *ctx);
+int phx_ns_lusgs_backward(phx_ctx *ctx);
+int phx_sa_lusgs_forward(phx_ctx *ctx);
+int phx_sa_lusgs_backward(phx_ctx *ctx);
+
+/* The smallest raw local time step of this zone after phx_ns_residual
+ * (synchronises), and the minimum over all zones that the ktmax clamp of the
+ * sweeps then uses (Controller::GetGlobalMinTimeStep, Controller.cpp:720-751). */
+int phx_ns_min_timestep(phx_ctx *ctx, double *out);
+int phx_ns_set_min_timestep(phx_ctx *ctx, double value);
+
+/* Status of the device work issued so far (synchronises): PHX_ERR_TIMEOUT if
+ * a sweep's bounded dependency wait ran out, PHX_ERR_NUMERIC if the positivity
+ * repair overflowed, else PHX_OK; the status is cleared once reported.  The
+ * phase calls above only launch; phx_ns_relaxation checks the same status
+ * itself. */
+int phx_step_status(phx_ctx *ctx);
 
 /* Outer step counter (drives the CFL ramp of NSSolver::ComputeCFL). */
 int phx_set_step(phx_ctx *ctx, int step);

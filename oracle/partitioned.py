@@ -6,7 +6,7 @@ The reference runs a partitioned grid as zones joined by INTERFACE faces
 (PHENGLEI::INTERFACE, API/Geometry/include/Geo_SimpleBC.h:32), and fills
 their ghosts from the neighbouring zone at these points:
 
-* set-up: the ghosts' cell centres, then the LSQ weights
+* set-up: the ghosts' cell centres and volumes, then the LSQ weights
   (Region::SwapGeometry, API/Physics/src/Region.cpp:3257-3268), and one
   average cell volume over all zones (Region::ComputeGlobalGridSize, :2655-2734);
 * after the update and at initialisation: q (NSSolver::PostSolve,
@@ -64,9 +64,11 @@ class PartitionedOracle:
                   for p in self.parts]
         self.viscous = params.get("viscousType", 0) > 0
         self.step = 0
-        # SwapGeometry: the interface ghosts take the neighbouring cells' centres,
-        # and the least-squares weights are formed again from them
-        for k in ("xcc", "ycc", "zcc"):
+        # SwapGeometry: the interface ghosts take the neighbouring cells' centres
+        # and volumes (UnstructGrid::TranslateCellCenter,
+        # API/Geometry/src/Geo_UnstructGrid.cpp:4500-4541), and the least-squares
+        # weights are formed again from them
+        for k in ("xcc", "ycc", "zcc", "vol"):
             self._exchange(lambda o, k=k: o.geo[k])
         for o in self.o:
             lib().ox_lsq_weights(C.byref(o.g), C.byref(o.m))

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libphx.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["phx_kernels.cu", "phx_sa.cu", "phx_mlp.cu", "phx_noalloc.cu", "phx_host.cpp"]
+SOURCES = ["phx_kernels.cu", "phx_sa.cu", "phx_mlp.cu", "phx_noalloc.cu", "phx_halo.cu", "phx_host.cpp"]
 # The face, gradient and SA passes of the FP32 working path use approximate
 # single-precision division and square root (2 ulp); these flags leave FP64
 # arithmetic alone.  At 16M cells: face pass 5.3 -> 4.3 ms, gradient 2.1 ->

@@ -78,6 +78,16 @@ struct phx_ctx {
     int step = 0;
     bool haveResidual = false;
     std::vector<int> rankOf;              // storage index of each reference cell
+    // partitioned grids (interface faces): the topology and storage maps that
+    // phx_swap_geometry needs to form the weights again, and the halo plan
+    bool hasInterface = false;
+    std::vector<int> hleft, hright;       // reference left / right cell of each face (boundary: nCell + f)
+    std::vector<int> forder, ord;         // storage face -> reference face, storage cell -> reference cell
+    std::vector<int> bfacePos;            // storage position of each reference boundary face
+    std::vector<uint8_t> itfFace;         // 1 for each reference boundary face of an interface region
+    int *haloSend = nullptr, *haloRecv = nullptr;   // storage indices (device)
+    int nHaloSend = 0, nHaloRecv = 0;
+    bool nsForwardDone = false, saForwardDone = false;   // a forward sweep waits for its backward sweep
 };
 
 namespace {
@@ -656,8 +666,9 @@ double total_pressure(double gama, double mach)
 
 bool limiter_zeroed(int bcType)
 {
-    // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775
-    return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW;
+    // SetLimitBoundary, Geo_UnstructGrid.cpp:10744-10775 (interface faces are left alone, :10758)
+    return bcType != PHX_BC_SYMMETRY && bcType != PHX_BC_SOLID_SURFACE && bcType != PHX_BC_OUTFLOW &&
+           bcType != PHX_BC_INTERFACE;
 }
 
 // Viscosity record of a laminar run: eddy viscosity 0, laminar viscosity of the
@@ -689,7 +700,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     r |= dalloc(ctx, &t.tface, nf * kTf);
     r |= dalloc(ctx, &t.tcoef, 2 * nf);
     r |= dalloc(ctx, &t.tdq, nc);
-    r |= dalloc(ctx, &t.tdqf, nc);
+    r |= dalloc(ctx, &t.tdqf, nt);
     r |= dalloc(ctx, &t.tdfl, nc);
     r |= dalloc(ctx, &t.tsrc, nc);
     if (ctx->prm.gradientName == 2) r |= dalloc(ctx, &t.qtnode, (size_t)ctx->nNode);
@@ -711,6 +722,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     PHX_CUDA(ctx, cudaMemcpy(t.qt64, q.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
     PHX_CUDA(ctx, cudaMemcpy(w.trec, rec.data(), sizeof(T) * nt * kTr, cudaMemcpyHostToDevice));
     PHX_CUDA(ctx, cudaMemset(t.tcoef, 0, sizeof(T) * 2 * nf));
+    PHX_CUDA(ctx, cudaMemset(t.tdqf, 0, sizeof(T) * nt));   // interface ghost rows until the first exchange
     return PHX_OK;
 }
 
@@ -720,13 +732,13 @@ int make_work(phx_ctx *ctx, Work<T> &w, const std::vector<double> &limInit)
     const size_t nt = ctx->nTotal, nc = ctx->nCell, nf = ctx->nFace;
     int r = 0;
     r |= dalloc(ctx, &w.qrec, nt * kQ);
-    r |= dalloc(ctx, &w.grec, nc * kG);
+    r |= dalloc(ctx, &w.grec, nt * kG);
     r |= dalloc(ctx, &w.flux, nf * kFlux);
     r |= dalloc(ctx, &w.coef, 2 * nf * kCoef);
     r |= dalloc(ctx, &w.crec, nc * kC);
     r |= dalloc(ctx, &w.dtraw, nc);
     r |= dalloc(ctx, &w.dqrec, nt * kD);
-    r |= dalloc(ctx, &w.dqfwd, nc * kD);
+    r |= dalloc(ctx, &w.dqfwd, nt * kD);
     r |= dalloc(ctx, &w.dflux, nc * kD);
     if (ctx->prm.gradientName == 2) r |= dalloc(ctx, &w.nrec, (size_t)ctx->nNode * kN);
     if (r) return r;
@@ -735,6 +747,8 @@ int make_work(phx_ctx *ctx, Work<T> &w, const std::vector<double> &limInit)
     for (size_t i = 0; i < nt; ++i) q[i * kQ + 7] = (T)limInit[i];
     PHX_CUDA(ctx, cudaMemcpy(w.qrec, q.data(), sizeof(T) * q.size(), cudaMemcpyHostToDevice));
     PHX_CUDA(ctx, cudaMemset(w.dqrec, 0, sizeof(T) * nt * kD));
+    PHX_CUDA(ctx, cudaMemset(w.dqfwd, 0, sizeof(T) * nt * kD));   // interface ghost rows until the first exchange
+    PHX_CUDA(ctx, cudaMemset(w.grec, 0, sizeof(T) * nt * kG));
     PHX_CUDA(ctx, cudaMemset(w.crec, 0, sizeof(T) * nc * kC));
     PHX_CUDA(ctx, cudaMemset(w.coef, 0, sizeof(T) * 2 * nf * kCoef));
     return PHX_OK;
@@ -1025,6 +1039,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         if (t == PHX_BC_SOLID_SURFACE) bkind[fs] = prm->viscousType ? BK_WALL : BK_SYMMETRY;
         else if (t == PHX_BC_SYMMETRY) bkind[fs] = BK_SYMMETRY;
         else if (t == PHX_BC_FARFIELD) bkind[fs] = BK_FARFIELD;
+        else if (t == PHX_BC_INTERFACE) bkind[fs] = BK_INTERFACE;
         else { delete ctx; return PHX_ERR_ARG; }
         // SetLimitBoundary zeroes the far-field ghosts' limiter only when a limiter
         // runs; with nolim every limit2D entry is 1 (ComputeLimiter :18213-18220)
@@ -1034,6 +1049,11 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
                 limInit[nc + fs] = 0.0;
         }
     }
+
+    // GG-node across zones needs the interpoint exchange of node values and
+    // weights (Controller::PostSolve, Controller.cpp:5063-5205), which is not built
+    ctx->hasInterface = std::find(bkind.begin(), bkind.end(), (int32_t)BK_INTERFACE) != bkind.end();
+    if (ctx->hasInterface && prm->gradientName == 2) { delete ctx; return PHX_ERR_ARG; }
 
     std::vector<double> iwt, m6;
     if (prm->gradientName == 1) lsq_weights(h, ctx->geom, iwt, m6);
@@ -1181,6 +1201,15 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         const int code = rc < 0 ? rc : PHX_ERR_CUDA;
         phx_ctx_destroy(ctx);
         return code;
+    }
+    if (ctx->hasInterface) {
+        ctx->hleft = h.left;
+        ctx->hright = h.right;
+        ctx->forder = forder;
+        ctx->ord = ord;
+        ctx->bfacePos.assign(fpos.begin(), fpos.begin() + nb);
+        ctx->itfFace.assign(nb, 0);
+        for (int fs = 0; fs < nb; ++fs) ctx->itfFace[forder[fs]] = bkind[fs] == BK_INTERFACE;
     }
     // free-stream initial state (NSSolverUnstruct::InitFlow), ghosts included
     std::vector<double> q0((size_t)5 * nt);
@@ -1440,15 +1469,35 @@ int phx_ns_residual(phx_ctx *ctx)
     return check_launch(ctx, 3);
 }
 
+static int ns_lusgs(phx_ctx *ctx, int sweeps)
+{
+    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "the LU-SGS sweeps need phx_ns_residual first");
+    if (sweeps == kSweepBackward && !ctx->nsForwardDone)
+        return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs_backward needs phx_ns_lusgs_forward first");
+    const int e = ctx->mixed
+                      ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->numSMs, ctx->stream, sweeps)
+                      : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->numSMs, ctx->stream, sweeps);
+    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
+    ctx->nsForwardDone = sweeps == kSweepForward;
+    return check_launch(ctx, (sweeps & kSweepForward) ? 2 : 1);
+}
+
+static int refuse_zone(phx_ctx *ctx, const char *what)
+{
+    return fail(ctx, PHX_ERR_STATE, std::string(what) +
+                                        ": the grid has interface faces; run the phases with the halo exchanges "
+                                        "(phx_ns_lusgs_forward / phx_ns_lusgs_backward and the SA pair)");
+}
+
 int phx_ns_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
-    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_lusgs needs phx_ns_residual first");
-    const int e = ctx->mixed ? launch_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->red, ctx->numSMs, ctx->stream)
-                             : launch_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->red, ctx->numSMs, ctx->stream);
-    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx, 2);
+    if (ctx->hasInterface) return refuse_zone(ctx, "phx_ns_lusgs");
+    return ns_lusgs(ctx, kSweepBoth);
 }
+
+int phx_ns_lusgs_forward(phx_ctx *ctx) { return ctx ? ns_lusgs(ctx, kSweepForward) : PHX_ERR_ARG; }
+int phx_ns_lusgs_backward(phx_ctx *ctx) { return ctx ? ns_lusgs(ctx, kSweepBackward) : PHX_ERR_ARG; }
 
 int phx_ns_update(phx_ctx *ctx)
 {
@@ -1502,17 +1551,29 @@ int phx_sa_residual(phx_ctx *ctx)
     return check_launch(ctx, mlp ? 6 : 5);
 }
 
+static int sa_lusgs(phx_ctx *ctx, int sweeps)
+{
+    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
+    if (sweeps == kSweepBackward && !ctx->saForwardDone)
+        return fail(ctx, PHX_ERR_STATE, "phx_sa_lusgs_backward needs phx_sa_lusgs_forward first");
+    const int e = ctx->mixed ? launch_sa_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->red, ctx->numSMs,
+                                                      ctx->stream, sweeps)
+                             : launch_sa_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->red, ctx->numSMs,
+                                                       ctx->stream, sweeps);
+    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
+    ctx->saForwardDone = sweeps == kSweepForward;
+    return check_launch(ctx, (sweeps & kSweepForward) ? 2 : 1);
+}
+
 int phx_sa_lusgs(phx_ctx *ctx)
 {
     if (!ctx) return PHX_ERR_ARG;
-    if (!ctx->sa) return fail(ctx, PHX_ERR_STATE, "the context has no SA model (viscousType != 3)");
-    const int e = ctx->mixed ? launch_sa_lusgs<float>(ctx->g, ctx->nc, ctx->w32, ctx->t32, ctx->red, ctx->numSMs,
-                                                      ctx->stream)
-                             : launch_sa_lusgs<double>(ctx->g, ctx->nc, ctx->w64, ctx->t64, ctx->red, ctx->numSMs,
-                                                       ctx->stream);
-    if (e) return fail(ctx, PHX_ERR_CUDA, std::string("cooperative launch failed: ") + cudaGetErrorString((cudaError_t)e));
-    return check_launch(ctx, 2);
+    if (ctx->hasInterface) return refuse_zone(ctx, "phx_sa_lusgs");
+    return sa_lusgs(ctx, kSweepBoth);
 }
+
+int phx_sa_lusgs_forward(phx_ctx *ctx) { return ctx ? sa_lusgs(ctx, kSweepForward) : PHX_ERR_ARG; }
+int phx_sa_lusgs_backward(phx_ctx *ctx) { return ctx ? sa_lusgs(ctx, kSweepBackward) : PHX_ERR_ARG; }
 
 int phx_sa_update(phx_ctx *ctx)
 {
@@ -1587,6 +1648,7 @@ static int relax_one(phx_ctx *ctx, double *dhist, int i, bool headDone, bool pre
 int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
 {
     if (!ctx || nsteps < 0) return PHX_ERR_ARG;
+    if (ctx->hasInterface) return refuse_zone(ctx, "phx_ns_relaxation");
     if (nsteps > ctx->histCap) {
         double *h = nullptr;
         const int rc = dalloc(ctx, &h, (size_t)nsteps);
@@ -1626,6 +1688,180 @@ int phx_ns_relaxation(phx_ctx *ctx, int nsteps, double *res_hist)
     }
     if (red.error == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
     if (red.error == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
+    return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Partitioned grids: SwapGeometry, the halo plan and its exchanges, the
+// minimum time step over all zones.
+// ---------------------------------------------------------------------------
+int phx_swap_geometry(phx_ctx *ctx, int64_t n, const int32_t *bfaces, const double *xcc, const double *ycc,
+                      const double *zcc, const double *vol, double avg_vol)
+{
+    if (!ctx || n < 0 || (n > 0 && (!bfaces || !xcc || !ycc || !zcc || !vol))) return PHX_ERR_ARG;
+    if (!ctx->hasInterface) return fail(ctx, PHX_ERR_STATE, "the grid has no interface faces");
+    const int nc = ctx->nCell, nb = ctx->nBFace, nf = ctx->nFace, nt = ctx->nTotal;
+    for (int64_t i = 0; i < n; ++i)
+        if (bfaces[i] < 0 || bfaces[i] >= nb || !ctx->itfFace[bfaces[i]])
+            return fail(ctx, PHX_ERR_ARG, "phx_swap_geometry: not an interface face");
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the records below may be in use
+    for (int64_t i = 0; i < n; ++i) {
+        const int re = nc + bfaces[i];
+        ctx->geom[7][re] = xcc[i];
+        ctx->geom[8][re] = ycc[i];
+        ctx->geom[9][re] = zcc[i];
+        ctx->geom[10][re] = vol[i];
+    }
+    HostGrid h{};
+    h.nCell = nc; h.nBFace = nb; h.nFace = nf; h.nNode = ctx->nNode;
+    h.left = ctx->hleft;
+    h.right = ctx->hright;
+    const phx_params *prm = &ctx->prm;
+    // face records (least-squares weight in slot 7), ghost centres, cell matrices
+    std::vector<double> iwt, m6;
+    if (prm->gradientName == 1) lsq_weights(h, ctx->geom, iwt, m6);
+    std::vector<double> frec((size_t)nf * kF), xrec((size_t)nt * kX);
+    for (int fs = 0; fs < nf; ++fs) {
+        const int f = ctx->forder[fs];
+        for (int k = 0; k < 7; ++k) frec[(size_t)fs * kF + k] = ctx->geom[k][f];
+        frec[(size_t)fs * kF + 7] = prm->gradientName == 1 ? iwt[f] : 0.0;
+    }
+    for (int i = 0; i < nt; ++i) {
+        const int c = i < nc ? ctx->ord[i] : nc + ctx->forder[i - nc];
+        for (int k = 0; k < 4; ++k) xrec[(size_t)i * kX + k] = ctx->geom[7 + k][c];
+    }
+    PHX_CUDA(ctx, cudaMemcpy(const_cast<double *>(ctx->g.frec), frec.data(), sizeof(double) * frec.size(),
+                             cudaMemcpyHostToDevice));
+    PHX_CUDA(ctx, cudaMemcpy(const_cast<double *>(ctx->g.xrec), xrec.data(), sizeof(double) * xrec.size(),
+                             cudaMemcpyHostToDevice));
+    if (prm->gradientName == 1) {
+        std::vector<double> lsqs((size_t)nc * 8, 0.0);
+        for (int i = 0; i < nc; ++i)
+            for (int k = 0; k < 6; ++k) lsqs[(size_t)i * 8 + k] = m6[(size_t)ctx->ord[i] * 6 + k];
+        PHX_CUDA(ctx, cudaMemcpy(const_cast<double *>(ctx->g.lsq), lsqs.data(), sizeof(double) * lsqs.size(),
+                                 cudaMemcpyHostToDevice));
+    }
+    if (prm->viscousType) {
+        const std::vector<uint8_t> vref = viscous_flags(h, ctx->geom, prm->skewnessAngle, prm->turbSkewnessAngle);
+        std::vector<uint8_t> vflag(nf);
+        for (int fs = 0; fs < nf; ++fs) vflag[fs] = vref[ctx->forder[fs]];
+        PHX_CUDA(ctx, cudaMemcpy(const_cast<uint8_t *>(ctx->g.vflag), vflag.data(), nf, cudaMemcpyHostToDevice));
+    }
+    if (avg_vol > 0.0) {
+        // the Venkatakrishnan threshold scales with the average cell volume of all zones
+        const double K = prm->venkatCoeff;
+        double kt = K * K * K;
+        kt *= 1.0 / std::pow(std::pow(avg_vol, 1.0 / 3.0), 3.0);
+        ctx->nc.venkatK3 = kt;
+        ctx->g.avgVol = avg_vol;
+    }
+    return PHX_OK;
+}
+
+int phx_set_halo(phx_ctx *ctx, int64_t n_send, const int32_t *send_cells, int64_t n_recv, const int32_t *recv_bfaces)
+{
+    if (!ctx || n_send < 0 || n_recv < 0 || (n_send > 0 && !send_cells) || (n_recv > 0 && !recv_bfaces))
+        return PHX_ERR_ARG;
+    if (!ctx->hasInterface) return fail(ctx, PHX_ERR_STATE, "the grid has no interface faces");
+    if (n_send > ctx->nCell || n_recv > ctx->nBFace) return PHX_ERR_ARG;
+    std::vector<int> snd((size_t)n_send), rcv((size_t)n_recv);
+    for (int64_t i = 0; i < n_send; ++i) {
+        if (send_cells[i] < 0 || send_cells[i] >= ctx->nCell) return fail(ctx, PHX_ERR_ARG, "phx_set_halo: bad cell");
+        snd[i] = ctx->rankOf[send_cells[i]];
+    }
+    for (int64_t i = 0; i < n_recv; ++i) {
+        const int f = recv_bfaces[i];
+        if (f < 0 || f >= ctx->nBFace || !ctx->itfFace[f])
+            return fail(ctx, PHX_ERR_ARG, "phx_set_halo: not an interface face");
+        rcv[i] = ctx->nCell + ctx->bfacePos[f];
+    }
+    int rc = 0;
+    const int *ds = nullptr, *dr = nullptr;
+    if (n_send > 0) rc |= upload(ctx, &ds, snd);
+    if (n_recv > 0) rc |= upload(ctx, &dr, rcv);
+    if (rc) return rc < 0 ? rc : PHX_ERR_CUDA;
+    ctx->haloSend = const_cast<int *>(ds);
+    ctx->haloRecv = const_cast<int *>(dr);
+    ctx->nHaloSend = (int)n_send;
+    ctx->nHaloRecv = (int)n_recv;
+    return PHX_OK;
+}
+
+static bool halo_field_ok(const phx_ctx *ctx, int field)
+{
+    if (field == PHX_HALO_TURB || field == PHX_HALO_TURB_DQ) return ctx->sa;
+    return field >= PHX_HALO_Q && field <= PHX_HALO_DQ;
+}
+
+int64_t phx_halo_row_bytes(const phx_ctx *ctx, int field)
+{
+    if (!ctx || !halo_field_ok(ctx, field)) return PHX_ERR_ARG;
+    return (int64_t)(ctx->mixed ? halo_row_bytes<float>(field) : halo_row_bytes<double>(field));
+}
+
+int phx_halo_pack(phx_ctx *ctx, int field, void *buf_dev)
+{
+    if (!ctx || !halo_field_ok(ctx, field) || (ctx->nHaloSend > 0 && !buf_dev)) return PHX_ERR_ARG;
+    if (!ctx->hasInterface) return fail(ctx, PHX_ERR_STATE, "the grid has no interface faces");
+    unsigned char *b = static_cast<unsigned char *>(buf_dev);
+    if (ctx->mixed)
+        launch_halo_pack<float>(ctx->g, field, ctx->q64[ctx->cur], ctx->w32, ctx->t32, ctx->haloSend, ctx->nHaloSend,
+                                b, ctx->stream);
+    else
+        launch_halo_pack<double>(ctx->g, field, ctx->q64[ctx->cur], ctx->w64, ctx->t64, ctx->haloSend,
+                                 ctx->nHaloSend, b, ctx->stream);
+    return check_launch(ctx, ctx->nHaloSend > 0 ? 1 : 0);
+}
+
+int phx_halo_unpack(phx_ctx *ctx, int field, const void *buf_dev)
+{
+    if (!ctx || !halo_field_ok(ctx, field) || (ctx->nHaloRecv > 0 && !buf_dev)) return PHX_ERR_ARG;
+    if (!ctx->hasInterface) return fail(ctx, PHX_ERR_STATE, "the grid has no interface faces");
+    const unsigned char *b = static_cast<const unsigned char *>(buf_dev);
+    if (ctx->mixed)
+        launch_halo_unpack<float>(ctx->g, ctx->nc, field, ctx->q64[ctx->cur], ctx->w32, ctx->t32, ctx->haloRecv,
+                                  ctx->nHaloRecv, b, ctx->stream);
+    else
+        launch_halo_unpack<double>(ctx->g, ctx->nc, field, ctx->q64[ctx->cur], ctx->w64, ctx->t64, ctx->haloRecv,
+                                   ctx->nHaloRecv, b, ctx->stream);
+    return check_launch(ctx, ctx->nHaloRecv > 0 ? 1 : 0);
+}
+
+int phx_ns_min_timestep(phx_ctx *ctx, double *out)
+{
+    if (!ctx || !out) return PHX_ERR_ARG;
+    if (!ctx->haveResidual) return fail(ctx, PHX_ERR_STATE, "phx_ns_min_timestep needs phx_ns_residual first");
+    unsigned long long bits = 0;
+    PHX_CUDA(ctx, cudaMemcpyAsync(&bits, &ctx->red->mindt_bits, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    double v;
+    std::memcpy(&v, &bits, sizeof(v));
+    *out = v;
+    return PHX_OK;
+}
+
+int phx_ns_set_min_timestep(phx_ctx *ctx, double value)
+{
+    if (!ctx || !(value > 0.0)) return PHX_ERR_ARG;
+    unsigned long long bits;
+    std::memcpy(&bits, &value, sizeof(bits));
+    PHX_CUDA(ctx, cudaMemcpyAsync(&ctx->red->mindt_bits, &bits, sizeof(bits), cudaMemcpyHostToDevice, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PHX_OK;
+}
+
+int phx_step_status(phx_ctx *ctx)
+{
+    if (!ctx) return PHX_ERR_ARG;
+    int err = 0;
+    PHX_CUDA(ctx, cudaMemcpyAsync(&err, &ctx->red->error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (err != 0) {
+        PHX_CUDA(ctx, cudaMemsetAsync(&ctx->red->error, 0, sizeof(int), ctx->stream));
+        PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    if (err == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
+    if (err == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
     return PHX_OK;
 }
 

@@ -31,6 +31,8 @@ enum BcKind : int32_t {
     BK_WALL = 1,       // ViscousAdiabaticWallBCRegion
     BK_FARFIELD = 2,   // FarfieldBCRegion
     BK_EXTRAP = 3,     // OutflowBCRegion / extrapolation
+    BK_INTERFACE = 4,  // a face cut by a partition (PHENGLEI::INTERFACE): the ghost is the neighbouring part's
+                       // cell, filled by halo exchanges; every pass but the boundary treats the face as interior
 };
 
 // Record strides (elements).
@@ -142,13 +144,14 @@ struct NsConst {
 template <class T>
 struct Work {
     T *qrec;        // [nTotal][kQ] working state, c2 = |gamma p / rho|, total enthalpy, limiter
-    T *grec;        // [nCell][kG] primitive gradients
+    T *grec;        // [nTotal][kG] primitive gradients (ghost rows: interface ghosts only, from the halo exchange)
     T *flux;        // [nFace][kFlux] face flux times area and inviscid spectral radius term
     T *coef;        // [2 nFace][kCoef] LU-SGS factors of each face use (side 0: the left cell's view)
     T *crec;        // [nCell][kC] residual, diagonal, spectral radii
     T *dtraw;       // [nCell] CFL * vol / spectral radius, before the ktmax clamp
     T *dqrec;       // [nTotal][kD] LU-SGS dq (backward sweep; write-once per sweep)
-    T *dqfwd;       // [nCell][kD] forward-sweep dq (write-once per sweep)
+    T *dqfwd;       // [nTotal][kD] forward-sweep dq (write-once per sweep; ghost rows: interface ghosts, from
+                    // the halo exchange between the sweeps)
     T *dflux;       // [nCell][kD] delta flux carried from the forward to the backward sweep (write-once)
     T *trec;        // [nTotal][kTr] SA variable, eddy and laminar viscosity (SA runs; else null)
     T *nrec;        // [nNode][kN] GG-node node values (GG-node runs; else null)
@@ -163,7 +166,7 @@ struct TurbWork {
     T *tface;       // [nFace][kTf] face terms
     T *tcoef;       // [2 nFace] LU-SGS matrix of each face use (side 0: left cell's view = mat_turbr)
     T *tdq;         // [nCell] LU-SGS dq (backward sweep; write-once per sweep)
-    T *tdqf;        // [nCell] forward-sweep dq (write-once per sweep)
+    T *tdqf;        // [nTotal] forward-sweep dq (write-once per sweep; interface ghosts from the halo exchange)
     T *tdfl;        // [nCell] forward delta flux (write-once per sweep)
     T *tsrc;        // [nCell] source computed by the learned-source kernel (sa_source != 0)
     T *qtnode;      // [nNode] GG-node node values of nu~ for the next SA gradient (GG-node runs; else null)
@@ -183,8 +186,12 @@ template <class T>
 void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &w, int nodePrev, cudaStream_t s);
 template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s);
+// LU-SGS sweeps: bit 0 of `sweeps` runs the forward sweep (after resetting
+// the sweep records), bit 1 the backward sweep; 3 runs both in one launch.
+constexpr int kSweepForward = 1, kSweepBackward = 2, kSweepBoth = 3;
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s);
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s,
+                 int sweeps = kSweepBoth);
 template <class T>
 void launch_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const double *q64, double *q64_new,
                    Reduce *red, int *neglist, int numSMs, cudaStream_t s);
@@ -231,7 +238,7 @@ template <class T>
 void launch_turb_node_values(const DevGrid &g, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s);
 template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
-                    int numSMs, cudaStream_t s);
+                    int numSMs, cudaStream_t s, int sweeps = kSweepBoth);
 template <class T>
 void launch_sa_update(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, cudaStream_t s);
 // Wall force sums (16 doubles, the last zero) of the current state.
@@ -242,5 +249,17 @@ void launch_forces(const DevGrid &g, const NsConst &c, const Work<T> &w, const d
 template <class T>
 void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t, const Work<T> &w, cudaStream_t s);
 void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s);
+// Halo exchange of a partitioned grid (phx_halo.cu): pack gathers rows of
+// the cells `send` (storage indices) into buf, unpack scatters rows of buf
+// into the ghosts `recv` (storage indices); `field` is a PHX_HALO_* code and
+// a row holds halo_row_bytes<T>(field) bytes.
+template <class T>
+size_t halo_row_bytes(int field);
+template <class T>
+void launch_halo_pack(const DevGrid &g, int field, const double *q64, const Work<T> &w, const TurbWork<T> &t,
+                      const int *send, int n, unsigned char *buf, cudaStream_t s);
+template <class T>
+void launch_halo_unpack(const DevGrid &g, const NsConst &c, int field, double *q64, const Work<T> &w,
+                        const TurbWork<T> &t, const int *recv, int n, const unsigned char *buf, cudaStream_t s);
 
 }  // namespace phx

@@ -21,7 +21,9 @@ namespace phx {
 // Boundary: ghost-cell state per boundary face (NSSolverUnstruct::Boundary,
 // NSSolverUnstruct.cpp:13404-13515): SymmetryBCRegion (:19413),
 // ViscousAdiabaticWallBCRegion (:20988), FarfieldBCRegion (:21195).
-// Computed in FP64 from the FP64 master state.
+// Computed in FP64 from the FP64 master state.  Interface ghosts keep the
+// state the last halo exchange gave them (Boundary skips INTERFACE faces,
+// :13474); their working record and laminar viscosity are formed from it.
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c, double *q, Work<T> w,
@@ -37,7 +39,10 @@ __global__ void __launch_bounds__(kThreads) boundary_kernel(DevGrid g, NsConst c
     const double xn = fr[0], yn = fr[1], zn = fr[2];
     double o[5] = {r, u, v, wv, p};
     const int kind = g.bkind[f];
-    if (kind == BK_SYMMETRY) {
+    if (kind == BK_INTERFACE) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) o[k] = q[k * nt + re];
+    } else if (kind == BK_SYMMETRY) {
         const double vn = xn * u + yn * v + zn * wv;
         o[1] = u - 2.0 * xn * vn;
         o[2] = v - 2.0 * yn * vn;
@@ -263,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) gradient_limiter_kernel(DevGrid g, N
                 else { gx[k] -= qf[k] * nx; gy[k] -= qf[k] * ny; gz[k] -= qf[k] * nz; }
             }
         }
-        if (f >= g.nBFace) {
+        if (f >= g.nBFace || ld(g.bkind + f) == BK_INTERFACE) {   // MinMaxDiff reads interface ghosts
             rmin = tmin(rmin, qn[0]); rmax = tmax(rmax, qn[0]);
             pmin = tmin(pmin, qn[4]); pmax = tmax(pmax, qn[4]);
         }
@@ -405,15 +410,16 @@ __device__ __forceinline__ void lusgs_coef(const T *qc, const T *qn, T nx, T ny,
     o[3] = T(0);
 }
 
-// MUSCL state of one side (ghost cells carry a zero gradient, so their state
-// is used as is).
+// MUSCL state of one side (boundary ghosts carry a zero gradient, so their
+// state is used as is; an interface ghost has the neighbouring zone's
+// gradient, limiter and centre, and is reconstructed like a cell).
 template <class T>
 __device__ __forceinline__ void reconstruct(const DevGrid &g, const Work<T> &w, int cell, const double *fc, T lim,
-                                            const T *qs, T *qo)
+                                            const T *qs, T *qo, bool interfaceGhost = false)
 {
 #pragma unroll
     for (int k = 0; k < 5; ++k) qo[k] = qs[k];
-    if (cell >= g.nCell) return;
+    if (cell >= g.nCell && !interfaceGhost) return;
     double xc[4];
     ld4(g.xrec + (size_t)cell * kX, xc);
     const T dx = (T)(fc[0] - xc[0]), dy = (T)(fc[1] - xc[1]), dz = (T)(fc[2] - xc[2]);
@@ -431,13 +437,14 @@ __device__ __forceinline__ void reconstruct(const DevGrid &g, const Work<T> &w, 
 }
 
 // Gradients of u, v, w (9 values) and of the temperature (3) of one side of
-// a face; a ghost has the owner's gradient (least squares, GG-node) or none
-// (GG-cell), as the reference's gradient routines leave them.
+// a face; a boundary ghost has the owner's gradient (least squares, GG-node)
+// or none (GG-cell), as the reference's gradient routines leave them; an
+// interface ghost has the neighbouring zone's.
 template <class T>
 __device__ __forceinline__ void side_gradients(const DevGrid &g, const NsConst &c, const Work<T> &w, int cell,
-                                               int owner, T *gv, T *gt)
+                                               int owner, T *gv, T *gt, bool interfaceGhost = false)
 {
-    const int src = cell < g.nCell ? cell : (c.gradient != 0 ? owner : -1);
+    const int src = (cell < g.nCell || interfaceGhost) ? cell : (c.gradient != 0 ? owner : -1);
     if (src < 0) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) gv[k] = T(0);
@@ -466,7 +473,10 @@ template <class T>
 __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c, const Work<T> &w, int f, int le,
                                              int re, const double *fr, const T *qL, const T *qR, T *fv, T &vspec)
 {
-    const bool bnd = f < g.nBFace;
+    // interface faces are interior faces here (FaceWeight, Geo_UnstructGrid.cpp:2475;
+    // GetVisFaceValue and ComputeVisflux, NSSolverUnstruct.cpp:7292, :13261)
+    const bool itf = f < g.nBFace && g.bkind[f] == BK_INTERFACE;
+    const bool bnd = f < g.nBFace && !itf;
     const bool wall = bnd && g.bkind[f] == BK_WALL;
     double xl[4], xr[4];
     ld4(g.xrec + (size_t)le * kX, xl);
@@ -510,7 +520,7 @@ __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c,
     const int vf = g.vflag[f];
     T gvl[9], gtl[3], gvr[9], gtr[3];
     side_gradients<T>(g, c, w, le, le, gvl, gtl);
-    side_gradients<T>(g, c, w, re, le, gvr, gtr);
+    side_gradients<T>(g, c, w, re, le, gvr, gtr, itf);
     T f1[3] = {qL[1], qL[2], qL[3]}, f2[3] = {qR[1], qR[2], qR[3]};
     T tL = tl0, tR = tr0;
     T fm[3];
@@ -597,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
         for (int k = 0; k < 5; ++k) { ql[k] = qL[k]; qr[k] = qR[k]; }
     } else {
         reconstruct<T>(g, w, le, fr + 4, limL, qL, ql);
-        reconstruct<T>(g, w, re, fr + 4, limR, qR, qr);
+        reconstruct<T>(g, w, re, fr + 4, limR, qR, qr, f < g.nBFace && g.bkind[f] == BK_INTERFACE);
     }
     const T xn = (T)fr[0], yn = (T)fr[1], zn = (T)fr[2], area = (T)fr[3];
     if (f < g.nBFace) {
@@ -893,12 +903,16 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     const int e1 = lead ? s.count : 0;
     const bool has = live && s.nb >= 0;
     // wait for the inputs other positions write: the neighbour's dq (forward:
-    // its forward dq; backward: its final dq; a ghost's comes from this cell's
-    // forward dq) and, backward, this cell's forward delta flux
+    // its forward dq; backward: its final dq; a boundary ghost's comes from
+    // this cell's forward dq) and, backward, this cell's forward delta flux.
+    // An interface ghost holds the neighbouring zone's forward dq, set by the
+    // halo exchange between the sweeps (SetGhostDQLUSGS leaves it to
+    // CommunicationDQ, Controller.cpp:1917-1924).
     const bool ghost = !kForward && has && s.nb >= nc;
+    const bool itfGhost = ghost && s.kind == BK_INTERFACE;
     const T *src1 = !has ? nullptr
-                         : ghost ? w.dqfwd + (size_t)cell * kD
-                                 : (kForward ? w.dqfwd : w.dqrec) + (size_t)s.nb * kD;
+                         : (ghost && !itfGhost) ? w.dqfwd + (size_t)cell * kD
+                                                : (kForward || itfGhost ? w.dqfwd : w.dqrec) + (size_t)s.nb * kD;
     const T *src2 = (!kForward && lead && lane == 0) ? w.dflux + (size_t)cell * kD : nullptr;
     T v1[5], fl[5];
     bool r1 = !src1 || poll5(src1, v1);
@@ -946,7 +960,7 @@ __device__ __forceinline__ bool sweep_position(const DevGrid &g, const NsConst &
     T df[5] = {0, 0, 0, 0, 0};
     if (has) {
         T dq[5];
-        if (ghost) {
+        if (ghost && !itfGhost) {
             ghost_dq<T>(s.kind, s.nx, s.ny, s.nz, gs, v1, dq);
         } else {
 #pragma unroll
@@ -1061,7 +1075,8 @@ __device__ __forceinline__ bool sweep_all(const DevGrid &g, const NsConst &c, co
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red)
+__global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst c, Work<T> w, Reduce *red,
+                                                              int sweeps)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kSweepLanes, lane = tid % kSweepLanes;   // slot lane group
@@ -1069,8 +1084,9 @@ __global__ void __launch_bounds__(kSweepThreads) lusgs_kernel(DevGrid g, NsConst
     const int wgroup0 = group & ~(kSweepSlots - 1);   // first group of this warp
     const int base = (threadIdx.x & 31) & ~(kSweepLanes - 1);
     const double mindt = __longlong_as_double((long long)red->mindt_bits);
-    if (!sweep_all<T, true>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base)) return;
-    sweep_all<T, false>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base);
+    if ((sweeps & kSweepForward) && !sweep_all<T, true>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base))
+        return;
+    if (sweeps & kSweepBackward) sweep_all<T, false>(g, c, w, red, mindt, group, wgroup0, ngroups, lane, base);
 }
 
 // Fills the sweep's output records (forward dq, forward delta flux, final dq)
@@ -1111,7 +1127,8 @@ static int sweep_blocks(K kernel, int &perSM, const DevGrid &g, int numSMs)
 }
 
 template <class T>
-int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s)
+int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, int numSMs, cudaStream_t s,
+                 int sweeps)
 {
     // residency of the cooperative launch, per device (a process may drive several)
     static int perSMcache[kMaxDevices][2];
@@ -1126,12 +1143,14 @@ int launch_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *r
     const int blocks = sweep_blocks(lusgs_kernel<T>, perSMcache[dev][sizeof(T) == 8 ? 0 : 1], g, numSMs);
     const long long quads = (long long)g.nCell * kD / 4;
     const int rb = (int)std::min<long long>((quads + kThreads - 1) / kThreads, (long long)numSMs * 16);
-    sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, w.dqfwd, w.dflux, w.dqrec);
+    if (sweeps & kSweepForward)
+        sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, w.dqfwd, w.dflux, w.dqrec);
     DevGrid gg = g;
     NsConst cc = c;
     Work<T> ww = w;
     Reduce *rr = red;
-    void *args[] = {&gg, &cc, &ww, &rr};
+    int sw = sweeps;
+    void *args[] = {&gg, &cc, &ww, &rr, &sw};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((void *)lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
@@ -1417,7 +1436,8 @@ void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream
     template void launch_gradient_limiter<T>(const DevGrid &, const NsConst &, const Work<T> &, int, cudaStream_t); \
     template void launch_residual<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, double,           \
                                      cudaStream_t);                                                                 \
-    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t);   \
+    template int launch_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, Reduce *, int, cudaStream_t,   \
+                                 int);                                                                             \
     template void launch_boundary_post<T>(const DevGrid &, const NsConst &, double *, const Work<T> &,           \
                                           cudaStream_t);                                                            \
     template void launch_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const double *, double *,     \

@@ -35,6 +35,9 @@ __global__ void __launch_bounds__(kThreads) sa_boundary_kernel(DevGrid g, NsCons
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nBFace) return;
     const int nt = g.nTotal;
+    // interface ghosts keep nu~ and the eddy viscosity of the last halo
+    // exchange (TurbSolverUnstr::Boundary skips INTERFACE faces)
+    if (g.bkind[f] == BK_INTERFACE) return;
     const int le = g.lr[f].x, re = g.nCell + f;
     T *tl = w.trec + (size_t)le * kTr;
     T *tg = w.trec + (size_t)re * kTr;
@@ -204,7 +207,9 @@ __global__ void __launch_bounds__(kThreads) sa_face_kernel(DevGrid g, NsConst c,
     if (f >= g.nFace) return;
     const int2 lr = ld(g.lr + f);
     const int le = lr.x, re = lr.y;
-    const bool bnd = f < g.nBFace;
+    // interface faces are interior faces for the face states and face values
+    // (TurbSolverUnstr.cpp:5041, :5125, :3950, :4569)
+    const bool bnd = f < g.nBFace && g.bkind[f] != BK_INTERFACE;
     const int bt = bnd ? g.btype[f] : 0;
     double fr[8];
     ld8(g.frec + (size_t)f * kF, fr);
@@ -407,8 +412,10 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
 // the face matrices of each face use.  Same dataflow schedule, write-once
 // records and bounded waits as the NS sweep (phx_kernels.cu): tdqf (forward
 // dq), tdfl (forward delta flux) and tdq (final dq) hold the sentinel until
-// written.  dq of the ghosts is the ghost residual, which is zero, so ghost
-// entries of the backward sweep add nothing and are skipped.
+// written.  dq of a boundary ghost is the ghost residual, which is zero, so
+// those entries of the backward sweep add nothing and are skipped; an
+// interface ghost holds the neighbouring zone's forward dq, set by the halo
+// exchange between the sweeps, and is read like a cell's.
 // ---------------------------------------------------------------------------
 // Static inputs of one slot for one lane (loaded a round ahead): neighbour
 // (-1: none or a ghost), its face matrix, and (lane 0 of the cell's first
@@ -426,7 +433,7 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
     s.cell = info.x;
     s.count = info.y;
     s.nb = -1;
-    if (info.x >= 0 && en.x >= 0 && en.x < g.nCell) {
+    if (info.x >= 0 && en.x >= 0 && (en.x < g.nCell || ld(g.bkind + (en.x - g.nCell)) == BK_INTERFACE)) {
         s.nb = en.x;
         s.mat = t.tcoef[en.z];
     }
@@ -440,16 +447,17 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
 
 template <class T, bool kForward>
 __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *red, const SaSweepIn<T> &s, int lane,
-                                                  int base, long long spinLimit)
+                                                  int base, long long spinLimit, int nCell)
 {
     const int cell = s.cell;
     const bool live = cell >= 0;
     const bool lead = live && s.count >= 0;   // the cell's first slot
     const int e1 = lead ? s.count : 0;
     const bool has = live && s.nb >= 0;
-    // the neighbour's dq (forward: its forward dq; backward: its final dq)
-    // and, backward, this cell's forward delta flux
-    const T *src1 = has ? (kForward ? t.tdqf : t.tdq) + s.nb : nullptr;
+    // the neighbour's dq (forward: its forward dq; backward: its final dq,
+    // or an interface ghost's forward dq) and, backward, this cell's forward
+    // delta flux
+    const T *src1 = has ? (kForward || s.nb >= nCell ? t.tdqf : t.tdq) + s.nb : nullptr;
     const T *src2 = (!kForward && lead && lane == 0) ? t.tdfl + cell : nullptr;
     T v1 = T(0), fl = T(0);
     bool r1 = true, r2 = true;
@@ -520,7 +528,7 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
         SaSweepIn<T> nxt;
         sa_sweep_load<T>(g, t, info, en, lane, nxt);
         entry(p + 2 * ngroups, info, en);
-        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base, spinLimit)) return false;
+        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base, spinLimit, g.nCell)) return false;
         if (en.x >= 0 && en.x < g.nCell) prefetch_l2(t.tcoef + en.z);
         if (lane == 0 && info.x >= 0 && info.y >= 0) prefetch_l2(t.tcrec + (size_t)info.x * kTc);
         cur = nxt;
@@ -531,15 +539,16 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
 
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads) sa_lusgs_kernel(DevGrid g, TurbWork<T> t, Reduce *red,
-                                                                 long long spinLimit)
+                                                                 long long spinLimit, int sweeps)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = tid / kSweepLanes, lane = tid % kSweepLanes;
     const int ngroups = (gridDim.x * blockDim.x) / kSweepLanes;
     const int wgroup0 = group & ~(kSweepSlots - 1);
     const int base = (threadIdx.x & 31) & ~(kSweepLanes - 1);
-    if (!sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit)) return;
-    sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit);
+    if ((sweeps & kSweepForward) && !sa_sweep_all<T, true>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit))
+        return;
+    if (sweeps & kSweepBackward) sa_sweep_all<T, false>(g, t, red, group, wgroup0, ngroups, lane, base, spinLimit);
 }
 
 // Fills the SA sweep's output records with the sentinel.
@@ -556,7 +565,7 @@ __global__ void __launch_bounds__(kThreads) sa_sweep_reset_kernel(int n, T *a, T
 
 template <class T>
 int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const TurbWork<T> &t, Reduce *red,
-                    int numSMs, cudaStream_t s)
+                    int numSMs, cudaStream_t s, int sweeps)
 {
     (void)w;
     // residency of the cooperative launch, per device (a process may drive several)
@@ -591,12 +600,14 @@ int launch_sa_lusgs(const DevGrid &g, const NsConst &c, const Work<T> &w, const 
     }
     if (blocks < 1) blocks = 1;
     const int rb = std::min((g.nCell + kThreads - 1) / kThreads, numSMs * 16);
-    sa_sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, t.tdqf, t.tdfl, t.tdq);
+    if (sweeps & kSweepForward)
+        sa_sweep_reset_kernel<T><<<rb > 0 ? rb : 1, kThreads, 0, s>>>(g.nCell, t.tdqf, t.tdfl, t.tdq);
     DevGrid gg = g;
     TurbWork<T> tt = t;
     Reduce *rr = red;
     long long lim = c.spinLimit;
-    void *args[] = {&gg, &tt, &rr, &lim};
+    int sw = sweeps;
+    void *args[] = {&gg, &tt, &rr, &lim, &sw};
     const cudaError_t e =
         cudaLaunchCooperativeKernel((void *)sa_lusgs_kernel<T>, dim3(blocks), dim3(kSweepThreads), args, 0, s);
     return e == cudaSuccess ? 0 : (int)e;
@@ -644,7 +655,7 @@ void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t
                                         const TurbWork<T> &, Reduce *, const MlpDev *, unsigned long long *, int, \
                                         cudaStream_t);                                                            \
     template int launch_sa_lusgs<T>(const DevGrid &, const NsConst &, const Work<T> &, const TurbWork<T> &,       \
-                                    Reduce *, int, cudaStream_t);                                                 \
+                                    Reduce *, int, cudaStream_t, int);                                            \
     template void launch_sa_update<T>(const DevGrid &, const NsConst &, const Work<T> &, const TurbWork<T> &,     \
                                       cudaStream_t);                                                              \
     template void launch_turb_node_values<T>(const DevGrid &, const Work<T> &, const TurbWork<T> &, cudaStream_t); \

@@ -24,6 +24,8 @@ PHX_Q, PHX_RES, PHX_DT, PHX_LIMIT, PHX_GRADX, PHX_GRADY, PHX_GRADZ, PHX_DQ, PHX_
 PHX_Q_TURB, PHX_VISL, PHX_VIST, PHX_RES_TURB = 10, 11, 12, 13
 PHX_SA_SRC = 15
 PHX_GRAD_TURB = 16
+# halo fields of a partitioned grid (include/phx.h PHX_HALO_*)
+PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB, PHX_HALO_TURB_DQ = range(5)
 ERRORS = {-1: "PHX_ERR_ARG", -2: "PHX_ERR_CUDA", -3: "PHX_ERR_TIMEOUT", -4: "PHX_ERR_NUMERIC", -5: "PHX_ERR_STATE"}
 
 _dp = C.POINTER(C.c_double)
@@ -80,8 +82,18 @@ def lib() -> C.CDLL:
         _lib.phx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         for name in ("phx_ns_boundary", "phx_ns_gradient_limiter", "phx_ns_residual", "phx_ns_lusgs",
                      "phx_ns_update", "phx_ctx_destroy", "phx_launch_count", "phx_get_step", "phx_sa_boundary",
-                     "phx_sa_residual", "phx_sa_lusgs", "phx_sa_update"):
+                     "phx_sa_residual", "phx_sa_lusgs", "phx_sa_update", "phx_ns_lusgs_forward",
+                     "phx_ns_lusgs_backward", "phx_sa_lusgs_forward", "phx_sa_lusgs_backward", "phx_step_status"):
             getattr(_lib, name).argtypes = [C.c_void_p]
+        _lib.phx_swap_geometry.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_double]
+        _lib.phx_set_halo.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
+        _lib.phx_halo_row_bytes.argtypes = [C.c_void_p, C.c_int]
+        _lib.phx_halo_row_bytes.restype = C.c_int64
+        _lib.phx_halo_pack.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.phx_halo_unpack.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.phx_ns_min_timestep.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        _lib.phx_ns_set_min_timestep.argtypes = [C.c_void_p, C.c_double]
         _lib.phx_set_step.argtypes = [C.c_void_p, C.c_int]
         _lib.phx_residual_norm.argtypes = [C.c_void_p, C.c_void_p]
         _lib.phx_forces.argtypes = [C.c_void_p, C.c_void_p]
@@ -265,6 +277,63 @@ class NSSolverUnstruct:
 
     def TurbUpdateFlowField(self):
         self._check(lib().phx_sa_update(self.h), "phx_sa_update")
+
+    # -- one zone of a partitioned grid (interface faces) ----------------------
+    def LUSGSForward(self):
+        """SolveLUSGSForward (NSSolverUnstruct.cpp:15118); the dq exchange follows."""
+        self._check(lib().phx_ns_lusgs_forward(self.h), "phx_ns_lusgs_forward")
+
+    def LUSGSBackward(self):
+        """SolveLUSGSBackward (NSSolverUnstruct.cpp:15446), after the dq exchange."""
+        self._check(lib().phx_ns_lusgs_backward(self.h), "phx_ns_lusgs_backward")
+
+    def TurbLUSGSForward(self):
+        self._check(lib().phx_sa_lusgs_forward(self.h), "phx_sa_lusgs_forward")
+
+    def TurbLUSGSBackward(self):
+        self._check(lib().phx_sa_lusgs_backward(self.h), "phx_sa_lusgs_backward")
+
+    def SwapGeometry(self, bfaces, xcc, ycc, zcc, vol, avg_vol: float = 0.0):
+        """Region::SwapGeometry / ComputeGlobalGridSize: the neighbouring zones'
+        cell centres and volumes behind the interface faces `bfaces`, and the
+        average cell volume over all zones (0: keep this zone's)."""
+        b = np.ascontiguousarray(bfaces, np.int32)
+        x, y, z, v = (np.ascontiguousarray(a, np.float64) for a in (xcc, ycc, zcc, vol))
+        if not (len(b) == len(x) == len(y) == len(z) == len(v)):
+            raise ValueError("one centre and volume per interface face")
+        self._check(lib().phx_swap_geometry(self.h, len(b), b.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                            z.ctypes.data, v.ctypes.data, float(avg_vol)), "phx_swap_geometry")
+
+    def set_halo(self, send_cells, recv_bfaces):
+        """The halo plan: cells whose rows this zone sends, interface faces whose
+        ghosts it fills (each concatenated over the neighbours)."""
+        sc = np.ascontiguousarray(send_cells, np.int32)
+        rb = np.ascontiguousarray(recv_bfaces, np.int32)
+        self._check(lib().phx_set_halo(self.h, len(sc), sc.ctypes.data, len(rb), rb.ctypes.data), "phx_set_halo")
+
+    def halo_row_bytes(self, field: int) -> int:
+        n = int(lib().phx_halo_row_bytes(self.h, field))
+        if n < 0:
+            raise PhxError(f"phx_halo_row_bytes: {ERRORS.get(n, n)}")
+        return n
+
+    def halo_pack(self, field: int, buf_ptr: int):
+        self._check(lib().phx_halo_pack(self.h, field, C.c_void_p(buf_ptr)), "phx_halo_pack")
+
+    def halo_unpack(self, field: int, buf_ptr: int):
+        self._check(lib().phx_halo_unpack(self.h, field, C.c_void_p(buf_ptr)), "phx_halo_unpack")
+
+    def min_timestep(self) -> float:
+        v = C.c_double()
+        self._check(lib().phx_ns_min_timestep(self.h, C.byref(v)), "phx_ns_min_timestep")
+        return v.value
+
+    def set_min_timestep(self, value: float):
+        self._check(lib().phx_ns_set_min_timestep(self.h, float(value)), "phx_ns_set_min_timestep")
+
+    def status(self):
+        """Raises PhxError if a sweep's wait ran out or the repair overflowed."""
+        self._check(lib().phx_step_status(self.h), "phx_step_status")
 
     # -- learned SA source --------------------------------------------------------
     def capture_sa_samples(self):
