@@ -10,9 +10,15 @@ resident in HBM (CUDA events on the library's stream, max over ranks);
 host memory: every step uploads the primitive state, runs the iteration and
 downloads the updated state and the residual monitor.
 
-Multi-GPU: the path is not partitioned in this release (one zone per GPU);
-N ranks run N independent replicas of the same workload ("replicas only"),
-each timed on its own device, and `value` sums their throughput.
+Multi-GPU (N ranks, one per GPU): domain decomposition with weak scaling.
+Rank r builds zone r of a channel N times the workload's length (the
+workload's own mesh per rank, its x extent and cell count times N for the
+whole job), with interface faces at the cuts, and steps it phase by phase with
+the reference's halo exchanges (phenlei_b200.zones): NCCL point-to-point halos
+and all-reduces.  `value` is all ranks' cells x steps over the slowest rank's
+device time.  With fewer GPUs than ranks (the halo path on one GPU) the ranks
+share it and the rows go through gloo on the host.  Workloads that are not a
+channel split their one mesh into N zones instead (strong scaling).
 
 `--impl reference` times the CPU restatement of the reference path
 (oracle/, single-threaded, the reference's LU-SGS is sequential) on a bounded
@@ -52,6 +58,7 @@ def workloads():
         # Config-5 mesh size and flow Mach number, inviscid physics.
         "transonic_bump_euler_16M": dict(
             mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001),
+            channel=dict(nx=1024, ny=92, nz=128, thickness=0.08, length=3.0, wall_spacing=0.001),
             params=dict(cases.EULER_BUMP, refMachNumber=0.8, CFLEnd=20.0),
             desc="3-D transonic channel bump 8% thick, 1024x92x128 hex (12.06M cells), M=0.8, Roe+Venkat, "
                  "GG-cell, LU-SGS CFL 20, inviscid"),
@@ -60,12 +67,14 @@ def workloads():
         "transonic_bump_sa_16M": dict(
             mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001,
                                         prism_layers=30),
+            channel=dict(nx=1024, ny=92, nz=128, thickness=0.08, length=3.0, wall_spacing=0.001, prism_layers=30),
             params=dict(cases.SA_BUMP),
             wall_dist=True,
             desc="config 5: 3-D transonic channel bump 8% thick, 1024x92x128 with 30 prism layers at the walls "
                  "(15.99M hex+prism cells), M=0.8, Re=1e7, Spalart-Allmaras, Roe+Venkat, GG-cell, LU-SGS CFL 20"),
         "sa_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 92, 32, thickness=0.08, wall_spacing=0.001, prism_layers=30),
+            channel=dict(nx=256, ny=92, nz=32, thickness=0.08, length=3.0, wall_spacing=0.001, prism_layers=30),
             params=dict(cases.SA_BUMP),
             wall_dist=True,
             desc="SA channel bump 256x92x32 with 30 prism layers (1.0M hex+prism cells), M=0.8, Re=1e7"),
@@ -75,6 +84,7 @@ def workloads():
             desc="config 1: Euler channel bump 64x32x4 hex (8,192 cells), M=0.5"),
         "euler_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 128, 32),
+            channel=dict(nx=256, ny=128, nz=32),
             params=dict(cases.EULER_BUMP),
             desc="Euler channel bump 256x128x32 hex (1.05M cells), M=0.5"),
         # Config 2: 100^3 hexes x 6 jittered tetrahedra, laminar, least squares.
@@ -280,8 +290,6 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
     sampler.start()
     launches0 = s.launches
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        torch.distributed.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     hist = s.Relaxation(args.steps)
@@ -358,6 +366,193 @@ def run_phx(args, rank, world, precision, m, wd, e2e=True, mlp_blob=None, train=
                hist=hist, setup_s=setup_s, nt=s.nt, forces=forces, mlp=mlp_info, vist=vist, iters=iters)
     s.close()
     return res
+
+
+def run_zones(args, rank, world, precision, wl, zone, wd, mlp_blob=None, train=False, e2e=True):
+    """One arm of the multi-GPU run: this rank's zone stepped with the halo
+    exchanges (phenlei_b200.zones.DistributedZone); warm-up, then K timed
+    iterations between a barrier and a synchronize on both sides."""
+    import torch
+    import torch.distributed as dist
+
+    from phenlei_b200 import solver as S
+    from phenlei_b200.zones import DistributedZone
+
+    params = dict(wl["params"])
+    if mlp_blob is not None:
+        params["sa_source"] = "mlp_fallback"
+    t0 = time.time()
+    if zone is not None:
+        dz = DistributedZone(None, params, wall_dist=wd, precision=precision, part=zone)
+    else:
+        dz = DistributedZone(wl["mesh"](), params, wall_dist=wd, precision=precision)
+    z = dz.zones[0]
+    if mlp_blob is not None:
+        z.set_mlp_blob(mlp_blob)
+    setup_s = time.time() - t0
+    dz.iterate(args.warmup)
+    torch.cuda.synchronize()
+    early = z.capture_sa_samples()[:2] if train else None
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    launches0 = z.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    hist = dz.iterate(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = z.launches - launches0
+    clocks = sampler.stop()
+    timer = {}
+    reps = max(1, min(args.steps, 10))
+    dz.iterate(reps, timer=timer)
+    torch.cuda.synchronize()
+    phase_ms = {k: sum(a.elapsed_time(b) for a, b in v) / reps for k, v in timer.items()}
+    forces = dz.AirForceCoef() if params.get("viscousType", 0) > 0 else None
+    nc = z.mesh.n_cell
+    mlp_info = {"cells_learned": z.mlp_cells()} if mlp_blob is not None else None
+    if train:
+        # the learned source's training set, as on one GPU: every zone's
+        # samples after the warm-up and at the end, subsampled evenly over the
+        # (ln chi, ln s) plane to a share of the 2M samples, gathered on rank 0,
+        # which trains; the model goes to every rank
+        f, t, _, _ = z.capture_sa_samples()
+        f, t = np.concatenate([early[0], f]), np.concatenate([early[1], t])
+        f, t = balanced_subsample(f, t, 2_000_000 // world, seed=rank)
+        got = [None] * world
+        dist.all_gather_object(got, (f, t))
+        blob = [None]
+        info = [None]
+        if rank == 0:
+            f = np.concatenate([g[0] for g in got])
+            t = np.concatenate([g[1] for g in got])
+            t1 = time.perf_counter()
+            loss = z.train_sa_mlp(f, t, epochs=60, batch=8192, lr=1e-3, seed=0)
+            blob = [z.mlp_blob()]
+            info = [{"samples": int(len(t)), "epochs": 60, "batch": 8192, "final_loss": loss,
+                     "train_s": round(time.perf_counter() - t1, 2)}]
+        dist.broadcast_object_list(blob, src=0)
+        dist.broadcast_object_list(info, src=0)
+        mlp_info = dict(info[0], blob=blob[0])
+    e2e_s = None
+    if e2e:
+        # end to end through the public API: every step uploads this zone's
+        # primitive state from pinned host memory (and its interface ghosts
+        # from the neighbours), runs the iteration and reads the state back
+        qh = torch.empty((5, z.nt), dtype=torch.float64).pin_memory()
+        qh.copy_(torch.from_numpy(z.get(S.PHX_Q)))
+        lib = S.lib()
+        steps = max(1, min(args.steps, 20))
+        dist.barrier()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(steps):
+            z._check(lib.phx_set_state(z.h, S.PHX_Q, qh.data_ptr(), 5 * z.nt), "set_state")
+            dz._exchange_state()
+            dz.iterate(1)
+            z._check(lib.phx_get_state(z.h, S.PHX_Q, qh.data_ptr(), 5 * z.nt), "get_state")
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t1) / steps
+    out = dict(ms=ms, launches=launches, clocks=clocks, phase_ms=phase_ms, e2e_s=e2e_s, nc=nc, mesh=z.mesh,
+               hist=hist, setup_s=setup_s, nt=z.nt, forces=forces, mlp=mlp_info, iters=z.step,
+               cells_total=dz.n_cell_total)
+    dz.close()
+    return out
+
+
+def main_zones(args, rank, world, wl):
+    """bench.py --gpus N (N > 1): the workload decomposed into N zones."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from phenlei_b200 import mesh as M
+    from phenlei_b200.zones import channel_zone
+
+    ndev = torch.cuda.device_count()
+    torch.cuda.set_device(rank % max(ndev, 1))
+    backend = "nccl" if ndev >= world else "gloo"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    sa = wl["params"].get("viscousType", 0) == 3
+    if "channel" in wl:
+        # weak scaling: this rank's slab of a channel `world` times as long
+        ch = dict(wl["channel"])
+        nx, length = ch.pop("nx"), ch.pop("length", 3.0)
+        zone = channel_zone(rank, world, nx=nx * world, length=length * world, dz=length / nx, **ch)
+        # the zone's own walls: the wall distance of a cell near a cut can
+        # differ from the whole channel's (an input field, not a result)
+        wd = M.wall_distance(zone.mesh) if sa else None
+        scaling, layout = "weak", "channel %d x the workload's length, one %d-cell slab per rank" % (
+            world, zone.mesh.n_cell)
+    else:
+        zone, scaling = None, "strong"
+        wd = M.wall_distance(wl["mesh"]()) if sa else None
+        layout = "the workload's mesh split into %d slabs" % world
+    r64 = blob = None
+    if args.mlp_blob:
+        blob = np.load(args.mlp_blob).astype(np.float32)
+    if args.precision == "mixed" and not args.no_fp64_arm:
+        r64 = run_zones(args, rank, world, "fp64", wl, zone, wd, e2e=False,
+                        train=sa and not args.exact_source and blob is None)
+        if r64["mlp"]:
+            blob = r64["mlp"].pop("blob")
+    r = run_zones(args, rank, world, args.precision, wl, zone, wd, mlp_blob=blob)
+
+    def slowest(v):
+        t = torch.tensor([v], dtype=torch.float64, device="cuda" if backend == "nccl" else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = slowest(r["ms"])
+    e2e_s = slowest(r["e2e_s"])
+    ms64 = slowest(r64["ms"]) if r64 is not None else None
+    tot = r["cells_total"]
+    value = tot * args.steps / (ms / 1e3) / 1e6
+    peak, peak_kind = measured_peaks()
+    kb = kernel_bytes(r["mesh"], args.precision, wl["params"].get("viscousType", 0),
+                      wl["params"].get("gradientName", "ggcell"))
+    phase = r["phase_ms"]
+    dom = max(phase, key=phase.get)
+    achieved = kb[dom] / (phase[dom] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mcell-iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": scaling, "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded generated mesh, free-stream start)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "cells": tot, "cells_per_rank": r["nc"],
+                   "precision": args.precision, "layout": layout,
+                   "parallelism": "dp%d domain decomposition (interface halos over %s)" % (
+                       world, "NCCL" if backend == "nccl" else "gloo, host-staged: ranks share a GPU"),
+                   "l2": "inputs larger than L2 (state %.0f MB per rank)" % (5 * 8 * r["nt"] / 1e6)},
+        "gpu_launches": int(r["launches"]),
+        "phase_ms": {k: round(v, 4) for k, v in phase.items()},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "algorithmic_bytes": kb[dom],
+                     "traffic": None, "rank": 0},
+        "clocks": r["clocks"],
+        "e2e": {"value": round(tot / e2e_s / 1e6, 3), "unit": "Mcell-iters/s",
+                "h2d_bytes_per_step": 5 * 8 * r["nt"] * world, "d2h_bytes_per_step": 5 * 8 * r["nt"] * world},
+        "residual_last": float(r["hist"][-1]) if len(r["hist"]) else None,
+    }
+    if r64 is not None:
+        v64 = tot * args.steps / (ms64 / 1e3) / 1e6
+        line["fp64_arm"] = {"value": round(v64, 3), "ms_per_step": round(ms64 / args.steps, 4)}
+        line["speedup_vs_fp64"] = round(value / v64, 3)
+        if r["forces"] and r64["forces"]:
+            line["accuracy_vs_fp64"] = {"dCL": abs(r["forces"]["CL"] - r64["forces"]["CL"]),
+                                        "dCD": abs(r["forces"]["CD"] - r64["forces"]["CD"]),
+                                        "after_iterations": r["iters"]}
+    line["config"]["sa_source"] = (("learned (MLP, exact outside its hull)" if blob is not None else "exact")
+                                   if sa else None)
+    if rank == 0:
+        print(json.dumps(line))
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 def converge(args, m, wd):
@@ -560,16 +755,11 @@ def main():
         return
 
     if world > 1:
-        import torch.distributed as dist
-        import datetime
-
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        return main_zones(args, rank, world, wl)
     from phenlei_b200 import mesh as M
+    import torch
 
-    if world == 1:
-        import torch
-
-        torch.cuda.set_device(0)
+    torch.cuda.set_device(0)
     m = wl["mesh"]()
     wd = M.wall_distance(m) if wl.get("wall_dist") else None
     sa = wl["params"].get("viscousType", 0) == 3
@@ -594,13 +784,6 @@ def main():
         rx = run_phx(args, rank, world, args.precision, m, wd, e2e=False)
     r = run_phx(args, rank, world, args.precision, m, wd, mlp_blob=blob)
     ms = r["ms"]
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     nc = r["nc"]
     per_gpu = nc * args.steps / (ms / 1e3) / 1e6
     value = per_gpu * world
@@ -619,7 +802,7 @@ def main():
         "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded generated mesh, free-stream start)",
         "config": {"workload": args.workload, "desc": wl["desc"], "cells": nc, "precision": args.precision,
-                   "parallelism": "replicas only" if world > 1 else "1 GPU",
+                   "parallelism": "1 GPU",
                    "l2": "inputs larger than L2 (state %.0f MB)" % (5 * 8 * r["nt"] / 1e6)},
         "gpu_launches": int(r["launches"]),
         "phase_ms": {k: round(v, 4) for k, v in phase.items()},
@@ -679,14 +862,9 @@ def main():
     if blob is not None:
         line["mlp"] = dict((r64 or {}).get("mlp") or {"loaded": args.mlp_blob}, cells_learned_per_iteration=round(
             r["mlp"]["cells_learned"] / r["iters"], 1), cells=nc)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.workload)
-    if rank == 0:
-        print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

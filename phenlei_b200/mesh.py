@@ -35,6 +35,7 @@ BC_SYMMETRY = 3
 BC_FARFIELD = 4
 BC_INFLOW = 5
 BC_OUTFLOW = 6
+BC_INTERFACE = -1   # PHENGLEI::INTERFACE: a face cut by a partition (ghost = the neighbouring zone's cell)
 
 
 @dataclasses.dataclass
@@ -409,12 +410,17 @@ def tanh_one_sided(n: int, first: float) -> np.ndarray:
 
 
 def channel_bump(nx=64, ny=32, nz=4, thickness=0.10, length=3.0, height=1.0,
-                 wall_spacing=0.01, dz=None, lower_region="Wall", upper_region="Wall", prism_layers=0) -> Mesh:
+                 wall_spacing=0.01, dz=None, lower_region="Wall", upper_region="Wall", prism_layers=0,
+                 zone=None) -> Mesh:
     """3-D channel with a circular-arc bump of chord 1 on x in [1,2] of the lower wall.
 
     x and z are uniform (dz defaults to dx), y is tanh-stretched from the lower
     wall with first spacing wall_spacing*height.  Regions: lower and upper walls
     (solid surface), inlet/outlet (far field), z planes (symmetry).
+
+    zone=(r, n): the r-th of n equal slabs in x of this channel (i in
+    [r nx/n, (r+1) nx/n]); a cut side belongs to a fifth region "Interface" of
+    type BC_INTERFACE.
     """
     x = np.linspace(0.0, length, nx + 1)
     t = thickness
@@ -431,6 +437,18 @@ def channel_bump(nx=64, ny=32, nz=4, thickness=0.10, length=3.0, height=1.0,
     regions = [(BC_SOLID_SURFACE, "LowerWall"), (BC_SOLID_SURFACE, "UpperWall"),
                (BC_FARFIELD, "Farfield"), (BC_SYMMETRY, "Symmetry")]
     side = {"jmin": 0, "jmax": 1, "imin": 2, "imax": 2, "kmin": 3, "kmax": 3}
+    if zone is not None:
+        r, n = zone
+        if nx % n or not 0 <= r < n:
+            raise ValueError("zone (r, n) needs 0 <= r < n and n dividing nx")
+        w = nx // n
+        X = X[r * w:(r + 1) * w + 1]
+        if n > 1:
+            regions = regions + [(BC_INTERFACE, "Interface")]
+            if r > 0:
+                side["imin"] = 4
+            if r < n - 1:
+                side["imax"] = 4
     if prism_layers > 0:
         return _hex_prism_block(X, prism_layers, side, regions)
     return _hex_block(X, side, regions)

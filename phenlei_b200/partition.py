@@ -28,9 +28,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .mesh import Mesh
-
-BC_INTERFACE = -1   # PHENGLEI::INTERFACE
+from .mesh import BC_INTERFACE, Mesh   # noqa: F401  (BC_INTERFACE: PHENGLEI::INTERFACE)
 
 
 @dataclass

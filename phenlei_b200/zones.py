@@ -44,6 +44,51 @@ from .solver import (PHX_HALO_DQ, PHX_HALO_GRADIENT, PHX_HALO_Q, PHX_HALO_TURB, 
                      NSSolverUnstruct, PhxError, force_coefficients)
 
 
+def channel_zone(rank: int, world: int, **channel_kw) -> P.Part:
+    """Zone `rank` of `world` equal slabs in x of mesh.channel_bump(**channel_kw),
+    built alone (no process holds the whole channel), with its halo plan.  The
+    cut sides are interface faces; across a cut, the faces of both zones list
+    the same (k, j) rows in the order of their own cells' numbers, so zone r
+    sends the cells behind its upper cut in that order and zone r + 1 fills
+    the ghosts of its lower cut in that order.  Global cell numbers are
+    r n_cell + local number."""
+    from . import mesh as M
+
+    m = M.channel_bump(zone=(rank, world), **channel_kw)
+    nb, nc = m.n_bface, m.n_cell
+    breg = np.asarray(m.bface_region, np.int64)
+    itf = np.flatnonzero(breg == len(m.regions) - 1) if world > 1 else np.zeros(0, np.int64)
+    foff = m.face_offsets()
+    f2n = np.asarray(m.face2node, np.int64)
+    xs = np.asarray(m.x)
+    fx = np.array([xs[f2n[foff[f]:foff[f + 1]]].mean() for f in itf]) if itf.size else np.zeros(0)
+    lo = itf[np.abs(fx - xs.min()) < np.abs(fx - xs.max())]
+    hi = np.setdiff1d(itf, lo)
+    left = np.asarray(m.left, np.int64)
+    halo = P.Halo(neighbors=[], send={}, recv={})
+    for q, faces in ((rank - 1, lo), (rank + 1, hi)):
+        if 0 <= q < world:
+            faces = faces[np.argsort(left[faces], kind="stable")]
+            halo.recv[q] = nc + faces
+            halo.send[q] = left[faces]
+            halo.neighbors.append(q)
+    first = int(itf[0]) if itf.size else nb
+    if itf.size and not np.array_equal(itf, np.arange(first, nb)):
+        raise AssertionError("interface faces are not the last boundary faces")
+    return P.Part(rank=rank, mesh=m, cells=rank * nc + np.arange(nc), faces=np.zeros(0, np.int64),
+                  flipped=np.zeros(0, bool), nodes=np.zeros(0, np.int64), iface_first=first,
+                  n_iface=int(itf.size), halo=halo)
+
+
+def _wall_of(wall_dist, own=False):
+    """Per-part wall distances: the whole mesh's values at the part's cells,
+    or (own) the values given, which are already the part's."""
+    if wall_dist is None:
+        return None
+    wd = np.asarray(wall_dist)
+    return (lambda p: wd) if own else (lambda p: wd[p.cells])
+
+
 def _plan(part):
     """Concatenated send cells and receiving boundary faces of a part, and
     per neighbour the (offset, count) of its rows in each list."""
@@ -66,17 +111,17 @@ class _Zones:
 
     FIELDS = (PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB, PHX_HALO_TURB_DQ)
 
-    def _setup(self, mesh, parts, params, precision, wall_dist):
+    def _setup(self, mesh, parts, params, precision, wall_of):
+        """wall_of(part): the part's wall distances, or None."""
         import torch
 
         if params.get("gradientName", "ggcell") in ("ggnode", 2):
             raise ValueError("GG-node across zones needs the interpoint exchange; not built")
         self.mesh = mesh
         self.sa = params.get("viscousType", 0) == 3
-        if self.sa and wall_dist is None:
+        if self.sa and wall_of is None:
             raise ValueError("the SA model needs the wall distance of every cell")
-        self.zones = [NSSolverUnstruct(p.mesh, precision=precision,
-                                       wall_dist=None if wall_dist is None else np.asarray(wall_dist)[p.cells],
+        self.zones = [NSSolverUnstruct(p.mesh, precision=precision, wall_dist=None if wall_of is None else wall_of(p),
                                        **params) for p in self.parts]
         self.plans = [_plan(p) for p in self.parts]
         # zones without interface faces (a single zone) take part in the sums only
@@ -139,43 +184,56 @@ class _Zones:
         self._exchange_state()
 
     # -- one outer iteration -----------------------------------------------------
-    def iterate(self, nsteps: int = 1) -> np.ndarray:
+    def iterate(self, nsteps: int = 1, timer: dict | None = None) -> np.ndarray:
         """`nsteps` outer iterations; returns the global residual monitor
-        sqrt(sum res_rho^2 / nCell) of each."""
+        sqrt(sum res_rho^2 / nCell) of each.  With `timer` (a dict), CUDA
+        events bracket every phase's kernels on the current stream, the
+        exchanges between them left out: timer[phase] lists (start, end)
+        pairs."""
         hist = []
         zs = self.zones
+
+        def phase(name, fn):
+            if timer is None:
+                for z in zs:
+                    fn(z)
+                return
+            import torch
+
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for z in zs:
+                fn(z)
+            b.record()
+            timer.setdefault(name, []).append((a, b))
+
         for _ in range(nsteps):
             for z in zs:
                 z.step = z.step + 1   # Simulation::UpdateOuterIterationStep
-                z.Boundary()
-                z.ComputeGradientAndLimiter()
+            phase("boundary", lambda z: z.Boundary())
+            phase("gradient_limiter", lambda z: z.ComputeGradientAndLimiter())
             self._exchange(PHX_HALO_GRADIENT)
-            for z in zs:
-                z.UpdateResiduals()
+            phase("residual", lambda z: z.UpdateResiduals())
             mindt = self._allmin(min(z.min_timestep() for z in zs))
             for z in zs:
                 z.set_min_timestep(mindt)
-                z.LUSGSForward()
+            phase("lusgs", lambda z: z.LUSGSForward())
             self._exchange(PHX_HALO_DQ)
-            for z in zs:
-                z.LUSGSBackward()
+            phase("lusgs", lambda z: z.LUSGSBackward())
             s = 0.0
             for z in zs:
                 r = z.GetResidual()[0]
                 s += r * r * z.mesh.n_cell
             s = self._allsum(s)
             h = float(np.sqrt(s / self.n_cell_total))
-            for z in zs:
-                z.UpdateFlowField()
+            phase("update", lambda z: z.UpdateFlowField())
             self._exchange(PHX_HALO_Q)
             if self.sa:
-                for z in zs:
-                    z.TurbUpdateResiduals()
-                    z.TurbLUSGSForward()
+                phase("sa_residual", lambda z: z.TurbUpdateResiduals())
+                phase("sa_lusgs", lambda z: z.TurbLUSGSForward())
                 self._exchange(PHX_HALO_TURB_DQ)
-                for z in zs:
-                    z.TurbLUSGSBackward()
-                    z.TurbUpdateFlowField()
+                phase("sa_lusgs", lambda z: z.TurbLUSGSBackward())
+                phase("sa_update", lambda z: z.TurbUpdateFlowField())
                 self._exchange(PHX_HALO_TURB)
             for z in zs:
                 z.status()
@@ -210,7 +268,7 @@ class ZoneSet(_Zones):
     def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None, precision="fp64"):
         self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
         self.parts = P.split(mesh, self.owner)
-        self._setup(mesh, self.parts, params, precision, wall_dist)
+        self._setup(mesh, self.parts, params, precision, _wall_of(wall_dist))
 
     def _centres(self, cc):
         out = []
@@ -260,18 +318,23 @@ class DistributedZone(_Zones):
     torch.distributed group takes part r).  Every rank builds the same
     partition and calls the same steps."""
 
-    def __init__(self, mesh, params: dict, owner=None, wall_dist=None, precision="fp64"):
+    def __init__(self, mesh, params: dict, owner=None, wall_dist=None, precision="fp64", part=None):
+        """`mesh` is the whole grid, split here; or `part` is this rank's zone,
+        built alone (channel_zone), with `wall_dist` then its own cells'."""
         import torch.distributed as dist
 
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self._nccl = dist.get_backend() == "nccl"
+        if part is not None:
+            self.parts = [part]
+            self._setup(None, self.parts, params, precision, _wall_of(wall_dist, own=True))
+            return
         self.owner = P.slab_owner(mesh, self.world) if owner is None else np.asarray(owner, np.int32)
         parts = P.split(mesh, self.owner)
         if len(parts) != self.world:
             raise ValueError("one part per rank")
-        self.all_parts = parts
         self.parts = [parts[self.rank]]
-        self._nccl = dist.get_backend() == "nccl"
-        self._setup(mesh, self.parts, params, precision, wall_dist)
+        self._setup(mesh, self.parts, params, precision, _wall_of(wall_dist))
 
     @property
     def part(self):

@@ -266,3 +266,43 @@ def test_distributed_oracle_world_size_2_equals_in_process(tmp_path, case):
         assert np.array_equal(d["q"][:, cells], q[:, cells])
         if case == "sa":
             assert np.array_equal(d["qt"][cells], po.gather("qt")[cells])
+
+
+# --- zones built alone (phenlei_b200.zones.channel_zone) ------------------------------------------
+
+@pytest.mark.parametrize("prism", [0, 3])
+@pytest.mark.parametrize("world", [2, 3])
+def test_channel_zones_built_alone_equal_the_split_channel(prism, world):
+    """Zone r of a channel built alone holds the cells that slab_owner + split
+    give part r of the whole channel, and each interface ghost's halo source is
+    the neighbouring zone's cell across that face (the face's nodes are the
+    cell's nodes)."""
+    from phenlei_b200.zones import channel_zone
+
+    kw = dict(nx=12 * world, ny=6, nz=2, length=1.5 * world, dz=0.125, prism_layers=prism)
+    whole = M.channel_bump(**kw)
+    parts = P.split(whole, P.slab_owner(whole, world))
+    zones = [channel_zone(r, world, **kw) for r in range(world)]
+    for r, (z, p) in enumerate(zip(zones, parts)):
+        a = P.cell_centroids(z.mesh)
+        b = P.cell_centroids(p.mesh)
+        assert a.shape == b.shape
+        assert np.allclose(a[np.lexsort(a.T)], b[np.lexsort(b.T)], rtol=0, atol=1e-12)
+        assert z.n_iface == p.n_iface and z.halo.neighbors == p.halo.neighbors
+        assert z.mesh.solver_regions()[0].tolist().count(P.BC_INTERFACE) == (1 if world > 1 else 0)
+    xyz = [np.stack([z.mesh.x, z.mesh.y, z.mesh.z], 1) for z in zones]
+    for r, z in enumerate(zones):
+        m = z.mesh
+        foff = m.face_offsets()
+        for q in z.halo.neighbors:
+            nq = zones[q].mesh
+            coff = np.zeros(nq.n_cell + 1, np.int64)
+            np.cumsum(nq.cell_nnode, out=coff[1:])
+            src = zones[q].halo.send[r]
+            assert len(src) == len(z.halo.recv[q])
+            for ghost, c in zip(z.halo.recv[q], src):
+                f = int(ghost) - m.n_cell
+                fpts = xyz[r][np.asarray(m.face2node)[foff[f]:foff[f + 1]]]
+                cpts = xyz[q][np.asarray(nq.cell2node)[coff[c]:coff[c + 1]]]
+                d = np.min(np.abs(fpts[:, None, :] - cpts[None, :, :]).sum(-1), axis=1)
+                assert np.all(d < 1e-12)
