@@ -78,7 +78,6 @@ extern "C" {
 #define PHX_HALO_DQ 2        /* forward-sweep dq between the LU-SGS sweeps (Controller::LUSGS, :1917-1924) */
 #define PHX_HALO_TURB 3      /* nu~ and eddy viscosity (TurbSolverUnstr::UploadInterfaceValue,
                                 CFD/TurbSolver/src/TurbSolverUnstr.cpp:7130-7145) */
-#define PHX_HALO_TURB_DQ 4   /* forward-sweep SA dq between the SA sweeps */
 
 /* state selectors for phx_set_state / phx_get_state */
 #define PHX_Q 0          /* primitive state [5][nTotal] */
@@ -317,10 +316,12 @@ int phx_fault_hold_cell(phx_ctx *ctx, int32_t cell);
  * CFD/Solver/src/Controller.cpp:549-587; the interface communication of
  * Controller::CommunicationInterfaceData, :3389): boundary, gradient and
  * limiter, HALO GRADIENT, residual, the minimum time step over all zones,
- * forward sweep, HALO DQ, backward sweep, update, HALO Q; with SA: SA
- * residual, SA forward sweep, HALO TURB_DQ, SA backward sweep, SA update,
- * HALO TURB.  The gradient of nu~ needs no exchange here: only its own cell
- * reads it.  The fused
+ * forward sweep, HALO DQ (when swapDq is set, as the reference's parameter
+ * file sets it), backward sweep, update, HALO Q; with SA: SA residual, SA
+ * forward and backward sweeps, SA update, HALO TURB.  The SA dq is not
+ * exchanged (Controller::CommunicationDQ, Controller.cpp:2874-2880, serves the
+ * NS solver only), and the gradient of nu~ needs no exchange here: only its
+ * own cell reads it.  The fused
  * phx_ns_relaxation, phx_ns_lusgs and phx_sa_lusgs refuse a context with
  * interface faces (PHX_ERR_STATE).  GG-node gradients are not supported
  * across zones (PHX_ERR_ARG at creation). */
@@ -353,8 +354,9 @@ int phx_halo_unpack(phx_ctx *ctx, int field, const void *buf_dev);
 
 /* The two LU-SGS sweeps of phx_ns_lusgs / phx_sa_lusgs as separate calls,
  * for the dq exchange between them (Controller::LUSGS, Controller.cpp:1917-1924;
- * CommunicationDQ :2874).  The backward sweep reads the interface ghosts' dq
- * from HALO DQ (TURB_DQ). */
+ * CommunicationDQ :2874).  The NS backward sweep reads the interface ghosts'
+ * dq from HALO DQ (zero without the exchange); the SA backward sweep, like the
+ * reference's, takes an interface ghost's dq as zero. */
 int phx_ns_lusgs_forward(phx_ctx *ctx);
 int phx_ns_lusgs_backward(phx_ctx *ctx);
 int phx_sa_lusgs_forward(phx_ctx *ctx);

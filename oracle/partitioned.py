@@ -14,17 +14,19 @@ their ghosts from the neighbouring zone at these points:
 * after the gradient: the primitive and temperature gradients
   (Controller::ComputeGradient, CFD/Solver/src/Controller.cpp:1288);
 * after the limiter: limit2D (Controller.cpp:1321);
-* between the forward and the backward LU-SGS sweep: dq (Controller.cpp:1917-1924).
+* between the forward and the backward LU-SGS sweep: dq (Controller.cpp:1917-1924),
+  for the NS solver only and when swapDq is set (Controller::CommunicationDQ,
+  :2874-2886; the reference's parameter file sets it).
 
 The residual norm is a sum over all zones (PH_AllReduce).  The exchanges here
 are plain array copies between the in-process parts; phenlei_b200.partition.exchange
 moves the same values between ranks.
 
-With Spalart-Allmaras the turbulence step exchanges in the same places: the
-gradient of nu~, its dq between the sweeps (TurbSolverUnstr::SetGhostDQLUSGS
-leaves interface ghosts to that exchange, TurbSolverUnstr.cpp:1660), and
-q_turb with vist in its PostSolve (TurbSolverUnstr::UploadInterfaceValue,
-:7130-7145).  The wall distance of every part is the whole mesh's.
+With Spalart-Allmaras the turbulence step exchanges the gradient of nu~ and,
+in its PostSolve, q_turb with vist (TurbSolverUnstr::UploadInterfaceValue,
+:7130-7145).  Its dq is not exchanged between the sweeps (CommunicationDQ
+returns for every solver but the NS one), so an interface ghost's SA dq stays
+its ghost residual, zero.  The wall distance of every part is given.
 
 The ktmax clamp of the local time step takes the minimum over all zones
 (Controller::GetGlobalMinTimeStep, Controller.cpp:720-751).
@@ -63,6 +65,7 @@ class PartitionedOracle:
         self.o = [Oracle(p.mesh, params, wall_dist=None if wall_dist is None else np.asarray(wall_dist)[p.cells])
                   for p in self.parts]
         self.viscous = params.get("viscousType", 0) > 0
+        self.swap_dq = int(params.get("swapDq", 1)) != 0
         self.step = 0
         # SwapGeometry: the interface ghosts take the neighbouring cells' centres
         # and volumes (UnstructGrid::TranslateCellCenter,
@@ -184,7 +187,8 @@ class PartitionedOracle:
                 o._dflux = np.zeros((5, o.nt))
                 L.ox_lusgs_forward(g, m, p, _p(o.q), _p(w["gama"]), _p(w["visl"]), _p(w["vist"]), _p(w["res"]),
                                    _p(w["dt"]), _p(w["inv_spec"]), _p(w["vis_spec"]), _p(w["dq"]), _p(o._dflux))
-            self._exchange(lambda o: o.w_arrays["dq"])
+            if self.swap_dq:
+                self._exchange(lambda o: o.w_arrays["dq"])
             s, n = 0.0, 0
             for o in self.o:
                 w = o.w_arrays
@@ -218,7 +222,6 @@ class PartitionedOracle:
             L.ox_sa_residual_phase(*a)
             o._dfl = np.zeros(o.nt)
             L.ox_sa_lusgs_forward(a[0], a[1], a[4], _p(o._dfl))
-        self._exchange(lambda o: o.w_arrays["dqt"])
         for o, a in zip(self.o, args):
             L.ox_sa_lusgs_backward(a[0], a[1], a[4], _p(o._dfl))
         self._exchange(lambda o: o.w_arrays["qt"])

@@ -1920,7 +1920,7 @@ static void sa_diffusion(const ox_grid *g, const ox_metrics *m, const ox_params 
         /* mlt */
         double nl = qt[le], vl = visl[le], rl = q[le];
         double nr = qt[re], vr = visl[re], rr = q[re];
-        if (f < nb && t != OX_BC_INTERFACE) {   /* GetVisFaceValue: interface faces as interior (:3950) */
+        if (f < nb) {   /* GetVisFaceValue's mlt loop takes every boundary face alike, interface faces too (:3990-4003) */
             if (nl < 0.0) {
                 nl = positive_sa(nl, vl, rl);
                 if (is_wall(t)) nr = -nl;

@@ -11,11 +11,17 @@
 //   outer loop         Main/src/Simulation.cpp:1292-1327, 1190-1237, 1527-1559
 //
 // usage: ref_harness MESH RUNDIR OUTDIR NSTEPS [STATE] [name:rows:cols ...]
-//   MESH   binary mesh (format written by phenlei_b200/mesh.py:write_mesh)
+//   MESH   binary mesh (format written by phenlei_b200/mesh.py:write_mesh), or
+//          a comma-separated list of meshes, one zone each, all on this rank;
+//          a zone's MESH.itf file, when present, holds its interface data as
+//          the reference's grid files do (IO_HDF5Read::ReadInterfaceInfo,
+//          Pre_HDF5File.cpp:1366-1401): int64 nIFace, then interFace2ZoneID,
+//          interFace2InterFaceID and interFace2BoundaryFace (int32 each).
+//          Several zones write their dumps to OUTDIR/zone<i>/.
 //   RUNDIR directory holding bin/key.hypara and the case files
 //   STATE  optional binary primitive state (nEq x nTotalCell doubles, then
 //          optionally nTurb x nTotalCell) that replaces the initial field; "-"
-//          for none
+//          for none; one file per zone, comma-separated
 //   name:rows:cols  grid data arrays to dump after the last step (rows=0 means
 //          a 1-D array of cols values)
 #include <chrono>
@@ -25,6 +31,7 @@
 #include <string>
 #include <vector>
 #include <unistd.h>
+#include <sys/stat.h>
 #include <execinfo.h>
 #include <signal.h>
 #include <sstream>
@@ -147,6 +154,34 @@ MeshFile ReadMesh(const char *path)
     return m;
 }
 
+struct ItfFile
+{
+    long long nIFace = 0;
+    std::vector<int> zoneID, interFaceID, boundaryFace;
+};
+
+ItfFile ReadItf(const std::string &path)
+{
+    ItfFile itf;
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return itf;
+    if (fread(&itf.nIFace, sizeof(long long), 1, f) != 1) Die("short interface file");
+    ReadVec(f, itf.zoneID, itf.nIFace);
+    ReadVec(f, itf.interFaceID, itf.nIFace);
+    ReadVec(f, itf.boundaryFace, itf.nIFace);
+    fclose(f);
+    return itf;
+}
+
+std::vector<std::string> SplitList(const std::string &s)
+{
+    std::vector<std::string> out;
+    std::stringstream ss(s);
+    std::string item;
+    while (std::getline(ss, item, ',')) out.push_back(item);
+    return out;
+}
+
 template <class T>
 T *Dup(const std::vector<T> &v)
 {
@@ -157,9 +192,9 @@ T *Dup(const std::vector<T> &v)
 
 // Mirrors IO_HDF5Read::ReadUnstructGrid / ReadFaceTopology / ReadCellTopology /
 // ReadUnstrBCName (Pre_HDF5File.cpp:1753-1940) with the arrays taken from MESH.
-UnstructGrid *BuildGrid(const MeshFile &m)
+UnstructGrid *BuildGrid(const MeshFile &m, int zoneIndex, const ItfFile &itf)
 {
-    GridID *index = new GridID(0);
+    GridID *index = new GridID(zoneIndex);
     UnstructGrid *grid = new UnstructGrid();
     grid->InitGrid(index, 0, PHSPACE::GetDim(), UNSTRUCTGRID);
     grid->SetIBlock(0);
@@ -181,6 +216,17 @@ UnstructGrid *BuildGrid(const MeshFile &m)
     grid->SpecifyRightCellofBC();
 
     grid->SetInterfaceInfo(0);
+    if (itf.nIFace > 0)
+    {
+        InterfaceInfo *info = new InterfaceInfo((int)itf.nIFace, grid);
+        for (long long i = 0; i < itf.nIFace; ++i)
+        {
+            info->GetInterFace2ZoneID()[i] = itf.zoneID[i];
+            info->GetInterFace2InterFaceID()[i] = itf.interFaceID[i];
+            info->GetInterFace2BoundaryFace()[i] = itf.boundaryFace[i];
+        }
+        grid->SetInterfaceInfo(info);
+    }
     grid->SetNodeNumberOfEachCell(Dup(m.nodePerCell));
     grid->SetCell2Node(Dup(m.cell2node));
 
@@ -222,20 +268,25 @@ UnstructGrid *BuildGrid(const MeshFile &m)
     return grid;
 }
 
-void SetLayoutOneZone()
+// Every zone on this rank (processor 0), as a one-rank run of a partitioned
+// grid lays them out.
+void SetLayout(int nZones)
 {
-    PHMPI::SetNumberOfGlobalZones(1);
-    PHMPI::CreateZoneProcessorIDDump(1);
-    PHMPI::CreateZoneProcessorID(1);
-    PHMPI::CreateZoneGridID(1);
-    PHMPI::CreateZoneGridType(1);
-    PHMPI::CreateZoneFileID(1);
-    PHMPI::GetZoneProcessorID()[0] = 0;
-    PHMPI::GetZoneProcessorIDForGrid()[0] = -1;
-    PHMPI::GetZoneGridType()[0] = UNSTRUCTGRID;
-    PHMPI::GetZoneGridID()[0] = 0;
-    PHMPI::GetZoneFileID()[0] = 0;
-    PHMPI::GetZoneProcessorIDDump()[0] = 0;
+    PHMPI::SetNumberOfGlobalZones(nZones);
+    PHMPI::CreateZoneProcessorIDDump(nZones);
+    PHMPI::CreateZoneProcessorID(nZones);
+    PHMPI::CreateZoneGridID(nZones);
+    PHMPI::CreateZoneGridType(nZones);
+    PHMPI::CreateZoneFileID(nZones);
+    for (int z = 0; z < nZones; ++z)
+    {
+        PHMPI::GetZoneProcessorID()[z] = 0;
+        PHMPI::GetZoneProcessorIDForGrid()[z] = -1;
+        PHMPI::GetZoneGridType()[z] = UNSTRUCTGRID;
+        PHMPI::GetZoneGridID()[z] = z;
+        PHMPI::GetZoneFileID()[z] = 0;
+        PHMPI::GetZoneProcessorIDDump()[z] = 0;
+    }
     int sysGridType = UNSTRUCTGRID;
     GlobalDataBase::UpdateData("sys_gridtype", &sysGridType, PHINT, 1);
 }
@@ -254,7 +305,16 @@ int main(int argc, char **argv)
     if (argc < 5) Die("usage: ref_harness MESH RUNDIR OUTDIR NSTEPS [STATE] [name:rows:cols ...]");
     signal(SIGSEGV, OnFault);
     signal(SIGBUS, OnFault);
-    MeshFile mesh = ReadMesh(argv[1]);
+    const std::vector<std::string> meshPaths = SplitList(argv[1]);
+    const int nZones = (int)meshPaths.size();
+    if (nZones < 1) Die("no mesh");
+    std::vector<MeshFile> meshes;
+    std::vector<ItfFile> itfs;
+    for (const std::string &mp : meshPaths)
+    {
+        meshes.push_back(ReadMesh(mp.c_str()));
+        itfs.push_back(ReadItf(mp + ".itf"));
+    }
     std::string outdir = argv[3];
     int nSteps = atoi(argv[4]);
     if (chdir(argv[2]) != 0) Die("cannot chdir to RUNDIR");
@@ -269,14 +329,18 @@ int main(int argc, char **argv)
 
     STAGE("self check done");
     Region *region = new Region();
-    SetLayoutOneZone();
-    UnstructGrid *grid = BuildGrid(mesh);
+    SetLayout(nZones);
+    std::vector<UnstructGrid *> grids;
+    for (int z = 0; z < nZones; ++z)
     {
+        // IO_HDF5Read::CreateZones (Pre_HDF5File.cpp:2206-2235)
+        UnstructGrid *grid = BuildGrid(meshes[z], z, itfs[z]);
         grid->GetGridID()->SetLocalIndex(PHMPI::GetNumberofLocalZones());
-        Zone *zone = new Zone(0);
+        Zone *zone = new Zone(z);
         zone->AddGridAndCopyZonePara(grid);
-        zone->AddGridToGlobal(0);
+        zone->AddGridToGlobal(z);
         region->AddZone(zone);
+        grids.push_back(grid);
     }
     STAGE("grid built");
     GlobalBoundaryCondition::ReadGlobalBoundaryCondition();
@@ -289,11 +353,12 @@ int main(int argc, char **argv)
     STAGE("geometry");
     region->SwapGeometry();
 
-    // Simulation::DefineAndCreateSolvers (Simulation.cpp:977-1188), one zone.
+    // Simulation::DefineAndCreateSolvers (Simulation.cpp:977-1188), every zone.
     STAGE("swap geometry");
     InitGlobalValuesOfAllZones();
+    for (int z = 0; z < nZones; ++z)
     {
-        Zone *zone = region->GetZone(0);
+        Zone *zone = region->GetZone(z);
         std::vector<PHSolver *> solvers;
         PHSolver *ns = new NSSolverUnstruct();
         ns->SetName("NSSolverUnstruct");
@@ -333,12 +398,17 @@ int main(int argc, char **argv)
             const char *wdFile = getenv("PHX_REF_WALLDIST");
             if (wdFile && *wdFile)
             {
-                FILE *wf = fopen(wdFile, "rb");
-                if (!wf) Die("cannot open PHX_REF_WALLDIST");
-                RDouble *wd = grid->GetWallDist();
-                const size_t nread = fread(wd, sizeof(RDouble), grid->GetNTotalCell(), wf);
-                fclose(wf);
-                if ((int)nread != grid->GetNTotalCell()) Die("short PHX_REF_WALLDIST file");
+                const std::vector<std::string> wdPaths = SplitList(wdFile);
+                if ((int)wdPaths.size() != nZones) Die("PHX_REF_WALLDIST needs one file per zone");
+                for (int z = 0; z < nZones; ++z)
+                {
+                    FILE *wf = fopen(wdPaths[z].c_str(), "rb");
+                    if (!wf) Die("cannot open PHX_REF_WALLDIST");
+                    RDouble *wd = grids[z]->GetWallDist();
+                    const size_t nread = fread(wd, sizeof(RDouble), grids[z]->GetNTotalCell(), wf);
+                    fclose(wf);
+                    if ((int)nread != grids[z]->GetNTotalCell()) Die("short PHX_REF_WALLDIST file");
+                }
             }
             else
             {
@@ -361,47 +431,57 @@ int main(int argc, char **argv)
     STAGE("initialized");
     CreateAleManager();
 
-    int nTotalCell = grid->GetNTotalCell();
-    int nBoundFace = grid->GetNBoundFace();
-    int nTotal = nTotalCell + nBoundFace;
     int nl = GlobalDataBase::GetIntParaFromDB("nl");
     int nTurb = (nSolver > 1) ? GlobalDataBase::GetIntParaFromDB("n_turb") : 0;
 
     if (argc > 5 && strcmp(argv[5], "-") != 0)
     {
-        FILE *f = fopen(argv[5], "rb");
-        if (!f) Die("cannot open STATE");
-        RDouble **q = reinterpret_cast<RDouble **>(grid->GetDataPtr("q"));
-        for (int m = 0; m < nl; ++m)
-            if (fread(q[m], sizeof(double), nTotalCell, f) != (size_t)nTotalCell) Die("short STATE");
-        if (nTurb)
+        const std::vector<std::string> statePaths = SplitList(argv[5]);
+        if ((int)statePaths.size() != nZones) Die("STATE needs one file per zone");
+        for (int z = 0; z < nZones; ++z)
         {
-            RDouble **qt = reinterpret_cast<RDouble **>(grid->GetDataPtr("q_turb"));
-            for (int m = 0; m < nTurb; ++m)
-            {
-                size_t got = fread(qt[m], sizeof(double), nTotalCell, f);
-                if (got != 0 && got != (size_t)nTotalCell) Die("short STATE (turb)");
-            }
-        }
-        fclose(f);
-        // GG-node gradients read node values that the solver forms at
-        // initialisation (NSSolver::InitDependentVariables, NSSolver.cpp:757-790,
-        // then Controller::Initialize's ModifyNodeValue) and in each PostSolve;
-        // a loaded state gets them the way an initialisation from a restart does.
-        if (GlobalDataBase::GetStrParaFromDB("gradientName") == "ggnode")
-        {
-            NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(0, 0));
-            ns->InitDependentVariables();
-            ns->ModifyNodeValue(grid);
+            UnstructGrid *grid = grids[z];
+            const int nTotalCell = grid->GetNTotalCell();
+            FILE *f = fopen(statePaths[z].c_str(), "rb");
+            if (!f) Die("cannot open STATE");
+            RDouble **q = reinterpret_cast<RDouble **>(grid->GetDataPtr("q"));
+            for (int m = 0; m < nl; ++m)
+                if (fread(q[m], sizeof(double), nTotalCell, f) != (size_t)nTotalCell) Die("short STATE");
             if (nTurb)
             {
-                // the SA solver's node values of nu~ (TurbSolver::InitDependentVariables,
-                // TurbSolver.cpp:46-56, then ModifyQTurbNodeValue)
-                TurbSolverUnstr *turb = static_cast<TurbSolverUnstr *>(GlobalSolvers::GetSolver(0, 1));
-                turb->InitDependentVariables();
-                turb->ModifyQTurbNodeValue(grid);
+                RDouble **qt = reinterpret_cast<RDouble **>(grid->GetDataPtr("q_turb"));
+                for (int m = 0; m < nTurb; ++m)
+                {
+                    size_t got = fread(qt[m], sizeof(double), nTotalCell, f);
+                    if (got != 0 && got != (size_t)nTotalCell) Die("short STATE (turb)");
+                }
+            }
+            fclose(f);
+            // GG-node gradients read node values that the solver forms at
+            // initialisation (NSSolver::InitDependentVariables, NSSolver.cpp:757-790,
+            // then Controller::Initialize's ModifyNodeValue) and in each PostSolve;
+            // a loaded state gets them the way an initialisation from a restart does.
+            if (GlobalDataBase::GetStrParaFromDB("gradientName") == "ggnode")
+            {
+                NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(z, 0));
+                ns->InitDependentVariables();
+                ns->ModifyNodeValue(grid);
+                if (nTurb)
+                {
+                    // the SA solver's node values of nu~ (TurbSolver::InitDependentVariables,
+                    // TurbSolver.cpp:46-56, then ModifyQTurbNodeValue)
+                    TurbSolverUnstr *turb = static_cast<TurbSolverUnstr *>(GlobalSolvers::GetSolver(z, 1));
+                    turb->InitDependentVariables();
+                    turb->ModifyQTurbNodeValue(grid);
+                }
             }
         }
+        // Controller::Initialize ends with the interface communication of
+        // every zone (Controller.cpp:153-172); the loaded state takes its place
+        // here, so the interface ghosts receive the neighbours' loaded cells
+        if (nZones > 1)
+            for (int iSolver = 0; iSolver < nSolver; ++iSolver)
+                for (int z = 0; z < nZones; ++z) GlobalSolvers::GetSolver(z, iSolver)->CommunicationInterfaceData();
     }
 
     // Outer loop: Simulation::SolveSimulation / SolveOneOuterStep without the
@@ -438,66 +518,86 @@ int main(int argc, char **argv)
             delete controller;
         }
 
-        // Residual monitor of NS equation 0 (Residual.cpp:184-224 definition).
-        RDouble **res = reinterpret_cast<RDouble **>(grid->GetDataPtr("res"));
+        // Residual monitor of NS equation 0 (Residual.cpp:184-224 definition),
+        // summed over the zones (PH_AllReduce)
         double s = 0.0;
-        for (int c = 0; c < nTotalCell; ++c) s += res[0][c] * res[0][c];
-        resHist.push_back(sqrt(s / nTotalCell));
+        long long n = 0;
+        for (int z = 0; z < nZones; ++z)
+        {
+            RDouble **res = reinterpret_cast<RDouble **>(grids[z]->GetDataPtr("res"));
+            const int nc = grids[z]->GetNTotalCell();
+            for (int c = 0; c < nc; ++c) s += res[0][c] * res[0][c];
+            n += nc;
+        }
+        resHist.push_back(sqrt(s / n));
     }
     const double loopSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - loopStart).count();
     WriteRaw(outdir + "/iter_seconds.bin", &loopSeconds, 1);
     WriteRaw(outdir + "/res_hist.bin", resHist.data(), resHist.size());
 
-    for (int a = 6; a < argc; ++a)
+    for (int z = 0; z < nZones; ++z)
     {
-        char name[256];
-        int rows = 0, cols = 0;
-        if (sscanf(argv[a], "%255[^:]:%d:%d", name, &rows, &cols) != 3) Die("bad dump spec");
-        void *p = grid->GetDataPtr(name);
-        if (!p)
+        UnstructGrid *grid = grids[z];
+        const int nTotalCell = grid->GetNTotalCell();
+        const int nTotal = nTotalCell + grid->GetNBoundFace();
+        std::string outdir = argv[3];
+        if (nZones > 1)
         {
-            fprintf(stderr, "ref_harness: no array %s\n", name);
-            continue;
+            outdir += "/zone" + std::to_string(z);
+            mkdir(outdir.c_str(), 0755);
         }
-        std::vector<double> buf;
-        if (rows == 0)
+        for (int a = 6; a < argc; ++a)
         {
-            buf.assign((RDouble *)p, (RDouble *)p + cols);
+            char name[256];
+            int rows = 0, cols = 0;
+            if (sscanf(argv[a], "%255[^:]:%d:%d", name, &rows, &cols) != 3) Die("bad dump spec");
+            void *p = grid->GetDataPtr(name);
+            if (!p)
+            {
+                fprintf(stderr, "ref_harness: no array %s\n", name);
+                continue;
+            }
+            std::vector<double> buf;
+            if (rows == 0)
+            {
+                buf.assign((RDouble *)p, (RDouble *)p + cols);
+            }
+            else
+            {
+                RDouble **pp = reinterpret_cast<RDouble **>(p);
+                for (int r = 0; r < rows; ++r) buf.insert(buf.end(), pp[r], pp[r] + cols);
+            }
+            WriteRaw(outdir + "/" + name + ".bin", buf.data(), buf.size());
         }
-        else
+        // Geometry as the reference computed it.
+        WriteRaw(outdir + "/xfn.bin", grid->GetFaceNormalX(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/yfn.bin", grid->GetFaceNormalY(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/zfn.bin", grid->GetFaceNormalZ(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/area.bin", grid->GetFaceArea(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/xfc.bin", grid->GetFaceCenterX(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/yfc.bin", grid->GetFaceCenterY(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/zfc.bin", grid->GetFaceCenterZ(), grid->GetNTotalFace());
+        WriteRaw(outdir + "/xcc.bin", grid->GetCellCenterX(), nTotal);
+        WriteRaw(outdir + "/ycc.bin", grid->GetCellCenterY(), nTotal);
+        WriteRaw(outdir + "/zcc.bin", grid->GetCellCenterZ(), nTotal);
+        WriteRaw(outdir + "/vol.bin", grid->GetCellVolume(), nTotal);
+        if (grid->GetWallDist()) WriteRaw(outdir + "/walldist.bin", grid->GetWallDist(), nTotalCell);
+        // Wall force sums of NSSolverUnstruct::AirForceCoefParts (all parts): CA_f CA_p
+        // CN_f CN_p CZ_f CZ_p cpx cpy cpz Cl_f Cl_p Cn_f Cn_p Cm_f Cm_p hingeMoment.
         {
-            RDouble **pp = reinterpret_cast<RDouble **>(p);
-            for (int r = 0; r < rows; ++r) buf.insert(buf.end(), pp[r], pp[r] + cols);
+            NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(z, 0));
+            ActionKey *ak = new ActionKey();
+            ak->level = 0;
+            ns->AirForceCoefParts(ak, -1);
+            DataContainer *cd = ak->GetData();
+            cd->MoveToBegin();
+            std::vector<RDouble> f(16, 0.0);
+            for (int k = 0; k < 16; ++k) cd->Read(&f[k], sizeof(RDouble));
+            WriteRaw(outdir + "/forces.bin", f.data(), f.size());
+            delete ak;
         }
-        WriteRaw(outdir + "/" + name + ".bin", buf.data(), buf.size());
     }
-    // Geometry as the reference computed it.
-    WriteRaw(outdir + "/xfn.bin", grid->GetFaceNormalX(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/yfn.bin", grid->GetFaceNormalY(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/zfn.bin", grid->GetFaceNormalZ(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/area.bin", grid->GetFaceArea(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/xfc.bin", grid->GetFaceCenterX(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/yfc.bin", grid->GetFaceCenterY(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/zfc.bin", grid->GetFaceCenterZ(), grid->GetNTotalFace());
-    WriteRaw(outdir + "/xcc.bin", grid->GetCellCenterX(), nTotal);
-    WriteRaw(outdir + "/ycc.bin", grid->GetCellCenterY(), nTotal);
-    WriteRaw(outdir + "/zcc.bin", grid->GetCellCenterZ(), nTotal);
-    WriteRaw(outdir + "/vol.bin", grid->GetCellVolume(), nTotal);
-    if (grid->GetWallDist()) WriteRaw(outdir + "/walldist.bin", grid->GetWallDist(), nTotalCell);
-    // Wall force sums of NSSolverUnstruct::AirForceCoefParts (all parts): CA_f CA_p
-    // CN_f CN_p CZ_f CZ_p cpx cpy cpz Cl_f Cl_p Cn_f Cn_p Cm_f Cm_p hingeMoment.
-    {
-        NSSolverUnstruct *ns = static_cast<NSSolverUnstruct *>(GlobalSolvers::GetSolver(0, 0));
-        ActionKey *ak = new ActionKey();
-        ak->level = 0;
-        ns->AirForceCoefParts(ak, -1);
-        DataContainer *cd = ak->GetData();
-        cd->MoveToBegin();
-        std::vector<RDouble> f(16, 0.0);
-        for (int k = 0; k < 16; ++k) cd->Read(&f[k], sizeof(RDouble));
-        WriteRaw(outdir + "/forces.bin", f.data(), f.size());
-        delete ak;
-    }
-    fprintf(stdout, "ref_harness: done %d steps, nTotalCell=%d nBoundFace=%d\n", nSteps, nTotalCell, nBoundFace);
+    fprintf(stdout, "ref_harness: done %d steps, %d zone(s), zone 0 nTotalCell=%d nBoundFace=%d\n", nSteps, nZones,
+            grids[0]->GetNTotalCell(), grids[0]->GetNBoundFace());
     return 0;
 }

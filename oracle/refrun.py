@@ -105,3 +105,98 @@ def run_reference(mesh, params: dict, nsteps: int, dumps=(), state=None, workdir
             out[n] = out[n].reshape(r, c)
     out["_log"] = proc.stdout
     return out
+
+
+def interface_arrays(parts):
+    """Per part, the interface data a partitioned grid file of the reference
+    holds for a zone (IO_HDF5Read::ReadInterfaceInfo,
+    API/PreProcess/src/Pre_HDF5File.cpp:1366-1401): for each interface face k
+    (the part's boundary faces iface_first + k), the neighbouring zone, the
+    index of the same face in that zone's interface list, and the boundary
+    face number."""
+    index = []
+    for part in parts:
+        g = part.faces[part.iface_first:part.iface_first + part.n_iface]
+        index.append({int(f): k for k, f in enumerate(g)})
+    out = []
+    for part in parts:
+        n = part.n_iface
+        g = part.faces[part.iface_first:part.iface_first + n]
+        zone = np.empty(n, np.int32)
+        for q, other in enumerate(parts):
+            if q != part.rank:
+                hit = np.array([int(f) in index[q] for f in g], bool)
+                zone[hit] = q
+        inter = np.array([index[zone[k]][int(g[k])] for k in range(n)], np.int32)
+        out.append((zone, inter, np.arange(part.iface_first, part.iface_first + n, dtype=np.int32)))
+    return out
+
+
+def run_reference_zones(parts, params: dict, nsteps: int, dumps=(), states=None, workdir=None):
+    """`nsteps` outer iterations of the reference solver on the zones `parts`
+    (phenlei_b200.partition.split), all in one process as the reference runs
+    several zones on one rank.  dumps: (name, rows, cols) per zone, where
+    cols may be a callable of the part.  states: per zone the input field as
+    for run_reference.  Returns {"res_hist": global monitor, "zones": [dict per zone]}."""
+    from phenlei_b200.mesh import write_mesh
+
+    if not available():
+        raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle/refbuild REF=<root> all harness)")
+    tmp = os.path.abspath(workdir or tempfile.mkdtemp(prefix="phx_ref_zones_"))
+    for d in ("bin", "grid", "results", "out"):
+        os.makedirs(os.path.join(tmp, d), exist_ok=True)
+    p = dict(BASE_PARAMS)
+    p.update(params)
+    with open(os.path.join(tmp, "bin", "key.hypara"), "w") as f:
+        f.write('string title = "oracle";\n')
+        f.write(f'string defaultParaFile = "{DEFAULT_PARA}";\n')
+        f.write("int ndim = 3;\nint nparafile = 1;\nint nsimutask = 0;\n")
+        f.write('string parafilename = "./bin/case.hypara";\nint numberOfGridProcessor = 0;\n')
+    with open(os.path.join(tmp, "bin", "case.hypara"), "w") as f:
+        for k, v in p.items():
+            f.write(_fmt(k, v) + "\n")
+    with open(os.path.join(tmp, "bin", "boundary_condition.hypara"), "w") as f:
+        f.write("int nBoundaryConditions = 0;\n")
+    mpaths, spaths = [], []
+    for part, (zone, inter, bface) in zip(parts, interface_arrays(parts)):
+        mp = os.path.join(tmp, "grid", f"zone{part.rank}.bin")
+        write_mesh(mp, part.mesh)
+        with open(mp + ".itf", "wb") as f:
+            np.array([len(zone)], "<i8").tofile(f)
+            for a in (zone, inter, bface):
+                np.ascontiguousarray(a, "<i4").tofile(f)
+        mpaths.append(mp)
+        if states is not None:
+            sp = os.path.join(tmp, "grid", f"state{part.rank}.bin")
+            np.ascontiguousarray(states[part.rank], dtype="<f8").tofile(sp)
+            spaths.append(sp)
+    spec = []
+    for (n, r, c) in dumps:
+        spec.append((n, r, c))
+    # the dump sizes differ per zone: dump the largest and cut per zone
+    args = [HARNESS, ",".join(mpaths), tmp, os.path.join(tmp, "out"), str(nsteps), ",".join(spaths) or "-"]
+    sizes = {}
+    for (n, r, c) in spec:
+        cmax = max(c(part) for part in parts) if callable(c) else c
+        sizes[n] = (r, c)
+        args.append(f"{n}:{r}:{cmax}")
+    env = dict(os.environ)
+    env.pop("PHX_REF_WALLDIST", None)
+    proc = subprocess.run(args, capture_output=True, text=True, env=env)
+    if proc.returncode != 0:
+        raise RuntimeError(f"reference harness failed ({proc.returncode}):\n{proc.stdout[-4000:]}\n{proc.stderr[-4000:]}")
+    res = {"res_hist": np.fromfile(os.path.join(tmp, "out", "res_hist.bin"), dtype="<f8"), "zones": [],
+           "_log": proc.stdout}
+    for part in parts:
+        zdir = os.path.join(tmp, "out", f"zone{part.rank}")
+        z = {}
+        for fn in os.listdir(zdir):
+            if fn.endswith(".bin"):
+                z[fn[:-4]] = np.fromfile(os.path.join(zdir, fn), dtype="<f8")
+        for n, (r, c) in sizes.items():
+            if n in z:
+                cz = c(part) if callable(c) else c
+                cmax = z[n].size // max(r, 1)
+                z[n] = z[n].reshape(r, cmax)[:, :cz] if r > 0 else z[n][:cz]
+        res["zones"].append(z)
+    return res

@@ -20,7 +20,6 @@ namespace phx {
 //  GRADIENT  kG T: the gradient record, slot 15 (padding) carrying the limiter
 //  DQ        kD T: the forward-sweep dq record
 //  TURB      2 doubles: master nu~, eddy viscosity
-//  TURB_DQ   1 T: the forward-sweep SA dq
 template <class T>
 size_t halo_row_bytes(int field)
 {
@@ -29,7 +28,6 @@ size_t halo_row_bytes(int field)
     case PHX_HALO_GRADIENT: return kG * sizeof(T);
     case PHX_HALO_DQ: return kD * sizeof(T);
     case PHX_HALO_TURB: return 2 * sizeof(double);
-    case PHX_HALO_TURB_DQ: return sizeof(T);
     default: return 0;
     }
 }
@@ -62,8 +60,6 @@ __global__ void __launch_bounds__(kThreads) halo_pack_kernel(DevGrid g, int fiel
         double *o = reinterpret_cast<double *>(buf) + (size_t)i * 2;
         o[0] = t.qt64[c];
         o[1] = (double)w.trec[(size_t)c * kTr + 1];
-    } else if (field == PHX_HALO_TURB_DQ) {
-        reinterpret_cast<T *>(buf)[i] = t.tdqf[c];
     }
 }
 
@@ -103,8 +99,6 @@ __global__ void __launch_bounds__(kThreads) halo_unpack_kernel(DevGrid g, NsCons
         t.qt64[c] = v[0];
         w.trec[(size_t)c * kTr] = (T)v[0];
         w.trec[(size_t)c * kTr + 1] = (T)v[1];
-    } else if (field == PHX_HALO_TURB_DQ) {
-        t.tdqf[c] = reinterpret_cast<const T *>(buf)[i];
     }
 }
 

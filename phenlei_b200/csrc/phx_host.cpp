@@ -700,7 +700,7 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     r |= dalloc(ctx, &t.tface, nf * kTf);
     r |= dalloc(ctx, &t.tcoef, 2 * nf);
     r |= dalloc(ctx, &t.tdq, nc);
-    r |= dalloc(ctx, &t.tdqf, nt);
+    r |= dalloc(ctx, &t.tdqf, nc);
     r |= dalloc(ctx, &t.tdfl, nc);
     r |= dalloc(ctx, &t.tsrc, nc);
     if (ctx->prm.gradientName == 2) r |= dalloc(ctx, &t.qtnode, (size_t)ctx->nNode);
@@ -722,7 +722,6 @@ int make_turb(phx_ctx *ctx, Work<T> &w, TurbWork<T> &t)
     PHX_CUDA(ctx, cudaMemcpy(t.qt64, q.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
     PHX_CUDA(ctx, cudaMemcpy(w.trec, rec.data(), sizeof(T) * nt * kTr, cudaMemcpyHostToDevice));
     PHX_CUDA(ctx, cudaMemset(t.tcoef, 0, sizeof(T) * 2 * nf));
-    PHX_CUDA(ctx, cudaMemset(t.tdqf, 0, sizeof(T) * nt));   // interface ghost rows until the first exchange
     return PHX_OK;
 }
 
@@ -1789,7 +1788,7 @@ int phx_set_halo(phx_ctx *ctx, int64_t n_send, const int32_t *send_cells, int64_
 
 static bool halo_field_ok(const phx_ctx *ctx, int field)
 {
-    if (field == PHX_HALO_TURB || field == PHX_HALO_TURB_DQ) return ctx->sa;
+    if (field == PHX_HALO_TURB) return ctx->sa;
     return field >= PHX_HALO_Q && field <= PHX_HALO_DQ;
 }
 

@@ -166,7 +166,7 @@ struct TurbWork {
     T *tface;       // [nFace][kTf] face terms
     T *tcoef;       // [2 nFace] LU-SGS matrix of each face use (side 0: left cell's view = mat_turbr)
     T *tdq;         // [nCell] LU-SGS dq (backward sweep; write-once per sweep)
-    T *tdqf;        // [nTotal] forward-sweep dq (write-once per sweep; interface ghosts from the halo exchange)
+    T *tdqf;        // [nCell] forward-sweep dq (write-once per sweep)
     T *tdfl;        // [nCell] forward delta flux (write-once per sweep)
     T *tsrc;        // [nCell] source computed by the learned-source kernel (sa_source != 0)
     T *qtnode;      // [nNode] GG-node node values of nu~ for the next SA gradient (GG-node runs; else null)

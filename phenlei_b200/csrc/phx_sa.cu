@@ -207,8 +207,8 @@ __global__ void __launch_bounds__(kThreads) sa_face_kernel(DevGrid g, NsConst c,
     if (f >= g.nFace) return;
     const int2 lr = ld(g.lr + f);
     const int le = lr.x, re = lr.y;
-    // interface faces are interior faces for the face states and face values
-    // (TurbSolverUnstr.cpp:5041, :5125, :3950, :4569)
+    // interface faces are interior faces for the face states (GetQlQrTurbulence,
+    // GetQlQrNS, TurbSolverUnstr.cpp:5041, :5125) and the normal derivative (:4569)
     const bool bnd = f < g.nBFace && g.bkind[f] != BK_INTERFACE;
     const int bt = bnd ? g.btype[f] : 0;
     double fr[8];
@@ -239,11 +239,13 @@ __global__ void __launch_bounds__(kThreads) sa_face_kernel(DevGrid g, NsConst c,
         const T vnrr = T(0.5) * (vnr - fabs(vnr));
         out[0] = (vnll * ql + vnrr * qr) * area;
     }
-    // diffusion
+    // diffusion: the face value mlt takes interface faces as boundary faces
+    // (GetVisFaceValue's mlt loop, TurbSolverUnstr.cpp:3990-4003); the normal
+    // derivative below takes them as interior faces (:4569)
     {
         T nl = tl[0], nr = tr[0];
         const T vl = tl[2], vr = tr[2], rl = qL[0], rr = qR[0];
-        if (bnd) {
+        if (f < g.nBFace) {
             if (nl < T(0)) {
                 nl = positive_sa(nl, vl, rl);
                 if (bt == PHX_BC_SOLID_SURFACE) nr = -nl;
@@ -412,10 +414,10 @@ void launch_sa_residual(const DevGrid &g, const NsConst &c, const double *q64, c
 // the face matrices of each face use.  Same dataflow schedule, write-once
 // records and bounded waits as the NS sweep (phx_kernels.cu): tdqf (forward
 // dq), tdfl (forward delta flux) and tdq (final dq) hold the sentinel until
-// written.  dq of a boundary ghost is the ghost residual, which is zero, so
-// those entries of the backward sweep add nothing and are skipped; an
-// interface ghost holds the neighbouring zone's forward dq, set by the halo
-// exchange between the sweeps, and is read like a cell's.
+// written.  dq of the ghosts is the ghost residual, which is zero, so ghost
+// entries of the backward sweep add nothing and are skipped; an interface
+// ghost's too, as the reference exchanges no SA dq between the sweeps
+// (Controller::CommunicationDQ, CFD/Solver/src/Controller.cpp:2874-2880).
 // ---------------------------------------------------------------------------
 // Static inputs of one slot for one lane (loaded a round ahead): neighbour
 // (-1: none or a ghost), its face matrix, and (lane 0 of the cell's first
@@ -433,7 +435,7 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
     s.cell = info.x;
     s.count = info.y;
     s.nb = -1;
-    if (info.x >= 0 && en.x >= 0 && (en.x < g.nCell || ld(g.bkind + (en.x - g.nCell)) == BK_INTERFACE)) {
+    if (info.x >= 0 && en.x >= 0 && en.x < g.nCell) {
         s.nb = en.x;
         s.mat = t.tcoef[en.z];
     }
@@ -447,17 +449,16 @@ __device__ __forceinline__ void sa_sweep_load(const DevGrid &g, const TurbWork<T
 
 template <class T, bool kForward>
 __device__ __forceinline__ bool sa_sweep_position(const TurbWork<T> &t, Reduce *red, const SaSweepIn<T> &s, int lane,
-                                                  int base, long long spinLimit, int nCell)
+                                                  int base, long long spinLimit)
 {
     const int cell = s.cell;
     const bool live = cell >= 0;
     const bool lead = live && s.count >= 0;   // the cell's first slot
     const int e1 = lead ? s.count : 0;
     const bool has = live && s.nb >= 0;
-    // the neighbour's dq (forward: its forward dq; backward: its final dq,
-    // or an interface ghost's forward dq) and, backward, this cell's forward
-    // delta flux
-    const T *src1 = has ? (kForward || s.nb >= nCell ? t.tdqf : t.tdq) + s.nb : nullptr;
+    // the neighbour's dq (forward: its forward dq; backward: its final dq)
+    // and, backward, this cell's forward delta flux
+    const T *src1 = has ? (kForward ? t.tdqf : t.tdq) + s.nb : nullptr;
     const T *src2 = (!kForward && lead && lane == 0) ? t.tdfl + cell : nullptr;
     T v1 = T(0), fl = T(0);
     bool r1 = true, r2 = true;
@@ -528,7 +529,7 @@ __device__ __forceinline__ bool sa_sweep_all(const DevGrid &g, const TurbWork<T>
         SaSweepIn<T> nxt;
         sa_sweep_load<T>(g, t, info, en, lane, nxt);
         entry(p + 2 * ngroups, info, en);
-        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base, spinLimit, g.nCell)) return false;
+        if (!sa_sweep_position<T, kForward>(t, red, cur, lane, base, spinLimit)) return false;
         if (en.x >= 0 && en.x < g.nCell) prefetch_l2(t.tcoef + en.z);
         if (lane == 0 && info.x >= 0 && info.y >= 0) prefetch_l2(t.tcrec + (size_t)info.x * kTc);
         cur = nxt;

@@ -25,7 +25,7 @@ PHX_Q_TURB, PHX_VISL, PHX_VIST, PHX_RES_TURB = 10, 11, 12, 13
 PHX_SA_SRC = 15
 PHX_GRAD_TURB = 16
 # halo fields of a partitioned grid (include/phx.h PHX_HALO_*)
-PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB, PHX_HALO_TURB_DQ = range(5)
+PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB = range(4)
 ERRORS = {-1: "PHX_ERR_ARG", -2: "PHX_ERR_CUDA", -3: "PHX_ERR_TIMEOUT", -4: "PHX_ERR_NUMERIC", -5: "PHX_ERR_STATE"}
 
 _dp = C.POINTER(C.c_double)

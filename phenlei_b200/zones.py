@@ -12,14 +12,17 @@ then exchanges, through Controller::CommunicationInterfaceData (:3389):
 * the minimum local time step over all zones before the ktmax clamp
   (Controller::GetGlobalMinTimeStep, :720-751);
 * dq between the forward and the backward LU-SGS sweep (Controller::LUSGS,
-  :1917-1924, CommunicationDQ :2874);
+  :1917-1924, CommunicationDQ :2874), for the NS solver and when swapDq is
+  set (the reference's parameter file sets it);
 * the residual sums (PH_AllReduce);
 * q after the update (NSSolver::PostSolve, CFD/NSSolver/src/NSSolver.cpp:139-142);
-* with Spalart-Allmaras, the SA dq between its sweeps and nu~ with the eddy
-  viscosity after its update (TurbSolverUnstr::UploadInterfaceValue,
-  CFD/TurbSolver/src/TurbSolverUnstr.cpp:7130-7145).  The reference also
-  exchanges the gradient of nu~; here only a cell's own gradient is ever read,
-  so that exchange moves nothing anyone reads and is left out.
+* with Spalart-Allmaras, nu~ with the eddy viscosity after its update
+  (TurbSolverUnstr::UploadInterfaceValue,
+  CFD/TurbSolver/src/TurbSolverUnstr.cpp:7130-7145); the SA dq is not
+  exchanged between its sweeps (CommunicationDQ serves the NS solver only).
+  The reference also exchanges the gradient of nu~; here only a cell's own
+  gradient is ever read, so that exchange moves nothing anyone reads and is
+  left out.
 
 The set-up follows Region::SwapGeometry (API/Physics/src/Region.cpp:3257-3268):
 the interface ghosts take the neighbouring cells' centres and volumes and the
@@ -40,8 +43,8 @@ from __future__ import annotations
 import numpy as np
 
 from . import partition as P
-from .solver import (PHX_HALO_DQ, PHX_HALO_GRADIENT, PHX_HALO_Q, PHX_HALO_TURB, PHX_HALO_TURB_DQ,
-                     NSSolverUnstruct, PhxError, force_coefficients)
+from .solver import (PHX_HALO_DQ, PHX_HALO_GRADIENT, PHX_HALO_Q, PHX_HALO_TURB, NSSolverUnstruct, PhxError,
+                     force_coefficients)
 
 
 def channel_zone(rank: int, world: int, **channel_kw) -> P.Part:
@@ -109,7 +112,7 @@ class _Zones:
     """The phase sequence of one partitioned outer iteration over the zones
     this process drives; subclasses move the halo rows and form the sums."""
 
-    FIELDS = (PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB, PHX_HALO_TURB_DQ)
+    FIELDS = (PHX_HALO_Q, PHX_HALO_GRADIENT, PHX_HALO_DQ, PHX_HALO_TURB)
 
     def _setup(self, mesh, parts, params, precision, wall_of):
         """wall_of(part): the part's wall distances, or None."""
@@ -119,6 +122,7 @@ class _Zones:
             raise ValueError("GG-node across zones needs the interpoint exchange; not built")
         self.mesh = mesh
         self.sa = params.get("viscousType", 0) == 3
+        self.swap_dq = int(params.get("swapDq", 1)) != 0
         if self.sa and wall_of is None:
             raise ValueError("the SA model needs the wall distance of every cell")
         self.zones = [NSSolverUnstruct(p.mesh, precision=precision, wall_dist=None if wall_of is None else wall_of(p),
@@ -134,7 +138,7 @@ class _Zones:
         for z, (send, recv, _, _) in zip(self.zones, self.plans):
             b = {}
             for f in self.FIELDS:
-                if f in (PHX_HALO_TURB, PHX_HALO_TURB_DQ) and not self.sa:
+                if f == PHX_HALO_TURB and not self.sa:
                     continue
                 w = z.halo_row_bytes(f)
                 b[f] = (torch.empty(max(len(send), 1) * w, dtype=torch.uint8, device=dev),
@@ -218,7 +222,8 @@ class _Zones:
             for z in zs:
                 z.set_min_timestep(mindt)
             phase("lusgs", lambda z: z.LUSGSForward())
-            self._exchange(PHX_HALO_DQ)
+            if self.swap_dq:
+                self._exchange(PHX_HALO_DQ)
             phase("lusgs", lambda z: z.LUSGSBackward())
             s = 0.0
             for z in zs:
@@ -231,7 +236,6 @@ class _Zones:
             if self.sa:
                 phase("sa_residual", lambda z: z.TurbUpdateResiduals())
                 phase("sa_lusgs", lambda z: z.TurbLUSGSForward())
-                self._exchange(PHX_HALO_TURB_DQ)
                 phase("sa_lusgs", lambda z: z.TurbLUSGSBackward())
                 phase("sa_update", lambda z: z.TurbUpdateFlowField())
                 self._exchange(PHX_HALO_TURB)

@@ -110,6 +110,56 @@ def fixture(name, kind, args, params, nsteps, perturb_seed=None, amplitude=0.02,
     print(path, os.path.getsize(path))
 
 
+def zone_fixture(name, kind, args, params, nsteps, nparts, perturb_seed, turb_seed=None):
+    """The reference run on `nparts` zones of the mesh (phenlei_b200.partition:
+    slab_owner, then split), all on one rank as the reference runs several
+    zones per process, with the reference's interface exchanges.  Stores the
+    partition (owner), the input state, the global residual monitor and the
+    zones' arrays gathered into global cell order."""
+    from oracle.refrun import run_reference_zones
+    from phenlei_b200 import partition as P
+
+    m = getattr(M, kind)(**args)
+    nc = m.n_cell
+    owner = P.slab_owner(m, nparts)
+    parts = P.split(m, owner)
+    q0 = perturbed_state(m, params, seed=perturb_seed)
+    sa = params.get("viscousType", 0) == 3
+    state = q0
+    if sa:
+        state = np.vstack([q0, turb_state(m, params, turb_seed)[None, :]])
+    nt = lambda p: p.mesh.n_cell + p.mesh.n_bface  # noqa: E731
+    ncz = lambda p: p.mesh.n_cell  # noqa: E731
+    dumps = [("q", 5, nt), ("res", 5, nt), ("dt", 0, nt), ("limit2D", 5, nt), ("gradPrimtiveVarX", 5, nt)]
+    if sa:
+        dumps += [("q_turb", 1, nt), ("vist", 0, nt), ("walldist", 0, ncz)]
+    r = run_reference_zones(parts, params, nsteps, dumps=dumps, states=[state[:, p.cells] for p in parts])
+    out = {"params": json.dumps(params), "mesh": json.dumps({"kind": kind, "args": args}), "nsteps": nsteps,
+           "nparts": nparts, "owner": owner.astype(np.int32), "state_in": state, "res_hist": r["res_hist"]}
+    gathered = {"q": np.zeros((5, nc)), "res": np.zeros((5, nc)), "dt": np.zeros(nc), "limit": np.zeros(nc),
+                "gradPrimtiveVarX": np.zeros((5, nc))}
+    if sa:
+        gathered.update(q_turb=np.zeros(nc), vist=np.zeros(nc), walldist=np.zeros(nc))
+    forces = np.zeros(16)
+    for part, z in zip(parts, r["zones"]):
+        c, n = part.cells, part.mesh.n_cell
+        gathered["q"][:, c] = z["q"][:, :n]
+        gathered["res"][:, c] = z["res"][:, :n]
+        gathered["dt"][c] = z["dt"][:n]
+        gathered["limit"][c] = z["limit2D"][0, :n]
+        gathered["gradPrimtiveVarX"][:, c] = z["gradPrimtiveVarX"][:, :n]
+        if sa:
+            gathered["q_turb"][c] = z["q_turb"].reshape(-1)[:n]
+            gathered["vist"][c] = z["vist"][:n]
+            gathered["walldist"][c] = z["walldist"][:n]
+        forces += z["forces"]
+    out.update(gathered)
+    out["forces"] = forces
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path))
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     if only:
@@ -118,6 +168,12 @@ if __name__ == "__main__":
         def fixture(name, *a, **k):  # noqa: F811 - regenerate the named fixtures only
             if name in only:
                 _fixture(name, *a, **k)
+
+        _zone_fixture = zone_fixture
+
+        def zone_fixture(name, *a, **k):  # noqa: F811
+            if name in only:
+                _zone_fixture(name, *a, **k)
     # Euler bump, seeded perturbation, one iteration: every intermediate array.
     fixture("euler_bump_16x8x2_step1", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, EULER_BUMP, 1, perturb_seed=7)
     # Euler bump from the free stream, 40 iterations through the CFL ramp.
@@ -198,3 +254,15 @@ if __name__ == "__main__":
             SA_PLATE, 2, perturb_seed=7, turb_seed=5)
     fixture("sa_plate_16x8x2_ausmpwp_step20", "flat_plate", {"nx": 16, "ny": 8, "nz": 2, "first_spacing": 1e-4},
             SA_PLATE, 20)
+    # Partitioned grids: the reference's own run on 2 and 3 zones of the bump (slab
+    # partition), interface exchanges between the zones, 10 iterations.
+    zone_fixture("zones2_euler_bump_16x8x2_step10", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, EULER_BUMP, 10,
+                 2, perturb_seed=3)
+    zone_fixture("zones3_laminar_bump_16x8x2_lsq_step10", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+                 dict(LAMINAR, gradientName="lsq"), 10, 3, perturb_seed=5)
+    zone_fixture("zones2_euler_bump_16x8x2_barth_ktmax_step10", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
+                 dict(EULER_BUMP, uns_limiter_name="barth", ktmax=1.5), 10, 2, perturb_seed=7)
+    zone_fixture("zones2_sa_bump_16x8x2_step10", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, SA, 10, 2,
+                 perturb_seed=7, turb_seed=9)
+    zone_fixture("zones3_sa_bump_16x8x2_prism_step5", "channel_bump", {"nx": 16, "ny": 8, "nz": 2, "prism_layers": 3},
+                 SA, 5, 3, perturb_seed=11, turb_seed=13)

@@ -153,3 +153,37 @@ def test_oracle_matches_reference_sa_ggnode(golden, name):
     assert rel_err(o.work("dntx")[:nc], d["gradTurbulenceX"][:nc]) <= 1e-12
     assert rel_err(o.work("qtnode"), d["qTurbNode"]) <= 1e-14
     assert rel_err(o.forces(), d["forces"]) <= 1e-12
+
+
+ZONE_CASES = ["zones2_euler_bump_16x8x2_step10", "zones3_laminar_bump_16x8x2_lsq_step10",
+              "zones2_euler_bump_16x8x2_barth_ktmax_step10", "zones2_sa_bump_16x8x2_step10",
+              "zones3_sa_bump_16x8x2_prism_step5"]
+
+
+@pytest.mark.parametrize("name", ZONE_CASES)
+def test_partitioned_oracle_matches_reference_zones(golden, name):
+    """The oracle on a partitioned grid (oracle/partitioned.py) against the
+    reference's own run on the same zones, all on one rank: interface ghosts,
+    SwapGeometry, the minimum time step over the zones, the NS dq exchanged
+    between the sweeps and no SA dq, over 5-10 iterations."""
+    from oracle.partitioned import PartitionedOracle
+
+    d = golden(name)
+    m = d["mesh_obj"]
+    nc = m.n_cell
+    params = d["params_dict"]
+    sa = params.get("viscousType", 0) == 3
+    po = PartitionedOracle(m, params, int(d["nparts"]), owner=d["owner"],
+                           wall_dist=d["walldist"] if sa else None)
+    st = d["state_in"]
+    po.set_state(st[:5], st[5] if sa else None)
+    hist = po.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-12
+    assert rel_err(po.gather("q"), d["q"]) <= 1e-12
+    assert rel_err(po.gather("res"), d["res"]) <= 1e-12
+    assert rel_err(po.gather("dt"), d["dt"]) <= 1e-12
+    assert rel_err(po.gather("limit"), d["limit"]) <= 1e-12
+    assert rel_err(po.gather("dqdx"), d["gradPrimtiveVarX"]) <= 1e-12
+    if sa:
+        assert rel_err(po.gather("qt"), d["q_turb"]) <= 1e-12
+        assert rel_err(po.gather("vist"), d["vist"]) <= 1e-12

@@ -1,8 +1,9 @@
 """The CUDA solver on a partitioned grid (phenlei_b200.zones): one context per
 zone on one GPU, joined by interface faces (PHENGLEI::INTERFACE), stepped
 phase by phase with the halo rows moved between the zones by the host, against
-the oracle's partitioned run (oracle/partitioned.py) on the same seeded
-inputs, meshes and partitions.  No kernel waits on another zone.
+the reference's own runs on the same zones (golden fixtures) and the oracle's
+partitioned run (oracle/partitioned.py, itself pinned to those fixtures) on
+seeded inputs, meshes and partitions.  No kernel waits on another zone.
 
 Tolerances (norm-wise, max|a-b|/max|ref|): FP64 1e-12 per array after one
 iteration and 1e-10 over ten-iteration histories; mixed precision 1e-5 after
@@ -217,3 +218,33 @@ def test_distributed_zones_world_size_2_equal_the_zone_set(tmp_path, case):
         assert np.array_equal(d["hist"], h)
         assert np.array_equal(d["q"], zs.zones[r].get(S.PHX_Q)[:, : zs.zones[r].mesh.n_cell])
         assert rel_err(d["forces"], f) <= 1e-14
+
+
+@pytest.mark.parametrize("name", ["zones2_euler_bump_16x8x2_step10", "zones3_laminar_bump_16x8x2_lsq_step10",
+                                  "zones2_euler_bump_16x8x2_barth_ktmax_step10", "zones2_sa_bump_16x8x2_step10",
+                                  "zones3_sa_bump_16x8x2_prism_step5"])
+def test_fp64_zones_match_reference_golden(golden, name):
+    """The CUDA zones against the reference's own run on the same zones
+    (tests/golden/make_golden.py, zone_fixture): residual history, state,
+    residual, time step, limiter, gradient and wall forces after 5-10
+    iterations."""
+    from phenlei_b200.zones import ZoneSet
+
+    d = golden(name)
+    m = d["mesh_obj"]
+    params = d["params_dict"]
+    sa = params.get("viscousType", 0) == 3
+    zs = ZoneSet(m, params, int(d["nparts"]), owner=d["owner"], wall_dist=d["walldist"] if sa else None)
+    st = d["state_in"]
+    zs.set_state(st[:5], st[5] if sa else None)
+    hist = zs.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-10
+    assert rel_err(zs.gather(S.PHX_Q), d["q"]) <= 1e-10
+    assert rel_err(zs.gather(S.PHX_RES), d["res"]) <= 1e-10
+    assert rel_err(zs.gather(S.PHX_DT), d["dt"]) <= 1e-10
+    assert rel_err(zs.gather(S.PHX_LIMIT), d["limit"]) <= 1e-10
+    assert rel_err(zs.gather(S.PHX_GRADX), d["gradPrimtiveVarX"]) <= 1e-10
+    assert rel_err(zs.forces(), d["forces"]) <= 1e-10
+    if sa:
+        assert rel_err(zs.gather(S.PHX_Q_TURB), d["q_turb"]) <= 1e-10
+        assert rel_err(zs.gather(S.PHX_VIST), d["vist"]) <= 1e-10
