@@ -174,7 +174,8 @@ int phx_set_stream(phx_ctx *ctx, void *stream);
 int phx_device(const phx_ctx *ctx);
 
 /* Host <-> device state copies in the reference SoA layout.  n is the element
- * count of the host array (checked against the selector's size). */
+ * count of the host array (checked against the selector's size).  PHX_Q,
+ * PHX_Q_TURB and PHX_VIST can be set; every selector can be read. */
 int phx_set_state(phx_ctx *ctx, int which, const double *host, int64_t n);
 int phx_get_state(phx_ctx *ctx, int which, double *host, int64_t n);
 /* Device-pointer variants (FP64 device memory of the same layout). */
@@ -374,6 +375,21 @@ int phx_ns_set_min_timestep(phx_ctx *ctx, double value);
  * phase calls above only launch; phx_ns_relaxation checks the same status
  * itself. */
 int phx_step_status(phx_ctx *ctx);
+
+/* Restart files.  phx_write_restart writes what the reference's restart holds
+ * (NSSolverUnstruct::DumpRestartH5, CFD/NSSolver/src/NSSolverUnstruct.cpp:1247-1320;
+ * TurbSolverUnstr::DumpRestartH5, CFD/TurbSolver/src/TurbSolverUnstr.cpp:506-560):
+ * the outer step (outnstep), the primitive state q of cells and ghosts and,
+ * with SA, q_turb and the eddy viscosity (visturb), in FP64, plus the
+ * learned-source model when one is set; in a binary layout of its own (this
+ * library reads no HDF5).  phx_read_restart loads such a file into a context
+ * of the same grid (PHX_ERR_ARG when the cell or boundary-face counts differ,
+ * as ReadRestartH5 checks nTotalCell, TurbSolverUnstr.cpp:669-676), so the run
+ * continues from that step: an uninterrupted run and a restarted one give the
+ * same state bit for bit (GG-cell and least-squares gradients; GG-node forms
+ * its node values from the loaded state, as the reference's restart does). */
+int phx_write_restart(phx_ctx *ctx, const char *path);
+int phx_read_restart(phx_ctx *ctx, const char *path);
 
 /* Outer step counter (drives the CFL ramp of NSSolver::ComputeCFL). */
 int phx_set_step(phx_ctx *ctx, int step);

@@ -1370,6 +1370,18 @@ static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n,
 {
     if (!ctx || !src) return PHX_ERR_ARG;
     const int nt = ctx->nTotal;
+    if (which == PHX_VIST) {
+        if (!ctx->sa) return fail(ctx, PHX_ERR_ARG, "SA state selector on a context without the SA model");
+        if (n != (int64_t)nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
+        PHX_CUDA(ctx, cudaMemcpyAsync(ctx->tmp, src, sizeof(double) * n, hostSide ? cudaMemcpyHostToDevice
+                                                                                 : cudaMemcpyDeviceToDevice, ctx->stream));
+        if (ctx->mixed) launch_import_vist<float>(ctx->g, ctx->tmp, ctx->w32, ctx->stream);
+        else launch_import_vist<double>(ctx->g, ctx->tmp, ctx->w64, ctx->stream);
+        int rc = check_launch(ctx);
+        if (rc) return rc;
+        PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return PHX_OK;
+    }
     if (which == PHX_Q_TURB) {
         if (!ctx->sa) return fail(ctx, PHX_ERR_ARG, "SA state selector on a context without the SA model");
         if (n != (int64_t)nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
@@ -1383,7 +1395,7 @@ static int set_state_impl(phx_ctx *ctx, int which, const double *src, int64_t n,
         PHX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         return PHX_OK;
     }
-    if (which != PHX_Q) return fail(ctx, PHX_ERR_ARG, "only PHX_Q and PHX_Q_TURB can be set");
+    if (which != PHX_Q) return fail(ctx, PHX_ERR_ARG, "only PHX_Q, PHX_Q_TURB and PHX_VIST can be set");
     if (n != (int64_t)5 * nt) return fail(ctx, PHX_ERR_ARG, "state size does not match the selector");
     PHX_CUDA(ctx, cudaMemcpyAsync(ctx->tmp, src, sizeof(double) * n, hostSide ? cudaMemcpyHostToDevice
                                                                              : cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1862,6 +1874,93 @@ int phx_step_status(phx_ctx *ctx)
     if (err == PHX_ERR_TIMEOUT) return fail(ctx, PHX_ERR_TIMEOUT, "LU-SGS dependency wait timed out");
     if (err == PHX_ERR_NUMERIC) return fail(ctx, PHX_ERR_NUMERIC, "residual is not finite (divergence)");
     return PHX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Restart files: the content of the reference's restart (Version, outnstep,
+// nTotalCell, q; with SA q_turb and visturb) and the learned-source model.
+// Layout (little-endian): "PHXRST01", int32 version, int32 flags (1: SA
+// arrays, 2: model), int64 nCell, nBFace, outnstep, then q [5][nTotal], with
+// SA q_turb [nTotal] and visturb [nTotal] (FP64, reference order), and with a
+// model int64 n and n floats.
+// ---------------------------------------------------------------------------
+static const char kRestartMagic[8] = {'P', 'H', 'X', 'R', 'S', 'T', '0', '1'};
+static constexpr int32_t kRestartVersion = 1;
+
+int phx_write_restart(phx_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return PHX_ERR_ARG;
+    const int64_t nt = ctx->nTotal;
+    std::vector<double> q((size_t)(5 * nt)), qt, vt;
+    int rc = phx_get_state(ctx, PHX_Q, q.data(), 5 * nt);
+    if (rc) return rc;
+    if (ctx->sa) {
+        qt.resize((size_t)nt);
+        vt.resize((size_t)nt);
+        if ((rc = phx_get_state(ctx, PHX_Q_TURB, qt.data(), nt))) return rc;
+        if ((rc = phx_get_state(ctx, PHX_VIST, vt.data(), nt))) return rc;
+    }
+    const bool model = ctx->sa && ctx->mlpReady;
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(ctx, PHX_ERR_ARG, std::string("cannot write ") + path);
+    const int32_t hdr[2] = {kRestartVersion, (ctx->sa ? 1 : 0) | (model ? 2 : 0)};
+    const int64_t sizes[3] = {ctx->nCell, ctx->nBFace, ctx->step};
+    bool ok = fwrite(kRestartMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof(hdr), 1, f) == 1 &&
+              fwrite(sizes, sizeof(sizes), 1, f) == 1 && fwrite(q.data(), sizeof(double), q.size(), f) == q.size();
+    if (ok && ctx->sa)
+        ok = fwrite(qt.data(), sizeof(double), qt.size(), f) == qt.size() &&
+             fwrite(vt.data(), sizeof(double), vt.size(), f) == vt.size();
+    if (ok && model) {
+        const int64_t n = (int64_t)ctx->mlpBlob.size();
+        ok = fwrite(&n, sizeof(n), 1, f) == 1 && fwrite(ctx->mlpBlob.data(), sizeof(float), (size_t)n, f) == (size_t)n;
+    }
+    ok = (fclose(f) == 0) && ok;
+    return ok ? PHX_OK : fail(ctx, PHX_ERR_ARG, std::string("short write to ") + path);
+}
+
+int phx_read_restart(phx_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return PHX_ERR_ARG;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(ctx, PHX_ERR_ARG, std::string("cannot read ") + path);
+    char magic[8];
+    int32_t hdr[2];
+    int64_t sizes[3];
+    auto bad = [&](const char *why) {
+        fclose(f);
+        return fail(ctx, PHX_ERR_ARG, std::string("restart ") + path + ": " + why);
+    };
+    if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kRestartMagic, 8) != 0) return bad("not a phx restart file");
+    if (fread(hdr, sizeof(hdr), 1, f) != 1 || hdr[0] != kRestartVersion) return bad("unknown version");
+    if (fread(sizes, sizeof(sizes), 1, f) != 1) return bad("short header");
+    // as TurbSolverUnstr::ReadRestartH5 checks nTotalCell against the grid (TurbSolverUnstr.cpp:669-676)
+    if (sizes[0] != ctx->nCell || sizes[1] != ctx->nBFace) return bad("cell or boundary-face count differs from the grid");
+    if (((hdr[1] & 1) != 0) != ctx->sa) return bad("SA arrays present in one of file and context only");
+    if (sizes[2] < 0 || sizes[2] > 0x7fffffff) return bad("bad step");
+    const int64_t nt = ctx->nTotal;
+    std::vector<double> q((size_t)(5 * nt)), qt, vt;
+    if (fread(q.data(), sizeof(double), q.size(), f) != q.size()) return bad("short q");
+    if (ctx->sa) {
+        qt.resize((size_t)nt);
+        vt.resize((size_t)nt);
+        if (fread(qt.data(), sizeof(double), qt.size(), f) != qt.size() ||
+            fread(vt.data(), sizeof(double), vt.size(), f) != vt.size())
+            return bad("short SA arrays");
+    }
+    std::vector<float> blob;
+    if (hdr[1] & 2) {
+        int64_t n = 0;
+        if (fread(&n, sizeof(n), 1, f) != 1 || n != kMlpBlobFloats) return bad("bad model size");
+        blob.resize((size_t)n);
+        if (fread(blob.data(), sizeof(float), blob.size(), f) != blob.size()) return bad("short model");
+    }
+    fclose(f);
+    int rc = phx_set_state(ctx, PHX_Q, q.data(), 5 * nt);
+    if (!rc && ctx->sa) rc = phx_set_state(ctx, PHX_Q_TURB, qt.data(), nt);
+    if (!rc && ctx->sa) rc = phx_set_state(ctx, PHX_VIST, vt.data(), nt);
+    if (!rc && !blob.empty()) rc = phx_mlp_set(ctx, blob.data(), (int64_t)blob.size());
+    if (!rc) ctx->step = (int)sizes[2];   // outnstep: the CFL ramp and the flow-initialisation phase resume
+    return rc;
 }
 
 int phx_set_wait_limit(phx_ctx *ctx, int64_t polls)

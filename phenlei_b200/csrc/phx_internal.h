@@ -249,6 +249,9 @@ void launch_forces(const DevGrid &g, const NsConst &c, const Work<T> &w, const d
 template <class T>
 void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t, const Work<T> &w, cudaStream_t s);
 void launch_finish_step(Reduce *r, double *hist, int i, double ncell, cudaStream_t s);
+// trec slot 1 (eddy viscosity) of cells and ghosts from in[orig[i]].
+template <class T>
+void launch_import_vist(const DevGrid &g, const double *in, const Work<T> &w, cudaStream_t s);
 // Halo exchange of a partitioned grid (phx_halo.cu): pack gathers rows of
 // the cells `send` (storage indices) into buf, unpack scatters rows of buf
 // into the ghosts `recv` (storage indices); `field` is a PHX_HALO_* code and

@@ -649,6 +649,21 @@ void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t
     import_turb_kernel<T><<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, in, t, w);
 }
 
+// trec slot 1 (eddy viscosity) of cells and ghosts from a reference-order array.
+template <class T>
+__global__ void __launch_bounds__(kThreads) import_vist_kernel(DevGrid g, const double *in, Work<T> w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nTotal) return;
+    w.trec[(size_t)i * kTr + 1] = (T)in[g.orig[i]];
+}
+
+template <class T>
+void launch_import_vist(const DevGrid &g, const double *in, const Work<T> &w, cudaStream_t s)
+{
+    import_vist_kernel<T><<<(g.nTotal + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, in, w);
+}
+
 #define PHX_SA_INSTANTIATE(T)                                                                                     \
     template void launch_sa_boundary<T>(const DevGrid &, const NsConst &, const double *, const Work<T> &,        \
                                         const TurbWork<T> &, cudaStream_t);                                       \
@@ -661,7 +676,8 @@ void launch_import_turb(const DevGrid &g, const double *in, const TurbWork<T> &t
                                       cudaStream_t);                                                              \
     template void launch_turb_node_values<T>(const DevGrid &, const Work<T> &, const TurbWork<T> &, cudaStream_t); \
     template void launch_import_turb<T>(const DevGrid &, const double *, const TurbWork<T> &, const Work<T> &,    \
-                                        cudaStream_t);
+                                        cudaStream_t);                                                            \
+    template void launch_import_vist<T>(const DevGrid &, const double *, const Work<T> &, cudaStream_t);
 PHX_SA_INSTANTIATE(double)
 PHX_SA_INSTANTIATE(float)
 

@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         _lib.phx_mlp_loss_grad.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                            C.POINTER(C.c_double)]
         _lib.phx_set_wait_limit.argtypes = [C.c_void_p, C.c_int64]
+        _lib.phx_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+        _lib.phx_read_restart.argtypes = [C.c_void_p, C.c_char_p]
         _lib.phx_fault_hold_cell.argtypes = [C.c_void_p, C.c_int32]
     return _lib
 
@@ -208,6 +210,7 @@ class NSSolverUnstruct:
         return out
 
     def set(self, which, values: np.ndarray):
+        """PHX_Q, PHX_Q_TURB or PHX_VIST of cells and ghosts."""
         v = np.ascontiguousarray(values, dtype=np.float64)
         self._check(lib().phx_set_state(self.h, which, v.ctypes.data, v.size), "phx_set_state")
 
@@ -229,6 +232,16 @@ class NSSolverUnstruct:
         out = np.empty(n)
         self._check(lib().phx_get_geometry(self.h, name.encode(), out.ctypes.data, n), "phx_get_geometry")
         return out
+
+    def DumpRestart(self, path: str):
+        """The restart file (NSSolverUnstruct::DumpRestartH5 and
+        TurbSolverUnstr::DumpRestartH5 content: outnstep, q, q_turb, visturb;
+        plus the learned-source model)."""
+        self._check(lib().phx_write_restart(self.h, os.fsencode(path)), "phx_write_restart")
+
+    def ReadRestart(self, path: str):
+        """Continues from a restart file of the same grid."""
+        self._check(lib().phx_read_restart(self.h, os.fsencode(path)), "phx_read_restart")
 
     def set_wait_limit(self, polls: int):
         """Bound on every device-side dependency wait of the LU-SGS sweeps, in polls."""
