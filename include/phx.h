@@ -52,6 +52,7 @@ extern "C" {
 #define PHX_SCHEME_HLLE 4         /* "hlle" */
 #define PHX_SCHEME_AUSMDV 5       /* "ausmdv" */
 #define PHX_SCHEME_AUSMPW 6       /* "ausmpw" */
+#define PHX_SCHEME_VANLEER_ROTATE 7 /* "vanleer_Rotate" */
 
 /* Limiters (uns_limiter_name; GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300) */
 #define PHX_LIMITER_NOLIM 0       /* "nolim" */

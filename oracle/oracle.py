@@ -50,7 +50,8 @@ class _Params(C.Structure):
 # uns_limiter_name (GetLimiterID, API/Physics/src/Limiter.cpp:1279-1300)
 LIMITERS = {"nolim": 0, "vencat": 1, "1st": 2, "barth": 3}
 # uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86)
-SCHEMES = {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5, "ausmpw": 6}
+SCHEMES = {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5, "ausmpw": 6,
+           "vanleer_Rotate": 7}
 
 
 class _Work(C.Structure):

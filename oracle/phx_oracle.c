@@ -704,6 +704,77 @@ static void vanleer_flux(const double *ql, const double *qr, double gl, double g
     for (int k = 0; k < 5; ++k) f[k] = a[k] + b[k];
 }
 
+/* GetAngleOfTwoVector (API/DataStruct/include/PHMatrix.h:203-217): the dot
+ * product over both norms (DotProduct, GetNorm: sums from zero), clamped, acos. */
+static double angle_of(const double *a, const double *b)
+{
+    double dot = 0.0, na = 0.0, nb = 0.0;
+    for (int i = 0; i < 3; ++i) dot += a[i] * b[i];
+    for (int i = 0; i < 3; ++i) na += a[i] * a[i];
+    for (int i = 0; i < 3; ++i) nb += b[i] * b[i];
+    double c = dot / sqrt(na) / sqrt(nb);
+    if (c > 1.0) return 0.0;
+    if (c < -1.0) return OX_PI;
+    return acos(c);
+}
+
+/* CrossProduct (API/Math/src/Math_BasisFunction.cpp:98-104). */
+static void cross3(const double *a, const double *b, double *c)
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* Rotate_Vanleer_Scheme (Flux_Inviscid.cpp:12952-13180): Van Leer's splitting
+ * along n1, the direction of the velocity jump across the face (x when there
+ * is none), turned to the face normal's side, and along n2, normal to n1 in
+ * the plane of n1 and the face normal (y when n1 is the normal), each weighted
+ * by the cosine of its angle to the face normal. */
+static void vanleer_rotate_flux(const double *ql, const double *qr, double gl, double gr, double xsn, double ysn,
+                                double zsn, double *f)
+{
+    const double n[3] = {xsn, ysn, zsn};
+    double n1[3], n2[3];
+    const double du = qr[1] - ql[1], dv = qr[2] - ql[2], dw = qr[3] - ql[3];
+    if (du == 0 && dv == 0 && dw == 0) {
+        n1[0] = 1; n1[1] = 0; n1[2] = 0;
+    } else {
+        const double sqdv = sqrt(pow(du, 2) + pow(dv, 2) + pow(dw, 2));
+        n1[0] = du / sqdv; n1[1] = dv / sqdv; n1[2] = dw / sqdv;
+    }
+    double angle1 = angle_of(n1, n);
+    if (cos(angle1) < 0) {
+        n1[0] = -n1[0]; n1[1] = -n1[1]; n1[2] = -n1[2];
+        angle1 = angle_of(n1, n);
+    }
+    if (fabs(n1[0] - xsn) < 1.0e-8 && fabs(n1[1] - ysn) < 1.0e-8 && fabs(n1[2] - zsn) < 1.0e-8) {
+        n2[0] = 0; n2[1] = 1; n2[2] = 0;
+    } else {
+        double t[3];
+        cross3(n1, n, t);
+        cross3(t, n1, n2);
+    }
+    double nn = 0.0;
+    for (int i = 0; i < 3; ++i) nn += n2[i] * n2[i];
+    const double normn2 = sqrt(nn);
+    if (cos(angle_of(n2, n)) < 0) {
+        n2[0] = -n2[0] / normn2; n2[1] = -n2[1] / normn2; n2[2] = -n2[2] / normn2;
+    } else {
+        n2[0] = n2[0] / normn2; n2[1] = n2[1] / normn2; n2[2] = n2[2] / normn2;
+    }
+    const double angle2 = angle_of(n2, n);
+    for (int k = 0; k < 5; ++k) f[k] = 0.0;
+    for (int dir = 1; dir <= 2; ++dir) {
+        const double *d = dir == 1 ? n1 : n2;
+        double a[5], b[5];
+        vanleer_side(ql, gl, d[0], d[1], d[2], 1, a);
+        vanleer_side(qr, gr, d[0], d[1], d[2], 0, b);
+        const double c = cos(dir == 1 ? angle1 : angle2);
+        for (int k = 0; k < 5; ++k) f[k] = f[k] + c * (a[k] + b[k]);
+    }
+}
+
 /* Hlle_Scheme, Flux_Inviscid.cpp:13917-14077: the HLLE flux with signal
  * speeds from the Roe average and both sides; the conserved jump from
  * PerfectGas::Primitive2Conservative (PerfectGas.cpp:284-323). */
@@ -969,6 +1040,7 @@ void ox_inviscid_flux(const ox_grid *g, const ox_metrics *m, const ox_params *p,
         case OX_SCHEME_AUSMPW_PLUS: ausmpwp_flux(ql, qr, gama[le], gama[re], xn, yn, zn, p->ausmpw_limiter, fl); break;
         case OX_SCHEME_STEGER: steger_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_VANLEER: vanleer_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
+        case OX_SCHEME_VANLEER_ROTATE: vanleer_rotate_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_HLLE: hlle_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_AUSMDV: ausmdv_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;
         case OX_SCHEME_AUSMPW: ausmpw_flux(ql, qr, gama[le], gama[re], xn, yn, zn, fl); break;

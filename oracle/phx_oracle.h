@@ -89,7 +89,7 @@ enum { OX_LIMITER_NOLIM = 0, OX_LIMITER_VENCAT = 1, OX_LIMITER_FIRST = 2, OX_LIM
 
 /* uns_scheme_name (GetSchemeID, API/Physics/src/Flux_Inviscid.cpp:16-86) */
 enum { OX_SCHEME_ROE = 0, OX_SCHEME_AUSMPW_PLUS = 1, OX_SCHEME_STEGER = 2, OX_SCHEME_VANLEER = 3,
-       OX_SCHEME_HLLE = 4, OX_SCHEME_AUSMDV = 5, OX_SCHEME_AUSMPW = 6 };
+       OX_SCHEME_HLLE = 4, OX_SCHEME_AUSMDV = 5, OX_SCHEME_AUSMPW = 6, OX_SCHEME_VANLEER_ROTATE = 7 };
 
 /* Grid metrics: API/Geometry/src/Geo_UnstructGrid.cpp:5911-6156 (faces),
  * 6545-6819 (cells), 2206-2340 (skewness), Region.cpp:2655-2734 (avg volume),

@@ -822,7 +822,7 @@ int phx_ctx_create(const phx_grid_desc *gd, const phx_params *prm, phx_ctx **out
         return PHX_ERR_ARG;
     // gradientName 0 ggcell, 1 lsq, 2 ggnode
     if (prm->gradientName < 0 || prm->gradientName > 2 ||
-        prm->uns_scheme_name < PHX_SCHEME_ROE || prm->uns_scheme_name > PHX_SCHEME_AUSMPW ||
+        prm->uns_scheme_name < PHX_SCHEME_ROE || prm->uns_scheme_name > PHX_SCHEME_VANLEER_ROTATE ||
         prm->roeEntropyFixMethod != 3 || prm->flowInitStep < 0 ||
         prm->uns_limiter_name < PHX_LIMITER_NOLIM || prm->uns_limiter_name > PHX_LIMITER_BARTH ||
         (prm->flowInitMethod != 0 && prm->flowInitMethod != 2) ||

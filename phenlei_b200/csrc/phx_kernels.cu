@@ -381,7 +381,8 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 // Residual, pass 1 (one thread per face): MUSCL face states (GetQlQr /
 // ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193), the wall /
 // symmetry face fix (BoundaryQlQrFix, :13725-13951), the inviscid flux (Roe,
-// or with kRoe = false the scheme uns_scheme_name selects) times the face area
+// with kFlux = 1 the other scheme uns_scheme_name selects, with kFlux = 2 the
+// rotated Van Leer scheme in an instantiation of its own) times the face area
 // (InviscidFluxWrap, :14466-14488), the face term of the inviscid
 // spectral radius (SpectrumRadiusInviscid, :5749-5850), and the dq-independent
 // LU-SGS factors of both face uses (RoeAveragedVariables + GetRad +
@@ -587,7 +588,7 @@ __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c,
 // Three blocks per SM on the mixed path (at most 85 registers): the face pass
 // is latency-bound on its arithmetic, and 16M cells take 5.3 ms against 6.2 ms
 // at the two blocks its natural 101 registers allow.
-template <class T, bool kVisc, bool kRoe>
+template <class T, bool kVisc, int kFlux>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_kernel(DevGrid g, NsConst c, Work<T> w)
 {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,7 +603,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     T limL = qL[7], limR = qR[7];
     if (c.reconMethod == 1) { const T m = tmin(limL, limR); limL = limR = m; }
     T ql[5], qr[5];
-    if (!kRoe && c.firstOrder) {
+    if (kFlux != 0 && c.firstOrder) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) { ql[k] = qL[k]; qr[k] = qR[k]; }
     } else {
@@ -626,7 +627,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     }
     const T gm = (T)c.gama;
     T fl[8];
-    if (kRoe) roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
+    if (kFlux == 0) roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
+    else if (kFlux == 2) vanleer_rotate_flux_fp64<T>(ql, qr, gm, gm, xn, yn, zn, fl);
     else other_flux<T>(c.scheme, ql, qr, gm, gm, xn, yn, zn, (T)c.ausmpwLim, fl);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fl[k] *= area;
@@ -754,14 +756,16 @@ template <class T>
 void launch_residual(const DevGrid &g, const NsConst &c, const Work<T> &w, Reduce *red, double cfl, cudaStream_t s)
 {
     const int fb = (g.nFace + kThreads - 1) / kThreads, cb = (g.nCell + kThreads - 1) / kThreads;
-    const bool roe = c.scheme == PHX_SCHEME_ROE;
+    const int kind = c.scheme == PHX_SCHEME_ROE ? 0 : c.scheme == PHX_SCHEME_VANLEER_ROTATE ? 2 : 1;
     if (c.viscous) {
-        if (roe) face_flux_kernel<T, true, true><<<fb, kThreads, 0, s>>>(g, c, w);
-        else face_flux_kernel<T, true, false><<<fb, kThreads, 0, s>>>(g, c, w);
+        if (kind == 0) face_flux_kernel<T, true, 0><<<fb, kThreads, 0, s>>>(g, c, w);
+        else if (kind == 2) face_flux_kernel<T, true, 2><<<fb, kThreads, 0, s>>>(g, c, w);
+        else face_flux_kernel<T, true, 1><<<fb, kThreads, 0, s>>>(g, c, w);
         cell_residual_kernel<T, true><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
     } else {
-        if (roe) face_flux_kernel<T, false, true><<<fb, kThreads, 0, s>>>(g, c, w);
-        else face_flux_kernel<T, false, false><<<fb, kThreads, 0, s>>>(g, c, w);
+        if (kind == 0) face_flux_kernel<T, false, 0><<<fb, kThreads, 0, s>>>(g, c, w);
+        else if (kind == 2) face_flux_kernel<T, false, 2><<<fb, kThreads, 0, s>>>(g, c, w);
+        else face_flux_kernel<T, false, 1><<<fb, kThreads, 0, s>>>(g, c, w);
         cell_residual_kernel<T, false><<<cb, kThreads, 0, s>>>(g, c, w, red, cfl);
     }
 }

@@ -142,6 +142,93 @@ __device__ __forceinline__ void vanleer_side(const T *q, T g, T xsn, T ysn, T zs
     }
 }
 
+// GetAngleOfTwoVector (API/DataStruct/include/PHMatrix.h:203-217): the dot
+// product over both norms (sums from zero), clamped, acos.
+template <class T>
+__device__ __forceinline__ T angle_of(const T *a, const T *b)
+{
+    T dot = T(0), na = T(0), nb = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dot += a[i] * b[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) na += a[i] * a[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nb += b[i] * b[i];
+    const T c = dot / sqrt(na) / sqrt(nb);
+    if (c > T(1)) return T(0);
+    if (c < T(-1)) return T(3.141592653589793);
+    return acos(c);
+}
+
+// Rotate_Vanleer_Scheme (Flux_Inviscid.cpp:12952-13180): Van Leer's splitting
+// along n1, the direction of the velocity jump across the face (x when there
+// is none), turned to the face normal's side, and along n2, normal to n1 in
+// the plane of n1 and the face normal (y when n1 is the normal), each weighted
+// by the cosine of its angle to the face normal (CrossProduct,
+// API/Math/src/Math_BasisFunction.cpp:98-104).
+template <class T>
+__device__ __forceinline__ void vanleer_rotate_flux(const T *ql, const T *qr, T gl, T gr, T xsn, T ysn, T zsn,
+                                                    T *f)
+{
+    const T n[3] = {xsn, ysn, zsn};
+    T n1[3], n2[3];
+    const T du = qr[1] - ql[1], dv = qr[2] - ql[2], dw = qr[3] - ql[3];
+    if (du == T(0) && dv == T(0) && dw == T(0)) {
+        n1[0] = T(1); n1[1] = T(0); n1[2] = T(0);
+    } else {
+        const T sqdv = sqrt(du * du + dv * dv + dw * dw);
+        n1[0] = du / sqdv; n1[1] = dv / sqdv; n1[2] = dw / sqdv;
+    }
+    T angle1 = angle_of<T>(n1, n);
+    if (cos(angle1) < T(0)) {
+        n1[0] = -n1[0]; n1[1] = -n1[1]; n1[2] = -n1[2];
+        angle1 = angle_of<T>(n1, n);
+    }
+    if (fabs(n1[0] - xsn) < T(1.0e-8) && fabs(n1[1] - ysn) < T(1.0e-8) && fabs(n1[2] - zsn) < T(1.0e-8)) {
+        n2[0] = T(0); n2[1] = T(1); n2[2] = T(0);
+    } else {
+        const T t[3] = {n1[1] * n[2] - n1[2] * n[1], n1[2] * n[0] - n1[0] * n[2], n1[0] * n[1] - n1[1] * n[0]};
+        n2[0] = t[1] * n1[2] - t[2] * n1[1];
+        n2[1] = t[2] * n1[0] - t[0] * n1[2];
+        n2[2] = t[0] * n1[1] - t[1] * n1[0];
+    }
+    T nn = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nn += n2[i] * n2[i];
+    const T normn2 = sqrt(nn);
+    const T sgn = cos(angle_of<T>(n2, n)) < T(0) ? T(-1) : T(1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n2[i] = (sgn * n2[i]) / normn2;
+    const T angle2 = angle_of<T>(n2, n);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) f[k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+        const T *d = dir == 0 ? n1 : n2;
+        T a[5], b[5];
+        vanleer_side<T, true>(ql, gl, d[0], d[1], d[2], a);
+        vanleer_side<T, false>(qr, gr, d[0], d[1], d[2], b);
+        const T c = cos(dir == 0 ? angle1 : angle2);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) f[k] = f[k] + c * (a[k] + b[k]);
+    }
+}
+
+// The rotated Van Leer flux formed in FP64 on both paths: the rotation
+// degenerates in single precision (its 1e-8 test of n1 against the normal
+// lies below FP32 resolution, and a zero cross product then divides 0 by 0).
+template <class T>
+__device__ __forceinline__ void vanleer_rotate_flux_fp64(const T *ql, const T *qr, T gl, T gr, T xsn, T ysn, T zsn,
+                                                         T *f)
+{
+    double dl[5], dr[5], fd[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { dl[k] = (double)ql[k]; dr[k] = (double)qr[k]; }
+    vanleer_rotate_flux<double>(dl, dr, (double)gl, (double)gr, (double)xsn, (double)ysn, (double)zsn, fd);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) f[k] = (T)fd[k];
+}
+
 // Hlle_Scheme (Flux_Inviscid.cpp:13917-14077): HLLE with signal speeds from
 // the Roe average and both sides; conserved jump as
 // PerfectGas::Primitive2Conservative (PerfectGas.cpp:284-323) forms it.

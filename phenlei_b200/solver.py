@@ -57,7 +57,8 @@ class Params(C.Structure):
 _STRING_KEYS = {
     "gradientName": {"ggcell": 0, "lsq": 1, "ggnode": 2},
     "uns_limiter_name": {"nolim": 0, "vencat": 1, "1st": 2, "barth": 3},
-    "uns_scheme_name": {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5, "ausmpw": 6},
+    "uns_scheme_name": {"roe": 0, "ausmpw+": 1, "steger": 2, "vanleer": 3, "hlle": 4, "ausmdv": 5, "ausmpw": 6,
+                        "vanleer_Rotate": 7},
     "precision": {"fp64": PHX_FP64, "mixed": PHX_MIXED},
     "sa_source": {"exact": 0, "mlp": 1, "mlp_fallback": 2},
 }

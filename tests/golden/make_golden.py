@@ -221,7 +221,7 @@ if __name__ == "__main__":
     # 3 iterations; and a supersonic free stream (M = 1.6) through jittered tetrahedra, perturbed,
     # 2 iterations, so the supersonic branches of each splitting run.
     for scheme, tag in (("steger", "steger"), ("vanleer", "vanleer"), ("hlle", "hlle"), ("ausmdv", "ausmdv"),
-                        ("ausmpw+", "ausmpwp"), ("ausmpw", "ausmpw")):
+                        ("ausmpw+", "ausmpwp"), ("ausmpw", "ausmpw"), ("vanleer_Rotate", "vanleerrot")):
         fixture(f"euler_bump_16x8x2_{tag}_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
                 dict(EULER_BUMP, uns_scheme_name=scheme), 3, perturb_seed=7)
         fixture(f"euler_tetcube_4_{tag}_m16_step2", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},

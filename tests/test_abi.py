@@ -66,7 +66,7 @@ def _create_error(**kw):
 
 @pytest.mark.parametrize("kw", [dict(flowInitMethod=1), dict(flowInitMethod=3), dict(flowInitStep=-1),
                                 dict(roeEntropyFixMethod=2), dict(nLUSGSSweeps=2), dict(ivencat=6),
-                                dict(gradientName=3), dict(uns_scheme_name=7), dict(uns_limiter_name=4),
+                                dict(gradientName=3), dict(uns_scheme_name=8), dict(uns_limiter_name=4),
                                 dict(viscousType=2), dict(precision=7)])
 def test_unsupported_settings_are_rejected(kw):
     """Settings outside the path (other entropy fixes, several LU-SGS sweeps,
@@ -77,7 +77,7 @@ def test_unsupported_settings_are_rejected(kw):
     assert _create_error(**kw) == "PHX_ERR_ARG"
 
 
-@pytest.mark.parametrize("kw", [dict(uns_scheme_name=s) for s in ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+", "ausmpw")]
+@pytest.mark.parametrize("kw", [dict(uns_scheme_name=s) for s in ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+", "ausmpw", "vanleer_Rotate")]
                          + [dict(uns_limiter_name=n) for n in ("nolim", "1st", "barth")]
                          + [dict(flowInitStep=100), dict(flowInitMethod=2), dict(gradientName="ggnode")])
 def test_supported_settings_pass_the_checks(kw):

@@ -9,7 +9,7 @@ from tests.conftest import rel_err
 GEOM = ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc", "xcc", "ycc", "zcc", "vol")
 
 
-SCHEME_TAGS = ("steger", "vanleer", "hlle", "ausmdv", "ausmpwp", "ausmpw")
+SCHEME_TAGS = ("steger", "vanleer", "hlle", "ausmdv", "ausmpwp", "ausmpw", "vanleerrot")
 SCHEME_CASES = [f"euler_bump_16x8x2_{t}_step3" for t in SCHEME_TAGS] + \
     [f"euler_tetcube_4_{t}_m16_step2" for t in SCHEME_TAGS]
 

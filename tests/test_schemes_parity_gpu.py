@@ -21,9 +21,9 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 MIXED_TOL = 1e-5
-SCHEMES = ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+", "ausmpw")
+SCHEMES = ("steger", "vanleer", "hlle", "ausmdv", "ausmpw+", "ausmpw", "vanleer_Rotate")
 TAG = {"steger": "steger", "vanleer": "vanleer", "hlle": "hlle", "ausmdv": "ausmdv", "ausmpw+": "ausmpwp",
-       "ausmpw": "ausmpw"}
+       "ausmpw": "ausmpw", "vanleer_Rotate": "vanleerrot"}
 
 
 @pytest.mark.parametrize("name", [f"euler_bump_16x8x2_{TAG[s]}_step3" for s in SCHEMES]

@@ -248,3 +248,24 @@ def test_fp64_zones_match_reference_golden(golden, name):
     if sa:
         assert rel_err(zs.gather(S.PHX_Q_TURB), d["q_turb"]) <= 1e-10
         assert rel_err(zs.gather(S.PHX_VIST), d["vist"]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["zones2_euler_bump_16x8x2_step10", "zones2_sa_bump_16x8x2_step10"])
+def test_mixed_zones_follow_reference_golden(golden, name):
+    """The mixed-precision zones against the reference's own multi-zone run:
+    the residual history and the state over 10 iterations within 1e-4."""
+    from phenlei_b200.zones import ZoneSet
+
+    d = golden(name)
+    m = d["mesh_obj"]
+    params = d["params_dict"]
+    sa = params.get("viscousType", 0) == 3
+    zs = ZoneSet(m, params, int(d["nparts"]), owner=d["owner"], wall_dist=d["walldist"] if sa else None,
+                 precision="mixed")
+    st = d["state_in"]
+    zs.set_state(st[:5], st[5] if sa else None)
+    hist = zs.iterate(int(d["nsteps"]))
+    assert rel_err(hist, d["res_hist"]) <= 1e-4
+    assert rel_err(zs.gather(S.PHX_Q), d["q"]) <= 1e-4
+    if sa:
+        assert rel_err(zs.gather(S.PHX_Q_TURB), d["q_turb"]) <= 1e-4
