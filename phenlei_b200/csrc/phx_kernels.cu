@@ -381,8 +381,8 @@ void launch_gradient_limiter(const DevGrid &g, const NsConst &c, const Work<T> &
 // Residual, pass 1 (one thread per face): MUSCL face states (GetQlQr /
 // ReConstructFaceValue, NSSolverUnstruct.cpp:5507, :13991-14193), the wall /
 // symmetry face fix (BoundaryQlQrFix, :13725-13951), the inviscid flux (Roe,
-// with kFlux = 1 the other scheme uns_scheme_name selects, with kFlux = 2 the
-// rotated Van Leer scheme in an instantiation of its own) times the face area
+// with kScheme = 1 the other scheme uns_scheme_name selects, with kScheme = 2
+// the rotated Van Leer scheme in an instantiation of its own) times the face area
 // (InviscidFluxWrap, :14466-14488), the face term of the inviscid
 // spectral radius (SpectrumRadiusInviscid, :5749-5850), and the dq-independent
 // LU-SGS factors of both face uses (RoeAveragedVariables + GetRad +
@@ -588,7 +588,7 @@ __device__ __forceinline__ void viscous_face(const DevGrid &g, const NsConst &c,
 // Three blocks per SM on the mixed path (at most 85 registers): the face pass
 // is latency-bound on its arithmetic, and 16M cells take 5.3 ms against 6.2 ms
 // at the two blocks its natural 101 registers allow.
-template <class T, bool kVisc, int kFlux>
+template <class T, bool kVisc, int kScheme>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_kernel(DevGrid g, NsConst c, Work<T> w)
 {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     T limL = qL[7], limR = qR[7];
     if (c.reconMethod == 1) { const T m = tmin(limL, limR); limL = limR = m; }
     T ql[5], qr[5];
-    if (kFlux != 0 && c.firstOrder) {
+    if (kScheme != 0 && c.firstOrder) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) { ql[k] = qL[k]; qr[k] = qR[k]; }
     } else {
@@ -627,8 +627,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) face_flux_ke
     }
     const T gm = (T)c.gama;
     T fl[8];
-    if (kFlux == 0) roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
-    else if (kFlux == 2) vanleer_rotate_flux_fp64<T>(ql, qr, gm, gm, xn, yn, zn, fl);
+    if (kScheme == 0) roe_flux<T>(ql, qr, gm, gm, xn, yn, zn, (T)c.acoustic, (T)c.convective, fl);
+    else if (kScheme == 2) vanleer_rotate_flux_fp64<T>(ql, qr, gm, gm, xn, yn, zn, fl);
     else other_flux<T>(c.scheme, ql, qr, gm, gm, xn, yn, zn, (T)c.ausmpwLim, fl);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fl[k] *= area;
