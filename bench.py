@@ -673,19 +673,47 @@ def cpu_sample(wl_name):
     return m, "the workload's own mesh"
 
 
+def host_threads() -> int:
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_baseline(args, wl_name, budget_s=25.0):
-    """The reference's own CPU solver (oracle/_ref/ref_harness, built from its
-    sources: single zone, one core, its Controller relaxations) on a bounded
-    sample of the workload; the oracle port (single-threaded C restatement,
-    bit-exact with the reference) when the reference build is absent.  The
+    """The reference's own CPU solver on a bounded sample of the workload, with
+    every host thread it can use: the reference parallelises across zones
+    (its OpenMP loops over zones, e.g. Controller::TimeStep,
+    CFD/Solver/src/Controller.cpp:684-704), so the sample is split into one
+    slab zone per thread and run by oracle/_ref/ref_harness_omp (the reference
+    built from its sources with USE_OMP).  Without that build, one zone on one
+    core (oracle/_ref/ref_harness); without either, the oracle port
+    (single-threaded C restatement, bit-exact with the reference).  The
     throughput is taken over the iteration loop alone."""
     from oracle import refrun
     from phenlei_b200 import mesh as M
+    from phenlei_b200 import partition as P
 
     wl = workloads()[wl_name]
     m, what = cpu_sample(wl_name)
     wd = M.wall_distance(m) if wl.get("wall_dist") else None
     params = dict(wl["params"])
+    threads = host_threads()
+    if refrun.available() and os.path.exists(refrun.HARNESS_OMP) and threads > 1:
+        parts = P.split(m, P.slab_owner(m, threads))
+        # about 0.35 Mcell-iterations/s on one thread, each further thread adding about 0.15 of that
+        # (the reference threads only some of its loops over zones): as many iterations as fit the
+        # budget, at least 2
+        n = int(max(2, min(args.steps, budget_s * 0.35e6 * (1 + 0.15 * (threads - 1)) / m.n_cell)))
+        r = refrun.run_reference_zones(parts, params, n, threads=threads,
+                                       wall_dists=None if wd is None else [wd[p.cells] for p in parts])
+        sec = r["loop_s"]
+        return {"value": round(m.n_cell * n / sec / 1e6, 4), "unit": "Mcell-iters/s", "cores": threads,
+                "kind": "reference", "ms_per_step": round(sec / n * 1e3, 2), "iterations": n, "cells": m.n_cell,
+                "sample": f"{what}, split into {threads} slab zones; {n} iterations in {sec:.1f} s by the "
+                          f"reference solver built from its own sources with its OpenMP zone loops "
+                          f"(oracle/_ref/ref_harness_omp), one zone per thread on {threads} host threads"}
     if refrun.available():
         # about 0.35 Mcell-iterations/s: as many iterations as fit the budget, at least 2
         n = int(max(2, min(args.steps, budget_s * 0.35e6 / m.n_cell)))
@@ -738,7 +766,8 @@ def main():
                 "n_gpus": args.gpus, "steps": cb["iterations"], "warmup": 0, "ms_per_step": cb["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generated mesh, free-stream start)",
-                "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "1 CPU core",
+                "config": {"workload": args.workload, "desc": wl["desc"],
+                           "parallelism": f"{cb['cores']} CPU thread(s), one zone each",
                            "same_config": cb["sample"].startswith("the workload's own mesh"),
                            "sample": cb["sample"]},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-iters/s",

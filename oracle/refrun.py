@@ -18,6 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+# the same harness over the reference built with its OpenMP loops over zones
+# (make -C oracle/refbuild OMP=1 ...): one zone per thread
+HARNESS_OMP = os.path.join(HERE, "_ref", "ref_harness_omp")
 # the reference's default parameter file, staged beside the harness by the build
 DEFAULT_PARA = os.path.join(HERE, "_ref", "cfd_para.hypara")
 
@@ -132,12 +135,17 @@ def interface_arrays(parts):
     return out
 
 
-def run_reference_zones(parts, params: dict, nsteps: int, dumps=(), states=None, workdir=None):
+def run_reference_zones(parts, params: dict, nsteps: int, dumps=(), states=None, workdir=None, threads=0,
+                        wall_dists=None):
     """`nsteps` outer iterations of the reference solver on the zones `parts`
     (phenlei_b200.partition.split), all in one process as the reference runs
     several zones on one rank.  dumps: (name, rows, cols) per zone, where
     cols may be a callable of the part.  states: per zone the input field as
-    for run_reference.  Returns {"res_hist": global monitor, "zones": [dict per zone]}."""
+    for run_reference.  threads > 0 runs the OpenMP build of the reference with
+    that many threads (its loops over zones run in parallel).  wall_dists: per
+    zone wall distances that replace the reference's search.  Returns
+    {"res_hist": global monitor, "zones": [dict per zone], "loop_s": the
+    iteration loop's wall time}."""
     from phenlei_b200.mesh import write_mesh
 
     if not available():
@@ -174,7 +182,12 @@ def run_reference_zones(parts, params: dict, nsteps: int, dumps=(), states=None,
     for (n, r, c) in dumps:
         spec.append((n, r, c))
     # the dump sizes differ per zone: dump the largest and cut per zone
-    args = [HARNESS, ",".join(mpaths), tmp, os.path.join(tmp, "out"), str(nsteps), ",".join(spaths) or "-"]
+    harness = HARNESS
+    if threads > 0:
+        if not os.path.exists(HARNESS_OMP):
+            raise RuntimeError("oracle/_ref/ref_harness_omp is not built (make -C oracle/refbuild OMP=1 ...)")
+        harness = HARNESS_OMP
+    args = [harness, ",".join(mpaths), tmp, os.path.join(tmp, "out"), str(nsteps), ",".join(spaths) or "-"]
     sizes = {}
     for (n, r, c) in spec:
         cmax = max(c(part) for part in parts) if callable(c) else c
@@ -182,10 +195,20 @@ def run_reference_zones(parts, params: dict, nsteps: int, dumps=(), states=None,
         args.append(f"{n}:{r}:{cmax}")
     env = dict(os.environ)
     env.pop("PHX_REF_WALLDIST", None)
+    if threads > 0:
+        env["OMP_NUM_THREADS"] = str(threads)
+    if wall_dists is not None:
+        wpaths = []
+        for part in parts:
+            wp = os.path.join(tmp, "grid", f"walldist{part.rank}.bin")
+            np.ascontiguousarray(wall_dists[part.rank], dtype="<f8").tofile(wp)
+            wpaths.append(wp)
+        env["PHX_REF_WALLDIST"] = ",".join(wpaths)
     proc = subprocess.run(args, capture_output=True, text=True, env=env)
     if proc.returncode != 0:
         raise RuntimeError(f"reference harness failed ({proc.returncode}):\n{proc.stdout[-4000:]}\n{proc.stderr[-4000:]}")
     res = {"res_hist": np.fromfile(os.path.join(tmp, "out", "res_hist.bin"), dtype="<f8"), "zones": [],
+           "loop_s": float(np.fromfile(os.path.join(tmp, "out", "iter_seconds.bin"), dtype="<f8")[0]),
            "_log": proc.stdout}
     for part in parts:
         zdir = os.path.join(tmp, "out", f"zone{part.rank}")
