@@ -55,14 +55,14 @@ def workloads():
     from phenlei_b200 import mesh as M
 
     return {
-        # Config-5 mesh size and flow Mach number, inviscid physics.
+        # The 16M-cell transonic bump's mesh size and Mach number with inviscid physics.
         "transonic_bump_euler_16M": dict(
             mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001),
             channel=dict(nx=1024, ny=92, nz=128, thickness=0.08, length=3.0, wall_spacing=0.001),
             params=dict(cases.EULER_BUMP, refMachNumber=0.8, CFLEnd=20.0),
             desc="3-D transonic channel bump 8% thick, 1024x92x128 hex (12.06M cells), M=0.8, Roe+Venkat, "
                  "GG-cell, LU-SGS CFL 20, inviscid"),
-        # Config 5: mixed hex / prism bump, 1024x92x128 with the 30 wall-adjacent
+        # Mixed hex / prism bump, 1024x92x128 with the 30 wall-adjacent
         # layers as prisms (15,990,784 cells), M=0.8, Re=1e7, SA, Roe + Venkat, CFL 20.
         "transonic_bump_sa_16M": dict(
             mesh=lambda: M.channel_bump(1024, 92, 128, thickness=0.08, length=3.0, wall_spacing=0.001,
@@ -70,7 +70,7 @@ def workloads():
             channel=dict(nx=1024, ny=92, nz=128, thickness=0.08, length=3.0, wall_spacing=0.001, prism_layers=30),
             params=dict(cases.SA_BUMP),
             wall_dist=True,
-            desc="config 5: 3-D transonic channel bump 8% thick, 1024x92x128 with 30 prism layers at the walls "
+            desc="3-D transonic channel bump 8% thick, 1024x92x128 with 30 prism layers at the walls "
                  "(15.99M hex+prism cells), M=0.8, Re=1e7, Spalart-Allmaras, Roe+Venkat, GG-cell, LU-SGS CFL 20"),
         "sa_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 92, 32, thickness=0.08, wall_spacing=0.001, prism_layers=30),
@@ -81,32 +81,32 @@ def workloads():
         "euler_bump_8k": dict(
             mesh=lambda: M.channel_bump(64, 32, 4),
             params=dict(cases.EULER_BUMP),
-            desc="config 1: Euler channel bump 64x32x4 hex (8,192 cells), M=0.5"),
+            desc="Euler channel bump 64x32x4 hex (8,192 cells), M=0.5"),
         "euler_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 128, 32),
             channel=dict(nx=256, ny=128, nz=32),
             params=dict(cases.EULER_BUMP),
             desc="Euler channel bump 256x128x32 hex (1.05M cells), M=0.5"),
-        # Config 2: 100^3 hexes x 6 jittered tetrahedra, laminar, least squares.
+        # 100^3 hexes x 6 jittered tetrahedra, laminar, least squares.
         "laminar_cube_6M": dict(
             mesh=lambda: M.tet_cube(100, jitter=0.15, seed=1),
             params=dict(cases.LAMINAR, gradientName="lsq"),
-            desc="config 2: laminar cube, 100^3 hexes x 6 jittered tets (6.0M cells), M=0.3, Re=1e4, LSQ, "
+            desc="laminar cube, 100^3 hexes x 6 jittered tets (6.0M cells), M=0.3, Re=1e4, LSQ, "
                  "Roe+Venkat, LU-SGS"),
-        # Config 3: SA flat plate 512x192x32 (3.1M hexes), first cell y+ about 1, M 0.2, Re 5e6, AUSMPW+, CFL 50,
-        # 5,000 iterations.  Config 4 trains the learned source on its states (2M samples, 20 epochs) and also
-        # runs the unseen flow M 0.3, Re 3e6.
+        # SA flat plate 512x192x32 (3.1M hexes), first cell y+ about 1, M 0.2, Re 5e6, AUSMPW+, CFL 50,
+        # 5,000 iterations.  Its converged run trains the learned source on its states (2M samples, 20 epochs)
+        # and then also runs the unseen flow M 0.3, Re 3e6.
         "sa_plate_3M": dict(
             mesh=lambda: M.flat_plate(512, 192, 32),
             params=dict(cases.SA_PLATE),
             wall_dist=True, iterations=5000, train_epochs=20, unseen=dict(cases.SA_PLATE_UNSEEN),
-            desc="config 3/4: SA flat plate 512x192x32 hex (3.15M cells), lead-in 0.33, plate 2, M=0.2, Re=5e6, "
+            desc="SA flat plate 512x192x32 hex (3.15M cells), lead-in 0.33, plate 2, M=0.2, Re=5e6, "
                  "T=300 K, AUSMPW+, Venkat, GG-cell, LU-SGS CFL 50; unseen flow M=0.3, Re=3e6"),
         "sa_plate_200k": dict(
             mesh=lambda: M.flat_plate(128, 96, 16, first_spacing=1e-5),
             params=dict(cases.SA_PLATE),
             wall_dist=True, iterations=5000, train_epochs=20, unseen=dict(cases.SA_PLATE_UNSEEN),
-            desc="SA flat plate 128x96x16 hex (197k cells), config-3 flow"),
+            desc="SA flat plate 128x96x16 hex (197k cells), M=0.2, Re=5e6, AUSMPW+, CFL 50"),
         "laminar_bump_1M": dict(
             mesh=lambda: M.channel_bump(256, 128, 32),
             params=dict(cases.LAMINAR),
@@ -600,7 +600,7 @@ def main_zones(args, rank, world, wl):
 
 
 def converge(args, m, wd):
-    """The configuration's full iteration count for the three arms on one GPU
+    """The workload's full iteration count for the three arms on one GPU
     (FP64 exact source, mixed exact source, mixed learned source), from the
     free stream.  The learned source is trained on FP64 states captured along
     the FP64 run (early, middle and final), so it sees the flow it meets.
@@ -707,7 +707,7 @@ def cpu_sample(wl_name):
 
     if wl_name == "transonic_bump_sa_16M":
         return (M.channel_bump(256, 92, 32, thickness=0.08, length=3.0, wall_spacing=0.001, prism_layers=30),
-                "256x92x32 channel bump with 30 prism layers (999,424 cells): config 5's case kind and layer count")
+                "256x92x32 channel bump with 30 prism layers (999,424 cells): the 16M bump's case kind and layer count")
     if wl_name == "transonic_bump_euler_16M":
         return (M.channel_bump(256, 92, 32, thickness=0.08, length=3.0, wall_spacing=0.001),
                 "256x92x32 hex channel bump (753,664 cells), the same case kind")
@@ -794,9 +794,9 @@ def main():
     ap.add_argument("--mlp-blob", default=None, help="use this learned-source model (.npy) instead of training one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--converge", action="store_true",
-                    help="run the configuration's full iteration count for every arm and report converged CL/CD")
+                    help="run the workload's full iteration count for every arm and report converged CL/CD")
     ap.add_argument("--iterations", type=int, default=0,
-                    help="iterations of a --converge run (default: the configuration's own count)")
+                    help="iterations of a --converge run (default: the workload's own count)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -850,7 +850,7 @@ def main():
             blob = r64["mlp"].pop("blob")
             if args.save_mlp and rank == 0:
                 np.save(args.save_mlp, blob)
-    # the mixed path with the exact SA source: the third configuration the
+    # the mixed path with the exact SA source: the third arm the
     # headline is read against (what the learned source adds or costs)
     rx = None
     if r64 is not None and blob is not None:

@@ -1,16 +1,16 @@
 """The benchmark cases: hypara keys and initial states.
 
 Synthetic, seeded stand-ins with the shapes, sizes and flow parameters of the
-five configurations (no external grids or data are used; the meshes come from
+benchmark cases (no external grids or data are used; the meshes come from
 phenlei_b200.mesh):
 
-1. ``EULER_BUMP``  inviscid 3-D channel, 10% circular-arc bump, 64x32x4 hexes
-2. ``LAMINAR``     laminar NS (with gradientName "lsq" on the 100^3 x 6 jittered
-                   tetrahedral cube), free stream plus seeded sinusoids
-3. ``SA_PLATE``    Spalart-Allmaras flat plate, 512x192x32 hexes, M 0.2, Re 5e6
-4. ``SA_PLATE`` with sa_source "mlp_fallback" (the learned source), and
-   ``SA_PLATE_UNSEEN`` (M 0.3, Re 3e6) for its generalisation
-5. ``SA_BUMP``     transonic channel bump, 16M hex / prism cells, M 0.8, Re 1e7
+* ``EULER_BUMP``  inviscid 3-D channel, 10% circular-arc bump, 64x32x4 hexes
+* ``LAMINAR``     laminar NS (with gradientName "lsq" on the 100^3 x 6 jittered
+                  tetrahedral cube), free stream plus seeded sinusoids
+* ``SA_PLATE``    Spalart-Allmaras flat plate, 512x192x32 hexes, M 0.2, Re 5e6;
+                  with sa_source "mlp_fallback" it runs the learned source, and
+                  ``SA_PLATE_UNSEEN`` (M 0.3, Re 3e6) tests its generalisation
+* ``SA_BUMP``     transonic channel bump, 16M hex / prism cells, M 0.8, Re 1e7
 """
 from __future__ import annotations
 
@@ -25,23 +25,23 @@ EULER_BUMP = {"viscousType": 0, "uns_scheme_name": "roe", "uns_limiter_name": "v
               "tscheme": 4, "nLUSGSSweeps": 1, "CFLStart": 0.01, "CFLEnd": 10.0, "CFLVaryStep": 500,
               "refMachNumber": 0.5, "attackd": 0.0, "refGama": 1.4, "flowInitStep": 0}
 
-# Laminar NS (config 2 keys): Sutherland viscosity, Re 1e4 per unit length,
+# Laminar NS (the laminar cube's keys): Sutherland viscosity, Re 1e4 per unit length,
 # adiabatic no-slip walls.
 LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, refDimensionalTemperature=288.15,
                prl=0.72, wallTemperature=-1.0)
 
-# Config 5 flow: transonic bump, Spalart-Allmaras, Re 1e7 per unit length.
+# Transonic bump flow, Spalart-Allmaras, Re 1e7 per unit length.
 SA_BUMP = dict(EULER_BUMP, viscousType=3, refMachNumber=0.8, refReNumber=1.0e7, refDimensionalTemperature=288.15,
                prl=0.72, prt=0.9, wallTemperature=-1.0, muoo=3.0, CFLEnd=20.0)
 
 
-# Config 3: SA flat plate, M 0.2, Re 5e6 per unit length, T_inf 300 K, adiabatic
+# SA flat plate, M 0.2, Re 5e6 per unit length, T_inf 300 K, adiabatic
 # no-slip plate, nu~_inf = 3 nu, CFL 50.  AUSM+ is not in the reference's
 # unstructured flux dispatcher (Flux_Inviscid.cpp:88-134); AUSMPW+ stands in.
 SA_PLATE = dict(EULER_BUMP, viscousType=3, refMachNumber=0.2, refReNumber=5.0e6, refDimensionalTemperature=300.0,
                 prl=0.72, prt=0.9, wallTemperature=-1.0, muoo=3.0, uns_scheme_name="ausmpw+", CFLEnd=50.0)
 
-# Config 4's unseen flow: the same plate at M 0.3, Re 3e6.
+# The learned source's unseen flow: the same plate at M 0.3, Re 3e6.
 SA_PLATE_UNSEEN = dict(SA_PLATE, refMachNumber=0.3, refReNumber=3.0e6)
 
 

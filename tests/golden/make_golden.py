@@ -37,7 +37,7 @@ LAMINAR = dict(EULER_BUMP, viscousType=1, refMachNumber=0.3, refReNumber=1.0e4, 
 # Spalart-Allmaras (NSMB formation), adiabatic no-slip walls, Re 1e5.
 SA = dict(LAMINAR, viscousType=3, viscousName="1eq-sa", refReNumber=1.0e5, muoo=3.0)
 
-# Config 3: SA flat plate, M 0.2, Re 5e6 per unit length, T 300 K, AUSMPW+, CFL 50.
+# SA flat plate, M 0.2, Re 5e6 per unit length, T 300 K, AUSMPW+, CFL 50.
 SA_PLATE = dict(SA, refMachNumber=0.2, refReNumber=5.0e6, refDimensionalTemperature=300.0, prt=0.9,
                 uns_scheme_name="ausmpw+", CFLEnd=50.0)
 
@@ -186,7 +186,7 @@ if __name__ == "__main__":
             dict(LAMINAR, gradientName="lsq"), 1, perturb_seed=7)
     # Laminar bump, GG-cell gradient, 20 iterations from the free stream.
     fixture("laminar_bump_16x8x2_step20", "channel_bump", {"nx": 16, "ny": 8, "nz": 2}, LAMINAR, 20)
-    # Laminar jittered tetrahedra (config-2 element type), LSQ, perturbed, 3 iterations.
+    # Laminar jittered tetrahedra (the laminar cube's element type), LSQ, perturbed, 3 iterations.
     fixture("laminar_tetcube_4_lsq_step3", "tet_cube", {"n": 4, "jitter": 0.15, "seed": 3},
             dict(LAMINAR, gradientName="lsq"), 3, perturb_seed=11)
     # SA bump, perturbed flow and nu~ (negative cells included), one iteration.
@@ -247,7 +247,7 @@ if __name__ == "__main__":
             dict(EULER_BUMP, uns_limiter_name="barth", refMachNumber=0.3), 2, perturb_seed=11)
     fixture("euler_bump_16x8x2_1st_step3", "channel_bump", {"nx": 16, "ny": 8, "nz": 2},
             dict(EULER_BUMP, uns_limiter_name="1st"), 3, perturb_seed=7)
-    # Config-3 flow on a small flat plate (no-slip plate after a symmetry lead-in): SA, M 0.2, Re 5e6,
+    # The SA flat plate flow on a small plate (no-slip plate after a symmetry lead-in): SA, M 0.2, Re 5e6,
     # T 300 K, AUSMPW+ (the unstructured dispatcher has no AUSM+), CFL 50; perturbed flow and nu~,
     # 2 iterations; and 20 iterations from the free stream.
     fixture("sa_plate_16x8x2_ausmpwp_step2", "flat_plate", {"nx": 16, "ny": 8, "nz": 2, "first_spacing": 1e-4},

@@ -77,7 +77,7 @@ def test_laminar_single_iteration_vs_oracle(grad, precision, tol):
 
 
 def test_laminar_tet_cube_vs_oracle():
-    """Config-2 element type: jittered tetrahedra, LSQ, far field all round."""
+    """The laminar cube's element type: jittered tetrahedra, LSQ, far field all round."""
     from oracle.oracle import Oracle
 
     m = M.tet_cube(10, jitter=0.15, seed=5)

@@ -1,13 +1,13 @@
-"""The named configurations run as stated, against the oracle (the CPU
+"""Two benchmark cases run as stated, against the oracle (the CPU
 restatement of the reference path, pinned bit-exact to the reference build).
 
-* Config 1, the Euler bump (64x32x4 hexes, uniform free stream, CFL ramp to
-  10): all 2,000 iterations.  The FP64 path follows the oracle's residual
+* The Euler bump (64x32x4 hexes, uniform free stream, CFL ramp to 10): all
+  2,000 iterations.  The FP64 path follows the oracle's residual
   history (1e-9) and wall force sums (1e-10) over the whole run, and the mixed
   path's CL and CD after 2,000 iterations lie within 1e-4 of the oracle's:
-  the accuracy condition of the headline metric, on the configuration the
-  oracle can run to the end in seconds.
-* Config 2 at its full size, the laminar cube (100^3 hexes x 6 jittered tets,
+  the accuracy condition of the headline metric, on the case the oracle can
+  run to the end in seconds.
+* The laminar cube at its full size (100^3 hexes x 6 jittered tets,
   6,000,000 cells, least-squares gradient, free stream plus seeded
   sinusoids): one residual and one LU-SGS sweep.  Residual 1e-12 (FP64) and
   1e-5 (mixed); dq after the sweep 1e-12 (FP64) and 1e-4 (mixed).
@@ -24,24 +24,24 @@ from tests.conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
-CONFIG1_STEPS = 2000
+EULER_BUMP_STEPS = 2000
 
 
 @pytest.fixture(scope="module")
-def config1():
+def euler_bump_run():
     from oracle.oracle import Oracle
 
     m = M.channel_bump(64, 32, 4)
     params = dict(cases.EULER_BUMP)
     o = Oracle(m, params)
-    hist = o.iterate(CONFIG1_STEPS)
+    hist = o.iterate(EULER_BUMP_STEPS)
     return m, params, hist, o.forces(), o.q.copy()
 
 
-def test_config1_fp64_full_run_matches_oracle(config1):
-    m, params, ho, fo, qo = config1
+def test_euler_bump_fp64_full_run_matches_oracle(euler_bump_run):
+    m, params, ho, fo, qo = euler_bump_run
     s = S.NSSolverUnstruct(m, precision="fp64", **params)
-    hs = s.Relaxation(CONFIG1_STEPS)
+    hs = s.Relaxation(EULER_BUMP_STEPS)
     # the run converges: the residual monitor drops by more than three orders
     assert ho[-1] < 1e-3 * ho[0]
     assert rel_err(hs, ho) <= 1e-9
@@ -49,10 +49,10 @@ def test_config1_fp64_full_run_matches_oracle(config1):
     assert rel_err(s.get(S.PHX_Q)[:, : m.n_cell], qo[:, : m.n_cell]) <= 1e-10
 
 
-def test_config1_mixed_forces_within_1e4_of_oracle(config1):
-    m, params, ho, fo, _ = config1
+def test_euler_bump_mixed_forces_within_1e4_of_oracle(euler_bump_run):
+    m, params, ho, fo, _ = euler_bump_run
     s = S.NSSolverUnstruct(m, precision="mixed", **params)
-    hs = s.Relaxation(CONFIG1_STEPS)
+    hs = s.Relaxation(EULER_BUMP_STEPS)
     f = s.AirForceCoef()
     ref = S.force_coefficients(fo, params.get("attackd", 0.0), params.get("angleSlide", 0.0))
     assert abs(f["CL"] - ref["CL"]) <= 1e-4
@@ -61,7 +61,7 @@ def test_config1_mixed_forces_within_1e4_of_oracle(config1):
     assert hs[-1] <= 2.0 * ho[-1]
 
 
-def test_config2_laminar_cube_6M_residual_and_sweep():
+def test_laminar_cube_6M_residual_and_sweep():
     from oracle.oracle import Oracle
 
     m = M.tet_cube(100, jitter=0.15, seed=1)

@@ -64,7 +64,7 @@ def _oracle_case(m, params, seed):
 
 @pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
 def test_single_iteration_vs_oracle_euler_bump_64x32x4(precision, tol):
-    """Config-1 mesh (8,192 hexes), perturbed state: every intermediate array."""
+    """The Euler bump mesh (8,192 hexes), perturbed state: every intermediate array."""
     m = M.channel_bump(64, 32, 4)
     params = cases.EULER_BUMP
     o, q0 = _oracle_case(m, params, seed=1)

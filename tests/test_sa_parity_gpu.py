@@ -160,7 +160,7 @@ def test_sa_requires_wall_distance():
 
 @pytest.mark.parametrize("precision,tol,turb_tol", [("fp64", FP64_TOL, FP64_TOL), ("mixed", MIXED_TOL, MIXED_TURB_TOL)])
 def test_plate_vs_oracle(precision, tol, turb_tol):
-    """Config-3 flow (SA, AUSMPW+, M 0.2, Re 5e6, CFL 50) on a 32x12x2 flat
+    """The SA flat plate flow (SA, AUSMPW+, M 0.2, Re 5e6, CFL 50) on a 32x12x2 flat
     plate, perturbed flow and nu~: one iteration, then 30 more."""
     m = M.flat_plate(32, 12, 2, first_spacing=1e-4)
     wd = M.wall_distance(m)
