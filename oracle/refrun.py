@@ -47,6 +47,12 @@ BASE_PARAMS = {
     "intervalStepForce": 100000000, "intervalStepRes": 100000000,
     "flowInitStep": 0, "nMGLevel": 1, "gridfile": "./grid/inmemory.fts",
     "isPlotVolumeField": 0, "numberOfGridProcessor": 0,
+    # NSSolver::ComputeCFL (CFD/NSSolver/src/NSSolver.cpp:619-626) inserts CFLMethod = 0
+    # into the global parameter map when the key is absent.  In the OpenMP build that
+    # insert runs from every zone thread at once (Controller::TimeStep's parallel zone
+    # loop) and races on the map; it crashed a few percent of 8-thread runs.  The key
+    # set here has the same value and leaves the threads read-only lookups.
+    "CFLMethod": 0,
 }
 
 
