@@ -167,6 +167,9 @@ class Oracle:
     """Oracle state for one mesh: grid, metrics and the primitive field."""
 
     def __init__(self, mesh, params: dict, wall_dist=None):
+        if mesh.n_face and int(np.min(mesh.face_nnode)) < 3:
+            # the restated path is the three-dimensional one (phx_ctx_create refuses the same grids)
+            raise ValueError("faces of fewer than three nodes: a two-dimensional grid")
         self.mesh = mesh
         self.keep = []
         nf, nc, nb = mesh.n_face, mesh.n_cell, mesh.n_bface

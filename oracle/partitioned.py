@@ -47,7 +47,10 @@ from .oracle import Oracle, _p, lib
 
 
 class PartitionedOracle:
-    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None):
+    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None, parts=None):
+        """The parts of `mesh` (slabs, or the cell-to-part map `owner`), or the
+        parts given (e.g. phenlei_b200.fts.zone_parts of a grid file's zones;
+        `mesh` is then None); wall_dist in global cell numbers."""
         if params.get("gradientName", "ggcell") == "ggnode":
             raise ValueError("GG-node across parts needs the interpoint exchange; not restated")
         if params.get("viscousType", 0) not in (0, 1, 3):
@@ -60,8 +63,11 @@ class PartitionedOracle:
         if params.get("nLUSGSSweeps", 1) != 1:
             raise ValueError("one LU-SGS sweep only")
         self.mesh = mesh
-        self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
-        self.parts = self._local(P.split(mesh, self.owner))
+        if parts is None:
+            self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
+            parts = P.split(mesh, self.owner)
+        self.n_cell_total = int(sum(p.mesh.n_cell for p in parts))
+        self.parts = self._local(parts)
         self.o = [Oracle(p.mesh, params, wall_dist=None if wall_dist is None else np.asarray(wall_dist)[p.cells])
                   for p in self.parts]
         self.viscous = params.get("viscousType", 0) > 0
@@ -125,7 +131,7 @@ class PartitionedOracle:
     def gather(self, name_or_array) -> np.ndarray:
         """A per-cell work array (or 'q') of every part, in global cell order."""
         first = self._cells(self.o[0], name_or_array)
-        out = np.zeros(first.shape[:-1] + (self.mesh.n_cell,))
+        out = np.zeros(first.shape[:-1] + (self.n_cell_total,))
         for part, o in zip(self.parts, self.o):
             out[..., part.cells] = self._cells(o, name_or_array)
         return out

@@ -269,9 +269,15 @@ class _Zones:
 class ZoneSet(_Zones):
     """All zones of a partitioned grid in this process, on the current device."""
 
-    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None, precision="fp64"):
-        self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
-        self.parts = P.split(mesh, self.owner)
+    def __init__(self, mesh, params: dict, nparts: int = 2, owner=None, wall_dist=None, precision="fp64",
+                 parts=None):
+        """The parts of `mesh` (slabs, or the cell-to-part map `owner`), or the
+        parts given (e.g. phenlei_b200.fts.zone_parts of a grid file's zones;
+        `mesh` is then None); wall_dist in global cell numbers."""
+        if parts is None:
+            self.owner = P.slab_owner(mesh, nparts) if owner is None else np.asarray(owner, np.int32)
+            parts = P.split(mesh, self.owner)
+        self.parts = parts
         self._setup(mesh, self.parts, params, precision, _wall_of(wall_dist))
 
     def _centres(self, cc):
@@ -311,7 +317,7 @@ class ZoneSet(_Zones):
         """A per-cell field (solver.PHX_* selector) of every zone in global cell order."""
         first = self.zones[0].get(which)
         shape = first.shape[:-1]
-        out = np.zeros(shape + (self.mesh.n_cell,))
+        out = np.zeros(shape + (self.n_cell_total,))
         for part, z in zip(self.parts, self.zones):
             out[..., part.cells] = z.get(which)[..., : z.mesh.n_cell]
         return out

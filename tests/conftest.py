@@ -16,6 +16,20 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built phx library")
 
 
+def reference_file(rel):
+    """A file of the reference project (path relative to its root), or None
+    where this machine does not hold the project.  The root comes from
+    PHX_REFERENCE_ROOT or from the one the build of oracle/_ref recorded."""
+    root = os.environ.get("PHX_REFERENCE_ROOT")
+    rec = os.path.join(ROOT, "oracle", "_ref", "reference_root.txt")
+    if not root and os.path.exists(rec):
+        root = open(rec).read().strip()
+    if not root:
+        return None
+    p = os.path.join(root, rel)
+    return p if os.path.exists(p) else None
+
+
 def load_golden(name):
     """A fixture written by tests/golden/make_golden.py from the reference solver."""
     from phenlei_b200 import mesh as M

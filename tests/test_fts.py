@@ -1,0 +1,202 @@
+"""The .fts grid reader (phenlei_b200.fts over phenlei_b200.h5lite), on the CPU.
+
+Pinned on the reference's own example grid, rae2822_hybrid2d__4.fts (the
+RAE 2822 aerofoil, hybrid triangles and quadrilaterals, four zones: the grid
+of the reference's cfd_para_transonic.hypara), against the Fluent case
+rae2822_hybrid2d.cas it was converted from, parsed independently
+(tests/fluent_cas.py): the zones hold exactly the case's nodes, faces and
+cells, each face with its two cells on the same sides and each boundary face
+with the matching boundary condition.  The interface lists of the zones
+point back at each other and join faces with the same nodes, and the halo
+plans made from them give the file's lists back.
+
+The example grid is two-dimensional, which the solver path does not take;
+`zone_parts` is checked on three-dimensional zones by rebuilding the parts of
+a split channel from their interface lists alone: the partitioned oracle then
+steps bit for bit as on the split itself.
+"""
+import numpy as np
+import pytest
+
+from oracle import refrun
+from oracle.partitioned import PartitionedOracle
+from phenlei_b200 import cases, fts
+from phenlei_b200 import mesh as M
+from phenlei_b200 import partition as P
+from phenlei_b200.h5lite import H5Error, H5File
+from tests.conftest import reference_file
+from tests.fluent_cas import FLUENT_PRESSURE_FAR_FIELD, FLUENT_WALL, read_cas
+
+EXAMPLE = "PHengLEI/examples/grid/rae2822_hybrid2d__4_0.fts"
+CASE = "PHengLEI/examples/grid/rae2822_hybrid2d.cas"
+
+needs_example = pytest.mark.skipif(reference_file(EXAMPLE) is None or reference_file(CASE) is None,
+                                   reason="the reference project's example grid is not on this machine")
+
+
+@pytest.fixture(scope="module")
+def grid():
+    path = reference_file(EXAMPLE)
+    # the grid is named without the file number, as the parameter file names it
+    return fts.read_fts(path.replace("__4_0.fts", "__4.fts"))
+
+
+@pytest.fixture(scope="module")
+def case():
+    return read_cas(reference_file(CASE))
+
+
+@needs_example
+def test_reads_every_zone_of_the_example_grid(grid):
+    assert grid.version == 2.0
+    assert len(grid.files) == 1 and grid.files[0].endswith("__4_0.fts")
+    assert [z.index for z in grid.zones] == [0, 1, 2, 3]
+    assert [z.proc for z in grid.zones] == [0, 1, 2, 3]
+    assert [z.mesh.n_cell for z in grid.zones] == [9009, 9010, 9008, 9009]
+    for z in grid.zones:
+        m = z.mesh
+        assert z.ndim == 2
+        assert m.n_node == np.unique(m.face2node).size
+        assert m.left.min() >= 0 and m.right[m.n_bface:].min() >= 0 and (m.right[: m.n_bface] == -1).all()
+        kinds = {t for t, _ in m.regions}
+        assert M.BC_INTERFACE in kinds and len(z.interface[0]) == int(
+            (np.array([m.regions[r][0] for r in m.bface_region]) == M.BC_INTERFACE).sum())
+
+
+@needs_example
+def test_zones_hold_the_fluent_case_they_were_converted_from(grid, case):
+    xyz = case["xyz"]
+    node_of = {(float(a), float(b)): i for i, (a, b) in enumerate(xyz)}
+    assert len(node_of) == xyz.shape[0]
+    cas_face = {}
+    cell_nodes = [set() for _ in range(case["n_cell"])]
+    for zone, bc, nodes, c0, c1 in case["faces"]:
+        cas_face[frozenset(nodes)] = (zone, bc, nodes, c0, c1)
+        for c in (c0, c1):
+            if c >= 0:
+                cell_nodes[c].update(nodes)
+    cell_of = {frozenset(s): c for c, s in enumerate(cell_nodes)}
+    assert len(cell_of) == case["n_cell"]
+
+    seen_cells = np.zeros(case["n_cell"], np.int64)
+    face_uses = {}
+    bc_of = {4: FLUENT_PRESSURE_FAR_FIELD, 2: FLUENT_WALL}
+    for z in grid.zones:
+        m = z.mesh
+        gnode = np.array([node_of[(float(a), float(b))] for a, b in zip(m.x, m.y)])
+        assert (m.z == 0.0).all()
+        coff = m.cell_offsets()
+        gcell = np.array([cell_of[frozenset(gnode[m.cell2node[coff[c]:coff[c + 1]]].tolist())]
+                          for c in range(m.n_cell)])
+        seen_cells[gcell] += 1
+        foff = m.face_offsets()
+        for f in range(m.n_face):
+            nodes = tuple(gnode[m.face2node[foff[f]:foff[f + 1]]].tolist())
+            zone, bc, cnodes, c0, c1 = cas_face[frozenset(nodes)]
+            face_uses[frozenset(nodes)] = face_uses.get(frozenset(nodes), 0) + 1
+            left = gcell[m.left[f]]
+            if f < m.n_bface:
+                t, name = m.regions[m.bface_region[f]]
+                if t == M.BC_INTERFACE:
+                    assert bc == 2 and left in (c0, c1)        # an interior face of the case, cut
+                    continue
+                # the boundary type, and the region name of the case's face zone
+                assert bc == bc_of[t] and name == case["zone_names"][zone][0]
+                right = -1
+            else:
+                right = gcell[m.right[f]]
+            # the same face with the same cells on the same sides: the node
+            # order of the case with its c0 on the left, or reversed with c1
+            assert (nodes == cnodes and (left, right) == (c0, c1)) or \
+                   (nodes == cnodes[::-1] and (left, right) == (c1, c0))
+    assert (seen_cells == 1).all()
+    assert len(face_uses) == len(case["faces"])
+    # interior faces cut by the partition appear in two zones, all others in one
+    n_itf = sum(len(z.interface[0]) for z in grid.zones)
+    assert sum(face_uses.values()) == len(case["faces"]) + n_itf // 2
+
+
+@needs_example
+def test_interface_lists_point_back_and_join_the_same_faces(grid):
+    zones = grid.zones
+    for i, z in enumerate(zones):
+        zid, iid, bf = z.interface
+        m = z.mesh
+        foff = m.face_offsets()
+        for k in range(len(zid)):
+            o = zones[zid[k]]
+            j = iid[k]
+            assert o.interface[0][j] == i and o.interface[1][j] == k
+            f, g = bf[k], o.interface[2][j]
+            a = {(float(m.x[n]), float(m.y[n])) for n in m.face2node[foff[f]:foff[f + 1]]}
+            ofo = o.mesh.face_offsets()
+            b = {(float(o.mesh.x[n]), float(o.mesh.y[n])) for n in o.mesh.face2node[ofo[g]:ofo[g + 1]]}
+            assert a == b
+
+
+@needs_example
+def test_halo_plans_give_the_file_interface_lists_back(grid):
+    parts = fts.zone_parts(grid.zones)
+    for z, p, (zid, iid, bf) in zip(grid.zones, parts, refrun.interface_arrays(parts)):
+        assert np.array_equal(zid, z.interface[0])
+        assert np.array_equal(iid, z.interface[1])
+        assert np.array_equal(bf, z.interface[2])
+        assert p.halo.neighbors == sorted(set(z.interface[0].tolist()))
+    assert parts[2].halo.send[3].size == parts[3].halo.recv[2].size == 127
+
+
+@needs_example
+def test_two_dimensional_zones_are_refused_by_the_path(grid):
+    from oracle.oracle import Oracle
+
+    with pytest.raises(ValueError, match="two-dimensional"):
+        Oracle(grid.zones[0].mesh, dict(cases.EULER_BUMP))
+
+
+@needs_example
+def test_reader_names_what_it_does_not_read(grid):
+    f = H5File(grid.files[0])
+    with pytest.raises(H5Error, match="not a group"):
+        f.keys("/Grid-0/iDimensions")
+    with pytest.raises(H5Error, match="not a dataset"):
+        f.read("/Grid-0/FaceTopology")
+    with pytest.raises(KeyError):
+        f.read("/Grid-9/iDimensions")
+
+
+def test_not_an_hdf5_file(tmp_path):
+    p = tmp_path / "x.fts"
+    p.write_bytes(b"not hdf5" * 100)
+    with pytest.raises(H5Error, match="signature"):
+        H5File(str(p))
+    with pytest.raises(FileNotFoundError):
+        fts.read_fts(str(tmp_path / "missing.fts"))
+
+
+@pytest.mark.parametrize("case_name,nparts", [("laminar", 3), ("sa", 2)])
+def test_zone_parts_from_interface_lists_step_like_the_split(case_name, nparts):
+    m = M.channel_bump(16, 8, 2)
+    params = dict(cases.LAMINAR if case_name == "laminar" else cases.SA_BUMP)
+    wd = M.wall_distance(m) if case_name == "sa" else None
+    owner = P.slab_owner(m, nparts)
+    split = P.split(m, owner)
+    # the zones as a grid file holds them: their meshes and interface lists only
+    zones = [fts.FtsZone(index=p.rank, proc=p.rank, mesh=p.mesh, ndim=3, interface=itf)
+             for p, itf in zip(split, refrun.interface_arrays(split))]
+    parts = fts.zone_parts(zones)
+    for a, b in zip(split, parts):
+        assert a.halo.neighbors == b.halo.neighbors
+        for q in a.halo.neighbors:
+            assert np.array_equal(a.halo.send[q], b.halo.send[q])
+            assert np.array_equal(a.halo.recv[q], b.halo.recv[q])
+    # the global cell numbers of the rebuilt parts follow the zones; the split's are the mesh's
+    gnum = np.concatenate([p.cells for p in split])
+    q0 = cases.perturbed_state(m, params, seed=5)
+    ref = PartitionedOracle(m, params, owner=owner, wall_dist=wd)
+    ref.set_state(q0)
+    h_ref = ref.iterate(3)
+    got = PartitionedOracle(None, params, parts=parts, wall_dist=None if wd is None else wd[gnum])
+    got.set_state(q0[:, gnum])
+    h_got = got.iterate(3)
+    assert np.array_equal(h_ref, h_got)
+    assert np.array_equal(ref.gather("q")[:, gnum], got.gather("q"))

@@ -269,3 +269,35 @@ def test_mixed_zones_follow_reference_golden(golden, name):
     assert rel_err(zs.gather(S.PHX_Q), d["q"]) <= 1e-4
     if sa:
         assert rel_err(zs.gather(S.PHX_Q_TURB), d["q_turb"]) <= 1e-4
+
+
+@pytest.mark.parametrize("case", ["laminar", "sa"])
+def test_zones_built_from_interface_lists_equal_the_split(case):
+    """Zones as a grid file gives them (meshes and interface lists, read by
+    phenlei_b200.fts.zone_parts) step bit for bit as the same split built
+    from the whole mesh."""
+    from oracle import refrun
+    from phenlei_b200 import fts
+    from phenlei_b200 import partition as P
+    from phenlei_b200.zones import ZoneSet
+
+    params = _case(case)
+    m, q0, qt0, wd = _inputs(params)
+    owner = P.slab_owner(m, 3)
+    split = P.split(m, owner)
+    zones = [fts.FtsZone(index=p.rank, proc=p.rank, mesh=p.mesh, ndim=3, interface=itf)
+             for p, itf in zip(split, refrun.interface_arrays(split))]
+    gnum = np.concatenate([p.cells for p in split])
+    a = ZoneSet(m, params, 3, owner=owner, wall_dist=wd)
+    a.set_state(q0, qt0)
+    ha = a.iterate(4)
+    b = ZoneSet(None, params, parts=fts.zone_parts(zones), wall_dist=None if wd is None else wd[gnum])
+    b.set_state(q0[:, gnum], None if qt0 is None else qt0[gnum])
+    hb = b.iterate(4)
+    assert np.array_equal(a.gather(S.PHX_Q)[:, gnum], b.gather(S.PHX_Q))
+    if qt0 is not None:
+        assert np.array_equal(a.gather(S.PHX_Q_TURB)[gnum], b.gather(S.PHX_Q_TURB))
+    # the residual monitor sums with FP64 atomics: equal up to the order of the sums
+    assert rel_err(hb, ha) <= 1e-13
+    a.close()
+    b.close()
