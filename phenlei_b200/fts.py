@@ -9,7 +9,9 @@ The reference reads them with IO_HDF5Read (API/PreProcess/src/Pre_HDF5File.cpp):
   block_type) and holds zone i in the group /Grid-i (ReadEachGrid, :1270-1316);
 * ReadUnstructGrid (:1753-1797) reads iDimensions (nodes, faces, cells),
   GridCoordinates, FaceTopology, InterfaceInfo, CellTopology, BCName and
-  InterpointInfo.
+  InterpointInfo;
+* the stored wall distances sit beside each grid file in `name_i.wdt`
+  (ReadWallDist, :910-1024).
 
 ReadFaceTopology (:1799-1847) reverses the node list of every face whose left
 cell is negative and swaps its two cells, so that every face has a cell on its
@@ -165,6 +167,31 @@ def read_fts(path: str) -> FtsGrid:
     if [z.index for z in zones] != list(range(len(zones))):
         raise ValueError("the zone indices are not 0..n-1")
     return FtsGrid(version=version, files=files, zones=zones)
+
+
+def read_wall_distance(grid: FtsGrid) -> list:
+    """The wall distance of every cell of every zone from the grid's `.wdt`
+    files, the reference's stored wall distances (IO_HDF5Read::ReadWallDist,
+    API/PreProcess/src/Pre_HDF5File.cpp:910-1024): beside each grid file
+    `name_i.fts` the file `name_i.wdt` holds one dataset Grid-<zone> of n_cell
+    values per zone.  Returns a list in zone order, or None where the files
+    are missing (the reference then computes the distances itself)."""
+    per_zone = {}
+    for fn in grid.files:
+        wdt = os.path.splitext(fn)[0] + ".wdt"
+        if not os.path.exists(wdt):
+            return None
+        f = H5File(wdt)
+        for k in f.keys("/"):
+            if k.startswith("Grid-") and k[5:].isdigit():
+                per_zone[int(k[5:])] = np.asarray(f.read("/" + k), np.float64).reshape(-1)
+    out = []
+    for z in grid.zones:
+        d = per_zone.get(z.index)
+        if d is None or d.size != z.mesh.n_cell:
+            raise ValueError(f"zone {z.index}: the wall distance file does not hold one value per cell")
+        out.append(d)
+    return out
 
 
 def zone_parts(zones: list) -> list:

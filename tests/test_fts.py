@@ -146,6 +146,41 @@ def test_halo_plans_give_the_file_interface_lists_back(grid):
 
 
 @needs_example
+def test_stored_wall_distances(grid):
+    """The example's .wdt file: one distance per cell of every zone.  In the
+    two zones away from the aerofoil (triangles only) every value is the
+    distance from the cell's node mean to the nearest wall segment, to
+    rounding; near the wall (zones 2 and 3, with quadrilaterals) the
+    reference's search takes other centres, so those are held to 25 %."""
+    wd = fts.read_wall_distance(grid)
+    assert [d.size for d in wd] == [z.mesh.n_cell for z in grid.zones]
+    seg = []
+    for z in grid.zones:
+        m = z.mesh
+        off = m.face_offsets()
+        for f in range(m.n_bface):
+            if m.regions[m.bface_region[f]][0] == M.BC_SOLID_SURFACE:
+                a, b = m.face2node[off[f]:off[f + 1]]
+                seg.append((m.x[a], m.y[a], m.x[b], m.y[b]))
+    x0, y0, x1, y1 = (np.array(seg)[:, k][None, :] for k in range(4))
+    for z, d in zip(grid.zones, wd):
+        m = z.mesh
+        cnn = np.asarray(m.cell_nnode)
+        cell = np.repeat(np.arange(m.n_cell), cnn)
+        px = (np.bincount(cell, m.x[m.cell2node]) / cnn)[:, None]
+        py = (np.bincount(cell, m.y[m.cell2node]) / cnn)[:, None]
+        dx, dy = x1 - x0, y1 - y0
+        t = np.clip(((px - x0) * dx + (py - y0) * dy) / (dx * dx + dy * dy), 0.0, 1.0)
+        exact = np.sqrt((px - x0 - t * dx) ** 2 + (py - y0 - t * dy) ** 2).min(axis=1)
+        rel = np.abs(exact - d) / d
+        assert (d > 0).all()
+        if int(cnn.max()) == 3:
+            assert np.median(rel) <= 1e-13 and rel.max() <= 1e-5
+        else:
+            assert rel.max() <= 0.25
+
+
+@needs_example
 def test_two_dimensional_zones_are_refused_by_the_path(grid):
     from oracle.oracle import Oracle
 
