@@ -521,6 +521,9 @@ def main_zones(args, rank, world, wl):
     torch.cuda.set_device(rank % max(ndev, 1))
     backend = "nccl" if ndev >= world else "gloo"
     dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    # one collective of all ranks first: the halo exchanges that follow are
+    # point-to-point batches between neighbours only
+    dist.barrier()
     sa = wl["params"].get("viscousType", 0) == 3
     if "channel" in wl:
         # weak scaling: this rank's slab of a channel `world` times as long
