@@ -156,13 +156,16 @@ def read_fts(path: str) -> FtsGrid:
         idx = _ints(f, "/Information/block_idx")
         proc = _ints(f, "/Information/block_proc")
         btype = _ints(f, "/Information/block_type")
+        if min(idx.size, proc.size, btype.size) < n:
+            raise ValueError(f"{fn}: /Information lists fewer than nBlocks zones")
         for i in range(n):
-            # ReadEachGrid: the file's i-th zone is the group Grid-<block_idx[i]>,
-            # and block_proc / block_type are indexed by that global index
+            # ReadTotalInfo / ReadEachGrid (:1149-1203, :1270-1316): the file's
+            # i-th entries give the zone's global index, its processor and its
+            # type; the zone is the group Grid-<global index>
             gi = int(idx[i])
-            if int(btype[gi]) != UNSTRUCTGRID:
+            if int(btype[i]) != UNSTRUCTGRID:
                 raise ValueError(f"zone {gi} is a structured zone; only unstructured zones are read")
-            zones.append(_zone(f, f"/Grid-{gi}", gi, int(proc[gi])))
+            zones.append(_zone(f, f"/Grid-{gi}", gi, int(proc[i])))
     zones.sort(key=lambda z: z.index)
     if [z.index for z in zones] != list(range(len(zones))):
         raise ValueError("the zone indices are not 0..n-1")
@@ -191,6 +194,47 @@ def read_wall_distance(grid: FtsGrid) -> list:
         if d is None or d.size != z.mesh.n_cell:
             raise ValueError(f"zone {z.index}: the wall distance file does not hold one value per cell")
         out.append(d)
+    return out
+
+
+def read_restart_h5(path: str, zone: int, n_cell: int, n_bface: int, turb_path: str | None = None) -> dict:
+    """The reference's HDF5 restart of one zone, as NSSolverUnstruct::ReadRestartH5
+    (CFD/NSSolver/src/NSSolverUnstruct.cpp:1400-1440) and
+    TurbSolverUnstr::ReadRestartH5 (CFD/TurbSolver/src/TurbSolverUnstr.cpp:638-693)
+    read it.  The flow file holds `outnstep` and, in the group Group<zone>
+    (CFDSolver::CreateH5RestartFile, CFD/Solver/src/CFDSolver.cpp:2345-2522),
+    `nTotalCell` and `q` [nEquation][nTotalCell + nBoundFace] of FP64
+    primitive variables of the cells and their ghosts (and `t`); the
+    turbulence file holds `q_turb` [nTurbulenceEquation][...] and `visturb`.
+    A restart of another grid (its nTotalCell differs) is refused, as the
+    reference refuses it.  Returns outnstep, q [5][nTotal] and, with
+    `turb_path`, q_turb [nTotal] and vist [nTotal] (None where the file has
+    no visturb, which the reference then leaves as it was)."""
+    nt = n_cell + n_bface
+    g = f"/Group{zone}"
+
+    def zone_group(f: H5File, what: str):
+        if not f.exists(g):
+            raise ValueError(f"the {what} restart has no group {g[1:]}")
+        n = int(np.asarray(f.read(g + "/nTotalCell")).reshape(-1)[0])
+        if n != n_cell:
+            raise ValueError(f"the {what} restart holds {n} cells, the grid {n_cell}")
+
+    def rows(a: np.ndarray, nrow: int) -> np.ndarray:
+        a = np.asarray(a, np.float64).reshape(-1)
+        if a.size < nrow * nt or a.size % nrow:
+            raise ValueError(f"{a.size} values cannot hold {nrow} rows of {nt}")
+        return a.reshape(nrow, -1)[:, :nt].copy()
+
+    f = H5File(path)
+    zone_group(f, "flow")
+    out = {"outnstep": int(np.asarray(f.read("/outnstep")).reshape(-1)[0]),
+           "q": rows(f.read(g + "/q"), 5)}
+    if turb_path is not None:
+        ft = H5File(turb_path)
+        zone_group(ft, "turbulence")
+        out["q_turb"] = rows(ft.read(g + "/q_turb"), 1)[0]
+        out["vist"] = rows(ft.read(g + "/visturb"), 1)[0] if ft.exists(g + "/visturb") else None
     return out
 
 

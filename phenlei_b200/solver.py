@@ -244,6 +244,21 @@ class NSSolverUnstruct:
         """Continues from a restart file of the same grid."""
         self._check(lib().phx_read_restart(self.h, os.fsencode(path)), "phx_read_restart")
 
+    def ReadRestartH5(self, flow_path: str, zone: int = 0, turb_path: str | None = None):
+        """Continues from the reference's own HDF5 restart files of this zone
+        (phenlei_b200.fts.read_restart_h5): the step count, the state of the
+        cells and ghosts and, with the turbulence file, nu~ and the eddy
+        viscosity."""
+        from .fts import read_restart_h5
+
+        r = read_restart_h5(flow_path, zone, self.mesh.n_cell, self.mesh.n_bface, turb_path)
+        self.set(PHX_Q, r["q"])
+        if turb_path is not None:
+            self.set(PHX_Q_TURB, r["q_turb"])
+            if r["vist"] is not None:
+                self.set(PHX_VIST, r["vist"])
+        self.step = r["outnstep"]
+
     def set_wait_limit(self, polls: int):
         """Bound on every device-side dependency wait of the LU-SGS sweeps, in polls."""
         self._check(lib().phx_set_wait_limit(self.h, int(polls)), "phx_set_wait_limit")

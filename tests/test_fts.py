@@ -235,3 +235,112 @@ def test_zone_parts_from_interface_lists_step_like_the_split(case_name, nparts):
     h_got = got.iterate(3)
     assert np.array_equal(h_ref, h_got)
     assert np.array_equal(ref.gather("q")[:, gnum], got.gather("q"))
+
+
+def _fts_tree(parts, itfs, turned=()):
+    """A grid file's groups for the zones `parts` in the reference's layout
+    (IO_HDF5Read, Pre_HDF5File.cpp:1270-1990).  Boundary faces listed in
+    `turned` are stored the other way round (no left cell, nodes reversed),
+    which the reader must undo."""
+    n = len(parts)
+    tree = {"Version": {"VersionData": np.array([2.0])},
+            "Information": {"nBlocks": np.array([n], np.int32), "block_idx": np.arange(n, dtype=np.int32),
+                            "block_proc": np.zeros(n, np.int32), "block_type": np.zeros(n, np.int32)}}
+    for p, (zid, iid, bf) in zip(parts, itfs):
+        m = p.mesh
+        nb = m.n_bface
+        left = np.asarray(m.left, np.int32).copy()
+        right = np.asarray(m.right, np.int32).copy()
+        f2n = np.asarray(m.face2node, np.int32).copy()
+        off = m.face_offsets()
+        for f in turned:
+            if f < nb:
+                f2n[off[f]:off[f + 1]] = f2n[off[f]:off[f + 1]][::-1].copy()
+                left[f], right[f] = -1, left[f]
+        btype = np.array([m.regions[r][0] for r in m.bface_region], np.int32)
+        names = b"".join(m.regions[r][1].encode() + b"\0" for r in m.bface_region)
+        tree[f"Grid-{p.rank}"] = {
+            "iDimensions": np.array([m.n_node, m.n_face, m.n_cell], np.int32),
+            "GridCoordinates": {"CoordinateX": m.x, "CoordinateY": m.y, "CoordinateZ": m.z},
+            "FaceTopology": {"nodeNumberOfEachFace": np.asarray(m.face_nnode, np.int32), "face2Node": f2n,
+                             "leftCellOfFace": left, "rightCellOfFace": right,
+                             "nBoundFace": np.array([nb], np.int32), "BcType": btype},
+            "CellTopology": {"nodeNumberOfEachCell": np.asarray(m.cell_nnode, np.int32),
+                             "cell2Node": np.asarray(m.cell2node, np.int32)},
+            "BCName": {"BCName": np.frombuffer(names, np.int8)},
+            "InterfaceInfo": {"nIFace": np.array([len(zid)], np.int32), "interFace2ZoneID": zid,
+                              "interFace2InterFaceID": iid, "interFace2BoundaryFace": bf},
+        }
+    return tree
+
+
+def test_a_three_dimensional_grid_file_reads_back_and_steps_like_the_split(tmp_path):
+    """Zones of a split hex/prism channel written as a grid file (numbered
+    files, some boundary faces stored the other way round) come back as the
+    same meshes and interface lists, and step bit for bit as the split."""
+    from tests.h5write import write_h5
+
+    m = M.channel_bump(16, 8, 2, prism_layers=2)
+    params = dict(cases.LAMINAR)
+    owner = P.slab_owner(m, 3)
+    split = P.split(m, owner)
+    itfs = refrun.interface_arrays(split)
+    tree = _fts_tree(split, itfs, turned=(0, 3, 5))
+    # the reference's writer names the files of a grid name_0, name_1, ...:
+    # two files here, zones 0 and 1 in the first, zone 2 in the second
+    # (each file's /Information lists its own zones)
+    info = lambda idx: {"nBlocks": np.array([len(idx)], np.int32), "block_idx": np.array(idx, np.int32),  # noqa: E731
+                        "block_proc": np.array(idx, np.int32), "block_type": np.zeros(len(idx), np.int32)}
+    first = {k: v for k, v in tree.items() if k != "Grid-2"}
+    first["Information"] = info([0, 1])
+    second = {"Version": tree["Version"], "Grid-2": tree["Grid-2"], "Information": info([2])}
+    write_h5(str(tmp_path / "chan__3_0.fts"), first)
+    write_h5(str(tmp_path / "chan__3_1.fts"), second)
+    grid = fts.read_fts(str(tmp_path / "chan__3.fts"))
+    assert len(grid.files) == 2 and [z.index for z in grid.zones] == [0, 1, 2]
+    assert [z.proc for z in grid.zones] == [0, 1, 2]
+    for z, p, itf in zip(grid.zones, split, itfs):
+        a, b = z.mesh, p.mesh
+        assert z.ndim == 3
+        for k in ("x", "y", "z", "face_nnode", "face2node", "left", "right", "cell_nnode", "cell2node"):
+            assert np.array_equal(getattr(a, k), getattr(b, k)), k
+        assert a.n_bface == b.n_bface
+        assert [a.regions[r] for r in a.bface_region] == [b.regions[r] for r in b.bface_region]
+        for x, y in zip(z.interface, itf):
+            assert np.array_equal(x, y)
+    gnum = np.concatenate([p.cells for p in split])
+    q0 = cases.perturbed_state(m, params, seed=9)
+    ref = PartitionedOracle(m, params, owner=owner)
+    ref.set_state(q0)
+    got = PartitionedOracle(None, params, parts=fts.zone_parts(grid.zones))
+    got.set_state(q0[:, gnum])
+    assert np.array_equal(ref.iterate(3), got.iterate(3))
+    assert np.array_equal(ref.gather("q")[:, gnum], got.gather("q"))
+
+
+def test_the_reference_restart_layout_reads_back(tmp_path):
+    """Restart files in the layout of CFDSolver::CreateH5RestartFile and the
+    DumpRestartH5 methods: the flow file's q of cells and ghosts and
+    outnstep, the turbulence file's q_turb and visturb; a restart of
+    another grid is refused."""
+    from tests.h5write import write_h5
+
+    nc, nb = 40, 12
+    nt = nc + nb
+    rng = np.random.default_rng(4)
+    q = rng.standard_normal((5, nt))
+    write_h5(str(tmp_path / "flow.dat"), {
+        "Version": np.array([1], np.int32), "outnstep": np.array([1234], np.int32),
+        "Group3": {"q": q, "t": rng.standard_normal((1, nt)), "nTotalCell": np.array([nc], np.int32)}})
+    qt, vt = rng.standard_normal((1, nt)), rng.standard_normal((1, nt))
+    write_h5(str(tmp_path / "turb.dat"), {
+        "Version": np.array([1], np.int32), "outnstep": np.array([1234], np.int32),
+        "Group3": {"q_turb": qt, "visturb": vt, "nTotalCell": np.array([nc], np.int32)}})
+    r = fts.read_restart_h5(str(tmp_path / "flow.dat"), 3, nc, nb, str(tmp_path / "turb.dat"))
+    assert r["outnstep"] == 1234
+    assert np.array_equal(r["q"], q)
+    assert np.array_equal(r["q_turb"], qt[0]) and np.array_equal(r["vist"], vt[0])
+    with pytest.raises(ValueError, match="cells"):
+        fts.read_restart_h5(str(tmp_path / "flow.dat"), 3, nc + 1, nb)
+    with pytest.raises(ValueError, match="Group0"):
+        fts.read_restart_h5(str(tmp_path / "flow.dat"), 0, nc, nb)
