@@ -242,10 +242,10 @@ class DistributedOracle(PartitionedOracle):
     default torch.distributed group (gloo) and the global sums by all_reduce.
     Every rank builds the same partition and calls the same steps."""
 
-    def __init__(self, mesh, params: dict, rank: int, world: int, owner=None, wall_dist=None):
+    def __init__(self, mesh, params: dict, rank: int, world: int, owner=None, wall_dist=None, parts=None):
         self._rank = rank
         self._world = world
-        super().__init__(mesh, params, world, owner=owner, wall_dist=wall_dist)
+        super().__init__(mesh, params, world, owner=owner, wall_dist=wall_dist, parts=parts)
 
     def _local(self, parts):
         if len(parts) != self._world:

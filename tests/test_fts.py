@@ -344,3 +344,53 @@ def test_the_reference_restart_layout_reads_back(tmp_path):
         fts.read_restart_h5(str(tmp_path / "flow.dat"), 3, nc + 1, nb)
     with pytest.raises(ValueError, match="Group0"):
         fts.read_restart_h5(str(tmp_path / "flow.dat"), 0, nc, nb)
+
+
+def _file_rank_main(rank, world, port, path, out):
+    import datetime
+    import os
+
+    import torch.distributed as dist
+
+    from oracle.partitioned import DistributedOracle
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        grid = fts.read_fts(path)
+        params = dict(cases.LAMINAR)
+        do = DistributedOracle(None, params, rank, world, parts=fts.zone_parts(grid.zones))
+        n = sum(z.mesh.n_cell for z in grid.zones)
+        q0 = cases.perturbed_state(M.channel_bump(16, 8, 2), params, seed=2)[:, :n]
+        do.set_state(q0)
+        hist = do.iterate(3)
+        np.savez(os.path.join(out, f"rank{rank}.npz"), hist=hist, cells=do.local_cells(), q=do.gather("q"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_grid_file_zones_on_two_gloo_ranks_equal_in_process(tmp_path):
+    """Each of two ranks reads the grid file and steps its own zone, halos
+    over gloo: the same history and state as all zones in one process."""
+    import torch.multiprocessing as mp
+
+    from tests.h5write import write_h5
+    from tests.test_partition import _free_port
+
+    m = M.channel_bump(16, 8, 2)
+    split = P.split(m, P.slab_owner(m, 2))
+    path = str(tmp_path / "two.fts")
+    write_h5(path, _fts_tree(split, refrun.interface_arrays(split)))
+    mp.spawn(_file_rank_main, args=(2, _free_port(), path, str(tmp_path)), nprocs=2, join=True)
+    grid = fts.read_fts(path)
+    params = dict(cases.LAMINAR)
+    po = PartitionedOracle(None, params, parts=fts.zone_parts(grid.zones))
+    n = sum(z.mesh.n_cell for z in grid.zones)
+    po.set_state(cases.perturbed_state(m, params, seed=2)[:, :n])
+    h = po.iterate(3)
+    q = po.gather("q")
+    for r in range(2):
+        d = np.load(tmp_path / f"rank{r}.npz")
+        assert np.array_equal(d["hist"], h)
+        assert np.array_equal(d["q"][:, d["cells"]], q[:, d["cells"]])
