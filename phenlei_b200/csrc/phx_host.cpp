@@ -1774,7 +1774,10 @@ int phx_set_halo(phx_ctx *ctx, int64_t n_send, const int32_t *send_cells, int64_
     if (!ctx || n_send < 0 || n_recv < 0 || (n_send > 0 && !send_cells) || (n_recv > 0 && !recv_bfaces))
         return PHX_ERR_ARG;
     if (!ctx->hasInterface) return fail(ctx, PHX_ERR_STATE, "the grid has no interface faces");
-    if (n_send > ctx->nCell || n_recv > ctx->nBFace) return PHX_ERR_ARG;
+    // a cell may be sent more than once (one row per interface face behind
+    // it, to one or several zones), so only the receive side is bounded by a
+    // grid count: every interface face is received once
+    if (n_send > INT32_MAX || n_recv > ctx->nBFace) return PHX_ERR_ARG;
     std::vector<int> snd((size_t)n_send), rcv((size_t)n_recv);
     for (int64_t i = 0; i < n_send; ++i) {
         if (send_cells[i] < 0 || send_cells[i] >= ctx->nCell) return fail(ctx, PHX_ERR_ARG, "phx_set_halo: bad cell");

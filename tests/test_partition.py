@@ -306,3 +306,25 @@ def test_channel_zones_built_alone_equal_the_split_channel(prism, world):
                 cpts = xyz[q][np.asarray(nq.cell2node)[coff[c]:coff[c + 1]]]
                 d = np.min(np.abs(fpts[:, None, :] - cpts[None, :, :]).sum(-1), axis=1)
                 assert np.all(d < 1e-12)
+
+
+def test_a_zone_one_cell_thick_sends_each_cell_across_both_cuts():
+    """A slab one cell thick between two zones: each of its cells is sent
+    across both cuts (twice as many send rows as cells), and the partitioned
+    oracle steps it."""
+    from oracle.partitioned import PartitionedOracle
+    from phenlei_b200 import cases
+
+    m = MESHES["bump"]()
+    cx = P.cell_centroids(m)[:, 0]
+    order = np.lexsort((np.arange(m.n_cell), cx))
+    column = np.empty(m.n_cell, np.int64)
+    column[order] = np.arange(m.n_cell) * 16 // m.n_cell
+    owner = np.where(column < 7, 0, np.where(column == 7, 1, 2)).astype(np.int32)
+    parts = P.split(m, owner)
+    assert [p.halo.neighbors for p in parts] == [[1], [0, 2], [1]]
+    assert parts[1].halo.n_send() == 2 * parts[1].mesh.n_cell == parts[1].n_iface
+    params = _case("laminar")
+    po = PartitionedOracle(m, params, 3, owner=owner)
+    po.set_state(cases.perturbed_state(m, params, seed=3))
+    assert np.isfinite(po.iterate(2)).all()

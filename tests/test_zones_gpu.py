@@ -301,3 +301,31 @@ def test_zones_built_from_interface_lists_equal_the_split(case):
     assert rel_err(hb, ha) <= 1e-13
     a.close()
     b.close()
+
+
+def test_a_zone_one_cell_thick_sends_more_rows_than_it_has_cells():
+    """A slab zone one cell thick between two others sends each cell across
+    both cuts, so its halo lists more send rows than cells; it runs as the
+    partitioned oracle runs (FP64 1e-12 after one iteration)."""
+    from oracle.partitioned import PartitionedOracle
+    from phenlei_b200 import partition as P
+    from phenlei_b200.zones import ZoneSet
+
+    params = _case("laminar")
+    m, q0, _, _ = _inputs(params)
+    cx = P.cell_centroids(m)[:, 0]
+    order = np.lexsort((np.arange(m.n_cell), cx))
+    column = np.empty(m.n_cell, np.int64)
+    column[order] = np.arange(m.n_cell) * 16 // m.n_cell     # 16 columns of cells along x
+    owner = np.where(column < 7, 0, np.where(column == 7, 1, 2)).astype(np.int32)
+    po = PartitionedOracle(m, params, 3, owner=owner)
+    po.set_state(q0)
+    zs = ZoneSet(m, params, 3, owner=owner)
+    zs.set_state(q0)
+    thin = zs.parts[1]
+    assert thin.halo.n_send() == 2 * thin.mesh.n_cell
+    h_o, h_z = po.iterate(1), zs.iterate(1)
+    assert rel_err(h_z, h_o) <= 1e-12
+    assert rel_err(zs.gather(S.PHX_Q), po.gather("q")) <= 1e-12
+    assert rel_err(zs.gather(S.PHX_DQ), po.gather("dq")) <= 1e-12
+    zs.close()
