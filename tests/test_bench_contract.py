@@ -5,6 +5,8 @@
   higher_is_better, config, cpu_baseline, e2e with zero copy bytes), its
   throughput agreeing with its own step time.
 * Under a launcher (RANK > 0) the reference arm exits without work or output.
+* When the threaded reference run fails twice, the arm times one zone on one
+  core instead of failing.
 * The compulsory-byte count of the minimal pass structure never exceeds this
   build's own per-pass count, and both grow with the cell count.
 """
@@ -67,3 +69,23 @@ def test_compulsory_bytes_below_this_build_per_pass_bytes(precision, viscous, gr
         assert 0 < mb <= kb["iteration"]
     assert bench.minimal_bytes(large, precision, viscous, gradient) > bench.minimal_bytes(small, precision, viscous,
                                                                                            gradient)
+
+
+@pytest.mark.skipif(not refrun.available(), reason="the reference build (oracle/_ref) is absent")
+def test_reference_arm_falls_back_to_one_core_when_the_threaded_run_fails(monkeypatch):
+    import argparse
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    calls = []
+
+    def broken(*a, **k):
+        calls.append(1)
+        raise RuntimeError("reference harness failed (-11)")
+
+    monkeypatch.setattr(refrun, "run_reference_zones", broken)
+    monkeypatch.setattr(bench, "host_threads", lambda: 4)
+    cb = bench.cpu_baseline(argparse.Namespace(steps=2), "euler_bump_8k")
+    assert len(calls) == 2
+    assert cb["cores"] == 1 and cb["kind"] == "reference" and cb["value"] > 0
