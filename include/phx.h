@@ -342,7 +342,9 @@ int phx_swap_geometry(phx_ctx *ctx, int64_t n, const int32_t *bfaces, const doub
 /* The halo plan of this zone: the n_send cells (this zone's cell numbers)
  * whose values the neighbouring zones receive, and the n_recv interface faces
  * (boundary face numbers) whose ghosts receive, each in the caller's order
- * (concatenated over the neighbours).  Host arrays, copied. */
+ * (concatenated over the neighbours).  A cell is listed once per interface
+ * face behind it, so n_send may exceed the cell count; each interface face is
+ * listed once at most.  Host arrays, copied. */
 int phx_set_halo(phx_ctx *ctx, int64_t n_send, const int32_t *send_cells, int64_t n_recv,
                  const int32_t *recv_bfaces);
 /* Bytes of one row of a halo field (it depends on the precision). */
