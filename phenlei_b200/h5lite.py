@@ -23,6 +23,9 @@ being misread.
 """
 from __future__ import annotations
 
+import mmap
+import os
+
 import numpy as np
 
 _SIGNATURE = b"\x89HDF\r\n\x1a\n"
@@ -45,8 +48,12 @@ class H5Error(ValueError):
 
 class H5File:
     def __init__(self, path: str):
+        # mapped, not read: a grid file of a large mesh is read in the parts asked for
         with open(path, "rb") as f:
-            self.b = f.read()
+            size = os.fstat(f.fileno()).st_size
+            if size < 8:
+                raise H5Error("no HDF5 signature")
+            self.b = mmap.mmap(f.fileno(), 0, access=mmap.ACCESS_READ)
         base = self._find_superblock()
         ver = self.b[base + 8]
         if ver not in (0, 1):
@@ -120,7 +127,9 @@ class H5File:
         # signature, version, reserved (3), data segment size, free-list offset, data segment address
         data = self._abs(self._addr(h + 8 + 2 * self.sl))
         s = data + off
-        e = self.b.index(b"\0", s)
+        e = self.b.find(b"\0", s)
+        if e < 0:
+            raise H5Error("unterminated name in a local heap")
         return self.b[s:e].decode()
 
     def _btree_group(self, node: int, heap: int, out: dict):
