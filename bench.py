@@ -18,7 +18,8 @@ the reference's halo exchanges (phenlei_b200.zones): NCCL point-to-point halos
 and all-reduces.  `value` is all ranks' cells x steps over the slowest rank's
 device time.  With fewer GPUs than ranks (the halo path on one GPU) the ranks
 share it and the rows go through gloo on the host.  Workloads that are not a
-channel split their one mesh into N zones instead (strong scaling).
+channel split their one mesh into N zones by recursive coordinate bisection
+instead (strong scaling).
 
 `--impl reference` times the reference's own solver, built from its sources
 with its OpenMP loops over zones (oracle/_ref/ref_harness_omp), on a bounded
@@ -421,6 +422,7 @@ def run_zones(args, rank, world, precision, wl, zone, wd, mlp_blob=None, train=F
     import torch
     import torch.distributed as dist
 
+    from phenlei_b200 import partition as P
     from phenlei_b200 import solver as S
     from phenlei_b200.zones import DistributedZone
 
@@ -431,7 +433,9 @@ def run_zones(args, rank, world, precision, wl, zone, wd, mlp_blob=None, train=F
     if zone is not None:
         dz = DistributedZone(None, params, wall_dist=wd, precision=precision, part=zone)
     else:
-        dz = DistributedZone(wl["mesh"](), params, wall_dist=wd, precision=precision)
+        mesh = wl["mesh"]()
+        # strong scaling of one mesh: recursive bisection keeps the cut faces fewer than slabs
+        dz = DistributedZone(mesh, params, owner=P.rcb_owner(mesh, world), wall_dist=wd, precision=precision)
     z = dz.zones[0]
     if mlp_blob is not None:
         z.set_mlp_blob(mlp_blob)
@@ -540,7 +544,7 @@ def main_zones(args, rank, world, wl):
     else:
         zone, scaling = None, "strong"
         wd = M.wall_distance(wl["mesh"]()) if sa else None
-        layout = "the workload's mesh split into %d slabs" % world
+        layout = "the workload's mesh split into %d parts by recursive coordinate bisection" % world
     r64 = blob = None
     if args.mlp_blob:
         blob = np.load(args.mlp_blob).astype(np.float32)

@@ -89,6 +89,34 @@ def slab_owner(m: Mesh, nparts: int, axis: int | None = None) -> np.ndarray:
     return owner
 
 
+def rcb_owner(m: Mesh, nparts: int) -> np.ndarray:
+    """Part of every cell by recursive coordinate bisection of the cell
+    centroids: a set of cells bound for k parts is cut across its longest
+    extent at the floor(k/2)/k quantile (ties broken by cell number), and the
+    two sides go on with floor(k/2) and k - floor(k/2) parts.  Part sizes
+    differ by at most one cell per level of cuts, and the cuts follow the
+    mesh's shape instead of one axis, so for many parts the interface faces
+    (the halo volume) stay fewer than with slabs."""
+    if nparts < 1:
+        raise ValueError("nparts must be >= 1")
+    c = cell_centroids(m)
+    owner = np.empty(m.n_cell, dtype=np.int32)
+    stack = [(np.arange(m.n_cell), 0, nparts)]
+    while stack:
+        cells, first, k = stack.pop()
+        if k == 1 or cells.size == 0:
+            owner[cells] = first
+            continue
+        pts = c[cells]
+        axis = int(np.argmax(pts.max(axis=0) - pts.min(axis=0)))
+        order = cells[np.lexsort((cells, pts[:, axis]))]
+        kl = k // 2
+        nl = (cells.size * kl) // k
+        stack.append((order[:nl], first, kl))
+        stack.append((order[nl:], first + kl, k - kl))
+    return owner
+
+
 def _ranks(counts: np.ndarray) -> np.ndarray:
     """0, 1, .., n-1 for each run length n in `counts`, concatenated."""
     counts = np.asarray(counts, np.int64)

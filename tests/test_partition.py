@@ -328,3 +328,32 @@ def test_a_zone_one_cell_thick_sends_each_cell_across_both_cuts():
     po = PartitionedOracle(m, params, 3, owner=owner)
     po.set_state(cases.perturbed_state(m, params, seed=3))
     assert np.isfinite(po.iterate(2)).all()
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 3, 7, 8, 16])
+def test_recursive_bisection_balances_parts_and_cuts_fewer_faces(nparts):
+    """rcb_owner: every part non-empty, sizes within one cell per level of
+    cuts, a valid split; from 7 parts on the jittered-tet cube it cuts fewer
+    faces than slabs."""
+    m = MESHES["tets"]() if nparts < 7 else M.tet_cube(12, jitter=0.15, seed=1)
+    owner = P.rcb_owner(m, nparts)
+    cnt = np.bincount(owner, minlength=nparts)
+    assert cnt.size == nparts and cnt.min() > 0
+    assert cnt.max() - cnt.min() <= int(np.ceil(np.log2(nparts))) if nparts > 1 else cnt[0] == m.n_cell
+    assert np.array_equal(P.rcb_owner(m, nparts), owner)     # deterministic
+    parts = P.split(m, owner)
+    assert sum(p.mesh.n_cell for p in parts) == m.n_cell
+    if nparts >= 7:
+        cut = lambda o: sum(p.n_iface for p in P.split(m, o)) // 2  # noqa: E731
+        assert cut(owner) < cut(P.slab_owner(m, nparts)) / 2
+
+
+def test_recursive_bisection_parts_step_in_the_partitioned_oracle():
+    from oracle.partitioned import PartitionedOracle
+    from phenlei_b200 import cases
+
+    m = MESHES["bump"]()
+    params = _case("laminar")
+    po = PartitionedOracle(m, params, 4, owner=P.rcb_owner(m, 4))
+    po.set_state(cases.perturbed_state(m, params, seed=3))
+    assert np.isfinite(po.iterate(2)).all()
