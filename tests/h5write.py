@@ -4,8 +4,8 @@ reference's grid and restart files are written, and the only layout
 phenlei_b200.h5lite reads), after the published HDF5 File Format
 Specification:
 
-* a version 0 superblock whose root symbol-table entry caches the root
-  group's B-tree and local heap;
+* a version 0 (or 1) superblock whose root symbol-table entry caches the
+  root group's B-tree and local heap;
 * version 1 object headers;
 * groups: a symbol-table message, one level-0 group B-tree node, one
   symbol-table node with the members sorted by name, a local heap of names;
@@ -30,8 +30,9 @@ def _pad8(b: bytes) -> bytes:
 
 
 class _Writer:
-    def __init__(self):
-        self.buf = bytearray(96)          # the superblock with the root entry, written last
+    def __init__(self, sb_size=96):
+        self.sb_size = sb_size
+        self.buf = bytearray(sb_size)     # the superblock with the root entry, written last
 
     def _alloc(self, data: bytes) -> int:
         addr = len(self.buf)
@@ -98,18 +99,20 @@ class _Writer:
         hdr = self._alloc(self._header([(0x0011, struct.pack("<QQ", btree, heap))]))
         return hdr, btree, heap
 
-    def finish(self, root) -> bytes:
+    def finish(self, root, version=0) -> bytes:
         hdr, btree, heap = root
-        sb = (b"\x89HDF\r\n\x1a\n" + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", 4, 16, 0)
-              + struct.pack("<QQQQ", 0, UNDEF, len(self.buf), UNDEF)
+        # version 1 adds the indexed-storage internal node K (2 bytes) and 2 reserved bytes
+        extra = struct.pack("<HH", 32, 0) if version == 1 else b""
+        sb = (b"\x89HDF\r\n\x1a\n" + bytes([version, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", 4, 16, 0)
+              + extra + struct.pack("<QQQQ", 0, UNDEF, len(self.buf), UNDEF)
               + struct.pack("<QQII", 0, hdr, 1, 0) + struct.pack("<QQ", btree, heap))
-        assert len(sb) == 96
-        self.buf[:96] = sb
+        assert len(sb) == self.sb_size
+        self.buf[:self.sb_size] = sb
         return bytes(self.buf)
 
 
-def write_h5(path: str, tree: dict) -> None:
-    w = _Writer()
+def write_h5(path: str, tree: dict, superblock_version: int = 0) -> None:
+    w = _Writer(100 if superblock_version == 1 else 96)
     root = w.group(tree)
     with open(path, "wb") as f:
-        f.write(w.finish(root))
+        f.write(w.finish(root, superblock_version))

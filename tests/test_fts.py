@@ -394,3 +394,23 @@ def test_grid_file_zones_on_two_gloo_ranks_equal_in_process(tmp_path):
         d = np.load(tmp_path / f"rank{r}.npz")
         assert np.array_equal(d["hist"], h)
         assert np.array_equal(d["q"][:, d["cells"]], q[:, d["cells"]])
+
+
+@pytest.mark.parametrize("version", [0, 1])
+def test_superblock_versions_and_damaged_files(tmp_path, version):
+    """Both superblock versions the library writes with default settings
+    read; a file cut short raises H5Error instead of misreading."""
+    from tests.h5write import write_h5
+
+    a = np.arange(1000, dtype=np.float64)
+    path = tmp_path / "x.h5"
+    write_h5(str(path), {"g": {"a": a, "n": np.array([7], np.int32)}}, superblock_version=version)
+    f = H5File(str(path))
+    assert np.array_equal(f.read("/g/a"), a) and int(f.read("/g/n")[0]) == 7
+    data = path.read_bytes()
+    cut = tmp_path / "cut.h5"
+    cut.write_bytes(data[: len(data) // 3])
+    with pytest.raises(H5Error):
+        g = H5File(str(cut))
+        g.read("/g/a")
+        g.read("/g/n")
