@@ -261,6 +261,24 @@ class _Zones:
         p = self.zones[0].params
         return force_coefficients(self.forces(), p.attackd, p.angleSlide, reference_area)
 
+    # -- restart ----------------------------------------------------------------
+    def DumpRestart(self, prefix: str):
+        """One restart file per zone this process drives, `prefix.zone<i>`
+        (i the zone's part number), as the reference writes one group per zone
+        (NSSolverUnstruct::DumpRestartH5, CFD/NSSolver/src/NSSolverUnstruct.cpp:1247)."""
+        for part, z in zip(self.parts, self.zones):
+            z.DumpRestart(f"{prefix}.zone{part.rank}")
+
+    def ReadRestart(self, prefix: str):
+        """Continues from DumpRestart's files of the same partition; the
+        interface ghosts are refreshed from the neighbours as after an update."""
+        for part, z in zip(self.parts, self.zones):
+            z.ReadRestart(f"{prefix}.zone{part.rank}")
+        steps = {z.step for z in self.zones}
+        if len(steps) != 1:
+            raise PhxError("the zones' restart files hold different steps: PHX_ERR_ARG")
+        self._exchange_state()
+
     def close(self):
         for z in self.zones:
             z.close()
